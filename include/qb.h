@@ -1,0 +1,173 @@
+/*
+ * qb.h -- C ABI of libqb, a B200 (sm_100a) replacement for the MD step of Q's
+ * qdyn (src/q6/md.f90:3917 md_run and everything it calls).
+ *
+ * The reference exposes no in-process interface: its boundary is the
+ * executable `qdyn[p] <file.inp>` (src/q6/qdyn.f90:18-134) plus its file
+ * contracts (.inp/.top/.fep/.re in, .en/.re/log out).  These entry points are
+ * what a host (ctypes from Python, or any FFI) binds to reproduce that
+ * executable in-process and to run many systems (lambda windows, replicas,
+ * spheres) together on one GPU.
+ *
+ * Conventions
+ *  - Every function returns an int status (enum qb_status); no exception or
+ *    longjmp crosses the ABI.  qb_last_error() returns the message of the last
+ *    failure on the calling thread.
+ *  - The library owns all host and device state.  Callers pass host buffers
+ *    they own; data moves only inside the get/set calls.
+ *  - Handles are not thread-safe; distinct handles may be used from distinct
+ *    threads.  One batch runs on one CUDA stream.
+ *  - Atom, system and state indices are 0-based.
+ */
+#ifndef QB_H
+#define QB_H
+
+#include <stddef.h>
+#include "qb_system.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  Each reference failure path named on the right. */
+enum qb_status {
+  QB_OK = 0,
+  QB_ERR_ARG = 1,           /* invalid argument */
+  QB_ERR_IO = 2,            /* cannot open/read/write a file (md.f90:1382 open_files) */
+  QB_ERR_PARSE = 3,         /* invalid .inp/.top/.fep/.re content (md.f90:2528, topo.f90:1073, qatom.f90:874) */
+  QB_ERR_UNSUPPORTED = 4,   /* valid Q input outside this engine's scope (PBC, arithmetic rule, EVB, ...) */
+  QB_ERR_SHAKE = 5,         /* SHAKE did not converge in 1000 iterations (md.f90:14533-14551 'shake failure') */
+  QB_ERR_NAN = 6,           /* non-finite energy or coordinate */
+  QB_ERR_LIST_OVERFLOW = 7, /* a pair list exceeded its device capacity */
+  QB_ERR_TIMEOUT = 8,       /* a bounded device wait gave up */
+  QB_ERR_CUDA = 9,          /* CUDA runtime error, or no usable GPU */
+  QB_ERR_STATE = 10         /* call not valid in the handle's current state */
+};
+
+/* Arithmetic mode of the per-step kernels. */
+enum qb_precision {
+  QB_FP64 = 0,   /* all pair math in FP64: the plain engine, parity mode */
+  QB_MIXED = 1   /* FP32 pair math, compensated FP64 energy/force sums; FP64 LRF, SHAKE, update */
+};
+
+typedef struct qb_options {
+  int precision;   /* enum qb_precision */
+  int device;      /* CUDA device ordinal */
+  int verbose;     /* 0 quiet, 1 print the qdyn-style setup log on stdout */
+  int reserved[5];
+} qb_options;
+
+typedef struct qb_handle qb_handle; /* one prepared system, host side */
+typedef struct qb_batch qb_batch;   /* device-resident systems stepped together */
+
+/* Library version string, e.g. "qb 0.1.0 (sm_100a)". */
+int qb_version(char *buf, size_t n);
+
+/* Message of the last failure on this thread ("" if none). */
+int qb_last_error(char *buf, size_t n);
+
+/* Number of usable CUDA devices (0 on a machine without a GPU). */
+int qb_device_count(int *out);
+
+/* ---------------------------------------------------------------- systems */
+
+/* Parse an .inp file and everything it names, and prepare the system exactly
+ * as qdyn does before its first step (qdyn.f90:80-96).  Host only: needs no GPU.
+ * Replaces: `qdyn <file.inp>` startup, src/q6/qdyn.f90:80-96. */
+int qb_open(const char *inp_path, const qb_options *opt, qb_handle **out);
+
+/* Same, with the [lambdas] and random_seed of the .inp overridden (n_lambda = 0
+ * or seed < 0 keeps the file's value).  Used to fan one .inp out into windows
+ * and replicas.  Replaces: editing md_X.inp per window (QligFEP qligfep.py:723). */
+int qb_open_override(const char *inp_path, const qb_options *opt,
+                     const double *lambdas, int n_lambda, int seed, qb_handle **out);
+
+/* Flat read-only view of the prepared system (valid until qb_close). */
+int qb_get_view(const qb_handle *h, qb_sysview *out);
+
+void qb_close(qb_handle *h);
+
+/* ------------------------------------------------------------------ batch */
+
+/* Upload n prepared systems to the GPU and compute their initial temperatures
+ * (md.f90:3960-3963).  All systems must share NBcycle. */
+int qb_batch_create(qb_handle *const *systems, int n, const qb_options *opt, qb_batch **out);
+
+/* Advance every system by nsteps MD steps with md_run's per-step semantics
+ * (md.f90:4003-4175): pair lists every NBcycle steps, potential and gradient,
+ * leapfrog with Berendsen scaling, SHAKE, temperature.  Energy summaries are
+ * recorded on the device at each system's output/energy intervals.
+ * Replaces: the `do istep` loop of md_run, src/q6/md.f90:4003-4175. */
+int qb_batch_run(qb_batch *b, int nsteps);
+
+/* The post-loop evaluation of md_run (md.f90:4186-4188): rebuild the lists and
+ * evaluate the potential at the final coordinates, for the FINAL summary. */
+int qb_batch_final_energy(qb_batch *b);
+
+/* Energies of system `sys` from the last potential evaluation.
+ * E_out: QB_NE doubles; EQ_out: nstates*QB_NEQ doubles (may be NULL). */
+int qb_batch_energies(qb_batch *b, int sys, double *E_out, double *EQ_out);
+
+/* Temperatures after the last step: out[0..4] = Temp, Tfree, Tfree_solute,
+ * Tfree_solvent, Tscale_solvent. */
+int qb_batch_temperature(qb_batch *b, int sys, double *out);
+
+/* Gradient dU/dx from the last potential evaluation, 3*natom doubles. */
+int qb_batch_gradient(qb_batch *b, int sys, double *d_out);
+
+int qb_batch_get_coords(qb_batch *b, int sys, double *x_out);
+int qb_batch_set_coords(qb_batch *b, int sys, const double *x_in);
+int qb_batch_get_velocities(qb_batch *b, int sys, double *v_out);
+int qb_batch_set_velocities(qb_batch *b, int sys, const double *v_in);
+
+/* Water polarisation shell corrections (float theta_corr, md.f90:15205). */
+int qb_batch_get_theta_corr(qb_batch *b, int sys, float *out, int n);
+
+/* Energy records gathered during qb_batch_run for system `sys`:
+ * count = number of records; steps[i], E[i*QB_NE...], EQ[i*nstates*QB_NEQ...],
+ * kin (E%kinetic at the record) included in E.  Buffers may be NULL to query
+ * the count.  kind: 0 = output summaries (iout_cycle), 1 = energy file (iene_cycle). */
+int qb_batch_history(qb_batch *b, int sys, int kind, int *count, int *steps,
+                     double *E, double *EQ);
+int qb_batch_clear_history(qb_batch *b);
+
+/* Per-system status (enum qb_status) raised on the device, e.g. QB_ERR_SHAKE. */
+int qb_batch_status(qb_batch *b, int sys, int *status);
+
+/* Kernel timing: when enabled, every kernel launch in qb_batch_run is bracketed
+ * with CUDA events on the batch stream.  names/ms/launches receive up to n
+ * entries (names as a '\n'-separated list). */
+int qb_batch_set_profiling(qb_batch *b, int on);
+int qb_batch_profile(qb_batch *b, char *names, size_t names_len, double *ms,
+                     long long *launches, int n, int *n_kernels);
+
+/* Device work totals of the last qb_batch_run (for roofline arithmetic):
+ * out[0] ww molecule pairs/step (sum over systems), out[1] pw pairs,
+ * out[2] pp pairs, out[3] qp pairs, out[4] qw (q, water) pairs, out[5] atoms,
+ * out[6] shake constraints, out[7] charge groups. */
+int qb_batch_workload(qb_batch *b, double *out, int n);
+
+void qb_batch_destroy(qb_batch *b);
+
+/* ------------------------------------------------------------------ files */
+
+/* Write a qdyn restart file: gfortran unformatted sequential records
+ * (nat3, x), (nat3, v), and (nshell, theta_corr) when nshell > 0.
+ * Replaces: write_xfin, src/q6/md.f90:15452-15470. */
+int qb_write_re(const char *path, int natom, const double *x, const double *v,
+                int nshell, const float *theta_corr);
+
+/* Append one energy-file frame: per state a record (int32 state, 15 doubles)
+ * and one empty off-diagonal record.  Replaces: put_ene, src/q6/nrgy.f90:94-119. */
+int qb_append_en(const char *path, int nstates, const double *EQ);
+
+/* Maxwell-Boltzmann velocities drawn exactly as qdyn draws them: gauss (12
+ * uniforms from randm) per component, sd = sqrt(boltz*T/mass), before initial
+ * shaking.  v_out: 3*natom doubles.
+ * Replaces: maxwell/gauss/randm, src/q6/md.f90:3787-3810, 1453-1469, 14408-14442. */
+int qb_maxwell(int seed, double temperature, int natom, const double *mass, double *v_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QB_H */

@@ -1,0 +1,31 @@
+/*
+ * qoracle.h -- CPU oracle of the Q MD step (TEST INFRASTRUCTURE ONLY: used by
+ * tests/, the smoke check and bench.py's CPU-baseline leg as the checker; the
+ * product never links it).  See qoracle.c.
+ */
+#ifndef QORACLE_H
+#define QORACLE_H
+#include "qb_system.h"
+
+typedef struct qo_state qo_state;
+
+/* Copy the prepared system's coordinates/velocities and compute the initial
+ * temperature, as md_run does before its loop. */
+qo_state *qo_create(const qb_sysview *s, int history_capacity);
+void qo_destroy(qo_state *st);
+/* nsteps passes of the md_run loop body; returns 0 or 5 (SHAKE failure). */
+int qo_run(qo_state *st, int nsteps);
+/* post-loop list rebuild and potential evaluation */
+int qo_final_energy(qo_state *st);
+void qo_energies(const qo_state *st, double *E, double *EQ);
+void qo_gradient(const qo_state *st, double *d);
+void qo_coords(const qo_state *st, double *x);
+void qo_velocities(const qo_state *st, double *v);
+void qo_set_coords(qo_state *st, const double *x);
+void qo_set_velocities(qo_state *st, const double *v);
+void qo_theta_corr(const qo_state *st, float *tc);
+void qo_temperature(const qo_state *st, double *out);
+int qo_history(const qo_state *st, int kind, int *steps, double *E, double *EQ);
+void qo_list_counts(const qo_state *st, int *out);
+int qo_status(const qo_state *st);
+#endif

@@ -1,0 +1,164 @@
+"""ctypes binding of libqb (include/qb.h).
+
+The shared library is built in-tree by ``q_b200/build.py`` (or
+``__graft_entry__.build()``) into ``q_b200/libqb.so``.  There is no fallback:
+if the library is missing, importing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(_HERE)
+LIB_PATH = os.environ.get("QB_LIBRARY", os.path.join(_HERE, "libqb.so"))
+INCLUDE = os.path.join(REPO, "include")
+
+QB_NE = 29
+QB_NEQ = 15
+QB_MAX_STATES = 10
+
+STATUS = {
+    0: "QB_OK", 1: "QB_ERR_ARG", 2: "QB_ERR_IO", 3: "QB_ERR_PARSE", 4: "QB_ERR_UNSUPPORTED",
+    5: "QB_ERR_SHAKE", 6: "QB_ERR_NAN", 7: "QB_ERR_LIST_OVERFLOW", 8: "QB_ERR_TIMEOUT",
+    9: "QB_ERR_CUDA", 10: "QB_ERR_STATE",
+}
+
+# Energy vector names in qb_energy_index order (nrgy.f90:43-49).
+E_NAMES = [
+    "potential", "kinetic", "LRF",
+    "p_bond", "p_angle", "p_torsion", "p_improper",
+    "w_bond", "w_angle", "w_torsion", "w_improper",
+    "q_bond", "q_angle", "q_torsion", "q_improper",
+    "pp_el", "pp_vdw", "pw_el", "pw_vdw", "ww_el", "ww_vdw", "qx_el", "qx_vdw",
+    "rst_total", "rst_fix", "rst_shell", "rst_protein", "rst_solvent_radial", "rst_water_pol",
+]
+EQ_NAMES = [
+    "lambda", "total", "bond", "angle", "torsion", "improper",
+    "qx_el", "qx_vdw", "qq_el", "qq_vdw", "qp_el", "qp_vdw", "qw_el", "qw_vdw", "restraint",
+]
+
+
+class QBError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def _struct_from_header(path: str, name: str) -> type:
+    """Build a ctypes.Structure for `typedef struct <name> {...} <name>;` by
+    reading the declaration in the public header, so the layout has a single
+    source of truth."""
+    src = open(path).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    m = re.search(r"typedef struct %s \{(.*?)\} %s;" % (name, name), src, flags=re.S)
+    if not m:
+        raise RuntimeError(f"{name} not found in {path}")
+    base = {"int": C.c_int, "double": C.c_double, "float": C.c_float,
+            "unsigned char": C.c_ubyte, "signed char": C.c_byte, "unsigned int": C.c_uint}
+    fields = []
+    for decl in m.group(1).split(";"):
+        decl = " ".join(decl.split())
+        if not decl:
+            continue
+        const = decl.startswith("const ")
+        if const:
+            decl = decl[6:]
+        tname = None
+        for t in sorted(base, key=len, reverse=True):
+            if decl.startswith(t + " ") or decl.startswith(t + "*"):
+                tname = t
+                break
+        if tname is None:
+            raise RuntimeError(f"unparsed field: {decl}")
+        rest = decl[len(tname):]
+        for item in rest.split(","):
+            item = item.strip()
+            ptr = item.startswith("*")
+            item = item.lstrip("*").strip()
+            arr = re.match(r"(\w+)\[(\d+)\]", item)
+            if arr:
+                fields.append((arr.group(1), base[tname] * int(arr.group(2))))
+            elif ptr:
+                fields.append((item, C.POINTER(base[tname])))
+            else:
+                fields.append((item, base[tname]))
+    return type(name, (C.Structure,), {"_fields_": fields})
+
+
+SysView = _struct_from_header(os.path.join(INCLUDE, "qb_system.h"), "qb_sysview")
+
+
+class Options(C.Structure):
+    _fields_ = [("precision", C.c_int), ("device", C.c_int), ("verbose", C.c_int),
+                ("reserved", C.c_int * 5)]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"libqb not built: {LIB_PATH} is missing (run `python -m q_b200.build`)")
+    lib = C.CDLL(LIB_PATH)
+    vp, ip, dp, fp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_float)
+    sig = {
+        "qb_version": (C.c_int, [C.c_char_p, C.c_size_t]),
+        "qb_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
+        "qb_device_count": (C.c_int, [ip]),
+        "qb_open": (C.c_int, [C.c_char_p, C.POINTER(Options), C.POINTER(vp)]),
+        "qb_open_override": (C.c_int, [C.c_char_p, C.POINTER(Options), dp, C.c_int, C.c_int,
+                                       C.POINTER(vp)]),
+        "qb_get_view": (C.c_int, [vp, C.POINTER(SysView)]),
+        "qb_close": (None, [vp]),
+        "qb_batch_create": (C.c_int, [C.POINTER(vp), C.c_int, C.POINTER(Options), C.POINTER(vp)]),
+        "qb_batch_run": (C.c_int, [vp, C.c_int]),
+        "qb_batch_final_energy": (C.c_int, [vp]),
+        "qb_batch_energies": (C.c_int, [vp, C.c_int, dp, dp]),
+        "qb_batch_temperature": (C.c_int, [vp, C.c_int, dp]),
+        "qb_batch_gradient": (C.c_int, [vp, C.c_int, dp]),
+        "qb_batch_get_coords": (C.c_int, [vp, C.c_int, dp]),
+        "qb_batch_set_coords": (C.c_int, [vp, C.c_int, dp]),
+        "qb_batch_get_velocities": (C.c_int, [vp, C.c_int, dp]),
+        "qb_batch_set_velocities": (C.c_int, [vp, C.c_int, dp]),
+        "qb_batch_get_theta_corr": (C.c_int, [vp, C.c_int, fp, C.c_int]),
+        "qb_batch_history": (C.c_int, [vp, C.c_int, C.c_int, ip, ip, dp, dp]),
+        "qb_batch_clear_history": (C.c_int, [vp]),
+        "qb_batch_status": (C.c_int, [vp, C.c_int, ip]),
+        "qb_batch_set_profiling": (C.c_int, [vp, C.c_int]),
+        "qb_batch_profile": (C.c_int, [vp, C.c_char_p, C.c_size_t, dp, C.POINTER(C.c_longlong),
+                                       C.c_int, ip]),
+        "qb_batch_workload": (C.c_int, [vp, dp, C.c_int]),
+        "qb_batch_destroy": (None, [vp]),
+        "qb_write_re": (C.c_int, [C.c_char_p, C.c_int, dp, dp, C.c_int, fp]),
+        "qb_append_en": (C.c_int, [C.c_char_p, C.c_int, dp]),
+        "qb_maxwell": (C.c_int, [C.c_int, C.c_double, C.c_int, dp, dp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(4096)
+    lib.qb_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        raise QBError(rc, last_error())
+
+
+def exported_symbols() -> list[str]:
+    """Names of every function declared in include/*.h."""
+    names = []
+    for h in sorted(os.listdir(INCLUDE)):
+        if h.endswith(".h"):
+            src = re.sub(r"/\*.*?\*/", "", open(os.path.join(INCLUDE, h)).read(), flags=re.S)
+            names += re.findall(r"^\s*(?:int|void)\s+\**\s*(qb_\w+)\s*\(", src, flags=re.M)
+    return names

@@ -1,0 +1,215 @@
+"""Python host API over libqb (the QligFEP-side driver of the engine).
+
+    sys = System.open("md.inp")                # parse + qdyn set-up (host only)
+    batch = Batch([sys1, sys2, ...])           # upload to the GPU
+    batch.run(1000)                            # md_run steps for every system
+    E, EQ = batch.energies(0)
+
+Energies are returned as dicts keyed by the names of the reference's energy
+types (nrgy.f90:43-58).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import E_NAMES, EQ_NAMES, QB_NE, QB_NEQ, Options, SysView, check, lib
+
+FP64 = 0
+MIXED = 1
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class System:
+    """One prepared system (qb_open)."""
+
+    def __init__(self, handle: C.c_void_p, path: str):
+        self._h = handle
+        self.path = path
+        self.view = SysView()
+        check(lib.qb_get_view(self._h, C.byref(self.view)))
+
+    @classmethod
+    def open(cls, inp_path: str, lambdas: Sequence[float] | None = None, seed: int = -1) -> "System":
+        h = C.c_void_p()
+        if lambdas is None and seed < 0:
+            check(lib.qb_open(inp_path.encode(), None, C.byref(h)))
+        else:
+            lam = np.ascontiguousarray(lambdas if lambdas is not None else [], dtype=np.float64)
+            check(lib.qb_open_override(inp_path.encode(), None, _dp(lam) if lam.size else None,
+                                       int(lam.size), int(seed), C.byref(h)))
+        return cls(h, inp_path)
+
+    @property
+    def natom(self) -> int:
+        return self.view.natom
+
+    @property
+    def nstates(self) -> int:
+        return self.view.nstates
+
+    def array(self, name: str, n: int | None = None, dtype=None) -> np.ndarray:
+        """Copy of a pointer field of the view (n elements)."""
+        ptr = getattr(self.view, name)
+        if n is None:
+            n = 3 * self.natom
+        return np.ctypeslib.as_array(ptr, shape=(n,)).copy()
+
+    def close(self) -> None:
+        if self._h:
+            lib.qb_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Systems stepped together on one GPU (qb_batch_*)."""
+
+    def __init__(self, systems: Sequence[System], precision: int = FP64, device: int = 0):
+        self.systems = list(systems)
+        arr = (C.c_void_p * len(self.systems))(*[s._h for s in self.systems])
+        opt = Options(precision=precision, device=device, verbose=0)
+        self._b = C.c_void_p()
+        check(lib.qb_batch_create(arr, len(self.systems), C.byref(opt), C.byref(self._b)))
+
+    def run(self, nsteps: int) -> None:
+        check(lib.qb_batch_run(self._b, int(nsteps)))
+
+    def final_energy(self) -> None:
+        check(lib.qb_batch_final_energy(self._b))
+
+    def energies(self, sys: int) -> tuple[dict, list[dict]]:
+        E = np.zeros(QB_NE)
+        S = self.systems[sys].nstates
+        EQ = np.zeros(max(S, 1) * QB_NEQ)
+        check(lib.qb_batch_energies(self._b, sys, _dp(E), _dp(EQ)))
+        return (dict(zip(E_NAMES, E.tolist())),
+                [dict(zip(EQ_NAMES, EQ[k * QB_NEQ:(k + 1) * QB_NEQ].tolist())) for k in range(S)])
+
+    def energy_vectors(self, sys: int) -> tuple[np.ndarray, np.ndarray]:
+        E = np.zeros(QB_NE)
+        S = self.systems[sys].nstates
+        EQ = np.zeros(max(S, 1) * QB_NEQ)
+        check(lib.qb_batch_energies(self._b, sys, _dp(E), _dp(EQ)))
+        return E, EQ[:S * QB_NEQ].reshape(S, QB_NEQ)
+
+    def temperature(self, sys: int) -> np.ndarray:
+        t = np.zeros(5)
+        check(lib.qb_batch_temperature(self._b, sys, _dp(t)))
+        return t
+
+    def _vec(self, fn, sys: int) -> np.ndarray:
+        out = np.zeros(3 * self.systems[sys].natom)
+        check(fn(self._b, sys, _dp(out)))
+        return out
+
+    def gradient(self, sys: int) -> np.ndarray:
+        return self._vec(lib.qb_batch_gradient, sys)
+
+    def coords(self, sys: int) -> np.ndarray:
+        return self._vec(lib.qb_batch_get_coords, sys)
+
+    def velocities(self, sys: int) -> np.ndarray:
+        return self._vec(lib.qb_batch_get_velocities, sys)
+
+    def set_coords(self, sys: int, x: np.ndarray) -> None:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        check(lib.qb_batch_set_coords(self._b, sys, _dp(x)))
+
+    def set_velocities(self, sys: int, v: np.ndarray) -> None:
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        check(lib.qb_batch_set_velocities(self._b, sys, _dp(v)))
+
+    def theta_corr(self, sys: int, n: int = 4) -> np.ndarray:
+        out = np.zeros(n, dtype=np.float32)
+        check(lib.qb_batch_get_theta_corr(self._b, sys, out.ctypes.data_as(C.POINTER(C.c_float)), n))
+        return out
+
+    def history(self, sys: int, kind: int = 0):
+        """(steps, E[n, QB_NE], EQ[n, S, QB_NEQ]) recorded during run()."""
+        cnt = C.c_int()
+        check(lib.qb_batch_history(self._b, sys, kind, C.byref(cnt), None, None, None))
+        n = cnt.value
+        S = self.systems[sys].nstates
+        steps = np.zeros(max(n, 1), dtype=np.int32)
+        E = np.zeros((max(n, 1), QB_NE))
+        EQ = np.zeros((max(n, 1), max(S, 1), QB_NEQ))
+        check(lib.qb_batch_history(self._b, sys, kind, C.byref(cnt),
+                                   steps.ctypes.data_as(C.POINTER(C.c_int)), _dp(E), _dp(EQ)))
+        return steps[:n], E[:n], EQ[:n, :S]
+
+    def clear_history(self) -> None:
+        check(lib.qb_batch_clear_history(self._b))
+
+    def set_profiling(self, on: bool) -> None:
+        check(lib.qb_batch_set_profiling(self._b, 1 if on else 0))
+
+    def profile(self) -> dict:
+        n = 64
+        names = C.create_string_buffer(8192)
+        ms = np.zeros(n)
+        launches = np.zeros(n, dtype=np.int64)
+        nk = C.c_int()
+        check(lib.qb_batch_profile(self._b, names, len(names), _dp(ms),
+                                   launches.ctypes.data_as(C.POINTER(C.c_longlong)), n, C.byref(nk)))
+        keys = names.value.decode().split("\n")[:nk.value]
+        return {k: (float(ms[i]), int(launches[i])) for i, k in enumerate(keys)}
+
+    def workload(self) -> np.ndarray:
+        out = np.zeros(8)
+        check(lib.qb_batch_workload(self._b, _dp(out), 8))
+        return out
+
+    def status(self, sys: int) -> int:
+        st = C.c_int()
+        check(lib.qb_batch_status(self._b, sys, C.byref(st)))
+        return st.value
+
+    def close(self) -> None:
+        if self._b:
+            lib.qb_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def device_count() -> int:
+    n = C.c_int()
+    lib.qb_device_count(C.byref(n))
+    return n.value
+
+
+def write_restart(path: str, x: np.ndarray, v: np.ndarray, theta_corr: np.ndarray | None = None) -> None:
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    ns = 0 if theta_corr is None else int(theta_corr.size)
+    tc = None if theta_corr is None else np.ascontiguousarray(theta_corr, dtype=np.float32)
+    check(lib.qb_write_re(path.encode(), x.size // 3, _dp(x), _dp(v), ns,
+                          tc.ctypes.data_as(C.POINTER(C.c_float)) if tc is not None else None))
+
+
+def append_energy(path: str, EQ: np.ndarray) -> None:
+    EQ = np.ascontiguousarray(EQ, dtype=np.float64)
+    check(lib.qb_append_en(path.encode(), EQ.shape[0] if EQ.ndim == 2 else 0, _dp(EQ)))
+
+
+def maxwell(seed: int, temperature: float, mass: np.ndarray) -> np.ndarray:
+    mass = np.ascontiguousarray(mass, dtype=np.float64)
+    out = np.zeros(3 * mass.size)
+    check(lib.qb_maxwell(int(seed), float(temperature), mass.size, _dp(mass), _dp(out)))
+    return out

@@ -9,10 +9,6 @@
 
 #include "qsystem.hpp"
 
-struct qb_handle {
-  qb::System sys;
-};
-
 namespace qb {
 thread_local std::string g_last_error;
 void set_error(const std::string &m) { g_last_error = m; }

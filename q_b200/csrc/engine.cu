@@ -1,0 +1,824 @@
+// engine.cu -- device engine of libqb: packs prepared systems into one batch
+// on the GPU and runs md_run's step loop (src/q6/md.f90:4003-4175) with the
+// kernels of kernels.cuh.  Batch entry points of the C ABI (include/qb.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "qsystem.hpp"
+
+namespace qb {
+void set_error(const std::string &m);
+
+#define CUDA_TRY(call)                                                                     \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess) ::qb::fail(QB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class T>
+T *dev_upload(const std::vector<T> &h, std::vector<void *> &owned) {
+  size_t n = std::max<size_t>(h.size(), 1);
+  T *p = nullptr;
+  CUDA_TRY(cudaMalloc(&p, n * sizeof(T)));
+  owned.push_back(p);
+  if (!h.empty()) CUDA_TRY(cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  else CUDA_TRY(cudaMemset(p, 0, sizeof(T)));
+  return p;
+}
+
+template <class T>
+T *dev_alloc(size_t n, std::vector<void *> &owned) {
+  n = std::max<size_t>(n, 1);
+  T *p = nullptr;
+  CUDA_TRY(cudaMalloc(&p, n * sizeof(T)));
+  owned.push_back(p);
+  CUDA_TRY(cudaMemset(p, 0, n * sizeof(T)));
+  return p;
+}
+
+struct KernelStat { double ms = 0; long long launches = 0; };
+
+struct Batch {
+  int nsys = 0;
+  qb_options opt{};
+  std::vector<const System *> systems;
+  std::vector<qb_sysview> views;
+  std::vector<SysDev> sysh;
+  DevPtrs P{};
+  std::vector<void *> owned;
+  cudaStream_t stream = nullptr;
+  int NB = 1;
+  long long istep = 0;
+  int max_natom = 0, max_nwat = 0, max_ncgp_sol = 0, max_terms = 0, max_pp = 0, max_pw = 0, max_qp = 0;
+  bool any_lrf = false, any_q = false, any_shake = false, any_wpol = false, any_prestr = false, any_qq = false,
+       any_qb = false;
+  size_t watpol_smem = 0;
+  // profiling
+  bool profiling = false;
+  std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+  std::vector<cudaEvent_t> event_pool;
+  std::map<std::string, KernelStat> stats;
+  std::vector<std::string> order;
+  double workload[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+
+  ~Batch() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto &e : event_pool) cudaEventDestroy(e);
+    for (auto &pe : pending) { cudaEventDestroy(pe.second.first); cudaEventDestroy(pe.second.second); }
+    for (void *p : owned) cudaFree(p);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  cudaEvent_t take_event() {
+    if (!event_pool.empty()) { auto e = event_pool.back(); event_pool.pop_back(); return e; }
+    cudaEvent_t e;
+    CUDA_TRY(cudaEventCreate(&e));
+    return e;
+  }
+
+  template <class F>
+  void launch(const char *name, F &&f) {
+    if (!profiling) { f(); return; }
+    cudaEvent_t a = take_event(), b = take_event();
+    CUDA_TRY(cudaEventRecord(a, stream));
+    f();
+    CUDA_TRY(cudaEventRecord(b, stream));
+    pending.push_back({name, {a, b}});
+    if (pending.size() > 4096) collect();
+  }
+
+  void collect() {
+    CUDA_TRY(cudaStreamSynchronize(stream));
+    for (auto &pe : pending) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, pe.second.first, pe.second.second);
+      auto it = stats.find(pe.first);
+      if (it == stats.end()) { order.push_back(pe.first); it = stats.emplace(pe.first, KernelStat{}).first; }
+      it->second.ms += ms;
+      it->second.launches++;
+      event_pool.push_back(pe.second.first);
+      event_pool.push_back(pe.second.second);
+    }
+    pending.clear();
+  }
+
+  void check_launch(const char *what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) fail(QB_ERR_CUDA, std::string("launch of ") + what + ": " + cudaGetErrorString(e));
+  }
+
+  static int cdiv(long long a, long long b) { return (int)std::max<long long>(1, (a + b - 1) / b); }
+
+  void build_lists() {
+    DevPtrs &p = P;
+    dim3 b256(256);
+    if (any_lrf)
+      launch("cgp_centers", [&] { k_cgp_centers<<<cdiv(p.ncgp_tot, 256), b256, 0, stream>>>(p); });
+    launch("lists_begin", [&] { k_lists_begin<<<cdiv(nsys, 128), 128, 0, stream>>>(p); });
+    if (max_ncgp_sol > 0) {
+      launch("list_pp", [&] { k_list_pp<<<dim3(max_ncgp_sol, nsys), 128, 0, stream>>>(p); });
+      if (max_nwat > 0) launch("list_pw", [&] { k_list_pw<<<dim3(max_ncgp_sol, nsys), 256, 0, stream>>>(p); });
+    }
+    if (any_q) {
+      launch("list_qp", [&] { k_list_qp<<<nsys, 256, 0, stream>>>(p, 0); });
+      if (max_nwat > 0) launch("list_qw", [&] { k_list_qw<<<nsys, 256, 0, stream>>>(p, 0); });
+    }
+    if (max_nwat > 0) launch("list_ww", [&] { k_list_ww<<<dim3(cdiv(max_nwat, 8), nsys), 256, 0, stream>>>(p); });
+    if (any_lrf)
+      launch("lrf_gather", [&] { k_lrf_gather<<<cdiv((long long)p.ncgp_tot * 32, 128), 128, 0, stream>>>(p); });
+    launch("lists_end", [&] { k_lists_end<<<cdiv(nsys, 128), 128, 0, stream>>>(p); });
+    check_launch("list kernels");
+  }
+
+  void pot_energy() {
+    DevPtrs &p = P;
+    CUDA_TRY(cudaMemsetAsync(p.d, 0, sizeof(double4) * (size_t)p.natoms_tot, stream));
+    CUDA_TRY(cudaMemsetAsync(p.E, 0, sizeof(double) * QB_NE * (size_t)nsys, stream));
+    CUDA_TRY(cudaMemsetAsync(p.EQ, 0, sizeof(double) * MAXS * QB_NEQ * (size_t)nsys, stream));
+    if (max_pp > 0)
+      launch("nb_pp", [&] { k_nb_pair<true><<<dim3(std::min(cdiv(max_pp, 256), 64), nsys), 256, 0, stream>>>(p); });
+    if (max_pw > 0)
+      launch("nb_pw", [&] { k_nb_pair<false><<<dim3(std::min(cdiv(max_pw, 256), 128), nsys), 256, 0, stream>>>(p); });
+    if (any_q && max_qp > 0)
+      launch("nb_qp", [&] { k_nb_qp<<<dim3(std::min(cdiv(max_qp, 256), 32), nsys), 256, 0, stream>>>(p); });
+    if (max_nwat > 0) {
+      launch("nb_ww", [&] { k_nb_ww<<<dim3(cdiv(max_nwat, 8), nsys), 256, 0, stream>>>(p); });
+      if (any_q) launch("nb_qw", [&] { k_nb_qw<<<dim3(cdiv(max_nwat, 128), nsys), 128, 0, stream>>>(p); });
+    }
+    if (any_lrf)
+      launch("lrf_taylor", [&] { k_lrf_taylor<<<dim3(cdiv(max_natom, 256), nsys), 256, 0, stream>>>(p); });
+    if (max_terms > 0)
+      launch("bonded", [&] { k_bonded<<<dim3(cdiv(max_terms, 256), nsys), 256, 0, stream>>>(p); });
+    launch("restrain_atoms", [&] { k_restrain_atoms<<<dim3(cdiv(max_natom, 256), nsys), 256, 0, stream>>>(p); });
+    if (any_prestr) launch("prestrain", [&] { k_prestrain<<<nsys, 256, 0, stream>>>(p); });
+    if (any_wpol) launch("watpol", [&] { k_watpol<<<nsys, 1024, watpol_smem, stream>>>(p); });
+    if (any_qq) launch("nb_qq", [&] { k_nb_qq<<<nsys, 128, 0, stream>>>(p); });
+    if (any_qb) launch("qbonded", [&] { k_qbonded<<<nsys, 128, 0, stream>>>(p); });
+    launch("finalize_energy", [&] { k_finalize_energy<<<cdiv(nsys, 128), 128, 0, stream>>>(p); });
+    check_launch("force kernels");
+  }
+
+  void step() {
+    DevPtrs &p = P;
+    if (istep % NB == 0) build_lists();
+    pot_energy();
+    launch("leapfrog", [&] { k_leapfrog<<<cdiv(p.natoms_tot, 256), 256, 0, stream>>>(p); });
+    if (any_shake && p.nshake_tot > 0)
+      launch("shake", [&] { k_shake<<<cdiv(p.nshake_tot, 128), 128, 0, stream>>>(p); });
+    launch("finish", [&] { k_finish<<<nsys, 512, 0, stream>>>(p, 1); });
+    check_launch("step kernels");
+    istep++;
+  }
+
+  void sync_status() {
+    CUDA_TRY(cudaStreamSynchronize(stream));
+    std::vector<SysState> st(nsys);
+    CUDA_TRY(cudaMemcpy(st.data(), P.st, sizeof(SysState) * nsys, cudaMemcpyDeviceToHost));
+    for (int s = 0; s < nsys; s++)
+      if (st[s].status != 0) {
+        char buf[160];
+        std::snprintf(buf, sizeof buf, "system %d raised status %d on the device at step %d", s, st[s].status,
+                      st[s].istep);
+        fail(st[s].status, buf);
+      }
+  }
+};
+
+// ------------------------------------------------------------- packing
+
+namespace {
+
+double d2(const double *x, int a, int b) {
+  double s = 0;
+  for (int k = 0; k < 3; k++) { double t = x[3 * a + k] - x[3 * b + k]; s += t * t; }
+  return s;
+}
+
+void build(Batch &B, qb_handle *const *hs, int n) {
+  B.nsys = n;
+  B.views.resize(n);
+  for (int s = 0; s < n; s++) {
+    B.systems.push_back(&hs[s]->sys);
+    hs[s]->sys.fill_view(&B.views[s]);
+  }
+  B.NB = B.views[0].NBcycle;
+  for (auto &v : B.views)
+    if (v.NBcycle != B.NB) fail(QB_ERR_ARG, "all systems of a batch must share the non_bond interval");
+
+  // host staging
+  std::vector<double4> x, v, d0;
+  std::vector<float> crg, winv;
+  std::vector<double> mass, lja, ljb, xtop;
+  std::vector<int> iac, iq, cgp, asys;
+  std::vector<uint8_t> flags, ljcod;
+  std::vector<uint32_t> lx, l14;
+  std::vector<int2> exl, l14l;
+  std::vector<int> cg_first, cg_last, cg_sw, cg_atoms, cg_sys;
+  std::vector<int> iqseq, qiac;
+  std::vector<float> qcrg;
+  std::vector<double> qavdw, qbvdw, sc, qq_el;
+  std::vector<int8_t> qconn;
+  std::vector<int4> qq;
+  std::vector<int2> bij; std::vector<double2> bpar;
+  std::vector<int4> aijk; std::vector<double2> apar;
+  std::vector<int4> tijkl; std::vector<float4> tpar;
+  std::vector<int4> iijkl; std::vector<float2> ipar;
+  std::vector<int2> qbij; std::vector<uint8_t> qb_on; std::vector<double4> qbpar;
+  std::vector<int4> qaijk; std::vector<uint8_t> qa_on; std::vector<double2> qapar;
+  std::vector<int4> qtijkl; std::vector<uint8_t> qt_on; std::vector<double4> qtpar;
+  std::vector<int4> qiijkl; std::vector<uint8_t> qi_on; std::vector<double2> qipar;
+  std::vector<int> sh_first, sh_n, sh_sys; std::vector<int2> sh_ij; std::vector<double> sh_d2;
+  std::vector<int4> rs; std::vector<double> rs_fk;
+  std::vector<int2> rp; std::vector<double> rp_x, rp_fk;
+  std::vector<int4> rd; std::vector<double4> rd_p;
+  std::vector<int4> ra; std::vector<double2> ra_p;
+  std::vector<int4> rw; std::vector<double4> rw_p;
+  std::vector<SysState> sst(n);
+  B.sysh.resize(n);
+  int ww_cap = 64;
+  long long pp_tot = 0, pw_tot = 0, qp_tot = 0, qw_tot = 0;
+
+  for (int s = 0; s < n; s++) {
+    const qb_sysview &V = B.views[s];
+    SysDev &S = B.sysh[s];
+    std::memset(&S, 0, sizeof S);
+    if (V.nstates > MAXS) fail(QB_ERR_UNSUPPORTED, "too many states");
+    if (V.iuse_switch_atom != 1) fail(QB_ERR_UNSUPPORTED, "charge-group cut-offs on any atom are not supported");
+    const int aoff = (int)x.size();
+    S.aoff = aoff; S.natom = V.natom; S.nsol = V.nat_solute; S.nwat = V.nwat;
+    S.woff = 0;
+    S.coff = (int)cg_first.size(); S.ncgp = V.ncgp; S.ncgp_sol = V.ncgp_solute;
+    S.qoff = (int)iqseq.size(); S.nq = V.nqat; S.S = V.nstates; S.natyps = V.natyps;
+    S.ljoff = (int)ljcod.size(); S.qlib_off = (int)qavdw.size(); S.sc_off = (int)sc.size();
+    S.qconn_off = (int)qconn.size();
+    for (int i = 0; i < V.natom; i++) {
+      x.push_back(make_double4(V.x0[3 * i], V.x0[3 * i + 1], V.x0[3 * i + 2], 0));
+      v.push_back(make_double4(V.v0[3 * i], V.v0[3 * i + 1], V.v0[3 * i + 2], 0));
+      for (int k = 0; k < 3; k++) xtop.push_back(V.xtop[3 * i + k]);
+      crg.push_back(V.crg[i]);
+      winv.push_back(V.winv[i]);
+      mass.push_back(V.mass[i]);
+      int t = V.iac[i];
+      iac.push_back(t);
+      for (int k = 0; k < 3; k++) { lja.push_back(V.type_avdw[3 * t + k]); ljb.push_back(V.type_bvdw[3 * t + k]); }
+      iq.push_back(V.iqatom[i]);
+      cgp.push_back(S.coff + V.iwhich_cgp[i]);
+      asys.push_back(s);
+      flags.push_back((V.excl[i] ? F_EXCL : 0) | (V.shell[i] ? F_SHELL : 0) | (V.heavy[i] ? F_HEAVY : 0));
+      lx.push_back(i < V.nat_solute ? V.listex_bits[i] : 0u);
+      l14.push_back(i < V.nat_solute ? V.list14_bits[i] : 0u);
+    }
+    for (int k = 0; k < V.natyps * V.natyps; k++) ljcod.push_back(V.ljcod[k]);
+    S.exl_off = (int)exl.size(); S.nexl = V.nexlong;
+    for (int k = 0; k < V.nexlong; k++) exl.push_back(make_int2(V.listexlong[2 * k], V.listexlong[2 * k + 1]));
+    S.l14_off = (int)l14l.size(); S.nl14 = V.n14long;
+    for (int k = 0; k < V.n14long; k++) l14l.push_back(make_int2(V.list14long[2 * k], V.list14long[2 * k + 1]));
+    for (int g = 0; g < V.ncgp; g++) {
+      cg_first.push_back((int)cg_atoms.size() + (V.cgp_first[g] - V.cgp_first[0]));
+      cg_last.push_back((int)cg_atoms.size() + (V.cgp_last[g] - V.cgp_first[0]));
+      cg_sw.push_back(aoff + V.cgp_iswitch[g]);
+      cg_sys.push_back(s);
+    }
+    for (int a = 0; a < V.natom; a++) cg_atoms.push_back(aoff + V.cgpatom[a]);
+    // water groups must be O,H,H with the oxygen as switching atom
+    for (int iw = 0; iw < V.nwat; iw++) {
+      int g = V.ncgp_solute + iw;
+      int o = V.nat_solute + 3 * iw;
+      if (g >= V.ncgp || V.cgp_iswitch[g] != o || V.iwhich_cgp[o] != g)
+        fail(QB_ERR_UNSUPPORTED, "water charge groups must follow the solute groups, one per water, switching on O");
+    }
+    // Q atoms
+    for (int q = 0; q < V.nqat; q++) {
+      iqseq.push_back(aoff + V.iqseq[q]);
+      for (int st = 0; st < MAXS; st++) {
+        qcrg.push_back(st < V.nstates ? V.qcrg[q * V.nstates + st] : 0.0f);
+        qiac.push_back(st < V.nstates ? V.qiac[q * V.nstates + st] : 0);
+      }
+    }
+    for (int k = 0; k < V.nqlib * 3; k++) { qavdw.push_back(V.qavdw[k]); qbvdw.push_back(V.qbvdw[k]); }
+    size_t nsc = (size_t)V.nqat * (V.natyps + V.nqat) * V.nstates;
+    for (size_t k = 0; k < nsc; k++) sc.push_back(V.sc_lookup[k]);
+    size_t nqc = (size_t)V.nstates * V.nat_solute * V.nqat;
+    for (size_t k = 0; k < nqc; k++) qconn.push_back(V.qconn[k]);
+    S.qq_off = (int)qq.size();
+    for (int st = 0; st < V.nstates; st++)
+      for (int k = V.nbqq_off[st]; k < V.nbqq_off[st] + V.nbqq_count[st]; k++) {
+        int jq = V.nbqq_jq[k];
+        qq.push_back(make_int4(S.qoff + V.nbqq_iq[k], aoff + V.nbqq_j[k], jq >= 0 ? S.qoff + jq : -1,
+                               V.nbqq_ljcod[k] | (st << 8)));
+        qq_el.push_back(V.nbqq_el_scale[k]);
+      }
+    S.nqq = (int)qq.size() - S.qq_off;
+    // bonded terms
+    S.b_off = (int)bij.size(); S.nb = V.nbonds; S.nb_sol = V.nbonds_solute;
+    for (int k = 0; k < V.nbonds; k++) {
+      bij.push_back(make_int2(aoff + V.bnd_i[k], aoff + V.bnd_j[k]));
+      bpar.push_back(make_double2(V.bnd_fk[k], V.bnd_b0[k]));
+    }
+    S.a_off = (int)aijk.size(); S.na = V.nangles; S.na_sol = V.nangles_solute;
+    for (int k = 0; k < V.nangles; k++) {
+      aijk.push_back(make_int4(aoff + V.ang_i[k], aoff + V.ang_j[k], aoff + V.ang_k[k], 0));
+      apar.push_back(make_double2(V.ang_fk[k], V.ang_th0[k]));
+    }
+    S.t_off = (int)tijkl.size(); S.nt = V.ntors; S.nt_sol = V.ntors_solute;
+    for (int k = 0; k < V.ntors; k++) {
+      tijkl.push_back(make_int4(aoff + V.tor_i[k], aoff + V.tor_j[k], aoff + V.tor_k[k], aoff + V.tor_l[k]));
+      tpar.push_back(make_float4(V.tor_fk[k], V.tor_rmult[k], V.tor_deltor[k], V.tor_paths[k]));
+    }
+    S.i_off = (int)iijkl.size(); S.ni = V.nimps; S.ni_sol = V.nimps_solute;
+    for (int k = 0; k < V.nimps; k++) {
+      iijkl.push_back(make_int4(aoff + V.imp_i[k], aoff + V.imp_j[k], aoff + V.imp_k[k], aoff + V.imp_l[k]));
+      ipar.push_back(make_float2(V.imp_fk[k], V.imp_imp0[k]));
+    }
+    const int NSt = V.nstates;
+    S.qb_off = (int)qbij.size(); S.nqb = V.nqbond;
+    for (int k = 0; k < V.nqbond; k++) {
+      qbij.push_back(make_int2(aoff + V.qbnd_i[k], aoff + V.qbnd_j[k]));
+      for (int st = 0; st < MAXS; st++) {
+        bool on = st < NSt && V.qbnd_on[k * NSt + st];
+        qb_on.push_back(on);
+        qbpar.push_back(on ? make_double4(V.qbnd_Dmz[k * NSt + st], V.qbnd_amz[k * NSt + st], V.qbnd_r0[k * NSt + st],
+                                          V.qbnd_fk[k * NSt + st])
+                           : make_double4(0, 0, 0, 0));
+      }
+    }
+    S.qa_off = (int)qaijk.size(); S.nqa = V.nqangle;
+    for (int k = 0; k < V.nqangle; k++) {
+      qaijk.push_back(make_int4(aoff + V.qang_i[k], aoff + V.qang_j[k], aoff + V.qang_k[k], 0));
+      for (int st = 0; st < MAXS; st++) {
+        bool on = st < NSt && V.qang_on[k * NSt + st];
+        qa_on.push_back(on);
+        qapar.push_back(on ? make_double2(V.qang_fk[k * NSt + st], V.qang_th0[k * NSt + st]) : make_double2(0, 0));
+      }
+    }
+    S.qt_off = (int)qtijkl.size(); S.nqt = V.nqtor;
+    for (int k = 0; k < V.nqtor; k++) {
+      qtijkl.push_back(make_int4(aoff + V.qtor_i[k], aoff + V.qtor_j[k], aoff + V.qtor_k[k], aoff + V.qtor_l[k]));
+      for (int st = 0; st < MAXS; st++) {
+        bool on = st < NSt && V.qtor_on[k * NSt + st];
+        qt_on.push_back(on);
+        qtpar.push_back(on ? make_double4(V.qtor_fk[k * NSt + st], V.qtor_rmult[k * NSt + st], V.qtor_deltor[k * NSt + st], 0)
+                           : make_double4(0, 0, 0, 0));
+      }
+    }
+    S.qi_off = (int)qiijkl.size(); S.nqi = V.nqimp;
+    for (int k = 0; k < V.nqimp; k++) {
+      qiijkl.push_back(make_int4(aoff + V.qimp_i[k], aoff + V.qimp_j[k], aoff + V.qimp_k[k], aoff + V.qimp_l[k]));
+      for (int st = 0; st < MAXS; st++) {
+        bool on = st < NSt && V.qimp_on[k * NSt + st];
+        qi_on.push_back(on);
+        qipar.push_back(on ? make_double2(V.qimp_fk[k * NSt + st], V.qimp_imp0[k * NSt + st]) : make_double2(0, 0));
+      }
+    }
+    // shake molecules
+    S.sh_off = (int)sh_first.size(); S.nsh = V.shake_molecules;
+    for (int m = 0; m < V.shake_molecules; m++) {
+      sh_first.push_back((int)sh_ij.size() + (V.shake_mol_first[m] - (V.shake_molecules ? V.shake_mol_first[0] : 0)));
+      sh_n.push_back(V.shake_mol_n[m]);
+      sh_sys.push_back(s);
+    }
+    for (int c = 0; c < V.shake_constraints; c++) {
+      sh_ij.push_back(make_int2(aoff + V.shake_i[c], aoff + V.shake_j[c]));
+      sh_d2.push_back(V.shake_dist2[c]);
+    }
+    S.has_shake = V.shake_constraints > 0;
+    // restraints
+    S.rs_off = (int)rs.size(); S.nrs = V.nrstr_seq;
+    for (int r = 0; r < V.nrstr_seq; r++) {
+      rs.push_back(make_int4(aoff + V.rseq_i[r], aoff + V.rseq_j[r], V.rseq_ih[r], V.rseq_to_center[r]));
+      rs_fk.push_back(V.rseq_fk[r]);
+    }
+    S.rp_off = (int)rp.size(); S.nrp = V.nrstr_pos;
+    for (int r = 0; r < V.nrstr_pos; r++) {
+      rp.push_back(make_int2(aoff + V.rpos_i[r], V.rpos_ipsi[r]));
+      for (int k = 0; k < 3; k++) { rp_x.push_back(V.rpos_x[3 * r + k]); rp_fk.push_back(V.rpos_fk[3 * r + k]); }
+    }
+    S.rd_off = (int)rd.size(); S.nrd = V.nrstr_dist;
+    for (int r = 0; r < V.nrstr_dist; r++) {
+      rd.push_back(make_int4(aoff + V.rdis_i[r], aoff + V.rdis_j[r], V.rdis_ipsi[r], 0));
+      rd_p.push_back(make_double4(V.rdis_d1[r], V.rdis_d2[r], V.rdis_fk[r], 0));
+    }
+    S.ra_off = (int)ra.size(); S.nra = V.nrstr_angl;
+    for (int r = 0; r < V.nrstr_angl; r++) {
+      ra.push_back(make_int4(aoff + V.rang_i[r], aoff + V.rang_j[r], aoff + V.rang_k[r], V.rang_ipsi[r]));
+      ra_p.push_back(make_double2(V.rang_ang[r], V.rang_fk[r]));
+    }
+    S.rw_off = (int)rw.size(); S.nrw = V.nrstr_wall;
+    for (int r = 0; r < V.nrstr_wall; r++) {
+      rw.push_back(make_int4(aoff + V.rwal_i[r], aoff + V.rwal_j[r], V.rwal_ih[r], 0));
+      rw_p.push_back(make_double4(V.rwal_d[r], V.rwal_fk[r], V.rwal_aMorse[r], V.rwal_dMorse[r]));
+    }
+    // scalars
+    S.ff_type = V.ff_type; S.use_lrf = V.use_LRF; S.qvdw = V.qvdw_flag;
+    S.wpol = V.wpol_restr && V.nwpolr_shell > 0; S.nshell = V.nwpolr_shell;
+    if (S.nshell > MAX_SHELLS) fail(QB_ERR_UNSUPPORTED, "too many water polarisation shells");
+    S.iac_ow = V.iac_ow; S.separate_scaling = V.separate_scaling; S.detail_temps = V.detail_temps;
+    S.qp_once = V.Rcq > V.rexcl_o;
+    S.iout = V.iout_cycle; S.iene = V.iene_cycle; S.NB = V.NBcycle;
+    S.Ndegf = V.Ndegf; S.Ndegfree = V.Ndegfree; S.Ndegfree_sol = V.Ndegfree_solute; S.Ndegfree_solv = V.Ndegfree_solvent;
+    S.dt = V.dt; S.Temp0 = V.Temp0; S.tau_T = V.tau_T; S.el14 = V.el14_scale; S.A_OO = V.A_OO; S.B_OO = V.B_OO;
+    S.Rcpp2 = V.Rcpp * V.Rcpp; S.Rcpw2 = V.Rcpw * V.Rcpw; S.Rcww2 = V.Rcww * V.Rcww; S.Rcq2 = V.Rcq * V.Rcq;
+    S.RcLRF2 = V.RcLRF * V.RcLRF;
+    S.crg_ow = V.crg_ow; S.crg_hw = V.crg_hw;
+    for (int k = 0; k < 3; k++) { S.xp[k] = V.xpcent[k]; S.xw[k] = V.xwcent[k]; }
+    S.rwat = V.rwat; S.fk_ws = V.fk_wsphere; S.Dwmz = V.Dwmz; S.awmz = V.awmz; S.fkwpol = V.fkwpol;
+    S.fk_pshell = V.fk_pshell; S.fk_fix = V.fk_fix;
+    for (int k = 0; k < S.nshell; k++) { S.ws_rout[k] = V.wshell_rout[k]; S.ws_dr[k] = V.wshell_dr[k]; S.ws_cstb[k] = V.wshell_cstb[k]; }
+    for (int k = 0; k < V.nstates; k++) S.lambda[k] = V.lambda[k];
+    if (V.nwat > 0) {
+      S.aO[0] = V.type_avdw[3 * V.iac_ow]; S.aO[1] = V.type_avdw[3 * V.iac_ow + 1];
+      S.bO[0] = V.type_bvdw[3 * V.iac_ow]; S.bO[1] = V.type_bvdw[3 * V.iac_ow + 1];
+    }
+    SysState &st = sst[s];
+    std::memset(&st, 0, sizeof st);
+    st.Tscale_sol = st.Tscale_solv = 1.0;
+    for (int k = 0; k < S.nshell; k++) st.theta_corr[k] = V.wshell_theta_corr0[k];
+    // list capacities from the starting coordinates, with margins for motion
+    {
+      const double *X = V.x0;
+      long long pp = 0, pw = 0;
+      double rpp = V.Rcpp + 3.0, rpw = V.Rcpw + 3.0, rww = V.Rcww + 2.0;
+      for (int ig = 0; ig < V.ncgp_solute; ig++) {
+        int si = V.cgp_iswitch[ig];
+        int na = V.cgp_last[ig] - V.cgp_first[ig] + 1;
+        for (int jg = ig; jg < V.ncgp_solute; jg++) {
+          int sj = V.cgp_iswitch[jg];
+          if (d2(X, si, sj) <= rpp * rpp) pp += (long long)na * (V.cgp_last[jg] - V.cgp_first[jg] + 1);
+        }
+        for (int iw = 0; iw < V.nwat; iw++)
+          if (d2(X, si, V.nat_solute + 3 * iw) <= rpw * rpw) pw += 3LL * na;
+      }
+      S.pp_cap = (int)(pp * 1.3 + 256);
+      S.pw_cap = (int)(pw * 1.3 + 256);
+      S.qp_cap = V.nqat * V.nat_solute + 16;
+      S.qw_cap = V.nwat + 16;
+      int mx = 0;
+      for (int iw = 0; iw < V.nwat; iw++) {
+        int c = 0;
+        for (int jw = 0; jw < V.nwat; jw++)
+          if (jw != iw && d2(X, V.nat_solute + 3 * iw, V.nat_solute + 3 * jw) <= rww * rww) c++;
+        mx = std::max(mx, c);
+      }
+      ww_cap = std::max(ww_cap, ((int)(mx * 1.15) + 31) / 32 * 32);
+    }
+    S.pp_off = (int)pp_tot; pp_tot += S.pp_cap;
+    S.pw_off = (int)pw_tot; pw_tot += S.pw_cap;
+    S.qp_off = (int)qp_tot; qp_tot += S.qp_cap;
+    S.qw_off = (int)qw_tot; qw_tot += S.qw_cap;
+    B.max_natom = std::max(B.max_natom, V.natom);
+    B.max_nwat = std::max(B.max_nwat, V.nwat);
+    B.max_ncgp_sol = std::max(B.max_ncgp_sol, V.ncgp_solute);
+    B.max_terms = std::max(B.max_terms, V.nbonds + V.nangles + V.ntors + V.nimps);
+    B.max_pp = std::max(B.max_pp, S.pp_cap);
+    B.max_pw = V.nwat > 0 ? std::max(B.max_pw, S.pw_cap) : B.max_pw;
+    B.max_qp = std::max(B.max_qp, S.qp_cap);
+    B.any_lrf |= V.use_LRF != 0;
+    B.any_q |= V.nqat > 0;
+    B.any_shake |= V.shake_constraints > 0;
+    B.any_wpol |= S.wpol != 0;
+    B.any_prestr |= (V.nrstr_seq + V.nrstr_pos + V.nrstr_dist + V.nrstr_angl + V.nrstr_wall) > 0;
+    B.any_qq |= S.nqq > 0;
+    B.any_qb |= (V.nqbond + V.nqangle + V.nqtor + V.nqimp) > 0;
+  }
+  // water offsets
+  int woff = 0;
+  for (int s = 0; s < n; s++) { B.sysh[s].woff = woff; woff += B.sysh[s].nwat; }
+
+  // device upload
+  DevPtrs &P = B.P;
+  P.nsys = n;
+  P.natoms_tot = (int)x.size();
+  P.nwat_tot = woff;
+  P.ncgp_tot = (int)cg_first.size();
+  P.nshake_tot = (int)sh_first.size();
+  auto &o = B.owned;
+  P.sys = dev_upload(B.sysh, o);
+  P.st = dev_upload(sst, o);
+  P.x = dev_upload(x, o); P.v = dev_upload(v, o);
+  P.xx = dev_alloc<double4>(x.size(), o); P.d = dev_alloc<double4>(x.size(), o);
+  P.crg = dev_upload(crg, o); P.winv = dev_upload(winv, o); P.mass = dev_upload(mass, o);
+  P.iac = dev_upload(iac, o); P.iq = dev_upload(iq, o); P.cgp = dev_upload(cgp, o); P.asys = dev_upload(asys, o);
+  P.flags = dev_upload(flags, o); P.lja = dev_upload(lja, o); P.ljb = dev_upload(ljb, o);
+  P.lx = dev_upload(lx, o); P.l14 = dev_upload(l14, o); P.exl = dev_upload(exl, o); P.l14l = dev_upload(l14l, o);
+  P.ljcod = dev_upload(ljcod, o);
+  P.xtop = dev_upload(xtop, o);
+  P.cg_first = dev_upload(cg_first, o); P.cg_last = dev_upload(cg_last, o); P.cg_sw = dev_upload(cg_sw, o);
+  P.cg_atoms = dev_upload(cg_atoms, o); P.cg_sys = dev_upload(cg_sys, o);
+  P.lrf = dev_alloc<double>((size_t)P.ncgp_tot * LRF_STRIDE, o);
+  P.iqseq = dev_upload(iqseq, o); P.qcrg = dev_upload(qcrg, o); P.qiac = dev_upload(qiac, o);
+  P.qavdw = dev_upload(qavdw, o); P.qbvdw = dev_upload(qbvdw, o); P.sc = dev_upload(sc, o);
+  P.qconn = dev_upload(qconn, o); P.qq = dev_upload(qq, o); P.qq_el = dev_upload(qq_el, o);
+  P.bij = dev_upload(bij, o); P.bpar = dev_upload(bpar, o); P.aijk = dev_upload(aijk, o); P.apar = dev_upload(apar, o);
+  P.tijkl = dev_upload(tijkl, o); P.tpar = dev_upload(tpar, o); P.iijkl = dev_upload(iijkl, o); P.ipar = dev_upload(ipar, o);
+  P.qbij = dev_upload(qbij, o); P.qb_on = dev_upload(qb_on, o); P.qbpar = dev_upload(qbpar, o);
+  P.qaijk = dev_upload(qaijk, o); P.qa_on = dev_upload(qa_on, o); P.qapar = dev_upload(qapar, o);
+  P.qtijkl = dev_upload(qtijkl, o); P.qt_on = dev_upload(qt_on, o); P.qtpar = dev_upload(qtpar, o);
+  P.qiijkl = dev_upload(qiijkl, o); P.qi_on = dev_upload(qi_on, o); P.qipar = dev_upload(qipar, o);
+  P.sh_first = dev_upload(sh_first, o); P.sh_n = dev_upload(sh_n, o); P.sh_sys = dev_upload(sh_sys, o);
+  P.sh_ij = dev_upload(sh_ij, o); P.sh_d2 = dev_upload(sh_d2, o);
+  P.rs = dev_upload(rs, o); P.rs_fk = dev_upload(rs_fk, o); P.rp = dev_upload(rp, o); P.rp_x = dev_upload(rp_x, o);
+  P.rp_fk = dev_upload(rp_fk, o); P.rd = dev_upload(rd, o); P.rd_p = dev_upload(rd_p, o);
+  P.ra = dev_upload(ra, o); P.ra_p = dev_upload(ra_p, o); P.rw = dev_upload(rw, o); P.rw_p = dev_upload(rw_p, o);
+  P.pp = dev_alloc<int4>(pp_tot, o); P.pw = dev_alloc<int4>(pw_tot, o);
+  P.qp = dev_alloc<int4>(qp_tot, o); P.qw = dev_alloc<int>(qw_tot, o);
+  P.ww_cap = ww_cap;
+  P.ww = dev_alloc<int>((size_t)std::max(woff, 1) * ww_cap, o);
+  P.ww_n = dev_alloc<int>(std::max(woff, 1), o);
+  P.E = dev_alloc<double>((size_t)n * QB_NE, o);
+  P.EQ = dev_alloc<double>((size_t)n * MAXS * QB_NEQ, o);
+  P.hist = nullptr;
+  P.hist_cap = 0;
+  B.watpol_smem = (size_t)B.max_nwat * sizeof(double) + (size_t)MAX_SHELLS * B.max_nwat * sizeof(int);
+  if (B.any_wpol) {
+    if (B.watpol_smem > 200 * 1024) fail(QB_ERR_UNSUPPORTED, "too many waters for the polarisation kernel");
+    CUDA_TRY(cudaFuncSetAttribute(k_watpol, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B.watpol_smem));
+  }
+}
+
+}  // namespace
+
+void ensure_history(Batch &B, int nsteps) {
+  // records needed: one per output/energy interval hit, plus slack
+  long long need = 2;
+  for (auto &S : B.sysh) {
+    long long a = S.iout > 0 ? nsteps / S.iout + 2 : 2;
+    long long b = S.iene > 0 ? nsteps / S.iene + 2 : 2;
+    need = std::max(need, std::max(a, b));
+  }
+  std::vector<SysState> st(B.nsys);
+  CUDA_TRY(cudaMemcpy(st.data(), B.P.st, sizeof(SysState) * B.nsys, cudaMemcpyDeviceToHost));
+  int used = 0;
+  for (auto &x : st) used = std::max(used, std::max(x.hist_n[0], x.hist_n[1]));
+  long long cap = used + need;
+  if (cap <= B.P.hist_cap) return;
+  size_t rec = QB_NE + MAXS * QB_NEQ + 1;
+  double *nh = nullptr;
+  CUDA_TRY(cudaMalloc(&nh, sizeof(double) * rec * cap * 2 * B.nsys));
+  CUDA_TRY(cudaMemset(nh, 0, sizeof(double) * rec * cap * 2 * B.nsys));
+  if (B.P.hist) {
+    for (int kind = 0; kind < 2; kind++)
+      for (int s = 0; s < B.nsys; s++)
+        CUDA_TRY(cudaMemcpy(nh + (((size_t)kind * B.nsys + s) * cap) * rec,
+                            B.P.hist + (((size_t)kind * B.nsys + s) * B.P.hist_cap) * rec,
+                            sizeof(double) * rec * B.P.hist_cap, cudaMemcpyDeviceToDevice));
+    for (auto &p : B.owned)
+      if (p == B.P.hist) { cudaFree(p); p = nh; }
+  } else {
+    B.owned.push_back(nh);
+  }
+  B.P.hist = nh;
+  B.P.hist_cap = (int)cap;
+}
+
+template <class F>
+int guarded_batch(F &&f) {
+  try {
+    f();
+    return QB_OK;
+  } catch (const Error &e) {
+    set_error(e.what());
+    return e.code;
+  } catch (const std::exception &e) {
+    set_error(e.what());
+    return QB_ERR_ARG;
+  }
+}
+
+}  // namespace qb
+
+struct qb_batch {
+  qb::Batch b;
+};
+
+using qb::Batch;
+using qb::guarded_batch;
+
+extern "C" {
+
+int qb_device_count(int *out) {
+  if (!out) return QB_ERR_ARG;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) n = 0;
+  *out = n;
+  return QB_OK;
+}
+
+int qb_batch_create(qb_handle *const *systems, int n, const qb_options *opt, qb_batch **out) {
+  if (!systems || n <= 0 || !out) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
+  *out = nullptr;
+  qb_batch *b = new qb_batch();
+  int rc = guarded_batch([&] {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) qb::fail(QB_ERR_CUDA, "no CUDA device available");
+    if (opt) b->b.opt = *opt;
+    CUDA_TRY(cudaSetDevice(b->b.opt.device));
+    if (b->b.opt.precision != QB_FP64 && b->b.opt.precision != QB_MIXED) qb::fail(QB_ERR_ARG, "unknown precision");
+    CUDA_TRY(cudaStreamCreateWithFlags(&b->b.stream, cudaStreamNonBlocking));
+    qb::build(b->b, systems, n);
+    // md_run's initial temperature (md.f90:3960-3963)
+    qb::k_finish<<<n, 512, 0, b->b.stream>>>(b->b.P, 0);
+    b->b.check_launch("initial temperature");
+    CUDA_TRY(cudaStreamSynchronize(b->b.stream));
+  });
+  if (rc != QB_OK) { delete b; return rc; }
+  *out = b;
+  return QB_OK;
+}
+
+int qb_batch_run(qb_batch *bb, int nsteps) {
+  if (!bb || nsteps < 0) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
+  return guarded_batch([&] {
+    Batch &B = bb->b;
+    CUDA_TRY(cudaSetDevice(B.opt.device));
+    qb::ensure_history(B, nsteps);
+    for (int k = 0; k < nsteps; k++) B.step();
+    if (B.profiling) B.collect();
+    B.sync_status();
+    // workload of the current lists
+    std::vector<qb::SysState> st(B.nsys);
+    CUDA_TRY(cudaMemcpy(st.data(), B.P.st, sizeof(qb::SysState) * B.nsys, cudaMemcpyDeviceToHost));
+    std::vector<int> wwn(std::max(B.P.nwat_tot, 1));
+    CUDA_TRY(cudaMemcpy(wwn.data(), B.P.ww_n, sizeof(int) * wwn.size(), cudaMemcpyDeviceToHost));
+    double ww = 0;
+    for (int k = 0; k < B.P.nwat_tot; k++) ww += wwn[k];
+    double pw = 0, pp = 0, qp = 0, qw = 0, sh = 0, cg = B.P.ncgp_tot;
+    for (int s = 0; s < B.nsys; s++) {
+      pp += st[s].pp_n; pw += st[s].pw_n; qp += (double)st[s].qp_n * B.sysh[s].S;
+      qw += (double)st[s].qw_n * B.sysh[s].nq * B.sysh[s].S;
+      sh += B.views[s].shake_constraints;
+    }
+    double w[8] = {ww / 2, pw, pp, qp, qw, (double)B.P.natoms_tot, sh, cg};
+    std::memcpy(B.workload, w, sizeof w);
+  });
+}
+
+int qb_batch_final_energy(qb_batch *bb) {
+  if (!bb) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
+  return guarded_batch([&] {
+    Batch &B = bb->b;
+    B.build_lists();
+    B.pot_energy();
+    B.sync_status();
+  });
+}
+
+static int sys_check(qb_batch *bb, int sys) {
+  if (!bb || sys < 0 || sys >= bb->b.nsys) { qb::set_error("invalid batch or system index"); return QB_ERR_ARG; }
+  return QB_OK;
+}
+
+int qb_batch_energies(qb_batch *bb, int sys, double *E_out, double *EQ_out) {
+  if (int rc = sys_check(bb, sys)) return rc;
+  return guarded_batch([&] {
+    Batch &B = bb->b;
+    CUDA_TRY(cudaStreamSynchronize(B.stream));
+    if (E_out) CUDA_TRY(cudaMemcpy(E_out, B.P.E + (size_t)sys * QB_NE, sizeof(double) * QB_NE, cudaMemcpyDeviceToHost));
+    if (EQ_out && B.sysh[sys].S > 0)
+      CUDA_TRY(cudaMemcpy(EQ_out, B.P.EQ + (size_t)sys * qb::MAXS * QB_NEQ, sizeof(double) * QB_NEQ * B.sysh[sys].S,
+                          cudaMemcpyDeviceToHost));
+  });
+}
+
+int qb_batch_temperature(qb_batch *bb, int sys, double *out) {
+  if (int rc = sys_check(bb, sys)) return rc;
+  return guarded_batch([&] {
+    qb::SysState st;
+    CUDA_TRY(cudaStreamSynchronize(bb->b.stream));
+    CUDA_TRY(cudaMemcpy(&st, bb->b.P.st + sys, sizeof st, cudaMemcpyDeviceToHost));
+    out[0] = st.Temp; out[1] = st.Tfree; out[2] = st.Tfree_sol; out[3] = st.Tfree_solv; out[4] = st.Tscale_solv;
+  });
+}
+
+static int get_vec(qb_batch *bb, int sys, double4 *src, double *out) {
+  if (int rc = sys_check(bb, sys)) return rc;
+  if (!out) { qb::set_error("null buffer"); return QB_ERR_ARG; }
+  return guarded_batch([&] {
+    Batch &B = bb->b;
+    const qb::SysDev &S = B.sysh[sys];
+    std::vector<double4> tmp(S.natom);
+    CUDA_TRY(cudaStreamSynchronize(B.stream));
+    CUDA_TRY(cudaMemcpy(tmp.data(), src + S.aoff, sizeof(double4) * S.natom, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < S.natom; i++) { out[3 * i] = tmp[i].x; out[3 * i + 1] = tmp[i].y; out[3 * i + 2] = tmp[i].z; }
+  });
+}
+
+static int set_vec(qb_batch *bb, int sys, double4 *dst, const double *in) {
+  if (int rc = sys_check(bb, sys)) return rc;
+  if (!in) { qb::set_error("null buffer"); return QB_ERR_ARG; }
+  return guarded_batch([&] {
+    Batch &B = bb->b;
+    const qb::SysDev &S = B.sysh[sys];
+    std::vector<double4> tmp(S.natom);
+    for (int i = 0; i < S.natom; i++) tmp[i] = make_double4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0);
+    CUDA_TRY(cudaStreamSynchronize(B.stream));
+    CUDA_TRY(cudaMemcpy(dst + S.aoff, tmp.data(), sizeof(double4) * S.natom, cudaMemcpyHostToDevice));
+  });
+}
+
+int qb_batch_gradient(qb_batch *b, int sys, double *d) { return get_vec(b, sys, b ? b->b.P.d : nullptr, d); }
+int qb_batch_get_coords(qb_batch *b, int sys, double *x) { return get_vec(b, sys, b ? b->b.P.x : nullptr, x); }
+int qb_batch_set_coords(qb_batch *b, int sys, const double *x) { return set_vec(b, sys, b ? b->b.P.x : nullptr, x); }
+int qb_batch_get_velocities(qb_batch *b, int sys, double *v) { return get_vec(b, sys, b ? b->b.P.v : nullptr, v); }
+int qb_batch_set_velocities(qb_batch *b, int sys, const double *v) { return set_vec(b, sys, b ? b->b.P.v : nullptr, v); }
+
+int qb_batch_get_theta_corr(qb_batch *bb, int sys, float *out, int n) {
+  if (int rc = sys_check(bb, sys)) return rc;
+  return guarded_batch([&] {
+    qb::SysState st;
+    CUDA_TRY(cudaStreamSynchronize(bb->b.stream));
+    CUDA_TRY(cudaMemcpy(&st, bb->b.P.st + sys, sizeof st, cudaMemcpyDeviceToHost));
+    for (int k = 0; k < n && k < qb::MAX_SHELLS; k++) out[k] = st.theta_corr[k];
+  });
+}
+
+int qb_batch_history(qb_batch *bb, int sys, int kind, int *count, int *steps, double *E, double *EQ) {
+  if (int rc = sys_check(bb, sys)) return rc;
+  if (kind < 0 || kind > 1 || !count) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
+  return guarded_batch([&] {
+    Batch &B = bb->b;
+    qb::SysState st;
+    CUDA_TRY(cudaStreamSynchronize(B.stream));
+    CUDA_TRY(cudaMemcpy(&st, B.P.st + sys, sizeof st, cudaMemcpyDeviceToHost));
+    int c = std::min(st.hist_n[kind], B.P.hist_cap);
+    *count = c;
+    if (c == 0 || (!steps && !E && !EQ)) return;
+    size_t rec = QB_NE + qb::MAXS * QB_NEQ + 1;
+    std::vector<double> h(rec * c);
+    CUDA_TRY(cudaMemcpy(h.data(), B.P.hist + (((size_t)kind * B.nsys + sys) * B.P.hist_cap) * rec,
+                        sizeof(double) * rec * c, cudaMemcpyDeviceToHost));
+    int S = B.sysh[sys].S;
+    for (int r = 0; r < c; r++) {
+      const double *p = h.data() + rec * r;
+      if (steps) steps[r] = (int)p[0];
+      if (E) std::memcpy(E + (size_t)r * QB_NE, p + 1, sizeof(double) * QB_NE);
+      if (EQ && S > 0) std::memcpy(EQ + (size_t)r * S * QB_NEQ, p + 1 + QB_NE, sizeof(double) * S * QB_NEQ);
+    }
+  });
+}
+
+int qb_batch_clear_history(qb_batch *bb) {
+  if (!bb) return QB_ERR_ARG;
+  return guarded_batch([&] {
+    Batch &B = bb->b;
+    std::vector<qb::SysState> st(B.nsys);
+    CUDA_TRY(cudaStreamSynchronize(B.stream));
+    CUDA_TRY(cudaMemcpy(st.data(), B.P.st, sizeof(qb::SysState) * B.nsys, cudaMemcpyDeviceToHost));
+    for (auto &x : st) x.hist_n[0] = x.hist_n[1] = 0;
+    CUDA_TRY(cudaMemcpy(B.P.st, st.data(), sizeof(qb::SysState) * B.nsys, cudaMemcpyHostToDevice));
+  });
+}
+
+int qb_batch_status(qb_batch *bb, int sys, int *status) {
+  if (int rc = sys_check(bb, sys)) return rc;
+  return guarded_batch([&] {
+    qb::SysState st;
+    CUDA_TRY(cudaStreamSynchronize(bb->b.stream));
+    CUDA_TRY(cudaMemcpy(&st, bb->b.P.st + sys, sizeof st, cudaMemcpyDeviceToHost));
+    *status = st.status;
+  });
+}
+
+int qb_batch_set_profiling(qb_batch *bb, int on) {
+  if (!bb) return QB_ERR_ARG;
+  bb->b.profiling = on != 0;
+  if (on) { bb->b.stats.clear(); bb->b.order.clear(); }
+  return QB_OK;
+}
+
+int qb_batch_profile(qb_batch *bb, char *names, size_t names_len, double *ms, long long *launches, int n,
+                     int *n_kernels) {
+  if (!bb) return QB_ERR_ARG;
+  Batch &B = bb->b;
+  std::string all;
+  int k = 0;
+  for (auto &name : B.order) {
+    if (k < n) {
+      if (ms) ms[k] = B.stats[name].ms;
+      if (launches) launches[k] = B.stats[name].launches;
+      all += name + "\n";
+    }
+    k++;
+  }
+  if (names && names_len) std::snprintf(names, names_len, "%s", all.c_str());
+  if (n_kernels) *n_kernels = k;
+  return QB_OK;
+}
+
+int qb_batch_workload(qb_batch *bb, double *out, int n) {
+  if (!bb || !out) return QB_ERR_ARG;
+  for (int k = 0; k < n && k < 8; k++) out[k] = bb->b.workload[k];
+  return QB_OK;
+}
+
+void qb_batch_destroy(qb_batch *bb) { delete bb; }
+
+}  // extern "C"

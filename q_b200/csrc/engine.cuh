@@ -1,0 +1,111 @@
+// engine.cuh -- device-side data layout of a batch of Q systems.
+//
+// All systems of a batch live in one set of device arrays, concatenated; a
+// per-system SysDev record holds each system's offsets and scalar parameters.
+// Global indices: atoms g = aoff + i, waters gw = woff + iw (O atom
+// aoff + nsol + 3*iw), charge groups gc = coff + ig, Q atoms gq = qoff + iq.
+#pragma once
+#include <cstdint>
+
+#include "qb.h"
+
+namespace qb {
+
+constexpr int MAXS = QB_MAX_STATES;
+constexpr int LRF_STRIDE = 44;   // centre[3], phi0, phi1[3], phi2[9], phi3[27], pad
+constexpr int MAX_SHELLS = 4;
+constexpr int NQ_SHARED = 64;    // Q atoms whose water forces are reduced in shared memory
+enum AtomFlags : uint8_t { F_EXCL = 1, F_SHELL = 2, F_HEAVY = 4 };
+
+// Per-system record (read-only on the device during a run).
+struct SysDev {
+  int aoff, natom, nsol, nwat, woff, coff, ncgp, ncgp_sol;
+  int qoff, nq, S, natyps, ljoff, qlib_off, sc_off, qconn_off;
+  int exl_off, nexl, l14_off, nl14;
+  // static term ranges (global offsets into term arrays)
+  int b_off, nb, nb_sol, a_off, na, na_sol, t_off, nt, nt_sol, i_off, ni, ni_sol;
+  int qb_off, nqb, qa_off, nqa, qt_off, nqt, qi_off, nqi;
+  int qq_off, nqq;            // flattened nbqq entries of all states
+  int sh_off, nsh;            // shake molecules
+  int rs_off, nrs, rp_off, nrp, rd_off, nrd, ra_off, nra, rw_off, nrw;
+  // dynamic list segments
+  int pp_off, pp_cap, pw_off, pw_cap, qp_off, qp_cap, qw_off, qw_cap;
+  int ff_type, use_lrf, qvdw, wpol, nshell, iac_ow, separate_scaling, has_shake, detail_temps;
+  int qp_once;                // lists with Q atoms are built once (Rcq > exclusion radius)
+  int iout, iene, NB;
+  int Ndegf, Ndegfree, Ndegfree_sol, Ndegfree_solv;
+  double dt, Temp0, tau_T, el14, A_OO, B_OO;
+  double Rcpp2, Rcpw2, Rcww2, Rcq2, RcLRF2;
+  float crg_ow, crg_hw;
+  double xp[3], xw[3], rwat, fk_ws, Dwmz, awmz, fkwpol, fk_pshell, fk_fix;
+  float ws_rout[MAX_SHELLS], ws_dr[MAX_SHELLS], ws_cstb[MAX_SHELLS];
+  double lambda[MAXS];
+  double aO[2], bO[2];
+};
+
+// Per-system state written by the device.
+struct SysState {
+  double Tscale_sol, Tscale_solv, Temp, Tfree, Tfree_sol, Tfree_solv, kinetic;
+  float theta_corr[MAX_SHELLS], avtheta[MAX_SHELLS], avn_insh[MAX_SHELLS];
+  int istep, status, pp_n, pw_n, qp_n, qw_n, lists_built, hist_n[2];
+};
+
+struct DevPtrs {
+  int nsys, natoms_tot, nwat_tot, ncgp_tot, nshake_tot;
+  SysDev *sys;
+  SysState *st;
+  // atoms
+  double4 *x, *v, *xx, *d;
+  float *crg, *winv;
+  double *mass;
+  int *iac, *iq, *cgp, *asys;
+  uint8_t *flags;
+  double *lja, *ljb;        // [3*g + code-1]
+  uint32_t *lx, *l14;       // exclusion / 1-4 bits per atom (solute atoms)
+  int2 *exl, *l14l;         // long lists (local indices), per system segments
+  uint8_t *ljcod;           // per system natyps^2
+  const double *xtop;       // [3*g]
+  // charge groups
+  int *cg_first, *cg_last, *cg_sw, *cg_atoms, *cg_sys;
+  double *lrf;              // [gc*LRF_STRIDE]
+  // Q atoms
+  int *iqseq;               // global atom of global Q atom
+  float *qcrg;              // [gq*MAXS + st]
+  int *qiac;                // [gq*MAXS + st] local Q type
+  double *qavdw, *qbvdw;    // per system segments [qlib_off + 3*t + code-1]
+  double *sc;               // per system segments [sc_off + (iq*(natyps+nq)+col)*S + st]
+  int8_t *qconn;            // per system segments [qconn_off + (st*nsol + i)*nq + iq]
+  int4 *qq;                 // (gq, gj, gjq or -1, lj | st<<8)
+  double *qq_el;
+  // bonded terms (global atom indices)
+  int2 *bij; double2 *bpar;               // fk, b0
+  int4 *aijk; double2 *apar;              // fk, th0
+  int4 *tijkl; float4 *tpar;              // fk, rmult, deltor, paths
+  int4 *iijkl; float2 *ipar;              // fk, imp0
+  int2 *qbij; uint8_t *qb_on; double4 *qbpar;           // [term*MAXS+st] Dmz, amz, r0, fk
+  int4 *qaijk; uint8_t *qa_on; double2 *qapar;          // fk, th0
+  int4 *qtijkl; uint8_t *qt_on; double4 *qtpar;         // fk, rmult, deltor
+  int4 *qiijkl; uint8_t *qi_on; double2 *qipar;         // fk, imp0
+  // shake
+  int *sh_first, *sh_n, *sh_sys; int2 *sh_ij; double *sh_d2;
+  // restraints (global atoms)
+  int4 *rs; double *rs_fk;                 // i, j, ih, to_center
+  int2 *rp; double *rp_x, *rp_fk;          // i, ipsi; x[3], fk[3]
+  int4 *rd; double4 *rd_p;                 // i, j, ipsi; d1, d2, fk
+  int4 *ra; double2 *ra_p;                 // i, j, k, ipsi; ang, fk
+  int4 *rw; double4 *rw_p;                 // i, j, ih; d, fk, aMorse, dMorse
+  // dynamic lists
+  int4 *pp, *pw;                           // i, j, lj
+  int4 *qp;                                // gq, j, lj, qlj
+  int *qw;                                 // water O atoms
+  int *ww, *ww_n;                          // [gw*ww_cap + k], count per water
+  int ww_cap;
+  // energies
+  double *E;                               // [s*QB_NE]
+  double *EQ;                              // [(s*MAXS + st)*QB_NEQ]
+  // history [kind][s][rec][QB_NE + MAXS*QB_NEQ + 1]
+  double *hist;
+  int hist_cap;
+};
+
+}  // namespace qb

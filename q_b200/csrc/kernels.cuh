@@ -1,0 +1,1470 @@
+// kernels.cuh -- per-step device kernels of the Q MD step (sm_100a).
+//
+// One launch covers every system of a batch.  Most kernels use a 2-D grid:
+// blockIdx.y selects the system and blockIdx.x/threadIdx stride over that
+// system's items, so each block reduces energies of one system only.
+// Each kernel names the reference routine (src/q6/md.f90) it restates.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "engine.cuh"
+
+namespace qb {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr float kBoltzF = 0.001986f;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  return v;
+}
+
+// Reduce v over the warp and add it to *dst once (lane 0).  All 32 lanes of
+// the warp must call it.
+__device__ __forceinline__ void warp_add(double *dst, double v) {
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(dst, v);
+}
+
+__device__ __forceinline__ double3 ld3(const double4 *p, int g) {
+  double4 a = p[g];
+  return make_double3(a.x, a.y, a.z);
+}
+
+__device__ __forceinline__ void atomic_add3(double4 *d, int g, double fx, double fy, double fz) {
+  atomicAdd(&d[g].x, fx);
+  atomicAdd(&d[g].y, fy);
+  atomicAdd(&d[g].z, fz);
+}
+
+__device__ __forceinline__ void set_status(SysState *st, int code) { atomicCAS(&st->status, 0, code); }
+
+__device__ __forceinline__ double dev_pi() { return (double)(4.0f * atanf(1.0f)); }
+
+// ------------------------------------------------------------------ lists
+
+// cgp_centers (md.f90:1000): group centres, multipoles zeroed.
+__global__ void k_cgp_centers(DevPtrs P) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= P.ncgp_tot) return;
+  double c[3] = {0, 0, 0};
+  int f = P.cg_first[g], l = P.cg_last[g];
+  for (int a = f; a <= l; a++) {
+    double3 xa = ld3(P.x, P.cg_atoms[a]);
+    c[0] += xa.x; c[1] += xa.y; c[2] += xa.z;
+  }
+  double n = (double)(float)(l - f + 1);
+  double *L = P.lrf + (size_t)g * LRF_STRIDE;
+  for (int k = 0; k < 3; k++) L[k] = c[k] / n;
+  for (int k = 3; k < LRF_STRIDE; k++) L[k] = 0.0;
+}
+
+// Multipole contribution of charge q at offset dr from a group centre
+// (md.f90:5581-5636), accumulated into m[40] = phi0, phi1[3], phi2[9], phi3[27].
+__device__ __forceinline__ void lrf_accumulate(double *m, double q, double dx, double dy, double dz) {
+  double dr[3] = {dx, dy, dz};
+  double r2 = dx * dx + dy * dy + dz * dz;
+  double f0 = q / (r2 * sqrt(r2));
+  m[0] += f0 * r2;
+#pragma unroll
+  for (int k = 0; k < 3; k++) m[1 + k] -= f0 * dr[k];
+  double f1 = 3. * f0 / r2;
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      m[4 + 3 * a + b] += f1 * dr[a] * dr[b];
+      if (a == b) m[4 + 3 * a + b] -= f0;
+    }
+  double f2 = -f1 / r2;
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        double t = 5. * dr[a] * dr[b] * dr[c];
+        if (a == b && b == c) t -= r2 * 3. * dr[a];
+        else {
+          if (a == b) t -= r2 * dr[c];
+          if (a == c) t -= r2 * dr[b];
+          if (b == c) t -= r2 * dr[a];
+        }
+        m[13 + 9 * a + 3 * b + c] += f2 * t;
+      }
+}
+
+// LRF multipoles of every charge group, gathered (nbpplist_lrf 5448,
+// nbpwlist_lrf 6864, nbwwlist_lrf 8370).  A group g receives the charges of
+// every group h whose switching atoms lie beyond the pair's cut-off but within
+// RcLRF (both switching atoms inside the sphere; Q atoms carry no charge here).
+// The reference visits each unordered pair once and adds to both groups; the
+// gather adds the same contributions.  One warp per group.
+__global__ void k_lrf_gather(DevPtrs P) {
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= P.ncgp_tot) return;
+  int g = warp;
+  int s = P.cg_sys[g];
+  const SysDev &S = P.sys[s];
+  int swg = P.cg_sw[g];
+  if (P.flags[swg] & F_EXCL) return;
+  double *L = P.lrf + (size_t)g * LRF_STRIDE;
+  double cx = L[0], cy = L[1], cz = L[2];
+  double3 xs = ld3(P.x, swg);
+  bool g_sol = (g - S.coff) < S.ncgp_sol;
+  double m[40];
+#pragma unroll
+  for (int k = 0; k < 40; k++) m[k] = 0.0;
+  for (int hl = lane; hl < S.ncgp; hl += 32) {
+    int h = S.coff + hl;
+    if (h == g) continue;
+    int swh = P.cg_sw[h];
+    if (P.flags[swh] & F_EXCL) continue;
+    double3 xh = ld3(P.x, swh);
+    double dx = xs.x - xh.x, dy = xs.y - xh.y, dz = xs.z - xh.z;
+    double r2 = dx * dx + dy * dy + dz * dz;
+    bool h_sol = hl < S.ncgp_sol;
+    double rc2 = (g_sol && h_sol) ? S.Rcpp2 : ((g_sol || h_sol) ? S.Rcpw2 : S.Rcww2);
+    if (!(r2 > rc2 && r2 <= S.RcLRF2)) continue;
+    for (int a = P.cg_first[h]; a <= P.cg_last[h]; a++) {
+      int at = P.cg_atoms[a];
+      if (h_sol && P.iq[at] >= 0) continue;
+      double3 xa = ld3(P.x, at);
+      lrf_accumulate(m, (double)P.crg[at], xa.x - cx, xa.y - cy, xa.z - cz);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 40; k++) {
+    double t = warp_sum(m[k]);
+    if (lane == 0) L[3 + k] = t;
+  }
+}
+
+// Water-water neighbour list (nbwwlist / nbwwlist_lrf, md.f90:8233, 8370),
+// stored in both directions: water i lists every other water j inside the
+// sphere whose O lies within Rcww of i's O.  One warp per water.
+__global__ void k_list_ww(DevPtrs P) {
+  int s = blockIdx.y;
+  const SysDev &S = P.sys[s];
+  int wpb = blockDim.x >> 5;
+  int iw = blockIdx.x * wpb + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (iw >= S.nwat) return;
+  int gw = S.woff + iw;
+  int oi = S.aoff + S.nsol + 3 * iw;
+  int cnt = 0;
+  int *out = P.ww + (size_t)gw * P.ww_cap;
+  if (!(P.flags[oi] & F_EXCL)) {
+    double3 xi = ld3(P.x, oi);
+    for (int base = 0; base < S.nwat; base += 32) {
+      int jw = base + lane;
+      bool ok = false;
+      int oj = S.aoff + S.nsol + 3 * jw;
+      if (jw < S.nwat && jw != iw && !(P.flags[oj] & F_EXCL)) {
+        double3 xj = ld3(P.x, oj);
+        double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        ok = dx * dx + dy * dy + dz * dz <= S.Rcww2;
+      }
+      unsigned bal = __ballot_sync(FULL, ok);
+      if (ok) {
+        int pos = cnt + __popc(bal & ((1u << lane) - 1u));
+        if (pos < P.ww_cap) out[pos] = oj;
+      }
+      cnt += __popc(bal);
+    }
+  }
+  if (lane == 0) {
+    if (cnt > P.ww_cap) { set_status(&P.st[s], QB_ERR_LIST_OVERFLOW); cnt = P.ww_cap; }
+    P.ww_n[gw] = cnt;
+  }
+}
+
+__device__ __forceinline__ bool excluded_pair(const DevPtrs &P, const SysDev &S, int i, int j) {
+  // i, j global solute atoms
+  int d = j - i;
+  if (d <= QB_NBR_RANGE && d >= -QB_NBR_RANGE) {
+    if (d > 0) return (P.lx[i] >> (d - 1)) & 1u;
+    return (P.lx[j] >> (-d - 1)) & 1u;
+  }
+  int li = i - S.aoff, lj = j - S.aoff;
+  for (int n = 0; n < S.nexl; n++) {
+    int2 p = P.exl[S.exl_off + n];
+    if ((p.x == li && p.y == lj) || (p.x == lj && p.y == li)) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ bool is14(const DevPtrs &P, const SysDev &S, int i, int j) {
+  int d = j - i;
+  if (d <= QB_NBR_RANGE && d >= -QB_NBR_RANGE) {
+    if (d > 0) return (P.l14[i] >> (d - 1)) & 1u;
+    return (P.l14[j] >> (-d - 1)) & 1u;
+  }
+  int li = i - S.aoff, lj = j - S.aoff;
+  bool r = false;
+  for (int n = 0; n < S.nl14; n++) {
+    int2 p = P.l14l[S.l14_off + n];
+    if ((p.x == li && p.y == lj) || (p.x == lj && p.y == li)) r = true;
+  }
+  return r;
+}
+
+__device__ __forceinline__ int ljcode(const DevPtrs &P, const SysDev &S, int gi, int gj) {
+  return P.ljcod[S.ljoff + P.iac[gi] * S.natyps + P.iac[gj]];
+}
+
+// all-zero pair test (md.f90:5495-5501)
+__device__ __forceinline__ bool zero_pair(const DevPtrs &P, int i, int j, int lj) {
+  float qq = P.crg[i] * P.crg[j];
+  return qq == 0.0f && P.lja[3 * i + lj - 1] * P.lja[3 * j + lj - 1] == 0.0 &&
+         P.ljb[3 * i + lj - 1] * P.ljb[3 * j + lj - 1] == 0.0;
+}
+
+// Solute-solute pair list (nbpplist, md.f90:5175): block (ig, system),
+// threads over jg.  Group pairs are taken once, by the reference's parity rule.
+__global__ void k_list_pp(DevPtrs P) {
+  int s = blockIdx.y;
+  const SysDev &S = P.sys[s];
+  int ig = blockIdx.x;
+  if (ig >= S.ncgp_sol) return;
+  int gi = S.coff + ig;
+  int swi = P.cg_sw[gi];
+  if (P.flags[swi] & F_EXCL) return;
+  double3 xs = ld3(P.x, swi);
+  for (int jg = threadIdx.x; jg < S.ncgp_sol; jg += blockDim.x) {
+    if ((ig > jg && ((ig + jg) & 1) == 0) || (ig < jg && ((ig + jg) & 1) == 1)) continue;
+    int gj = S.coff + jg;
+    int swj = P.cg_sw[gj];
+    if (P.flags[swj] & F_EXCL) continue;
+    double3 xj = ld3(P.x, swj);
+    double dx = xs.x - xj.x, dy = xs.y - xj.y, dz = xs.z - xj.z;
+    if (dx * dx + dy * dy + dz * dz > S.Rcpp2) continue;
+    for (int ia = P.cg_first[gi]; ia <= P.cg_last[gi]; ia++) {
+      int i = P.cg_atoms[ia];
+      if (P.iq[i] >= 0) continue;
+      for (int ja = P.cg_first[gj]; ja <= P.cg_last[gj]; ja++) {
+        int j = P.cg_atoms[ja];
+        if (ig == jg && i >= j) continue;
+        if (P.iq[j] >= 0) continue;
+        int lj = ljcode(P, S, i, j);
+        if (zero_pair(P, i, j, lj)) continue;
+        if (excluded_pair(P, S, i, j)) continue;
+        if (is14(P, S, i, j)) lj = 3;
+        int k = atomicAdd(&P.st[s].pp_n, 1);
+        if (k < S.pp_cap) P.pp[S.pp_off + k] = make_int4(i, j, lj, 0);
+        else set_status(&P.st[s], QB_ERR_LIST_OVERFLOW);
+      }
+    }
+  }
+}
+
+// Solute-water pair list (nbpwlist, md.f90:6684): block (ig, system),
+// threads over waters.
+__global__ void k_list_pw(DevPtrs P) {
+  int s = blockIdx.y;
+  const SysDev &S = P.sys[s];
+  int ig = blockIdx.x;
+  if (ig >= S.ncgp_sol) return;
+  int gi = S.coff + ig;
+  int swi = P.cg_sw[gi];
+  if (P.flags[swi] & F_EXCL) return;
+  double3 xs = ld3(P.x, swi);
+  for (int iw = threadIdx.x; iw < S.nwat; iw += blockDim.x) {
+    int o = S.aoff + S.nsol + 3 * iw;
+    if (P.flags[o] & F_EXCL) continue;
+    double3 xo = ld3(P.x, o);
+    double dx = xs.x - xo.x, dy = xs.y - xo.y, dz = xs.z - xo.z;
+    if (dx * dx + dy * dy + dz * dz > S.Rcpw2) continue;
+    for (int ia = P.cg_first[gi]; ia <= P.cg_last[gi]; ia++) {
+      int i = P.cg_atoms[ia];
+      if (P.iq[i] >= 0) continue;
+      for (int j = o; j < o + 3; j++) {
+        int lj = ljcode(P, S, i, j);
+        if (zero_pair(P, i, j, lj)) continue;
+        int k = atomicAdd(&P.st[s].pw_n, 1);
+        if (k < S.pw_cap) P.pw[S.pw_off + k] = make_int4(i, j, lj, 0);
+        else set_status(&P.st[s], QB_ERR_LIST_OVERFLOW);
+      }
+    }
+  }
+}
+
+// Q-atom / solute list (nbqplist, md.f90:7875): block per system, threads
+// over solute atoms of groups within Rcq of the solute centre; atoms bonded
+// within 1-3 to any Q atom (in any state) belong to the Q-Q list instead.
+__global__ void k_list_qp(DevPtrs P, int force) {
+  int s = blockIdx.x;
+  const SysDev &S = P.sys[s];
+  if (S.nq == 0) return;
+  if (!force && S.qp_once && P.st[s].lists_built) return;
+  __syncthreads();
+  if (threadIdx.x == 0) P.st[s].qp_n = 0;
+  __syncthreads();
+  for (int ig = 0; ig < S.ncgp_sol; ig++) {
+    int gi = S.coff + ig;
+    int sw = P.cg_sw[gi];
+    if (P.flags[sw] & F_EXCL) continue;
+    double3 xs = ld3(P.x, sw);
+    double dx = xs.x - S.xp[0], dy = xs.y - S.xp[1], dz = xs.z - S.xp[2];
+    if (dx * dx + dy * dy + dz * dz > S.Rcq2) continue;
+    int f = P.cg_first[gi], n = P.cg_last[gi] - f + 1;
+    for (int t = threadIdx.x; t < n * S.nq; t += blockDim.x) {
+      int i = P.cg_atoms[f + t / S.nq], iq = t % S.nq;
+      int li = i - S.aoff;
+      bool near = false;
+      for (int st = 0; st < S.S && !near; st++)
+        for (int q = 0; q < S.nq; q++)
+          if (P.qconn[S.qconn_off + ((size_t)st * S.nsol + li) * S.nq + q] <= 3) { near = true; break; }
+      if (near) continue;
+      int qa = P.iqseq[S.qoff + iq];
+      int lj = ljcode(P, S, i, qa);
+      if (P.qconn[S.qconn_off + ((size_t)0 * S.nsol + li) * S.nq + iq] == 4) lj = 3;
+      int qlj = lj == 2 ? 1 : lj;
+      int k = atomicAdd(&P.st[s].qp_n, 1);
+      if (k < S.qp_cap) P.qp[S.qp_off + k] = make_int4(S.qoff + iq, i, lj, qlj);
+      else set_status(&P.st[s], QB_ERR_LIST_OVERFLOW);
+    }
+  }
+}
+
+// Q-atom / water list (nbqwlist, md.f90:8066): waters with O within Rcq of the
+// solute centre.  Block per system; order of the list follows the waters.
+__global__ void k_list_qw(DevPtrs P, int force) {
+  int s = blockIdx.x;
+  const SysDev &S = P.sys[s];
+  if (S.nq == 0) return;
+  if (!force && S.qp_once && P.st[s].lists_built) return;
+  __shared__ int base;
+  if (threadIdx.x == 0) base = 0;
+  __syncthreads();
+  for (int w0 = 0; w0 < S.nwat; w0 += blockDim.x) {
+    int iw = w0 + threadIdx.x;
+    bool ok = false;
+    int o = S.aoff + S.nsol + 3 * iw;
+    if (iw < S.nwat && !(P.flags[o] & F_EXCL)) {
+      double3 xo = ld3(P.x, o);
+      double dx = xo.x - S.xp[0], dy = xo.y - S.xp[1], dz = xo.z - S.xp[2];
+      ok = dx * dx + dy * dy + dz * dz <= S.Rcq2;
+    }
+    // block-wide ordered compaction
+    __shared__ int wcount[32];
+    unsigned bal = __ballot_sync(FULL, ok);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) wcount[wid] = __popc(bal);
+    __syncthreads();
+    int off = base;
+    for (int w = 0; w < wid; w++) off += wcount[w];
+    if (ok) {
+      int k = off + __popc(bal & ((1u << lane) - 1u));
+      if (k < S.qw_cap) P.qw[S.qw_off + k] = o;
+      else set_status(&P.st[s], QB_ERR_LIST_OVERFLOW);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int tot = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) tot += wcount[w];
+      base += tot;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) P.st[s].qw_n = base < S.qw_cap ? base : S.qw_cap;
+}
+
+__global__ void k_lists_begin(DevPtrs P) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= P.nsys) return;
+  P.st[s].pp_n = 0;
+  P.st[s].pw_n = 0;
+}
+
+__global__ void k_lists_end(DevPtrs P) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= P.nsys) return;
+  SysState &st = P.st[s];
+  const SysDev &S = P.sys[s];
+  if (st.pp_n > S.pp_cap) st.pp_n = S.pp_cap;
+  if (st.pw_n > S.pw_cap) st.pw_n = S.pw_cap;
+  if (st.qp_n > S.qp_cap) st.qp_n = S.qp_cap;
+  st.lists_built = 1;
+}
+
+// ------------------------------------------------------------- nonbonded
+
+// nonbond_ww_spc (md.f90:11823): one warp per water i, lanes over its
+// neighbours; the 9 gradient components of i are reduced with warp shuffles.
+// Each unordered pair is evaluated from both sides; energies are halved.
+__global__ void k_nb_ww(DevPtrs P) {
+  int s = blockIdx.y;
+  const SysDev &S = P.sys[s];
+  int wpb = blockDim.x >> 5;
+  int iw = blockIdx.x * wpb + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  bool active = iw < S.nwat;
+  double el = 0, vdw = 0;
+  double f[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) f[k] = 0;
+  int oi = S.aoff + S.nsol + 3 * iw;
+  if (active) {
+    int gw = S.woff + iw;
+    int n = P.ww_n[gw];
+    const int *nb = P.ww + (size_t)gw * P.ww_cap;
+    double3 xi[3] = {ld3(P.x, oi), ld3(P.x, oi + 1), ld3(P.x, oi + 2)};
+    const float qo = S.crg_ow, qh = S.crg_hw;
+    const float qoo = qo * qo, qoh = qo * qh, qhh = qh * qh;
+    for (int k = lane; k < n; k += 32) {
+      int oj = nb[k];
+      double3 xj[3] = {ld3(P.x, oj), ld3(P.x, oj + 1), ld3(P.x, oj + 2)};
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+          double dx = xj[b].x - xi[a].x, dy = xj[b].y - xi[a].y, dz = xj[b].z - xi[a].z;
+          double rinv = sqrt(1.0 / (dx * dx + dy * dy + dz * dz));
+          double r2 = rinv * rinv;
+          float qq = (a == 0 && b == 0) ? qoo : ((a == 0 || b == 0) ? qoh : qhh);
+          double Vel = (double)qq * rinv, dv;
+          if (a == 0 && b == 0) {
+            double r6 = r2 * r2 * r2;
+            double Va = S.A_OO * r6 * r6, Vb = S.B_OO * r6;
+            vdw += Va - Vb;
+            dv = r2 * (-Vel - 12. * Va + 6. * Vb);
+          } else {
+            dv = r2 * (-Vel);
+          }
+          el += Vel;
+          f[3 * a + 0] -= dv * dx;
+          f[3 * a + 1] -= dv * dy;
+          f[3 * a + 2] -= dv * dz;
+        }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 9; k++) f[k] = warp_sum(f[k]);
+  if (active && lane == 0) {
+    for (int a = 0; a < 3; a++) {
+      double4 dd = P.d[oi + a];
+      dd.x += f[3 * a]; dd.y += f[3 * a + 1]; dd.z += f[3 * a + 2];
+      P.d[oi + a] = dd;
+    }
+  }
+  warp_add(&P.E[s * QB_NE + QB_E_WW_EL], 0.5 * el);
+  warp_add(&P.E[s * QB_NE + QB_E_WW_VDW], 0.5 * vdw);
+}
+
+// nonbond_pp (md.f90:10387) and nonbond_pw (10631): one thread per pair.
+template <bool PP>
+__global__ void k_nb_pair(DevPtrs P) {
+  int s = blockIdx.y;
+  const SysDev &S = P.sys[s];
+  int n = PP ? P.st[s].pp_n : P.st[s].pw_n;
+  const int4 *L = PP ? P.pp + S.pp_off : P.pw + S.pw_off;
+  double el = 0, vdw = 0;
+  for (int k0 = blockIdx.x * blockDim.x; k0 < n; k0 += gridDim.x * blockDim.x) {
+    int k = k0 + threadIdx.x;
+    if (k < n) {
+      int4 p = L[k];
+      int i = p.x, j = p.y, lj = p.z;
+      double3 xi = ld3(P.x, i), xj = ld3(P.x, j);
+      double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+      double r2 = 1. / (dx * dx + dy * dy + dz * dz);
+      double r = sqrt(r2), r6 = r2 * r2 * r2;
+      float qq = P.crg[i] * P.crg[j];
+      double Vel = (double)qq * r;
+      if (PP && lj == 3) Vel = Vel * S.el14;
+      double Va = r6 * r6 * P.lja[3 * i + lj - 1] * P.lja[3 * j + lj - 1];
+      double Vb = r6 * P.ljb[3 * i + lj - 1] * P.ljb[3 * j + lj - 1];
+      double dv = r2 * (-Vel - 12. * Va + 6. * Vb);
+      atomic_add3(P.d, i, -dv * dx, -dv * dy, -dv * dz);
+      atomic_add3(P.d, j, dv * dx, dv * dy, dv * dz);
+      el += Vel;
+      vdw += Va - Vb;
+    }
+  }
+  warp_add(&P.E[s * QB_NE + (PP ? QB_E_PP_EL : QB_E_PW_EL)], el);
+  warp_add(&P.E[s * QB_NE + (PP ? QB_E_PP_VDW : QB_E_PW_VDW)], vdw);
+}
+
+// nonbond_qp (md.f90:10980) / nonbond_qp_qvdw (11138): one thread per pair,
+// all states in the thread.
+__global__ void k_nb_qp(DevPtrs P) {
+  int s = blockIdx.y;
+  const SysDev &S = P.sys[s];
+  int n = P.st[s].qp_n;
+  const int NS = S.S;
+  const int ncol = S.natyps + S.nq;
+  double el[MAXS], vdw[MAXS];
+  for (int st = 0; st < MAXS; st++) { el[st] = 0; vdw[st] = 0; }
+  for (int k0 = blockIdx.x * blockDim.x; k0 < n; k0 += gridDim.x * blockDim.x) {
+    int k = k0 + threadIdx.x;
+    if (k < n) {
+      int4 p = P.qp[S.qp_off + k];
+      int gq = p.x, j = p.y, lj = p.z, qlj = p.w;
+      int i = P.iqseq[gq], iq = gq - S.qoff;
+      double3 xi = ld3(P.x, i), xj = ld3(P.x, j);
+      double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+      double r2 = dx * dx + dy * dy + dz * dz;
+      double dvsum = 0;
+      if (!S.qvdw) {
+        r2 = 1. / r2;
+        double r6 = r2 * r2 * r2, r = sqrt(r2);
+        double aLJ = P.lja[3 * i + lj - 1] * P.lja[3 * j + lj - 1];
+        double bLJ = P.ljb[3 * i + lj - 1] * P.ljb[3 * j + lj - 1];
+        for (int st = 0; st < NS; st++) {
+          float qq = P.qcrg[gq * MAXS + st] * P.crg[j];
+          double Vel = (double)qq * r;
+          if (lj == 3) Vel = Vel * S.el14;
+          double Va = aLJ * r6 * r6, Vb = bLJ * r6;
+          dvsum += r2 * (-Vel - 12. * Va + 6. * Vb) * S.lambda[st];
+          el[st] += Vel;
+          vdw[st] += Va - Vb;
+        }
+      } else {
+        double r6 = r2 * r2 * r2;
+        r2 = 1. / r2;
+        double r = sqrt(r2);
+        int tj = P.iac[j];
+        for (int st = 0; st < NS; st++) {
+          int ti = P.qiac[gq * MAXS + st];
+          double aLJ = P.qavdw[S.qlib_off + 3 * ti + qlj - 1] * P.lja[3 * j + lj - 1];
+          double bLJ = P.qbvdw[S.qlib_off + 3 * ti + qlj - 1] * P.ljb[3 * j + lj - 1];
+          float qq = P.qcrg[gq * MAXS + st] * P.crg[j];
+          double Vel = (double)qq * r;
+          if (lj == 3) Vel = Vel * S.el14;
+          double r6sc = r6 + P.sc[S.sc_off + ((size_t)iq * ncol + tj) * NS + st];
+          double Va = aLJ / (r6sc * r6sc), Vb = bLJ / r6sc;
+          dvsum += r2 * (-Vel - (12. * Va - 6. * Vb) * (r6 / r6sc)) * S.lambda[st];
+          el[st] += Vel;
+          vdw[st] += Va - Vb;
+        }
+      }
+      atomic_add3(P.d, i, -dvsum * dx, -dvsum * dy, -dvsum * dz);
+      atomic_add3(P.d, j, dvsum * dx, dvsum * dy, dvsum * dz);
+    }
+  }
+  for (int st = 0; st < NS; st++) {
+    warp_add(&P.EQ[((size_t)s * MAXS + st) * QB_NEQ + QB_EQ_QP_EL], el[st]);
+    warp_add(&P.EQ[((size_t)s * MAXS + st) * QB_NEQ + QB_EQ_QP_VDW], vdw[st]);
+  }
+}
+
+// nonbond_qw_spc (md.f90:11302): one thread per water of the Q-water list,
+// looping over Q atoms; Q-atom gradients are reduced in shared memory.
+__global__ void k_nb_qw(DevPtrs P) {
+  int s = blockIdx.y;
+  const SysDev &S = P.sys[s];
+  __shared__ double fq[NQ_SHARED * 3];
+  if (S.nq == 0) return;
+  const bool shq = S.nq <= NQ_SHARED;
+  for (int t = threadIdx.x; t < NQ_SHARED * 3; t += blockDim.x) fq[t] = 0;
+  __syncthreads();
+  int n = P.st[s].qw_n;
+  const int NS = S.S, ncol = S.natyps + S.nq;
+  double el[MAXS], vdw[MAXS];
+  for (int st = 0; st < MAXS; st++) { el[st] = 0; vdw[st] = 0; }
+  for (int k0 = blockIdx.x * blockDim.x; k0 < n; k0 += gridDim.x * blockDim.x) {
+    int k = k0 + threadIdx.x;
+    if (k < n) {
+      int j = P.qw[S.qw_off + k];
+      double3 xO = ld3(P.x, j), xH1 = ld3(P.x, j + 1), xH2 = ld3(P.x, j + 2);
+      double fw[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int iq = 0; iq < S.nq; iq++) {
+        int gq = S.qoff + iq;
+        int i = P.iqseq[gq];
+        double3 xi = ld3(P.x, i);
+        double dO[3] = {xO.x - xi.x, xO.y - xi.y, xO.z - xi.z};
+        double dH1[3] = {xH1.x - xi.x, xH1.y - xi.y, xH1.z - xi.z};
+        double dH2[3] = {xH2.x - xi.x, xH2.y - xi.y, xH2.z - xi.z};
+        double r2O = dO[0] * dO[0] + dO[1] * dO[1] + dO[2] * dO[2];
+        double rH1 = sqrt(1.0 / (dH1[0] * dH1[0] + dH1[1] * dH1[1] + dH1[2] * dH1[2]));
+        double rH2 = sqrt(1.0 / (dH2[0] * dH2[0] + dH2[1] * dH2[1] + dH2[2] * dH2[2]));
+        double r6hc = r2O * r2O * r2O;
+        r2O = 1.0 / r2O;
+        double rO = sqrt(r2O);
+        double r2H1 = rH1 * rH1, r2H2 = rH2 * rH2;
+        double r6sc = r6hc, dvO = 0, dvH1 = 0, dvH2 = 0, Va = 0, Vb = 0;
+        int lj = P.ljcod[S.ljoff + S.iac_ow * S.natyps + P.iac[i]];
+        if (!S.qvdw) {
+          double r6O = 1. / r6hc;
+          Va = P.lja[3 * i + lj - 1] * S.aO[lj - 1] * r6O * r6O;
+          Vb = P.ljb[3 * i + lj - 1] * S.bO[lj - 1] * r6O;
+        }
+        for (int st = 0; st < NS; st++) {
+          if (S.qvdw) {
+            int ti = P.qiac[gq * MAXS + st];
+            double aLJ = P.qavdw[S.qlib_off + 3 * ti], bLJ = P.qbvdw[S.qlib_off + 3 * ti];
+            r6sc = r6hc + P.sc[S.sc_off + ((size_t)iq * ncol + S.iac_ow) * NS + st];
+            Va = aLJ * S.aO[lj - 1] / (r6sc * r6sc);
+            Vb = bLJ * S.bO[lj - 1] / r6sc;
+          }
+          float q = P.qcrg[gq * MAXS + st];
+          double VelO = (double)(S.crg_ow * q) * rO;
+          double VelH1 = (double)(S.crg_hw * q) * rH1;
+          double VelH2 = (double)(S.crg_hw * q) * rH2;
+          double lam = S.lambda[st];
+          dvO += r2O * (-VelO - ((12. * Va - 6. * Vb) * (r6hc / r6sc))) * lam;
+          dvH1 -= r2H1 * VelH1 * lam;
+          dvH2 -= r2H2 * VelH2 * lam;
+          el[st] += VelO + VelH1 + VelH2;
+          vdw[st] += Va - Vb;
+        }
+        double fi[3];
+        for (int c = 0; c < 3; c++) {
+          fi[c] = -(dvO * dO[c] + dvH1 * dH1[c] + dvH2 * dH2[c]);
+          fw[c] += dvO * dO[c];
+          fw[3 + c] += dvH1 * dH1[c];
+          fw[6 + c] += dvH2 * dH2[c];
+        }
+        if (shq) {
+          atomicAdd(&fq[3 * iq], fi[0]);
+          atomicAdd(&fq[3 * iq + 1], fi[1]);
+          atomicAdd(&fq[3 * iq + 2], fi[2]);
+        } else {
+          atomic_add3(P.d, i, fi[0], fi[1], fi[2]);
+        }
+      }
+      for (int a = 0; a < 3; a++) {
+        double4 dd = P.d[j + a];
+        dd.x += fw[3 * a]; dd.y += fw[3 * a + 1]; dd.z += fw[3 * a + 2];
+        P.d[j + a] = dd;
+      }
+    }
+  }
+  for (int st = 0; st < NS; st++) {
+    warp_add(&P.EQ[((size_t)s * MAXS + st) * QB_NEQ + QB_EQ_QW_EL], el[st]);
+    warp_add(&P.EQ[((size_t)s * MAXS + st) * QB_NEQ + QB_EQ_QW_VDW], vdw[st]);
+  }
+  __syncthreads();
+  if (shq)
+    for (int t = threadIdx.x; t < S.nq * 3; t += blockDim.x)
+      if (fq[t] != 0.0) {
+        int i = P.iqseq[S.qoff + t / 3];
+        double *dp = &P.d[i].x + (t % 3);
+        atomicAdd(dp, fq[t]);
+      }
+}
+
+// nonbond_qq (md.f90:10763): Q-Q and Q-to-bonded-neighbour pairs, all states.
+__global__ void k_nb_qq(DevPtrs P) {
+  int s = blockIdx.x;
+  const SysDev &S = P.sys[s];
+  const int NS = S.S, ncol = S.natyps + S.nq;
+  for (int k0 = 0; k0 < S.nqq; k0 += blockDim.x) {
+    int k = k0 + threadIdx.x;
+    double Vel = 0, V = 0;
+    int st = 0;
+    bool qq_pair = false, act = k < S.nqq;
+    if (act) {
+      int4 e = P.qq[S.qq_off + k];
+      int gq = e.x, j = e.y, gjq = e.z, lj = e.w & 0xff;
+      st = e.w >> 8;
+      int iq = gq - S.qoff;
+      int jq = gjq >= 0 ? gjq - S.qoff : -1;
+      int i = P.iqseq[gq];
+      double qi = (double)P.qcrg[gq * MAXS + st], qj, aLJ, bLJ;
+      double els = P.qq_el[S.qq_off + k];
+      if (!S.qvdw) {
+        aLJ = P.lja[3 * i + lj - 1] * P.lja[3 * j + lj - 1];
+        bLJ = P.ljb[3 * i + lj - 1] * P.ljb[3 * j + lj - 1];
+        qj = jq >= 0 ? (double)P.qcrg[gjq * MAXS + st] : (double)P.crg[j];
+      } else {
+        int ti = P.qiac[gq * MAXS + st];
+        aLJ = P.qavdw[S.qlib_off + 3 * ti + lj - 1];
+        bLJ = P.qbvdw[S.qlib_off + 3 * ti + lj - 1];
+        if (jq >= 0) {
+          int tj = P.qiac[gjq * MAXS + st];
+          aLJ *= P.qavdw[S.qlib_off + 3 * tj + lj - 1];
+          bLJ *= P.qbvdw[S.qlib_off + 3 * tj + lj - 1];
+          qj = P.qcrg[gjq * MAXS + st];
+        } else {
+          if (lj == 2) { aLJ = P.qavdw[S.qlib_off + 3 * ti]; bLJ = P.qbvdw[S.qlib_off + 3 * ti]; }
+          aLJ *= P.lja[3 * j + lj - 1];
+          bLJ *= P.ljb[3 * j + lj - 1];
+          qj = P.crg[j];
+        }
+      }
+      double3 xi = ld3(P.x, i), xj = ld3(P.x, j);
+      double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+      double r2 = dx * dx + dy * dy + dz * dz;
+      double r6hc = r2 * r2 * r2;
+      // jq = -1 reads the reference's sc_lookup(iq, natyps+0, state)
+      double r6 = r2 * r2 * r2 + P.sc[S.sc_off + ((size_t)iq * ncol + (S.natyps + jq)) * NS + st];
+      r6 = 1. / r6;
+      double r12 = r6 * r6;
+      r2 = 1. / r2;
+      double r = sqrt(r2);
+      Vel = qi * qj * r * els;
+      if (lj == 3) Vel = Vel * S.el14;
+      double Va, Vb, dv;
+      if (S.qvdw && jq >= 0 && lj == 2) {
+        Va = aLJ * exp(-bLJ / r);
+        Vb = 0.0;
+        dv = r2 * (-Vel - bLJ * Va / r) * S.lambda[st];
+      } else {
+        Va = aLJ * r12;
+        Vb = bLJ * r6;
+        dv = r2 * (-Vel - (12. * Va - 6. * Vb) * r6hc * r6) * S.lambda[st];
+      }
+      V = Va - Vb;
+      qq_pair = jq >= 0;
+      atomic_add3(P.d, i, -dv * dx, -dv * dy, -dv * dz);
+      atomic_add3(P.d, j, dv * dx, dv * dy, dv * dz);
+      double *eq = &P.EQ[((size_t)s * MAXS + st) * QB_NEQ];
+      atomicAdd(&eq[qq_pair ? QB_EQ_QQ_EL : QB_EQ_QP_EL], Vel);
+      atomicAdd(&eq[qq_pair ? QB_EQ_QQ_VDW : QB_EQ_QP_VDW], V);
+    }
+  }
+}
+
+// lrf_taylor (md.f90:3646): potential and field of each atom's own group
+// multipoles; one thread per atom.
+__global__ void k_lrf_taylor(DevPtrs P) {
+  int s = blockIdx.y;
+  const SysDev &S = P.sys[s];
+  double e = 0;
+  for (int i0 = blockIdx.x * blockDim.x; i0 < S.natom; i0 += gridDim.x * blockDim.x) {
+    int il = i0 + threadIdx.x;
+    if (il < S.natom) {
+      int i = S.aoff + il;
+      if (!(P.flags[i] & F_EXCL) && P.iq[i] < 0) {
+        const double *L = P.lrf + (size_t)P.cgp[i] * LRF_STRIDE;
+        double3 xi = ld3(P.x, i);
+        double dr[3] = {L[0] - xi.x, L[1] - xi.y, L[2] - xi.z};
+        const double *p1 = L + 4, *p2 = L + 7, *p3 = L + 16;
+        double V = L[3] + p1[0] * dr[0] + p1[1] * dr[1] + p1[2] * dr[2];
+        for (int a = 0; a < 3; a++) V += 0.5 * (p2[3 * a] * dr[0] + p2[3 * a + 1] * dr[1] + p2[3 * a + 2] * dr[2]) * dr[a];
+        double q = (double)P.crg[i];
+        e += 0.5 * q * V;
+        double g[3];
+        for (int c = 0; c < 3; c++) {
+          double df = p1[c] + p2[3 * c] * dr[0] + p2[3 * c + 1] * dr[1] + p2[3 * c + 2] * dr[2];
+          for (int a = 0; a < 3; a++) {
+            const double *p = p3 + 9 * c + 3 * a;
+            df += 0.5 * (p[0] * dr[0] + p[1] * dr[1] + p[2] * dr[2]) * dr[a];
+          }
+          g[c] = q * df;
+        }
+        double4 dd = P.d[i];
+        dd.x -= g[0]; dd.y -= g[1]; dd.z -= g[2];
+        P.d[i] = dd;
+      }
+    }
+  }
+  warp_add(&P.E[s * QB_NE + QB_E_LRF], e);
+}
+
+// ---------------------------------------------------------------- bonded
+
+__device__ __forceinline__ double dihedral(const DevPtrs &P, int i, int j, int k, int l, double dp[12]) {
+  double3 xi = ld3(P.x, i), xj = ld3(P.x, j), xk = ld3(P.x, k), xl = ld3(P.x, l);
+  double rji[3] = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
+  double rjk[3] = {xk.x - xj.x, xk.y - xj.y, xk.z - xj.z};
+  double rkl[3] = {xl.x - xk.x, xl.y - xk.y, xl.z - xk.z};
+  double rnj[3], rnk[3], di[3], dl[3], rki[3], rlj[3];
+  rnj[0] = rji[1] * rjk[2] - rji[2] * rjk[1];
+  rnj[1] = rji[2] * rjk[0] - rji[0] * rjk[2];
+  rnj[2] = rji[0] * rjk[1] - rji[1] * rjk[0];
+  rnk[0] = -rjk[1] * rkl[2] + rjk[2] * rkl[1];
+  rnk[1] = -rjk[2] * rkl[0] + rjk[0] * rkl[2];
+  rnk[2] = -rjk[0] * rkl[1] + rjk[1] * rkl[0];
+  double bj2inv = 1. / (rnj[0] * rnj[0] + rnj[1] * rnj[1] + rnj[2] * rnj[2]);
+  double bk2inv = 1. / (rnk[0] * rnk[0] + rnk[1] * rnk[1] + rnk[2] * rnk[2]);
+  double bjinv = sqrt(bj2inv), bkinv = sqrt(bk2inv);
+  double scp = (rnj[0] * rnk[0] + rnj[1] * rnk[1] + rnj[2] * rnk[2]) * (bjinv * bkinv);
+  double phi;
+  if (scp > 1.0) { scp = 1.0; phi = (double)acosf(1.0f); }
+  else if (scp < -1.0) { scp = -1.0; phi = (double)acosf(-1.0f); }
+  else phi = acos(scp);
+  double sgn = rjk[0] * (rnj[1] * rnk[2] - rnj[2] * rnk[1]) + rjk[1] * (rnj[2] * rnk[0] - rnj[0] * rnk[2]) +
+               rjk[2] * (rnj[0] * rnk[1] - rnj[1] * rnk[0]);
+  if (sgn < 0) phi = -phi;
+  double f1 = sin(phi);
+  if (fabs(f1) < 1.e-12) f1 = 1.e-12;
+  f1 = -1.0 / f1;
+  for (int c = 0; c < 3; c++) {
+    di[c] = f1 * (rnk[c] * (bjinv * bkinv) - scp * rnj[c] * bj2inv);
+    dl[c] = f1 * (rnj[c] * (bjinv * bkinv) - scp * rnk[c] * bk2inv);
+    rki[c] = rji[c] - rjk[c];
+    rlj[c] = -rjk[c] - rkl[c];
+  }
+  dp[0] = rjk[1] * di[2] - rjk[2] * di[1];
+  dp[1] = rjk[2] * di[0] - rjk[0] * di[2];
+  dp[2] = rjk[0] * di[1] - rjk[1] * di[0];
+  dp[3] = rki[1] * di[2] - rki[2] * di[1] + rkl[1] * dl[2] - rkl[2] * dl[1];
+  dp[4] = rki[2] * di[0] - rki[0] * di[2] + rkl[2] * dl[0] - rkl[0] * dl[2];
+  dp[5] = rki[0] * di[1] - rki[1] * di[0] + rkl[0] * dl[1] - rkl[1] * dl[0];
+  dp[6] = rlj[1] * dl[2] - rlj[2] * dl[1] - rji[1] * di[2] + rji[2] * di[1];
+  dp[7] = rlj[2] * dl[0] - rlj[0] * dl[2] - rji[2] * di[0] + rji[0] * di[2];
+  dp[8] = rlj[0] * dl[1] - rlj[1] * dl[0] - rji[0] * di[1] + rji[1] * di[0];
+  dp[9] = rjk[1] * dl[2] - rjk[2] * dl[1];
+  dp[10] = rjk[2] * dl[0] - rjk[0] * dl[2];
+  dp[11] = rjk[0] * dl[1] - rjk[1] * dl[0];
+  return phi;
+}
+
+__device__ __forceinline__ void apply4(const DevPtrs &P, int i, int j, int k, int l, double dv, const double dp[12]) {
+  atomic_add3(P.d, i, dv * dp[0], dv * dp[1], dv * dp[2]);
+  atomic_add3(P.d, j, dv * dp[3], dv * dp[4], dv * dp[5]);
+  atomic_add3(P.d, k, dv * dp[6], dv * dp[7], dv * dp[8]);
+  atomic_add3(P.d, l, dv * dp[9], dv * dp[10], dv * dp[11]);
+}
+
+// bond (954), angle (814), torsion (14793), improper (1677) / improper2 (1789):
+// one thread per term; items are bonds, then angles, torsions, impropers.
+__global__ void k_bonded(DevPtrs P) {
+  int s = blockIdx.y;
+  const SysDev &S = P.sys[s];
+  int n = S.nb + S.na + S.nt + S.ni;
+  double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // p bond, angle, torsion, improper; w ...
+  const double pi = dev_pi();
+  for (int k0 = blockIdx.x * blockDim.x; k0 < n; k0 += gridDim.x * blockDim.x) {
+    int k = k0 + threadIdx.x;
+    if (k >= n) continue;
+    if (k < S.nb) {
+      int2 b = P.bij[S.b_off + k];
+      double2 prm = P.bpar[S.b_off + k];
+      double3 xi = ld3(P.x, b.x), xj = ld3(P.x, b.y);
+      double r[3] = {xj.x - xi.x, xj.y - xi.y, xj.z - xi.z};
+      double bl = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+      double db = bl - prm.y;
+      e[k < S.nb_sol ? 0 : 4] += 0.5 * prm.x * db * db;
+      double dv = prm.x * db / bl;
+      atomic_add3(P.d, b.y, r[0] * dv, r[1] * dv, r[2] * dv);
+      atomic_add3(P.d, b.x, -r[0] * dv, -r[1] * dv, -r[2] * dv);
+    } else if (k < S.nb + S.na) {
+      int a = k - S.nb;
+      int4 t = P.aijk[S.a_off + a];
+      double2 prm = P.apar[S.a_off + a];
+      double3 xi = ld3(P.x, t.x), xj = ld3(P.x, t.y), xk = ld3(P.x, t.z);
+      double rji[3] = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
+      double rjk[3] = {xk.x - xj.x, xk.y - xj.y, xk.z - xj.z};
+      double bji2inv = 1. / (rji[0] * rji[0] + rji[1] * rji[1] + rji[2] * rji[2]);
+      double bjk2inv = 1. / (rjk[0] * rjk[0] + rjk[1] * rjk[1] + rjk[2] * rjk[2]);
+      double bjiinv = sqrt(bji2inv), bjkinv = sqrt(bjk2inv);
+      double scp = (rji[0] * rjk[0] + rji[1] * rjk[1] + rji[2] * rjk[2]) * bjiinv * bjkinv;
+      if (scp > 1.0) scp = 1.0;
+      else if (scp < -1.0) scp = -1.0;
+      double ang = acos(scp);
+      double da = ang - prm.y;
+      e[a < S.na_sol ? 1 : 5] += 0.5 * prm.x * da * da;
+      double dv = prm.x * da;
+      double f1 = sin(ang);
+      if (fabs(f1) < 1.e-12) f1 = -1.e12;
+      else f1 = -1.0 / f1;
+      double di[3], dk[3];
+      for (int c = 0; c < 3; c++) {
+        di[c] = f1 * (rjk[c] * bjiinv * bjkinv - scp * rji[c] * bji2inv);
+        dk[c] = f1 * (rji[c] * bjiinv * bjkinv - scp * rjk[c] * bjk2inv);
+      }
+      atomic_add3(P.d, t.x, dv * di[0], dv * di[1], dv * di[2]);
+      atomic_add3(P.d, t.z, dv * dk[0], dv * dk[1], dv * dk[2]);
+      atomic_add3(P.d, t.y, -dv * (di[0] + dk[0]), -dv * (di[1] + dk[1]), -dv * (di[2] + dk[2]));
+    } else if (k < S.nb + S.na + S.nt) {
+      int t = k - S.nb - S.na;
+      int4 q = P.tijkl[S.t_off + t];
+      float4 prm = P.tpar[S.t_off + t];  // fk, rmult, deltor, paths
+      double dp[12];
+      double phi = dihedral(P, q.x, q.y, q.z, q.w, dp);
+      double arg = (double)prm.y * phi - (double)prm.z;
+      e[t < S.nt_sol ? 2 : 6] += (double)prm.x * (1.0 + cos(arg)) * (double)prm.w;
+      float rf = prm.y * prm.x;
+      double dv = -((double)rf * sin(arg) * (double)prm.w);
+      apply4(P, q.x, q.y, q.z, q.w, dv, dp);
+    } else {
+      int t = k - S.nb - S.na - S.nt;
+      int4 q = P.iijkl[S.i_off + t];
+      float2 prm = P.ipar[S.i_off + t];  // fk, imp0
+      double dp[12];
+      double phi = dihedral(P, q.x, q.y, q.z, q.w, dp);
+      double dv, ee;
+      if (S.ff_type == 2) {
+        double arg = 2 * phi - (double)prm.y;
+        ee = (double)prm.x * (1 + cos(arg));
+        dv = -2 * (double)prm.x * sin(arg);
+      } else {
+        double arg = phi - (double)prm.y;
+        arg = arg - 2. * pi * (double)llround(arg / (2. * pi));
+        dv = (double)prm.x * arg;
+        ee = 0.5 * dv * arg;
+      }
+      e[t < S.ni_sol ? 3 : 7] += ee;
+      apply4(P, q.x, q.y, q.z, q.w, dv, dp);
+    }
+  }
+  const int idx[8] = {QB_E_P_BOND, QB_E_P_ANGLE, QB_E_P_TORSION, QB_E_P_IMPROPER,
+                      QB_E_W_BOND, QB_E_W_ANGLE, QB_E_W_TORSION, QB_E_W_IMPROPER};
+  for (int c = 0; c < 8; c++) warp_add(&P.E[s * QB_NE + idx[c]], e[c]);
+}
+
+// qbond (14060), qangle (13896), qtorsion (14262), qimproper (14117):
+// one block per system, threads over (term, state).
+__global__ void k_qbonded(DevPtrs P) {
+  int s = blockIdx.x;
+  const SysDev &S = P.sys[s];
+  const int NS = S.S;
+  int n1 = S.nqb * NS, n2 = n1 + S.nqa * NS, n3 = n2 + S.nqt * NS, n4 = n3 + S.nqi * NS;
+  const double pi = dev_pi();
+  for (int k = threadIdx.x; k < n4; k += blockDim.x) {
+    double *eq;
+    if (k < n1) {
+      int b = k / NS, st = k % NS;
+      if (!P.qb_on[(S.qb_off + b) * MAXS + st]) continue;
+      eq = &P.EQ[((size_t)s * MAXS + st) * QB_NEQ];
+      int2 ij = P.qbij[S.qb_off + b];
+      double4 prm = P.qbpar[(S.qb_off + b) * MAXS + st];  // Dmz, amz, r0, fk
+      double3 xi = ld3(P.x, ij.x), xj = ld3(P.x, ij.y);
+      double r[3] = {xj.x - xi.x, xj.y - xi.y, xj.z - xi.z};
+      double bl = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+      double db = bl - prm.z;
+      double fexp = exp(-prm.y * db);
+      atomicAdd(&eq[QB_EQ_BOND], prm.x * (fexp * fexp - 2. * fexp) + 0.5 * prm.w * db * db);
+      double dv = (2. * prm.x * prm.y * (fexp - fexp * fexp) + prm.w * db) * S.lambda[st] / bl;
+      atomic_add3(P.d, ij.x, -dv * r[0], -dv * r[1], -dv * r[2]);
+      atomic_add3(P.d, ij.y, dv * r[0], dv * r[1], dv * r[2]);
+    } else if (k < n2) {
+      int a = (k - n1) / NS, st = (k - n1) % NS;
+      if (!P.qa_on[(S.qa_off + a) * MAXS + st]) continue;
+      eq = &P.EQ[((size_t)s * MAXS + st) * QB_NEQ];
+      int4 t = P.qaijk[S.qa_off + a];
+      double2 prm = P.qapar[(S.qa_off + a) * MAXS + st];
+      double3 xi = ld3(P.x, t.x), xj = ld3(P.x, t.y), xk = ld3(P.x, t.z);
+      double rji[3] = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
+      double rjk[3] = {xk.x - xj.x, xk.y - xj.y, xk.z - xj.z};
+      double bji = sqrt(rji[0] * rji[0] + rji[1] * rji[1] + rji[2] * rji[2]);
+      double bjk = sqrt(rjk[0] * rjk[0] + rjk[1] * rjk[1] + rjk[2] * rjk[2]);
+      double scp = (rji[0] * rjk[0] + rji[1] * rjk[1] + rji[2] * rjk[2]) / (bji * bjk);
+      if (scp > 1.0) scp = 1.0;
+      if (scp < -1.0) scp = -1.0;
+      double ang = acos(scp);
+      double da = ang - prm.y;
+      atomicAdd(&eq[QB_EQ_ANGLE], 0.5 * prm.x * da * da);
+      double dv = prm.x * da * S.lambda[st];
+      double f1 = sin(ang);
+      if (fabs(f1) < 1.e-12) f1 = 1.e-12;
+      f1 = -1.0 / f1;
+      double di[3], dk[3];
+      for (int c = 0; c < 3; c++) {
+        di[c] = f1 * (rjk[c] / (bji * bjk) - scp * rji[c] / (bji * bji));
+        dk[c] = f1 * (rji[c] / (bji * bjk) - scp * rjk[c] / (bjk * bjk));
+      }
+      atomic_add3(P.d, t.x, dv * di[0], dv * di[1], dv * di[2]);
+      atomic_add3(P.d, t.z, dv * dk[0], dv * dk[1], dv * dk[2]);
+      atomic_add3(P.d, t.y, -dv * (di[0] + dk[0]), -dv * (di[1] + dk[1]), -dv * (di[2] + dk[2]));
+    } else if (k < n3) {
+      int t = (k - n2) / NS, st = (k - n2) % NS;
+      if (!P.qt_on[(S.qt_off + t) * MAXS + st]) continue;
+      eq = &P.EQ[((size_t)s * MAXS + st) * QB_NEQ];
+      int4 q = P.qtijkl[S.qt_off + t];
+      double4 prm = P.qtpar[(S.qt_off + t) * MAXS + st];  // fk, rmult, deltor
+      double dp[12];
+      double phi = dihedral(P, q.x, q.y, q.z, q.w, dp);
+      double arg = prm.y * phi - prm.z;
+      atomicAdd(&eq[QB_EQ_TORSION], prm.x * (1.0 + cos(arg)));
+      double dv = -prm.y * prm.x * sin(arg) * S.lambda[st];
+      apply4(P, q.x, q.y, q.z, q.w, dv, dp);
+    } else {
+      int t = (k - n3) / NS, st = (k - n3) % NS;
+      if (!P.qi_on[(S.qi_off + t) * MAXS + st]) continue;
+      eq = &P.EQ[((size_t)s * MAXS + st) * QB_NEQ];
+      int4 q = P.qiijkl[S.qi_off + t];
+      double2 prm = P.qipar[(S.qi_off + t) * MAXS + st];  // fk, imp0
+      double dp[12];
+      double phi = dihedral(P, q.x, q.y, q.z, q.w, dp);
+      double arg = phi - prm.y;
+      arg = arg - 2. * pi * (double)llround(arg / (2. * pi));
+      double dv = prm.x * arg;
+      atomicAdd(&eq[QB_EQ_IMPROPER], 0.5 * dv * arg);
+      dv = dv * S.lambda[st];
+      apply4(P, q.x, q.y, q.z, q.w, dv, dp);
+    }
+  }
+}
+
+// ------------------------------------------------------------ restraints
+
+// fix_shell (md.f90:1414) for excluded and shell atoms, and restrain_solvent
+// (14910) for water oxygens: one thread per atom.
+__global__ void k_restrain_atoms(DevPtrs P) {
+  int s = blockIdx.y;
+  const SysDev &S = P.sys[s];
+  double efix = 0, eshell = 0, erad = 0;
+  double Tfree = P.st[s].Tfree;
+  double shift = S.fk_ws != 0. ? sqrt((double)kBoltzF * Tfree / S.fk_ws) : 0.;
+  for (int i0 = blockIdx.x * blockDim.x; i0 < S.natom; i0 += gridDim.x * blockDim.x) {
+    int il = i0 + threadIdx.x;
+    if (il >= S.natom) continue;
+    int i = S.aoff + il;
+    uint8_t fl = P.flags[i];
+    double3 xi = ld3(P.x, i);
+    double g[3] = {0, 0, 0};
+    if (fl & (F_EXCL | F_SHELL)) {
+      double fk = (fl & F_EXCL) ? S.fk_fix : S.fk_pshell;
+      double dr[3] = {xi.x - P.xtop[3 * i], xi.y - P.xtop[3 * i + 1], xi.z - P.xtop[3 * i + 2]};
+      double e = 0.5 * fk * (dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+      if (fl & F_EXCL) efix += e;
+      if (fl & F_SHELL) eshell += e;
+      for (int k = 0; k < 3; k++) g[k] += fk * dr[k];
+    }
+    if (il >= S.nsol && ((il - S.nsol) % 3) == 0 && !(fl & F_EXCL)) {
+      double dr[3] = {xi.x - S.xw[0], xi.y - S.xw[1], xi.z - S.xw[2]};
+      double b = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+      double db = b - (S.rwat - shift), e, dv;
+      if (db > 0) { e = 0.5 * S.fk_ws * db * db - S.Dwmz; dv = S.fk_ws * db / b; }
+      else if (b > 0.0) {
+        double fexp = exp(S.awmz * db);
+        e = S.Dwmz * (fexp * fexp - 2. * fexp);
+        dv = -2. * S.Dwmz * S.awmz * (fexp - fexp * fexp) / b;
+      } else { e = 0; dv = 0; }
+      erad += e;
+      for (int k = 0; k < 3; k++) g[k] += dv * dr[k];
+    }
+    if (g[0] != 0 || g[1] != 0 || g[2] != 0) {
+      double4 dd = P.d[i];
+      dd.x += g[0]; dd.y += g[1]; dd.z += g[2];
+      P.d[i] = dd;
+    }
+  }
+  warp_add(&P.E[s * QB_NE + QB_E_RST_FIX], efix);
+  warp_add(&P.E[s * QB_NE + QB_E_RST_SHELL], eshell);
+  warp_add(&P.E[s * QB_NE + QB_E_RST_SOLVENT_RADIAL], erad);
+}
+
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+  v = warp_sum(v);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double t = 0;
+  for (int w = 0; w < nw; w++) t += sh[w];
+  return t;
+}
+
+__device__ __forceinline__ void rst_energy(const DevPtrs &P, int s, int nstates, int ipsi, double e) {
+  if (ipsi == 0) {
+    for (int k = 0; k < nstates; k++) atomicAdd(&P.EQ[((size_t)s * MAXS + k) * QB_NEQ + QB_EQ_RESTRAINT], e);
+    if (nstates == 0) atomicAdd(&P.E[s * QB_NE + QB_E_RST_PROTEIN], e);
+  } else {
+    atomicAdd(&P.EQ[((size_t)s * MAXS + ipsi - 1) * QB_NEQ + QB_EQ_RESTRAINT], e);
+  }
+}
+
+// p_restrain (md.f90:12940): sequence, atom, distance, angle and wall
+// restraints.  One block per system.
+__global__ void k_prestrain(DevPtrs P) {
+  int s = blockIdx.x;
+  const SysDev &S = P.sys[s];
+  __shared__ double sh[32];
+  for (int r = 0; r < S.nrs; r++) {
+    int4 q = P.rs[S.rs_off + r];  // i, j, ih, to_center
+    double fk = P.rs_fk[S.rs_off + r];
+    if (q.w == 1 || q.w == 2) {
+      double acc[4] = {0, 0, 0, 0};
+      for (int i = q.x + threadIdx.x; i <= q.y; i += blockDim.x) {
+        if (!((P.flags[i] & F_HEAVY) || q.z == 1)) continue;
+        double w = q.w == 2 ? P.mass[i] : 1.0;
+        double3 xi = ld3(P.x, i);
+        acc[0] += (xi.x - P.xtop[3 * i]) * w;
+        acc[1] += (xi.y - P.xtop[3 * i + 1]) * w;
+        acc[2] += (xi.z - P.xtop[3 * i + 2]) * w;
+        acc[3] += w;
+      }
+      double tot[4];
+      for (int k = 0; k < 4; k++) tot[k] = block_sum(acc[k], sh);
+      if (tot[3] > 0) {
+        double dr[3];
+        for (int k = 0; k < 3; k++) dr[k] = tot[k] / tot[3];
+        double r2 = dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2];
+        if (threadIdx.x == 0) atomicAdd(&P.E[s * QB_NE + QB_E_RST_PROTEIN], 0.5 * fk * r2);
+        for (int i = q.x + threadIdx.x; i <= q.y; i += blockDim.x) {
+          if (!((P.flags[i] & F_HEAVY) || q.z == 1)) continue;
+          double sc = q.w == 1 ? fk * P.mass[i] / (double)12.010f : fk;
+          atomic_add3(P.d, i, sc * dr[0], sc * dr[1], sc * dr[2]);
+        }
+      }
+      __syncthreads();
+    } else {
+      double e = 0;
+      for (int i = q.x + threadIdx.x; i <= q.y; i += blockDim.x) {
+        if (!((P.flags[i] & F_HEAVY) || q.z == 1)) continue;
+        double3 xi = ld3(P.x, i);
+        double dr[3] = {xi.x - P.xtop[3 * i], xi.y - P.xtop[3 * i + 1], xi.z - P.xtop[3 * i + 2]};
+        e += 0.5 * fk * (dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+        atomic_add3(P.d, i, fk * dr[0], fk * dr[1], fk * dr[2]);
+      }
+      double t = block_sum(e, sh);
+      if (threadIdx.x == 0) atomicAdd(&P.E[s * QB_NE + QB_E_RST_PROTEIN], t);
+      __syncthreads();
+    }
+  }
+  const double deg2rad = dev_pi() / 180.0;
+  int nall = S.nrp + S.nrd + S.nra;
+  for (int k = threadIdx.x; k < nall; k += blockDim.x) {
+    if (k < S.nrp) {
+      int2 q = P.rp[S.rp_off + k];  // i, ipsi
+      const double *xr = P.rp_x + 3 * (S.rp_off + k), *fk = P.rp_fk + 3 * (S.rp_off + k);
+      double3 xi = ld3(P.x, q.x);
+      double dr[3] = {xi.x - xr[0], xi.y - xr[1], xi.z - xr[2]};
+      double wgt = q.y != 0 ? S.lambda[q.y - 1] : 1.0, e = 0;
+      for (int c = 0; c < 3; c++) e += 0.5 * fk[c] * dr[c] * dr[c];
+      atomic_add3(P.d, q.x, fk[0] * dr[0] * wgt, fk[1] * dr[1] * wgt, fk[2] * dr[2] * wgt);
+      rst_energy(P, s, S.S, q.y, e);
+    } else if (k < S.nrp + S.nrd) {
+      int r = k - S.nrp;
+      int4 q = P.rd[S.rd_off + r];  // i, j, ipsi
+      double4 prm = P.rd_p[S.rd_off + r];  // d1, d2, fk
+      double3 xi = ld3(P.x, q.x), xj = ld3(P.x, q.y);
+      double dr[3] = {xj.x - xi.x, xj.y - xi.y, xj.z - xi.z};
+      double wgt = q.z != 0 ? S.lambda[q.z - 1] : 1.0;
+      double b = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]), db;
+      if (b < prm.x) db = b - prm.x;
+      else if (b > prm.y) db = b - prm.y;
+      else continue;
+      double e = 0.5 * prm.z * db * db, dv = wgt * prm.z * db / b;
+      atomic_add3(P.d, q.y, dr[0] * dv, dr[1] * dv, dr[2] * dv);
+      atomic_add3(P.d, q.x, -dr[0] * dv, -dr[1] * dv, -dr[2] * dv);
+      rst_energy(P, s, S.S, q.z, e);
+    } else {
+      int r = k - S.nrp - S.nrd;
+      int4 q = P.ra[S.ra_off + r];  // i, j, k, ipsi
+      double2 prm = P.ra_p[S.ra_off + r];  // ang, fk
+      double3 xi = ld3(P.x, q.x), xj = ld3(P.x, q.y), xk = ld3(P.x, q.z);
+      double d1[3] = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z}, d2[3] = {xk.x - xj.x, xk.y - xj.y, xk.z - xj.z};
+      double wgt = q.w != 0 ? S.lambda[q.w - 1] : 1.0;
+      double r2ij = d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2], r2jk = d2[0] * d2[0] + d2[1] * d2[1] + d2[2] * d2[2];
+      double rij = sqrt(r2ij), rjk = sqrt(r2jk);
+      double scp = (d1[0] * d2[0] + d1[1] * d2[1] + d1[2] * d2[2]) / (rij * rjk);
+      if (scp > 1.0) scp = 1.0;
+      if (scp < -1.0) scp = -1.0;
+      double th = acos(scp);
+      double db = th - prm.x * deg2rad;
+      double e = 0.5 * prm.y * db * db, dv = wgt * prm.y * db;
+      double f1 = sin(th);
+      if (fabs(f1) < 1.e-12) f1 = -1.e12;
+      else f1 = -1.0 / f1;
+      double di[3], dk[3];
+      for (int c = 0; c < 3; c++) {
+        di[c] = f1 * (d2[c] / (rij * rjk) - scp * d1[c] / r2ij);
+        dk[c] = f1 * (d1[c] / (rij * rjk) - scp * d2[c] / r2jk);
+      }
+      atomic_add3(P.d, q.x, dv * di[0], dv * di[1], dv * di[2]);
+      atomic_add3(P.d, q.z, dv * dk[0], dv * dk[1], dv * dk[2]);
+      atomic_add3(P.d, q.y, -dv * (di[0] + dk[0]), -dv * (di[1] + dk[1]), -dv * (di[2] + dk[2]));
+      rst_energy(P, s, S.S, q.w, e);
+    }
+  }
+  for (int r = 0; r < S.nrw; r++) {
+    int4 q = P.rw[S.rw_off + r];  // i, j, ih
+    double4 prm = P.rw_p[S.rw_off + r];  // d, fk, aMorse, dMorse
+    double e = 0;
+    for (int i = q.x + threadIdx.x; i <= q.y; i += blockDim.x) {
+      if (!((P.flags[i] & F_HEAVY) || q.z == 1)) continue;
+      double3 xi = ld3(P.x, i);
+      double dr[3] = {xi.x - S.xw[0], xi.y - S.xw[1], xi.z - S.xw[2]};
+      double b = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+      double db = b - prm.x, dv;
+      if (db > 0.) { e += 0.5 * prm.y * db * db - prm.w; dv = prm.y * db / b; }
+      else {
+        double fexp = exp(prm.z * db);
+        e += prm.w * (fexp * fexp - 2. * fexp);
+        dv = -2. * prm.w * prm.z * (fexp - fexp * fexp) / b;
+      }
+      atomic_add3(P.d, i, dv * dr[0], dv * dr[1], dv * dr[2]);
+    }
+    double t = block_sum(e, sh);
+    if (threadIdx.x == 0) atomicAdd(&P.E[s * QB_NE + QB_E_RST_PROTEIN], t);
+    __syncthreads();
+  }
+}
+
+// watpol (md.f90:15122): water dipole orientation restraint.  One block per
+// system.  Waters are assigned to shells by O radius, ordered within a shell
+// by angle theta (ties by water index, as the reference's selection sort
+// does), and restrained to theta_0(rank).
+__global__ void k_watpol(DevPtrs P) {
+  extern __shared__ unsigned char smem[];
+  int s = blockIdx.x;
+  const SysDev &S = P.sys[s];
+  if (!S.wpol || S.nshell == 0) return;
+  const int nw = S.nwat, ns = S.nshell;
+  double *theta = (double *)smem;
+  int *list = (int *)(theta + nw);        // members of each shell, [ns][nw]
+  __shared__ int cnt[MAX_SHELLS];
+  __shared__ double shsum[32];
+  const double pi = dev_pi();
+  if (threadIdx.x < MAX_SHELLS) cnt[threadIdx.x] = 0;
+  __syncthreads();
+  for (int iw = threadIdx.x; iw < nw; iw += blockDim.x) {
+    int i = S.aoff + S.nsol + 3 * iw;
+    theta[iw] = 0.0;
+    if (P.flags[i] & F_EXCL) continue;
+    double3 xO = ld3(P.x, i), x1 = ld3(P.x, i + 1), x2 = ld3(P.x, i + 2);
+    double rmu[3] = {x1.x + x2.x - 2. * xO.x, x1.y + x2.y - 2. * xO.y, x1.z + x2.z - 2. * xO.z};
+    double rm = sqrt(rmu[0] * rmu[0] + rmu[1] * rmu[1] + rmu[2] * rmu[2]);
+    for (int k = 0; k < 3; k++) rmu[k] /= rm;
+    double rcu[3] = {xO.x - S.xw[0], xO.y - S.xw[1], xO.z - S.xw[2]};
+    double rc = sqrt(rcu[0] * rcu[0] + rcu[1] * rcu[1] + rcu[2] * rcu[2]);
+    for (int k = 0; k < 3; k++) rcu[k] /= rc;
+    double scp = rmu[0] * rcu[0] + rmu[1] * rcu[1] + rmu[2] * rcu[2];
+    if (scp > 1.0) scp = 1.0;
+    if (scp < -1.0) scp = -1.0;
+    theta[iw] = acos(scp);
+    float inner = S.ws_rout[ns - 1] - S.ws_dr[ns - 1];
+    if (rc > (double)inner) {
+      int is;
+      for (is = ns - 1; is >= 1; is--)
+        if (rc <= (double)S.ws_rout[is]) break;
+      int k = atomicAdd(&cnt[is], 1);
+      list[is * nw + k] = iw;
+    }
+  }
+  __syncthreads();
+  SysState &st = P.st[s];
+  if (threadIdx.x == 0 && st.istep != 0 && st.istep % 100 == 0) {
+    for (int is = 0; is < ns; is++) {
+      st.avtheta[is] = st.avtheta[is] / (float)100;
+      st.avn_insh[is] = st.avn_insh[is] / (float)100;
+      st.theta_corr[is] = st.theta_corr[is] + st.avtheta[is] - acosf(S.ws_cstb[is]);
+      st.avtheta[is] = 0.0f;
+      st.avn_insh[is] = 0.0f;
+    }
+  }
+  __syncthreads();
+  double epol = 0;
+  for (int is = 0; is < ns; is++) {
+    int n = cnt[is];
+    double tsum = 0;
+    float tc = st.theta_corr[is];
+    float cstb = S.ws_cstb[is];
+    for (int m = threadIdx.x; m < n; m += blockDim.x) {
+      int iw = list[is * nw + m];
+      double th = theta[iw];
+      int rank = 0;
+      for (int u = 0; u < n; u++) {
+        int jw = list[is * nw + u];
+        double tj = theta[jw];
+        rank += (tj < th || (tj == th && jw < iw)) ? 1 : 0;
+      }
+      float arg = 1.0f + (1.0f - 2.0f * (float)(rank + 1)) / (float)n;
+      double th0 = (double)acosf(arg);
+      th0 = th0 - 3. * sin(th0) * (double)cstb / 2.;
+      if (th0 < 0.0) th0 = 0.0;
+      if (th0 > pi) th0 = pi;
+      tsum += th;
+      double dth = th - th0 + (double)tc;
+      epol += 0.5 * S.fkwpol * dth * dth;
+      double dv = S.fkwpol * dth;
+      int i = S.aoff + S.nsol + 3 * iw;
+      double3 xO = ld3(P.x, i), x1 = ld3(P.x, i + 1), x2 = ld3(P.x, i + 2);
+      double rmu[3] = {x1.x + x2.x - 2. * xO.x, x1.y + x2.y - 2. * xO.y, x1.z + x2.z - 2. * xO.z};
+      double rm = sqrt(rmu[0] * rmu[0] + rmu[1] * rmu[1] + rmu[2] * rmu[2]);
+      for (int k = 0; k < 3; k++) rmu[k] /= rm;
+      double rcu[3] = {xO.x - S.xw[0], xO.y - S.xw[1], xO.z - S.xw[2]};
+      double rc = sqrt(rcu[0] * rcu[0] + rcu[1] * rcu[1] + rcu[2] * rcu[2]);
+      for (int k = 0; k < 3; k++) rcu[k] /= rc;
+      double scp = rmu[0] * rcu[0] + rmu[1] * rcu[1] + rmu[2] * rcu[2];
+      if (scp > 1.0) scp = 1.0;
+      if (scp < -1.0) scp = -1.0;
+      double f0 = sin(acos(scp));
+      if (fabs(f0) < 1.e-12) f0 = 1.e-12;
+      f0 = -1.0 / f0;
+      f0 = dv * f0;
+      double gO[3], gH[3];
+      for (int k = 0; k < 3; k++) {
+        double f1 = (rcu[k] - rmu[k] * scp) / rm;
+        double f2 = (rmu[k] - rcu[k] * scp) / rc;
+        gO[k] = f0 * (-2. * f1 + f2);
+        gH[k] = f0 * f1;
+      }
+      double4 d0 = P.d[i], d1 = P.d[i + 1], d2 = P.d[i + 2];
+      d0.x += gO[0]; d0.y += gO[1]; d0.z += gO[2];
+      d1.x += gH[0]; d1.y += gH[1]; d1.z += gH[2];
+      d2.x += gH[0]; d2.y += gH[1]; d2.z += gH[2];
+      P.d[i] = d0; P.d[i + 1] = d1; P.d[i + 2] = d2;
+    }
+    double tot = block_sum(tsum, shsum);
+    if (threadIdx.x == 0 && n > 0) {
+      st.avtheta[is] = (float)((double)st.avtheta[is] + tot / (double)(float)n);
+      st.avn_insh[is] = st.avn_insh[is] + (float)n;
+    }
+    __syncthreads();
+  }
+  double et = block_sum(epol, shsum);
+  if (threadIdx.x == 0) atomicAdd(&P.E[s * QB_NE + QB_E_RST_WATER_POL], et);
+}
+
+// --------------------------------------------------------------- dynamics
+
+// The sums of pot_energy (md.f90:13443-13472): per-state totals and the
+// lambda-weighted Q energies; one thread per system.
+__global__ void k_finalize_energy(DevPtrs P) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= P.nsys) return;
+  const SysDev &S = P.sys[s];
+  double *E = P.E + s * QB_NE;
+  for (int k = 0; k < S.S; k++) {
+    double *q = P.EQ + ((size_t)s * MAXS + k) * QB_NEQ;
+    double lam = S.lambda[k];
+    q[QB_EQ_LAMBDA] = lam;
+    q[QB_EQ_QX_EL] = q[QB_EQ_QQ_EL] + q[QB_EQ_QP_EL] + q[QB_EQ_QW_EL];
+    q[QB_EQ_QX_VDW] = q[QB_EQ_QQ_VDW] + q[QB_EQ_QP_VDW] + q[QB_EQ_QW_VDW];
+    q[QB_EQ_TOTAL] = q[QB_EQ_BOND] + q[QB_EQ_ANGLE] + q[QB_EQ_TORSION] + q[QB_EQ_IMPROPER] + q[QB_EQ_QX_EL] +
+                     q[QB_EQ_QX_VDW] + q[QB_EQ_RESTRAINT];
+    E[QB_E_Q_BOND] += q[QB_EQ_BOND] * lam;
+    E[QB_E_Q_ANGLE] += q[QB_EQ_ANGLE] * lam;
+    E[QB_E_Q_TORSION] += q[QB_EQ_TORSION] * lam;
+    E[QB_E_Q_IMPROPER] += q[QB_EQ_IMPROPER] * lam;
+    E[QB_E_QX_EL] += q[QB_EQ_QX_EL] * lam;
+    E[QB_E_QX_VDW] += q[QB_EQ_QX_VDW] * lam;
+    E[QB_E_RST_PROTEIN] += q[QB_EQ_RESTRAINT] * lam;
+  }
+  E[QB_E_RST_TOTAL] = E[QB_E_RST_FIX] + E[QB_E_RST_SHELL] + E[QB_E_RST_PROTEIN] + E[QB_E_RST_SOLVENT_RADIAL] +
+                      E[QB_E_RST_WATER_POL];
+  E[QB_E_POTENTIAL] = E[QB_E_P_BOND] + E[QB_E_W_BOND] + E[QB_E_P_ANGLE] + E[QB_E_W_ANGLE] + E[QB_E_P_TORSION] +
+                      E[QB_E_P_IMPROPER] + E[QB_E_PP_EL] + E[QB_E_PP_VDW] + E[QB_E_PW_EL] + E[QB_E_PW_VDW] +
+                      E[QB_E_WW_EL] + E[QB_E_WW_VDW] + E[QB_E_Q_BOND] + E[QB_E_Q_ANGLE] + E[QB_E_Q_TORSION] +
+                      E[QB_E_Q_IMPROPER] + E[QB_E_QX_EL] + E[QB_E_QX_VDW] + E[QB_E_RST_TOTAL] + E[QB_E_LRF];
+  E[QB_E_KINETIC] = P.st[s].kinetic;
+  if (!isfinite(E[QB_E_POTENTIAL])) set_status(&P.st[s], QB_ERR_NAN);
+}
+
+// Leapfrog with Berendsen scaling (md.f90:4082-4110): one thread per atom.
+__global__ void k_leapfrog(DevPtrs P) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= P.natoms_tot) return;
+  int s = P.asys[g];
+  const SysDev &S = P.sys[s];
+  double ts = (g - S.aoff) < S.nsol ? P.st[s].Tscale_sol : P.st[s].Tscale_solv;
+  double w = (double)P.winv[g], dt = S.dt;
+  double4 x = P.x[g], v = P.v[g], d = P.d[g];
+  v.x = (v.x - d.x * w * dt) * ts;
+  v.y = (v.y - d.y * w * dt) * ts;
+  v.z = (v.z - d.z * w * dt) * ts;
+  P.xx[g] = x;
+  x.x = x.x + v.x * dt;
+  x.y = x.y + v.y * dt;
+  x.z = x.z + v.z * dt;
+  P.x[g] = x;
+  P.v[g] = v;
+}
+
+// shake (md.f90:14445): Gauss-Seidel iterations over one molecule's
+// constraints per thread, to relative tolerance 1e-4, at most 1000 passes.
+__global__ void k_shake(DevPtrs P) {
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= P.nshake_tot) return;
+  int f = P.sh_first[m], n = P.sh_n[m];
+  if (n == 0) return;
+  bool done = false;
+  int nits = 0;
+  // readiness flags of up to 64*64 constraints in thread-local memory
+  unsigned long long rd[64];
+  int nwords = (n + 63) / 64;
+  if (nwords > 64) { set_status(&P.st[P.sh_sys[m]], QB_ERR_UNSUPPORTED); return; }
+  for (int w = 0; w < nwords; w++) rd[w] = 0;
+  while (!done) {
+    for (int c = 0; c < n; c++) {
+      if ((rd[c >> 6] >> (c & 63)) & 1ull) continue;
+      int2 ij = P.sh_ij[f + c];
+      double4 xi = P.x[ij.x], xj = P.x[ij.y];
+      double4 xxi = P.xx[ij.x], xxj = P.xx[ij.y];
+      double xij[3] = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
+      double xij2 = xij[0] * xij[0] + xij[1] * xij[1] + xij[2] * xij[2];
+      double d2 = P.sh_d2[f + c];
+      double diff = d2 - xij2;
+      if (fabs(diff) < 0.0001 * d2) rd[c >> 6] |= 1ull << (c & 63);
+      double xxij[3] = {xxi.x - xxj.x, xxi.y - xxj.y, xxi.z - xxj.z};
+      double scp = xij[0] * xxij[0] + xij[1] * xxij[1] + xij[2] * xxij[2];
+      float wi = P.winv[ij.x], wj = P.winv[ij.y];
+      float wsum = wi + wj;
+      double corr = diff / (2. * scp * (double)wsum);
+      xi.x += xxij[0] * corr * (double)wi; xi.y += xxij[1] * corr * (double)wi; xi.z += xxij[2] * corr * (double)wi;
+      xj.x -= xxij[0] * corr * (double)wj; xj.y -= xxij[1] * corr * (double)wj; xj.z -= xxij[2] * corr * (double)wj;
+      P.x[ij.x] = xi;
+      P.x[ij.y] = xj;
+    }
+    nits++;
+    done = true;
+    for (int c = 0; c < n && done; c++) done = (rd[c >> 6] >> (c & 63)) & 1ull;
+    if (!done && nits >= 1000) {
+      set_status(&P.st[P.sh_sys[m]], QB_ERR_SHAKE);
+      return;
+    }
+  }
+}
+
+// End of a step: velocities from the shaken coordinates, kinetic energy and
+// temperature (md.f90:3813), Berendsen factors, and the energy records of
+// md_run's output intervals.  mode 0: the initial temperature before the loop.
+__global__ void k_finish(DevPtrs P, int mode) {
+  int s = blockIdx.x;
+  const SysDev &S = P.sys[s];
+  SysState &st = P.st[s];
+  __shared__ double sh[32];
+  double acc[4] = {0, 0, 0, 0};  // solute all, solute free, solvent all, solvent free
+  for (int il = threadIdx.x; il < S.natom; il += blockDim.x) {
+    int g = S.aoff + il;
+    double4 v = P.v[g];
+    if (mode == 1 && S.has_shake) {
+      double4 x = P.x[g], xx = P.xx[g];
+      v.x = (x.x - xx.x) / S.dt;
+      v.y = (x.y - xx.y) / S.dt;
+      v.z = (x.z - xx.z) / S.dt;
+      P.v[g] = v;
+    }
+    double e = 0.5 * P.mass[g] * (v.x * v.x + v.y * v.y + v.z * v.z);
+    bool free_ = !(P.flags[g] & F_EXCL);
+    if (il < S.nsol) { acc[0] += e; if (free_) acc[1] += e; }
+    else { acc[2] += e; if (free_) acc[3] += e; }
+  }
+  double tot[4];
+  for (int k = 0; k < 4; k++) tot[k] = block_sum(acc[k], sh);
+  if (threadIdx.x == 0) {
+    const double kb = (double)kBoltzF;
+    double Tfree_sol = tot[1], Tfree_solv = tot[3];
+    double Tfree = Tfree_solv + Tfree_sol;
+    double Temp = tot[0] + tot[2];
+    st.kinetic = Temp;
+    Temp = 2.0 * Temp / kb / (double)(float)S.Ndegf;
+    Tfree = 2.0 * Tfree / kb / (double)(float)S.Ndegfree;
+    if (S.detail_temps) {
+      Tfree_sol = 2.0 * Tfree_sol / kb / (double)(float)S.Ndegfree_sol;
+      Tfree_solv = 2.0 * Tfree_solv / kb / (double)(float)S.Ndegfree_solv;
+    }
+    double a = S.dt / S.tau_T;
+    if (S.separate_scaling) {
+      if (Tfree_solv != 0) st.Tscale_solv = S.Temp0 / Tfree_solv - 1.0;
+      st.Tscale_solv = sqrt(1 + a * st.Tscale_solv);
+      if (Tfree_sol != 0) st.Tscale_sol = S.Temp0 / Tfree_sol - 1.0;
+      st.Tscale_sol = sqrt(1 + a * st.Tscale_sol);
+    } else {
+      if (Tfree != 0) st.Tscale_solv = S.Temp0 / Tfree - 1.0;
+      st.Tscale_solv = sqrt(1 + a * st.Tscale_solv);
+      st.Tscale_sol = st.Tscale_solv;
+    }
+    st.Temp = Temp;
+    st.Tfree = Tfree;
+    st.Tfree_sol = Tfree_sol;
+    st.Tfree_solv = Tfree_solv;
+    if (mode == 1) {
+      P.E[s * QB_NE + QB_E_KINETIC] = st.kinetic;
+      int is = st.istep;
+      int rec_len = QB_NE + MAXS * QB_NEQ + 1;
+      for (int kind = 0; kind < 2; kind++) {
+        int cyc = kind == 0 ? S.iout : S.iene;
+        bool want = (is % cyc == 0) && (kind == 0 || is > 0);
+        if (!want) continue;
+        int c = st.hist_n[kind];
+        if (c < P.hist_cap) {
+          double *r = P.hist + (((size_t)kind * P.nsys + s) * P.hist_cap + c) * rec_len;
+          r[0] = (double)is;
+          for (int k = 0; k < QB_NE; k++) r[1 + k] = P.E[s * QB_NE + k];
+          for (int k = 0; k < MAXS * QB_NEQ; k++) r[1 + QB_NE + k] = P.EQ[(size_t)s * MAXS * QB_NEQ + k];
+        }
+        st.hist_n[kind] = c + 1;
+      }
+      st.istep = is + 1;
+    }
+  }
+}
+
+}  // namespace qb

@@ -209,3 +209,8 @@ double fortran_pi();
 double fortran_deg2rad();
 
 }  // namespace qb
+
+// Opaque handle of the C ABI: one prepared system.
+struct qb_handle {
+  qb::System sys;
+};

@@ -1,0 +1,108 @@
+"""GPU engine (libqb, through its C ABI) against the CPU oracle.
+
+Both run the same prepared system.  Tolerances follow the parity bar of this
+path: every energy term and per-state energy within 1e-3 kcal/mol, gradients
+within 1e-4 relative (per atom, relative to the larger of the atom's gradient
+norm and 1% of the RMS gradient), in FP64.
+"""
+import numpy as np
+import pytest
+
+from q_b200 import FP64, MIXED, Batch, E_NAMES, System
+
+pytestmark = pytest.mark.gpu
+
+E_TOL = 1e-3
+G_TOL = 1e-4
+
+
+def grad_err(g, ref):
+    g = g.reshape(-1, 3)
+    ref = ref.reshape(-1, 3)
+    nrm = np.linalg.norm(ref, axis=1)
+    floor = 0.01 * np.sqrt(np.mean(nrm ** 2)) + 1e-12
+    return float(np.max(np.linalg.norm(g - ref, axis=1) / np.maximum(nrm, floor)))
+
+
+def energy_diffs(Eg, EQg, Eo, EQo):
+    out = {n: abs(a - b) for n, a, b in zip(E_NAMES, Eg, Eo)}
+    if EQo.size:
+        out["EQ"] = float(np.max(np.abs(EQg - EQo)))
+    return out
+
+
+def assert_energies(Eg, EQg, Eo, EQo, tol=E_TOL):
+    d = energy_diffs(Eg, EQg, Eo, EQo)
+    bad = {k: v for k, v in d.items() if v > tol}
+    assert not bad, bad
+
+
+def single_point(oracle, inp):
+    sys_ = System.open(inp)
+    b = Batch([sys_], precision=FP64)
+    b.run(1)
+    o = oracle.create(sys_)
+    o.run(1)
+    return sys_, b, o
+
+
+@pytest.mark.parametrize("case", ["test1", "benzene"])
+def test_step0_energies_and_gradient(golden, oracle, case):
+    inp = str(golden / case / "eq1.inp")
+    sys_, b, o = single_point(oracle, inp)
+    # energies of step 0 are the first output record of both engines
+    _, Eg, EQg = b.history(0, 0)
+    _, Eo, EQo = o.history(0)
+    assert_energies(Eg[0], EQg[0], Eo[0], EQo[0])
+
+
+@pytest.mark.parametrize("case", ["test1", "benzene"])
+def test_gradient_single_point(golden, oracle, case):
+    inp = str(golden / case / "eq1.inp")
+    sys_ = System.open(inp)
+    b = Batch([sys_], precision=FP64)
+    b.final_energy()          # lists + potential at the starting coordinates
+    o = oracle.create(sys_)
+    o.final_energy()
+    Eg, EQg = b.energy_vectors(0)
+    Eo, EQo = o.energy_vectors()
+    assert_energies(Eg, EQg, Eo, EQo)
+    assert grad_err(b.gradient(0), o.gradient()) < G_TOL
+
+
+def test_test1_trajectory_matches_oracle(golden, oracle):
+    """100 steps of eq1 (LRF, SHAKE, restraints, watpol): output records at
+    steps 0 and 50 and the FINAL energies."""
+    inp = str(golden / "test1" / "eq1.inp")
+    sys_ = System.open(inp)
+    b = Batch([sys_], precision=FP64)
+    o = oracle.create(sys_)
+    b.run(100)
+    o.run(100)
+    sg, Eg, EQg = b.history(0, 0)
+    so, Eo, EQo = o.history(0)
+    assert list(sg) == list(so) == [0, 50]
+    for k in range(2):
+        assert_energies(Eg[k], EQg[k], Eo[k], EQo[k])
+    b.final_energy()
+    o.final_energy()
+    Eg, EQg = b.energy_vectors(0)
+    Eo, EQo = o.energy_vectors()
+    assert_energies(Eg, EQg, Eo, EQo)
+    x_err = np.max(np.abs(b.coords(0) - o.coords()))
+    assert x_err < 1e-6
+
+
+def test_batch_of_systems_is_independent(golden, oracle):
+    """A batch of different systems gives each system its own-run results."""
+    a = System.open(str(golden / "test1" / "eq1.inp"))
+    c = System.open(str(golden / "benzene" / "eq1.inp"))
+    b = Batch([a, c, a], precision=FP64)
+    b.run(3)
+    o = oracle.create(a)
+    o.run(3)
+    _, Eo, EQo = o.history(0)
+    for s in (0, 2):
+        _, Eg, EQg = b.history(s, 0)
+        assert_energies(Eg[0], EQg[0], Eo[0], EQo[0])
+    assert np.max(np.abs(b.coords(0) - b.coords(2))) < 1e-9

@@ -90,7 +90,8 @@ void qb_close(qb_handle *h);
 /* ------------------------------------------------------------------ batch */
 
 /* Upload n prepared systems to the GPU and compute their initial temperatures
- * (md.f90:3960-3963).  All systems must share NBcycle. */
+ * (md.f90:3960-3963).  Systems step together; each keeps its own pair-list
+ * interval, output intervals and parameters. */
 int qb_batch_create(qb_handle *const *systems, int n, const qb_options *opt, qb_batch **out);
 
 /* Advance every system by nsteps MD steps with md_run's per-step semantics

@@ -118,25 +118,34 @@ struct Batch {
 
   static int cdiv(long long a, long long b) { return (int)std::max<long long>(1, (a + b - 1) / b); }
 
-  void build_lists() {
+  // Pair lists and LRF multipoles of the systems due at this step
+  // (force: every system, as the post-loop rebuild).
+  void build_lists(int force) {
     DevPtrs &p = P;
     dim3 b256(256);
     if (any_lrf)
-      launch("cgp_centers", [&] { k_cgp_centers<<<cdiv(p.ncgp_tot, 256), b256, 0, stream>>>(p); });
-    launch("lists_begin", [&] { k_lists_begin<<<cdiv(nsys, 128), 128, 0, stream>>>(p); });
+      launch("cgp_centers", [&] { k_cgp_centers<<<cdiv(p.ncgp_tot, 256), b256, 0, stream>>>(p, force); });
+    launch("lists_begin", [&] { k_lists_begin<<<cdiv(nsys, 128), 128, 0, stream>>>(p, force); });
     if (max_ncgp_sol > 0) {
-      launch("list_pp", [&] { k_list_pp<<<dim3(max_ncgp_sol, nsys), 128, 0, stream>>>(p); });
-      if (max_nwat > 0) launch("list_pw", [&] { k_list_pw<<<dim3(max_ncgp_sol, nsys), 256, 0, stream>>>(p); });
+      launch("list_pp", [&] { k_list_pp<<<dim3(max_ncgp_sol, nsys), 128, 0, stream>>>(p, force); });
+      if (max_nwat > 0) launch("list_pw", [&] { k_list_pw<<<dim3(max_ncgp_sol, nsys), 256, 0, stream>>>(p, force); });
     }
     if (any_q) {
-      launch("list_qp", [&] { k_list_qp<<<nsys, 256, 0, stream>>>(p, 0); });
-      if (max_nwat > 0) launch("list_qw", [&] { k_list_qw<<<nsys, 256, 0, stream>>>(p, 0); });
+      launch("list_qp", [&] { k_list_qp<<<nsys, 256, 0, stream>>>(p, force); });
+      if (max_nwat > 0) launch("list_qw", [&] { k_list_qw<<<nsys, 256, 0, stream>>>(p, force); });
     }
-    if (max_nwat > 0) launch("list_ww", [&] { k_list_ww<<<dim3(cdiv(max_nwat, 8), nsys), 256, 0, stream>>>(p); });
+    if (max_nwat > 0)
+      launch("list_ww", [&] { k_list_ww<<<dim3(cdiv(max_nwat, 8), nsys), 256, 0, stream>>>(p, force); });
     if (any_lrf)
-      launch("lrf_gather", [&] { k_lrf_gather<<<cdiv((long long)p.ncgp_tot * 32, 128), 128, 0, stream>>>(p); });
-    launch("lists_end", [&] { k_lists_end<<<cdiv(nsys, 128), 128, 0, stream>>>(p); });
+      launch("lrf_gather", [&] { k_lrf_gather<<<cdiv((long long)p.ncgp_tot * 32, 128), 128, 0, stream>>>(p, force); });
+    launch("lists_end", [&] { k_lists_end<<<cdiv(nsys, 128), 128, 0, stream>>>(p, force); });
     check_launch("list kernels");
+  }
+
+  bool lists_due() const {
+    for (auto &S : sysh)
+      if (istep % S.NB == 0) return true;
+    return false;
   }
 
   void pot_energy() {
@@ -169,7 +178,7 @@ struct Batch {
 
   void step() {
     DevPtrs &p = P;
-    if (istep % NB == 0) build_lists();
+    if (lists_due()) build_lists(0);
     pot_energy();
     launch("leapfrog", [&] { k_leapfrog<<<cdiv(p.natoms_tot, 256), 256, 0, stream>>>(p); });
     if (any_shake && p.nshake_tot > 0)
@@ -211,8 +220,6 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     hs[s]->sys.fill_view(&B.views[s]);
   }
   B.NB = B.views[0].NBcycle;
-  for (auto &v : B.views)
-    if (v.NBcycle != B.NB) fail(QB_ERR_ARG, "all systems of a batch must share the non_bond interval");
 
   // host staging
   std::vector<double4> x, v, d0;
@@ -665,7 +672,7 @@ int qb_batch_final_energy(qb_batch *bb) {
   if (!bb) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
   return guarded_batch([&] {
     Batch &B = bb->b;
-    B.build_lists();
+    B.build_lists(1);
     B.pot_energy();
     B.sync_status();
   });

@@ -44,10 +44,17 @@ __device__ __forceinline__ double dev_pi() { return (double)(4.0f * atanf(1.0f))
 
 // ------------------------------------------------------------------ lists
 
+// Lists of system s are rebuilt at steps that are multiples of its non_bond
+// interval (md.f90:4005), or on request (the post-loop rebuild, md.f90:4186).
+__device__ __forceinline__ bool list_due(const DevPtrs &P, int s, int force) {
+  return force || (P.st[s].istep % P.sys[s].NB) == 0;
+}
+
 // cgp_centers (md.f90:1000): group centres, multipoles zeroed.
-__global__ void k_cgp_centers(DevPtrs P) {
+__global__ void k_cgp_centers(DevPtrs P, int force) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= P.ncgp_tot) return;
+  if (!list_due(P, P.cg_sys[g], force)) return;
   double c[3] = {0, 0, 0};
   int f = P.cg_first[g], l = P.cg_last[g];
   for (int a = f; a <= l; a++) {
@@ -101,11 +108,12 @@ __device__ __forceinline__ void lrf_accumulate(double *m, double q, double dx, d
 // RcLRF (both switching atoms inside the sphere; Q atoms carry no charge here).
 // The reference visits each unordered pair once and adds to both groups; the
 // gather adds the same contributions.  One warp per group.
-__global__ void k_lrf_gather(DevPtrs P) {
+__global__ void k_lrf_gather(DevPtrs P, int force) {
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (warp >= P.ncgp_tot) return;
   int g = warp;
   int s = P.cg_sys[g];
+  if (!list_due(P, s, force)) return;
   const SysDev &S = P.sys[s];
   int swg = P.cg_sw[g];
   if (P.flags[swg] & F_EXCL) return;
@@ -144,8 +152,9 @@ __global__ void k_lrf_gather(DevPtrs P) {
 // Water-water neighbour list (nbwwlist / nbwwlist_lrf, md.f90:8233, 8370),
 // stored in both directions: water i lists every other water j inside the
 // sphere whose O lies within Rcww of i's O.  One warp per water.
-__global__ void k_list_ww(DevPtrs P) {
+__global__ void k_list_ww(DevPtrs P, int force) {
   int s = blockIdx.y;
+  if (!list_due(P, s, force)) return;
   const SysDev &S = P.sys[s];
   int wpb = blockDim.x >> 5;
   int iw = blockIdx.x * wpb + (threadIdx.x >> 5), lane = threadIdx.x & 31;
@@ -222,8 +231,9 @@ __device__ __forceinline__ bool zero_pair(const DevPtrs &P, int i, int j, int lj
 
 // Solute-solute pair list (nbpplist, md.f90:5175): block (ig, system),
 // threads over jg.  Group pairs are taken once, by the reference's parity rule.
-__global__ void k_list_pp(DevPtrs P) {
+__global__ void k_list_pp(DevPtrs P, int force) {
   int s = blockIdx.y;
+  if (!list_due(P, s, force)) return;
   const SysDev &S = P.sys[s];
   int ig = blockIdx.x;
   if (ig >= S.ncgp_sol) return;
@@ -260,8 +270,9 @@ __global__ void k_list_pp(DevPtrs P) {
 
 // Solute-water pair list (nbpwlist, md.f90:6684): block (ig, system),
 // threads over waters.
-__global__ void k_list_pw(DevPtrs P) {
+__global__ void k_list_pw(DevPtrs P, int force) {
   int s = blockIdx.y;
+  if (!list_due(P, s, force)) return;
   const SysDev &S = P.sys[s];
   int ig = blockIdx.x;
   if (ig >= S.ncgp_sol) return;
@@ -295,8 +306,8 @@ __global__ void k_list_pw(DevPtrs P) {
 __global__ void k_list_qp(DevPtrs P, int force) {
   int s = blockIdx.x;
   const SysDev &S = P.sys[s];
-  if (S.nq == 0) return;
-  if (!force && S.qp_once && P.st[s].lists_built) return;
+  if (S.nq == 0 || !list_due(P, s, force)) return;
+  if (S.qp_once && P.st[s].lists_built) return;
   __syncthreads();
   if (threadIdx.x == 0) P.st[s].qp_n = 0;
   __syncthreads();
@@ -332,8 +343,8 @@ __global__ void k_list_qp(DevPtrs P, int force) {
 __global__ void k_list_qw(DevPtrs P, int force) {
   int s = blockIdx.x;
   const SysDev &S = P.sys[s];
-  if (S.nq == 0) return;
-  if (!force && S.qp_once && P.st[s].lists_built) return;
+  if (S.nq == 0 || !list_due(P, s, force)) return;
+  if (S.qp_once && P.st[s].lists_built) return;
   __shared__ int base;
   if (threadIdx.x == 0) base = 0;
   __syncthreads();
@@ -370,16 +381,16 @@ __global__ void k_list_qw(DevPtrs P, int force) {
   if (threadIdx.x == 0) P.st[s].qw_n = base < S.qw_cap ? base : S.qw_cap;
 }
 
-__global__ void k_lists_begin(DevPtrs P) {
+__global__ void k_lists_begin(DevPtrs P, int force) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= P.nsys) return;
+  if (s >= P.nsys || !list_due(P, s, force)) return;
   P.st[s].pp_n = 0;
   P.st[s].pw_n = 0;
 }
 
-__global__ void k_lists_end(DevPtrs P) {
+__global__ void k_lists_end(DevPtrs P, int force) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= P.nsys) return;
+  if (s >= P.nsys || !list_due(P, s, force)) return;
   SysState &st = P.st[s];
   const SysDev &S = P.sys[s];
   if (st.pp_n > S.pp_cap) st.pp_n = S.pp_cap;
@@ -563,11 +574,13 @@ __global__ void k_nb_qw(DevPtrs P) {
   for (int st = 0; st < MAXS; st++) { el[st] = 0; vdw[st] = 0; }
   for (int k0 = blockIdx.x * blockDim.x; k0 < n; k0 += gridDim.x * blockDim.x) {
     int k = k0 + threadIdx.x;
-    if (k < n) {
-      int j = P.qw[S.qw_off + k];
+    bool act = k < n;
+    int j = act ? P.qw[S.qw_off + k] : P.qw[S.qw_off];
+    {
       double3 xO = ld3(P.x, j), xH1 = ld3(P.x, j + 1), xH2 = ld3(P.x, j + 2);
       double fw[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
       for (int iq = 0; iq < S.nq; iq++) {
+        double qacc[3] = {0, 0, 0};
         int gq = S.qoff + iq;
         int i = P.iqseq[gq];
         double3 xi = ld3(P.x, i);
@@ -604,8 +617,10 @@ __global__ void k_nb_qw(DevPtrs P) {
           dvO += r2O * (-VelO - ((12. * Va - 6. * Vb) * (r6hc / r6sc))) * lam;
           dvH1 -= r2H1 * VelH1 * lam;
           dvH2 -= r2H2 * VelH2 * lam;
-          el[st] += VelO + VelH1 + VelH2;
-          vdw[st] += Va - Vb;
+          if (act) {
+            el[st] += VelO + VelH1 + VelH2;
+            vdw[st] += Va - Vb;
+          }
         }
         double fi[3];
         for (int c = 0; c < 3; c++) {
@@ -614,19 +629,22 @@ __global__ void k_nb_qw(DevPtrs P) {
           fw[3 + c] += dvH1 * dH1[c];
           fw[6 + c] += dvH2 * dH2[c];
         }
-        if (shq) {
-          atomicAdd(&fq[3 * iq], fi[0]);
-          atomicAdd(&fq[3 * iq + 1], fi[1]);
-          atomicAdd(&fq[3 * iq + 2], fi[2]);
-        } else {
-          atomic_add3(P.d, i, fi[0], fi[1], fi[2]);
+        if (act) { qacc[0] = fi[0]; qacc[1] = fi[1]; qacc[2] = fi[2]; }
+        // Q-atom gradient: warp reduction, then one shared atomic per warp
+        for (int c = 0; c < 3; c++) {
+          double t = warp_sum(qacc[c]);
+          if ((threadIdx.x & 31) == 0 && t != 0.0) {
+            if (shq) atomicAdd(&fq[3 * iq + c], t);
+            else atomicAdd(&P.d[i].x + c, t);
+          }
         }
       }
-      for (int a = 0; a < 3; a++) {
-        double4 dd = P.d[j + a];
-        dd.x += fw[3 * a]; dd.y += fw[3 * a + 1]; dd.z += fw[3 * a + 2];
-        P.d[j + a] = dd;
-      }
+      if (act)
+        for (int a = 0; a < 3; a++) {
+          double4 dd = P.d[j + a];
+          dd.x += fw[3 * a]; dd.y += fw[3 * a + 1]; dd.z += fw[3 * a + 2];
+          P.d[j + a] = dd;
+        }
     }
   }
   for (int st = 0; st < NS; st++) {
@@ -1180,7 +1198,7 @@ __global__ void k_prestrain(DevPtrs P) {
 // system.  Waters are assigned to shells by O radius, ordered within a shell
 // by angle theta (ties by water index, as the reference's selection sort
 // does), and restrained to theta_0(rank).
-__global__ void k_watpol(DevPtrs P) {
+__global__ void __launch_bounds__(1024, 1) k_watpol(DevPtrs P) {
   extern __shared__ unsigned char smem[];
   int s = blockIdx.x;
   const SysDev &S = P.sys[s];
@@ -1395,7 +1413,7 @@ __global__ void k_shake(DevPtrs P) {
 // End of a step: velocities from the shaken coordinates, kinetic energy and
 // temperature (md.f90:3813), Berendsen factors, and the energy records of
 // md_run's output intervals.  mode 0: the initial temperature before the loop.
-__global__ void k_finish(DevPtrs P, int mode) {
+__global__ void __launch_bounds__(512) k_finish(DevPtrs P, int mode) {
   int s = blockIdx.x;
   const SysDev &S = P.sys[s];
   SysState &st = P.st[s];

@@ -101,6 +101,11 @@ int qb_batch_create(qb_handle *const *systems, int n, const qb_options *opt, qb_
  * Replaces: the `do istep` loop of md_run, src/q6/md.f90:4003-4175. */
 int qb_batch_run(qb_batch *b, int nsteps);
 
+/* qb_batch_run with the step loop bracketed by CUDA events on the batch
+ * stream: device_ms receives the elapsed device time of the nsteps steps and
+ * kernel_launches the number of kernels launched for them (either may be NULL). */
+int qb_batch_run_timed(qb_batch *b, int nsteps, double *device_ms, long long *kernel_launches);
+
 /* The post-loop evaluation of md_run (md.f90:4186-4188): rebuild the lists and
  * evaluate the potential at the final coordinates, for the FINAL summary. */
 int qb_batch_final_energy(qb_batch *b);
@@ -149,6 +154,11 @@ int qb_batch_profile(qb_batch *b, char *names, size_t names_len, double *ms,
 int qb_batch_workload(qb_batch *b, double *out, int n);
 
 void qb_batch_destroy(qb_batch *b);
+
+/* Measured FMA throughput of the CUDA cores of `device` (TFLOP/s, FMA = 2
+ * FLOP) in FP64 (precision QB_FP64) or FP32 (QB_MIXED): the denominator of the
+ * pair kernels' roofline. */
+int qb_peak_flops(int device, int precision, double *tflops);
 
 /* ------------------------------------------------------------------ files */
 

@@ -113,6 +113,8 @@ def _load():
         "qb_batch_create": (C.c_int, [C.POINTER(vp), C.c_int, C.POINTER(Options), C.POINTER(vp)]),
         "qb_batch_run": (C.c_int, [vp, C.c_int]),
         "qb_batch_final_energy": (C.c_int, [vp]),
+        "qb_batch_run_timed": (C.c_int, [vp, C.c_int, dp, C.POINTER(C.c_longlong)]),
+        "qb_peak_flops": (C.c_int, [C.c_int, C.c_int, dp]),
         "qb_batch_energies": (C.c_int, [vp, C.c_int, dp, dp]),
         "qb_batch_temperature": (C.c_int, [vp, C.c_int, dp]),
         "qb_batch_gradient": (C.c_int, [vp, C.c_int, dp]),

@@ -86,6 +86,13 @@ class Batch:
     def run(self, nsteps: int) -> None:
         check(lib.qb_batch_run(self._b, int(nsteps)))
 
+    def run_timed(self, nsteps: int) -> tuple[float, int]:
+        """Run nsteps; return (device milliseconds, kernel launches)."""
+        ms = C.c_double()
+        n = C.c_longlong()
+        check(lib.qb_batch_run_timed(self._b, int(nsteps), C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
     def final_energy(self) -> None:
         check(lib.qb_batch_final_energy(self._b))
 
@@ -192,6 +199,13 @@ def device_count() -> int:
     n = C.c_int()
     lib.qb_device_count(C.byref(n))
     return n.value
+
+
+def peak_tflops(precision: int = FP64, device: int = 0) -> float:
+    """Measured CUDA-core FMA throughput (TFLOP/s)."""
+    t = C.c_double()
+    check(lib.qb_peak_flops(device, precision, C.byref(t)))
+    return t.value
 
 
 def write_restart(path: str, x: np.ndarray, v: np.ndarray, theta_corr: np.ndarray | None = None) -> None:

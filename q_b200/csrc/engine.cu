@@ -85,8 +85,11 @@ struct Batch {
     return e;
   }
 
+  long long launches = 0;
+
   template <class F>
   void launch(const char *name, F &&f) {
+    launches++;
     if (!profiling) { f(); return; }
     cudaEvent_t a = take_event(), b = take_event();
     CUDA_TRY(cudaEventRecord(a, stream));
@@ -602,6 +605,23 @@ int guarded_batch(F &&f) {
 
 }  // namespace qb
 
+namespace qb {
+namespace {
+// FMA throughput probe: 8 independent FMA chains per thread.
+template <class T>
+__global__ void k_fma_peak(T *out, int iters, T a, T b) {
+  T x[8];
+  for (int k = 0; k < 8; k++) x[k] = (T)(threadIdx.x + k);
+  for (int it = 0; it < iters; it++)
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = x[k] * a + b;
+  T s = 0;
+  for (int k = 0; k < 8; k++) s += x[k];
+  if (s == (T)-1.2345) out[0] = s;
+}
+}  // namespace
+}  // namespace qb
+
 struct qb_batch {
   qb::Batch b;
 };
@@ -665,6 +685,32 @@ int qb_batch_run(qb_batch *bb, int nsteps) {
     }
     double w[8] = {ww / 2, pw, pp, qp, qw, (double)B.P.natoms_tot, sh, cg};
     std::memcpy(B.workload, w, sizeof w);
+  });
+}
+
+int qb_batch_run_timed(qb_batch *bb, int nsteps, double *device_ms, long long *kernel_launches) {
+  if (!bb || nsteps < 0) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
+  return guarded_batch([&] {
+    Batch &B = bb->b;
+    CUDA_TRY(cudaSetDevice(B.opt.device));
+    qb::ensure_history(B, nsteps);
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    long long l0 = B.launches;
+    CUDA_TRY(cudaStreamSynchronize(B.stream));
+    CUDA_TRY(cudaEventRecord(e0, B.stream));
+    for (int k = 0; k < nsteps; k++) B.step();
+    CUDA_TRY(cudaEventRecord(e1, B.stream));
+    CUDA_TRY(cudaEventSynchronize(e1));
+    float ms = 0;
+    CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (device_ms) *device_ms = ms;
+    if (kernel_launches) *kernel_launches = B.launches - l0;
+    if (B.profiling) B.collect();
+    B.sync_status();
   });
 }
 
@@ -827,5 +873,39 @@ int qb_batch_workload(qb_batch *bb, double *out, int n) {
 }
 
 void qb_batch_destroy(qb_batch *bb) { delete bb; }
+
+
+int qb_peak_flops(int device, int precision, double *tflops) {
+  if (!tflops) return QB_ERR_ARG;
+  return guarded_batch([&] {
+    CUDA_TRY(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    int blocks = prop.multiProcessorCount * 8, threads = 256, iters = 1 << 14;
+    void *buf = nullptr;
+    CUDA_TRY(cudaMalloc(&buf, 64));
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; rep++) {
+      CUDA_TRY(cudaEventRecord(e0));
+      if (precision == QB_FP64)
+        qb::k_fma_peak<double><<<blocks, threads>>>((double *)buf, iters, 0.999999, 1e-7);
+      else
+        qb::k_fma_peak<float><<<blocks, threads>>>((float *)buf, iters, 0.999999f, 1e-7f);
+      CUDA_TRY(cudaEventRecord(e1));
+      CUDA_TRY(cudaEventSynchronize(e1));
+      float ms;
+      CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+      if (rep > 0) best = std::min(best, ms);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(buf);
+    double flop = 2.0 * 8.0 * iters * (double)blocks * threads;
+    *tflops = flop / (best * 1e-3) / 1e12;
+  });
+}
 
 }  // extern "C"

@@ -117,7 +117,7 @@ class Records {
   // read(u,*) v1..vn: list-directed values across records
   std::vector<std::string> values(size_t n) {
     std::vector<std::string> out;
-    if (n == 0) { skip(); return out; }
+    if (n == 0) return out;  // `if (n > 0) read(...)` in the reference: nothing consumed
     while (out.size() < n) {
       if (eof()) err("unexpected end of file reading values");
       bool slash = false;

@@ -1,0 +1,680 @@
+"""Seeded synthetic Q systems of the benchmark shapes, written as Q files.
+
+The generator writes the Q topology format of topo_save (src/q6/topo.f90:1082,
+same records and column formats), FEP files in the [section] format read by
+qatom_load_fep (qatom.f90:874) and qdyn .inp files (md.f90:2528), so the engine
+reads them through the same readers as any Q input.
+
+Shapes (one generator per configuration):
+  water_sphere(R)   TIP3P on a cubic lattice at 0.0334 / A^3 inside radius R,
+                    seeded random orientations (config 0: R = 15).
+  fep_solute(...)   a 32-heavy-atom random tree with hydrogens up to 56 atoms,
+                    charges ~N(0, 0.3) shifted to net 0, LJ from a 6-type
+                    table, harmonic bonds/angles, periodic torsions (n=1..3),
+                    periodic impropers on 3-connected centres, 8 Q-atoms with
+                    two states (state 2: charge 0, epsilon x 0.5, soft-core),
+                    solvated in a TIP3P sphere (config 1: R = 20).
+  polymer_sphere()  a 3000-atom self-avoiding polymer walk (1.5 A steps,
+                    non-bonded atoms >= 2.5 A apart) around the config-1 solute
+                    in a 25 A sphere, charge groups of 10-15 atoms with net
+                    charge -1/0/+1, atoms beyond 23 A excluded (restrained at
+                    200 kcal/mol/A^2), remaining volume filled with water
+                    (config 2).
+Everything is deterministic in the seed (1234 + system id by default).
+"""
+from __future__ import annotations
+
+import math
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+DENSITY = 0.0334          # molecules / A^3
+R_OH, ANG_HOH = 0.9572, 104.52
+Q_O, Q_H = -0.834, 0.417
+SIG_O, EPS_O = 3.15061, 0.1521
+# the 6-type LJ table: sigma 3.0-3.5 A, epsilon 0.05-0.2 kcal/mol
+TYPE_TABLE = [(3.00, 0.050, 12.011), (3.10, 0.080, 12.011), (3.20, 0.110, 14.007),
+              (3.30, 0.140, 15.999), (3.40, 0.170, 12.011), (3.50, 0.200, 32.060)]
+SIG_H, EPS_H, M_H = 2.50, 0.030, 1.008
+
+
+def lj_sqrt(sigma: float, eps: float) -> tuple[float, float]:
+    """Q's geometric-rule sqrt(A), sqrt(B) with A = 4 eps sigma^12, B = 4 eps sigma^6."""
+    return 2.0 * math.sqrt(eps) * sigma ** 6, 2.0 * math.sqrt(eps) * sigma ** 3
+
+
+@dataclass
+class AtomType:
+    name: str
+    mass: float
+    sigma: float
+    eps: float
+
+    def columns(self):
+        a, b = lj_sqrt(self.sigma, self.eps)
+        # normal, polar, 1-4 (1-4 LJ at half epsilon)
+        return [(a, b), (a, b), (a / math.sqrt(2.0), b / math.sqrt(2.0))]
+
+
+@dataclass
+class Topology:
+    """Atoms and terms of a Q topology; indices are 0-based here."""
+    title: str = "synthetic"
+    x: list = field(default_factory=list)
+    iac: list = field(default_factory=list)
+    crg: list = field(default_factory=list)
+    types: list = field(default_factory=list)
+    bonds: list = field(default_factory=list)        # (i, j, code)
+    bond_lib: list = field(default_factory=list)     # (fk, b0)
+    angles: list = field(default_factory=list)       # (i, j, k, code)
+    angle_lib: list = field(default_factory=list)    # (fk, th0_deg)
+    tors: list = field(default_factory=list)         # (i, j, k, l, code)
+    tor_lib: list = field(default_factory=list)      # (fk, rmult, delta_deg, paths)
+    imps: list = field(default_factory=list)
+    imp_lib: list = field(default_factory=list)      # (fk, imp0_deg)
+    cgps: list = field(default_factory=list)         # (switch, [atoms])
+    mol_starts: list = field(default_factory=list)
+    res_starts: list = field(default_factory=list)
+    res_names: list = field(default_factory=list)
+    nat_solute: int = 0
+    nbonds_solute: int = 0
+    nangles_solute: int = 0
+    ntors_solute: int = 0
+    nimps_solute: int = 0
+    ncgp_solute: int = 0
+    excl14: tuple = ((), ())                         # (exclusion pairs, 1-4 pairs) of solute atoms
+    rexcl_o: float = 20.0
+    rwat: float = 20.0
+    excl: list = field(default_factory=list)
+
+    # ----------------------------------------------------------- writer
+    def write(self, path: str) -> None:
+        n = len(self.x)
+        ns = self.nat_solute
+        L = []
+        L.append("Q topology file")
+        L.append("TITLE      %s" % self.title)
+        L.append("DATE       synthetic")
+        L.append("VERSION     6.01")
+        L.append("FORCEFIELD synthetic-geometric")
+        L.append("FF_TYPE    2")
+        L.append("PRM_FILE   none")
+        L.append("END        of header")
+        L.append("%8d%8d = Total no. of atoms, no. of solute atoms. Coordinates: (2*3 per line)" % (n, ns))
+        flat = [c for p in self.x for c in p]
+        for k in range(0, len(flat), 6):
+            L.append(" ".join("%9.3f" % v for v in flat[k:k + 6]))
+        L.append("%8d = No. of integer atom codes. iac's: " % n)
+        for k in range(0, n, 16):
+            L.append(" ".join("%4d" % (t + 1) for t in self.iac[k:k + 16]))
+        L.append("%8d%8d = No. of bonds, no. of solute bonds. i - j - icode: (5 per line)"
+                 % (len(self.bonds), self.nbonds_solute))
+        for k in range(0, len(self.bonds), 5):
+            L.append(" ".join("%5d %5d %3d" % (i + 1, j + 1, c) for i, j, c in self.bonds[k:k + 5]))
+        L.append("%8d = No. of bond codes. Parameters: " % len(self.bond_lib))
+        for k, (fk, b0) in enumerate(self.bond_lib):
+            L.append("%5d%9.3f %10.4f" % (k + 1, fk, b0))
+        L.append("%8d%8d = No. of angles, no. of solute angles. i - j - k - icode: (3 per line)"
+                 % (len(self.angles), self.nangles_solute))
+        for k in range(0, len(self.angles), 3):
+            L.append(" ".join("%5d %5d %5d %3d" % (i + 1, j + 1, kk + 1, c) for i, j, kk, c in self.angles[k:k + 3]))
+        L.append("%8d = No. of angle codes. Parameters:" % len(self.angle_lib))
+        for k, (fk, th) in enumerate(self.angle_lib):
+            L.append("%5d%9.3f %9.3f %9.3f %11.5f" % (k + 1, fk, th, 0.0, 0.0))
+        L.append("%8d%8d = No. of torsions, solute torsions. i - j - k - l - icode: (2 per line)"
+                 % (len(self.tors), self.ntors_solute))
+        for k in range(0, len(self.tors), 2):
+            L.append(" ".join("%5d %5d %5d %5d %3d" % (a + 1, b + 1, c + 1, d + 1, e)
+                              for a, b, c, d, e in self.tors[k:k + 2]))
+        L.append("%8d = No. of torsion codes. Parameters:" % len(self.tor_lib))
+        for k, (fk, rm, dl, pa) in enumerate(self.tor_lib):
+            L.append("%5d%9.3f %9.3f %9.3f %5d" % (k + 1, fk, rm, dl, pa))
+        L.append("%8d%8d = No. of impropers, solute impr. i - j - k - l - icode: (2 per line)"
+                 % (len(self.imps), self.nimps_solute))
+        for k in range(0, len(self.imps), 2):
+            L.append(" ".join("%5d %5d %5d %5d %3d" % (a + 1, b + 1, c + 1, d + 1, e)
+                              for a, b, c, d, e in self.imps[k:k + 2]))
+        L.append("%8d%8d = No. of improper codes, type (1=harmonic,2=periodic). Parameters:" % (len(self.imp_lib), 2))
+        for k, (fk, i0) in enumerate(self.imp_lib):
+            L.append("%5d%10.3f %10.3f" % (k + 1, fk, i0))
+        L.append("%8d = No. of atomic charges" % n)
+        for k in range(0, n, 10):
+            L.append(" ".join("%7.4f" % q for q in self.crg[k:k + 10]))
+        L.append("%8d%8d%8d = No. of charge groups, no of solvent cgps, switch atoms flag. nat_cgp, iswitch / atom list: "
+                 % (len(self.cgps), self.ncgp_solute, 1))
+        for sw, atoms in self.cgps:
+            L.append("%5d %5d" % (len(atoms), sw + 1))
+            for k in range(0, len(atoms), 13):
+                L.append(" ".join("%5d" % (a + 1) for a in atoms[k:k + 13]))
+        nt = len(self.types)
+        L.append("%8d = No. of atom types" % nt)
+        L.append("%8d = vdW combination rule (1 = Geom. / 2 = Arit.)" % 1)
+        L.append("%8.5f%9.4f = Electrostatic 1-4 scaling factor and  Coulomb constant" % (0.5, 332.0))
+        L.append("Masses: ")
+        for k in range(0, nt, 10):
+            L.append(" ".join("%7.3f" % t.mass for t in self.types[k:k + 10]))
+        cols = [t.columns() for t in self.types]
+        for c, label in enumerate(["normal", "polar", "1-4"]):
+            for ab, nm in ((0, "Aii"), (1, "Bii")):
+                L.append("sqrt (%s) %s:" % (nm, label))
+                vals = [cols[t][c][ab] for t in range(nt)]
+                for k in range(0, nt, 8):
+                    L.append(" ".join("%8.2f" % v for v in vals[k:k + 8]))
+        L.append("%8d = No. of type-2 vdW interactions. pairs: " % 0)
+        ex_pairs, p14_pairs = self.excl14
+        for pairs, label in ((p14_pairs, "1-4 neighbours"), (ex_pairs, "exclusions")):
+            bits = np.zeros((ns, 25), dtype=np.int8)
+            longp = []
+            for i, j in pairs:
+                a, b = min(i, j), max(i, j)
+                if b - a <= 25:
+                    bits[a, b - a - 1] = 1
+                else:
+                    longp.append((a, b))
+            digits = "".join(str(v) for v in bits.reshape(-1))
+            L.append("%8d = No. of %s. list (range=max_nbr_range): " % (len(pairs) - len(longp), label))
+            for k in range(0, len(digits), 80):
+                L.append(digits[k:k + 80])
+            L.append("%8d = No. of long %s (>max_nbr_range). pairlist: " % (len(longp), label))
+            for a, b in longp:
+                L.append("%5d %5d" % (a + 1, b + 1))
+        nres = len(self.res_starts)
+        L.append("%8d%8d = No. of residues, No of solute residues. start atoms: " % (nres, 1 if ns else 0))
+        for k in range(0, nres, 13):
+            L.append(" ".join("%5d" % (a + 1) for a in self.res_starts[k:k + 13]))
+        L.append("Sequence: ")
+        for k in range(0, nres, 16):
+            L.append(" ".join("%-4s" % nm for nm in self.res_names[k:k + 16]))
+        L.append("%8d = No. of separate molecules. start atoms:" % len(self.mol_starts))
+        for k in range(0, len(self.mol_starts), 13):
+            L.append(" ".join("%5d" % (a + 1) for a in self.mol_starts[k:k + 13]))
+        L.append("%8d = No. of atom types:" % nt)
+        for k in range(0, nt, 8):
+            L.append(" ".join("%-8s" % t.name for t in self.types[k:k + 8]))
+        L.append("%8d = No. of SYBYL atom types:" % nt)
+        for k in range(0, nt, 13):
+            L.append(" ".join("%-5s" % "" for _ in self.types[k:k + 13]))
+        L.append("%8d = solvent type (0=SPC,1=3-atom,2=general)" % 0)
+        L.append("%8.3f%8.3f = Exclusion, solvent radii" % (self.rexcl_o, self.rwat))
+        L.append("%8.3f%8.3f%8.3f = Solute center" % (0.0, 0.0, 0.0))
+        L.append("%8.3f%8.3f%8.3f = Solvent center" % (0.0, 0.0, 0.0))
+        excl = self.excl or [False] * n
+        nexwat = sum(1 for k in range(ns, n, 3) if excl[k])
+        L.append("%8d%8d = No. of excluded atoms (incl. water), no. of excluded waters" % (sum(excl), nexwat))
+        s = "".join("T" if e else "F" for e in excl)
+        for k in range(0, n, 80):
+            L.append(s[k:k + 80])
+        with open(path, "w") as f:
+            f.write("\n".join(L) + "\n")
+
+
+# ------------------------------------------------------------- geometry
+
+def _rot(rng) -> np.ndarray:
+    """Uniform random rotation (random unit quaternion)."""
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    w, x, y, z = q
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                     [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                     [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+
+
+def _water_template() -> np.ndarray:
+    h = math.radians(ANG_HOH / 2)
+    return np.array([[0, 0, 0], [R_OH * math.sin(h), R_OH * math.cos(h), 0],
+                     [-R_OH * math.sin(h), R_OH * math.cos(h), 0]])
+
+
+def lattice_waters(radius: float, rng, avoid: np.ndarray | None = None, r_o: float = 2.8,
+                   inner: float = 0.0) -> list[np.ndarray]:
+    """TIP3P waters on a cubic lattice at DENSITY, O within `radius` of the
+    origin (and beyond `inner`), seeded random orientations; waters with O
+    within r_o of an `avoid` atom are dropped."""
+    a = (1.0 / DENSITY) ** (1.0 / 3.0)
+    n = int(math.ceil(radius / a)) + 1
+    g = (np.arange(-n, n + 1) + 0.5) * a
+    P = np.array(np.meshgrid(g, g, g, indexing="ij")).reshape(3, -1).T
+    r = np.linalg.norm(P, axis=1)
+    P = P[(r <= radius) & (r >= inner)]
+    P = P[np.lexsort((P[:, 2], P[:, 1], P[:, 0]))]
+    if avoid is not None and len(avoid):
+        from scipy.spatial import cKDTree
+        d, _ = cKDTree(avoid).query(P)
+        P = P[d >= r_o]
+    t = _water_template()
+    return [p + t @ _rot(rng).T for p in P]
+
+
+def _add_waters(top: Topology, waters: list[np.ndarray], excl_radius: float | None = None) -> None:
+    types = {t.name: i for i, t in enumerate(top.types)}
+    if "OW" not in types:
+        top.types.append(AtomType("OW", 15.999, SIG_O, EPS_O))
+        top.types.append(AtomType("HW", 1.008, 0.0, 0.0))
+        types = {t.name: i for i, t in enumerate(top.types)}
+    ow, hw = types["OW"], types["HW"]
+    top.bond_lib.append((1106.0, R_OH))
+    cb_oh = len(top.bond_lib)
+    hh = 2 * R_OH * math.sin(math.radians(ANG_HOH / 2))
+    top.bond_lib.append((0.0, hh))
+    cb_hh = len(top.bond_lib)
+    top.angle_lib.append((200.0, ANG_HOH))
+    ca = len(top.angle_lib)
+    for w in waters:
+        o = len(top.x)
+        top.mol_starts.append(o)
+        top.res_starts.append(o)
+        top.res_names.append("HOH")
+        for k in range(3):
+            top.x.append(tuple(float(c) for c in w[k]))
+        top.iac += [ow, hw, hw]
+        top.crg += [Q_O, Q_H, Q_H]
+        top.bonds += [(o, o + 1, cb_oh), (o, o + 2, cb_oh), (o + 1, o + 2, cb_hh)]
+        top.angles.append((o + 1, o, o + 2, ca))
+        top.cgps.append((o, [o, o + 1, o + 2]))
+        if excl_radius is not None:
+            out = float(np.linalg.norm(w[0])) > excl_radius
+            top.excl += [out] * 3
+
+
+def _finish_solute_lists(top: Topology, bonds: list[tuple[int, int]], n: int) -> None:
+    """1-2/1-3 exclusions and 1-4 pairs from the bond graph of solute atoms."""
+    nb = [set() for _ in range(n)]
+    for i, j in bonds:
+        nb[i].add(j)
+        nb[j].add(i)
+    ex, p14 = set(), set()
+    for i in range(n):
+        for j in nb[i]:
+            ex.add((min(i, j), max(i, j)))
+            for k in nb[j]:
+                if k != i:
+                    ex.add((min(i, k), max(i, k)))
+    for i in range(n):
+        for j in nb[i]:
+            for k in nb[j]:
+                if k == i:
+                    continue
+                for l in nb[k]:
+                    if l in (i, j):
+                        continue
+                    p = (min(i, l), max(i, l))
+                    if p not in ex:
+                        p14.add(p)
+    top.excl14 = (sorted(ex), sorted(p14))
+
+
+def _angle(a, b, c) -> float:
+    u, v = a - b, c - b
+    return math.degrees(math.acos(max(-1.0, min(1.0, float(u @ v / (np.linalg.norm(u) * np.linalg.norm(v)))))))
+
+
+def random_tree_solute(rng, n_heavy: int = 32, n_total: int = 56):
+    """Heavy-atom tree with hydrogens; returns coordinates, element kinds
+    (type index or -1 for H), bonds."""
+    X = [np.zeros(3)]
+    bonds = []
+    deg = [0]
+    while len(X) < n_heavy:
+        for _ in range(2000):
+            p = int(rng.integers(len(X)))
+            if deg[p] >= 3:
+                continue
+            u = rng.normal(size=3)
+            u /= np.linalg.norm(u)
+            c = X[p] + u * rng.uniform(1.40, 1.54)
+            d = np.linalg.norm(np.array(X) - c, axis=1)
+            d[p] = 99
+            if d.min() < 2.5:
+                continue
+            if any(_angle(X[q], X[p], c) < 105 for (a, b) in bonds for q in ((b,) if a == p else (a,) if b == p else ())):
+                continue
+            X.append(c)
+            deg.append(1)
+            deg[p] += 1
+            bonds.append((p, len(X) - 1))
+            break
+        else:
+            raise RuntimeError("tree growth failed")
+    kinds = [int(rng.integers(len(TYPE_TABLE))) for _ in range(n_heavy)]
+    # hydrogens on heavy atoms with free valence, leaves first
+    order = sorted(range(n_heavy), key=lambda i: (deg[i], i))
+    need = n_total - n_heavy
+    while need > 0:
+        placed = False
+        for p in order:
+            if need == 0:
+                break
+            if deg[p] >= 4:
+                continue
+            for _ in range(500):
+                u = rng.normal(size=3)
+                u /= np.linalg.norm(u)
+                c = X[p] + u * 1.09
+                d = np.linalg.norm(np.array(X) - c, axis=1)
+                d[p] = 99
+                if d.min() < 2.0:
+                    continue
+                nbrs = [b if a == p else a for a, b in bonds if p in (a, b)]
+                if any(_angle(X[q], X[p], c) < 100 for q in nbrs):
+                    continue
+                X.append(c)
+                kinds.append(-1)
+                deg.append(1)
+                deg[p] += 1
+                bonds.append((p, len(X) - 1))
+                need -= 1
+                placed = True
+                break
+        if not placed:
+            raise RuntimeError("hydrogen placement failed")
+    X = np.array(X)
+    return X - X.mean(axis=0), kinds, bonds
+
+
+def _solute_terms(top: Topology, X: np.ndarray, bonds, rng, offset: int = 0, heavy_fk=600.0) -> None:
+    n = len(X)
+    nb = [[] for _ in range(n)]
+    for i, j in bonds:
+        nb[i].append(j)
+        nb[j].append(i)
+    for i, j in bonds:
+        b0 = float(np.linalg.norm(X[i] - X[j]))
+        fk = 700.0 if b0 < 1.2 else heavy_fk
+        top.bond_lib.append((fk, round(b0, 4)))
+        top.bonds.append((offset + i, offset + j, len(top.bond_lib)))
+    for j in range(n):
+        for a in range(len(nb[j])):
+            for b in range(a + 1, len(nb[j])):
+                i, k = nb[j][a], nb[j][b]
+                top.angle_lib.append((70.0, round(_angle(X[i], X[j], X[k]), 3)))
+                top.angles.append((offset + i, offset + j, offset + k, len(top.angle_lib)))
+    for j, k in bonds:
+        for i in nb[j]:
+            if i == k:
+                continue
+            for l in nb[k]:
+                if l == j or l == i:
+                    continue
+                nmul = int(rng.integers(1, 4))
+                top.tor_lib.append((round(float(rng.uniform(0.2, 1.5)), 3), float(nmul),
+                                    float(rng.choice([0.0, 180.0])), 1))
+                top.tors.append((offset + i, offset + j, offset + k, offset + l, len(top.tor_lib)))
+    for j in range(n):
+        if len(nb[j]) == 3:
+            i, k, l = nb[j]
+            top.imp_lib.append((1.1, 180.0))
+            top.imps.append((offset + i, offset + j, offset + k, offset + l, len(top.imp_lib)))
+
+
+def _tree_types(kinds) -> tuple[list[AtomType], list[int]]:
+    types = [AtomType("H", M_H, SIG_H, EPS_H)] + [AtomType("T%d" % (k + 1), m, s, e)
+                                                  for k, (s, e, m) in enumerate(TYPE_TABLE)]
+    return types, [0 if k < 0 else k + 1 for k in kinds]
+
+
+def _net_zero_charges(rng, n: int, sd: float = 0.3, total: float = 0.0) -> list[float]:
+    q = rng.normal(0.0, sd, size=n)
+    q = q - q.mean() + total / n
+    q = np.round(q, 4)
+    q[-1] = round(total - float(q[:-1].sum()), 4)
+    return [float(v) for v in q]
+
+
+# -------------------------------------------------------------- systems
+
+@dataclass
+class Generated:
+    inp: str
+    top: str
+    fep: str | None
+    natom: int
+    nwat: int
+
+
+def write_inp(path: str, top: str, fep: str | None, *, steps: int, stepsize: float, temp: float = 298.0,
+              seed: int = 1, lambdas=None, shake_hydrogens: bool = False, bath: float = 100.0,
+              output: int = 100, energy: int = 10, non_bond: int = 25, shell_radius: float | None = None,
+              shell_force: float = 10.0, q_cutoff: float = 99.0, energy_file: str | None = None) -> None:
+    name = os.path.splitext(os.path.basename(path))[0]
+    L = ["[MD]", "steps %d" % steps, "stepsize %g" % stepsize, "temperature %g" % temp,
+         "bath_coupling %g" % bath, "random_seed %d" % seed, "initial_temperature %g" % temp,
+         "shake_solvent on", "shake_solute off", "shake_hydrogens %s" % ("on" if shake_hydrogens else "off"),
+         "lrf on", "", "[cut-offs]", "solute_solute 10", "solvent_solvent 10", "solute_solvent 10",
+         "q_atom %g" % q_cutoff, "lrf 99", "", "[sphere]"]
+    if shell_radius is not None:
+        L.append("shell_radius %g" % shell_radius)
+    L += ["shell_force %g" % shell_force, "", "[solvent]", "radial_force 60.0", "polarization on",
+          "polarization_force 20.0", "", "[intervals]", "non_bond %d" % non_bond, "output %d" % output,
+          "energy %d" % energy, "trajectory 0", "", "[files]", "topology %s" % os.path.basename(top),
+          "final %s.re" % name]
+    if energy > 0:
+        L.append("energy %s" % (energy_file or name + ".en"))
+    if fep:
+        L.append("fep %s" % os.path.basename(fep))
+        L += ["", "[lambdas]", " ".join("%g" % x for x in lambdas)]
+    with open(path, "w") as f:
+        f.write("\n".join(L) + "\n")
+
+
+def water_sphere(outdir: str, radius: float = 15.0, seed: int = 1234, steps: int = 1000, name: str = "c0",
+                 stepsize: float = 1.0) -> Generated:
+    """Config 0: TIP3P sphere, 1 fs, energies every 10 steps."""
+    os.makedirs(outdir, exist_ok=True)
+    rng = np.random.default_rng(seed)
+    top = Topology(title="water_sphere_%g" % radius, rexcl_o=radius, rwat=radius)
+    _add_waters(top, lattice_waters(radius, rng))
+    top.excl = [False] * len(top.x)
+    tp = os.path.join(outdir, name + ".top")
+    top.write(tp)
+    inp = os.path.join(outdir, name + ".inp")
+    write_inp(inp, tp, None, steps=steps, stepsize=stepsize, seed=seed % 100000 + 1, energy=10)
+    return Generated(inp, tp, None, len(top.x), (len(top.x)) // 3)
+
+
+def _fep_file(path: str, types: list[AtomType], iac: list[int], q: list[float], qatoms: list[int],
+              alpha: float = 20.0) -> None:
+    L = ["[FEP]", "states 2", "", "[atoms]"]
+    L += ["%d %d" % (k + 1, a + 1) for k, a in enumerate(qatoms)]
+    L += ["", "[change_charges]"]
+    L += ["%d %8.4f %8.4f" % (k + 1, q[a], 0.0) for k, a in enumerate(qatoms)]
+    L += ["", "[atom_types]"]
+    names = []
+    for k, a in enumerate(qatoms):
+        t = types[iac[a]]
+        for st, scale in ((1, 1.0), (2, 0.5)):
+            nm = "Q%d_%d" % (k + 1, st)
+            aa, bb = lj_sqrt(t.sigma, t.eps * scale)
+            L.append("%-8s %9.2f %8.2f %6.2f %6.2f %9.2f %8.2f %8.4f"
+                     % (nm, aa, bb, 0.0, 0.0, aa / math.sqrt(2), bb / math.sqrt(2), t.mass))
+        names.append(("Q%d_1" % (k + 1), "Q%d_2" % (k + 1)))
+    L += ["", "[change_atoms]"]
+    L += ["%d %s %s" % (k + 1, a, b) for k, (a, b) in enumerate(names)]
+    L += ["", "[softcore]"]
+    L += ["%d %g %g" % (k + 1, 0.0, alpha) for k in range(len(qatoms))]
+    with open(path, "w") as f:
+        f.write("\n".join(L) + "\n")
+
+
+def fep_solute(outdir: str, radius: float = 20.0, seed: int = 1234, steps: int = 5000, name: str = "c1",
+               lambdas=(0.5, 0.5), run_seed: int = 1) -> Generated:
+    """Config 1: 56-atom solute with 8 two-state Q-atoms in a TIP3P sphere,
+    2 fs with SHAKE on X-H bonds and water."""
+    os.makedirs(outdir, exist_ok=True)
+    rng = np.random.default_rng(seed)
+    X, kinds, bonds = random_tree_solute(rng)
+    types, iac = _tree_types(kinds)
+    n = len(X)
+    top = Topology(title="fep_solute", rexcl_o=radius, rwat=radius, types=types)
+    top.x = [tuple(float(c) for c in p) for p in X]
+    top.iac = iac
+    top.crg = _net_zero_charges(rng, n)
+    _solute_terms(top, X, bonds, rng)
+    top.nat_solute = n
+    top.nbonds_solute, top.nangles_solute = len(top.bonds), len(top.angles)
+    top.ntors_solute, top.nimps_solute = len(top.tors), len(top.imps)
+    nb = [[] for _ in range(n)]
+    for i, j in bonds:
+        nb[i].append(j)
+        nb[j].append(i)
+    for i in range(n):
+        if kinds[i] >= 0:
+            top.cgps.append((i, [i] + sorted(j for j in nb[i] if kinds[j] < 0)))
+    top.ncgp_solute = len(top.cgps)
+    top.mol_starts = [0]
+    top.res_starts, top.res_names = [0], ["LIG"]
+    _finish_solute_lists(top, bonds, n)
+    waters = lattice_waters(radius, rng, avoid=X)
+    _add_waters(top, waters)
+    top.excl = [False] * len(top.x)
+    tp = os.path.join(outdir, name + ".top")
+    top.write(tp)
+    fp = os.path.join(outdir, name + ".fep")
+    heavy = [i for i in range(n) if kinds[i] >= 0]
+    _fep_file(fp, types, iac, top.crg, heavy[:8])
+    inp = os.path.join(outdir, name + ".inp")
+    write_inp(inp, tp, fp, steps=steps, stepsize=2.0, seed=run_seed, lambdas=lambdas, shake_hydrogens=True)
+    return Generated(inp, tp, fp, len(top.x), len(waters))
+
+
+def polymer_sphere(outdir: str, radius: float = 25.0, seed: int = 1234, steps: int = 5000, name: str = "c2",
+                   n_polymer: int = 3000, restrain_beyond: float = 23.0, lambdas=(0.5, 0.5)) -> Generated:
+    """Config 2: 3000-atom polymer walk around the config-1 solute (ligand) in
+    a 25 A sphere; atoms beyond 23 A are excluded and restrained; waters fill
+    the remaining volume."""
+    os.makedirs(outdir, exist_ok=True)
+    rng = np.random.default_rng(seed)
+    Xl, kinds, lbonds = random_tree_solute(rng)
+    from scipy.spatial import cKDTree
+    # self-avoiding chains, restarted where a chain gets stuck
+    pts = [p for p in Xl]
+    chains = []
+    cell = 2.5
+
+    grid: dict = {}
+
+    def gkey(p):
+        return tuple((p // cell).astype(int))
+
+    def add(p):
+        grid.setdefault(gkey(p), []).append(len(pts) - 1)
+
+    for k in range(len(pts)):
+        grid.setdefault(gkey(pts[k]), []).append(k)
+
+    def free(p, skip):
+        if np.linalg.norm(p) > radius - 0.5:
+            return False
+        kx, ky, kz = gkey(p)
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    for q in grid.get((kx + dx, ky + dy, kz + dz), ()):
+                        if q != skip and np.linalg.norm(pts[q] - p) < 2.5:
+                            return False
+        return True
+
+    total = 0
+    while total < n_polymer:
+        for _ in range(5000):
+            start = rng.uniform(-radius, radius, size=3)
+            if np.linalg.norm(start) < radius - 1.0 and free(start, -1):
+                break
+        chain = [len(pts)]
+        pts.append(start)
+        add(start)
+        total += 1
+        while total < n_polymer:
+            ok = False
+            for _ in range(60):
+                u = rng.normal(size=3)
+                u /= np.linalg.norm(u)
+                c = pts[chain[-1]] + 1.5 * u
+                if len(chain) > 1 and _angle(pts[chain[-2]], pts[chain[-1]], c) < 100:
+                    continue
+                if free(c, chain[-1]):
+                    ok = True
+                    break
+            if not ok:
+                break
+            pts.append(c)
+            add(c)
+            chain.append(len(pts) - 1)
+            total += 1
+        chains.append(chain)
+    n_lig = len(Xl)
+    X = np.array(pts)
+    n = len(X)
+    types, _ = _tree_types(kinds)
+    iac = [0 if k < 0 else k + 1 for k in kinds] + [1 + int(rng.integers(len(TYPE_TABLE))) for _ in range(n - n_lig)]
+    top = Topology(title="polymer_sphere", rexcl_o=restrain_beyond, rwat=radius, types=types)
+    top.x = [tuple(float(c) for c in p) for p in X]
+    top.iac = iac
+    crg = _net_zero_charges(rng, n_lig)
+    pbonds = [(a, b) for ch in chains for a, b in zip(ch[:-1], ch[1:])]
+    # residue-like charge groups of 10-15 consecutive chain atoms, net charge -1/0/+1
+    groups = []
+    for ch in chains:
+        k = 0
+        while k < len(ch):
+            m = int(rng.integers(10, 16))
+            groups.append(ch[k:k + m])
+            k += m
+    pcrg = np.zeros(n)
+    for g in groups:
+        net = float(rng.choice([-1.0, 0.0, 1.0]))
+        pcrg[g] = _net_zero_charges(rng, len(g), sd=0.3, total=net)
+    top.crg = crg + [float(v) for v in pcrg[n_lig:]]
+    _solute_terms(top, Xl, lbonds, rng)
+    # polymer terms (harmonic bonds/angles, torsions along the chains)
+    nbp = [[] for _ in range(n)]
+    for i, j in pbonds:
+        nbp[i].append(j)
+        nbp[j].append(i)
+    for i, j in pbonds:
+        top.bond_lib.append((500.0, round(float(np.linalg.norm(X[i] - X[j])), 4)))
+        top.bonds.append((i, j, len(top.bond_lib)))
+    for ch in chains:
+        for a, b, c in zip(ch[:-2], ch[1:-1], ch[2:]):
+            top.angle_lib.append((60.0, round(_angle(X[a], X[b], X[c]), 3)))
+            top.angles.append((a, b, c, len(top.angle_lib)))
+        for a, b, c, d in zip(ch[:-3], ch[1:-2], ch[2:-1], ch[3:]):
+            top.tor_lib.append((round(float(rng.uniform(0.2, 1.5)), 3), float(rng.integers(1, 4)),
+                                float(rng.choice([0.0, 180.0])), 1))
+            top.tors.append((a, b, c, d, len(top.tor_lib)))
+    top.nat_solute = n
+    top.nbonds_solute, top.nangles_solute = len(top.bonds), len(top.angles)
+    top.ntors_solute, top.nimps_solute = len(top.tors), len(top.imps)
+    nbl = [[] for _ in range(n_lig)]
+    for i, j in lbonds:
+        nbl[i].append(j)
+        nbl[j].append(i)
+    for i in range(n_lig):
+        if kinds[i] >= 0:
+            top.cgps.append((i, [i] + sorted(j for j in nbl[i] if kinds[j] < 0)))
+    for g in groups:
+        top.cgps.append((g[len(g) // 2], sorted(g)))
+    top.ncgp_solute = len(top.cgps)
+    top.mol_starts = [0] + [ch[0] for ch in chains]
+    top.res_starts = [0] + [g[0] for g in groups]
+    top.res_names = ["LIG"] + ["POL"] * len(groups)
+    _finish_solute_lists(top, lbonds + pbonds, n)
+    top.excl = [bool(np.linalg.norm(X[i]) > restrain_beyond) for i in range(n)]
+    waters = lattice_waters(radius, rng, avoid=X, r_o=2.6)
+    _add_waters(top, waters, excl_radius=restrain_beyond)
+    tp = os.path.join(outdir, name + ".top")
+    top.write(tp)
+    fp = os.path.join(outdir, name + ".fep")
+    heavy = [i for i in range(n_lig) if kinds[i] >= 0]
+    _fep_file(fp, types, iac, top.crg, heavy[:8])
+    inp = os.path.join(outdir, name + ".inp")
+    write_inp(inp, tp, fp, steps=steps, stepsize=2.0, seed=1, lambdas=lambdas, shake_hydrogens=True,
+              q_cutoff=99.0, shell_radius=restrain_beyond - 0.01)
+    return Generated(inp, tp, fp, len(top.x), len(waters))
+
+
+def window_lambdas(n_windows: int) -> list[tuple[float, float]]:
+    """Uniform lambda windows (lambda_1, 1 - lambda_1) from 1 to 0."""
+    return [(1.0 - k / (n_windows - 1), k / (n_windows - 1)) for k in range(n_windows)]

@@ -106,3 +106,45 @@ def test_batch_of_systems_is_independent(golden, oracle):
         _, Eg, EQg = b.history(s, 0)
         assert_energies(Eg[0], EQg[0], Eo[0], EQo[0])
     assert np.max(np.abs(b.coords(0) - b.coords(2))) < 1e-9
+
+
+@pytest.fixture(scope="module")
+def synthetic(tmp_path_factory):
+    from q_b200 import synth
+    root = tmp_path_factory.mktemp("synth")
+    return {"c0": synth.water_sphere(str(root / "c0"), radius=15.0, seed=1234),
+            "c1": synth.fep_solute(str(root / "c1"), seed=1234)}
+
+
+@pytest.mark.parametrize("case", ["c0", "c1"])
+def test_synthetic_single_point(synthetic, oracle, case):
+    """Benchmark-shaped systems: water sphere (LRF, restraints, watpol) and the
+    8-Q-atom two-state soft-core FEP solute; energies and gradient."""
+    sys_ = System.open(synthetic[case].inp)
+    b = Batch([sys_], precision=FP64)
+    b.final_energy()
+    o = oracle.create(sys_)
+    o.final_energy()
+    Eg, EQg = b.energy_vectors(0)
+    Eo, EQo = o.energy_vectors()
+    assert_energies(Eg, EQg, Eo, EQo)
+    assert grad_err(b.gradient(0), o.gradient()) < G_TOL
+
+
+def test_synthetic_windows_trajectory(synthetic, oracle):
+    """Three lambda windows of the FEP system in one batch, 50 steps (two list
+    rebuilds), each against its own oracle run."""
+    inp = synthetic["c1"].inp
+    lams = [(1.0, 0.0), (0.5, 0.5), (0.0, 1.0)]
+    systems = [System.open(inp, lambdas=l, seed=7) for l in lams]
+    b = Batch(systems, precision=FP64)
+    b.run(50)
+    for k, s in enumerate(systems):
+        o = oracle.create(s)
+        o.run(50)
+        sg, Eg, EQg = b.history(k, 0)
+        so, Eo, EQo = o.history(0)
+        assert list(sg) == list(so)
+        for r in range(len(sg)):
+            assert_energies(Eg[r], EQg[r], Eo[r], EQo[r])
+        assert np.max(np.abs(b.coords(k) - o.coords())) < 1e-6

@@ -1,0 +1,148 @@
+"""Drop-in replacement of the `qdyn` executable for one input file.
+
+    python -m q_b200.qdyn md.inp > md.log
+
+Reads the same .inp/.top/.fep/.re as qdyn (src/q6/qdyn.f90:18-134), runs the
+MD steps on the GPU, and writes what the reference's scripts consume: the
+energy file (.en, put_ene records, nrgy.f90:94-119), the final restart (.re,
+write_xfin, md.f90:15452-15470) and an energy-summary log laid out as
+write_out (md.f90:15292-15440), ending with "terminated normally".
+"""
+from __future__ import annotations
+
+import os
+import sys
+import time
+
+import numpy as np
+
+
+def _fmt_label(label: str, values) -> str:
+    # format (A, T17, 6F10.2)
+    return "%-16s%s" % (label, "".join("%10.2f" % v for v in values))
+
+
+def write_out(E, EQ, step: int | None, nstates: int, nwat: int, use_lrf: bool, nqat: int, nat_solute: int) -> str:
+    """One energy summary in write_out's layout."""
+    e = dict(zip(__import__("q_b200").E_NAMES, E))
+    L = []
+    if step is None:
+        L.append("=========================== FINAL %15s =============================" % "Energy summary")
+    else:
+        L.append("======================= %15s at step %6d ========================" % ("Energy summary", step))
+    L.append(" " * 16 + "".join("%10s" % h for h in ("el", "vdW", "bond", "angle", "torsion", "improper")))
+    L.append(_fmt_label("solute", [e["pp_el"], e["pp_vdw"], e["p_bond"], e["p_angle"], e["p_torsion"], e["p_improper"]]))
+    if nwat > 0:
+        L.append(_fmt_label("solvent", [e["ww_el"], e["ww_vdw"], e["w_bond"], e["w_angle"], e["w_torsion"], e["w_improper"]]))
+    L.append(_fmt_label("solute-solvent", [e["pw_el"], e["pw_vdw"]]))
+    if use_lrf:
+        L.append(_fmt_label("LRF", [e["LRF"]]))
+    if nqat > 0:
+        L.append(_fmt_label("Q-atom", [e["qx_el"], e["qx_vdw"], e["q_bond"], e["q_angle"], e["q_torsion"], e["q_improper"]]))
+    L.append("")
+    L.append(" " * 16 + "".join("%10s" % h for h in ("total", "fix", "slvnt_rad", "slvnt_pol", "shell", "solute")))
+    L.append(_fmt_label("restraints", [e["rst_total"], e["rst_fix"], e["rst_solvent_radial"], e["rst_water_pol"],
+                                       e["rst_shell"], e["rst_protein"]]))
+    L.append("")
+    L.append(" " * 16 + "".join("%10s" % h for h in ("total", "potential", "kinetic")))
+    L.append(_fmt_label("SUM", [e["potential"] + e["kinetic"], e["potential"], e["kinetic"]]))
+    if nstates > 0:
+        if step is None:
+            L.append("=========================== FINAL %15s =============================" % "Q-atom energies")
+        else:
+            L.append("======================= %15s at step %6d ========================" % ("Q-atom energies", step))
+        L.append("type   st lambda" + "".join("%10s" % h for h in ("el", "vdW", "bond", "angle", "torsion", "improper")))
+
+        def row(name, st, a, b):
+            return "%-7s%2d%7.4f%10.2f%10.2f" % (name, st + 1, EQ[st][0], a, b)
+
+        for st in range(nstates):
+            L.append(row("Q-Q", st, EQ[st][8], EQ[st][9]))
+        L.append("")
+        if nat_solute > nqat:
+            for st in range(nstates):
+                L.append(row("Q-prot", st, EQ[st][10], EQ[st][11]))
+            L.append("")
+        if nwat > 0:
+            for st in range(nstates):
+                L.append(row("Q-wat", st, EQ[st][12], EQ[st][13]))
+            L.append("")
+        for st in range(nstates):
+            L.append(row("Q-surr.", st, EQ[st][10] + EQ[st][12], EQ[st][11] + EQ[st][13]))
+        L.append("")
+        for st in range(nstates):
+            L.append("%-7s%2d%7.4f" % ("Q-any", st + 1, EQ[st][0]) + "".join("%10.2f" % EQ[st][k] for k in (6, 7, 2, 3, 4, 5)))
+        L.append("")
+        L.append("type   st lambda" + "%10s%10s" % ("total", "restraint"))
+        for st in range(nstates):
+            L.append(row("Q-SUM", st, EQ[st][1], EQ[st][14]))
+    L.append("=" * 79)
+    return "\n".join(L)
+
+
+def run(inp: str, out=sys.stdout, chunk: int = 1000) -> int:
+    from q_b200 import Batch, System, append_energy, write_restart
+    from q_b200._lib import QBError
+
+    t0 = time.time()
+    try:
+        sys_ = System.open(inp)
+        v = sys_.view
+        batch = Batch([sys_])
+    except QBError as e:
+        print("!" * 79, file=out)
+        print("ABNORMAL TERMINATION of qdyn: %s" % e, file=out)
+        return 255
+    ns = v.nstates
+    d = os.path.dirname(os.path.abspath(inp))
+    ene = None
+    for line in open(inp):
+        t = line.split()
+        if len(t) >= 2 and t[0].lower() == "energy" and v.iene_cycle > 0:
+            ene = os.path.join(d, t[1])
+        if len(t) >= 2 and t[0].lower() == "final":
+            final = os.path.join(d, t[1])
+    if ene and os.path.exists(ene):
+        os.remove(ene)
+    T = batch.temperature(0)
+    print("Initial temperatures are : Ttot =%10.2f Tfree =%10.2f" % (T[0], T[1]), file=out)
+    done = 0
+    try:
+        while done < v.nsteps:
+            n = min(chunk, v.nsteps - done)
+            batch.run(n)
+            steps, E, EQ = batch.history(0, 0)
+            for k in range(len(steps)):
+                print(write_out(E[k], EQ[k], int(steps[k]), ns, v.nwat, bool(v.use_LRF), v.nqat, v.nat_solute), file=out)
+            if ene:
+                _, _, EQe = batch.history(0, 1)
+                for k in range(EQe.shape[0]):
+                    append_energy(ene, EQe[k])
+            batch.clear_history()
+            done += n
+        batch.final_energy()
+    except QBError as e:
+        print("!" * 79, file=out)
+        print("ABNORMAL TERMINATION of qdyn", file=out)
+        print("Terminating due to %s" % e, file=out)
+        return 255
+    E, EQ = batch.energy_vectors(0)
+    print("", file=out)
+    print(write_out(E, EQ, None, ns, v.nwat, bool(v.use_LRF), v.nqat, v.nat_solute), file=out)
+    tc = batch.theta_corr(0, v.nwpolr_shell) if v.nwpolr_shell > 0 else None
+    write_restart(final, batch.coords(0), batch.velocities(0), tc)
+    print("Total time of main loop: %24.1f(s)" % (time.time() - t0), file=out)
+    print(" qdyn version 6.0.1 terminated normally.", file=out)
+    return 0
+
+
+def main(argv=None) -> int:
+    argv = sys.argv[1:] if argv is None else argv
+    if not argv:
+        print("usage: python -m q_b200.qdyn file.inp", file=sys.stderr)
+        return 2
+    return run(argv[-1])
+
+
+if __name__ == "__main__":
+    sys.exit(main())

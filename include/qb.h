@@ -155,6 +155,43 @@ int qb_batch_workload(qb_batch *b, double *out, int n);
 
 void qb_batch_destroy(qb_batch *b);
 
+/* ------------------------------------------------------ allocation-free path */
+
+#define QB_STATIC_WW_MAX_WATERS 4096
+#define QB_STATIC_WW_MAX_NEIGHBOURS 192
+#define QB_STATIC_WW_SCRATCH_BYTES \
+  ((size_t)(QB_STATIC_WW_MAX_WATERS * QB_STATIC_WW_MAX_NEIGHBOURS + QB_STATIC_WW_MAX_WATERS) * 4)
+
+/* SPC/TIP3P water-water electrostatic and Lennard-Jones energy and gradient of
+ * one water sphere, computed on buffers the caller owns, with no device memory
+ * allocated by the call.  This entry point has no counterpart in the
+ * reference.  It exists for hosts that cannot let a library call cudaMalloc:
+ * callers that hand out device memory only from their own pool (a framework's
+ * caching allocator, a pre-sized arena in a long-running service) or that
+ * forbid allocation on the calling thread.
+ *
+ * x:      device, 9*nwat doubles, waters as O,H,H with x,y,z each
+ * excl:   device, nwat flags (1 = water outside the sphere), or NULL
+ * grad:   device, 9*nwat doubles, overwritten with dU/dx
+ * energy: device, 2 doubles, overwritten with (electrostatic, van der Waals)
+ * status: device, 1 int, overwritten: 0, or QB_ERR_LIST_OVERFLOW when a water
+ *         has more than QB_STATIC_WW_MAX_NEIGHBOURS neighbours
+ * stream: cudaStream_t (NULL = default stream); the work is queued on it and
+ *         the call returns without waiting.
+ *
+ * Its scratch (the neighbour list) is a fixed array in the library's device
+ * memory: every GPU that loads the library holds QB_STATIC_WW_SCRATCH_BYTES
+ * (about 3 MB) until the process exits.  Systems above
+ * QB_STATIC_WW_MAX_WATERS waters are rejected with QB_ERR_ARG.  All calls on a
+ * device share that array and it keeps the last call's contents (the call
+ * rewrites everything it reads), so calls that overlap on the GPU -- on two
+ * streams, or from two threads -- race and must be serialised by the caller.
+ * The first call on each device looks up the array's device address with that
+ * device current; make that first call before any stream capture. */
+int qb_ww_energy_static(const double *x, int nwat, float crg_ow, float crg_hw, double A_OO, double B_OO,
+                        double cutoff, const unsigned char *excl, double *grad, double *energy, int *status,
+                        void *stream);
+
 /* Measured FMA throughput of the CUDA cores of `device` (TFLOP/s, FMA = 2
  * FLOP) in FP64 (precision QB_FP64) or FP32 (QB_MIXED): the denominator of the
  * pair kernels' roofline. */

@@ -134,6 +134,9 @@ def _load():
         "qb_write_re": (C.c_int, [C.c_char_p, C.c_int, dp, dp, C.c_int, fp]),
         "qb_append_en": (C.c_int, [C.c_char_p, C.c_int, dp]),
         "qb_maxwell": (C.c_int, [C.c_int, C.c_double, C.c_int, dp, dp]),
+        "qb_ww_energy_static": (C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_double, C.c_double,
+                                          C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -47,7 +47,7 @@ FLOP_LJC = 37        # per LJ+Coulomb atom pair
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="qb", choices=["qb", "reference"])
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
@@ -83,7 +83,7 @@ def workload_files(root: str, rank: int, args):
 
 class ClockSampler:
     """nvidia-smi clock/throttle samples during the timed region."""
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -95,7 +95,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -105,7 +105,10 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self, which: str):
+        setattr(self, which, time.time())
 
     def __exit__(self, *a):
         if self.proc:
@@ -116,18 +119,22 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        """Samples that arrived while the timed steps ran (t0..t1)."""
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in self.lines:
+        t0, t1 = getattr(self, "t0", 0.0), getattr(self, "t1", 1e300)
+        for ts, l in self.lines:
+            if not (t0 <= ts <= t1 + 0.15):
+                continue
             f = [x.strip() for x in l.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
+                sm.append(float(f[2]))
+                smax = float(f[3])
             except ValueError:
                 continue
-            for n, v in zip(names, f[5:9]):
+            for n, v in zip(names, f[6:10]):
                 if v.lower().startswith("active"):
                     reasons.add(n)
         if not sm:
@@ -254,7 +261,10 @@ def main():
     barrier()
     torch.cuda.synchronize(local) if torch.cuda.is_available() else None
     with ClockSampler(local) as clk:
+        batch.run(max(args.warmup, 3) + 20)      # the sampler starts while the GPU is busy
+        clk.mark("t0")
         ms, launches = batch.run_timed(args.steps)
+        clk.mark("t1")
     barrier()
     elapsed = ms / 1e3
     if dist:
@@ -279,6 +289,12 @@ def main():
     ww_ms = ww[0] / max(ww[1], 1)
     ww_flop = FLOP_WW * ww_pairs
     peak = peak_tflops(FP64 if prec == FP64 else MIXED, local)
+    traffic = None
+    try:
+        tj = json.load(open(os.path.join(REPO, "profiles", "traffic.json")))
+        traffic = tj.get(args.precision, {}).get("bytes_per_launch")
+    except (OSError, ValueError):
+        pass
     achieved = ww_flop / (ww_ms * 1e-3) / 1e12 if ww_ms > 0 else 0.0
 
     # end to end through the C ABI with host buffers
@@ -324,7 +340,8 @@ def main():
         "roofline": {"kernel": "nb_ww (water-water SPC pair kernel)", "bound": "fp64" if prec == FP64 else "fp32",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                      "peak_source": "measured FMA loop (qb_peak_flops) on this GPU",
-                     "flop_per_launch": ww_flop, "launch_ms": ww_ms, "traffic": None,
+                     "flop_per_launch": ww_flop, "launch_ms": ww_ms, "traffic": traffic,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/traffic.json",
                      "share_of_step": ww[0] / tot if tot else None,
                      "top_kernel": top[0], "top_kernel_share": top[1][0] / tot if tot else None},
         "kernels_ms_per_step": {k: v[0] / args.steps for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])[:8]},

@@ -1,0 +1,175 @@
+"""Host-side logic of libqb, no GPU needed: the C ABI loads and exports what
+its headers declare, the Q file readers and writers, error paths, the
+synthetic generator, the qdyn log layout and the multi-rank helpers."""
+import os
+import struct
+
+import numpy as np
+import pytest
+
+from q_b200 import QBError, System, append_energy, synth, write_restart
+from q_b200._lib import exported_symbols, lib
+
+
+def test_library_exports_every_declared_symbol():
+    names = exported_symbols()
+    assert len(names) >= 30
+    for n in names:
+        assert hasattr(lib, n), n
+    import ctypes as C
+    buf = C.create_string_buffer(64)
+    assert lib.qb_version(buf, 64) == 0 and b"sm_100a" in buf.value
+
+
+def test_test1_topology_and_setup(golden):
+    s = System.open(str(golden / "test1" / "eq1.inp"))
+    v = s.view
+    assert (v.natom, v.nat_solute, v.nwat) == (3397, 46, 1117)
+    assert (v.ncgp, v.ncgp_solute, v.natyps) == (1150, 33, 93)
+    assert (v.nqat, v.nstates) == (46, 1)
+    assert v.ff_type == 2 and v.iuse_switch_atom == 1
+    # [cut_offs] is not the section name qdyn reads: defaults apply
+    assert (v.Rcpp, v.Rcww, v.Rcpw, v.Rcq, v.RcLRF) == (10.0, 10.0, 10.0, 99.0, 99.0)
+    assert v.use_LRF == 1 and v.NBcycle == 25 and v.iout_cycle == 50
+    assert abs(v.dt - 0.020462 * 0.1) < 1e-15
+    # solvent SHAKE: 3 constraints per water, the water angles removed
+    assert v.shake_constraints == 3 * 1117 and v.nangles == v.nangles_solute
+    assert v.Ndegf == 3 * 3397 - 3 * 1117
+    # sequence restraint "1 46 0.5 0 1": to the geometric centre
+    assert v.nrstr_seq == 1 and v.rseq_to_center[0] == 1 and v.rseq_fk[0] == 0.5
+    # rexcl_i = 16 A (absolute), shell force 20
+    assert v.rexcl_i == 16.0 and v.fk_pshell == 20.0
+    # charges are stored scaled by sqrt(332) in single precision
+    q = s.array("crg", v.natom)
+    assert q.dtype == np.float32
+    assert abs(q[v.nat_solute] - np.float32(-0.834 * np.sqrt(332.0))) < 1e-5
+    assert v.nwpolr_shell == 3
+
+
+def test_benzene_topology(golden):
+    v = System.open(str(golden / "benzene" / "eq1.inp")).view
+    assert (v.natom, v.nat_solute, v.nwat, v.nstates) == (12, 12, 0, 0)
+    assert v.nbonds == 12 and v.nangles == 18 and v.nimps == 6
+
+
+def test_restart_round_trip(tmp_path, golden):
+    s = System.open(str(golden / "benzene" / "eq1.inp"))
+    x = s.array("x0") + 0.01
+    v = np.arange(x.size, dtype=np.float64) * 1e-3
+    re = tmp_path / "in.re"
+    write_restart(str(re), x, v)
+    # gfortran records: (int32 nat3, 36 doubles) twice, each with 4-byte markers
+    raw = re.read_bytes()
+    assert len(raw) == 2 * (4 + 4 + 8 * 36 + 4)
+    assert struct.unpack("<ii", raw[:8]) == (4 + 8 * 36, 36)
+    inp = (golden / "benzene" / "eq1.inp").read_text()
+    inp = inp.replace("initial_temperature       1", "").replace("final ", "restart in.re\nfinal ")
+    inp = inp.replace("topology                  benzene-vacuum.top",
+                      "topology                  %s" % (golden / "benzene" / "benzene-vacuum.top"))
+    (tmp_path / "re.inp").write_text(inp)
+    s2 = System.open(str(tmp_path / "re.inp"))
+    assert np.array_equal(s2.array("x0"), x)
+    assert np.array_equal(s2.array("v0"), v)
+
+
+def test_energy_file_records(tmp_path):
+    path = tmp_path / "x.en"
+    EQ = np.arange(2 * 15, dtype=np.float64).reshape(2, 15)
+    append_energy(str(path), EQ)
+    append_energy(str(path), EQ + 1)
+    raw = path.read_bytes()
+    frame = 2 * (4 + 4 + 120 + 4) + 8
+    assert len(raw) == 2 * frame
+    n, st = struct.unpack("<ii", raw[:8])
+    assert (n, st) == (124, 1)
+    vals = struct.unpack("<15d", raw[8:128])
+    assert vals == tuple(EQ[0])
+    # the off-diagonal record of an empty list is a zero-length record
+    assert struct.unpack("<ii", raw[frame - 8:frame]) == (0, 0)
+
+
+def test_error_paths(tmp_path, golden):
+    with pytest.raises(QBError) as e:
+        System.open(str(tmp_path / "missing.inp"))
+    assert e.value.code == 2
+    bad = tmp_path / "pbc.inp"
+    bad.write_text("[PBC]\nrigid_box_center off\n[MD]\nsteps 1\n")
+    with pytest.raises(QBError) as e:
+        System.open(str(bad))
+    assert e.value.code == 4
+    txt = (golden / "benzene" / "eq1.inp").read_text().replace("stepsize                  1", "stepsize x")
+    (tmp_path / "b.inp").write_text(txt.replace("benzene-vacuum.top", str(golden / "benzene" / "benzene-vacuum.top")))
+    with pytest.raises(QBError) as e:
+        System.open(str(tmp_path / "b.inp"))
+    assert e.value.code == 3
+    # truncated restart file
+    (tmp_path / "t.re").write_bytes(b"\x00" * 10)
+    txt = (golden / "benzene" / "eq1.inp").read_text()
+    txt = txt.replace("initial_temperature       1", "").replace("final ", "restart t.re\nfinal ")
+    txt = txt.replace("benzene-vacuum.top", str(golden / "benzene" / "benzene-vacuum.top"))
+    (tmp_path / "r.inp").write_text(txt)
+    with pytest.raises(QBError) as e:
+        System.open(str(tmp_path / "r.inp"))
+    assert e.value.code == 3
+
+
+def test_synthetic_systems_parse(tmp_path):
+    g0 = synth.water_sphere(str(tmp_path / "c0"), radius=15.0, seed=1234)
+    v0 = System.open(g0.inp).view
+    assert v0.nat_solute == 0 and 440 <= v0.nwat <= 500
+    g1 = synth.fep_solute(str(tmp_path / "c1"), seed=1234)
+    s1 = System.open(g1.inp)
+    v1 = s1.view
+    assert v1.nat_solute == 56 and v1.nqat == 8 and v1.nstates == 2
+    assert 1000 <= v1.nwat <= 1130
+    assert v1.qvdw_flag == 1
+    q = s1.array("crg", v1.natom)[:56] / np.sqrt(332.0)
+    assert abs(q.sum()) < 1e-3
+    qc = s1.array("qcrg", 16).reshape(8, 2)
+    assert np.all(qc[:, 1] == 0.0)
+    lam = getattr(System.open(g1.inp, lambdas=(0.25, 0.75), seed=5).view, "lambda")
+    assert (lam[0], lam[1]) == (0.25, 0.75)
+
+
+def test_qdyn_log_layout():
+    from q_b200.qdyn import write_out
+    E = np.zeros(29)
+    EQ = np.zeros((1, 15))
+    EQ[0, 0] = 1.0
+    EQ[0, 12], EQ[0, 13] = 3.1214, 139.4273
+    text = write_out(E, EQ, 0, 1, 1117, True, 46, 46)
+    assert "Energy summary at step      0" in text
+    line = [l for l in text.split("\n") if l.startswith("Q-surr.")][0]
+    assert line == "Q-surr. 1 1.0000      3.12    139.43"
+
+
+def _gloo_worker(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    from q_b200.dist import max_over_ranks, shard, sum_over_ranks
+    mine = shard(100, rank, world)
+    t = max_over_ranks(1.0 + rank)
+    n = sum_over_ranks(len(mine))
+    out.put((rank, mine[:3], t, n))
+    dist.destroy_process_group()
+
+
+def test_multi_rank_helpers_gloo():
+    import socket
+
+    import torch.multiprocessing as tmp
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = tmp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_gloo_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+    assert res[0] == (0, [0, 2, 4], 2.0, 100.0)
+    assert res[1] == (1, [1, 3, 5], 2.0, 100.0)

@@ -127,7 +127,8 @@ def test_synthetic_systems_parse(tmp_path):
     assert abs(q.sum()) < 1e-3
     qc = s1.array("qcrg", 16).reshape(8, 2)
     assert np.all(qc[:, 1] == 0.0)
-    lam = getattr(System.open(g1.inp, lambdas=(0.25, 0.75), seed=5).view, "lambda")
+    s2 = System.open(g1.inp, lambdas=(0.25, 0.75), seed=5)   # the view lives as long as s2
+    lam = getattr(s2.view, "lambda")
     assert (lam[0], lam[1]) == (0.25, 0.75)
 
 

@@ -162,8 +162,11 @@ struct Batch {
       launch("nb_pw", [&] { k_nb_pair<false><<<dim3(std::min(cdiv(max_pw, 256), 128), nsys), 256, 0, stream>>>(p); });
     if (any_q && max_qp > 0)
       launch("nb_qp", [&] { k_nb_qp<<<dim3(std::min(cdiv(max_qp, 256), 32), nsys), 256, 0, stream>>>(p); });
+    const bool mixed = opt.precision == QB_MIXED;
+    if (mixed) launch("split_positions", [&] { k_split_positions<<<cdiv(p.natoms_tot, 256), 256, 0, stream>>>(p); });
     if (max_nwat > 0) {
-      launch("nb_ww", [&] { k_nb_ww<<<dim3(cdiv(max_nwat, 8), nsys), 256, 0, stream>>>(p); });
+      if (mixed) launch("nb_ww", [&] { k_nb_ww_mixed<<<dim3(cdiv(max_nwat, 8), nsys), 256, 0, stream>>>(p); });
+      else launch("nb_ww", [&] { k_nb_ww<<<dim3(cdiv(max_nwat, 8), nsys), 256, 0, stream>>>(p); });
       if (any_q) launch("nb_qw", [&] { k_nb_qw<<<dim3(cdiv(max_nwat, 128), nsys), 128, 0, stream>>>(p); });
     }
     if (any_lrf)
@@ -515,6 +518,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   P.st = dev_upload(sst, o);
   P.x = dev_upload(x, o); P.v = dev_upload(v, o);
   P.xx = dev_alloc<double4>(x.size(), o); P.d = dev_alloc<double4>(x.size(), o);
+  P.xhi = dev_alloc<float4>(x.size(), o); P.xlo = dev_alloc<float4>(x.size(), o);
   P.crg = dev_upload(crg, o); P.winv = dev_upload(winv, o); P.mass = dev_upload(mass, o);
   P.iac = dev_upload(iac, o); P.iq = dev_upload(iq, o); P.cgp = dev_upload(cgp, o); P.asys = dev_upload(asys, o);
   P.flags = dev_upload(flags, o); P.lja = dev_upload(lja, o); P.ljb = dev_upload(ljb, o);

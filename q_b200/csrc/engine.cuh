@@ -56,6 +56,7 @@ struct DevPtrs {
   SysState *st;
   // atoms
   double4 *x, *v, *xx, *d;
+  float4 *xhi, *xlo;         // positions as float hi + lo (mixed precision)
   float *crg, *winv;
   double *mass;
   int *iac, *iq, *cgp, *asys;

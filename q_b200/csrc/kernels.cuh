@@ -72,11 +72,13 @@ __global__ void k_cgp_centers(DevPtrs P, int force) {
 __device__ __forceinline__ void lrf_accumulate(double *m, double q, double dx, double dy, double dz) {
   double dr[3] = {dx, dy, dz};
   double r2 = dx * dx + dy * dy + dz * dz;
-  double f0 = q / (r2 * sqrt(r2));
+  // rsqrt-based form of q/(r2*sqrt(r2)), 3 f0/r2 and -f1/r2 (same values to ~1 ulp)
+  double rinv = rsqrt(r2), ri2 = rinv * rinv;
+  double f0 = q * rinv * ri2;
   m[0] += f0 * r2;
 #pragma unroll
   for (int k = 0; k < 3; k++) m[1 + k] -= f0 * dr[k];
-  double f1 = 3. * f0 / r2;
+  double f1 = 3. * f0 * ri2;
 #pragma unroll
   for (int a = 0; a < 3; a++)
 #pragma unroll
@@ -84,7 +86,7 @@ __device__ __forceinline__ void lrf_accumulate(double *m, double q, double dx, d
       m[4 + 3 * a + b] += f1 * dr[a] * dr[b];
       if (a == b) m[4 + 3 * a + b] -= f0;
     }
-  double f2 = -f1 / r2;
+  double f2 = -f1 * ri2;
 #pragma unroll
   for (int a = 0; a < 3; a++)
 #pragma unroll
@@ -404,7 +406,7 @@ __global__ void k_lists_end(DevPtrs P, int force) {
 // nonbond_ww_spc (md.f90:11823): one warp per water i, lanes over its
 // neighbours; the 9 gradient components of i are reduced with warp shuffles.
 // Each unordered pair is evaluated from both sides; energies are halved.
-__global__ void k_nb_ww(DevPtrs P) {
+__global__ void __launch_bounds__(256, 3) k_nb_ww(DevPtrs P) {
   int s = blockIdx.y;
   const SysDev &S = P.sys[s];
   int wpb = blockDim.x >> 5;
@@ -430,7 +432,7 @@ __global__ void k_nb_ww(DevPtrs P) {
 #pragma unroll
         for (int b = 0; b < 3; b++) {
           double dx = xj[b].x - xi[a].x, dy = xj[b].y - xi[a].y, dz = xj[b].z - xi[a].z;
-          double rinv = sqrt(1.0 / (dx * dx + dy * dy + dz * dz));
+          double rinv = rsqrt(dx * dx + dy * dy + dz * dz);
           double r2 = rinv * rinv;
           float qq = (a == 0 && b == 0) ? qoo : ((a == 0 || b == 0) ? qoh : qhh);
           double Vel = (double)qq * rinv, dv;
@@ -462,6 +464,89 @@ __global__ void k_nb_ww(DevPtrs P) {
   warp_add(&P.E[s * QB_NE + QB_E_WW_VDW], 0.5 * vdw);
 }
 
+// Positions as an unevaluated float sum hi + lo (hi = float(x), lo = float(x - hi)),
+// refreshed before each mixed-precision force evaluation.  A float difference
+// (hj - hi) + (lj - li) then carries ~1e-7 relative error, like an FP64
+// difference rounded to FP32.
+__global__ void k_split_positions(DevPtrs P) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= P.natoms_tot) return;
+  double4 x = P.x[g];
+  float hx = (float)x.x, hy = (float)x.y, hz = (float)x.z;
+  P.xhi[g] = make_float4(hx, hy, hz, 0.f);
+  P.xlo[g] = make_float4((float)(x.x - (double)hx), (float)(x.y - (double)hy), (float)(x.z - (double)hz), 0.f);
+}
+
+// nonbond_ww_spc (md.f90:11823) in mixed precision: the pair terms in FP32
+// (rsqrtf on the MUFU pipe), each neighbour molecule's 9 energy terms summed
+// in FP32 and added to FP64 accumulators, gradient partials reduced in FP64.
+__global__ void __launch_bounds__(256, 3) k_nb_ww_mixed(DevPtrs P) {
+  int s = blockIdx.y;
+  const SysDev &S = P.sys[s];
+  int wpb = blockDim.x >> 5;
+  int iw = blockIdx.x * wpb + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  bool active = iw < S.nwat;
+  double el = 0, vdw = 0;
+  float f[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) f[k] = 0.f;
+  int oi = S.aoff + S.nsol + 3 * iw;
+  if (active) {
+    int gw = S.woff + iw;
+    int n = P.ww_n[gw];
+    const int *nb = P.ww + (size_t)gw * P.ww_cap;
+    float4 hi[3] = {P.xhi[oi], P.xhi[oi + 1], P.xhi[oi + 2]};
+    float4 li[3] = {P.xlo[oi], P.xlo[oi + 1], P.xlo[oi + 2]};
+    const float qo = S.crg_ow, qh = S.crg_hw;
+    const float qoo = qo * qo, qoh = qo * qh, qhh = qh * qh;
+    const float A = (float)S.A_OO, B = (float)S.B_OO;
+    for (int k = lane; k < n; k += 32) {
+      int oj = nb[k];
+      float4 hj[3] = {P.xhi[oj], P.xhi[oj + 1], P.xhi[oj + 2]};
+      float4 lj[3] = {P.xlo[oj], P.xlo[oj + 1], P.xlo[oj + 2]};
+      float e_el = 0.f, e_vdw = 0.f;
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+          float dx = (hj[b].x - hi[a].x) + (lj[b].x - li[a].x);
+          float dy = (hj[b].y - hi[a].y) + (lj[b].y - li[a].y);
+          float dz = (hj[b].z - hi[a].z) + (lj[b].z - li[a].z);
+          float rinv = rsqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+          float r2 = rinv * rinv;
+          float qq = (a == 0 && b == 0) ? qoo : ((a == 0 || b == 0) ? qoh : qhh);
+          float Vel = qq * rinv, dv;
+          if (a == 0 && b == 0) {
+            float r6 = r2 * r2 * r2;
+            float Va = A * r6 * r6, Vb = B * r6;
+            e_vdw += Va - Vb;
+            dv = r2 * (-Vel - 12.f * Va + 6.f * Vb);
+          } else {
+            dv = -r2 * Vel;
+          }
+          e_el += Vel;
+          f[3 * a + 0] = fmaf(-dv, dx, f[3 * a + 0]);
+          f[3 * a + 1] = fmaf(-dv, dy, f[3 * a + 1]);
+          f[3 * a + 2] = fmaf(-dv, dz, f[3 * a + 2]);
+        }
+      el += (double)e_el;
+      vdw += (double)e_vdw;
+    }
+  }
+  double fd[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) fd[k] = warp_sum((double)f[k]);
+  if (active && lane == 0) {
+    for (int a = 0; a < 3; a++) {
+      double4 dd = P.d[oi + a];
+      dd.x += fd[3 * a]; dd.y += fd[3 * a + 1]; dd.z += fd[3 * a + 2];
+      P.d[oi + a] = dd;
+    }
+  }
+  warp_add(&P.E[s * QB_NE + QB_E_WW_EL], 0.5 * el);
+  warp_add(&P.E[s * QB_NE + QB_E_WW_VDW], 0.5 * vdw);
+}
+
 // nonbond_pp (md.f90:10387) and nonbond_pw (10631): one thread per pair.
 template <bool PP>
 __global__ void k_nb_pair(DevPtrs P) {
@@ -477,8 +562,8 @@ __global__ void k_nb_pair(DevPtrs P) {
       int i = p.x, j = p.y, lj = p.z;
       double3 xi = ld3(P.x, i), xj = ld3(P.x, j);
       double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-      double r2 = 1. / (dx * dx + dy * dy + dz * dz);
-      double r = sqrt(r2), r6 = r2 * r2 * r2;
+      double r = rsqrt(dx * dx + dy * dy + dz * dz);
+      double r2 = r * r, r6 = r2 * r2 * r2;
       float qq = P.crg[i] * P.crg[j];
       double Vel = (double)qq * r;
       if (PP && lj == 3) Vel = Vel * S.el14;
@@ -516,8 +601,9 @@ __global__ void k_nb_qp(DevPtrs P) {
       double r2 = dx * dx + dy * dy + dz * dz;
       double dvsum = 0;
       if (!S.qvdw) {
-        r2 = 1. / r2;
-        double r6 = r2 * r2 * r2, r = sqrt(r2);
+        double r = rsqrt(r2);
+        r2 = r * r;
+        double r6 = r2 * r2 * r2;
         double aLJ = P.lja[3 * i + lj - 1] * P.lja[3 * j + lj - 1];
         double bLJ = P.ljb[3 * i + lj - 1] * P.ljb[3 * j + lj - 1];
         for (int st = 0; st < NS; st++) {
@@ -531,8 +617,8 @@ __global__ void k_nb_qp(DevPtrs P) {
         }
       } else {
         double r6 = r2 * r2 * r2;
-        r2 = 1. / r2;
-        double r = sqrt(r2);
+        double r = rsqrt(r2);
+        r2 = r * r;
         int tj = P.iac[j];
         for (int st = 0; st < NS; st++) {
           int ti = P.qiac[gq * MAXS + st];
@@ -588,11 +674,11 @@ __global__ void k_nb_qw(DevPtrs P) {
         double dH1[3] = {xH1.x - xi.x, xH1.y - xi.y, xH1.z - xi.z};
         double dH2[3] = {xH2.x - xi.x, xH2.y - xi.y, xH2.z - xi.z};
         double r2O = dO[0] * dO[0] + dO[1] * dO[1] + dO[2] * dO[2];
-        double rH1 = sqrt(1.0 / (dH1[0] * dH1[0] + dH1[1] * dH1[1] + dH1[2] * dH1[2]));
-        double rH2 = sqrt(1.0 / (dH2[0] * dH2[0] + dH2[1] * dH2[1] + dH2[2] * dH2[2]));
+        double rH1 = rsqrt(dH1[0] * dH1[0] + dH1[1] * dH1[1] + dH1[2] * dH1[2]);
+        double rH2 = rsqrt(dH2[0] * dH2[0] + dH2[1] * dH2[1] + dH2[2] * dH2[2]);
         double r6hc = r2O * r2O * r2O;
-        r2O = 1.0 / r2O;
-        double rO = sqrt(r2O);
+        double rO = rsqrt(r2O);
+        r2O = rO * rO;
         double r2H1 = rH1 * rH1, r2H2 = rH2 * rH2;
         double r6sc = r6hc, dvO = 0, dvH1 = 0, dvH2 = 0, Va = 0, Vb = 0;
         int lj = P.ljcod[S.ljoff + S.iac_ow * S.natyps + P.iac[i]];
@@ -1367,11 +1453,74 @@ __global__ void k_leapfrog(DevPtrs P) {
 
 // shake (md.f90:14445): Gauss-Seidel iterations over one molecule's
 // constraints per thread, to relative tolerance 1e-4, at most 1000 passes.
+__device__ __forceinline__ double3 pick3(int k, double3 a, double3 b, double3 c) {
+  return k == 0 ? a : (k == 1 ? b : c);
+}
+__device__ __forceinline__ void put3(int k, double3 v, double3 &a, double3 &b, double3 &c) {
+  if (k == 0) a = v;
+  else if (k == 1) b = v;
+  else c = v;
+}
+
+// The same Gauss-Seidel iteration for a molecule of three consecutive atoms
+// with three constraints (rigid water), with its state held in registers.
+__device__ bool shake3(DevPtrs &P, int base, const int2 *ij, const double *d2) {
+  double3 p0 = ld3(P.x, base), p1 = ld3(P.x, base + 1), p2 = ld3(P.x, base + 2);
+  double3 r0 = ld3(P.xx, base), r1 = ld3(P.xx, base + 1), r2 = ld3(P.xx, base + 2);
+  float w0 = P.winv[base], w1 = P.winv[base + 1], w2 = P.winv[base + 2];
+  int ca[3], cb[3];
+  double dd[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) { ca[c] = ij[c].x - base; cb[c] = ij[c].y - base; dd[c] = d2[c]; }
+  bool ready[3] = {false, false, false};
+  int nits = 0;
+  for (;;) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      if (ready[c]) continue;
+      double3 xi = pick3(ca[c], p0, p1, p2), xj = pick3(cb[c], p0, p1, p2);
+      double3 ri = pick3(ca[c], r0, r1, r2), rj = pick3(cb[c], r0, r1, r2);
+      float wi = ca[c] == 0 ? w0 : (ca[c] == 1 ? w1 : w2);
+      float wj = cb[c] == 0 ? w0 : (cb[c] == 1 ? w1 : w2);
+      double xij[3] = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
+      double xij2 = xij[0] * xij[0] + xij[1] * xij[1] + xij[2] * xij[2];
+      double diff = dd[c] - xij2;
+      if (fabs(diff) < 0.0001 * dd[c]) ready[c] = true;
+      double xxij[3] = {ri.x - rj.x, ri.y - rj.y, ri.z - rj.z};
+      double scp = xij[0] * xxij[0] + xij[1] * xxij[1] + xij[2] * xxij[2];
+      float wsum = wi + wj;
+      double corr = diff / (2. * scp * (double)wsum);
+      xi.x += xxij[0] * corr * (double)wi; xi.y += xxij[1] * corr * (double)wi; xi.z += xxij[2] * corr * (double)wi;
+      xj.x -= xxij[0] * corr * (double)wj; xj.y -= xxij[1] * corr * (double)wj; xj.z -= xxij[2] * corr * (double)wj;
+      put3(ca[c], xi, p0, p1, p2);
+      put3(cb[c], xj, p0, p1, p2);
+    }
+    nits++;
+    if (ready[0] && ready[1] && ready[2]) break;
+    if (nits >= 1000) return false;
+  }
+  double4 o0 = P.x[base], o1 = P.x[base + 1], o2 = P.x[base + 2];
+  o0.x = p0.x; o0.y = p0.y; o0.z = p0.z;
+  o1.x = p1.x; o1.y = p1.y; o1.z = p1.z;
+  o2.x = p2.x; o2.y = p2.y; o2.z = p2.z;
+  P.x[base] = o0; P.x[base + 1] = o1; P.x[base + 2] = o2;
+  return true;
+}
+
 __global__ void k_shake(DevPtrs P) {
   int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= P.nshake_tot) return;
   int f = P.sh_first[m], n = P.sh_n[m];
   if (n == 0) return;
+  if (n == 3) {
+    int2 a = P.sh_ij[f], b = P.sh_ij[f + 1], c = P.sh_ij[f + 2];
+    int lo = min(min(min(a.x, a.y), min(b.x, b.y)), min(c.x, c.y));
+    int hi = max(max(max(a.x, a.y), max(b.x, b.y)), max(c.x, c.y));
+    if (hi - lo <= 2) {
+      if (!shake3(P, lo, P.sh_ij + f, P.sh_d2 + f)) set_status(&P.st[P.sh_sys[m]], QB_ERR_SHAKE);
+      return;
+    }
+  }
   bool done = false;
   int nits = 0;
   // readiness flags of up to 64*64 constraints in thread-local memory

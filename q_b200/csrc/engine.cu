@@ -58,7 +58,7 @@ struct Batch {
   cudaStream_t stream = nullptr;
   int NB = 1;
   long long istep = 0;
-  int max_natom = 0, max_nwat = 0, max_ncgp_sol = 0, max_terms = 0, max_pp = 0, max_pw = 0, max_qp = 0;
+  int max_natom = 0, max_nwat = 0, max_ncgp = 0, max_ncgp_sol = 0, max_terms = 0, max_pp = 0, max_pw = 0, max_qp = 0;
   bool any_lrf = false, any_q = false, any_shake = false, any_wpol = false, any_prestr = false, any_qq = false,
        any_qb = false;
   size_t watpol_smem = 0;
@@ -140,7 +140,7 @@ struct Batch {
     if (max_nwat > 0)
       launch("list_ww", [&] { k_list_ww<<<dim3(cdiv(max_nwat, 8), nsys), 256, 0, stream>>>(p, force); });
     if (any_lrf)
-      launch("lrf_gather", [&] { k_lrf_gather<<<cdiv((long long)p.ncgp_tot * 32, 128), 128, 0, stream>>>(p, force); });
+      launch("lrf_gather", [&] { k_lrf_gather<<<dim3(cdiv(max_ncgp, LRF_BLOCK), nsys), LRF_BLOCK, 0, stream>>>(p, force); });
     launch("lists_end", [&] { k_lists_end<<<cdiv(nsys, 128), 128, 0, stream>>>(p, force); });
     check_launch("list kernels");
   }
@@ -163,10 +163,16 @@ struct Batch {
     if (any_q && max_qp > 0)
       launch("nb_qp", [&] { k_nb_qp<<<dim3(std::min(cdiv(max_qp, 256), 32), nsys), 256, 0, stream>>>(p); });
     const bool mixed = opt.precision == QB_MIXED;
-    if (mixed) launch("split_positions", [&] { k_split_positions<<<cdiv(p.natoms_tot, 256), 256, 0, stream>>>(p); });
     if (max_nwat > 0) {
-      if (mixed) launch("nb_ww", [&] { k_nb_ww_mixed<<<dim3(cdiv(max_nwat, 8), nsys), 256, 0, stream>>>(p); });
-      else launch("nb_ww", [&] { k_nb_ww<<<dim3(cdiv(max_nwat, 8), nsys), 256, 0, stream>>>(p); });
+      dim3 gp(cdiv(max_nwat, 256), nsys), gw(cdiv(max_nwat, WW_WPB), nsys);
+      size_t smem = (size_t)p.ww_chunk * WREC * sizeof(float4);
+      if (mixed) {
+        launch("pack_waters", [&] { k_pack_waters<true><<<gp, 256, 0, stream>>>(p); });
+        launch("nb_ww", [&] { k_nb_ww<true><<<gw, WW_BLOCK, smem, stream>>>(p); });
+      } else {
+        launch("pack_waters", [&] { k_pack_waters<false><<<gp, 256, 0, stream>>>(p); });
+        launch("nb_ww", [&] { k_nb_ww<false><<<gw, WW_BLOCK, smem, stream>>>(p); });
+      }
       if (any_q) launch("nb_qw", [&] { k_nb_qw<<<dim3(cdiv(max_nwat, 128), nsys), 128, 0, stream>>>(p); });
     }
     if (any_lrf)
@@ -236,6 +242,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   std::vector<uint32_t> lx, l14;
   std::vector<int2> exl, l14l;
   std::vector<int> cg_first, cg_last, cg_sw, cg_atoms, cg_sys;
+  std::vector<int2> lrft;
   std::vector<int> iqseq, qiac;
   std::vector<float> qcrg;
   std::vector<double> qavdw, qbvdw, sc, qq_el;
@@ -268,6 +275,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     if (V.iuse_switch_atom != 1) fail(QB_ERR_UNSUPPORTED, "charge-group cut-offs on any atom are not supported");
     const int aoff = (int)x.size();
     S.aoff = aoff; S.natom = V.natom; S.nsol = V.nat_solute; S.nwat = V.nwat;
+    if (V.nwat > 65535) fail(QB_ERR_UNSUPPORTED, "more than 65535 waters in one system");
     S.woff = 0;
     S.coff = (int)cg_first.size(); S.ncgp = V.ncgp; S.ncgp_sol = V.ncgp_solute;
     S.qoff = (int)iqseq.size(); S.nq = V.nqat; S.S = V.nstates; S.natyps = V.natyps;
@@ -302,6 +310,22 @@ void build(Batch &B, qb_handle *const *hs, int n) {
       cg_sys.push_back(s);
     }
     for (int a = 0; a < V.natom; a++) cg_atoms.push_back(aoff + V.cgpatom[a]);
+    // LRF gather tiles: runs of consecutive groups with contiguous atom ranges
+    S.lrft_off = (int)lrft.size(); S.nlrft = 0;
+    if (V.use_LRF) {
+      int h0 = 0;
+      while (h0 < V.ncgp) {
+        int h1 = h0 + 1;
+        if (V.cgp_last[h0] - V.cgp_first[h0] + 1 > LRF_TILE_A)
+          fail(QB_ERR_UNSUPPORTED, "a charge group has more atoms than the LRF tile holds");
+        while (h1 < V.ncgp && h1 - h0 < LRF_TILE_G && V.cgp_first[h1] == V.cgp_last[h1 - 1] + 1 &&
+               V.cgp_last[h1] - V.cgp_first[h0] + 1 <= LRF_TILE_A)
+          h1++;
+        lrft.push_back(make_int2(h0, h1));
+        S.nlrft++;
+        h0 = h1;
+      }
+    }
     // water groups must be O,H,H with the oxygen as switching atom
     for (int iw = 0; iw < V.nwat; iw++) {
       int g = V.ncgp_solute + iw;
@@ -490,6 +514,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     B.max_natom = std::max(B.max_natom, V.natom);
     B.max_nwat = std::max(B.max_nwat, V.nwat);
     B.max_ncgp_sol = std::max(B.max_ncgp_sol, V.ncgp_solute);
+    B.max_ncgp = std::max(B.max_ncgp, V.ncgp);
     B.max_terms = std::max(B.max_terms, V.nbonds + V.nangles + V.ntors + V.nimps);
     B.max_pp = std::max(B.max_pp, S.pp_cap);
     B.max_pw = V.nwat > 0 ? std::max(B.max_pw, S.pw_cap) : B.max_pw;
@@ -518,7 +543,6 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   P.st = dev_upload(sst, o);
   P.x = dev_upload(x, o); P.v = dev_upload(v, o);
   P.xx = dev_alloc<double4>(x.size(), o); P.d = dev_alloc<double4>(x.size(), o);
-  P.xhi = dev_alloc<float4>(x.size(), o); P.xlo = dev_alloc<float4>(x.size(), o);
   P.crg = dev_upload(crg, o); P.winv = dev_upload(winv, o); P.mass = dev_upload(mass, o);
   P.iac = dev_upload(iac, o); P.iq = dev_upload(iq, o); P.cgp = dev_upload(cgp, o); P.asys = dev_upload(asys, o);
   P.flags = dev_upload(flags, o); P.lja = dev_upload(lja, o); P.ljb = dev_upload(ljb, o);
@@ -528,6 +552,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   P.cg_first = dev_upload(cg_first, o); P.cg_last = dev_upload(cg_last, o); P.cg_sw = dev_upload(cg_sw, o);
   P.cg_atoms = dev_upload(cg_atoms, o); P.cg_sys = dev_upload(cg_sys, o);
   P.lrf = dev_alloc<double>((size_t)P.ncgp_tot * LRF_STRIDE, o);
+  P.lrft = dev_upload(lrft, o);
   P.iqseq = dev_upload(iqseq, o); P.qcrg = dev_upload(qcrg, o); P.qiac = dev_upload(qiac, o);
   P.qavdw = dev_upload(qavdw, o); P.qbvdw = dev_upload(qbvdw, o); P.sc = dev_upload(sc, o);
   P.qconn = dev_upload(qconn, o); P.qq = dev_upload(qq, o); P.qq_el = dev_upload(qq_el, o);
@@ -544,9 +569,20 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   P.ra = dev_upload(ra, o); P.ra_p = dev_upload(ra_p, o); P.rw = dev_upload(rw, o); P.rw_p = dev_upload(rw_p, o);
   P.pp = dev_alloc<int4>(pp_tot, o); P.pw = dev_alloc<int4>(pw_tot, o);
   P.qp = dev_alloc<int4>(qp_tot, o); P.qw = dev_alloc<int>(qw_tot, o);
+  // water-water staging chunk: a multiple of 32 waters, two blocks per SM
+  P.ww_chunk = std::min((B.max_nwat + 31) / 32 * 32, WW_CHUNK_MAX);
+  P.ww_chunk = std::max(P.ww_chunk, 32);
+  P.ww_nch = (std::max(B.max_nwat, 1) + P.ww_chunk - 1) / P.ww_chunk;
   P.ww_cap = ww_cap;
-  P.ww = dev_alloc<int>((size_t)std::max(woff, 1) * ww_cap, o);
+  P.ww = dev_alloc<uint16_t>((size_t)std::max(woff, 1) * ww_cap, o);
   P.ww_n = dev_alloc<int>(std::max(woff, 1), o);
+  P.ww_sp = dev_alloc<int>((size_t)std::max(woff, 1) * P.ww_nch, o);
+  P.wrec = dev_alloc<float4>((size_t)std::max(woff, 1) * WREC, o);
+  {
+    int smem = P.ww_chunk * WREC * (int)sizeof(float4);
+    CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  }
   P.E = dev_alloc<double>((size_t)n * QB_NE, o);
   P.EQ = dev_alloc<double>((size_t)n * MAXS * QB_NEQ, o);
   P.hist = nullptr;

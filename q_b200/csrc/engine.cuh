@@ -22,6 +22,7 @@ struct SysDev {
   int aoff, natom, nsol, nwat, woff, coff, ncgp, ncgp_sol;
   int qoff, nq, S, natyps, ljoff, qlib_off, sc_off, qconn_off;
   int exl_off, nexl, l14_off, nl14;
+  int lrft_off, nlrft;        // LRF gather tiles (group ranges)
   // static term ranges (global offsets into term arrays)
   int b_off, nb, nb_sol, a_off, na, na_sol, t_off, nt, nt_sol, i_off, ni, ni_sol;
   int qb_off, nqb, qa_off, nqa, qt_off, nqt, qi_off, nqi;
@@ -56,7 +57,7 @@ struct DevPtrs {
   SysState *st;
   // atoms
   double4 *x, *v, *xx, *d;
-  float4 *xhi, *xlo;         // positions as float hi + lo (mixed precision)
+  float4 *wrec;              // per-water position records of the water-water kernel
   float *crg, *winv;
   double *mass;
   int *iac, *iq, *cgp, *asys;
@@ -69,6 +70,7 @@ struct DevPtrs {
   // charge groups
   int *cg_first, *cg_last, *cg_sw, *cg_atoms, *cg_sys;
   double *lrf;              // [gc*LRF_STRIDE]
+  int2 *lrft;               // per system segments: [first, end) local groups of a tile
   // Q atoms
   int *iqseq;               // global atom of global Q atom
   float *qcrg;              // [gq*MAXS + st]
@@ -99,8 +101,9 @@ struct DevPtrs {
   int4 *pp, *pw;                           // i, j, lj
   int4 *qp;                                // gq, j, lj, qlj
   int *qw;                                 // water O atoms
-  int *ww, *ww_n;                          // [gw*ww_cap + k], count per water
-  int ww_cap;
+  uint16_t *ww;                            // [gw*ww_cap + k] local water index
+  int *ww_n, *ww_sp;                       // count per water; [gw*ww_nch + c] count below chunk c's end
+  int ww_cap, ww_chunk, ww_nch;
   // energies
   double *E;                               // [s*QB_NE]
   double *EQ;                              // [(s*MAXS + st)*QB_NEQ]

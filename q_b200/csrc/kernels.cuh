@@ -67,93 +67,132 @@ __global__ void k_cgp_centers(DevPtrs P, int force) {
   for (int k = 3; k < LRF_STRIDE; k++) L[k] = 0.0;
 }
 
-// Multipole contribution of charge q at offset dr from a group centre
-// (md.f90:5581-5636), accumulated into m[40] = phi0, phi1[3], phi2[9], phi3[27].
+// Multipole contribution of charge q at offset (dx,dy,dz) from a group centre
+// (md.f90:5581-5636), accumulated in the symmetric form m[20] = phi0,
+// phi1[x,y,z], phi2[xx,xy,xz,yy,yz,zz], phi3[xxx,xxy,xxz,xyy,xyz,xzz,yyy,yyz,
+// yzz,zzz]; lrf_expand writes the full 1+3+9+27 layout the reference stores.
 __device__ __forceinline__ void lrf_accumulate(double *m, double q, double dx, double dy, double dz) {
-  double dr[3] = {dx, dy, dz};
   double r2 = dx * dx + dy * dy + dz * dz;
-  // rsqrt-based form of q/(r2*sqrt(r2)), 3 f0/r2 and -f1/r2 (same values to ~1 ulp)
   double rinv = rsqrt(r2), ri2 = rinv * rinv;
-  double f0 = q * rinv * ri2;
+  double f0 = q * rinv * ri2;              // q / r^3
   m[0] += f0 * r2;
-#pragma unroll
-  for (int k = 0; k < 3; k++) m[1 + k] -= f0 * dr[k];
+  m[1] -= f0 * dx; m[2] -= f0 * dy; m[3] -= f0 * dz;
   double f1 = 3. * f0 * ri2;
-#pragma unroll
-  for (int a = 0; a < 3; a++)
-#pragma unroll
-    for (int b = 0; b < 3; b++) {
-      m[4 + 3 * a + b] += f1 * dr[a] * dr[b];
-      if (a == b) m[4 + 3 * a + b] -= f0;
-    }
+  double f1x = f1 * dx, f1y = f1 * dy, f1z = f1 * dz;
+  m[4] += f1x * dx - f0; m[5] += f1x * dy; m[6] += f1x * dz;
+  m[7] += f1y * dy - f0; m[8] += f1y * dz; m[9] += f1z * dz - f0;
   double f2 = -f1 * ri2;
+  double x5 = 5. * dx, y5 = 5. * dy, z5 = 5. * dz;
+  double xx = x5 * dx, yy = y5 * dy, zz = z5 * dz, xy = x5 * dy;
+  m[10] += f2 * (xx * dx - 3. * r2 * dx);
+  m[11] += f2 * (xx * dy - r2 * dy);
+  m[12] += f2 * (xx * dz - r2 * dz);
+  m[13] += f2 * (yy * dx - r2 * dx);
+  m[14] += f2 * (xy * dz);
+  m[15] += f2 * (zz * dx - r2 * dx);
+  m[16] += f2 * (yy * dy - 3. * r2 * dy);
+  m[17] += f2 * (yy * dz - r2 * dz);
+  m[18] += f2 * (zz * dy - r2 * dy);
+  m[19] += f2 * (zz * dz - 3. * r2 * dz);
+}
+
+__device__ __forceinline__ void lrf_expand(const double *m, double *L) {
+  L[3] = m[0];
+  L[4] = m[1]; L[5] = m[2]; L[6] = m[3];
+  const int i2[9] = {4, 5, 6, 5, 7, 8, 6, 8, 9};
 #pragma unroll
-  for (int a = 0; a < 3; a++)
+  for (int k = 0; k < 9; k++) L[7 + k] = m[i2[k]];
+  // unique index of the sorted triple (a<=b<=c) for every (a,b,c)
+  const int i3[27] = {10, 11, 12, 11, 13, 14, 12, 14, 15, 11, 13, 14, 13, 16, 17, 14, 17, 18,
+                      12, 14, 15, 14, 17, 18, 15, 18, 19};
 #pragma unroll
-    for (int b = 0; b < 3; b++)
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        double t = 5. * dr[a] * dr[b] * dr[c];
-        if (a == b && b == c) t -= r2 * 3. * dr[a];
-        else {
-          if (a == b) t -= r2 * dr[c];
-          if (a == c) t -= r2 * dr[b];
-          if (b == c) t -= r2 * dr[a];
-        }
-        m[13 + 9 * a + 3 * b + c] += f2 * t;
-      }
+  for (int k = 0; k < 27; k++) L[16 + k] = m[i3[k]];
 }
 
 // LRF multipoles of every charge group, gathered (nbpplist_lrf 5448,
 // nbpwlist_lrf 6864, nbwwlist_lrf 8370).  A group g receives the charges of
 // every group h whose switching atoms lie beyond the pair's cut-off but within
-// RcLRF (both switching atoms inside the sphere; Q atoms carry no charge here).
-// The reference visits each unordered pair once and adds to both groups; the
-// gather adds the same contributions.  One warp per group.
-__global__ void k_lrf_gather(DevPtrs P, int force) {
-  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (warp >= P.ncgp_tot) return;
-  int g = warp;
-  int s = P.cg_sys[g];
+// RcLRF (both switching atoms inside the sphere; solute Q atoms carry no
+// charge here).  The reference visits each unordered pair once and adds to
+// both groups; the gather adds the same contributions.
+//
+// One thread per group g, blockIdx.y = system.  The system's groups are swept
+// in tiles (consecutive groups, at most LRF_TILE_G groups and LRF_TILE_A
+// atoms, boundaries precomputed on the host): a tile's switching atoms and
+// atom positions/charges are staged in shared memory and read as broadcasts.
+constexpr int LRF_TILE_G = 128, LRF_TILE_A = 512, LRF_BLOCK = 128;
+
+__global__ void __launch_bounds__(LRF_BLOCK) k_lrf_gather(DevPtrs P, int force) {
+  int s = blockIdx.y;
   if (!list_due(P, s, force)) return;
   const SysDev &S = P.sys[s];
-  int swg = P.cg_sw[g];
-  if (P.flags[swg] & F_EXCL) return;
-  double *L = P.lrf + (size_t)g * LRF_STRIDE;
-  double cx = L[0], cy = L[1], cz = L[2];
-  double3 xs = ld3(P.x, swg);
-  bool g_sol = (g - S.coff) < S.ncgp_sol;
-  double m[40];
+  if (!S.use_lrf || blockIdx.x * LRF_BLOCK >= S.ncgp) return;
+  __shared__ double4 hsw[LRF_TILE_G];      // switching atom; w: -1 excluded, 1 solute, 0 water
+  __shared__ int2 hrange[LRF_TILE_G];      // first atom slot, atom count
+  __shared__ double4 hat[LRF_TILE_A];      // atom position, charge
+  int gl = blockIdx.x * LRF_BLOCK + threadIdx.x;
+  int g = S.coff + gl;
+  bool active = gl < S.ncgp;
+  double cx = 0, cy = 0, cz = 0;
+  double3 xs = make_double3(0, 0, 0);
+  if (active) {
+    int swg = P.cg_sw[g];
+    active = !(P.flags[swg] & F_EXCL);
+    const double *L = P.lrf + (size_t)g * LRF_STRIDE;
+    cx = L[0]; cy = L[1]; cz = L[2];
+    xs = ld3(P.x, swg);
+  }
+  const bool g_sol = gl < S.ncgp_sol;
+  double m[20];
 #pragma unroll
-  for (int k = 0; k < 40; k++) m[k] = 0.0;
-  for (int hl = lane; hl < S.ncgp; hl += 32) {
-    int h = S.coff + hl;
-    if (h == g) continue;
-    int swh = P.cg_sw[h];
-    if (P.flags[swh] & F_EXCL) continue;
-    double3 xh = ld3(P.x, swh);
-    double dx = xs.x - xh.x, dy = xs.y - xh.y, dz = xs.z - xh.z;
-    double r2 = dx * dx + dy * dy + dz * dz;
-    bool h_sol = hl < S.ncgp_sol;
-    double rc2 = (g_sol && h_sol) ? S.Rcpp2 : ((g_sol || h_sol) ? S.Rcpw2 : S.Rcww2);
-    if (!(r2 > rc2 && r2 <= S.RcLRF2)) continue;
-    for (int a = P.cg_first[h]; a <= P.cg_last[h]; a++) {
-      int at = P.cg_atoms[a];
-      if (h_sol && P.iq[at] >= 0) continue;
-      double3 xa = ld3(P.x, at);
-      lrf_accumulate(m, (double)P.crg[at], xa.x - cx, xa.y - cy, xa.z - cz);
+  for (int k = 0; k < 20; k++) m[k] = 0.0;
+  for (int t = 0; t < S.nlrft; t++) {
+    int2 tile = P.lrft[S.lrft_off + t];
+    int nh = tile.y - tile.x;
+    int a0 = P.cg_first[S.coff + tile.x];
+    int na = P.cg_last[S.coff + tile.y - 1] - a0 + 1;
+    __syncthreads();
+    for (int i = threadIdx.x; i < nh; i += LRF_BLOCK) {
+      int h = S.coff + tile.x + i;
+      int sw = P.cg_sw[h];
+      double3 p = ld3(P.x, sw);
+      double w = (P.flags[sw] & F_EXCL) ? -1.0 : (tile.x + i < S.ncgp_sol ? 1.0 : 0.0);
+      hsw[i] = make_double4(p.x, p.y, p.z, w);
+      hrange[i] = make_int2(P.cg_first[h] - a0, P.cg_last[h] - P.cg_first[h] + 1);
+    }
+    for (int i = threadIdx.x; i < na; i += LRF_BLOCK) {
+      int at = P.cg_atoms[a0 + i];
+      double4 p = P.x[at];
+      bool qsol = (at - S.aoff) < S.nsol && P.iq[at] >= 0;
+      p.w = qsol ? 0.0 : (double)P.crg[at];
+      hat[i] = p;
+    }
+    __syncthreads();
+    if (active) {
+      for (int i = 0; i < nh; i++) {
+        double4 hs = hsw[i];
+        if (hs.w < 0.0 || tile.x + i == gl) continue;
+        double dx = xs.x - hs.x, dy = xs.y - hs.y, dz = xs.z - hs.z;
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double rc2 = (g_sol && hs.w > 0.0) ? S.Rcpp2 : ((g_sol || hs.w > 0.0) ? S.Rcpw2 : S.Rcww2);
+        if (!(r2 > rc2 && r2 <= S.RcLRF2)) continue;
+        int2 rg = hrange[i];
+        for (int k = 0; k < rg.y; k++) {
+          double4 a = hat[rg.x + k];
+          if (a.w != 0.0) lrf_accumulate(m, a.w, a.x - cx, a.y - cy, a.z - cz);
+        }
+      }
     }
   }
-#pragma unroll
-  for (int k = 0; k < 40; k++) {
-    double t = warp_sum(m[k]);
-    if (lane == 0) L[3 + k] = t;
-  }
+  if (active) lrf_expand(m, P.lrf + (size_t)g * LRF_STRIDE);
 }
 
 // Water-water neighbour list (nbwwlist / nbwwlist_lrf, md.f90:8233, 8370),
 // stored in both directions: water i lists every other water j inside the
-// sphere whose O lies within Rcww of i's O.  One warp per water.
+// sphere whose O lies within Rcww of i's O, as local water indices in
+// ascending order.  ww_sp[gw*ww_nch + c] counts the entries below the end of
+// staging chunk c (chunks of ww_chunk waters, a multiple of 32), so the force
+// kernel finds each chunk's slice of the list directly.  One warp per water.
 __global__ void k_list_ww(DevPtrs P, int force) {
   int s = blockIdx.y;
   if (!list_due(P, s, force)) return;
@@ -164,10 +203,12 @@ __global__ void k_list_ww(DevPtrs P, int force) {
   int gw = S.woff + iw;
   int oi = S.aoff + S.nsol + 3 * iw;
   int cnt = 0;
-  int *out = P.ww + (size_t)gw * P.ww_cap;
+  uint16_t *out = P.ww + (size_t)gw * P.ww_cap;
+  int *sp = P.ww_sp + (size_t)gw * P.ww_nch;
   if (!(P.flags[oi] & F_EXCL)) {
     double3 xi = ld3(P.x, oi);
     for (int base = 0; base < S.nwat; base += 32) {
+      if (base > 0 && base % P.ww_chunk == 0 && lane == 0) sp[base / P.ww_chunk - 1] = min(cnt, P.ww_cap);
       int jw = base + lane;
       bool ok = false;
       int oj = S.aoff + S.nsol + 3 * jw;
@@ -179,14 +220,17 @@ __global__ void k_list_ww(DevPtrs P, int force) {
       unsigned bal = __ballot_sync(FULL, ok);
       if (ok) {
         int pos = cnt + __popc(bal & ((1u << lane) - 1u));
-        if (pos < P.ww_cap) out[pos] = oj;
+        if (pos < P.ww_cap) out[pos] = (uint16_t)jw;
       }
       cnt += __popc(bal);
     }
+  } else if (lane == 0) {
+    for (int c = 0; c < P.ww_nch; c++) sp[c] = 0;
   }
   if (lane == 0) {
     if (cnt > P.ww_cap) { set_status(&P.st[s], QB_ERR_LIST_OVERFLOW); cnt = P.ww_cap; }
     P.ww_n[gw] = cnt;
+    for (int c = (S.nwat - 1) / P.ww_chunk; c < P.ww_nch; c++) sp[c] = cnt;
   }
 }
 
@@ -403,144 +447,192 @@ __global__ void k_lists_end(DevPtrs P, int force) {
 
 // ------------------------------------------------------------- nonbonded
 
-// nonbond_ww_spc (md.f90:11823): one warp per water i, lanes over its
-// neighbours; the 9 gradient components of i are reduced with warp shuffles.
-// Each unordered pair is evaluated from both sides; energies are halved.
-__global__ void __launch_bounds__(256, 3) k_nb_ww(DevPtrs P) {
+// Per-water position records of the water-water kernel: 80 bytes (five
+// 16-byte words) per water, O,H1,H2 x,y,z.  Mixed precision: hi[9] then lo[9]
+// floats (hi = float(x), lo = float(x - hi)) and two pad floats, so a float
+// difference (hj - hi) + (lj - li) carries ~1e-7 relative error, like an FP64
+// difference rounded to FP32.  FP64: x[9] doubles and one pad double.  The
+// 80-byte stride puts 8 consecutive waters on 8 distinct 16-byte bank groups.
+constexpr int WREC = 5;
+constexpr int WW_BLOCK = 512, WW_WPB = 128;   // threads, waters per block
+constexpr int WW_CHUNK_MAX = 1280;            // 100 KB of records: two blocks per SM
+
+template <bool MIXED>
+__global__ void k_pack_waters(DevPtrs P) {
   int s = blockIdx.y;
   const SysDev &S = P.sys[s];
-  int wpb = blockDim.x >> 5;
-  int iw = blockIdx.x * wpb + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  bool active = iw < S.nwat;
-  double el = 0, vdw = 0;
-  double f[9];
+  int iw = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iw >= S.nwat) return;
+  int o = S.aoff + S.nsol + 3 * iw;
+  double4 a = P.x[o], b = P.x[o + 1], c = P.x[o + 2];
+  float4 *r = P.wrec + (size_t)(S.woff + iw) * WREC;
+  if (MIXED) {
+    const double v[9] = {a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z};
+    float f[20];
 #pragma unroll
-  for (int k = 0; k < 9; k++) f[k] = 0;
-  int oi = S.aoff + S.nsol + 3 * iw;
-  if (active) {
-    int gw = S.woff + iw;
-    int n = P.ww_n[gw];
-    const int *nb = P.ww + (size_t)gw * P.ww_cap;
-    double3 xi[3] = {ld3(P.x, oi), ld3(P.x, oi + 1), ld3(P.x, oi + 2)};
-    const float qo = S.crg_ow, qh = S.crg_hw;
-    const float qoo = qo * qo, qoh = qo * qh, qhh = qh * qh;
-    for (int k = lane; k < n; k += 32) {
-      int oj = nb[k];
-      double3 xj[3] = {ld3(P.x, oj), ld3(P.x, oj + 1), ld3(P.x, oj + 2)};
-#pragma unroll
-      for (int a = 0; a < 3; a++)
-#pragma unroll
-        for (int b = 0; b < 3; b++) {
-          double dx = xj[b].x - xi[a].x, dy = xj[b].y - xi[a].y, dz = xj[b].z - xi[a].z;
-          double rinv = rsqrt(dx * dx + dy * dy + dz * dz);
-          double r2 = rinv * rinv;
-          float qq = (a == 0 && b == 0) ? qoo : ((a == 0 || b == 0) ? qoh : qhh);
-          double Vel = (double)qq * rinv, dv;
-          if (a == 0 && b == 0) {
-            double r6 = r2 * r2 * r2;
-            double Va = S.A_OO * r6 * r6, Vb = S.B_OO * r6;
-            vdw += Va - Vb;
-            dv = r2 * (-Vel - 12. * Va + 6. * Vb);
-          } else {
-            dv = r2 * (-Vel);
-          }
-          el += Vel;
-          f[3 * a + 0] -= dv * dx;
-          f[3 * a + 1] -= dv * dy;
-          f[3 * a + 2] -= dv * dz;
-        }
+    for (int k = 0; k < 9; k++) {
+      f[k] = (float)v[k];
+      f[9 + k] = (float)(v[k] - (double)f[k]);
     }
-  }
+    f[18] = f[19] = 0.f;
 #pragma unroll
-  for (int k = 0; k < 9; k++) f[k] = warp_sum(f[k]);
-  if (active && lane == 0) {
-    for (int a = 0; a < 3; a++) {
-      double4 dd = P.d[oi + a];
-      dd.x += f[3 * a]; dd.y += f[3 * a + 1]; dd.z += f[3 * a + 2];
-      P.d[oi + a] = dd;
-    }
+    for (int w = 0; w < WREC; w++) r[w] = make_float4(f[4 * w], f[4 * w + 1], f[4 * w + 2], f[4 * w + 3]);
+  } else {
+    double2 *rd = reinterpret_cast<double2 *>(r);
+    rd[0] = make_double2(a.x, a.y); rd[1] = make_double2(a.z, b.x); rd[2] = make_double2(b.y, b.z);
+    rd[3] = make_double2(c.x, c.y); rd[4] = make_double2(c.z, 0.0);
   }
-  warp_add(&P.E[s * QB_NE + QB_E_WW_EL], 0.5 * el);
-  warp_add(&P.E[s * QB_NE + QB_E_WW_VDW], 0.5 * vdw);
 }
 
-// Positions as an unevaluated float sum hi + lo (hi = float(x), lo = float(x - hi)),
-// refreshed before each mixed-precision force evaluation.  A float difference
-// (hj - hi) + (lj - li) then carries ~1e-7 relative error, like an FP64
-// difference rounded to FP32.
-__global__ void k_split_positions(DevPtrs P) {
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= P.natoms_tot) return;
-  double4 x = P.x[g];
-  float hx = (float)x.x, hy = (float)x.y, hz = (float)x.z;
-  P.xhi[g] = make_float4(hx, hy, hz, 0.f);
-  P.xlo[g] = make_float4((float)(x.x - (double)hx), (float)(x.y - (double)hy), (float)(x.z - (double)hz), 0.f);
+// One SPC/TIP3P molecule pair (md.f90:11823-11950, nonbond_ww_spc): the 9
+// Coulomb terms and the O-O Lennard-Jones term, gradient of molecule i added
+// to f[9].
+__device__ __forceinline__ void ww_pair_f64(const double *xi, const double *xj, double qoo, double qoh, double qhh,
+                                            double A, double B, double *f, double &el, double &vdw) {
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      double dx = xj[3 * b] - xi[3 * a], dy = xj[3 * b + 1] - xi[3 * a + 1], dz = xj[3 * b + 2] - xi[3 * a + 2];
+      double rinv = rsqrt(dx * dx + dy * dy + dz * dz);
+      double r2 = rinv * rinv;
+      double qq = (a == 0 && b == 0) ? qoo : ((a == 0 || b == 0) ? qoh : qhh);
+      double Vel = qq * rinv, dv;
+      if (a == 0 && b == 0) {
+        double r6 = r2 * r2 * r2;
+        double Va = A * r6 * r6, Vb = B * r6;
+        vdw += Va - Vb;
+        dv = r2 * (-Vel - 12. * Va + 6. * Vb);
+      } else {
+        dv = r2 * (-Vel);
+      }
+      el += Vel;
+      f[3 * a + 0] -= dv * dx;
+      f[3 * a + 1] -= dv * dy;
+      f[3 * a + 2] -= dv * dz;
+    }
 }
 
-// nonbond_ww_spc (md.f90:11823) in mixed precision: the pair terms in FP32
-// (rsqrtf on the MUFU pipe), each neighbour molecule's 9 energy terms summed
-// in FP32 and added to FP64 accumulators, gradient partials reduced in FP64.
-__global__ void __launch_bounds__(256, 3) k_nb_ww_mixed(DevPtrs P) {
+__device__ __forceinline__ void ww_pair_f32(const float *hi, const float *li, const float *hj, const float *lj,
+                                            float qoo, float qoh, float qhh, float A, float B, float *f,
+                                            float &el, float &vdw) {
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      float dx = (hj[3 * b] - hi[3 * a]) + (lj[3 * b] - li[3 * a]);
+      float dy = (hj[3 * b + 1] - hi[3 * a + 1]) + (lj[3 * b + 1] - li[3 * a + 1]);
+      float dz = (hj[3 * b + 2] - hi[3 * a + 2]) + (lj[3 * b + 2] - li[3 * a + 2]);
+      float rinv = rsqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+      float r2 = rinv * rinv;
+      float qq = (a == 0 && b == 0) ? qoo : ((a == 0 || b == 0) ? qoh : qhh);
+      float Vel = qq * rinv, dv;
+      if (a == 0 && b == 0) {
+        float r6 = r2 * r2 * r2;
+        float Va = A * r6 * r6, Vb = B * r6;
+        vdw += Va - Vb;
+        dv = r2 * (-Vel - 12.f * Va + 6.f * Vb);
+      } else {
+        dv = -r2 * Vel;
+      }
+      el += Vel;
+      f[3 * a + 0] = fmaf(-dv, dx, f[3 * a + 0]);
+      f[3 * a + 1] = fmaf(-dv, dy, f[3 * a + 1]);
+      f[3 * a + 2] = fmaf(-dv, dz, f[3 * a + 2]);
+    }
+}
+
+// nonbond_ww_spc (md.f90:11823) over the water-water list.  Block = 512
+// threads on WW_WPB consecutive waters of one system (blockIdx.y).  The
+// system's water records are staged in shared memory in chunks of ww_chunk
+// waters; for each chunk every half-warp takes one water i and its 16 lanes
+// walk i's list slice for that chunk, so neighbour records come from shared
+// memory.  Gradients of i are reduced over the half-warp and added once per
+// chunk; each unordered pair is evaluated from both sides, energies halved.
+// Mixed precision: pair terms in FP32 (rsqrtf), each neighbour molecule's
+// energy summed in FP32 and accumulated in FP64, gradients reduced in FP32.
+template <bool MIXED>
+__global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
+  extern __shared__ float4 wsm[];
   int s = blockIdx.y;
   const SysDev &S = P.sys[s];
-  int wpb = blockDim.x >> 5;
-  int iw = blockIdx.x * wpb + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  bool active = iw < S.nwat;
+  const int i0 = blockIdx.x * WW_WPB;
+  if (i0 >= S.nwat) return;
+  const int i1 = min(i0 + WW_WPB, S.nwat);
+  const int hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
+  const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
+  const float4 *rec = P.wrec + (size_t)S.woff * WREC;
+  const int W = P.ww_chunk;
+  const int nch = (S.nwat + W - 1) / W;
+  const float qo = S.crg_ow, qh = S.crg_hw;
   double el = 0, vdw = 0;
-  float f[9];
+  for (int c = 0; c < nch; c++) {
+    const int c0 = c * W, cn = min(W, S.nwat - c0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < cn * WREC; t += WW_BLOCK) wsm[t] = rec[(size_t)c0 * WREC + t];
+    __syncthreads();
+    for (int iw = i0 + hw; iw < i1; iw += WW_BLOCK / 16) {
+      const int gw = S.woff + iw;
+      const int *sp = P.ww_sp + (size_t)gw * P.ww_nch;
+      const int kb = c == 0 ? 0 : sp[c - 1], ke = sp[c];
+      if (kb >= ke) continue;
+      const uint16_t *nb = P.ww + (size_t)gw * P.ww_cap;
+      const float4 *ri = rec + (size_t)iw * WREC;
+      const int oi = S.aoff + S.nsol + 3 * iw;
+      double fd[9];
+      if (MIXED) {
+        float4 w0 = ri[0], w1 = ri[1], w2 = ri[2], w3 = ri[3], w4 = ri[4];
+        const float hi[9] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w, w2.x};
+        const float li[9] = {w2.y, w2.z, w2.w, w3.x, w3.y, w3.z, w3.w, w4.x, w4.y};
+        const float qoo = qo * qo, qoh = qo * qh, qhh = qh * qh;
+        const float A = (float)S.A_OO, B = (float)S.B_OO;
+        float f[9];
 #pragma unroll
-  for (int k = 0; k < 9; k++) f[k] = 0.f;
-  int oi = S.aoff + S.nsol + 3 * iw;
-  if (active) {
-    int gw = S.woff + iw;
-    int n = P.ww_n[gw];
-    const int *nb = P.ww + (size_t)gw * P.ww_cap;
-    float4 hi[3] = {P.xhi[oi], P.xhi[oi + 1], P.xhi[oi + 2]};
-    float4 li[3] = {P.xlo[oi], P.xlo[oi + 1], P.xlo[oi + 2]};
-    const float qo = S.crg_ow, qh = S.crg_hw;
-    const float qoo = qo * qo, qoh = qo * qh, qhh = qh * qh;
-    const float A = (float)S.A_OO, B = (float)S.B_OO;
-    for (int k = lane; k < n; k += 32) {
-      int oj = nb[k];
-      float4 hj[3] = {P.xhi[oj], P.xhi[oj + 1], P.xhi[oj + 2]};
-      float4 lj[3] = {P.xlo[oj], P.xlo[oj + 1], P.xlo[oj + 2]};
-      float e_el = 0.f, e_vdw = 0.f;
-#pragma unroll
-      for (int a = 0; a < 3; a++)
-#pragma unroll
-        for (int b = 0; b < 3; b++) {
-          float dx = (hj[b].x - hi[a].x) + (lj[b].x - li[a].x);
-          float dy = (hj[b].y - hi[a].y) + (lj[b].y - li[a].y);
-          float dz = (hj[b].z - hi[a].z) + (lj[b].z - li[a].z);
-          float rinv = rsqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
-          float r2 = rinv * rinv;
-          float qq = (a == 0 && b == 0) ? qoo : ((a == 0 || b == 0) ? qoh : qhh);
-          float Vel = qq * rinv, dv;
-          if (a == 0 && b == 0) {
-            float r6 = r2 * r2 * r2;
-            float Va = A * r6 * r6, Vb = B * r6;
-            e_vdw += Va - Vb;
-            dv = r2 * (-Vel - 12.f * Va + 6.f * Vb);
-          } else {
-            dv = -r2 * Vel;
-          }
-          e_el += Vel;
-          f[3 * a + 0] = fmaf(-dv, dx, f[3 * a + 0]);
-          f[3 * a + 1] = fmaf(-dv, dy, f[3 * a + 1]);
-          f[3 * a + 2] = fmaf(-dv, dz, f[3 * a + 2]);
+        for (int k = 0; k < 9; k++) f[k] = 0.f;
+        for (int k = kb + hl; k < ke; k += 16) {
+          const float4 *rj = wsm + (int)(nb[k] - c0) * WREC;
+          float4 v0 = rj[0], v1 = rj[1], v2 = rj[2], v3 = rj[3], v4 = rj[4];
+          const float hj[9] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w, v2.x};
+          const float lj[9] = {v2.y, v2.z, v2.w, v3.x, v3.y, v3.z, v3.w, v4.x, v4.y};
+          float e_el = 0.f, e_vdw = 0.f;
+          ww_pair_f32(hi, li, hj, lj, qoo, qoh, qhh, A, B, f, e_el, e_vdw);
+          el += (double)e_el;
+          vdw += (double)e_vdw;
         }
-      el += (double)e_el;
-      vdw += (double)e_vdw;
-    }
-  }
-  double fd[9];
 #pragma unroll
-  for (int k = 0; k < 9; k++) fd[k] = warp_sum((double)f[k]);
-  if (active && lane == 0) {
-    for (int a = 0; a < 3; a++) {
-      double4 dd = P.d[oi + a];
-      dd.x += fd[3 * a]; dd.y += fd[3 * a + 1]; dd.z += fd[3 * a + 2];
-      P.d[oi + a] = dd;
+        for (int k = 0; k < 9; k++) {
+          float t = f[k];
+#pragma unroll
+          for (int o = 8; o > 0; o >>= 1) t += __shfl_xor_sync(hmask, t, o);
+          fd[k] = (double)t;
+        }
+      } else {
+        const double2 *rd = reinterpret_cast<const double2 *>(ri);
+        double2 d0 = rd[0], d1 = rd[1], d2 = rd[2], d3 = rd[3], d4 = rd[4];
+        const double xi[9] = {d0.x, d0.y, d1.x, d1.y, d2.x, d2.y, d3.x, d3.y, d4.x};
+        const double qoo = (double)(qo * qo), qoh = (double)(qo * qh), qhh = (double)(qh * qh);
+#pragma unroll
+        for (int k = 0; k < 9; k++) fd[k] = 0.0;
+        for (int k = kb + hl; k < ke; k += 16) {
+          const double2 *rj = reinterpret_cast<const double2 *>(wsm + (int)(nb[k] - c0) * WREC);
+          double2 v0 = rj[0], v1 = rj[1], v2 = rj[2], v3 = rj[3], v4 = rj[4];
+          const double xj[9] = {v0.x, v0.y, v1.x, v1.y, v2.x, v2.y, v3.x, v3.y, v4.x};
+          ww_pair_f64(xi, xj, qoo, qoh, qhh, S.A_OO, S.B_OO, fd, el, vdw);
+        }
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+#pragma unroll
+          for (int o = 8; o > 0; o >>= 1) fd[k] += __shfl_xor_sync(hmask, fd[k], o);
+        }
+      }
+      if (hl == 0) {
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+          double4 dd = P.d[oi + a];
+          dd.x += fd[3 * a]; dd.y += fd[3 * a + 1]; dd.z += fd[3 * a + 2];
+          P.d[oi + a] = dd;
+        }
+      }
     }
   }
   warp_add(&P.E[s * QB_NE + QB_E_WW_EL], 0.5 * el);
@@ -824,6 +916,7 @@ __global__ void k_nb_qq(DevPtrs P) {
 __global__ void k_lrf_taylor(DevPtrs P) {
   int s = blockIdx.y;
   const SysDev &S = P.sys[s];
+  if (!S.use_lrf) return;
   double e = 0;
   for (int i0 = blockIdx.x * blockDim.x; i0 < S.natom; i0 += gridDim.x * blockDim.x) {
     int il = i0 + threadIdx.x;

@@ -113,10 +113,12 @@ def synthetic(tmp_path_factory):
     from q_b200 import synth
     root = tmp_path_factory.mktemp("synth")
     return {"c0": synth.water_sphere(str(root / "c0"), radius=15.0, seed=1234),
-            "c1": synth.fep_solute(str(root / "c1"), seed=1234)}
+            "c1": synth.fep_solute(str(root / "c1"), seed=1234),
+            # more waters than one shared-memory chunk of the water-water kernel
+            "c0_r25": synth.water_sphere(str(root / "c0_r25"), radius=25.0, seed=99)}
 
 
-@pytest.mark.parametrize("case", ["c0", "c1"])
+@pytest.mark.parametrize("case", ["c0", "c1", "c0_r25"])
 def test_synthetic_single_point(synthetic, oracle, case):
     """Benchmark-shaped systems: water sphere (LRF, restraints, watpol) and the
     8-Q-atom two-state soft-core FEP solute; energies and gradient."""
@@ -151,11 +153,11 @@ def test_synthetic_windows_trajectory(synthetic, oracle):
         assert np.max(np.abs(b.coords(k) - o.coords())) < 1e-4
 
 
-def test_mixed_precision_error_vs_fp64(synthetic):
+@pytest.mark.parametrize("case", ["c1", "c0_r25"])
+def test_mixed_precision_error_vs_fp64(synthetic, case):
     """The mixed-precision engine (FP32 water-water pair math, FP64 sums)
     against the FP64 engine on the same coordinates: the error it carries."""
-    from q_b200 import MIXED
-    sys_ = System.open(synthetic["c1"].inp)
+    sys_ = System.open(synthetic[case].inp)
     b64 = Batch([sys_], precision=FP64)
     b32 = Batch([sys_], precision=MIXED)
     b64.final_energy()
@@ -167,4 +169,20 @@ def test_mixed_precision_error_vs_fp64(synthetic):
     # carries a few 1e-3 kcal/mol; the stated budget of the mixed path is 0.05
     assert e["ww_el"] < 0.05 and e["ww_vdw"] < 0.05
     assert grad_err(b32.gradient(0), b64.gradient(0)) < G_TOL
-    assert np.max(np.abs(EQ32 - EQ64)) < 1e-6
+    assert np.max(np.abs(EQ32 - EQ64), initial=0.0) < 1e-6
+
+
+def test_mixed_sizes_in_one_batch(synthetic, oracle):
+    """Small and large spheres and the FEP system in one batch (one staging
+    chunk size for all): each system matches its own oracle run."""
+    names = ["c0", "c0_r25", "c1"]
+    systems = [System.open(synthetic[n].inp) for n in names]
+    b = Batch(systems, precision=FP64)
+    b.final_energy()
+    for k, s in enumerate(systems):
+        o = oracle.create(s)
+        o.final_energy()
+        Eg, EQg = b.energy_vectors(k)
+        Eo, EQo = o.energy_vectors()
+        assert_energies(Eg, EQg, Eo, EQo)
+        assert grad_err(b.gradient(k), o.gradient()) < G_TOL

@@ -346,7 +346,8 @@ def main():
                      "top_kernel": top[0], "top_kernel_share": top[1][0] / tot if tot else None},
         "kernels_ms_per_step": {k: v[0] / args.steps for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])[:8]},
         "workload_per_step": {"ww_molecule_pairs": ww_pairs, "pw_pairs": pw_pairs, "pp_pairs": pp_pairs,
-                              "qp_pairs_x_states": w[3], "qw_pairs_x_states": w[4]},
+                              "qp_pairs_x_states": w[3], "qw_pairs_x_states": w[4],
+                              "shake_iterations_mean": round(float(w[8]), 3), "shake_iterations_max": int(w[9])},
         "e2e": {"value": e2e, "unit": "ns/day", "h2d_bytes_per_step": h2d / args.steps,
                 "d2h_bytes_per_step": d2h / args.steps},
         "gpu_launches": launches,

@@ -150,7 +150,11 @@ int qb_batch_profile(qb_batch *b, char *names, size_t names_len, double *ms,
 /* Device work totals of the last qb_batch_run (for roofline arithmetic):
  * out[0] ww molecule pairs/step (sum over systems), out[1] pw pairs,
  * out[2] pp pairs, out[3] qp pairs, out[4] qw (q, water) pairs, out[5] atoms,
- * out[6] shake constraints, out[7] charge groups. */
+ * out[6] shake constraints, out[7] charge groups, out[8] SHAKE iterations per
+ * molecule and step on average (the niter shake() returns, md.f90:14560),
+ * out[9] most SHAKE iterations of one molecule in one step.  Fills up to n
+ * (at most QB_WORKLOAD_N) entries. */
+#define QB_WORKLOAD_N 10
 int qb_batch_workload(qb_batch *b, double *out, int n);
 
 void qb_batch_destroy(qb_batch *b);

@@ -174,8 +174,11 @@ class Batch:
         return {k: (float(ms[i]), int(launches[i])) for i, k in enumerate(keys)}
 
     def workload(self) -> np.ndarray:
-        out = np.zeros(8)
-        check(lib.qb_batch_workload(self._b, _dp(out), 8))
+        """Work totals of the last run: ww molecule pairs, pw, pp, qp, qw pairs,
+        atoms, SHAKE constraints, charge groups, mean SHAKE iterations per
+        molecule and step, most iterations of one molecule."""
+        out = np.zeros(10)
+        check(lib.qb_batch_workload(self._b, _dp(out), 10))
         return out
 
     def status(self, sys: int) -> int:

@@ -58,17 +58,18 @@ struct Batch {
   cudaStream_t stream = nullptr;
   int NB = 1;
   long long istep = 0;
-  int max_natom = 0, max_nwat = 0, max_ncgp = 0, max_ncgp_sol = 0, max_terms = 0, max_pp = 0, max_pw = 0, max_qp = 0;
+  int max_natom = 0, max_nwat = 0, max_ncgp = 0, max_ncgp_sol = 0, max_terms = 0, max_pp = 0, max_ncgp_sol_w = 0, max_qp = 0;
   bool any_lrf = false, any_q = false, any_shake = false, any_wpol = false, any_prestr = false, any_qq = false,
        any_qb = false;
   size_t watpol_smem = 0;
+  int q_states = 0;           // state count shared by every system with Q atoms (0: they differ)
   // profiling
   bool profiling = false;
   std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
   std::vector<cudaEvent_t> event_pool;
   std::map<std::string, KernelStat> stats;
   std::vector<std::string> order;
-  double workload[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double workload[QB_WORKLOAD_N] = {};
 
   ~Batch() {
     if (stream) cudaStreamSynchronize(stream);
@@ -131,7 +132,7 @@ struct Batch {
     launch("lists_begin", [&] { k_lists_begin<<<cdiv(nsys, 128), 128, 0, stream>>>(p, force); });
     if (max_ncgp_sol > 0) {
       launch("list_pp", [&] { k_list_pp<<<dim3(max_ncgp_sol, nsys), 128, 0, stream>>>(p, force); });
-      if (max_nwat > 0) launch("list_pw", [&] { k_list_pw<<<dim3(max_ncgp_sol, nsys), 256, 0, stream>>>(p, force); });
+      if (max_nwat > 0) launch("list_pw", [&] { k_list_pw<<<dim3(cdiv(max_ncgp_sol, 4), nsys), 128, 0, stream>>>(p, force); });
     }
     if (any_q) {
       launch("list_qp", [&] { k_list_qp<<<nsys, 256, 0, stream>>>(p, force); });
@@ -157,15 +158,24 @@ struct Batch {
     CUDA_TRY(cudaMemsetAsync(p.E, 0, sizeof(double) * QB_NE * (size_t)nsys, stream));
     CUDA_TRY(cudaMemsetAsync(p.EQ, 0, sizeof(double) * MAXS * QB_NEQ * (size_t)nsys, stream));
     if (max_pp > 0)
-      launch("nb_pp", [&] { k_nb_pair<true><<<dim3(std::min(cdiv(max_pp, 256), 64), nsys), 256, 0, stream>>>(p); });
-    if (max_pw > 0)
-      launch("nb_pw", [&] { k_nb_pair<false><<<dim3(std::min(cdiv(max_pw, 256), 128), nsys), 256, 0, stream>>>(p); });
+      launch("nb_pp", [&] { k_nb_pp<<<dim3(std::min(cdiv(max_pp, 256), 64), nsys), 256, 0, stream>>>(p); });
+    if (max_ncgp_sol_w > 0)
+      launch("nb_pw", [&] { k_nb_pw<<<dim3(max_ncgp_sol_w, nsys), PW_BLOCK, 0, stream>>>(p); });
     if (any_q && max_qp > 0)
-      launch("nb_qp", [&] { k_nb_qp<<<dim3(std::min(cdiv(max_qp, 256), 32), nsys), 256, 0, stream>>>(p); });
+      launch("nb_qp", [&] {
+        dim3 g(std::min(cdiv(max_qp, 256), 32), nsys);
+        switch (q_states) {
+          case 1: k_nb_qp<1><<<g, 256, 0, stream>>>(p); break;
+          case 2: k_nb_qp<2><<<g, 256, 0, stream>>>(p); break;
+          case 3: k_nb_qp<3><<<g, 256, 0, stream>>>(p); break;
+          case 4: k_nb_qp<4><<<g, 256, 0, stream>>>(p); break;
+          default: k_nb_qp<0><<<g, 256, 0, stream>>>(p);
+        }
+      });
     const bool mixed = opt.precision == QB_MIXED;
     if (max_nwat > 0) {
       dim3 gp(cdiv(max_nwat, 256), nsys), gw(cdiv(max_nwat, WW_WPB), nsys);
-      size_t smem = (size_t)p.ww_chunk * WREC * sizeof(float4);
+      size_t smem = (size_t)p.ww_chunk * (mixed ? WatRec<true>::words : WatRec<false>::words) * sizeof(float4);
       if (mixed) {
         launch("pack_waters", [&] { k_pack_waters<true><<<gp, 256, 0, stream>>>(p); });
         launch("nb_ww", [&] { k_nb_ww<true><<<gw, WW_BLOCK, smem, stream>>>(p); });
@@ -173,7 +183,16 @@ struct Batch {
         launch("pack_waters", [&] { k_pack_waters<false><<<gp, 256, 0, stream>>>(p); });
         launch("nb_ww", [&] { k_nb_ww<false><<<gw, WW_BLOCK, smem, stream>>>(p); });
       }
-      if (any_q) launch("nb_qw", [&] { k_nb_qw<<<dim3(cdiv(max_nwat, 128), nsys), 128, 0, stream>>>(p); });
+      if (any_q) launch("nb_qw", [&] {
+        dim3 g(cdiv(max_nwat, 128), nsys);
+        switch (q_states) {
+          case 1: k_nb_qw<1><<<g, 128, 0, stream>>>(p); break;
+          case 2: k_nb_qw<2><<<g, 128, 0, stream>>>(p); break;
+          case 3: k_nb_qw<3><<<g, 128, 0, stream>>>(p); break;
+          case 4: k_nb_qw<4><<<g, 128, 0, stream>>>(p); break;
+          default: k_nb_qw<0><<<g, 128, 0, stream>>>(p);
+        }
+      });
     }
     if (any_lrf)
       launch("lrf_taylor", [&] { k_lrf_taylor<<<dim3(cdiv(max_natom, 256), nsys), 256, 0, stream>>>(p); });
@@ -193,8 +212,10 @@ struct Batch {
     if (lists_due()) build_lists(0);
     pot_energy();
     launch("leapfrog", [&] { k_leapfrog<<<cdiv(p.natoms_tot, 256), 256, 0, stream>>>(p); });
-    if (any_shake && p.nshake_tot > 0)
-      launch("shake", [&] { k_shake<<<cdiv(p.nshake_tot, 128), 128, 0, stream>>>(p); });
+    if (any_shake && p.nsh3 > 0)
+      launch("shake", [&] { k_shake3<<<cdiv(p.nsh3, 128), 128, 0, stream>>>(p); });
+    if (any_shake && p.nshg > 0)
+      launch("shake_general", [&] { k_shake_general<<<p.nshg, SHG_BLOCK, p.shg_smem, stream>>>(p); });
     launch("finish", [&] { k_finish<<<nsys, 512, 0, stream>>>(p, 1); });
     check_launch("step kernels");
     istep++;
@@ -265,7 +286,8 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   std::vector<SysState> sst(n);
   B.sysh.resize(n);
   int ww_cap = 64;
-  long long pp_tot = 0, pw_tot = 0, qp_tot = 0, qw_tot = 0;
+  long long pp_tot = 0, qp_tot = 0, qw_tot = 0;
+  int ncgp_sol_tot = 0, pwg_cap = 32;
 
   for (int s = 0; s < n; s++) {
     const qb_sysview &V = B.views[s];
@@ -332,6 +354,11 @@ void build(Batch &B, qb_handle *const *hs, int n) {
       int o = V.nat_solute + 3 * iw;
       if (g >= V.ncgp || V.cgp_iswitch[g] != o || V.iwhich_cgp[o] != g)
         fail(QB_ERR_UNSUPPORTED, "water charge groups must follow the solute groups, one per water, switching on O");
+      // one water model: the solute-water kernel takes charges and types from the first water
+      const int o0 = V.nat_solute;
+      for (int k = 0; k < 3; k++)
+        if (V.crg[o + k] != V.crg[o0 + (k ? 1 : 0)] || V.iac[o + k] != V.iac[o0 + (k ? 1 : 0)])
+          fail(QB_ERR_UNSUPPORTED, "waters must share one charge and atom type per site (O, H, H)");
     }
     // Q atoms
     for (int q = 0; q < V.nqat; q++) {
@@ -482,7 +509,8 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     // list capacities from the starting coordinates, with margins for motion
     {
       const double *X = V.x0;
-      long long pp = 0, pw = 0;
+      long long pp = 0;
+      int pwmax = 0;
       double rpp = V.Rcpp + 3.0, rpw = V.Rcpw + 3.0, rww = V.Rcww + 2.0;
       for (int ig = 0; ig < V.ncgp_solute; ig++) {
         int si = V.cgp_iswitch[ig];
@@ -491,11 +519,14 @@ void build(Batch &B, qb_handle *const *hs, int n) {
           int sj = V.cgp_iswitch[jg];
           if (d2(X, si, sj) <= rpp * rpp) pp += (long long)na * (V.cgp_last[jg] - V.cgp_first[jg] + 1);
         }
+        int c = 0;
         for (int iw = 0; iw < V.nwat; iw++)
-          if (d2(X, si, V.nat_solute + 3 * iw) <= rpw * rpw) pw += 3LL * na;
+          if (d2(X, si, V.nat_solute + 3 * iw) <= rpw * rpw) c++;
+        pwmax = std::max(pwmax, c);
       }
       S.pp_cap = (int)(pp * 1.3 + 256);
-      S.pw_cap = (int)(pw * 1.3 + 256);
+      if (V.nwat > 0 && V.ncgp_solute > 0)
+        pwg_cap = std::max(pwg_cap, std::min(((int)(pwmax * 1.15) + 32 + 31) / 32 * 32, (V.nwat + 31) / 32 * 32));
       S.qp_cap = V.nqat * V.nat_solute + 16;
       S.qw_cap = V.nwat + 16;
       int mx = 0;
@@ -508,7 +539,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
       ww_cap = std::max(ww_cap, ((int)(mx * 1.15) + 31) / 32 * 32);
     }
     S.pp_off = (int)pp_tot; pp_tot += S.pp_cap;
-    S.pw_off = (int)pw_tot; pw_tot += S.pw_cap;
+    S.csoff = ncgp_sol_tot; ncgp_sol_tot += V.ncgp_solute;
     S.qp_off = (int)qp_tot; qp_tot += S.qp_cap;
     S.qw_off = (int)qw_tot; qw_tot += S.qw_cap;
     B.max_natom = std::max(B.max_natom, V.natom);
@@ -517,9 +548,10 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     B.max_ncgp = std::max(B.max_ncgp, V.ncgp);
     B.max_terms = std::max(B.max_terms, V.nbonds + V.nangles + V.ntors + V.nimps);
     B.max_pp = std::max(B.max_pp, S.pp_cap);
-    B.max_pw = V.nwat > 0 ? std::max(B.max_pw, S.pw_cap) : B.max_pw;
+    if (V.nwat > 0) B.max_ncgp_sol_w = std::max(B.max_ncgp_sol_w, V.ncgp_solute);
     B.max_qp = std::max(B.max_qp, S.qp_cap);
     B.any_lrf |= V.use_LRF != 0;
+    if (V.nqat > 0) B.q_states = (!B.any_q || B.q_states == V.nstates) ? V.nstates : 0;
     B.any_q |= V.nqat > 0;
     B.any_shake |= V.shake_constraints > 0;
     B.any_wpol |= S.wpol != 0;
@@ -564,25 +596,104 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   P.qiijkl = dev_upload(qiijkl, o); P.qi_on = dev_upload(qi_on, o); P.qipar = dev_upload(qipar, o);
   P.sh_first = dev_upload(sh_first, o); P.sh_n = dev_upload(sh_n, o); P.sh_sys = dev_upload(sh_sys, o);
   P.sh_ij = dev_upload(sh_ij, o); P.sh_d2 = dev_upload(sh_d2, o);
+  {
+    // rigid three-site molecules: relabel atoms so the constraints, in order,
+    // join (0,1), (0,2), (1,2)
+    std::vector<int4> at3; std::vector<double4> d3; std::vector<int> gen;
+    for (int m = 0; m < (int)sh_first.size(); m++) {
+      int f = sh_first[m];
+      bool tri = false;
+      if (sh_n[m] == 3) {
+        auto common = [](int2 a, int2 b) {
+          if (a.x == b.x || a.x == b.y) return a.x;
+          if (a.y == b.x || a.y == b.y) return a.y;
+          return -1;
+        };
+        int2 c0 = sh_ij[f], c1 = sh_ij[f + 1], c2 = sh_ij[f + 2];
+        int l0 = common(c0, c1), l1 = common(c0, c2), l2 = common(c1, c2);
+        auto joins = [](int2 c, int a, int b) { return (c.x == a && c.y == b) || (c.x == b && c.y == a); };
+        if (l0 >= 0 && l1 >= 0 && l2 >= 0 && l0 != l1 && l0 != l2 && l1 != l2 && joins(c0, l0, l1) &&
+            joins(c1, l0, l2) && joins(c2, l1, l2)) {
+          at3.push_back(make_int4(l0, l1, l2, sh_sys[m]));
+          d3.push_back(make_double4(sh_d2[f], sh_d2[f + 1], sh_d2[f + 2], 0.0));
+          tri = true;
+        }
+      }
+      if (!tri) gen.push_back(m);
+    }
+    P.nsh3 = (int)at3.size(); P.nshg = (int)gen.size();
+    P.sh3_at = dev_upload(at3, o); P.sh3_d2 = dev_upload(d3, o);
+    // other molecules: local atoms, constraints grouped into dependency levels
+    std::vector<int4> info, info2;
+    std::vector<int> gat, glev;
+    std::vector<int2> gc;
+    std::vector<double> gd2;
+    size_t smem_max = 0;
+    long long scratch = 0;
+    const size_t smem_cap = 200 * 1024;
+    for (int m : gen) {
+      int f = sh_first[m], n = sh_n[m];
+      std::map<int, int> loc;
+      std::vector<int> atoms;
+      for (int c = 0; c < n; c++)
+        for (int a : {sh_ij[f + c].x, sh_ij[f + c].y})
+          if (!loc.count(a)) { loc[a] = (int)atoms.size(); atoms.push_back(a); }
+      std::vector<int> last(atoms.size(), 0), level(n);
+      int nlev = 0;
+      for (int c = 0; c < n; c++) {
+        int i = loc[sh_ij[f + c].x], j = loc[sh_ij[f + c].y];
+        level[c] = std::max(last[i], last[j]) + 1;
+        last[i] = last[j] = level[c];
+        nlev = std::max(nlev, level[c]);
+      }
+      int4 in = make_int4((int)gat.size(), (int)atoms.size(), (int)gc.size(), n);
+      gat.insert(gat.end(), atoms.begin(), atoms.end());
+      int loff = (int)glev.size();
+      for (int L = 1; L <= nlev; L++) {
+        glev.push_back((int)gc.size() - in.z);
+        for (int c = 0; c < n; c++)
+          if (level[c] == L) {
+            gc.push_back(make_int2(loc[sh_ij[f + c].x], loc[sh_ij[f + c].y]));
+            gd2.push_back(sh_d2[f + c]);
+          }
+      }
+      glev.push_back((int)gc.size() - in.z);
+      size_t bytes = (size_t)(in.y + n) * sizeof(double4) + (size_t)n;
+      int soff = -1;
+      if (bytes <= smem_cap) smem_max = std::max(smem_max, bytes);
+      else { soff = (int)scratch; scratch += in.y + n + (n + 31) / 32; }
+      info.push_back(in);
+      info2.push_back(make_int4(loff, nlev, sh_sys[m], soff));
+    }
+    P.shg_info = dev_upload(info, o); P.shg_info2 = dev_upload(info2, o);
+    P.shg_at = dev_upload(gat, o); P.shg_c = dev_upload(gc, o); P.shg_d2 = dev_upload(gd2, o);
+    P.shg_lev = dev_upload(glev, o);
+    P.shg_scratch = dev_alloc<double4>((size_t)std::max<long long>(scratch, 1), o);
+    P.shg_smem = (smem_max + 15) / 16 * 16;
+    if (P.nshg > 0)
+      CUDA_TRY(cudaFuncSetAttribute(k_shake_general, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+  }
   P.rs = dev_upload(rs, o); P.rs_fk = dev_upload(rs_fk, o); P.rp = dev_upload(rp, o); P.rp_x = dev_upload(rp_x, o);
   P.rp_fk = dev_upload(rp_fk, o); P.rd = dev_upload(rd, o); P.rd_p = dev_upload(rd_p, o);
   P.ra = dev_upload(ra, o); P.ra_p = dev_upload(ra_p, o); P.rw = dev_upload(rw, o); P.rw_p = dev_upload(rw_p, o);
-  P.pp = dev_alloc<int4>(pp_tot, o); P.pw = dev_alloc<int4>(pw_tot, o);
+  P.pp = dev_alloc<int4>(pp_tot, o);
+  P.pwg_cap = pwg_cap;
+  P.pwg = dev_alloc<uint16_t>((size_t)std::max(ncgp_sol_tot, 1) * pwg_cap, o);
+  P.pwg_n = dev_alloc<int>(std::max(ncgp_sol_tot, 1), o);
   P.qp = dev_alloc<int4>(qp_tot, o); P.qw = dev_alloc<int>(qw_tot, o);
   // water-water staging chunk: a multiple of 32 waters, two blocks per SM
-  P.ww_chunk = std::min((B.max_nwat + 31) / 32 * 32, WW_CHUNK_MAX);
-  P.ww_chunk = std::max(P.ww_chunk, 32);
+  const int rec_words = B.opt.precision == QB_MIXED ? WatRec<true>::words : WatRec<false>::words;
+  const int chunk_max = WW_STAGE_BYTES / (16 * rec_words) / 32 * 32;
+  P.ww_chunk = std::max(std::min((B.max_nwat + 31) / 32 * 32, chunk_max), 32);
   P.ww_nch = (std::max(B.max_nwat, 1) + P.ww_chunk - 1) / P.ww_chunk;
   P.ww_cap = ww_cap;
   P.ww = dev_alloc<uint16_t>((size_t)std::max(woff, 1) * ww_cap, o);
   P.ww_n = dev_alloc<int>(std::max(woff, 1), o);
   P.ww_sp = dev_alloc<int>((size_t)std::max(woff, 1) * P.ww_nch, o);
-  P.wrec = dev_alloc<float4>((size_t)std::max(woff, 1) * WREC, o);
-  {
-    int smem = P.ww_chunk * WREC * (int)sizeof(float4);
-    CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  }
+  P.wrec = dev_alloc<float4>((size_t)std::max(woff, 1) * rec_words, o);
+  // the limit (not an allocation) covers every chunk size any batch may use
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
   P.E = dev_alloc<double>((size_t)n * QB_NE, o);
   P.EQ = dev_alloc<double>((size_t)n * MAXS * QB_NEQ, o);
   P.hist = nullptr;
@@ -590,7 +701,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   B.watpol_smem = (size_t)B.max_nwat * sizeof(double) + (size_t)MAX_SHELLS * B.max_nwat * sizeof(int);
   if (B.any_wpol) {
     if (B.watpol_smem > 200 * 1024) fail(QB_ERR_UNSUPPORTED, "too many waters for the polarisation kernel");
-    CUDA_TRY(cudaFuncSetAttribute(k_watpol, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B.watpol_smem));
+    CUDA_TRY(cudaFuncSetAttribute(k_watpol, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   }
 }
 
@@ -701,30 +812,50 @@ int qb_batch_create(qb_handle *const *systems, int n, const qb_options *opt, qb_
   return QB_OK;
 }
 
+namespace qb {
+namespace {
+
+void reset_counters(Batch &B) {
+  k_reset_counters<<<Batch::cdiv(B.nsys, 128), 128, 0, B.stream>>>(B.P);
+  B.check_launch("reset_counters");
+}
+
+// Work totals of the current lists and SHAKE statistics of the last run.
+void refresh_workload(Batch &B, int nsteps) {
+  std::vector<SysState> st(B.nsys);
+  CUDA_TRY(cudaMemcpy(st.data(), B.P.st, sizeof(SysState) * B.nsys, cudaMemcpyDeviceToHost));
+  std::vector<int> wwn(std::max(B.P.nwat_tot, 1));
+  CUDA_TRY(cudaMemcpy(wwn.data(), B.P.ww_n, sizeof(int) * wwn.size(), cudaMemcpyDeviceToHost));
+  double ww = 0;
+  for (int k = 0; k < B.P.nwat_tot; k++) ww += wwn[k];
+  double pw = 0, pp = 0, qp = 0, qw = 0, sh = 0, cg = B.P.ncgp_tot, its = 0, itmax = 0;
+  for (int s = 0; s < B.nsys; s++) {
+    pp += st[s].pp_n; pw += st[s].pw_n; qp += (double)st[s].qp_n * B.sysh[s].S;
+    qw += (double)st[s].qw_n * B.sysh[s].nq * B.sysh[s].S;
+    sh += B.views[s].shake_constraints;
+    its += (double)st[s].shake_its;
+    itmax = std::max(itmax, (double)st[s].shake_its_max);
+  }
+  double w[QB_WORKLOAD_N] = {ww / 2, pw, pp, qp, qw, (double)B.P.natoms_tot, sh, cg,
+                             B.P.nshake_tot > 0 && nsteps > 0 ? its / ((double)B.P.nshake_tot * nsteps) : 0.0,
+                             itmax};
+  std::memcpy(B.workload, w, sizeof w);
+}
+
+}  // namespace
+}  // namespace qb
+
 int qb_batch_run(qb_batch *bb, int nsteps) {
   if (!bb || nsteps < 0) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
   return guarded_batch([&] {
     Batch &B = bb->b;
     CUDA_TRY(cudaSetDevice(B.opt.device));
     qb::ensure_history(B, nsteps);
+    qb::reset_counters(B);
     for (int k = 0; k < nsteps; k++) B.step();
     if (B.profiling) B.collect();
     B.sync_status();
-    // workload of the current lists
-    std::vector<qb::SysState> st(B.nsys);
-    CUDA_TRY(cudaMemcpy(st.data(), B.P.st, sizeof(qb::SysState) * B.nsys, cudaMemcpyDeviceToHost));
-    std::vector<int> wwn(std::max(B.P.nwat_tot, 1));
-    CUDA_TRY(cudaMemcpy(wwn.data(), B.P.ww_n, sizeof(int) * wwn.size(), cudaMemcpyDeviceToHost));
-    double ww = 0;
-    for (int k = 0; k < B.P.nwat_tot; k++) ww += wwn[k];
-    double pw = 0, pp = 0, qp = 0, qw = 0, sh = 0, cg = B.P.ncgp_tot;
-    for (int s = 0; s < B.nsys; s++) {
-      pp += st[s].pp_n; pw += st[s].pw_n; qp += (double)st[s].qp_n * B.sysh[s].S;
-      qw += (double)st[s].qw_n * B.sysh[s].nq * B.sysh[s].S;
-      sh += B.views[s].shake_constraints;
-    }
-    double w[8] = {ww / 2, pw, pp, qp, qw, (double)B.P.natoms_tot, sh, cg};
-    std::memcpy(B.workload, w, sizeof w);
+    qb::refresh_workload(B, nsteps);
   });
 }
 
@@ -734,6 +865,7 @@ int qb_batch_run_timed(qb_batch *bb, int nsteps, double *device_ms, long long *k
     Batch &B = bb->b;
     CUDA_TRY(cudaSetDevice(B.opt.device));
     qb::ensure_history(B, nsteps);
+    qb::reset_counters(B);
     cudaEvent_t e0, e1;
     CUDA_TRY(cudaEventCreate(&e0));
     CUDA_TRY(cudaEventCreate(&e1));
@@ -751,6 +883,7 @@ int qb_batch_run_timed(qb_batch *bb, int nsteps, double *device_ms, long long *k
     if (kernel_launches) *kernel_launches = B.launches - l0;
     if (B.profiling) B.collect();
     B.sync_status();
+    qb::refresh_workload(B, nsteps);
   });
 }
 
@@ -908,7 +1041,7 @@ int qb_batch_profile(qb_batch *bb, char *names, size_t names_len, double *ms, lo
 
 int qb_batch_workload(qb_batch *bb, double *out, int n) {
   if (!bb || !out) return QB_ERR_ARG;
-  for (int k = 0; k < n && k < 8; k++) out[k] = bb->b.workload[k];
+  for (int k = 0; k < n && k < QB_WORKLOAD_N; k++) out[k] = bb->b.workload[k];
   return QB_OK;
 }
 

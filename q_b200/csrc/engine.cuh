@@ -30,7 +30,8 @@ struct SysDev {
   int sh_off, nsh;            // shake molecules
   int rs_off, nrs, rp_off, nrp, rd_off, nrd, ra_off, nra, rw_off, nrw;
   // dynamic list segments
-  int pp_off, pp_cap, pw_off, pw_cap, qp_off, qp_cap, qw_off, qw_cap;
+  int pp_off, pp_cap, qp_off, qp_cap, qw_off, qw_cap;
+  int csoff;                  // first solute group of this system among all systems' solute groups
   int ff_type, use_lrf, qvdw, wpol, nshell, iac_ow, separate_scaling, has_shake, detail_temps;
   int qp_once;                // lists with Q atoms are built once (Rcq > exclusion radius)
   int iout, iene, NB;
@@ -49,6 +50,8 @@ struct SysState {
   double Tscale_sol, Tscale_solv, Temp, Tfree, Tfree_sol, Tfree_solv, kinetic;
   float theta_corr[MAX_SHELLS], avtheta[MAX_SHELLS], avn_insh[MAX_SHELLS];
   int istep, status, pp_n, pw_n, qp_n, qw_n, lists_built, hist_n[2];
+  int shake_its_max;                 // most SHAKE iterations of one molecule since the counters were reset
+  unsigned long long shake_its;      // SHAKE iterations summed over molecules and steps
 };
 
 struct DevPtrs {
@@ -91,6 +94,17 @@ struct DevPtrs {
   int4 *qiijkl; uint8_t *qi_on; double2 *qipar;         // fk, imp0
   // shake
   int *sh_first, *sh_n, *sh_sys; int2 *sh_ij; double *sh_d2;
+  int4 *sh3_at; double4 *sh3_d2; int nsh3;   // three-atom, three-constraint molecules (relabelled), system in .w
+  // every other molecule (one block each): atoms, constraints in level order
+  int4 *shg_info;    // atom offset, atom count, constraint offset, constraint count
+  int4 *shg_info2;   // level offset, level count, system, global scratch offset (-1: shared memory)
+  int *shg_at;       // global atoms of each molecule
+  int2 *shg_c;       // constraints (local atom indices), level order
+  double *shg_d2;
+  int *shg_lev;      // level starts (level count + 1 per molecule)
+  double4 *shg_scratch;
+  int nshg;
+  size_t shg_smem;   // dynamic shared memory of the general SHAKE kernel
   // restraints (global atoms)
   int4 *rs; double *rs_fk;                 // i, j, ih, to_center
   int2 *rp; double *rp_x, *rp_fk;          // i, ipsi; x[3], fk[3]
@@ -98,7 +112,9 @@ struct DevPtrs {
   int4 *ra; double2 *ra_p;                 // i, j, k, ipsi; ang, fk
   int4 *rw; double4 *rw_p;                 // i, j, ih; d, fk, aMorse, dMorse
   // dynamic lists
-  int4 *pp, *pw;                           // i, j, lj
+  int4 *pp;                                // i, j, lj
+  uint16_t *pwg;                           // [solute group*pwg_cap + k] local water index
+  int *pwg_n, pwg_cap;                     // waters listed per solute group
   int4 *qp;                                // gq, j, lj, qlj
   int *qw;                                 // water O atoms
   uint16_t *ww;                            // [gw*ww_cap + k] local water index

@@ -314,35 +314,47 @@ __global__ void k_list_pp(DevPtrs P, int force) {
   }
 }
 
-// Solute-water pair list (nbpwlist, md.f90:6684): block (ig, system),
-// threads over waters.
+// Solute-water list (nbpwlist, md.f90:6684): per solute charge group, the
+// waters whose O lies within Rcpw of the group's switching atom (neither
+// excluded), as local water indices in ascending order.  The pairs are the
+// group's non-Q atoms with the three atoms of each listed water; pairs the
+// reference drops as all-zero (md.f90:5495) contribute exact zeros here.
+// One warp per solute group.
 __global__ void k_list_pw(DevPtrs P, int force) {
   int s = blockIdx.y;
   if (!list_due(P, s, force)) return;
   const SysDev &S = P.sys[s];
-  int ig = blockIdx.x;
+  int ig = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (ig >= S.ncgp_sol) return;
-  int gi = S.coff + ig;
+  int gi = S.coff + ig, sg = S.csoff + ig;
   int swi = P.cg_sw[gi];
-  if (P.flags[swi] & F_EXCL) return;
-  double3 xs = ld3(P.x, swi);
-  for (int iw = threadIdx.x; iw < S.nwat; iw += blockDim.x) {
-    int o = S.aoff + S.nsol + 3 * iw;
-    if (P.flags[o] & F_EXCL) continue;
-    double3 xo = ld3(P.x, o);
-    double dx = xs.x - xo.x, dy = xs.y - xo.y, dz = xs.z - xo.z;
-    if (dx * dx + dy * dy + dz * dz > S.Rcpw2) continue;
-    for (int ia = P.cg_first[gi]; ia <= P.cg_last[gi]; ia++) {
-      int i = P.cg_atoms[ia];
-      if (P.iq[i] >= 0) continue;
-      for (int j = o; j < o + 3; j++) {
-        int lj = ljcode(P, S, i, j);
-        if (zero_pair(P, i, j, lj)) continue;
-        int k = atomicAdd(&P.st[s].pw_n, 1);
-        if (k < S.pw_cap) P.pw[S.pw_off + k] = make_int4(i, j, lj, 0);
-        else set_status(&P.st[s], QB_ERR_LIST_OVERFLOW);
+  uint16_t *out = P.pwg + (size_t)sg * P.pwg_cap;
+  int cnt = 0;
+  if (!(P.flags[swi] & F_EXCL)) {
+    double3 xs = ld3(P.x, swi);
+    for (int base = 0; base < S.nwat; base += 32) {
+      int iw = base + lane;
+      int o = S.aoff + S.nsol + 3 * iw;
+      bool ok = false;
+      if (iw < S.nwat && !(P.flags[o] & F_EXCL)) {
+        double3 xo = ld3(P.x, o);
+        double dx = xs.x - xo.x, dy = xs.y - xo.y, dz = xs.z - xo.z;
+        ok = dx * dx + dy * dy + dz * dz <= S.Rcpw2;
       }
+      unsigned bal = __ballot_sync(FULL, ok);
+      if (ok) {
+        int pos = cnt + __popc(bal & ((1u << lane) - 1u));
+        if (pos < P.pwg_cap) out[pos] = (uint16_t)iw;
+      }
+      cnt += __popc(bal);
     }
+  }
+  if (lane == 0) {
+    if (cnt > P.pwg_cap) { set_status(&P.st[s], QB_ERR_LIST_OVERFLOW); cnt = P.pwg_cap; }
+    P.pwg_n[sg] = cnt;
+    int nat = 0;
+    for (int a = P.cg_first[gi]; a <= P.cg_last[gi]; a++) nat += P.iq[P.cg_atoms[a]] < 0;
+    if (cnt * nat) atomicAdd(&P.st[s].pw_n, 3 * cnt * nat);
   }
 }
 
@@ -427,6 +439,13 @@ __global__ void k_list_qw(DevPtrs P, int force) {
   if (threadIdx.x == 0) P.st[s].qw_n = base < S.qw_cap ? base : S.qw_cap;
 }
 
+// Per-run counters (SHAKE iterations) back to zero.
+__global__ void k_reset_counters(DevPtrs P) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= P.nsys) return;
+  P.st[s].shake_its = 0;
+  P.st[s].shake_its_max = 0;
+}
 __global__ void k_lists_begin(DevPtrs P, int force) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= P.nsys || !list_due(P, s, force)) return;
@@ -440,22 +459,25 @@ __global__ void k_lists_end(DevPtrs P, int force) {
   SysState &st = P.st[s];
   const SysDev &S = P.sys[s];
   if (st.pp_n > S.pp_cap) st.pp_n = S.pp_cap;
-  if (st.pw_n > S.pw_cap) st.pw_n = S.pw_cap;
   if (st.qp_n > S.qp_cap) st.qp_n = S.qp_cap;
   st.lists_built = 1;
 }
 
 // ------------------------------------------------------------- nonbonded
 
-// Per-water position records of the water-water kernel: 80 bytes (five
-// 16-byte words) per water, O,H1,H2 x,y,z.  Mixed precision: hi[9] then lo[9]
-// floats (hi = float(x), lo = float(x - hi)) and two pad floats, so a float
-// difference (hj - hi) + (lj - li) carries ~1e-7 relative error, like an FP64
-// difference rounded to FP32.  FP64: x[9] doubles and one pad double.  The
-// 80-byte stride puts 8 consecutive waters on 8 distinct 16-byte bank groups.
-constexpr int WREC = 5;
+// Per-water position records of the water-water kernel, 16-byte words.
+// FP64 (5 words, 80 bytes): O,H1,H2 x,y,z as doubles and one pad double.
+// Mixed (3 words, 48 bytes): the O position as an unevaluated float sum
+// hi + lo (hi = float(x), lo = float(x - hi)) and the two H positions relative
+// to their O, rounded to float: {hO.xyz, lO.x}, {lO.yz, rH1.xy},
+// {rH1.z, rH2.xyz}.  An atom-pair vector is then
+// ((hOj - hOi) + (lOj - lOi)) + rHj - rHi, which carries ~1e-7 relative error
+// like an FP64 difference rounded to FP32.  Both strides (3 and 5 words) put
+// 8 consecutive waters on 8 distinct 16-byte bank groups.
+template <bool MIXED> struct WatRec { static constexpr int words = MIXED ? 3 : 5; };
+constexpr int WREC_MAX = 5;
 constexpr int WW_BLOCK = 512, WW_WPB = 128;   // threads, waters per block
-constexpr int WW_CHUNK_MAX = 1280;            // 100 KB of records: two blocks per SM
+constexpr int WW_STAGE_BYTES = 112 * 1024;    // staged records per block: two blocks per SM
 
 template <bool MIXED>
 __global__ void k_pack_waters(DevPtrs P) {
@@ -465,18 +487,14 @@ __global__ void k_pack_waters(DevPtrs P) {
   if (iw >= S.nwat) return;
   int o = S.aoff + S.nsol + 3 * iw;
   double4 a = P.x[o], b = P.x[o + 1], c = P.x[o + 2];
-  float4 *r = P.wrec + (size_t)(S.woff + iw) * WREC;
+  constexpr int W = WatRec<MIXED>::words;
+  float4 *r = P.wrec + (size_t)(S.woff + iw) * W;
   if (MIXED) {
-    const double v[9] = {a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z};
-    float f[20];
-#pragma unroll
-    for (int k = 0; k < 9; k++) {
-      f[k] = (float)v[k];
-      f[9 + k] = (float)(v[k] - (double)f[k]);
-    }
-    f[18] = f[19] = 0.f;
-#pragma unroll
-    for (int w = 0; w < WREC; w++) r[w] = make_float4(f[4 * w], f[4 * w + 1], f[4 * w + 2], f[4 * w + 3]);
+    float hx = (float)a.x, hy = (float)a.y, hz = (float)a.z;
+    float lx = (float)(a.x - (double)hx), ly = (float)(a.y - (double)hy), lz = (float)(a.z - (double)hz);
+    r[0] = make_float4(hx, hy, hz, lx);
+    r[1] = make_float4(ly, lz, (float)(b.x - a.x), (float)(b.y - a.y));
+    r[2] = make_float4((float)(b.z - a.z), (float)(c.x - a.x), (float)(c.y - a.y), (float)(c.z - a.z));
   } else {
     double2 *rd = reinterpret_cast<double2 *>(r);
     rd[0] = make_double2(a.x, a.y); rd[1] = make_double2(a.z, b.x); rd[2] = make_double2(b.y, b.z);
@@ -513,17 +531,27 @@ __device__ __forceinline__ void ww_pair_f64(const double *xi, const double *xj, 
     }
 }
 
-__device__ __forceinline__ void ww_pair_f32(const float *hi, const float *li, const float *hj, const float *lj,
-                                            float qoo, float qoh, float qhh, float A, float B, float *f,
-                                            float &el, float &vdw) {
+// Mixed precision: i = {hO[3], lO[3], rH1[3], rH2[3]}, j likewise.
+__device__ __forceinline__ void ww_pair_f32(const float *i, const float *j, float qoo, float qoh, float qhh,
+                                            float A, float B, float *f, float &el, float &vdw) {
+  float dOO[3], t[2][3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    dOO[c] = (j[c] - i[c]) + (j[3 + c] - i[3 + c]);
+    t[0][c] = dOO[c] + j[6 + c];
+    t[1][c] = dOO[c] + j[9 + c];
+  }
 #pragma unroll
   for (int a = 0; a < 3; a++)
 #pragma unroll
     for (int b = 0; b < 3; b++) {
-      float dx = (hj[3 * b] - hi[3 * a]) + (lj[3 * b] - li[3 * a]);
-      float dy = (hj[3 * b + 1] - hi[3 * a + 1]) + (lj[3 * b + 1] - li[3 * a + 1]);
-      float dz = (hj[3 * b + 2] - hi[3 * a + 2]) + (lj[3 * b + 2] - li[3 * a + 2]);
-      float rinv = rsqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+      float d[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        float v = b == 0 ? dOO[c] : t[b - 1][c];
+        d[c] = a == 0 ? v : v - i[3 + 3 * a + c];
+      }
+      float rinv = rsqrtf(fmaf(d[0], d[0], fmaf(d[1], d[1], d[2] * d[2])));
       float r2 = rinv * rinv;
       float qq = (a == 0 && b == 0) ? qoo : ((a == 0 || b == 0) ? qoh : qhh);
       float Vel = qq * rinv, dv;
@@ -536,24 +564,31 @@ __device__ __forceinline__ void ww_pair_f32(const float *hi, const float *li, co
         dv = -r2 * Vel;
       }
       el += Vel;
-      f[3 * a + 0] = fmaf(-dv, dx, f[3 * a + 0]);
-      f[3 * a + 1] = fmaf(-dv, dy, f[3 * a + 1]);
-      f[3 * a + 2] = fmaf(-dv, dz, f[3 * a + 2]);
+#pragma unroll
+      for (int c = 0; c < 3; c++) f[3 * a + c] = fmaf(-dv, d[c], f[3 * a + c]);
     }
+}
+
+__device__ __forceinline__ void unpack_mixed(const float4 *r, float *v) {
+  float4 w0 = r[0], w1 = r[1], w2 = r[2];
+  v[0] = w0.x; v[1] = w0.y; v[2] = w0.z; v[3] = w0.w; v[4] = w1.x; v[5] = w1.y;
+  v[6] = w1.z; v[7] = w1.w; v[8] = w2.x; v[9] = w2.y; v[10] = w2.z; v[11] = w2.w;
 }
 
 // nonbond_ww_spc (md.f90:11823) over the water-water list.  Block = 512
 // threads on WW_WPB consecutive waters of one system (blockIdx.y).  The
 // system's water records are staged in shared memory in chunks of ww_chunk
 // waters; for each chunk every half-warp takes one water i and its 16 lanes
-// walk i's list slice for that chunk, so neighbour records come from shared
-// memory.  Gradients of i are reduced over the half-warp and added once per
-// chunk; each unordered pair is evaluated from both sides, energies halved.
-// Mixed precision: pair terms in FP32 (rsqrtf), each neighbour molecule's
-// energy summed in FP32 and accumulated in FP64, gradients reduced in FP32.
+// walk i's list slice for that chunk (the next entry prefetched), so
+// neighbour records come from shared memory.  Gradients of i are reduced over
+// the half-warp and added once per chunk; each unordered pair is evaluated
+// from both sides, energies halved.  Mixed precision: pair terms in FP32
+// (rsqrtf), each neighbour molecule's energy summed in FP32 and accumulated in
+// FP64, gradients reduced in FP32.
 template <bool MIXED>
 __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
   extern __shared__ float4 wsm[];
+  constexpr int W = WatRec<MIXED>::words;
   int s = blockIdx.y;
   const SysDev &S = P.sys[s];
   const int i0 = blockIdx.x * WW_WPB;
@@ -561,15 +596,15 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
   const int i1 = min(i0 + WW_WPB, S.nwat);
   const int hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
   const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
-  const float4 *rec = P.wrec + (size_t)S.woff * WREC;
-  const int W = P.ww_chunk;
-  const int nch = (S.nwat + W - 1) / W;
+  const float4 *rec = P.wrec + (size_t)S.woff * W;
+  const int CW = P.ww_chunk;
+  const int nch = (S.nwat + CW - 1) / CW;
   const float qo = S.crg_ow, qh = S.crg_hw;
   double el = 0, vdw = 0;
   for (int c = 0; c < nch; c++) {
-    const int c0 = c * W, cn = min(W, S.nwat - c0);
+    const int c0 = c * CW, cn = min(CW, S.nwat - c0);
     __syncthreads();
-    for (int t = threadIdx.x; t < cn * WREC; t += WW_BLOCK) wsm[t] = rec[(size_t)c0 * WREC + t];
+    for (int t = threadIdx.x; t < cn * W; t += WW_BLOCK) wsm[t] = rec[(size_t)c0 * W + t];
     __syncthreads();
     for (int iw = i0 + hw; iw < i1; iw += WW_BLOCK / 16) {
       const int gw = S.woff + iw;
@@ -577,34 +612,35 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
       const int kb = c == 0 ? 0 : sp[c - 1], ke = sp[c];
       if (kb >= ke) continue;
       const uint16_t *nb = P.ww + (size_t)gw * P.ww_cap;
-      const float4 *ri = rec + (size_t)iw * WREC;
+      const float4 *ri = rec + (size_t)iw * W;
       const int oi = S.aoff + S.nsol + 3 * iw;
       double fd[9];
+      int k = kb + hl;
+      int jn = k < ke ? (int)nb[k] : c0;
       if (MIXED) {
-        float4 w0 = ri[0], w1 = ri[1], w2 = ri[2], w3 = ri[3], w4 = ri[4];
-        const float hi[9] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w, w2.x};
-        const float li[9] = {w2.y, w2.z, w2.w, w3.x, w3.y, w3.z, w3.w, w4.x, w4.y};
+        float xi[12];
+        unpack_mixed(ri, xi);
         const float qoo = qo * qo, qoh = qo * qh, qhh = qh * qh;
         const float A = (float)S.A_OO, B = (float)S.B_OO;
         float f[9];
 #pragma unroll
-        for (int k = 0; k < 9; k++) f[k] = 0.f;
-        for (int k = kb + hl; k < ke; k += 16) {
-          const float4 *rj = wsm + (int)(nb[k] - c0) * WREC;
-          float4 v0 = rj[0], v1 = rj[1], v2 = rj[2], v3 = rj[3], v4 = rj[4];
-          const float hj[9] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w, v2.x};
-          const float lj[9] = {v2.y, v2.z, v2.w, v3.x, v3.y, v3.z, v3.w, v4.x, v4.y};
+        for (int q = 0; q < 9; q++) f[q] = 0.f;
+        for (; k < ke; k += 16) {
+          const int j = jn;
+          if (k + 16 < ke) jn = nb[k + 16];
+          float xj[12];
+          unpack_mixed(wsm + (j - c0) * W, xj);
           float e_el = 0.f, e_vdw = 0.f;
-          ww_pair_f32(hi, li, hj, lj, qoo, qoh, qhh, A, B, f, e_el, e_vdw);
+          ww_pair_f32(xi, xj, qoo, qoh, qhh, A, B, f, e_el, e_vdw);
           el += (double)e_el;
           vdw += (double)e_vdw;
         }
 #pragma unroll
-        for (int k = 0; k < 9; k++) {
-          float t = f[k];
+        for (int q = 0; q < 9; q++) {
+          float t = f[q];
 #pragma unroll
           for (int o = 8; o > 0; o >>= 1) t += __shfl_xor_sync(hmask, t, o);
-          fd[k] = (double)t;
+          fd[q] = (double)t;
         }
       } else {
         const double2 *rd = reinterpret_cast<const double2 *>(ri);
@@ -612,17 +648,19 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
         const double xi[9] = {d0.x, d0.y, d1.x, d1.y, d2.x, d2.y, d3.x, d3.y, d4.x};
         const double qoo = (double)(qo * qo), qoh = (double)(qo * qh), qhh = (double)(qh * qh);
 #pragma unroll
-        for (int k = 0; k < 9; k++) fd[k] = 0.0;
-        for (int k = kb + hl; k < ke; k += 16) {
-          const double2 *rj = reinterpret_cast<const double2 *>(wsm + (int)(nb[k] - c0) * WREC);
+        for (int q = 0; q < 9; q++) fd[q] = 0.0;
+        for (; k < ke; k += 16) {
+          const int j = jn;
+          if (k + 16 < ke) jn = nb[k + 16];
+          const double2 *rj = reinterpret_cast<const double2 *>(wsm + (j - c0) * W);
           double2 v0 = rj[0], v1 = rj[1], v2 = rj[2], v3 = rj[3], v4 = rj[4];
           const double xj[9] = {v0.x, v0.y, v1.x, v1.y, v2.x, v2.y, v3.x, v3.y, v4.x};
           ww_pair_f64(xi, xj, qoo, qoh, qhh, S.A_OO, S.B_OO, fd, el, vdw);
         }
 #pragma unroll
-        for (int k = 0; k < 9; k++) {
+        for (int q = 0; q < 9; q++) {
 #pragma unroll
-          for (int o = 8; o > 0; o >>= 1) fd[k] += __shfl_xor_sync(hmask, fd[k], o);
+          for (int o = 8; o > 0; o >>= 1) fd[q] += __shfl_xor_sync(hmask, fd[q], o);
         }
       }
       if (hl == 0) {
@@ -639,13 +677,12 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
   warp_add(&P.E[s * QB_NE + QB_E_WW_VDW], 0.5 * vdw);
 }
 
-// nonbond_pp (md.f90:10387) and nonbond_pw (10631): one thread per pair.
-template <bool PP>
-__global__ void k_nb_pair(DevPtrs P) {
+// nonbond_pp (md.f90:10387): one thread per pair.
+__global__ void k_nb_pp(DevPtrs P) {
   int s = blockIdx.y;
   const SysDev &S = P.sys[s];
-  int n = PP ? P.st[s].pp_n : P.st[s].pw_n;
-  const int4 *L = PP ? P.pp + S.pp_off : P.pw + S.pw_off;
+  int n = P.st[s].pp_n;
+  const int4 *L = P.pp + S.pp_off;
   double el = 0, vdw = 0;
   for (int k0 = blockIdx.x * blockDim.x; k0 < n; k0 += gridDim.x * blockDim.x) {
     int k = k0 + threadIdx.x;
@@ -658,7 +695,7 @@ __global__ void k_nb_pair(DevPtrs P) {
       double r2 = r * r, r6 = r2 * r2 * r2;
       float qq = P.crg[i] * P.crg[j];
       double Vel = (double)qq * r;
-      if (PP && lj == 3) Vel = Vel * S.el14;
+      if (lj == 3) Vel = Vel * S.el14;
       double Va = r6 * r6 * P.lja[3 * i + lj - 1] * P.lja[3 * j + lj - 1];
       double Vb = r6 * P.ljb[3 * i + lj - 1] * P.ljb[3 * j + lj - 1];
       double dv = r2 * (-Vel - 12. * Va + 6. * Vb);
@@ -668,20 +705,123 @@ __global__ void k_nb_pair(DevPtrs P) {
       vdw += Va - Vb;
     }
   }
-  warp_add(&P.E[s * QB_NE + (PP ? QB_E_PP_EL : QB_E_PW_EL)], el);
-  warp_add(&P.E[s * QB_NE + (PP ? QB_E_PP_VDW : QB_E_PW_VDW)], vdw);
+  warp_add(&P.E[s * QB_NE + QB_E_PP_EL], el);
+  warp_add(&P.E[s * QB_NE + QB_E_PP_VDW], vdw);
+}
+
+// nonbond_pw (md.f90:10631) over the group list: block per solute charge
+// group (blockIdx.x) of system blockIdx.y, one thread per listed water.  The
+// group's non-Q atoms are staged in shared memory with their charge products
+// (single precision, as crg(i)*crg(j)) and LJ products for the water O and H
+// types.  Each thread keeps its water's 9 gradient components in registers
+// and adds them with atomics once; the solute atoms' gradients are reduced
+// per warp into shared memory and written once by the block, which owns them.
+constexpr int PW_BLOCK = 128, PW_MAXA = 32;
+
+__global__ void __launch_bounds__(PW_BLOCK) k_nb_pw(DevPtrs P) {
+  int s = blockIdx.y;
+  const SysDev &S = P.sys[s];
+  int ig = blockIdx.x;
+  if (ig >= S.ncgp_sol) return;
+  int gi = S.coff + ig, sg = S.csoff + ig;
+  const int n = P.pwg_n[sg];
+  if (n == 0) return;
+  __shared__ int s_i[PW_MAXA];
+  __shared__ double4 s_x[PW_MAXA];
+  __shared__ double4 s_lj[PW_MAXA];     // A(i,O), B(i,O), A(i,H), B(i,H)
+  __shared__ float2 s_q[PW_MAXA];       // crg(i)*crg(O), crg(i)*crg(H)
+  __shared__ double s_f[PW_MAXA][3];
+  __shared__ int s_na;
+  const uint16_t *L = P.pwg + (size_t)sg * P.pwg_cap;
+  const int ow = S.aoff + S.nsol;       // first water O: charges and types of every water site
+  const int lane = threadIdx.x & 31;
+  double el = 0, vdw = 0;
+  const int f = P.cg_first[gi], l = P.cg_last[gi];
+  for (int a0 = f; a0 <= l; a0 += PW_MAXA) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int na = 0;
+      for (int a = a0; a <= l && a < a0 + PW_MAXA; a++) {
+        int i = P.cg_atoms[a];
+        if (P.iq[i] < 0) s_i[na++] = i;
+      }
+      s_na = na;
+    }
+    __syncthreads();
+    const int na = s_na;
+    for (int t = threadIdx.x; t < na; t += PW_BLOCK) {
+      int i = s_i[t];
+      s_x[t] = P.x[i];
+      int ljo = ljcode(P, S, i, ow), ljh = ljcode(P, S, i, ow + 1);
+      s_lj[t] = make_double4(P.lja[3 * i + ljo - 1] * P.lja[3 * ow + ljo - 1],
+                             P.ljb[3 * i + ljo - 1] * P.ljb[3 * ow + ljo - 1],
+                             P.lja[3 * i + ljh - 1] * P.lja[3 * (ow + 1) + ljh - 1],
+                             P.ljb[3 * i + ljh - 1] * P.ljb[3 * (ow + 1) + ljh - 1]);
+      s_q[t] = make_float2(P.crg[i] * P.crg[ow], P.crg[i] * P.crg[ow + 1]);
+      s_f[t][0] = s_f[t][1] = s_f[t][2] = 0.0;
+    }
+    __syncthreads();
+    for (int k0 = 0; k0 < n; k0 += PW_BLOCK) {
+      if (k0 + (threadIdx.x & ~31) >= n) break;        // whole warp past the list
+      const int k = k0 + threadIdx.x;
+      const bool act = k < n;
+      const int o = ow + 3 * (act ? (int)L[k] : 0);
+      double3 xw[3] = {ld3(P.x, o), ld3(P.x, o + 1), ld3(P.x, o + 2)};
+      double fw[9];
+#pragma unroll
+      for (int c = 0; c < 9; c++) fw[c] = 0.0;
+      for (int t = 0; t < na; t++) {
+        const double4 xi = s_x[t], lj = s_lj[t];
+        const float2 q = s_q[t];
+        double fi[3] = {0.0, 0.0, 0.0};
+        if (act) {
+#pragma unroll
+          for (int b = 0; b < 3; b++) {
+            double dx = xw[b].x - xi.x, dy = xw[b].y - xi.y, dz = xw[b].z - xi.z;
+            double r = rsqrt(dx * dx + dy * dy + dz * dz);
+            double r2 = r * r, r6 = r2 * r2 * r2;
+            double Vel = (double)(b == 0 ? q.x : q.y) * r;
+            double Va = (b == 0 ? lj.x : lj.z) * r6 * r6, Vb = (b == 0 ? lj.y : lj.w) * r6;
+            double dv = r2 * (-Vel - 12. * Va + 6. * Vb);
+            fi[0] -= dv * dx; fi[1] -= dv * dy; fi[2] -= dv * dz;
+            fw[3 * b] += dv * dx; fw[3 * b + 1] += dv * dy; fw[3 * b + 2] += dv * dz;
+            el += Vel;
+            vdw += Va - Vb;
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          double v = warp_sum(fi[c]);
+          if (lane == 0) atomicAdd(&s_f[t][c], v);
+        }
+      }
+      if (act)
+        for (int b = 0; b < 3; b++) atomic_add3(P.d, o + b, fw[3 * b], fw[3 * b + 1], fw[3 * b + 2]);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < na; t += PW_BLOCK) {
+      double4 dd = P.d[s_i[t]];
+      dd.x += s_f[t][0]; dd.y += s_f[t][1]; dd.z += s_f[t][2];
+      P.d[s_i[t]] = dd;
+    }
+  }
+  warp_add(&P.E[s * QB_NE + QB_E_PW_EL], el);
+  warp_add(&P.E[s * QB_NE + QB_E_PW_VDW], vdw);
 }
 
 // nonbond_qp (md.f90:10980) / nonbond_qp_qvdw (11138): one thread per pair,
 // all states in the thread.
+template <int NSC>
 __global__ void k_nb_qp(DevPtrs P) {
   int s = blockIdx.y;
   const SysDev &S = P.sys[s];
   int n = P.st[s].qp_n;
-  const int NS = S.S;
+  const int NS = NSC > 0 ? NSC : S.S;
   const int ncol = S.natyps + S.nq;
-  double el[MAXS], vdw[MAXS];
-  for (int st = 0; st < MAXS; st++) { el[st] = 0; vdw[st] = 0; }
+  constexpr int NA = NSC > 0 ? NSC : MAXS;
+  double el[NA], vdw[NA];
+#pragma unroll
+  for (int st = 0; st < NA; st++) { el[st] = 0; vdw[st] = 0; }
   for (int k0 = blockIdx.x * blockDim.x; k0 < n; k0 += gridDim.x * blockDim.x) {
     int k = k0 + threadIdx.x;
     if (k < n) {
@@ -738,6 +878,7 @@ __global__ void k_nb_qp(DevPtrs P) {
 
 // nonbond_qw_spc (md.f90:11302): one thread per water of the Q-water list,
 // looping over Q atoms; Q-atom gradients are reduced in shared memory.
+template <int NSC>
 __global__ void k_nb_qw(DevPtrs P) {
   int s = blockIdx.y;
   const SysDev &S = P.sys[s];
@@ -747,9 +888,11 @@ __global__ void k_nb_qw(DevPtrs P) {
   for (int t = threadIdx.x; t < NQ_SHARED * 3; t += blockDim.x) fq[t] = 0;
   __syncthreads();
   int n = P.st[s].qw_n;
-  const int NS = S.S, ncol = S.natyps + S.nq;
-  double el[MAXS], vdw[MAXS];
-  for (int st = 0; st < MAXS; st++) { el[st] = 0; vdw[st] = 0; }
+  const int NS = NSC > 0 ? NSC : S.S, ncol = S.natyps + S.nq;
+  constexpr int NA = NSC > 0 ? NSC : MAXS;
+  double el[NA], vdw[NA];
+#pragma unroll
+  for (int st = 0; st < NA; st++) { el[st] = 0; vdw[st] = 0; }
   for (int k0 = blockIdx.x * blockDim.x; k0 < n; k0 += gridDim.x * blockDim.x) {
     int k = k0 + threadIdx.x;
     bool act = k < n;
@@ -1544,111 +1687,151 @@ __global__ void k_leapfrog(DevPtrs P) {
   P.v[g] = v;
 }
 
-// shake (md.f90:14445): Gauss-Seidel iterations over one molecule's
-// constraints per thread, to relative tolerance 1e-4, at most 1000 passes.
-__device__ __forceinline__ double3 pick3(int k, double3 a, double3 b, double3 c) {
-  return k == 0 ? a : (k == 1 ? b : c);
-}
-__device__ __forceinline__ void put3(int k, double3 v, double3 &a, double3 &b, double3 &c) {
-  if (k == 0) a = v;
-  else if (k == 1) b = v;
-  else c = v;
-}
 
-// The same Gauss-Seidel iteration for a molecule of three consecutive atoms
-// with three constraints (rigid water), with its state held in registers.
-__device__ bool shake3(DevPtrs &P, int base, const int2 *ij, const double *d2) {
-  double3 p0 = ld3(P.x, base), p1 = ld3(P.x, base + 1), p2 = ld3(P.x, base + 2);
-  double3 r0 = ld3(P.xx, base), r1 = ld3(P.xx, base + 1), r2 = ld3(P.xx, base + 2);
-  float w0 = P.winv[base], w1 = P.winv[base + 1], w2 = P.winv[base + 2];
-  int ca[3], cb[3];
-  double dd[3];
-#pragma unroll
-  for (int c = 0; c < 3; c++) { ca[c] = ij[c].x - base; cb[c] = ij[c].y - base; dd[c] = d2[c]; }
-  bool ready[3] = {false, false, false};
-  int nits = 0;
-  for (;;) {
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      if (ready[c]) continue;
-      double3 xi = pick3(ca[c], p0, p1, p2), xj = pick3(cb[c], p0, p1, p2);
-      double3 ri = pick3(ca[c], r0, r1, r2), rj = pick3(cb[c], r0, r1, r2);
-      float wi = ca[c] == 0 ? w0 : (ca[c] == 1 ? w1 : w2);
-      float wj = cb[c] == 0 ? w0 : (cb[c] == 1 ? w1 : w2);
-      double xij[3] = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
-      double xij2 = xij[0] * xij[0] + xij[1] * xij[1] + xij[2] * xij[2];
-      double diff = dd[c] - xij2;
-      if (fabs(diff) < 0.0001 * dd[c]) ready[c] = true;
-      double xxij[3] = {ri.x - rj.x, ri.y - rj.y, ri.z - rj.z};
-      double scp = xij[0] * xxij[0] + xij[1] * xxij[1] + xij[2] * xxij[2];
-      float wsum = wi + wj;
-      double corr = diff / (2. * scp * (double)wsum);
-      xi.x += xxij[0] * corr * (double)wi; xi.y += xxij[1] * corr * (double)wi; xi.z += xxij[2] * corr * (double)wi;
-      xj.x -= xxij[0] * corr * (double)wj; xj.y -= xxij[1] * corr * (double)wj; xj.z -= xxij[2] * corr * (double)wj;
-      put3(ca[c], xi, p0, p1, p2);
-      put3(cb[c], xj, p0, p1, p2);
-    }
-    nits++;
-    if (ready[0] && ready[1] && ready[2]) break;
-    if (nits >= 1000) return false;
+// Iteration counts of SHAKE molecules (the reference's niter, averaged per
+// molecule) summed per system with the largest single count; every lane of
+// the warp calls it (sys < 0 for lanes without a molecule).
+__device__ __forceinline__ void shake_tally(DevPtrs &P, int sys, int its) {
+  unsigned grp = __match_any_sync(FULL, sys);
+  unsigned sum = __reduce_add_sync(grp, (unsigned)its);
+  unsigned mx = __reduce_max_sync(grp, (unsigned)its);
+  if (sys >= 0 && (threadIdx.x & 31) == __ffs(grp) - 1) {
+    atomicAdd(&P.st[sys].shake_its, (unsigned long long)sum);
+    atomicMax(&P.st[sys].shake_its_max, (int)mx);
   }
-  double4 o0 = P.x[base], o1 = P.x[base + 1], o2 = P.x[base + 2];
-  o0.x = p0.x; o0.y = p0.y; o0.z = p0.z;
-  o1.x = p1.x; o1.y = p1.y; o1.z = p1.z;
-  o2.x = p2.x; o2.y = p2.y; o2.z = p2.z;
-  P.x[base] = o0; P.x[base + 1] = o1; P.x[base + 2] = o2;
-  return true;
 }
 
-__global__ void k_shake(DevPtrs P) {
+// One constraint update of shake (md.f90:14500-14540); true when the
+// constraint was already within tolerance (it is still corrected, as there).
+__device__ __forceinline__ bool shake_pair(double3 &xi, double3 &xj, const double3 &xxi, const double3 &xxj,
+                                           float wi, float wj, double d2) {
+  double xij[3] = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
+  double xij2 = xij[0] * xij[0] + xij[1] * xij[1] + xij[2] * xij[2];
+  double diff = d2 - xij2;
+  bool ready = fabs(diff) < 0.0001 * d2;
+  double xxij[3] = {xxi.x - xxj.x, xxi.y - xxj.y, xxi.z - xxj.z};
+  double scp = xij[0] * xxij[0] + xij[1] * xxij[1] + xij[2] * xxij[2];
+  float wsum = wi + wj;
+  double corr = diff / (2. * scp * (double)wsum);
+  xi.x += xxij[0] * corr * (double)wi; xi.y += xxij[1] * corr * (double)wi; xi.z += xxij[2] * corr * (double)wi;
+  xj.x -= xxij[0] * corr * (double)wj; xj.y -= xxij[1] * corr * (double)wj; xj.z -= xxij[2] * corr * (double)wj;
+  return ready;
+}
+
+// shake (md.f90:14445) for molecules of three atoms and three constraints
+// (rigid waters), one thread per molecule.  The atoms are relabelled on the
+// host so that the constraints, in their own order, join (0,1), (0,2), (1,2);
+// sweeps, readiness flags and the 1000-sweep limit are the reference's.
+__global__ void __launch_bounds__(128, 7) k_shake3(DevPtrs P) {
   int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= P.nshake_tot) return;
-  int f = P.sh_first[m], n = P.sh_n[m];
-  if (n == 0) return;
-  if (n == 3) {
-    int2 a = P.sh_ij[f], b = P.sh_ij[f + 1], c = P.sh_ij[f + 2];
-    int lo = min(min(min(a.x, a.y), min(b.x, b.y)), min(c.x, c.y));
-    int hi = max(max(max(a.x, a.y), max(b.x, b.y)), max(c.x, c.y));
-    if (hi - lo <= 2) {
-      if (!shake3(P, lo, P.sh_ij + f, P.sh_d2 + f)) set_status(&P.st[P.sh_sys[m]], QB_ERR_SHAKE);
-      return;
+  int sys = -1, its = 0;
+  if (m < P.nsh3) {
+    const int4 at = P.sh3_at[m];
+    const double4 d2 = P.sh3_d2[m];
+    sys = at.w;
+    double3 x0 = ld3(P.x, at.x), x1 = ld3(P.x, at.y), x2 = ld3(P.x, at.z);
+    const double3 r0 = ld3(P.xx, at.x), r1 = ld3(P.xx, at.y), r2 = ld3(P.xx, at.z);
+    const float w0 = P.winv[at.x], w1 = P.winv[at.y], w2 = P.winv[at.z];
+    bool c0 = false, c1 = false, c2 = false;
+    for (;;) {
+      if (!c0) c0 = shake_pair(x0, x1, r0, r1, w0, w1, d2.x);
+      if (!c1) c1 = shake_pair(x0, x2, r0, r2, w0, w2, d2.y);
+      if (!c2) c2 = shake_pair(x1, x2, r1, r2, w1, w2, d2.z);
+      its++;
+      if (c0 && c1 && c2) break;
+      if (its >= 1000) break;
+    }
+    if (c0 && c1 && c2) {
+      double4 o;
+      o = P.x[at.x]; o.x = x0.x; o.y = x0.y; o.z = x0.z; P.x[at.x] = o;
+      o = P.x[at.y]; o.x = x1.x; o.y = x1.y; o.z = x1.z; P.x[at.y] = o;
+      o = P.x[at.z]; o.x = x2.x; o.y = x2.y; o.z = x2.z; P.x[at.z] = o;
+    } else {
+      set_status(&P.st[sys], QB_ERR_SHAKE);
     }
   }
-  bool done = false;
-  int nits = 0;
-  // readiness flags of up to 64*64 constraints in thread-local memory
-  unsigned long long rd[64];
-  int nwords = (n + 63) / 64;
-  if (nwords > 64) { set_status(&P.st[P.sh_sys[m]], QB_ERR_UNSUPPORTED); return; }
-  for (int w = 0; w < nwords; w++) rd[w] = 0;
+  shake_tally(P, sys, its);
+}
+
+// shake (md.f90:14445) for every other molecule, one block per molecule.
+// The reference sweeps the constraints in order (Gauss-Seidel), skipping
+// those already within tolerance.  The host groups them into levels: a
+// constraint's level is one more than that of the latest earlier constraint
+// sharing an atom, so constraints of one level touch disjoint atoms and every
+// update they depend on comes from an earlier level.  Running the levels in
+// order, each level in parallel, gives the reference's positions, readiness
+// flags and sweep count exactly.  The molecule's atoms (position, winv) and
+// its constraints (old bond vector, d2, readiness) live in shared memory, or
+// in a per-molecule global scratch slice when they do not fit.
+constexpr int SHG_BLOCK = 128;
+
+__global__ void __launch_bounds__(SHG_BLOCK) k_shake_general(DevPtrs P) {
+  extern __shared__ double4 shg_smem[];
+  const int g = blockIdx.x;
+  const int4 info = P.shg_info[g];       // atom offset, atoms, constraint offset, constraints
+  const int4 info2 = P.shg_info2[g];     // level offset, levels, system, global scratch offset (-1: shared)
+  const int na = info.y, nc = info.w, nlev = info2.y, sys = info2.z;
+  double4 *ax = info2.w < 0 ? shg_smem : P.shg_scratch + info2.w;   // x, y, z, winv
+  double4 *cx = ax + na;                                            // old bond vector, d2
+  uint8_t *rdy = reinterpret_cast<uint8_t *>(cx + nc);
+  const int *at = P.shg_at + info.x;
+  const int2 *cij = P.shg_c + info.z;
+  const int *lev = P.shg_lev + info2.x;
+  for (int t = threadIdx.x; t < na; t += SHG_BLOCK) {
+    double4 x = P.x[at[t]];
+    x.w = (double)P.winv[at[t]];
+    ax[t] = x;
+  }
+  for (int t = threadIdx.x; t < nc; t += SHG_BLOCK) {
+    int2 ij = cij[t];
+    double3 xi = ld3(P.xx, at[ij.x]), xj = ld3(P.xx, at[ij.y]);
+    cx[t] = make_double4(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, P.shg_d2[info.z + t]);
+    rdy[t] = 0;
+  }
+  __syncthreads();
+  int its = 0;
+  bool done = nc == 0;
   while (!done) {
-    for (int c = 0; c < n; c++) {
-      if ((rd[c >> 6] >> (c & 63)) & 1ull) continue;
-      int2 ij = P.sh_ij[f + c];
-      double4 xi = P.x[ij.x], xj = P.x[ij.y];
-      double4 xxi = P.xx[ij.x], xxj = P.xx[ij.y];
-      double xij[3] = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
-      double xij2 = xij[0] * xij[0] + xij[1] * xij[1] + xij[2] * xij[2];
-      double d2 = P.sh_d2[f + c];
-      double diff = d2 - xij2;
-      if (fabs(diff) < 0.0001 * d2) rd[c >> 6] |= 1ull << (c & 63);
-      double xxij[3] = {xxi.x - xxj.x, xxi.y - xxj.y, xxi.z - xxj.z};
-      double scp = xij[0] * xxij[0] + xij[1] * xxij[1] + xij[2] * xxij[2];
-      float wi = P.winv[ij.x], wj = P.winv[ij.y];
-      float wsum = wi + wj;
-      double corr = diff / (2. * scp * (double)wsum);
-      xi.x += xxij[0] * corr * (double)wi; xi.y += xxij[1] * corr * (double)wi; xi.z += xxij[2] * corr * (double)wi;
-      xj.x -= xxij[0] * corr * (double)wj; xj.y -= xxij[1] * corr * (double)wj; xj.z -= xxij[2] * corr * (double)wj;
-      P.x[ij.x] = xi;
-      P.x[ij.y] = xj;
+    for (int L = 0; L < nlev; L++) {
+      for (int t = lev[L] + threadIdx.x; t < lev[L + 1]; t += SHG_BLOCK) {
+        if (rdy[t]) continue;
+        const int2 ij = cij[t];
+        const double4 c = cx[t];
+        double4 xi = ax[ij.x], xj = ax[ij.y];
+        double xij[3] = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z};
+        double xij2 = xij[0] * xij[0] + xij[1] * xij[1] + xij[2] * xij[2];
+        double diff = c.w - xij2;
+        if (fabs(diff) < 0.0001 * c.w) rdy[t] = 1;
+        double scp = xij[0] * c.x + xij[1] * c.y + xij[2] * c.z;
+        float wi = (float)xi.w, wj = (float)xj.w;
+        float wsum = wi + wj;
+        double corr = diff / (2. * scp * (double)wsum);
+        xi.x += c.x * corr * (double)wi; xi.y += c.y * corr * (double)wi; xi.z += c.z * corr * (double)wi;
+        xj.x -= c.x * corr * (double)wj; xj.y -= c.y * corr * (double)wj; xj.z -= c.z * corr * (double)wj;
+        ax[ij.x] = xi;
+        ax[ij.y] = xj;
+      }
+      __syncthreads();
     }
-    nits++;
-    done = true;
-    for (int c = 0; c < n && done; c++) done = (rd[c >> 6] >> (c & 63)) & 1ull;
-    if (!done && nits >= 1000) {
-      set_status(&P.st[P.sh_sys[m]], QB_ERR_SHAKE);
-      return;
+    its++;
+    bool mine = true;
+    for (int t = threadIdx.x; t < nc; t += SHG_BLOCK) mine = mine && rdy[t];
+    done = __syncthreads_and(mine);
+    if (!done && its >= 1000) break;
+  }
+  if (done) {
+    for (int t = threadIdx.x; t < na; t += SHG_BLOCK) {
+      double4 o = P.x[at[t]];
+      const double4 x = ax[t];
+      o.x = x.x; o.y = x.y; o.z = x.z;
+      P.x[at[t]] = o;
     }
+  } else if (threadIdx.x == 0) {
+    set_status(&P.st[sys], QB_ERR_SHAKE);
+  }
+  if (threadIdx.x == 0) {
+    atomicAdd(&P.st[sys].shake_its, (unsigned long long)its);
+    atomicMax(&P.st[sys].shake_its_max, its);
   }
 }
 

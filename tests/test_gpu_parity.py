@@ -115,7 +115,9 @@ def synthetic(tmp_path_factory):
     return {"c0": synth.water_sphere(str(root / "c0"), radius=15.0, seed=1234),
             "c1": synth.fep_solute(str(root / "c1"), seed=1234),
             # more waters than one shared-memory chunk of the water-water kernel
-            "c0_r25": synth.water_sphere(str(root / "c0_r25"), radius=25.0, seed=99)}
+            "c0_r25": synth.water_sphere(str(root / "c0_r25"), radius=25.0, seed=99),
+            # more waters than one mixed-precision chunk
+            "c0_r27": synth.water_sphere(str(root / "c0_r27"), radius=27.0, seed=7)}
 
 
 @pytest.mark.parametrize("case", ["c0", "c1", "c0_r25"])
@@ -153,7 +155,7 @@ def test_synthetic_windows_trajectory(synthetic, oracle):
         assert np.max(np.abs(b.coords(k) - o.coords())) < 1e-4
 
 
-@pytest.mark.parametrize("case", ["c1", "c0_r25"])
+@pytest.mark.parametrize("case", ["c1", "c0_r25", "c0_r27"])
 def test_mixed_precision_error_vs_fp64(synthetic, case):
     """The mixed-precision engine (FP32 water-water pair math, FP64 sums)
     against the FP64 engine on the same coordinates: the error it carries."""

@@ -139,9 +139,13 @@ struct Batch {
       if (max_nwat > 0) launch("list_qw", [&] { k_list_qw<<<nsys, 256, 0, stream>>>(p, force); });
     }
     if (max_nwat > 0)
-      launch("list_ww", [&] { k_list_ww<<<dim3(cdiv(max_nwat, 8), nsys), 256, 0, stream>>>(p, force); });
+      launch("list_ww", [&] { k_list_ww<<<dim3(cdiv(max_nwat, WL_WPB), nsys), WL_BLOCK, 0, stream>>>(p, force); });
     if (any_lrf)
-      launch("lrf_gather", [&] { k_lrf_gather<<<dim3(cdiv(max_ncgp, LRF_BLOCK), nsys), LRF_BLOCK, 0, stream>>>(p, force); });
+      launch("lrf_gather", [&] {
+        dim3 g(cdiv(max_ncgp, LRF_BLOCK), nsys);
+        if (opt.precision == QB_MIXED) k_lrf_gather<true><<<g, LRF_BLOCK, 0, stream>>>(p, force);
+        else k_lrf_gather<false><<<g, LRF_BLOCK, 0, stream>>>(p, force);
+      });
     launch("lists_end", [&] { k_lists_end<<<cdiv(nsys, 128), 128, 0, stream>>>(p, force); });
     check_launch("list kernels");
   }
@@ -216,7 +220,8 @@ struct Batch {
       launch("shake", [&] { k_shake3<<<cdiv(p.nsh3, 128), 128, 0, stream>>>(p); });
     if (any_shake && p.nshg > 0)
       launch("shake_general", [&] { k_shake_general<<<p.nshg, SHG_BLOCK, p.shg_smem, stream>>>(p); });
-    launch("finish", [&] { k_finish<<<nsys, 512, 0, stream>>>(p, 1); });
+    launch("kinetic", [&] { k_kinetic<<<dim3(p.kin_nblk, nsys), KIN_BLOCK, 0, stream>>>(p, 1); });
+    launch("finish", [&] { k_finish<<<nsys, 32, 0, stream>>>(p, 1, p.kin_nblk); });
     check_launch("step kernels");
     istep++;
   }
@@ -694,6 +699,8 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   // the limit (not an allocation) covers every chunk size any batch may use
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  P.kin_nblk = std::max(1, (B.max_natom + KIN_BLOCK - 1) / KIN_BLOCK);
+  P.kin_part = dev_alloc<double>((size_t)n * P.kin_nblk * 4, o);
   P.E = dev_alloc<double>((size_t)n * QB_NE, o);
   P.EQ = dev_alloc<double>((size_t)n * MAXS * QB_NEQ, o);
   P.hist = nullptr;
@@ -803,7 +810,8 @@ int qb_batch_create(qb_handle *const *systems, int n, const qb_options *opt, qb_
     CUDA_TRY(cudaStreamCreateWithFlags(&b->b.stream, cudaStreamNonBlocking));
     qb::build(b->b, systems, n);
     // md_run's initial temperature (md.f90:3960-3963)
-    qb::k_finish<<<n, 512, 0, b->b.stream>>>(b->b.P, 0);
+    qb::k_kinetic<<<dim3(b->b.P.kin_nblk, n), qb::KIN_BLOCK, 0, b->b.stream>>>(b->b.P, 0);
+    qb::k_finish<<<n, 32, 0, b->b.stream>>>(b->b.P, 0, b->b.P.kin_nblk);
     b->b.check_launch("initial temperature");
     CUDA_TRY(cudaStreamSynchronize(b->b.stream));
   });

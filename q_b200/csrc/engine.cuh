@@ -12,7 +12,10 @@
 namespace qb {
 
 constexpr int MAXS = QB_MAX_STATES;
-constexpr int LRF_STRIDE = 44;   // centre[3], phi0, phi1[3], phi2[9], phi3[27], pad
+// LRF record of a charge group: centre[3], phi0, phi1[3], the 6 distinct
+// components of the symmetric phi2 (xx,xy,xz,yy,yz,zz) and the 10 of phi3
+// (xxx,xxy,xxz,xyy,xyz,xzz,yyy,yyz,yzz,zzz), pad.
+constexpr int LRF_STRIDE = 24;
 constexpr int MAX_SHELLS = 4;
 constexpr int NQ_SHARED = 64;    // Q atoms whose water forces are reduced in shared memory
 enum AtomFlags : uint8_t { F_EXCL = 1, F_SHELL = 2, F_HEAVY = 4 };
@@ -121,6 +124,8 @@ struct DevPtrs {
   int *ww_n, *ww_sp;                       // count per water; [gw*ww_nch + c] count below chunk c's end
   int ww_cap, ww_chunk, ww_nch;
   // energies
+  double *kin_part;                        // [(s*kin_nblk + block)*4] kinetic-energy partial sums
+  int kin_nblk;
   double *E;                               // [s*QB_NE]
   double *EQ;                              // [(s*MAXS + st)*QB_NEQ]
   // history [kind][s][rec][QB_NE + MAXS*QB_NEQ + 1]

@@ -7,6 +7,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "engine.cuh"
 
 namespace qb {
@@ -70,43 +72,34 @@ __global__ void k_cgp_centers(DevPtrs P, int force) {
 // Multipole contribution of charge q at offset (dx,dy,dz) from a group centre
 // (md.f90:5581-5636), accumulated in the symmetric form m[20] = phi0,
 // phi1[x,y,z], phi2[xx,xy,xz,yy,yz,zz], phi3[xxx,xxy,xxz,xyy,xyz,xzz,yyy,yyz,
-// yzz,zzz]; lrf_expand writes the full 1+3+9+27 layout the reference stores.
-__device__ __forceinline__ void lrf_accumulate(double *m, double q, double dx, double dy, double dz) {
-  double r2 = dx * dx + dy * dy + dz * dz;
-  double rinv = rsqrt(r2), ri2 = rinv * rinv;
-  double f0 = q * rinv * ri2;              // q / r^3
+// yzz,zzz]: the reference's 9 and 27 components are copies of these.
+__device__ __forceinline__ float rsq(float v) { return rsqrtf(v); }
+__device__ __forceinline__ double rsq(double v) { return rsqrt(v); }
+
+template <class R>
+__device__ __forceinline__ void lrf_accumulate(R *m, R q, R dx, R dy, R dz) {
+  R r2 = dx * dx + dy * dy + dz * dz;
+  R rinv = rsq(r2), ri2 = rinv * rinv;
+  R f0 = q * rinv * ri2;              // q / r^3
   m[0] += f0 * r2;
   m[1] -= f0 * dx; m[2] -= f0 * dy; m[3] -= f0 * dz;
-  double f1 = 3. * f0 * ri2;
-  double f1x = f1 * dx, f1y = f1 * dy, f1z = f1 * dz;
+  R f1 = R(3) * f0 * ri2;
+  R f1x = f1 * dx, f1y = f1 * dy, f1z = f1 * dz;
   m[4] += f1x * dx - f0; m[5] += f1x * dy; m[6] += f1x * dz;
   m[7] += f1y * dy - f0; m[8] += f1y * dz; m[9] += f1z * dz - f0;
-  double f2 = -f1 * ri2;
-  double x5 = 5. * dx, y5 = 5. * dy, z5 = 5. * dz;
-  double xx = x5 * dx, yy = y5 * dy, zz = z5 * dz, xy = x5 * dy;
-  m[10] += f2 * (xx * dx - 3. * r2 * dx);
+  R f2 = -f1 * ri2;
+  R x5 = R(5) * dx, y5 = R(5) * dy, z5 = R(5) * dz;
+  R xx = x5 * dx, yy = y5 * dy, zz = z5 * dz, xy = x5 * dy;
+  m[10] += f2 * (xx * dx - R(3) * r2 * dx);
   m[11] += f2 * (xx * dy - r2 * dy);
   m[12] += f2 * (xx * dz - r2 * dz);
   m[13] += f2 * (yy * dx - r2 * dx);
   m[14] += f2 * (xy * dz);
   m[15] += f2 * (zz * dx - r2 * dx);
-  m[16] += f2 * (yy * dy - 3. * r2 * dy);
+  m[16] += f2 * (yy * dy - R(3) * r2 * dy);
   m[17] += f2 * (yy * dz - r2 * dz);
   m[18] += f2 * (zz * dy - r2 * dy);
-  m[19] += f2 * (zz * dz - 3. * r2 * dz);
-}
-
-__device__ __forceinline__ void lrf_expand(const double *m, double *L) {
-  L[3] = m[0];
-  L[4] = m[1]; L[5] = m[2]; L[6] = m[3];
-  const int i2[9] = {4, 5, 6, 5, 7, 8, 6, 8, 9};
-#pragma unroll
-  for (int k = 0; k < 9; k++) L[7 + k] = m[i2[k]];
-  // unique index of the sorted triple (a<=b<=c) for every (a,b,c)
-  const int i3[27] = {10, 11, 12, 11, 13, 14, 12, 14, 15, 11, 13, 14, 13, 16, 17, 14, 17, 18,
-                      12, 14, 15, 14, 17, 18, 15, 18, 19};
-#pragma unroll
-  for (int k = 0; k < 27; k++) L[16 + k] = m[i3[k]];
+  m[19] += f2 * (zz * dz - R(3) * r2 * dz);
 }
 
 // LRF multipoles of every charge group, gathered (nbpplist_lrf 5448,
@@ -120,16 +113,23 @@ __device__ __forceinline__ void lrf_expand(const double *m, double *L) {
 // in tiles (consecutive groups, at most LRF_TILE_G groups and LRF_TILE_A
 // atoms, boundaries precomputed on the host): a tile's switching atoms and
 // atom positions/charges are staged in shared memory and read as broadcasts.
+// The group-pair window test is FP64 in both precisions.  Mixed precision:
+// atom offsets from the group centre in FP32 (positions relative to the
+// sphere centre, |offset| >= ~7 A here), each tile summed in FP32 and added to
+// FP64 totals.
 constexpr int LRF_TILE_G = 128, LRF_TILE_A = 512, LRF_BLOCK = 128;
 
+template <bool MIXED>
 __global__ void __launch_bounds__(LRF_BLOCK) k_lrf_gather(DevPtrs P, int force) {
+  using R = typename std::conditional<MIXED, float, double>::type;
+  using R4 = typename std::conditional<MIXED, float4, double4>::type;
   int s = blockIdx.y;
   if (!list_due(P, s, force)) return;
   const SysDev &S = P.sys[s];
   if (!S.use_lrf || blockIdx.x * LRF_BLOCK >= S.ncgp) return;
   __shared__ double4 hsw[LRF_TILE_G];      // switching atom; w: -1 excluded, 1 solute, 0 water
   __shared__ int2 hrange[LRF_TILE_G];      // first atom slot, atom count
-  __shared__ double4 hat[LRF_TILE_A];      // atom position, charge
+  __shared__ R4 hat[LRF_TILE_A];           // atom position (mixed: from the sphere centre), charge
   int gl = blockIdx.x * LRF_BLOCK + threadIdx.x;
   int g = S.coff + gl;
   bool active = gl < S.ncgp;
@@ -142,8 +142,11 @@ __global__ void __launch_bounds__(LRF_BLOCK) k_lrf_gather(DevPtrs P, int force) 
     cx = L[0]; cy = L[1]; cz = L[2];
     xs = ld3(P.x, swg);
   }
+  const double ox = MIXED ? S.xp[0] : 0.0, oy = MIXED ? S.xp[1] : 0.0, oz = MIXED ? S.xp[2] : 0.0;
+  const R ccx = (R)(cx - ox), ccy = (R)(cy - oy), ccz = (R)(cz - oz);
   const bool g_sol = gl < S.ncgp_sol;
   double m[20];
+  R mt[20];
 #pragma unroll
   for (int k = 0; k < 20; k++) m[k] = 0.0;
   for (int t = 0; t < S.nlrft; t++) {
@@ -164,11 +167,17 @@ __global__ void __launch_bounds__(LRF_BLOCK) k_lrf_gather(DevPtrs P, int force) 
       int at = P.cg_atoms[a0 + i];
       double4 p = P.x[at];
       bool qsol = (at - S.aoff) < S.nsol && P.iq[at] >= 0;
-      p.w = qsol ? 0.0 : (double)P.crg[at];
-      hat[i] = p;
+      R4 v;
+      v.x = (R)(p.x - ox); v.y = (R)(p.y - oy); v.z = (R)(p.z - oz);
+      v.w = qsol ? R(0) : (R)P.crg[at];
+      hat[i] = v;
     }
     __syncthreads();
     if (active) {
+      if (MIXED) {
+#pragma unroll
+        for (int k = 0; k < 20; k++) mt[k] = R(0);
+      }
       for (int i = 0; i < nh; i++) {
         double4 hs = hsw[i];
         if (hs.w < 0.0 || tile.x + i == gl) continue;
@@ -178,58 +187,98 @@ __global__ void __launch_bounds__(LRF_BLOCK) k_lrf_gather(DevPtrs P, int force) 
         if (!(r2 > rc2 && r2 <= S.RcLRF2)) continue;
         int2 rg = hrange[i];
         for (int k = 0; k < rg.y; k++) {
-          double4 a = hat[rg.x + k];
-          if (a.w != 0.0) lrf_accumulate(m, a.w, a.x - cx, a.y - cy, a.z - cz);
+          R4 a = hat[rg.x + k];
+          if (a.w != R(0)) {
+            if (MIXED) lrf_accumulate<R>(mt, a.w, a.x - ccx, a.y - ccy, a.z - ccz);
+            else lrf_accumulate<double>(m, (double)a.w, (double)a.x - cx, (double)a.y - cy, (double)a.z - cz);
+          }
         }
+      }
+      if (MIXED) {
+#pragma unroll
+        for (int k = 0; k < 20; k++) m[k] += (double)mt[k];
       }
     }
   }
-  if (active) lrf_expand(m, P.lrf + (size_t)g * LRF_STRIDE);
+  if (active) {
+    double *L = P.lrf + (size_t)g * LRF_STRIDE;
+#pragma unroll
+    for (int k = 0; k < 20; k++) L[3 + k] = m[k];
+  }
 }
 
 // Water-water neighbour list (nbwwlist / nbwwlist_lrf, md.f90:8233, 8370),
 // stored in both directions: water i lists every other water j inside the
 // sphere whose O lies within Rcww of i's O, as local water indices in
 // ascending order.  ww_sp[gw*ww_nch + c] counts the entries below the end of
-// staging chunk c (chunks of ww_chunk waters, a multiple of 32), so the force
-// kernel finds each chunk's slice of the list directly.  One warp per water.
-__global__ void k_list_ww(DevPtrs P, int force) {
+// force-kernel chunk c (chunks of ww_chunk waters, a multiple of 32), so the
+// force kernel finds each chunk's slice of the list directly.
+// Block = WL_WPB waters of one system, one warp per water at a time; the
+// system's O positions are staged in shared memory WL_STAGE waters at a time
+// (w = -1 for excluded waters) and scanned 32 at a time with a ballot.
+constexpr int WL_BLOCK = 512, WL_WPB = 128, WL_STAGE = 1408;   // 44 KB of staged O positions
+
+__global__ void __launch_bounds__(WL_BLOCK) k_list_ww(DevPtrs P, int force) {
   int s = blockIdx.y;
   if (!list_due(P, s, force)) return;
   const SysDev &S = P.sys[s];
-  int wpb = blockDim.x >> 5;
-  int iw = blockIdx.x * wpb + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  if (iw >= S.nwat) return;
-  int gw = S.woff + iw;
-  int oi = S.aoff + S.nsol + 3 * iw;
-  int cnt = 0;
-  uint16_t *out = P.ww + (size_t)gw * P.ww_cap;
-  int *sp = P.ww_sp + (size_t)gw * P.ww_nch;
-  if (!(P.flags[oi] & F_EXCL)) {
-    double3 xi = ld3(P.x, oi);
-    for (int base = 0; base < S.nwat; base += 32) {
-      if (base > 0 && base % P.ww_chunk == 0 && lane == 0) sp[base / P.ww_chunk - 1] = min(cnt, P.ww_cap);
-      int jw = base + lane;
-      bool ok = false;
-      int oj = S.aoff + S.nsol + 3 * jw;
-      if (jw < S.nwat && jw != iw && !(P.flags[oj] & F_EXCL)) {
-        double3 xj = ld3(P.x, oj);
-        double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-        ok = dx * dx + dy * dy + dz * dz <= S.Rcww2;
-      }
-      unsigned bal = __ballot_sync(FULL, ok);
-      if (ok) {
-        int pos = cnt + __popc(bal & ((1u << lane) - 1u));
-        if (pos < P.ww_cap) out[pos] = (uint16_t)jw;
-      }
-      cnt += __popc(bal);
+  const int i0 = blockIdx.x * WL_WPB;
+  if (i0 >= S.nwat) return;
+  const int i1 = min(i0 + WL_WPB, S.nwat);
+  __shared__ double4 so[WL_STAGE];
+  __shared__ int scnt[WL_WPB];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = WL_BLOCK / 32;
+  const int obase = S.aoff + S.nsol;
+  for (int t = threadIdx.x; t < WL_WPB; t += WL_BLOCK) scnt[t] = 0;
+  for (int c0 = 0; c0 < S.nwat; c0 += WL_STAGE) {
+    const int cn = min(WL_STAGE, S.nwat - c0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < cn; t += WL_BLOCK) {
+      int o = obase + 3 * (c0 + t);
+      double4 x = P.x[o];
+      x.w = (P.flags[o] & F_EXCL) ? -1.0 : 1.0;
+      so[t] = x;
     }
-  } else if (lane == 0) {
-    for (int c = 0; c < P.ww_nch; c++) sp[c] = 0;
+    __syncthreads();
+    for (int iw = i0 + warp; iw < i1; iw += nwarp) {
+      const int gw = S.woff + iw;
+      const int oi = obase + 3 * iw;
+      if (P.flags[oi] & F_EXCL) continue;
+      const double3 xi = ld3(P.x, oi);
+      uint16_t *out = P.ww + (size_t)gw * P.ww_cap;
+      int *sp = P.ww_sp + (size_t)gw * P.ww_nch;
+      int cnt = scnt[iw - i0];
+      for (int b = 0; b < cn; b += 32) {
+        const int base = c0 + b;
+        if (base > 0 && base % P.ww_chunk == 0 && lane == 0) sp[base / P.ww_chunk - 1] = min(cnt, P.ww_cap);
+        const int jl = b + lane, jw = base + lane;
+        bool ok = false;
+        if (jl < cn && jw != iw) {
+          double4 xj = so[jl];
+          double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+          ok = xj.w > 0.0 && dx * dx + dy * dy + dz * dz <= S.Rcww2;
+        }
+        unsigned bal = __ballot_sync(FULL, ok);
+        if (ok) {
+          int pos = cnt + __popc(bal & ((1u << lane) - 1u));
+          if (pos < P.ww_cap) out[pos] = (uint16_t)jw;
+        }
+        cnt += __popc(bal);
+      }
+      if (lane == 0) scnt[iw - i0] = cnt;
+      __syncwarp();
+    }
   }
-  if (lane == 0) {
+  __syncthreads();
+  for (int iw = i0 + warp; iw < i1; iw += nwarp) {
+    if (lane != 0) continue;
+    const int gw = S.woff + iw;
+    int cnt = (P.flags[obase + 3 * iw] & F_EXCL) ? 0 : scnt[iw - i0];
+    int *sp = P.ww_sp + (size_t)gw * P.ww_nch;
     if (cnt > P.ww_cap) { set_status(&P.st[s], QB_ERR_LIST_OVERFLOW); cnt = P.ww_cap; }
     P.ww_n[gw] = cnt;
+    if (cnt == 0)
+      for (int c = 0; c < P.ww_nch; c++) sp[c] = 0;
     for (int c = (S.nwat - 1) / P.ww_chunk; c < P.ww_nch; c++) sp[c] = cnt;
   }
 }
@@ -1055,31 +1104,44 @@ __global__ void k_nb_qq(DevPtrs P) {
 }
 
 // lrf_taylor (md.f90:3646): potential and field of each atom's own group
-// multipoles; one thread per atom.
+// multipoles; one thread per atom.  The reference's phi2(9) and phi3(27) are
+// read through the index of their distinct component, in its order of terms.
 __global__ void k_lrf_taylor(DevPtrs P) {
   int s = blockIdx.y;
   const SysDev &S = P.sys[s];
   if (!S.use_lrf) return;
+  constexpr int i2[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+  constexpr int i3[27] = {0, 1, 2, 1, 3, 4, 2, 4, 5, 1, 3, 4, 3, 6, 7, 4, 7, 8, 2, 4, 5, 4, 7, 8, 5, 8, 9};
   double e = 0;
   for (int i0 = blockIdx.x * blockDim.x; i0 < S.natom; i0 += gridDim.x * blockDim.x) {
     int il = i0 + threadIdx.x;
     if (il < S.natom) {
       int i = S.aoff + il;
       if (!(P.flags[i] & F_EXCL) && P.iq[i] < 0) {
-        const double *L = P.lrf + (size_t)P.cgp[i] * LRF_STRIDE;
+        const double4 *L4 = reinterpret_cast<const double4 *>(P.lrf + (size_t)P.cgp[i] * LRF_STRIDE);
+        double L[24];
+#pragma unroll
+        for (int w = 0; w < 6; w++) {
+          double4 q = L4[w];
+          L[4 * w] = q.x; L[4 * w + 1] = q.y; L[4 * w + 2] = q.z; L[4 * w + 3] = q.w;
+        }
         double3 xi = ld3(P.x, i);
         double dr[3] = {L[0] - xi.x, L[1] - xi.y, L[2] - xi.z};
-        const double *p1 = L + 4, *p2 = L + 7, *p3 = L + 16;
+        const double *p1 = L + 4, *p2 = L + 7, *p3 = L + 13;
         double V = L[3] + p1[0] * dr[0] + p1[1] * dr[1] + p1[2] * dr[2];
-        for (int a = 0; a < 3; a++) V += 0.5 * (p2[3 * a] * dr[0] + p2[3 * a + 1] * dr[1] + p2[3 * a + 2] * dr[2]) * dr[a];
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+          V += 0.5 * (p2[i2[3 * a]] * dr[0] + p2[i2[3 * a + 1]] * dr[1] + p2[i2[3 * a + 2]] * dr[2]) * dr[a];
         double q = (double)P.crg[i];
         e += 0.5 * q * V;
         double g[3];
+#pragma unroll
         for (int c = 0; c < 3; c++) {
-          double df = p1[c] + p2[3 * c] * dr[0] + p2[3 * c + 1] * dr[1] + p2[3 * c + 2] * dr[2];
+          double df = p1[c] + p2[i2[3 * c]] * dr[0] + p2[i2[3 * c + 1]] * dr[1] + p2[i2[3 * c + 2]] * dr[2];
+#pragma unroll
           for (int a = 0; a < 3; a++) {
-            const double *p = p3 + 9 * c + 3 * a;
-            df += 0.5 * (p[0] * dr[0] + p[1] * dr[1] + p[2] * dr[2]) * dr[a];
+            const int o = 9 * c + 3 * a;
+            df += 0.5 * (p3[i3[o]] * dr[0] + p3[i3[o + 1]] * dr[1] + p3[i3[o + 2]] * dr[2]) * dr[a];
           }
           g[c] = q * df;
         }
@@ -1835,16 +1897,19 @@ __global__ void __launch_bounds__(SHG_BLOCK) k_shake_general(DevPtrs P) {
   }
 }
 
-// End of a step: velocities from the shaken coordinates, kinetic energy and
-// temperature (md.f90:3813), Berendsen factors, and the energy records of
-// md_run's output intervals.  mode 0: the initial temperature before the loop.
-__global__ void __launch_bounds__(512) k_finish(DevPtrs P, int mode) {
-  int s = blockIdx.x;
+// temperature (md.f90:3817), first half, and the velocities of a SHAKE step
+// (md.f90:4119): v = (x - xx)/dt, then the kinetic energies of solute and
+// solvent atoms (all and not excluded).  Grid (blocks, systems); each block
+// writes its four partial sums, which k_finish adds in block order.
+constexpr int KIN_BLOCK = 256;
+
+__global__ void __launch_bounds__(KIN_BLOCK) k_kinetic(DevPtrs P, int mode) {
+  int s = blockIdx.y;
   const SysDev &S = P.sys[s];
-  SysState &st = P.st[s];
   __shared__ double sh[32];
   double acc[4] = {0, 0, 0, 0};  // solute all, solute free, solvent all, solvent free
-  for (int il = threadIdx.x; il < S.natom; il += blockDim.x) {
+  int il = blockIdx.x * KIN_BLOCK + threadIdx.x;
+  if (il < S.natom) {
     int g = S.aoff + il;
     double4 v = P.v[g];
     if (mode == 1 && S.has_shake) {
@@ -1856,12 +1921,29 @@ __global__ void __launch_bounds__(512) k_finish(DevPtrs P, int mode) {
     }
     double e = 0.5 * P.mass[g] * (v.x * v.x + v.y * v.y + v.z * v.z);
     bool free_ = !(P.flags[g] & F_EXCL);
-    if (il < S.nsol) { acc[0] += e; if (free_) acc[1] += e; }
-    else { acc[2] += e; if (free_) acc[3] += e; }
+    if (il < S.nsol) { acc[0] = e; if (free_) acc[1] = e; }
+    else { acc[2] = e; if (free_) acc[3] = e; }
   }
   double tot[4];
   for (int k = 0; k < 4; k++) tot[k] = block_sum(acc[k], sh);
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 4; k++) P.kin_part[((size_t)s * gridDim.x + blockIdx.x) * 4 + k] = tot[k];
+}
+
+// temperature (md.f90:3817), second half, one warp per system: temperatures,
+// the Berendsen scaling factors of the next step, output and energy-file
+// records of this step, step counter.
+__global__ void k_finish(DevPtrs P, int mode, int nblk) {
+  int s = blockIdx.x;
+  const SysDev &S = P.sys[s];
+  SysState &st = P.st[s];
+  int lane = threadIdx.x;
+  double tot[4] = {0, 0, 0, 0};
+  int nb = (S.natom + KIN_BLOCK - 1) / KIN_BLOCK;
+  for (int b = lane; b < nb; b += 32)
+    for (int k = 0; k < 4; k++) tot[k] += P.kin_part[((size_t)s * nblk + b) * 4 + k];
+  for (int k = 0; k < 4; k++) tot[k] = warp_sum(tot[k]);
+  if (lane == 0) {
     const double kb = (double)kBoltzF;
     double Tfree_sol = tot[1], Tfree_solv = tot[3];
     double Tfree = Tfree_solv + Tfree_sol;

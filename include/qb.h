@@ -121,6 +121,9 @@ int qb_batch_temperature(qb_batch *b, int sys, double *out);
 /* Gradient dU/dx from the last potential evaluation, 3*natom doubles. */
 int qb_batch_gradient(qb_batch *b, int sys, double *d_out);
 
+/* Coordinates of one system, 3*natom doubles.  Setting them marks the pair
+ * lists and LRF multipoles of every system stale: they are rebuilt before the
+ * next step, as qdyn builds them at step 0 of a restart. */
 int qb_batch_get_coords(qb_batch *b, int sys, double *x_out);
 int qb_batch_set_coords(qb_batch *b, int sys, const double *x_in);
 int qb_batch_get_velocities(qb_batch *b, int sys, double *v_out);

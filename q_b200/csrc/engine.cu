@@ -7,6 +7,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -63,6 +64,7 @@ struct Batch {
        any_qb = false;
   size_t watpol_smem = 0;
   int q_states = 0;           // state count shared by every system with Q atoms (0: they differ)
+  int max_nq = 0;
   // profiling
   bool profiling = false;
   std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
@@ -73,6 +75,7 @@ struct Batch {
 
   ~Batch() {
     if (stream) cudaStreamSynchronize(stream);
+    drop_graphs();
     for (auto &e : event_pool) cudaEventDestroy(e);
     for (auto &pe : pending) { cudaEventDestroy(pe.second.first); cudaEventDestroy(pe.second.second); }
     for (void *p : owned) cudaFree(p);
@@ -189,12 +192,13 @@ struct Batch {
       }
       if (any_q) launch("nb_qw", [&] {
         dim3 g(cdiv(max_nwat, 128), nsys);
+        if (max_nq > NQ_SHARED) { k_nb_qw<0, false><<<g, 128, 0, stream>>>(p); return; }
         switch (q_states) {
-          case 1: k_nb_qw<1><<<g, 128, 0, stream>>>(p); break;
-          case 2: k_nb_qw<2><<<g, 128, 0, stream>>>(p); break;
-          case 3: k_nb_qw<3><<<g, 128, 0, stream>>>(p); break;
-          case 4: k_nb_qw<4><<<g, 128, 0, stream>>>(p); break;
-          default: k_nb_qw<0><<<g, 128, 0, stream>>>(p);
+          case 1: k_nb_qw<1, true><<<g, 128, 0, stream>>>(p); break;
+          case 2: k_nb_qw<2, true><<<g, 128, 0, stream>>>(p); break;
+          case 3: k_nb_qw<3, true><<<g, 128, 0, stream>>>(p); break;
+          case 4: k_nb_qw<4, true><<<g, 128, 0, stream>>>(p); break;
+          default: k_nb_qw<0, true><<<g, 128, 0, stream>>>(p);
         }
       });
     }
@@ -204,16 +208,64 @@ struct Batch {
       launch("bonded", [&] { k_bonded<<<dim3(cdiv(max_terms, 256), nsys), 256, 0, stream>>>(p); });
     launch("restrain_atoms", [&] { k_restrain_atoms<<<dim3(cdiv(max_natom, 256), nsys), 256, 0, stream>>>(p); });
     if (any_prestr) launch("prestrain", [&] { k_prestrain<<<nsys, 256, 0, stream>>>(p); });
-    if (any_wpol) launch("watpol", [&] { k_watpol<<<nsys, 1024, watpol_smem, stream>>>(p); });
+    if (any_wpol) {
+      launch("watpol_rank", [&] { k_watpol_rank<<<dim3(MAX_SHELLS, nsys), WPOL_BLOCK, watpol_smem, stream>>>(p); });
+      launch("watpol", [&] { k_watpol_force<<<dim3(cdiv(max_nwat, WPOL_BLOCK), nsys), WPOL_BLOCK, 0, stream>>>(p); });
+    }
     if (any_qq) launch("nb_qq", [&] { k_nb_qq<<<nsys, 128, 0, stream>>>(p); });
     if (any_qb) launch("qbonded", [&] { k_qbonded<<<nsys, 128, 0, stream>>>(p); });
     launch("finalize_energy", [&] { k_finalize_energy<<<cdiv(nsys, 128), 128, 0, stream>>>(p); });
     check_launch("force kernels");
   }
 
+  // CUDA graphs of one step, with and without the list rebuild; kernel
+  // arguments are captured by value, so any change of P drops them.
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  long long graph_launches[2] = {0, 0};
+  bool use_graphs = true;
+
+  void drop_graphs() {
+    for (auto &g : graph)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  }
+
+  bool lists_stale = false;
+
   void step() {
+    int due = lists_due() ? 1 : 0;
+    if (lists_stale) {
+      build_lists(1);
+      lists_stale = false;
+      due = 0;
+    }
+    if (!use_graphs || profiling) { step_kernels(due); istep++; return; }
+    if (!graph[due]) {
+      cudaGraph_t g = nullptr;
+      long long l0 = launches;
+      CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      try {
+        step_kernels(due);
+      } catch (...) {
+        cudaStreamEndCapture(stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      CUDA_TRY(cudaStreamEndCapture(stream, &g));
+      cudaError_t e = cudaGraphInstantiate(&graph[due], g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) { graph[due] = nullptr; fail(QB_ERR_CUDA, std::string("graph instantiation: ") + cudaGetErrorString(e)); }
+      graph_launches[due] = launches - l0;
+      launches = l0;
+    }
+    CUDA_TRY(cudaGraphLaunch(graph[due], stream));
+    launches += graph_launches[due];
+    istep++;
+  }
+
+  // The kernels of one MD step (md_run's loop body, md.f90:4003-4175).
+  void step_kernels(int due) {
     DevPtrs &p = P;
-    if (lists_due()) build_lists(0);
+    if (due) build_lists(0);
     pot_energy();
     launch("leapfrog", [&] { k_leapfrog<<<cdiv(p.natoms_tot, 256), 256, 0, stream>>>(p); });
     if (any_shake && p.nsh3 > 0)
@@ -223,7 +275,6 @@ struct Batch {
     launch("kinetic", [&] { k_kinetic<<<dim3(p.kin_nblk, nsys), KIN_BLOCK, 0, stream>>>(p, 1); });
     launch("finish", [&] { k_finish<<<nsys, 32, 0, stream>>>(p, 1, p.kin_nblk); });
     check_launch("step kernels");
-    istep++;
   }
 
   void sync_status() {
@@ -558,6 +609,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     B.any_lrf |= V.use_LRF != 0;
     if (V.nqat > 0) B.q_states = (!B.any_q || B.q_states == V.nstates) ? V.nstates : 0;
     B.any_q |= V.nqat > 0;
+    B.max_nq = std::max(B.max_nq, V.nqat);
     B.any_shake |= V.shake_constraints > 0;
     B.any_wpol |= S.wpol != 0;
     B.any_prestr |= (V.nrstr_seq + V.nrstr_pos + V.nrstr_dist + V.nrstr_angl + V.nrstr_wall) > 0;
@@ -705,10 +757,18 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   P.EQ = dev_alloc<double>((size_t)n * MAXS * QB_NEQ, o);
   P.hist = nullptr;
   P.hist_cap = 0;
-  B.watpol_smem = (size_t)B.max_nwat * sizeof(double) + (size_t)MAX_SHELLS * B.max_nwat * sizeof(int);
+  {
+    size_t np = 1;
+    while (np < (size_t)B.max_nwat) np <<= 1;
+    B.watpol_smem = np * sizeof(WpolKey);     // sort keys, padded to a power of two
+  }
+  P.wtheta = dev_alloc<double>(std::max(woff, 1), o);
+  P.wshell = dev_alloc<int8_t>(std::max(woff, 1), o);
+  P.wrank = dev_alloc<int>(std::max(woff, 1), o);
+  P.wshn = dev_alloc<int>((size_t)n * MAX_SHELLS, o);
   if (B.any_wpol) {
     if (B.watpol_smem > 200 * 1024) fail(QB_ERR_UNSUPPORTED, "too many waters for the polarisation kernel");
-    CUDA_TRY(cudaFuncSetAttribute(k_watpol, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_watpol_rank, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   }
 }
 
@@ -745,6 +805,7 @@ void ensure_history(Batch &B, int nsteps) {
   }
   B.P.hist = nh;
   B.P.hist_cap = (int)cap;
+  B.drop_graphs();
 }
 
 template <class F>
@@ -808,6 +869,7 @@ int qb_batch_create(qb_handle *const *systems, int n, const qb_options *opt, qb_
     CUDA_TRY(cudaSetDevice(b->b.opt.device));
     if (b->b.opt.precision != QB_FP64 && b->b.opt.precision != QB_MIXED) qb::fail(QB_ERR_ARG, "unknown precision");
     CUDA_TRY(cudaStreamCreateWithFlags(&b->b.stream, cudaStreamNonBlocking));
+    b->b.use_graphs = std::getenv("QB_NO_GRAPHS") == nullptr;
     qb::build(b->b, systems, n);
     // md_run's initial temperature (md.f90:3960-3963)
     qb::k_kinetic<<<dim3(b->b.P.kin_nblk, n), qb::KIN_BLOCK, 0, b->b.stream>>>(b->b.P, 0);
@@ -960,7 +1022,11 @@ static int set_vec(qb_batch *bb, int sys, double4 *dst, const double *in) {
 
 int qb_batch_gradient(qb_batch *b, int sys, double *d) { return get_vec(b, sys, b ? b->b.P.d : nullptr, d); }
 int qb_batch_get_coords(qb_batch *b, int sys, double *x) { return get_vec(b, sys, b ? b->b.P.x : nullptr, x); }
-int qb_batch_set_coords(qb_batch *b, int sys, const double *x) { return set_vec(b, sys, b ? b->b.P.x : nullptr, x); }
+int qb_batch_set_coords(qb_batch *b, int sys, const double *x) {
+  int rc = set_vec(b, sys, b ? b->b.P.x : nullptr, x);
+  if (rc == QB_OK) b->b.lists_stale = true;   // new coordinates: lists and LRF rebuilt before the next step
+  return rc;
+}
 int qb_batch_get_velocities(qb_batch *b, int sys, double *v) { return get_vec(b, sys, b ? b->b.P.v : nullptr, v); }
 int qb_batch_set_velocities(qb_batch *b, int sys, const double *v) { return set_vec(b, sys, b ? b->b.P.v : nullptr, v); }
 

@@ -64,6 +64,10 @@ struct DevPtrs {
   // atoms
   double4 *x, *v, *xx, *d;
   float4 *wrec;              // per-water position records of the water-water kernel
+  double *wtheta;            // per water: dipole angle of the polarisation restraint
+  int8_t *wshell;            // per water: polarisation shell (-1: none)
+  int *wrank;                // per water: rank in its shell
+  int *wshn;                 // [s*MAX_SHELLS + shell] members
   float *crg, *winv;
   double *mass;
   int *iac, *iq, *cgp, *asys;

@@ -102,6 +102,42 @@ __device__ __forceinline__ void lrf_accumulate(R *m, R q, R dx, R dy, R dz) {
   m[19] += f2 * (zz * dz - R(3) * r2 * dz);
 }
 
+// The same sums with the diagonal terms of phi2 and phi3 factored out:
+// m[0..19] as above without them, plus t[0] = sum f0 and t[1..3] = sum
+// f2*r2*d; lrf_fold applies them once at the end (phi2_aa -= t0,
+// phi3_aab -= t_b for a != b, phi3_aaa -= 3 t_a).  22 fewer operations per
+// charge; used by the mixed-precision gather.
+__device__ __forceinline__ void lrf_accumulate_split(float *m, float *t, float q, float dx, float dy, float dz) {
+  float r2 = dx * dx + dy * dy + dz * dz;
+  float rinv = rsqrtf(r2), ri2 = rinv * rinv;
+  float f0 = q * rinv * ri2;
+  m[0] = fmaf(f0, r2, m[0]);
+  m[1] = fmaf(-f0, dx, m[1]); m[2] = fmaf(-f0, dy, m[2]); m[3] = fmaf(-f0, dz, m[3]);
+  t[0] += f0;
+  float f1 = 3.f * f0 * ri2;
+  float ax = f1 * dx, ay = f1 * dy, az = f1 * dz;
+  m[4] = fmaf(ax, dx, m[4]); m[5] = fmaf(ax, dy, m[5]); m[6] = fmaf(ax, dz, m[6]);
+  m[7] = fmaf(ay, dy, m[7]); m[8] = fmaf(ay, dz, m[8]); m[9] = fmaf(az, dz, m[9]);
+  float f2 = -f1 * ri2;
+  float w = f2 * r2;
+  t[1] = fmaf(w, dx, t[1]); t[2] = fmaf(w, dy, t[2]); t[3] = fmaf(w, dz, t[3]);
+  float u = 5.f * f2;
+  float px = u * dx, py = u * dy;
+  float qxx = px * dx, qxy = px * dy, qxz = px * dz, qyy = py * dy, qyz = py * dz, qzz = u * dz * dz;
+  m[10] = fmaf(qxx, dx, m[10]); m[11] = fmaf(qxx, dy, m[11]); m[12] = fmaf(qxx, dz, m[12]);
+  m[13] = fmaf(qxy, dy, m[13]); m[14] = fmaf(qxy, dz, m[14]); m[15] = fmaf(qxz, dz, m[15]);
+  m[16] = fmaf(qyy, dy, m[16]); m[17] = fmaf(qyy, dz, m[17]); m[18] = fmaf(qyz, dz, m[18]);
+  m[19] = fmaf(qzz, dz, m[19]);
+}
+
+__device__ __forceinline__ void lrf_fold(double *m, const double *t) {
+  m[4] -= t[0]; m[7] -= t[0]; m[9] -= t[0];
+  m[10] -= 3. * t[1]; m[11] -= t[2]; m[12] -= t[3];
+  m[13] -= t[1]; m[15] -= t[1];
+  m[16] -= 3. * t[2]; m[17] -= t[3]; m[18] -= t[2];
+  m[19] -= 3. * t[3];
+}
+
 // LRF multipoles of every charge group, gathered (nbpplist_lrf 5448,
 // nbpwlist_lrf 6864, nbwwlist_lrf 8370).  A group g receives the charges of
 // every group h whose switching atoms lie beyond the pair's cut-off but within
@@ -120,7 +156,7 @@ __device__ __forceinline__ void lrf_accumulate(R *m, R q, R dx, R dy, R dz) {
 constexpr int LRF_TILE_G = 128, LRF_TILE_A = 512, LRF_BLOCK = 128;
 
 template <bool MIXED>
-__global__ void __launch_bounds__(LRF_BLOCK) k_lrf_gather(DevPtrs P, int force) {
+__global__ void __launch_bounds__(LRF_BLOCK, MIXED ? 8 : 5) k_lrf_gather(DevPtrs P, int force) {
   using R = typename std::conditional<MIXED, float, double>::type;
   using R4 = typename std::conditional<MIXED, float4, double4>::type;
   int s = blockIdx.y;
@@ -145,10 +181,18 @@ __global__ void __launch_bounds__(LRF_BLOCK) k_lrf_gather(DevPtrs P, int force) 
   const double ox = MIXED ? S.xp[0] : 0.0, oy = MIXED ? S.xp[1] : 0.0, oz = MIXED ? S.xp[2] : 0.0;
   const R ccx = (R)(cx - ox), ccy = (R)(cy - oy), ccz = (R)(cz - oz);
   const bool g_sol = gl < S.ncgp_sol;
-  double m[20];
+  // FP64 totals: registers (FP64 path) or this thread's column in shared memory (mixed)
+  __shared__ double mtot[MIXED ? 24 : 1][MIXED ? LRF_BLOCK : 1];
+  double m[MIXED ? 1 : 20];
   R mt[20];
+  float tt[4];
+  if (MIXED) {
 #pragma unroll
-  for (int k = 0; k < 20; k++) m[k] = 0.0;
+    for (int k = 0; k < 24; k++) mtot[k][threadIdx.x] = 0.0;
+  } else {
+#pragma unroll
+    for (int k = 0; k < 20; k++) m[k] = 0.0;
+  }
   for (int t = 0; t < S.nlrft; t++) {
     int2 tile = P.lrft[S.lrft_off + t];
     int nh = tile.y - tile.x;
@@ -177,6 +221,8 @@ __global__ void __launch_bounds__(LRF_BLOCK) k_lrf_gather(DevPtrs P, int force) 
       if (MIXED) {
 #pragma unroll
         for (int k = 0; k < 20; k++) mt[k] = R(0);
+#pragma unroll
+        for (int k = 0; k < 4; k++) tt[k] = 0.f;
       }
       for (int i = 0; i < nh; i++) {
         double4 hs = hsw[i];
@@ -189,21 +235,35 @@ __global__ void __launch_bounds__(LRF_BLOCK) k_lrf_gather(DevPtrs P, int force) 
         for (int k = 0; k < rg.y; k++) {
           R4 a = hat[rg.x + k];
           if (a.w != R(0)) {
-            if (MIXED) lrf_accumulate<R>(mt, a.w, a.x - ccx, a.y - ccy, a.z - ccz);
+            if (MIXED) lrf_accumulate_split((float *)mt, tt, (float)a.w, (float)(a.x - ccx), (float)(a.y - ccy),
+                                            (float)(a.z - ccz));
             else lrf_accumulate<double>(m, (double)a.w, (double)a.x - cx, (double)a.y - cy, (double)a.z - cz);
           }
         }
       }
       if (MIXED) {
 #pragma unroll
-        for (int k = 0; k < 20; k++) m[k] += (double)mt[k];
+        for (int k = 0; k < 20; k++) mtot[k][threadIdx.x] += (double)mt[k];
+#pragma unroll
+        for (int k = 0; k < 4; k++) mtot[20 + k][threadIdx.x] += (double)tt[k];
       }
     }
   }
   if (active) {
     double *L = P.lrf + (size_t)g * LRF_STRIDE;
+    if (MIXED) {
+      double mm[20], t4[4];
 #pragma unroll
-    for (int k = 0; k < 20; k++) L[3 + k] = m[k];
+      for (int k = 0; k < 20; k++) mm[k] = mtot[k][threadIdx.x];
+#pragma unroll
+      for (int k = 0; k < 4; k++) t4[k] = mtot[20 + k][threadIdx.x];
+      lrf_fold(mm, t4);
+#pragma unroll
+      for (int k = 0; k < 20; k++) L[3 + k] = mm[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < 20; k++) L[3 + k] = m[MIXED ? 0 : k];
+    }
   }
 }
 
@@ -528,6 +588,37 @@ constexpr int WREC_MAX = 5;
 constexpr int WW_BLOCK = 512, WW_WPB = 128;   // threads, waters per block
 constexpr int WW_STAGE_BYTES = 112 * 1024;    // staged records per block: two blocks per SM
 
+// watpol (md.f90:15122), per water: the angle between the water dipole and
+// the radius vector from the restraint centre, and the polarisation shell the
+// O lies in (-1: none, or excluded).
+__device__ __forceinline__ void watpol_angle(const DevPtrs &P, const SysDev &S, int gw, bool excl, double4 xO,
+                                             double4 x1, double4 x2) {
+  int shell = -1;
+  double theta = 0.0;
+  if (!excl) {
+    double rmu[3] = {x1.x + x2.x - 2. * xO.x, x1.y + x2.y - 2. * xO.y, x1.z + x2.z - 2. * xO.z};
+    double rm = sqrt(rmu[0] * rmu[0] + rmu[1] * rmu[1] + rmu[2] * rmu[2]);
+    for (int k = 0; k < 3; k++) rmu[k] /= rm;
+    double rcu[3] = {xO.x - S.xw[0], xO.y - S.xw[1], xO.z - S.xw[2]};
+    double rc = sqrt(rcu[0] * rcu[0] + rcu[1] * rcu[1] + rcu[2] * rcu[2]);
+    for (int k = 0; k < 3; k++) rcu[k] /= rc;
+    double scp = rmu[0] * rcu[0] + rmu[1] * rcu[1] + rmu[2] * rcu[2];
+    if (scp > 1.0) scp = 1.0;
+    if (scp < -1.0) scp = -1.0;
+    theta = acos(scp);
+    const int ns = S.nshell;
+    float inner = S.ws_rout[ns - 1] - S.ws_dr[ns - 1];
+    if (rc > (double)inner) {
+      int is;
+      for (is = ns - 1; is >= 1; is--)
+        if (rc <= (double)S.ws_rout[is]) break;
+      shell = is;
+    }
+  }
+  P.wtheta[gw] = theta;
+  P.wshell[gw] = (int8_t)shell;
+}
+
 template <bool MIXED>
 __global__ void k_pack_waters(DevPtrs P) {
   int s = blockIdx.y;
@@ -536,6 +627,7 @@ __global__ void k_pack_waters(DevPtrs P) {
   if (iw >= S.nwat) return;
   int o = S.aoff + S.nsol + 3 * iw;
   double4 a = P.x[o], b = P.x[o + 1], c = P.x[o + 2];
+  if (S.wpol && S.nshell > 0) watpol_angle(P, S, S.woff + iw, (P.flags[o] & F_EXCL) != 0, a, b, c);
   constexpr int W = WatRec<MIXED>::words;
   float4 *r = P.wrec + (size_t)(S.woff + iw) * W;
   if (MIXED) {
@@ -637,6 +729,7 @@ __device__ __forceinline__ void unpack_mixed(const float4 *r, float *v) {
 template <bool MIXED>
 __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
   extern __shared__ float4 wsm[];
+  __shared__ int2 srange[WW_WPB];          // list slice of each of the block's waters in this chunk
   constexpr int W = WatRec<MIXED>::words;
   int s = blockIdx.y;
   const SysDev &S = P.sys[s];
@@ -654,18 +747,38 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
     const int c0 = c * CW, cn = min(CW, S.nwat - c0);
     __syncthreads();
     for (int t = threadIdx.x; t < cn * W; t += WW_BLOCK) wsm[t] = rec[(size_t)c0 * W + t];
+    for (int t = threadIdx.x; t < i1 - i0; t += WW_BLOCK) {
+      const int *sp = P.ww_sp + (size_t)(S.woff + i0 + t) * P.ww_nch;
+      srange[t] = make_int2(c == 0 ? 0 : sp[c - 1], sp[c]);
+    }
     __syncthreads();
+    // first list entry of the half-warp's next water, fetched one water ahead
+    int jn_next = c0;
+    {
+      const int iw = i0 + hw;
+      if (iw < i1) {
+        const int2 r = srange[iw - i0];
+        if (r.x + hl < r.y) jn_next = P.ww[(size_t)(S.woff + iw) * P.ww_cap + r.x + hl];
+      }
+    }
     for (int iw = i0 + hw; iw < i1; iw += WW_BLOCK / 16) {
       const int gw = S.woff + iw;
-      const int *sp = P.ww_sp + (size_t)gw * P.ww_nch;
-      const int kb = c == 0 ? 0 : sp[c - 1], ke = sp[c];
+      const int kb = srange[iw - i0].x, ke = srange[iw - i0].y;
+      int jn = jn_next;
+      {
+        const int iw2 = iw + WW_BLOCK / 16;
+        jn_next = c0;
+        if (iw2 < i1) {
+          const int2 r = srange[iw2 - i0];
+          if (r.x + hl < r.y) jn_next = P.ww[(size_t)(S.woff + iw2) * P.ww_cap + r.x + hl];
+        }
+      }
       if (kb >= ke) continue;
       const uint16_t *nb = P.ww + (size_t)gw * P.ww_cap;
-      const float4 *ri = rec + (size_t)iw * W;
+      const float4 *ri = (iw >= c0 && iw < c0 + cn) ? wsm + (iw - c0) * W : rec + (size_t)iw * W;
       const int oi = S.aoff + S.nsol + 3 * iw;
       double fd[9];
       int k = kb + hl;
-      int jn = k < ke ? (int)nb[k] : c0;
       if (MIXED) {
         float xi[12];
         unpack_mixed(ri, xi);
@@ -925,110 +1038,153 @@ __global__ void k_nb_qp(DevPtrs P) {
   }
 }
 
-// nonbond_qw_spc (md.f90:11302): one thread per water of the Q-water list,
-// looping over Q atoms; Q-atom gradients are reduced in shared memory.
-template <int NSC>
-__global__ void k_nb_qw(DevPtrs P) {
+// nonbond_qw_spc (md.f90:11302): Q atoms with the listed waters, one thread
+// per water, all Q atoms and states in the thread.  The Q atoms' positions
+// and per-state parameters (charge products with the water O and H in single
+// precision as crg_ow*qcrg, LJ products with the water O, soft-core shifts)
+// are staged in shared memory once per block.  Q-atom gradients are reduced
+// per warp, then per block in shared memory (NQ_SHARED atoms at most; global
+// atomics beyond).
+struct QwState { float qO, qH; double A, B, sc; };
+
+template <int NSC, bool SHQ>
+__global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
+  constexpr int NA = NSC > 0 ? NSC : MAXS;
   int s = blockIdx.y;
   const SysDev &S = P.sys[s];
   __shared__ double fq[NQ_SHARED * 3];
+  __shared__ double4 qx[NQ_SHARED];        // position; w: LJ code
+  __shared__ double2 qab[NQ_SHARED];       // A, B with the water O (same in every state)
+  __shared__ QwState qst[NQ_SHARED * NA];
   if (S.nq == 0) return;
-  const bool shq = S.nq <= NQ_SHARED;
-  for (int t = threadIdx.x; t < NQ_SHARED * 3; t += blockDim.x) fq[t] = 0;
-  __syncthreads();
-  int n = P.st[s].qw_n;
+  const int n = P.st[s].qw_n;
+  if (blockIdx.x * blockDim.x >= n) return;
   const int NS = NSC > 0 ? NSC : S.S, ncol = S.natyps + S.nq;
-  constexpr int NA = NSC > 0 ? NSC : MAXS;
+  const bool shq = SHQ;                    // every system's Q atoms fit the shared tables
+  const int nqs = shq ? S.nq : 0;
+  for (int t = threadIdx.x; t < NQ_SHARED * 3; t += blockDim.x) fq[t] = 0;
+  for (int iq = threadIdx.x; iq < nqs; iq += blockDim.x) {
+    int gq = S.qoff + iq, i = P.iqseq[gq];
+    int lj = P.ljcod[S.ljoff + S.iac_ow * S.natyps + P.iac[i]];
+    double4 x = P.x[i];
+    x.w = (double)lj;
+    qx[iq] = x;
+    qab[iq] = make_double2(P.lja[3 * i + lj - 1] * S.aO[lj - 1], P.ljb[3 * i + lj - 1] * S.bO[lj - 1]);
+    for (int st = 0; st < NS; st++) {
+      QwState q;
+      float c = P.qcrg[gq * MAXS + st];
+      q.qO = S.crg_ow * c;
+      q.qH = S.crg_hw * c;
+      int ti = P.qiac[gq * MAXS + st];
+      q.A = P.qavdw[S.qlib_off + 3 * ti] * S.aO[lj - 1];
+      q.B = P.qbvdw[S.qlib_off + 3 * ti] * S.bO[lj - 1];
+      q.sc = S.qvdw ? P.sc[S.sc_off + ((size_t)iq * ncol + S.iac_ow) * NS + st] : 0.0;
+      qst[iq * NA + st] = q;
+    }
+  }
+  __syncthreads();
   double el[NA], vdw[NA];
 #pragma unroll
   for (int st = 0; st < NA; st++) { el[st] = 0; vdw[st] = 0; }
-  for (int k0 = blockIdx.x * blockDim.x; k0 < n; k0 += gridDim.x * blockDim.x) {
-    int k = k0 + threadIdx.x;
-    bool act = k < n;
-    int j = act ? P.qw[S.qw_off + k] : P.qw[S.qw_off];
-    {
-      double3 xO = ld3(P.x, j), xH1 = ld3(P.x, j + 1), xH2 = ld3(P.x, j + 2);
-      double fw[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-      for (int iq = 0; iq < S.nq; iq++) {
-        double qacc[3] = {0, 0, 0};
-        int gq = S.qoff + iq;
-        int i = P.iqseq[gq];
-        double3 xi = ld3(P.x, i);
-        double dO[3] = {xO.x - xi.x, xO.y - xi.y, xO.z - xi.z};
-        double dH1[3] = {xH1.x - xi.x, xH1.y - xi.y, xH1.z - xi.z};
-        double dH2[3] = {xH2.x - xi.x, xH2.y - xi.y, xH2.z - xi.z};
-        double r2O = dO[0] * dO[0] + dO[1] * dO[1] + dO[2] * dO[2];
-        double rH1 = rsqrt(dH1[0] * dH1[0] + dH1[1] * dH1[1] + dH1[2] * dH1[2]);
-        double rH2 = rsqrt(dH2[0] * dH2[0] + dH2[1] * dH2[1] + dH2[2] * dH2[2]);
-        double r6hc = r2O * r2O * r2O;
-        double rO = rsqrt(r2O);
-        r2O = rO * rO;
-        double r2H1 = rH1 * rH1, r2H2 = rH2 * rH2;
-        double r6sc = r6hc, dvO = 0, dvH1 = 0, dvH2 = 0, Va = 0, Vb = 0;
-        int lj = P.ljcod[S.ljoff + S.iac_ow * S.natyps + P.iac[i]];
-        if (!S.qvdw) {
-          double r6O = 1. / r6hc;
-          Va = P.lja[3 * i + lj - 1] * S.aO[lj - 1] * r6O * r6O;
-          Vb = P.ljb[3 * i + lj - 1] * S.bO[lj - 1] * r6O;
-        }
-        for (int st = 0; st < NS; st++) {
-          if (S.qvdw) {
-            int ti = P.qiac[gq * MAXS + st];
-            double aLJ = P.qavdw[S.qlib_off + 3 * ti], bLJ = P.qbvdw[S.qlib_off + 3 * ti];
-            r6sc = r6hc + P.sc[S.sc_off + ((size_t)iq * ncol + S.iac_ow) * NS + st];
-            Va = aLJ * S.aO[lj - 1] / (r6sc * r6sc);
-            Vb = bLJ * S.bO[lj - 1] / r6sc;
-          }
-          float q = P.qcrg[gq * MAXS + st];
-          double VelO = (double)(S.crg_ow * q) * rO;
-          double VelH1 = (double)(S.crg_hw * q) * rH1;
-          double VelH2 = (double)(S.crg_hw * q) * rH2;
-          double lam = S.lambda[st];
-          dvO += r2O * (-VelO - ((12. * Va - 6. * Vb) * (r6hc / r6sc))) * lam;
-          dvH1 -= r2H1 * VelH1 * lam;
-          dvH2 -= r2H2 * VelH2 * lam;
-          if (act) {
-            el[st] += VelO + VelH1 + VelH2;
-            vdw[st] += Va - Vb;
-          }
-        }
-        double fi[3];
-        for (int c = 0; c < 3; c++) {
-          fi[c] = -(dvO * dO[c] + dvH1 * dH1[c] + dvH2 * dH2[c]);
-          fw[c] += dvO * dO[c];
-          fw[3 + c] += dvH1 * dH1[c];
-          fw[6 + c] += dvH2 * dH2[c];
-        }
-        if (act) { qacc[0] = fi[0]; qacc[1] = fi[1]; qacc[2] = fi[2]; }
-        // Q-atom gradient: warp reduction, then one shared atomic per warp
-        for (int c = 0; c < 3; c++) {
-          double t = warp_sum(qacc[c]);
-          if ((threadIdx.x & 31) == 0 && t != 0.0) {
-            if (shq) atomicAdd(&fq[3 * iq + c], t);
-            else atomicAdd(&P.d[i].x + c, t);
-          }
-        }
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = k < n;
+  const int j = act ? P.qw[S.qw_off + k] : P.qw[S.qw_off];
+  const double3 xO = ld3(P.x, j), xH1 = ld3(P.x, j + 1), xH2 = ld3(P.x, j + 2);
+  double fw[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int iq = 0; iq < S.nq; iq++) {
+    int gq = S.qoff + iq;
+    double4 xi4;
+    int lj;
+    double A0, B0;
+    if (shq) {
+      xi4 = qx[iq];
+      lj = (int)xi4.w;
+      A0 = qab[iq].x; B0 = qab[iq].y;
+    } else {
+      int i = P.iqseq[gq];
+      xi4 = P.x[i];
+      lj = P.ljcod[S.ljoff + S.iac_ow * S.natyps + P.iac[i]];
+      A0 = P.lja[3 * i + lj - 1] * S.aO[lj - 1];
+      B0 = P.ljb[3 * i + lj - 1] * S.bO[lj - 1];
+    }
+    double dO[3] = {xO.x - xi4.x, xO.y - xi4.y, xO.z - xi4.z};
+    double dH1[3] = {xH1.x - xi4.x, xH1.y - xi4.y, xH1.z - xi4.z};
+    double dH2[3] = {xH2.x - xi4.x, xH2.y - xi4.y, xH2.z - xi4.z};
+    double r2O = dO[0] * dO[0] + dO[1] * dO[1] + dO[2] * dO[2];
+    double rH1 = rsqrt(dH1[0] * dH1[0] + dH1[1] * dH1[1] + dH1[2] * dH1[2]);
+    double rH2 = rsqrt(dH2[0] * dH2[0] + dH2[1] * dH2[1] + dH2[2] * dH2[2]);
+    double r6hc = r2O * r2O * r2O;
+    double rO = rsqrt(r2O);
+    r2O = rO * rO;
+    double r2H1 = rH1 * rH1, r2H2 = rH2 * rH2;
+    double dvO = 0, dvH1 = 0, dvH2 = 0, Va = 0, Vb = 0;
+    if (!S.qvdw) {
+      double r6O = 1. / r6hc;
+      Va = A0 * r6O * r6O;
+      Vb = B0 * r6O;
+    }
+#pragma unroll
+    for (int st = 0; st < NA; st++) {
+      if (st >= NS) break;
+      QwState q;
+      if (shq) q = qst[iq * NA + st];
+      else {
+        float c = P.qcrg[gq * MAXS + st];
+        q.qO = S.crg_ow * c; q.qH = S.crg_hw * c;
+        int ti = P.qiac[gq * MAXS + st];
+        q.A = P.qavdw[S.qlib_off + 3 * ti] * S.aO[lj - 1];
+        q.B = P.qbvdw[S.qlib_off + 3 * ti] * S.bO[lj - 1];
+        q.sc = S.qvdw ? P.sc[S.sc_off + ((size_t)iq * ncol + S.iac_ow) * NS + st] : 0.0;
       }
-      if (act)
-        for (int a = 0; a < 3; a++) {
-          double4 dd = P.d[j + a];
-          dd.x += fw[3 * a]; dd.y += fw[3 * a + 1]; dd.z += fw[3 * a + 2];
-          P.d[j + a] = dd;
-        }
+      double r6sc = r6hc;
+      if (S.qvdw) {
+        r6sc = r6hc + q.sc;
+        Va = q.A / (r6sc * r6sc);
+        Vb = q.B / r6sc;
+      }
+      double VelO = (double)q.qO * rO;
+      double VelH1 = (double)q.qH * rH1;
+      double VelH2 = (double)q.qH * rH2;
+      double lam = S.lambda[st];
+      dvO += r2O * (-VelO - ((12. * Va - 6. * Vb) * (r6hc / r6sc))) * lam;
+      dvH1 -= r2H1 * VelH1 * lam;
+      dvH2 -= r2H2 * VelH2 * lam;
+      if (act) {
+        el[st] += VelO + VelH1 + VelH2;
+        vdw[st] += Va - Vb;
+      }
+    }
+    double qacc[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      qacc[c] = act ? -(dvO * dO[c] + dvH1 * dH1[c] + dvH2 * dH2[c]) : 0.0;
+      fw[c] += dvO * dO[c];
+      fw[3 + c] += dvH1 * dH1[c];
+      fw[6 + c] += dvH2 * dH2[c];
+    }
+    // Q-atom gradient: warp reduction, then one shared (or global) atomic per warp
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      double t = warp_sum(qacc[c]);
+      if ((threadIdx.x & 31) == 0 && t != 0.0) {
+        if (shq) atomicAdd(&fq[3 * iq + c], t);
+        else atomicAdd(&P.d[P.iqseq[gq]].x + c, t);
+      }
     }
   }
+  if (act)
+    for (int a = 0; a < 3; a++) {
+      double4 dd = P.d[j + a];
+      dd.x += fw[3 * a]; dd.y += fw[3 * a + 1]; dd.z += fw[3 * a + 2];
+      P.d[j + a] = dd;
+    }
   for (int st = 0; st < NS; st++) {
     warp_add(&P.EQ[((size_t)s * MAXS + st) * QB_NEQ + QB_EQ_QW_EL], el[st]);
     warp_add(&P.EQ[((size_t)s * MAXS + st) * QB_NEQ + QB_EQ_QW_VDW], vdw[st]);
   }
   __syncthreads();
-  if (shq)
-    for (int t = threadIdx.x; t < S.nq * 3; t += blockDim.x)
-      if (fq[t] != 0.0) {
-        int i = P.iqseq[S.qoff + t / 3];
-        double *dp = &P.d[i].x + (t % 3);
-        atomicAdd(dp, fq[t]);
-      }
+  for (int t = threadIdx.x; t < nqs * 3; t += blockDim.x)
+    if (fq[t] != 0.0) atomicAdd(&P.d[P.iqseq[S.qoff + t / 3]].x + (t % 3), fq[t]);
 }
 
 // nonbond_qq (md.f90:10763): Q-Q and Q-to-bonded-neighbour pairs, all states.
@@ -1578,120 +1734,146 @@ __global__ void k_prestrain(DevPtrs P) {
   }
 }
 
-// watpol (md.f90:15122): water dipole orientation restraint.  One block per
-// system.  Waters are assigned to shells by O radius, ordered within a shell
-// by angle theta (ties by water index, as the reference's selection sort
-// does), and restrained to theta_0(rank).
-__global__ void __launch_bounds__(1024, 1) k_watpol(DevPtrs P) {
+// watpol (md.f90:15122): water polarisation restraint, in two kernels.
+// k_watpol_rank, one block per (shell, system): the shell's members (angles
+// and shells from k_pack_waters) are sorted by (angle, water index) with a
+// bitonic network in shared memory, so a member's position is its rank in the
+// reference's selection order (ties by water index).  The block also keeps
+// the shell's running averages and updates theta_corr every 100 steps, in
+// the reference's order (update first, then this step's average).
+// k_watpol_force, one thread per water: target angle from the rank, restraint
+// energy and the force on the water dipole.
+struct WpolKey { double th; int iw, pad; };
+
+__device__ __forceinline__ bool wpol_less(const WpolKey &a, const WpolKey &b) {
+  return a.th < b.th || (a.th == b.th && a.iw < b.iw);
+}
+
+constexpr int WPOL_BLOCK = 256;
+
+__global__ void __launch_bounds__(WPOL_BLOCK) k_watpol_rank(DevPtrs P) {
   extern __shared__ unsigned char smem[];
-  int s = blockIdx.x;
+  const int is = blockIdx.x, s = blockIdx.y;
   const SysDev &S = P.sys[s];
-  if (!S.wpol || S.nshell == 0) return;
-  const int nw = S.nwat, ns = S.nshell;
-  double *theta = (double *)smem;
-  int *list = (int *)(theta + nw);        // members of each shell, [ns][nw]
-  __shared__ int cnt[MAX_SHELLS];
+  if (!S.wpol || is >= S.nshell) return;
+  const int nw = S.nwat;
+  __shared__ int cnt;
   __shared__ double shsum[32];
-  const double pi = dev_pi();
-  if (threadIdx.x < MAX_SHELLS) cnt[threadIdx.x] = 0;
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) cnt = 0;
   __syncthreads();
-  for (int iw = threadIdx.x; iw < nw; iw += blockDim.x) {
-    int i = S.aoff + S.nsol + 3 * iw;
-    theta[iw] = 0.0;
-    if (P.flags[i] & F_EXCL) continue;
-    double3 xO = ld3(P.x, i), x1 = ld3(P.x, i + 1), x2 = ld3(P.x, i + 2);
-    double rmu[3] = {x1.x + x2.x - 2. * xO.x, x1.y + x2.y - 2. * xO.y, x1.z + x2.z - 2. * xO.z};
-    double rm = sqrt(rmu[0] * rmu[0] + rmu[1] * rmu[1] + rmu[2] * rmu[2]);
-    for (int k = 0; k < 3; k++) rmu[k] /= rm;
-    double rcu[3] = {xO.x - S.xw[0], xO.y - S.xw[1], xO.z - S.xw[2]};
-    double rc = sqrt(rcu[0] * rcu[0] + rcu[1] * rcu[1] + rcu[2] * rcu[2]);
-    for (int k = 0; k < 3; k++) rcu[k] /= rc;
-    double scp = rmu[0] * rcu[0] + rmu[1] * rcu[1] + rmu[2] * rcu[2];
-    if (scp > 1.0) scp = 1.0;
-    if (scp < -1.0) scp = -1.0;
-    theta[iw] = acos(scp);
-    float inner = S.ws_rout[ns - 1] - S.ws_dr[ns - 1];
-    if (rc > (double)inner) {
-      int is;
-      for (is = ns - 1; is >= 1; is--)
-        if (rc <= (double)S.ws_rout[is]) break;
-      int k = atomicAdd(&cnt[is], 1);
-      list[is * nw + k] = iw;
+  const int8_t *wsh = P.wshell + S.woff;
+  const double *wth = P.wtheta + S.woff;
+  WpolKey *key = (WpolKey *)smem;
+  for (int w0 = 0; w0 < nw; w0 += WPOL_BLOCK) {
+    const int iw = w0 + threadIdx.x;
+    const bool mine = iw < nw && wsh[iw] == is;
+    const unsigned bal = __ballot_sync(FULL, mine);
+    int base = 0;
+    if (lane == 0 && bal) base = atomicAdd(&cnt, __popc(bal));
+    base = __shfl_sync(FULL, base, 0);
+    if (mine) {
+      WpolKey k;
+      k.th = wth[iw]; k.iw = iw; k.pad = 0;
+      key[base + __popc(bal & ((1u << lane) - 1u))] = k;
     }
   }
   __syncthreads();
-  SysState &st = P.st[s];
-  if (threadIdx.x == 0 && st.istep != 0 && st.istep % 100 == 0) {
-    for (int is = 0; is < ns; is++) {
+  const int n = cnt;
+  int np = 1;
+  while (np < n) np <<= 1;
+  for (int t = n + threadIdx.x; t < np; t += WPOL_BLOCK) {
+    WpolKey k;
+    k.th = 1e300; k.iw = 0x7fffffff; k.pad = 0;      // sorts after every member
+    key[t] = k;
+  }
+  __syncthreads();
+  for (int kk = 2; kk <= np; kk <<= 1)
+    for (int j = kk >> 1; j > 0; j >>= 1) {
+      for (int t = threadIdx.x; t < np; t += WPOL_BLOCK) {
+        const int u = t ^ j;
+        if (u > t) {
+          WpolKey a = key[t], b = key[u];
+          const bool up = (t & kk) == 0;
+          if (up ? wpol_less(b, a) : wpol_less(a, b)) { key[t] = b; key[u] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  double tsum = 0;
+  for (int r = threadIdx.x; r < n; r += WPOL_BLOCK) {
+    P.wrank[S.woff + key[r].iw] = r;
+    tsum += key[r].th;
+  }
+  double tot = block_sum(tsum, shsum);
+  if (threadIdx.x == 0) {
+    SysState &st = P.st[s];
+    if (st.istep != 0 && st.istep % 100 == 0) {
       st.avtheta[is] = st.avtheta[is] / (float)100;
       st.avn_insh[is] = st.avn_insh[is] / (float)100;
       st.theta_corr[is] = st.theta_corr[is] + st.avtheta[is] - acosf(S.ws_cstb[is]);
       st.avtheta[is] = 0.0f;
       st.avn_insh[is] = 0.0f;
     }
-  }
-  __syncthreads();
-  double epol = 0;
-  for (int is = 0; is < ns; is++) {
-    int n = cnt[is];
-    double tsum = 0;
-    float tc = st.theta_corr[is];
-    float cstb = S.ws_cstb[is];
-    for (int m = threadIdx.x; m < n; m += blockDim.x) {
-      int iw = list[is * nw + m];
-      double th = theta[iw];
-      int rank = 0;
-      for (int u = 0; u < n; u++) {
-        int jw = list[is * nw + u];
-        double tj = theta[jw];
-        rank += (tj < th || (tj == th && jw < iw)) ? 1 : 0;
-      }
-      float arg = 1.0f + (1.0f - 2.0f * (float)(rank + 1)) / (float)n;
-      double th0 = (double)acosf(arg);
-      th0 = th0 - 3. * sin(th0) * (double)cstb / 2.;
-      if (th0 < 0.0) th0 = 0.0;
-      if (th0 > pi) th0 = pi;
-      tsum += th;
-      double dth = th - th0 + (double)tc;
-      epol += 0.5 * S.fkwpol * dth * dth;
-      double dv = S.fkwpol * dth;
-      int i = S.aoff + S.nsol + 3 * iw;
-      double3 xO = ld3(P.x, i), x1 = ld3(P.x, i + 1), x2 = ld3(P.x, i + 2);
-      double rmu[3] = {x1.x + x2.x - 2. * xO.x, x1.y + x2.y - 2. * xO.y, x1.z + x2.z - 2. * xO.z};
-      double rm = sqrt(rmu[0] * rmu[0] + rmu[1] * rmu[1] + rmu[2] * rmu[2]);
-      for (int k = 0; k < 3; k++) rmu[k] /= rm;
-      double rcu[3] = {xO.x - S.xw[0], xO.y - S.xw[1], xO.z - S.xw[2]};
-      double rc = sqrt(rcu[0] * rcu[0] + rcu[1] * rcu[1] + rcu[2] * rcu[2]);
-      for (int k = 0; k < 3; k++) rcu[k] /= rc;
-      double scp = rmu[0] * rcu[0] + rmu[1] * rcu[1] + rmu[2] * rcu[2];
-      if (scp > 1.0) scp = 1.0;
-      if (scp < -1.0) scp = -1.0;
-      double f0 = sin(acos(scp));
-      if (fabs(f0) < 1.e-12) f0 = 1.e-12;
-      f0 = -1.0 / f0;
-      f0 = dv * f0;
-      double gO[3], gH[3];
-      for (int k = 0; k < 3; k++) {
-        double f1 = (rcu[k] - rmu[k] * scp) / rm;
-        double f2 = (rmu[k] - rcu[k] * scp) / rc;
-        gO[k] = f0 * (-2. * f1 + f2);
-        gH[k] = f0 * f1;
-      }
-      double4 d0 = P.d[i], d1 = P.d[i + 1], d2 = P.d[i + 2];
-      d0.x += gO[0]; d0.y += gO[1]; d0.z += gO[2];
-      d1.x += gH[0]; d1.y += gH[1]; d1.z += gH[2];
-      d2.x += gH[0]; d2.y += gH[1]; d2.z += gH[2];
-      P.d[i] = d0; P.d[i + 1] = d1; P.d[i + 2] = d2;
-    }
-    double tot = block_sum(tsum, shsum);
-    if (threadIdx.x == 0 && n > 0) {
+    if (n > 0) {
       st.avtheta[is] = (float)((double)st.avtheta[is] + tot / (double)(float)n);
       st.avn_insh[is] = st.avn_insh[is] + (float)n;
     }
-    __syncthreads();
+    P.wshn[s * MAX_SHELLS + is] = n;
   }
-  double et = block_sum(epol, shsum);
-  if (threadIdx.x == 0) atomicAdd(&P.E[s * QB_NE + QB_E_RST_WATER_POL], et);
+}
+
+__global__ void __launch_bounds__(WPOL_BLOCK) k_watpol_force(DevPtrs P) {
+  const int s = blockIdx.y;
+  const SysDev &S = P.sys[s];
+  if (!S.wpol || S.nshell == 0) return;
+  const int iw = blockIdx.x * WPOL_BLOCK + threadIdx.x;
+  double epol = 0;
+  const int is = iw < S.nwat ? (int)P.wshell[S.woff + iw] : -1;
+  if (is >= 0) {
+    const double pi = dev_pi();
+    const SysState &st = P.st[s];
+    const int n = P.wshn[s * MAX_SHELLS + is], rank = P.wrank[S.woff + iw];
+    const double th = P.wtheta[S.woff + iw];
+    const float tc = st.theta_corr[is];
+    const float cstb = S.ws_cstb[is];
+    float arg = 1.0f + (1.0f - 2.0f * (float)(rank + 1)) / (float)n;
+    double th0 = (double)acosf(arg);
+    th0 = th0 - 3. * sin(th0) * (double)cstb / 2.;
+    if (th0 < 0.0) th0 = 0.0;
+    if (th0 > pi) th0 = pi;
+    double dth = th - th0 + (double)tc;
+    epol = 0.5 * S.fkwpol * dth * dth;
+    double dv = S.fkwpol * dth;
+    int i = S.aoff + S.nsol + 3 * iw;
+    double3 xO = ld3(P.x, i), x1 = ld3(P.x, i + 1), x2 = ld3(P.x, i + 2);
+    double rmu[3] = {x1.x + x2.x - 2. * xO.x, x1.y + x2.y - 2. * xO.y, x1.z + x2.z - 2. * xO.z};
+    double rm = sqrt(rmu[0] * rmu[0] + rmu[1] * rmu[1] + rmu[2] * rmu[2]);
+    for (int c = 0; c < 3; c++) rmu[c] /= rm;
+    double rcu[3] = {xO.x - S.xw[0], xO.y - S.xw[1], xO.z - S.xw[2]};
+    double rc = sqrt(rcu[0] * rcu[0] + rcu[1] * rcu[1] + rcu[2] * rcu[2]);
+    for (int c = 0; c < 3; c++) rcu[c] /= rc;
+    double scp = rmu[0] * rcu[0] + rmu[1] * rcu[1] + rmu[2] * rcu[2];
+    if (scp > 1.0) scp = 1.0;
+    if (scp < -1.0) scp = -1.0;
+    double f0 = sin(th);                 // th = acos(scp) of the same clamped scp
+    if (fabs(f0) < 1.e-12) f0 = 1.e-12;
+    f0 = -1.0 / f0;
+    f0 = dv * f0;
+    double gO[3], gH[3];
+    for (int c = 0; c < 3; c++) {
+      double f1 = (rcu[c] - rmu[c] * scp) / rm;
+      double f2 = (rmu[c] - rcu[c] * scp) / rc;
+      gO[c] = f0 * (-2. * f1 + f2);
+      gH[c] = f0 * f1;
+    }
+    double4 d0 = P.d[i], d1 = P.d[i + 1], d2 = P.d[i + 2];
+    d0.x += gO[0]; d0.y += gO[1]; d0.z += gO[2];
+    d1.x += gH[0]; d1.y += gH[1]; d1.z += gH[2];
+    d2.x += gH[0]; d2.y += gH[1]; d2.z += gH[2];
+    P.d[i] = d0; P.d[i + 1] = d1; P.d[i + 2] = d2;
+  }
+  warp_add(&P.E[s * QB_NE + QB_E_RST_WATER_POL], epol);
 }
 
 // --------------------------------------------------------------- dynamics

@@ -188,3 +188,23 @@ def test_mixed_sizes_in_one_batch(synthetic, oracle):
         Eo, EQo = o.energy_vectors()
         assert_energies(Eg, EQg, Eo, EQo)
         assert grad_err(b.gradient(k), o.gradient()) < G_TOL
+
+
+def test_graph_replay_matches_direct_launches(synthetic, monkeypatch):
+    """Steps replayed from captured CUDA graphs (the default) against the same
+    kernels launched one by one: same records, same coordinates (to FP64
+    atomic-order noise)."""
+    inp = synthetic["c1"].inp
+    runs = []
+    for env in (None, "1"):
+        if env:
+            monkeypatch.setenv("QB_NO_GRAPHS", env)
+        s = System.open(inp, lambdas=(0.5, 0.5), seed=3)
+        b = Batch([s], precision=FP64)
+        b.run(60)          # crosses two list rebuilds
+        steps, E, EQ = b.history(0, 0)
+        runs.append((steps, E, EQ, b.coords(0)))
+    (s0, E0, Q0, x0), (s1, E1, Q1, x1) = runs
+    assert list(s0) == list(s1)
+    assert np.max(np.abs(E0 - E1)) < 1e-6 and np.max(np.abs(Q0 - Q1)) < 1e-6
+    assert np.max(np.abs(x0 - x1)) < 1e-8

@@ -59,7 +59,7 @@ struct Batch {
   cudaStream_t stream = nullptr;
   int NB = 1;
   long long istep = 0;
-  int max_natom = 0, max_nwat = 0, max_ncgp = 0, max_ncgp_sol = 0, max_terms = 0, max_pp = 0, max_ncgp_sol_w = 0, max_qp = 0;
+  int max_natom = 0, max_units = 0, max_nwat = 0, max_ncgp = 0, max_ncgp_sol = 0, max_terms = 0, max_pp = 0, max_ncgp_sol_w = 0, max_qp = 0;
   bool any_lrf = false, any_q = false, any_shake = false, any_wpol = false, any_prestr = false, any_qq = false,
        any_qb = false;
   size_t watpol_smem = 0;
@@ -167,7 +167,7 @@ struct Batch {
     if (max_pp > 0)
       launch("nb_pp", [&] { k_nb_pp<<<dim3(std::min(cdiv(max_pp, 256), 64), nsys), 256, 0, stream>>>(p); });
     if (max_ncgp_sol_w > 0)
-      launch("nb_pw", [&] { k_nb_pw<<<dim3(max_ncgp_sol_w, nsys), PW_BLOCK, 0, stream>>>(p); });
+      launch("nb_pw", [&] { k_nb_pw<<<dim3(cdiv(p.pwg_cap, PW_BLOCK), max_ncgp_sol_w, nsys), PW_BLOCK, 0, stream>>>(p); });
     if (any_q && max_qp > 0)
       launch("nb_qp", [&] {
         dim3 g(std::min(cdiv(max_qp, 256), 32), nsys);
@@ -202,11 +202,9 @@ struct Batch {
         }
       });
     }
-    if (any_lrf)
-      launch("lrf_taylor", [&] { k_lrf_taylor<<<dim3(cdiv(max_natom, 256), nsys), 256, 0, stream>>>(p); });
     if (max_terms > 0)
       launch("bonded", [&] { k_bonded<<<dim3(cdiv(max_terms, 256), nsys), 256, 0, stream>>>(p); });
-    launch("restrain_atoms", [&] { k_restrain_atoms<<<dim3(cdiv(max_natom, 256), nsys), 256, 0, stream>>>(p); });
+    launch("atom_terms", [&] { k_atom_terms<<<dim3(cdiv(max_units, 128), nsys), 128, 0, stream>>>(p); });
     if (any_prestr) launch("prestrain", [&] { k_prestrain<<<nsys, 256, 0, stream>>>(p); });
     if (any_wpol) {
       launch("watpol_rank", [&] { k_watpol_rank<<<dim3(MAX_SHELLS, nsys), WPOL_BLOCK, watpol_smem, stream>>>(p); });
@@ -214,7 +212,6 @@ struct Batch {
     }
     if (any_qq) launch("nb_qq", [&] { k_nb_qq<<<nsys, 128, 0, stream>>>(p); });
     if (any_qb) launch("qbonded", [&] { k_qbonded<<<nsys, 128, 0, stream>>>(p); });
-    launch("finalize_energy", [&] { k_finalize_energy<<<cdiv(nsys, 128), 128, 0, stream>>>(p); });
     check_launch("force kernels");
   }
 
@@ -272,8 +269,7 @@ struct Batch {
       launch("shake", [&] { k_shake3<<<cdiv(p.nsh3, 128), 128, 0, stream>>>(p); });
     if (any_shake && p.nshg > 0)
       launch("shake_general", [&] { k_shake_general<<<p.nshg, SHG_BLOCK, p.shg_smem, stream>>>(p); });
-    launch("kinetic", [&] { k_kinetic<<<dim3(p.kin_nblk, nsys), KIN_BLOCK, 0, stream>>>(p, 1); });
-    launch("finish", [&] { k_finish<<<nsys, 32, 0, stream>>>(p, 1, p.kin_nblk); });
+    launch("finish", [&] { k_finish<<<nsys, 32, 0, stream>>>(p, 1); });
     check_launch("step kernels");
   }
 
@@ -320,6 +316,8 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   std::vector<int2> exl, l14l;
   std::vector<int> cg_first, cg_last, cg_sw, cg_atoms, cg_sys;
   std::vector<int2> lrft;
+  std::vector<PwAtom> pwa;
+  std::vector<int> pwg_off;
   std::vector<int> iqseq, qiac;
   std::vector<float> qcrg;
   std::vector<double> qavdw, qbvdw, sc, qq_el;
@@ -359,6 +357,8 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     S.qoff = (int)iqseq.size(); S.nq = V.nqat; S.S = V.nstates; S.natyps = V.natyps;
     S.ljoff = (int)ljcod.size(); S.qlib_off = (int)qavdw.size(); S.sc_off = (int)sc.size();
     S.qconn_off = (int)qconn.size();
+    std::vector<char> shaken(V.natom, 0);
+    for (int c = 0; c < V.shake_constraints; c++) shaken[V.shake_i[c]] = shaken[V.shake_j[c]] = 1;
     for (int i = 0; i < V.natom; i++) {
       x.push_back(make_double4(V.x0[3 * i], V.x0[3 * i + 1], V.x0[3 * i + 2], 0));
       v.push_back(make_double4(V.v0[3 * i], V.v0[3 * i + 1], V.v0[3 * i + 2], 0));
@@ -372,7 +372,8 @@ void build(Batch &B, qb_handle *const *hs, int n) {
       iq.push_back(V.iqatom[i]);
       cgp.push_back(S.coff + V.iwhich_cgp[i]);
       asys.push_back(s);
-      flags.push_back((V.excl[i] ? F_EXCL : 0) | (V.shell[i] ? F_SHELL : 0) | (V.heavy[i] ? F_HEAVY : 0));
+      flags.push_back((V.excl[i] ? F_EXCL : 0) | (V.shell[i] ? F_SHELL : 0) | (V.heavy[i] ? F_HEAVY : 0) |
+                      (shaken[i] ? F_SHAKE : 0));
       lx.push_back(i < V.nat_solute ? V.listex_bits[i] : 0u);
       l14.push_back(i < V.nat_solute ? V.list14_bits[i] : 0u);
     }
@@ -596,9 +597,34 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     }
     S.pp_off = (int)pp_tot; pp_tot += S.pp_cap;
     S.csoff = ncgp_sol_tot; ncgp_sol_tot += V.ncgp_solute;
+    // solute-water tables: each solute group's non-Q atoms with their charge
+    // products (single precision, as crg(i)*crg(j)) and LJ products with the
+    // water O and H types
+    for (int ig = 0; ig < V.ncgp_solute; ig++) {
+      pwg_off.push_back((int)pwa.size());
+      if (V.nwat == 0) continue;
+      const int o = V.nat_solute;            // first water O; H is o + 1
+      const int to = V.iac[o], th = V.iac[o + 1];
+      for (int a = V.cgp_first[ig]; a <= V.cgp_last[ig]; a++) {
+        const int i = V.cgpatom[a];
+        if (V.iqatom[i] >= 0) continue;
+        const int ti = V.iac[i];
+        const int lo = V.ljcod[ti * V.natyps + to], lh = V.ljcod[ti * V.natyps + th];
+        PwAtom r;
+        r.lj = make_double4(V.type_avdw[3 * ti + lo - 1] * V.type_avdw[3 * to + lo - 1],
+                            V.type_bvdw[3 * ti + lo - 1] * V.type_bvdw[3 * to + lo - 1],
+                            V.type_avdw[3 * ti + lh - 1] * V.type_avdw[3 * th + lh - 1],
+                            V.type_bvdw[3 * ti + lh - 1] * V.type_bvdw[3 * th + lh - 1]);
+        r.q = make_float2(V.crg[i] * V.crg[o], V.crg[i] * V.crg[o + 1]);
+        r.atom = aoff + i;
+        r.pad = 0;
+        pwa.push_back(r);
+      }
+    }
     S.qp_off = (int)qp_tot; qp_tot += S.qp_cap;
     S.qw_off = (int)qw_tot; qw_tot += S.qw_cap;
     B.max_natom = std::max(B.max_natom, V.natom);
+    B.max_units = std::max(B.max_units, V.nat_solute + V.nwat);
     B.max_nwat = std::max(B.max_nwat, V.nwat);
     B.max_ncgp_sol = std::max(B.max_ncgp_sol, V.ncgp_solute);
     B.max_ncgp = std::max(B.max_ncgp, V.ncgp);
@@ -737,6 +763,9 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   P.pwg_cap = pwg_cap;
   P.pwg = dev_alloc<uint16_t>((size_t)std::max(ncgp_sol_tot, 1) * pwg_cap, o);
   P.pwg_n = dev_alloc<int>(std::max(ncgp_sol_tot, 1), o);
+  pwg_off.push_back((int)pwa.size());
+  P.pwa = dev_upload(pwa, o);
+  P.pwg_off = dev_upload(pwg_off, o);
   P.qp = dev_alloc<int4>(qp_tot, o); P.qw = dev_alloc<int>(qw_tot, o);
   // water-water staging chunk: a multiple of 32 waters, two blocks per SM
   const int rec_words = B.opt.precision == QB_MIXED ? WatRec<true>::words : WatRec<false>::words;
@@ -752,16 +781,12 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
   P.kin_nblk = std::max(1, (B.max_natom + KIN_BLOCK - 1) / KIN_BLOCK);
-  P.kin_part = dev_alloc<double>((size_t)n * P.kin_nblk * 4, o);
+  P.kin = dev_alloc<double>((size_t)n * 4, o);
   P.E = dev_alloc<double>((size_t)n * QB_NE, o);
   P.EQ = dev_alloc<double>((size_t)n * MAXS * QB_NEQ, o);
   P.hist = nullptr;
   P.hist_cap = 0;
-  {
-    size_t np = 1;
-    while (np < (size_t)B.max_nwat) np <<= 1;
-    B.watpol_smem = np * sizeof(WpolKey);     // sort keys, padded to a power of two
-  }
+  B.watpol_smem = (size_t)B.max_nwat * (sizeof(double) + sizeof(int));   // member angles and indices
   P.wtheta = dev_alloc<double>(std::max(woff, 1), o);
   P.wshell = dev_alloc<int8_t>(std::max(woff, 1), o);
   P.wrank = dev_alloc<int>(std::max(woff, 1), o);
@@ -872,8 +897,8 @@ int qb_batch_create(qb_handle *const *systems, int n, const qb_options *opt, qb_
     b->b.use_graphs = std::getenv("QB_NO_GRAPHS") == nullptr;
     qb::build(b->b, systems, n);
     // md_run's initial temperature (md.f90:3960-3963)
-    qb::k_kinetic<<<dim3(b->b.P.kin_nblk, n), qb::KIN_BLOCK, 0, b->b.stream>>>(b->b.P, 0);
-    qb::k_finish<<<n, 32, 0, b->b.stream>>>(b->b.P, 0, b->b.P.kin_nblk);
+    qb::k_kinetic<<<dim3(b->b.P.kin_nblk, n), qb::KIN_BLOCK, 0, b->b.stream>>>(b->b.P);
+    qb::k_finish<<<n, 32, 0, b->b.stream>>>(b->b.P, 0);
     b->b.check_launch("initial temperature");
     CUDA_TRY(cudaStreamSynchronize(b->b.stream));
   });
@@ -963,6 +988,8 @@ int qb_batch_final_energy(qb_batch *bb) {
     Batch &B = bb->b;
     B.build_lists(1);
     B.pot_energy();
+    qb::k_finish<<<B.nsys, 32, 0, B.stream>>>(B.P, 2);
+    B.check_launch("energy sums");
     B.sync_status();
   });
 }

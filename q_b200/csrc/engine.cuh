@@ -7,6 +7,8 @@
 #pragma once
 #include <cstdint>
 
+#include <cuda_runtime.h>
+
 #include "qb.h"
 
 namespace qb {
@@ -18,7 +20,16 @@ constexpr int MAXS = QB_MAX_STATES;
 constexpr int LRF_STRIDE = 24;
 constexpr int MAX_SHELLS = 4;
 constexpr int NQ_SHARED = 64;    // Q atoms whose water forces are reduced in shared memory
-enum AtomFlags : uint8_t { F_EXCL = 1, F_SHELL = 2, F_HEAVY = 4 };
+enum AtomFlags : uint8_t { F_EXCL = 1, F_SHELL = 2, F_HEAVY = 4, F_SHAKE = 8 };   // F_SHAKE: in a SHAKE constraint
+
+// A non-Q atom of a solute charge group with its interaction parameters for
+// the water O and H sites: LJ products A(O), B(O), A(H), B(H) and single
+// precision charge products q(O), q(H).
+struct PwAtom {
+  double4 lj;
+  float2 q;
+  int atom, pad;
+};
 
 // Per-system record (read-only on the device during a run).
 struct SysDev {
@@ -122,13 +133,15 @@ struct DevPtrs {
   int4 *pp;                                // i, j, lj
   uint16_t *pwg;                           // [solute group*pwg_cap + k] local water index
   int *pwg_n, pwg_cap;                     // waters listed per solute group
+  struct PwAtom *pwa;                      // non-Q atoms of each solute group (static)
+  int *pwg_off;                            // [solute group] first entry in pwa; one extra at the end
   int4 *qp;                                // gq, j, lj, qlj
   int *qw;                                 // water O atoms
   uint16_t *ww;                            // [gw*ww_cap + k] local water index
   int *ww_n, *ww_sp;                       // count per water; [gw*ww_nch + c] count below chunk c's end
   int ww_cap, ww_chunk, ww_nch;
   // energies
-  double *kin_part;                        // [(s*kin_nblk + block)*4] kinetic-energy partial sums
+  double *kin;                             // [s*4] kinetic energy of this step: solute all, free, solvent all, free
   int kin_nblk;
   double *E;                               // [s*QB_NE]
   double *EQ;                              // [(s*MAXS + st)*QB_NEQ]

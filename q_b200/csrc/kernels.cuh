@@ -871,102 +871,60 @@ __global__ void k_nb_pp(DevPtrs P) {
   warp_add(&P.E[s * QB_NE + QB_E_PP_VDW], vdw);
 }
 
-// nonbond_pw (md.f90:10631) over the group list: block per solute charge
-// group (blockIdx.x) of system blockIdx.y, one thread per listed water.  The
-// group's non-Q atoms are staged in shared memory with their charge products
-// (single precision, as crg(i)*crg(j)) and LJ products for the water O and H
-// types.  Each thread keeps its water's 9 gradient components in registers
-// and adds them with atomics once; the solute atoms' gradients are reduced
-// per warp into shared memory and written once by the block, which owns them.
-constexpr int PW_BLOCK = 128, PW_MAXA = 32;
+// nonbond_pw (md.f90:10631) over the group list: one thread per (listed
+// water, solute charge group); grid (water chunks, solute groups, systems).
+// The group's non-Q atoms and their parameters for the water O and H sites
+// (charge products in single precision, as crg(i)*crg(j); LJ products) are
+// static tables read as broadcasts.  Each thread adds its water's 9 gradient
+// components with atomics once; each solute atom's gradient is reduced over
+// the warp and added with one atomic per warp.
+constexpr int PW_BLOCK = 128;
 
 __global__ void __launch_bounds__(PW_BLOCK) k_nb_pw(DevPtrs P) {
-  int s = blockIdx.y;
+  const int s = blockIdx.z;
   const SysDev &S = P.sys[s];
-  int ig = blockIdx.x;
+  const int ig = blockIdx.y;
   if (ig >= S.ncgp_sol) return;
-  int gi = S.coff + ig, sg = S.csoff + ig;
+  const int sg = S.csoff + ig;
   const int n = P.pwg_n[sg];
-  if (n == 0) return;
-  __shared__ int s_i[PW_MAXA];
-  __shared__ double4 s_x[PW_MAXA];
-  __shared__ double4 s_lj[PW_MAXA];     // A(i,O), B(i,O), A(i,H), B(i,H)
-  __shared__ float2 s_q[PW_MAXA];       // crg(i)*crg(O), crg(i)*crg(H)
-  __shared__ double s_f[PW_MAXA][3];
-  __shared__ int s_na;
-  const uint16_t *L = P.pwg + (size_t)sg * P.pwg_cap;
-  const int ow = S.aoff + S.nsol;       // first water O: charges and types of every water site
+  const int k0 = blockIdx.x * PW_BLOCK;
+  if (k0 >= n) return;
+  const int k = k0 + threadIdx.x;
+  const bool act = k < n;
   const int lane = threadIdx.x & 31;
+  const int ow = S.aoff + S.nsol;
+  const int o = ow + 3 * (act ? (int)P.pwg[(size_t)sg * P.pwg_cap + k] : 0);
+  const double3 xw[3] = {ld3(P.x, o), ld3(P.x, o + 1), ld3(P.x, o + 2)};
+  double fw[9];
+#pragma unroll
+  for (int c = 0; c < 9; c++) fw[c] = 0.0;
   double el = 0, vdw = 0;
-  const int f = P.cg_first[gi], l = P.cg_last[gi];
-  for (int a0 = f; a0 <= l; a0 += PW_MAXA) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int na = 0;
-      for (int a = a0; a <= l && a < a0 + PW_MAXA; a++) {
-        int i = P.cg_atoms[a];
-        if (P.iq[i] < 0) s_i[na++] = i;
+  const int t1 = P.pwg_off[sg + 1];
+  for (int t = P.pwg_off[sg]; t < t1; t++) {
+    const PwAtom A = P.pwa[t];
+    const double3 xi = ld3(P.x, A.atom);
+    double fi[3] = {0.0, 0.0, 0.0};
+    if (act) {
+#pragma unroll
+      for (int b = 0; b < 3; b++) {
+        double dx = xw[b].x - xi.x, dy = xw[b].y - xi.y, dz = xw[b].z - xi.z;
+        double r = rsqrt(dx * dx + dy * dy + dz * dz);
+        double r2 = r * r, r6 = r2 * r2 * r2;
+        double Vel = (double)(b == 0 ? A.q.x : A.q.y) * r;
+        double Va = (b == 0 ? A.lj.x : A.lj.z) * r6 * r6, Vb = (b == 0 ? A.lj.y : A.lj.w) * r6;
+        double dv = r2 * (-Vel - 12. * Va + 6. * Vb);
+        fi[0] -= dv * dx; fi[1] -= dv * dy; fi[2] -= dv * dz;
+        fw[3 * b] += dv * dx; fw[3 * b + 1] += dv * dy; fw[3 * b + 2] += dv * dz;
+        el += Vel;
+        vdw += Va - Vb;
       }
-      s_na = na;
     }
-    __syncthreads();
-    const int na = s_na;
-    for (int t = threadIdx.x; t < na; t += PW_BLOCK) {
-      int i = s_i[t];
-      s_x[t] = P.x[i];
-      int ljo = ljcode(P, S, i, ow), ljh = ljcode(P, S, i, ow + 1);
-      s_lj[t] = make_double4(P.lja[3 * i + ljo - 1] * P.lja[3 * ow + ljo - 1],
-                             P.ljb[3 * i + ljo - 1] * P.ljb[3 * ow + ljo - 1],
-                             P.lja[3 * i + ljh - 1] * P.lja[3 * (ow + 1) + ljh - 1],
-                             P.ljb[3 * i + ljh - 1] * P.ljb[3 * (ow + 1) + ljh - 1]);
-      s_q[t] = make_float2(P.crg[i] * P.crg[ow], P.crg[i] * P.crg[ow + 1]);
-      s_f[t][0] = s_f[t][1] = s_f[t][2] = 0.0;
-    }
-    __syncthreads();
-    for (int k0 = 0; k0 < n; k0 += PW_BLOCK) {
-      if (k0 + (threadIdx.x & ~31) >= n) break;        // whole warp past the list
-      const int k = k0 + threadIdx.x;
-      const bool act = k < n;
-      const int o = ow + 3 * (act ? (int)L[k] : 0);
-      double3 xw[3] = {ld3(P.x, o), ld3(P.x, o + 1), ld3(P.x, o + 2)};
-      double fw[9];
 #pragma unroll
-      for (int c = 0; c < 9; c++) fw[c] = 0.0;
-      for (int t = 0; t < na; t++) {
-        const double4 xi = s_x[t], lj = s_lj[t];
-        const float2 q = s_q[t];
-        double fi[3] = {0.0, 0.0, 0.0};
-        if (act) {
-#pragma unroll
-          for (int b = 0; b < 3; b++) {
-            double dx = xw[b].x - xi.x, dy = xw[b].y - xi.y, dz = xw[b].z - xi.z;
-            double r = rsqrt(dx * dx + dy * dy + dz * dz);
-            double r2 = r * r, r6 = r2 * r2 * r2;
-            double Vel = (double)(b == 0 ? q.x : q.y) * r;
-            double Va = (b == 0 ? lj.x : lj.z) * r6 * r6, Vb = (b == 0 ? lj.y : lj.w) * r6;
-            double dv = r2 * (-Vel - 12. * Va + 6. * Vb);
-            fi[0] -= dv * dx; fi[1] -= dv * dy; fi[2] -= dv * dz;
-            fw[3 * b] += dv * dx; fw[3 * b + 1] += dv * dy; fw[3 * b + 2] += dv * dz;
-            el += Vel;
-            vdw += Va - Vb;
-          }
-        }
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-          double v = warp_sum(fi[c]);
-          if (lane == 0) atomicAdd(&s_f[t][c], v);
-        }
-      }
-      if (act)
-        for (int b = 0; b < 3; b++) atomic_add3(P.d, o + b, fw[3 * b], fw[3 * b + 1], fw[3 * b + 2]);
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < na; t += PW_BLOCK) {
-      double4 dd = P.d[s_i[t]];
-      dd.x += s_f[t][0]; dd.y += s_f[t][1]; dd.z += s_f[t][2];
-      P.d[s_i[t]] = dd;
-    }
+    for (int c = 0; c < 3; c++) fi[c] = warp_sum(fi[c]);
+    if (lane == 0) atomic_add3(P.d, A.atom, fi[0], fi[1], fi[2]);
   }
+  if (act)
+    for (int b = 0; b < 3; b++) atomic_add3(P.d, o + b, fw[3 * b], fw[3 * b + 1], fw[3 * b + 2]);
   warp_add(&P.E[s * QB_NE + QB_E_PW_EL], el);
   warp_add(&P.E[s * QB_NE + QB_E_PW_VDW], vdw);
 }
@@ -1259,55 +1217,127 @@ __global__ void k_nb_qq(DevPtrs P) {
   }
 }
 
-// lrf_taylor (md.f90:3646): potential and field of each atom's own group
-// multipoles; one thread per atom.  The reference's phi2(9) and phi3(27) are
-// read through the index of their distinct component, in its order of terms.
-__global__ void k_lrf_taylor(DevPtrs P) {
-  int s = blockIdx.y;
-  const SysDev &S = P.sys[s];
-  if (!S.use_lrf) return;
+// Per-atom terms (blockIdx.y = system), one update of each atom's gradient:
+//  - lrf_taylor (md.f90:3646): potential and field of the atom's own group
+//    multipoles; the reference's phi2(9) and phi3(27) are read through the
+//    index of their distinct component, in its order of terms;
+//  - fix_shell / restrain_solvent (md.f90:1414, 14910): harmonic restraints of
+//    excluded and shell atoms to their topology positions, and the radial
+//    restraint of water O atoms (harmonic outside the boundary less the
+//    thermal shift, Morse inside).
+// One thread per solute atom or per water (its three atoms share one LRF
+// record, loaded once).
+struct LrfRec { double v[24]; };
+
+__device__ __forceinline__ void lrf_load(const DevPtrs &P, int gc, LrfRec &L) {
+  const double4 *L4 = reinterpret_cast<const double4 *>(P.lrf + (size_t)gc * LRF_STRIDE);
+#pragma unroll
+  for (int w = 0; w < 6; w++) {
+    double4 q = L4[w];
+    L.v[4 * w] = q.x; L.v[4 * w + 1] = q.y; L.v[4 * w + 2] = q.z; L.v[4 * w + 3] = q.w;
+  }
+}
+
+// Taylor potential and field of one atom at xi, charge q: returns 0.5*q*V,
+// subtracts q*df from g.
+__device__ __forceinline__ double lrf_eval(const LrfRec &R, double3 xi, double q, double *g) {
   constexpr int i2[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
   constexpr int i3[27] = {0, 1, 2, 1, 3, 4, 2, 4, 5, 1, 3, 4, 3, 6, 7, 4, 7, 8, 2, 4, 5, 4, 7, 8, 5, 8, 9};
-  double e = 0;
-  for (int i0 = blockIdx.x * blockDim.x; i0 < S.natom; i0 += gridDim.x * blockDim.x) {
-    int il = i0 + threadIdx.x;
-    if (il < S.natom) {
-      int i = S.aoff + il;
-      if (!(P.flags[i] & F_EXCL) && P.iq[i] < 0) {
-        const double4 *L4 = reinterpret_cast<const double4 *>(P.lrf + (size_t)P.cgp[i] * LRF_STRIDE);
-        double L[24];
+  const double *L = R.v;
+  double dr[3] = {L[0] - xi.x, L[1] - xi.y, L[2] - xi.z};
+  const double *p1 = L + 4, *p2 = L + 7, *p3 = L + 13;
+  double V = L[3] + p1[0] * dr[0] + p1[1] * dr[1] + p1[2] * dr[2];
 #pragma unroll
-        for (int w = 0; w < 6; w++) {
-          double4 q = L4[w];
-          L[4 * w] = q.x; L[4 * w + 1] = q.y; L[4 * w + 2] = q.z; L[4 * w + 3] = q.w;
-        }
-        double3 xi = ld3(P.x, i);
-        double dr[3] = {L[0] - xi.x, L[1] - xi.y, L[2] - xi.z};
-        const double *p1 = L + 4, *p2 = L + 7, *p3 = L + 13;
-        double V = L[3] + p1[0] * dr[0] + p1[1] * dr[1] + p1[2] * dr[2];
+  for (int a = 0; a < 3; a++)
+    V += 0.5 * (p2[i2[3 * a]] * dr[0] + p2[i2[3 * a + 1]] * dr[1] + p2[i2[3 * a + 2]] * dr[2]) * dr[a];
 #pragma unroll
-        for (int a = 0; a < 3; a++)
-          V += 0.5 * (p2[i2[3 * a]] * dr[0] + p2[i2[3 * a + 1]] * dr[1] + p2[i2[3 * a + 2]] * dr[2]) * dr[a];
-        double q = (double)P.crg[i];
-        e += 0.5 * q * V;
-        double g[3];
+  for (int c = 0; c < 3; c++) {
+    double df = p1[c] + p2[i2[3 * c]] * dr[0] + p2[i2[3 * c + 1]] * dr[1] + p2[i2[3 * c + 2]] * dr[2];
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-          double df = p1[c] + p2[i2[3 * c]] * dr[0] + p2[i2[3 * c + 1]] * dr[1] + p2[i2[3 * c + 2]] * dr[2];
-#pragma unroll
-          for (int a = 0; a < 3; a++) {
-            const int o = 9 * c + 3 * a;
-            df += 0.5 * (p3[i3[o]] * dr[0] + p3[i3[o + 1]] * dr[1] + p3[i3[o + 2]] * dr[2]) * dr[a];
-          }
-          g[c] = q * df;
-        }
-        double4 dd = P.d[i];
-        dd.x -= g[0]; dd.y -= g[1]; dd.z -= g[2];
-        P.d[i] = dd;
-      }
+    for (int a = 0; a < 3; a++) {
+      const int o = 9 * c + 3 * a;
+      df += 0.5 * (p3[i3[o]] * dr[0] + p3[i3[o + 1]] * dr[1] + p3[i3[o + 2]] * dr[2]) * dr[a];
     }
+    g[c] -= q * df;
   }
-  warp_add(&P.E[s * QB_NE + QB_E_LRF], e);
+  return 0.5 * q * V;
+}
+
+// Harmonic restraint of an excluded or shell atom to its topology position.
+__device__ __forceinline__ void fix_shell_atom(const DevPtrs &P, const SysDev &S, int i, uint8_t fl, double3 xi,
+                                               double *g, double &efix, double &eshell) {
+  double fk = (fl & F_EXCL) ? S.fk_fix : S.fk_pshell;
+  double dr[3] = {xi.x - P.xtop[3 * i], xi.y - P.xtop[3 * i + 1], xi.z - P.xtop[3 * i + 2]};
+  double e = 0.5 * fk * (dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+  if (fl & F_EXCL) efix += e;
+  if (fl & F_SHELL) eshell += e;
+  for (int k = 0; k < 3; k++) g[k] += fk * dr[k];
+}
+
+__device__ __forceinline__ void add_grad(DevPtrs &P, int i, const double *g) {
+  if (g[0] != 0 || g[1] != 0 || g[2] != 0) {
+    double4 dd = P.d[i];
+    dd.x += g[0]; dd.y += g[1]; dd.z += g[2];
+    P.d[i] = dd;
+  }
+}
+
+__global__ void k_atom_terms(DevPtrs P) {
+  int s = blockIdx.y;
+  const SysDev &S = P.sys[s];
+  double elrf = 0, efix = 0, eshell = 0, erad = 0;
+  const int nunit = S.nsol + S.nwat;
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u < S.nsol) {
+    const int i = S.aoff + u;
+    const uint8_t fl = P.flags[i];
+    const double3 xi = ld3(P.x, i);
+    double g[3] = {0, 0, 0};
+    if (S.use_lrf && !(fl & F_EXCL) && P.iq[i] < 0) {
+      LrfRec R;
+      lrf_load(P, P.cgp[i], R);
+      elrf += lrf_eval(R, xi, (double)P.crg[i], g);
+    }
+    if (fl & (F_EXCL | F_SHELL)) fix_shell_atom(P, S, i, fl, xi, g, efix, eshell);
+    add_grad(P, i, g);
+  } else if (u < nunit) {
+    const int o = S.aoff + 3 * u - 2 * S.nsol;        // O of water u - nsol
+    const uint8_t fo = P.flags[o];
+    const double3 x[3] = {ld3(P.x, o), ld3(P.x, o + 1), ld3(P.x, o + 2)};
+    double g[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    if (S.use_lrf && !((fo & P.flags[o + 1] & P.flags[o + 2]) & F_EXCL)) {
+      LrfRec R;
+      lrf_load(P, P.cgp[o], R);
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+        if (!(P.flags[o + a] & F_EXCL) && P.iq[o + a] < 0) elrf += lrf_eval(R, x[a], (double)P.crg[o + a], g[a]);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const uint8_t fl = P.flags[o + a];
+      if (fl & (F_EXCL | F_SHELL)) fix_shell_atom(P, S, o + a, fl, x[a], g[a], efix, eshell);
+    }
+    if (!(fo & F_EXCL)) {
+      const double shift = S.fk_ws != 0. ? sqrt((double)kBoltzF * P.st[s].Tfree / S.fk_ws) : 0.;
+      double dr[3] = {x[0].x - S.xw[0], x[0].y - S.xw[1], x[0].z - S.xw[2]};
+      double b = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+      double db = b - (S.rwat - shift), e, dv;
+      if (db > 0) { e = 0.5 * S.fk_ws * db * db - S.Dwmz; dv = S.fk_ws * db / b; }
+      else if (b > 0.0) {
+        double fexp = exp(S.awmz * db);
+        e = S.Dwmz * (fexp * fexp - 2. * fexp);
+        dv = -2. * S.Dwmz * S.awmz * (fexp - fexp * fexp) / b;
+      } else { e = 0; dv = 0; }
+      erad += e;
+      for (int k = 0; k < 3; k++) g[0][k] += dv * dr[k];
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) add_grad(P, o + a, g[a]);
+  }
+  warp_add(&P.E[s * QB_NE + QB_E_LRF], elrf);
+  warp_add(&P.E[s * QB_NE + QB_E_RST_FIX], efix);
+  warp_add(&P.E[s * QB_NE + QB_E_RST_SHELL], eshell);
+  warp_add(&P.E[s * QB_NE + QB_E_RST_SOLVENT_RADIAL], erad);
 }
 
 // ---------------------------------------------------------------- bonded
@@ -1539,52 +1569,6 @@ __global__ void k_qbonded(DevPtrs P) {
 
 // ------------------------------------------------------------ restraints
 
-// fix_shell (md.f90:1414) for excluded and shell atoms, and restrain_solvent
-// (14910) for water oxygens: one thread per atom.
-__global__ void k_restrain_atoms(DevPtrs P) {
-  int s = blockIdx.y;
-  const SysDev &S = P.sys[s];
-  double efix = 0, eshell = 0, erad = 0;
-  double Tfree = P.st[s].Tfree;
-  double shift = S.fk_ws != 0. ? sqrt((double)kBoltzF * Tfree / S.fk_ws) : 0.;
-  for (int i0 = blockIdx.x * blockDim.x; i0 < S.natom; i0 += gridDim.x * blockDim.x) {
-    int il = i0 + threadIdx.x;
-    if (il >= S.natom) continue;
-    int i = S.aoff + il;
-    uint8_t fl = P.flags[i];
-    double3 xi = ld3(P.x, i);
-    double g[3] = {0, 0, 0};
-    if (fl & (F_EXCL | F_SHELL)) {
-      double fk = (fl & F_EXCL) ? S.fk_fix : S.fk_pshell;
-      double dr[3] = {xi.x - P.xtop[3 * i], xi.y - P.xtop[3 * i + 1], xi.z - P.xtop[3 * i + 2]};
-      double e = 0.5 * fk * (dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
-      if (fl & F_EXCL) efix += e;
-      if (fl & F_SHELL) eshell += e;
-      for (int k = 0; k < 3; k++) g[k] += fk * dr[k];
-    }
-    if (il >= S.nsol && ((il - S.nsol) % 3) == 0 && !(fl & F_EXCL)) {
-      double dr[3] = {xi.x - S.xw[0], xi.y - S.xw[1], xi.z - S.xw[2]};
-      double b = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
-      double db = b - (S.rwat - shift), e, dv;
-      if (db > 0) { e = 0.5 * S.fk_ws * db * db - S.Dwmz; dv = S.fk_ws * db / b; }
-      else if (b > 0.0) {
-        double fexp = exp(S.awmz * db);
-        e = S.Dwmz * (fexp * fexp - 2. * fexp);
-        dv = -2. * S.Dwmz * S.awmz * (fexp - fexp * fexp) / b;
-      } else { e = 0; dv = 0; }
-      erad += e;
-      for (int k = 0; k < 3; k++) g[k] += dv * dr[k];
-    }
-    if (g[0] != 0 || g[1] != 0 || g[2] != 0) {
-      double4 dd = P.d[i];
-      dd.x += g[0]; dd.y += g[1]; dd.z += g[2];
-      P.d[i] = dd;
-    }
-  }
-  warp_add(&P.E[s * QB_NE + QB_E_RST_FIX], efix);
-  warp_add(&P.E[s * QB_NE + QB_E_RST_SHELL], eshell);
-  warp_add(&P.E[s * QB_NE + QB_E_RST_SOLVENT_RADIAL], erad);
-}
 
 __device__ __forceinline__ double block_sum(double v, double *sh) {
   v = warp_sum(v);
@@ -1735,20 +1719,14 @@ __global__ void k_prestrain(DevPtrs P) {
 }
 
 // watpol (md.f90:15122): water polarisation restraint, in two kernels.
-// k_watpol_rank, one block per (shell, system): the shell's members (angles
-// and shells from k_pack_waters) are sorted by (angle, water index) with a
-// bitonic network in shared memory, so a member's position is its rank in the
-// reference's selection order (ties by water index).  The block also keeps
+// k_watpol_rank, one block per (shell, system): each member of the shell
+// (angles and shells from k_pack_waters) is ranked by counting the members
+// before it in (angle, water index) order, the reference's selection order
+// with ties by water index.  The block also keeps
 // the shell's running averages and updates theta_corr every 100 steps, in
 // the reference's order (update first, then this step's average).
 // k_watpol_force, one thread per water: target angle from the rank, restraint
 // energy and the force on the water dipole.
-struct WpolKey { double th; int iw, pad; };
-
-__device__ __forceinline__ bool wpol_less(const WpolKey &a, const WpolKey &b) {
-  return a.th < b.th || (a.th == b.th && a.iw < b.iw);
-}
-
 constexpr int WPOL_BLOCK = 256;
 
 __global__ void __launch_bounds__(WPOL_BLOCK) k_watpol_rank(DevPtrs P) {
@@ -1764,7 +1742,9 @@ __global__ void __launch_bounds__(WPOL_BLOCK) k_watpol_rank(DevPtrs P) {
   __syncthreads();
   const int8_t *wsh = P.wshell + S.woff;
   const double *wth = P.wtheta + S.woff;
-  WpolKey *key = (WpolKey *)smem;
+  // member angles as bit patterns (non-negative doubles order like their bits)
+  long long *kth = (long long *)smem;
+  int *kiw = (int *)(kth + nw);                 // member water indices
   for (int w0 = 0; w0 < nw; w0 += WPOL_BLOCK) {
     const int iw = w0 + threadIdx.x;
     const bool mine = iw < nw && wsh[iw] == is;
@@ -1773,37 +1753,34 @@ __global__ void __launch_bounds__(WPOL_BLOCK) k_watpol_rank(DevPtrs P) {
     if (lane == 0 && bal) base = atomicAdd(&cnt, __popc(bal));
     base = __shfl_sync(FULL, base, 0);
     if (mine) {
-      WpolKey k;
-      k.th = wth[iw]; k.iw = iw; k.pad = 0;
-      key[base + __popc(bal & ((1u << lane) - 1u))] = k;
+      const int k = base + __popc(bal & ((1u << lane) - 1u));
+      kth[k] = __double_as_longlong(wth[iw]);
+      kiw[k] = iw;
     }
   }
   __syncthreads();
   const int n = cnt;
-  int np = 1;
-  while (np < n) np <<= 1;
-  for (int t = n + threadIdx.x; t < np; t += WPOL_BLOCK) {
-    WpolKey k;
-    k.th = 1e300; k.iw = 0x7fffffff; k.pad = 0;      // sorts after every member
-    key[t] = k;
-  }
-  __syncthreads();
-  for (int kk = 2; kk <= np; kk <<= 1)
-    for (int j = kk >> 1; j > 0; j >>= 1) {
-      for (int t = threadIdx.x; t < np; t += WPOL_BLOCK) {
-        const int u = t ^ j;
-        if (u > t) {
-          WpolKey a = key[t], b = key[u];
-          const bool up = (t & kk) == 0;
-          if (up ? wpol_less(b, a) : wpol_less(a, b)) { key[t] = b; key[u] = a; }
-        }
-      }
-      __syncthreads();
-    }
+  // rank = members before this one in (angle, water index) order; the
+  // shared-memory reads are broadcasts
   double tsum = 0;
-  for (int r = threadIdx.x; r < n; r += WPOL_BLOCK) {
-    P.wrank[S.woff + key[r].iw] = r;
-    tsum += key[r].th;
+  for (int m = threadIdx.x; m < n; m += WPOL_BLOCK) {
+    const long long th = kth[m];
+    const int iw = kiw[m];
+    int r[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int u = 0;
+    for (; u + 8 <= n; u += 8) {
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        const long long tu = kth[u + q];
+        r[q] += (tu < th || (tu == th && kiw[u + q] < iw)) ? 1 : 0;
+      }
+    }
+    for (; u < n; u++) {
+      const long long tu = kth[u];
+      r[0] += (tu < th || (tu == th && kiw[u] < iw)) ? 1 : 0;
+    }
+    P.wrank[S.woff + iw] = r[0] + r[1] + r[2] + r[3] + r[4] + r[5] + r[6] + r[7];
+    tsum += __longlong_as_double(th);
   }
   double tot = block_sum(tsum, shsum);
   if (threadIdx.x == 0) {
@@ -1878,57 +1855,71 @@ __global__ void __launch_bounds__(WPOL_BLOCK) k_watpol_force(DevPtrs P) {
 
 // --------------------------------------------------------------- dynamics
 
-// The sums of pot_energy (md.f90:13443-13472): per-state totals and the
-// lambda-weighted Q energies; one thread per system.
-__global__ void k_finalize_energy(DevPtrs P) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= P.nsys) return;
-  const SysDev &S = P.sys[s];
-  double *E = P.E + s * QB_NE;
-  for (int k = 0; k < S.S; k++) {
-    double *q = P.EQ + ((size_t)s * MAXS + k) * QB_NEQ;
-    double lam = S.lambda[k];
-    q[QB_EQ_LAMBDA] = lam;
-    q[QB_EQ_QX_EL] = q[QB_EQ_QQ_EL] + q[QB_EQ_QP_EL] + q[QB_EQ_QW_EL];
-    q[QB_EQ_QX_VDW] = q[QB_EQ_QQ_VDW] + q[QB_EQ_QP_VDW] + q[QB_EQ_QW_VDW];
-    q[QB_EQ_TOTAL] = q[QB_EQ_BOND] + q[QB_EQ_ANGLE] + q[QB_EQ_TORSION] + q[QB_EQ_IMPROPER] + q[QB_EQ_QX_EL] +
-                     q[QB_EQ_QX_VDW] + q[QB_EQ_RESTRAINT];
-    E[QB_E_Q_BOND] += q[QB_EQ_BOND] * lam;
-    E[QB_E_Q_ANGLE] += q[QB_EQ_ANGLE] * lam;
-    E[QB_E_Q_TORSION] += q[QB_EQ_TORSION] * lam;
-    E[QB_E_Q_IMPROPER] += q[QB_EQ_IMPROPER] * lam;
-    E[QB_E_QX_EL] += q[QB_EQ_QX_EL] * lam;
-    E[QB_E_QX_VDW] += q[QB_EQ_QX_VDW] * lam;
-    E[QB_E_RST_PROTEIN] += q[QB_EQ_RESTRAINT] * lam;
-  }
-  E[QB_E_RST_TOTAL] = E[QB_E_RST_FIX] + E[QB_E_RST_SHELL] + E[QB_E_RST_PROTEIN] + E[QB_E_RST_SOLVENT_RADIAL] +
-                      E[QB_E_RST_WATER_POL];
-  E[QB_E_POTENTIAL] = E[QB_E_P_BOND] + E[QB_E_W_BOND] + E[QB_E_P_ANGLE] + E[QB_E_W_ANGLE] + E[QB_E_P_TORSION] +
-                      E[QB_E_P_IMPROPER] + E[QB_E_PP_EL] + E[QB_E_PP_VDW] + E[QB_E_PW_EL] + E[QB_E_PW_VDW] +
-                      E[QB_E_WW_EL] + E[QB_E_WW_VDW] + E[QB_E_Q_BOND] + E[QB_E_Q_ANGLE] + E[QB_E_Q_TORSION] +
-                      E[QB_E_Q_IMPROPER] + E[QB_E_QX_EL] + E[QB_E_QX_VDW] + E[QB_E_RST_TOTAL] + E[QB_E_LRF];
-  E[QB_E_KINETIC] = P.st[s].kinetic;
-  if (!isfinite(E[QB_E_POTENTIAL])) set_status(&P.st[s], QB_ERR_NAN);
-}
 
 // Leapfrog with Berendsen scaling (md.f90:4082-4110): one thread per atom.
+// Kinetic energy of one atom into acc[4] (solute all, solute free, solvent
+// all, solvent free), as temperature() sums it (md.f90:3817).
+__device__ __forceinline__ void kin_add(const DevPtrs &P, const SysDev &S, int g, const double4 &v, double *acc) {
+  double e = 0.5 * P.mass[g] * (v.x * v.x + v.y * v.y + v.z * v.z);
+  bool free_ = !(P.flags[g] & F_EXCL);
+  if (g - S.aoff < S.nsol) { acc[0] += e; if (free_) acc[1] += e; }
+  else { acc[2] += e; if (free_) acc[3] += e; }
+}
+
+// Adds each lane's acc[4] to its system's kinetic-energy sums (s < 0: none):
+// one warp reduction and one atomic per distinct system in the warp.  Every
+// lane of the warp calls it.
+__device__ __forceinline__ void kin_tally(DevPtrs &P, int s, const double *acc) {
+  const int lane = threadIdx.x & 31;
+  unsigned todo = __ballot_sync(FULL, s >= 0);
+  while (todo) {
+    const int leader = __ffs(todo) - 1;
+    const int s0 = __shfl_sync(FULL, s, leader);
+    const bool mine = s == s0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      double v = warp_sum(mine ? acc[k] : 0.0);
+      if (lane == leader && v != 0.0) atomicAdd(&P.kin[s0 * 4 + k], v);
+    }
+    todo &= ~__ballot_sync(FULL, mine);
+  }
+}
+
+// Leap-frog update (md.f90:4080-4108): v from the gradient with the
+// Berendsen factor of solute or solvent, x from v.  With SHAKE the reference
+// then sets v = (x - xx)/dt for every atom (md.f90:4119); for atoms in no
+// constraint that is done here (their x is final), for the others by the
+// SHAKE kernels.  The kinetic energy of atoms whose velocity is final here
+// is added to the system's sums.
 __global__ void k_leapfrog(DevPtrs P) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= P.natoms_tot) return;
-  int s = P.asys[g];
-  const SysDev &S = P.sys[s];
-  double ts = (g - S.aoff) < S.nsol ? P.st[s].Tscale_sol : P.st[s].Tscale_solv;
-  double w = (double)P.winv[g], dt = S.dt;
-  double4 x = P.x[g], v = P.v[g], d = P.d[g];
-  v.x = (v.x - d.x * w * dt) * ts;
-  v.y = (v.y - d.y * w * dt) * ts;
-  v.z = (v.z - d.z * w * dt) * ts;
-  P.xx[g] = x;
-  x.x = x.x + v.x * dt;
-  x.y = x.y + v.y * dt;
-  x.z = x.z + v.z * dt;
-  P.x[g] = x;
-  P.v[g] = v;
+  int s = -1;
+  double acc[4] = {0, 0, 0, 0};
+  if (g < P.natoms_tot) {
+    s = P.asys[g];
+    const SysDev &S = P.sys[s];
+    double ts = (g - S.aoff) < S.nsol ? P.st[s].Tscale_sol : P.st[s].Tscale_solv;
+    double w = (double)P.winv[g], dt = S.dt;
+    double4 x = P.x[g], v = P.v[g], d = P.d[g];
+    v.x = (v.x - d.x * w * dt) * ts;
+    v.y = (v.y - d.y * w * dt) * ts;
+    v.z = (v.z - d.z * w * dt) * ts;
+    P.xx[g] = x;
+    double4 xn = x;
+    xn.x = x.x + v.x * dt;
+    xn.y = x.y + v.y * dt;
+    xn.z = x.z + v.z * dt;
+    P.x[g] = xn;
+    const bool shaken = P.flags[g] & F_SHAKE;
+    if (S.has_shake && !shaken) {
+      v.x = (xn.x - x.x) / dt;
+      v.y = (xn.y - x.y) / dt;
+      v.z = (xn.z - x.z) / dt;
+    }
+    P.v[g] = v;
+    if (!shaken) kin_add(P, S, g, v, acc);
+  }
+  kin_tally(P, s, acc);
 }
 
 
@@ -1966,9 +1957,10 @@ __device__ __forceinline__ bool shake_pair(double3 &xi, double3 &xj, const doubl
 // (rigid waters), one thread per molecule.  The atoms are relabelled on the
 // host so that the constraints, in their own order, join (0,1), (0,2), (1,2);
 // sweeps, readiness flags and the 1000-sweep limit are the reference's.
-__global__ void __launch_bounds__(128, 7) k_shake3(DevPtrs P) {
+__global__ void __launch_bounds__(128, 6) k_shake3(DevPtrs P) {
   int m = blockIdx.x * blockDim.x + threadIdx.x;
   int sys = -1, its = 0;
+  double acc[4] = {0, 0, 0, 0};
   if (m < P.nsh3) {
     const int4 at = P.sh3_at[m];
     const double4 d2 = P.sh3_d2[m];
@@ -1986,15 +1978,28 @@ __global__ void __launch_bounds__(128, 7) k_shake3(DevPtrs P) {
       if (its >= 1000) break;
     }
     if (c0 && c1 && c2) {
-      double4 o;
-      o = P.x[at.x]; o.x = x0.x; o.y = x0.y; o.z = x0.z; P.x[at.x] = o;
-      o = P.x[at.y]; o.x = x1.x; o.y = x1.y; o.z = x1.z; P.x[at.y] = o;
-      o = P.x[at.z]; o.x = x2.x; o.y = x2.y; o.z = x2.z; P.x[at.z] = o;
+      const SysDev &S = P.sys[sys];
+      const double dt = S.dt;
+      double3 xs[3] = {x0, x1, x2}, rs[3] = {r0, r1, r2};
+      const int ids[3] = {at.x, at.y, at.z};
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        double4 o = P.x[ids[a]];
+        o.x = xs[a].x; o.y = xs[a].y; o.z = xs[a].z;
+        P.x[ids[a]] = o;
+        double4 v = P.v[ids[a]];
+        v.x = (xs[a].x - rs[a].x) / dt;
+        v.y = (xs[a].y - rs[a].y) / dt;
+        v.z = (xs[a].z - rs[a].z) / dt;
+        P.v[ids[a]] = v;
+        kin_add(P, S, ids[a], v, acc);
+      }
     } else {
       set_status(&P.st[sys], QB_ERR_SHAKE);
     }
   }
   shake_tally(P, sys, its);
+  kin_tally(P, sys, acc);
 }
 
 // shake (md.f90:14445) for every other molecule, one block per molecule.
@@ -2063,15 +2068,29 @@ __global__ void __launch_bounds__(SHG_BLOCK) k_shake_general(DevPtrs P) {
     done = __syncthreads_and(mine);
     if (!done && its >= 1000) break;
   }
+  double acc[4] = {0, 0, 0, 0};
   if (done) {
+    const SysDev &S = P.sys[sys];
     for (int t = threadIdx.x; t < na; t += SHG_BLOCK) {
-      double4 o = P.x[at[t]];
-      const double4 x = ax[t];
+      const int g = at[t];
+      double4 o = P.x[g];
+      const double4 x = ax[t], xx = P.xx[g];
       o.x = x.x; o.y = x.y; o.z = x.z;
-      P.x[at[t]] = o;
+      P.x[g] = o;
+      double4 v = P.v[g];
+      v.x = (x.x - xx.x) / S.dt;
+      v.y = (x.y - xx.y) / S.dt;
+      v.z = (x.z - xx.z) / S.dt;
+      P.v[g] = v;
+      kin_add(P, S, g, v, acc);
     }
   } else if (threadIdx.x == 0) {
     set_status(&P.st[sys], QB_ERR_SHAKE);
+  }
+  __shared__ double ksh[32];
+  for (int k = 0; k < 4; k++) {
+    double t = block_sum(acc[k], ksh);
+    if (threadIdx.x == 0 && t != 0.0) atomicAdd(&P.kin[sys * 4 + k], t);
   }
   if (threadIdx.x == 0) {
     atomicAdd(&P.st[sys].shake_its, (unsigned long long)its);
@@ -2079,53 +2098,79 @@ __global__ void __launch_bounds__(SHG_BLOCK) k_shake_general(DevPtrs P) {
   }
 }
 
-// temperature (md.f90:3817), first half, and the velocities of a SHAKE step
-// (md.f90:4119): v = (x - xx)/dt, then the kinetic energies of solute and
-// solvent atoms (all and not excluded).  Grid (blocks, systems); each block
-// writes its four partial sums, which k_finish adds in block order.
+// Kinetic energy sums of the current velocities (the temperature before the
+// first step, md.f90:3960): grid (blocks, systems).
 constexpr int KIN_BLOCK = 256;
 
-__global__ void __launch_bounds__(KIN_BLOCK) k_kinetic(DevPtrs P, int mode) {
+__global__ void __launch_bounds__(KIN_BLOCK) k_kinetic(DevPtrs P) {
   int s = blockIdx.y;
   const SysDev &S = P.sys[s];
   __shared__ double sh[32];
-  double acc[4] = {0, 0, 0, 0};  // solute all, solute free, solvent all, solvent free
+  double acc[4] = {0, 0, 0, 0};
   int il = blockIdx.x * KIN_BLOCK + threadIdx.x;
-  if (il < S.natom) {
-    int g = S.aoff + il;
-    double4 v = P.v[g];
-    if (mode == 1 && S.has_shake) {
-      double4 x = P.x[g], xx = P.xx[g];
-      v.x = (x.x - xx.x) / S.dt;
-      v.y = (x.y - xx.y) / S.dt;
-      v.z = (x.z - xx.z) / S.dt;
-      P.v[g] = v;
-    }
-    double e = 0.5 * P.mass[g] * (v.x * v.x + v.y * v.y + v.z * v.z);
-    bool free_ = !(P.flags[g] & F_EXCL);
-    if (il < S.nsol) { acc[0] = e; if (free_) acc[1] = e; }
-    else { acc[2] = e; if (free_) acc[3] = e; }
+  if (il < S.natom) kin_add(P, S, S.aoff + il, P.v[S.aoff + il], acc);
+  for (int k = 0; k < 4; k++) {
+    double t = block_sum(acc[k], sh);
+    if (threadIdx.x == 0 && t != 0.0) atomicAdd(&P.kin[s * 4 + k], t);
   }
-  double tot[4];
-  for (int k = 0; k < 4; k++) tot[k] = block_sum(acc[k], sh);
-  if (threadIdx.x == 0)
-    for (int k = 0; k < 4; k++) P.kin_part[((size_t)s * gridDim.x + blockIdx.x) * 4 + k] = tot[k];
 }
 
-// temperature (md.f90:3817), second half, one warp per system: temperatures,
-// the Berendsen scaling factors of the next step, output and energy-file
-// records of this step, step counter.
-__global__ void k_finish(DevPtrs P, int mode, int nblk) {
+// pot_energy's sums (md.f90:13500-13560): per-state Q totals, the
+// lambda-weighted Q terms and the potential.  Lane st handles state st; the
+// system totals follow on lane 0 in the reference's order.
+__device__ __forceinline__ void finalize_energy(DevPtrs &P, int s) {
+  const SysDev &S = P.sys[s];
+  const int lane = threadIdx.x;
+  double *E = P.E + s * QB_NE;
+  if (lane < S.S) {
+    double *q = P.EQ + ((size_t)s * MAXS + lane) * QB_NEQ;
+    q[QB_EQ_LAMBDA] = S.lambda[lane];
+    q[QB_EQ_QX_EL] = q[QB_EQ_QQ_EL] + q[QB_EQ_QP_EL] + q[QB_EQ_QW_EL];
+    q[QB_EQ_QX_VDW] = q[QB_EQ_QQ_VDW] + q[QB_EQ_QP_VDW] + q[QB_EQ_QW_VDW];
+    q[QB_EQ_TOTAL] = q[QB_EQ_BOND] + q[QB_EQ_ANGLE] + q[QB_EQ_TORSION] + q[QB_EQ_IMPROPER] + q[QB_EQ_QX_EL] +
+                     q[QB_EQ_QX_VDW] + q[QB_EQ_RESTRAINT];
+  }
+  __syncwarp();
+  if (lane == 0) {
+    for (int k = 0; k < S.S; k++) {
+      const double *q = P.EQ + ((size_t)s * MAXS + k) * QB_NEQ;
+      double lam = S.lambda[k];
+      E[QB_E_Q_BOND] += q[QB_EQ_BOND] * lam;
+      E[QB_E_Q_ANGLE] += q[QB_EQ_ANGLE] * lam;
+      E[QB_E_Q_TORSION] += q[QB_EQ_TORSION] * lam;
+      E[QB_E_Q_IMPROPER] += q[QB_EQ_IMPROPER] * lam;
+      E[QB_E_QX_EL] += q[QB_EQ_QX_EL] * lam;
+      E[QB_E_QX_VDW] += q[QB_EQ_QX_VDW] * lam;
+      E[QB_E_RST_PROTEIN] += q[QB_EQ_RESTRAINT] * lam;
+    }
+    E[QB_E_RST_TOTAL] = E[QB_E_RST_FIX] + E[QB_E_RST_SHELL] + E[QB_E_RST_PROTEIN] + E[QB_E_RST_SOLVENT_RADIAL] +
+                        E[QB_E_RST_WATER_POL];
+    E[QB_E_POTENTIAL] = E[QB_E_P_BOND] + E[QB_E_W_BOND] + E[QB_E_P_ANGLE] + E[QB_E_W_ANGLE] + E[QB_E_P_TORSION] +
+                        E[QB_E_P_IMPROPER] + E[QB_E_PP_EL] + E[QB_E_PP_VDW] + E[QB_E_PW_EL] + E[QB_E_PW_VDW] +
+                        E[QB_E_WW_EL] + E[QB_E_WW_VDW] + E[QB_E_Q_BOND] + E[QB_E_Q_ANGLE] + E[QB_E_Q_TORSION] +
+                        E[QB_E_Q_IMPROPER] + E[QB_E_QX_EL] + E[QB_E_QX_VDW] + E[QB_E_RST_TOTAL] + E[QB_E_LRF];
+    E[QB_E_KINETIC] = P.st[s].kinetic;
+    if (!isfinite(E[QB_E_POTENTIAL])) set_status(&P.st[s], QB_ERR_NAN);
+  }
+  __syncwarp();
+}
+
+// End of a step, one warp per system.  mode 1 (a step): pot_energy's sums,
+// then temperature (md.f90:3817) from the kinetic-energy sums of the
+// leap-frog and SHAKE kernels, the Berendsen factors of the next step, the
+// output and energy-file records of this step, and the step counter.
+// mode 0: the temperature before the first step.  mode 2: the sums only
+// (the energies after the loop).
+__global__ void k_finish(DevPtrs P, int mode) {
   int s = blockIdx.x;
   const SysDev &S = P.sys[s];
   SysState &st = P.st[s];
   int lane = threadIdx.x;
-  double tot[4] = {0, 0, 0, 0};
-  int nb = (S.natom + KIN_BLOCK - 1) / KIN_BLOCK;
-  for (int b = lane; b < nb; b += 32)
-    for (int k = 0; k < 4; k++) tot[k] += P.kin_part[((size_t)s * nblk + b) * 4 + k];
-  for (int k = 0; k < 4; k++) tot[k] = warp_sum(tot[k]);
+  if (mode != 0) finalize_energy(P, s);
+  if (mode == 2) return;
   if (lane == 0) {
+    double tot[4];
+    for (int k = 0; k < 4; k++) { tot[k] = P.kin[s * 4 + k]; P.kin[s * 4 + k] = 0.0; }
     const double kb = (double)kBoltzF;
     double Tfree_sol = tot[1], Tfree_solv = tot[3];
     double Tfree = Tfree_solv + Tfree_sol;
@@ -2152,25 +2197,29 @@ __global__ void k_finish(DevPtrs P, int mode, int nblk) {
     st.Tfree = Tfree;
     st.Tfree_sol = Tfree_sol;
     st.Tfree_solv = Tfree_solv;
-    if (mode == 1) {
-      P.E[s * QB_NE + QB_E_KINETIC] = st.kinetic;
-      int is = st.istep;
-      int rec_len = QB_NE + MAXS * QB_NEQ + 1;
-      for (int kind = 0; kind < 2; kind++) {
-        int cyc = kind == 0 ? S.iout : S.iene;
-        bool want = (is % cyc == 0) && (kind == 0 || is > 0);
-        if (!want) continue;
-        int c = st.hist_n[kind];
-        if (c < P.hist_cap) {
-          double *r = P.hist + (((size_t)kind * P.nsys + s) * P.hist_cap + c) * rec_len;
-          r[0] = (double)is;
-          for (int k = 0; k < QB_NE; k++) r[1 + k] = P.E[s * QB_NE + k];
-          for (int k = 0; k < MAXS * QB_NEQ; k++) r[1 + QB_NE + k] = P.EQ[(size_t)s * MAXS * QB_NEQ + k];
-        }
-        st.hist_n[kind] = c + 1;
+    if (mode == 1) P.E[s * QB_NE + QB_E_KINETIC] = st.kinetic;
+  }
+  __syncwarp();
+  if (mode == 1) {
+    // output and energy-file records of this step, copied by the whole warp
+    const int is = st.istep;
+    const int rec_len = QB_NE + MAXS * QB_NEQ + 1;
+    for (int kind = 0; kind < 2; kind++) {
+      int cyc = kind == 0 ? S.iout : S.iene;
+      bool want = (is % cyc == 0) && (kind == 0 || is > 0);
+      if (!want) continue;
+      int c = st.hist_n[kind];
+      if (c < P.hist_cap) {
+        double *r = P.hist + (((size_t)kind * P.nsys + s) * P.hist_cap + c) * rec_len;
+        for (int k = lane; k < rec_len; k += 32)
+          r[k] = k == 0 ? (double)is
+                        : (k <= QB_NE ? P.E[s * QB_NE + k - 1] : P.EQ[(size_t)s * MAXS * QB_NEQ + k - 1 - QB_NE]);
       }
-      st.istep = is + 1;
+      __syncwarp();
+      if (lane == 0) st.hist_n[kind] = c + 1;
     }
+    __syncwarp();
+    if (lane == 0) st.istep = is + 1;
   }
 }
 

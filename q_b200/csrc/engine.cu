@@ -164,21 +164,31 @@ struct Batch {
     CUDA_TRY(cudaMemsetAsync(p.d, 0, sizeof(double4) * (size_t)p.natoms_tot, stream));
     CUDA_TRY(cudaMemsetAsync(p.E, 0, sizeof(double) * QB_NE * (size_t)nsys, stream));
     CUDA_TRY(cudaMemsetAsync(p.EQ, 0, sizeof(double) * MAXS * QB_NEQ * (size_t)nsys, stream));
-    if (max_pp > 0)
-      launch("nb_pp", [&] { k_nb_pp<<<dim3(std::min(cdiv(max_pp, 256), 64), nsys), 256, 0, stream>>>(p); });
+    // solute terms in one launch (nonbond_pp, nonbond_qp, bonded, nonbond_qq,
+    // Q bonded, restraints)
+    {
+      SoluteGrid G{};
+      G.pp = max_pp > 0 ? std::min(cdiv(max_pp, 256), 64) : 0;
+      G.qp = any_q && max_qp > 0 ? std::min(cdiv(max_qp, 256), 32) : 0;
+      G.bonded = max_terms > 0 ? cdiv(max_terms, 256) : 0;
+      G.qq = any_qq ? 1 : 0;
+      G.qb = any_qb ? 1 : 0;
+      G.pre = any_prestr ? 1 : 0;
+      const int nb = G.pp + G.qp + G.bonded + G.qq + G.qb + G.pre;
+      if (nb > 0)
+        launch("solute_terms", [&] {
+          dim3 g(nb, nsys);
+          switch (q_states) {
+            case 1: k_solute_terms<1><<<g, 256, 0, stream>>>(p, G); break;
+            case 2: k_solute_terms<2><<<g, 256, 0, stream>>>(p, G); break;
+            case 3: k_solute_terms<3><<<g, 256, 0, stream>>>(p, G); break;
+            case 4: k_solute_terms<4><<<g, 256, 0, stream>>>(p, G); break;
+            default: k_solute_terms<0><<<g, 256, 0, stream>>>(p, G);
+          }
+        });
+    }
     if (max_ncgp_sol_w > 0)
       launch("nb_pw", [&] { k_nb_pw<<<dim3(cdiv(p.pwg_cap, PW_BLOCK), max_ncgp_sol_w, nsys), PW_BLOCK, 0, stream>>>(p); });
-    if (any_q && max_qp > 0)
-      launch("nb_qp", [&] {
-        dim3 g(std::min(cdiv(max_qp, 256), 32), nsys);
-        switch (q_states) {
-          case 1: k_nb_qp<1><<<g, 256, 0, stream>>>(p); break;
-          case 2: k_nb_qp<2><<<g, 256, 0, stream>>>(p); break;
-          case 3: k_nb_qp<3><<<g, 256, 0, stream>>>(p); break;
-          case 4: k_nb_qp<4><<<g, 256, 0, stream>>>(p); break;
-          default: k_nb_qp<0><<<g, 256, 0, stream>>>(p);
-        }
-      });
     const bool mixed = opt.precision == QB_MIXED;
     if (max_nwat > 0) {
       dim3 gp(cdiv(max_nwat, 256), nsys), gw(cdiv(max_nwat, WW_WPB), nsys);
@@ -202,16 +212,11 @@ struct Batch {
         }
       });
     }
-    if (max_terms > 0)
-      launch("bonded", [&] { k_bonded<<<dim3(cdiv(max_terms, 256), nsys), 256, 0, stream>>>(p); });
     launch("atom_terms", [&] { k_atom_terms<<<dim3(cdiv(max_units, 128), nsys), 128, 0, stream>>>(p); });
-    if (any_prestr) launch("prestrain", [&] { k_prestrain<<<nsys, 256, 0, stream>>>(p); });
     if (any_wpol) {
       launch("watpol_rank", [&] { k_watpol_rank<<<dim3(MAX_SHELLS, nsys), WPOL_BLOCK, watpol_smem, stream>>>(p); });
       launch("watpol", [&] { k_watpol_force<<<dim3(cdiv(max_nwat, WPOL_BLOCK), nsys), WPOL_BLOCK, 0, stream>>>(p); });
     }
-    if (any_qq) launch("nb_qq", [&] { k_nb_qq<<<nsys, 128, 0, stream>>>(p); });
-    if (any_qb) launch("qbonded", [&] { k_qbonded<<<nsys, 128, 0, stream>>>(p); });
     check_launch("force kernels");
   }
 

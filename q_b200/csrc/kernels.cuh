@@ -840,13 +840,12 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
 }
 
 // nonbond_pp (md.f90:10387): one thread per pair.
-__global__ void k_nb_pp(DevPtrs P) {
-  int s = blockIdx.y;
+__device__ __forceinline__ void nb_pp_body(DevPtrs &P, int bx, int s, int gx) {
   const SysDev &S = P.sys[s];
   int n = P.st[s].pp_n;
   const int4 *L = P.pp + S.pp_off;
   double el = 0, vdw = 0;
-  for (int k0 = blockIdx.x * blockDim.x; k0 < n; k0 += gridDim.x * blockDim.x) {
+  for (int k0 = bx * blockDim.x; k0 < n; k0 += gx * blockDim.x) {
     int k = k0 + threadIdx.x;
     if (k < n) {
       int4 p = L[k];
@@ -932,8 +931,7 @@ __global__ void __launch_bounds__(PW_BLOCK) k_nb_pw(DevPtrs P) {
 // nonbond_qp (md.f90:10980) / nonbond_qp_qvdw (11138): one thread per pair,
 // all states in the thread.
 template <int NSC>
-__global__ void k_nb_qp(DevPtrs P) {
-  int s = blockIdx.y;
+__device__ __forceinline__ void nb_qp_body(DevPtrs &P, int bx, int s, int gx) {
   const SysDev &S = P.sys[s];
   int n = P.st[s].qp_n;
   const int NS = NSC > 0 ? NSC : S.S;
@@ -942,7 +940,7 @@ __global__ void k_nb_qp(DevPtrs P) {
   double el[NA], vdw[NA];
 #pragma unroll
   for (int st = 0; st < NA; st++) { el[st] = 0; vdw[st] = 0; }
-  for (int k0 = blockIdx.x * blockDim.x; k0 < n; k0 += gridDim.x * blockDim.x) {
+  for (int k0 = bx * blockDim.x; k0 < n; k0 += gx * blockDim.x) {
     int k = k0 + threadIdx.x;
     if (k < n) {
       int4 p = P.qp[S.qp_off + k];
@@ -1146,8 +1144,7 @@ __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
 }
 
 // nonbond_qq (md.f90:10763): Q-Q and Q-to-bonded-neighbour pairs, all states.
-__global__ void k_nb_qq(DevPtrs P) {
-  int s = blockIdx.x;
+__device__ __forceinline__ void nb_qq_body(DevPtrs &P, int s) {
   const SysDev &S = P.sys[s];
   const int NS = S.S, ncol = S.natyps + S.nq;
   for (int k0 = 0; k0 < S.nqq; k0 += blockDim.x) {
@@ -1398,13 +1395,12 @@ __device__ __forceinline__ void apply4(const DevPtrs &P, int i, int j, int k, in
 
 // bond (954), angle (814), torsion (14793), improper (1677) / improper2 (1789):
 // one thread per term; items are bonds, then angles, torsions, impropers.
-__global__ void k_bonded(DevPtrs P) {
-  int s = blockIdx.y;
+__device__ __forceinline__ void bonded_body(DevPtrs &P, int bx, int s, int gx) {
   const SysDev &S = P.sys[s];
   int n = S.nb + S.na + S.nt + S.ni;
   double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // p bond, angle, torsion, improper; w ...
   const double pi = dev_pi();
-  for (int k0 = blockIdx.x * blockDim.x; k0 < n; k0 += gridDim.x * blockDim.x) {
+  for (int k0 = bx * blockDim.x; k0 < n; k0 += gx * blockDim.x) {
     int k = k0 + threadIdx.x;
     if (k >= n) continue;
     if (k < S.nb) {
@@ -1485,8 +1481,7 @@ __global__ void k_bonded(DevPtrs P) {
 
 // qbond (14060), qangle (13896), qtorsion (14262), qimproper (14117):
 // one block per system, threads over (term, state).
-__global__ void k_qbonded(DevPtrs P) {
-  int s = blockIdx.x;
+__device__ __forceinline__ void qbonded_body(DevPtrs &P, int s) {
   const SysDev &S = P.sys[s];
   const int NS = S.S;
   int n1 = S.nqb * NS, n2 = n1 + S.nqa * NS, n3 = n2 + S.nqt * NS, n4 = n3 + S.nqi * NS;
@@ -1592,8 +1587,7 @@ __device__ __forceinline__ void rst_energy(const DevPtrs &P, int s, int nstates,
 
 // p_restrain (md.f90:12940): sequence, atom, distance, angle and wall
 // restraints.  One block per system.
-__global__ void k_prestrain(DevPtrs P) {
-  int s = blockIdx.x;
+__device__ __forceinline__ void prestrain_body(DevPtrs &P, int s) {
   const SysDev &S = P.sys[s];
   __shared__ double sh[32];
   for (int r = 0; r < S.nrs; r++) {
@@ -1718,6 +1712,30 @@ __global__ void k_prestrain(DevPtrs P) {
   }
 }
 
+// The solute force terms, one launch: blocks [0, pp) take nonbond_pp, then
+// nonbond_qp, the bonded terms, nonbond_qq, the Q-atom bonded terms and the
+// sequence/position/distance/angle/wall restraints, each on its own block
+// range (blockIdx.y = system).  All of them add gradients with atomics, so
+// they run concurrently.
+struct SoluteGrid { int pp, qp, bonded, qq, qb, pre; };
+
+template <int NSC>
+__global__ void __launch_bounds__(256) k_solute_terms(DevPtrs P, SoluteGrid G) {
+  int b = blockIdx.x;
+  const int s = blockIdx.y;
+  if (b < G.pp) { nb_pp_body(P, b, s, G.pp); return; }
+  b -= G.pp;
+  if (b < G.qp) { nb_qp_body<NSC>(P, b, s, G.qp); return; }
+  b -= G.qp;
+  if (b < G.bonded) { bonded_body(P, b, s, G.bonded); return; }
+  b -= G.bonded;
+  if (b < G.qq) { nb_qq_body(P, s); return; }
+  b -= G.qq;
+  if (b < G.qb) { qbonded_body(P, s); return; }
+  b -= G.qb;
+  if (b < G.pre) prestrain_body(P, s);
+}
+
 // watpol (md.f90:15122): water polarisation restraint, in two kernels.
 // k_watpol_rank, one block per (shell, system): each member of the shell
 // (angles and shells from k_pack_waters) is ranked by counting the members
@@ -1766,20 +1784,23 @@ __global__ void __launch_bounds__(WPOL_BLOCK) k_watpol_rank(DevPtrs P) {
   for (int m = threadIdx.x; m < n; m += WPOL_BLOCK) {
     const long long th = kth[m];
     const int iw = kiw[m];
-    int r[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    // branch-free: both words of every key are read, no short-circuit
+    int r[4] = {0, 0, 0, 0};
     int u = 0;
-    for (; u + 8 <= n; u += 8) {
+    for (; u + 4 <= n; u += 4) {
 #pragma unroll
-      for (int q = 0; q < 8; q++) {
+      for (int q = 0; q < 4; q++) {
         const long long tu = kth[u + q];
-        r[q] += (tu < th || (tu == th && kiw[u + q] < iw)) ? 1 : 0;
+        const int iu = kiw[u + q];
+        r[q] += (int)(tu < th) + ((int)(tu == th) & (int)(iu < iw));
       }
     }
     for (; u < n; u++) {
       const long long tu = kth[u];
-      r[0] += (tu < th || (tu == th && kiw[u] < iw)) ? 1 : 0;
+      const int iu = kiw[u];
+      r[0] += (int)(tu < th) + ((int)(tu == th) & (int)(iu < iw));
     }
-    P.wrank[S.woff + iw] = r[0] + r[1] + r[2] + r[3] + r[4] + r[5] + r[6] + r[7];
+    P.wrank[S.woff + iw] = r[0] + r[1] + r[2] + r[3];
     tsum += __longlong_as_double(th);
   }
   double tot = block_sum(tsum, shsum);
@@ -2116,41 +2137,58 @@ __global__ void __launch_bounds__(KIN_BLOCK) k_kinetic(DevPtrs P) {
 }
 
 // pot_energy's sums (md.f90:13500-13560): per-state Q totals, the
-// lambda-weighted Q terms and the potential.  Lane st handles state st; the
-// system totals follow on lane 0 in the reference's order.
+// lambda-weighted Q terms and the potential.  Lane st handles state st (its
+// row loaded at once); lane 0 then adds the states in order and forms the
+// totals from one load of the system's energy terms.
 __device__ __forceinline__ void finalize_energy(DevPtrs &P, int s) {
   const SysDev &S = P.sys[s];
   const int lane = threadIdx.x;
   double *E = P.E + s * QB_NE;
+  double w[7] = {0, 0, 0, 0, 0, 0, 0};   // this state's bond, angle, torsion, improper, qx_el, qx_vdw, restraint, x lambda
   if (lane < S.S) {
     double *q = P.EQ + ((size_t)s * MAXS + lane) * QB_NEQ;
-    q[QB_EQ_LAMBDA] = S.lambda[lane];
-    q[QB_EQ_QX_EL] = q[QB_EQ_QQ_EL] + q[QB_EQ_QP_EL] + q[QB_EQ_QW_EL];
-    q[QB_EQ_QX_VDW] = q[QB_EQ_QQ_VDW] + q[QB_EQ_QP_VDW] + q[QB_EQ_QW_VDW];
-    q[QB_EQ_TOTAL] = q[QB_EQ_BOND] + q[QB_EQ_ANGLE] + q[QB_EQ_TORSION] + q[QB_EQ_IMPROPER] + q[QB_EQ_QX_EL] +
-                     q[QB_EQ_QX_VDW] + q[QB_EQ_RESTRAINT];
+    double r[QB_NEQ];
+#pragma unroll
+    for (int k = 0; k < QB_NEQ; k++) r[k] = q[k];
+    const double lam = S.lambda[lane];
+    r[QB_EQ_LAMBDA] = lam;
+    r[QB_EQ_QX_EL] = r[QB_EQ_QQ_EL] + r[QB_EQ_QP_EL] + r[QB_EQ_QW_EL];
+    r[QB_EQ_QX_VDW] = r[QB_EQ_QQ_VDW] + r[QB_EQ_QP_VDW] + r[QB_EQ_QW_VDW];
+    r[QB_EQ_TOTAL] = r[QB_EQ_BOND] + r[QB_EQ_ANGLE] + r[QB_EQ_TORSION] + r[QB_EQ_IMPROPER] + r[QB_EQ_QX_EL] +
+                     r[QB_EQ_QX_VDW] + r[QB_EQ_RESTRAINT];
+    q[QB_EQ_LAMBDA] = r[QB_EQ_LAMBDA];
+    q[QB_EQ_QX_EL] = r[QB_EQ_QX_EL];
+    q[QB_EQ_QX_VDW] = r[QB_EQ_QX_VDW];
+    q[QB_EQ_TOTAL] = r[QB_EQ_TOTAL];
+    w[0] = r[QB_EQ_BOND] * lam; w[1] = r[QB_EQ_ANGLE] * lam; w[2] = r[QB_EQ_TORSION] * lam;
+    w[3] = r[QB_EQ_IMPROPER] * lam; w[4] = r[QB_EQ_QX_EL] * lam; w[5] = r[QB_EQ_QX_VDW] * lam;
+    w[6] = r[QB_EQ_RESTRAINT] * lam;
   }
-  __syncwarp();
+  double e[QB_NE];
   if (lane == 0) {
-    for (int k = 0; k < S.S; k++) {
-      const double *q = P.EQ + ((size_t)s * MAXS + k) * QB_NEQ;
-      double lam = S.lambda[k];
-      E[QB_E_Q_BOND] += q[QB_EQ_BOND] * lam;
-      E[QB_E_Q_ANGLE] += q[QB_EQ_ANGLE] * lam;
-      E[QB_E_Q_TORSION] += q[QB_EQ_TORSION] * lam;
-      E[QB_E_Q_IMPROPER] += q[QB_EQ_IMPROPER] * lam;
-      E[QB_E_QX_EL] += q[QB_EQ_QX_EL] * lam;
-      E[QB_E_QX_VDW] += q[QB_EQ_QX_VDW] * lam;
-      E[QB_E_RST_PROTEIN] += q[QB_EQ_RESTRAINT] * lam;
+#pragma unroll
+    for (int k = 0; k < QB_NE; k++) e[k] = E[k];
+  }
+  for (int k = 0; k < S.S; k++) {
+    double v[7];
+#pragma unroll
+    for (int c = 0; c < 7; c++) v[c] = __shfl_sync(FULL, w[c], k);
+    if (lane == 0) {
+      e[QB_E_Q_BOND] += v[0]; e[QB_E_Q_ANGLE] += v[1]; e[QB_E_Q_TORSION] += v[2]; e[QB_E_Q_IMPROPER] += v[3];
+      e[QB_E_QX_EL] += v[4]; e[QB_E_QX_VDW] += v[5]; e[QB_E_RST_PROTEIN] += v[6];
     }
-    E[QB_E_RST_TOTAL] = E[QB_E_RST_FIX] + E[QB_E_RST_SHELL] + E[QB_E_RST_PROTEIN] + E[QB_E_RST_SOLVENT_RADIAL] +
-                        E[QB_E_RST_WATER_POL];
-    E[QB_E_POTENTIAL] = E[QB_E_P_BOND] + E[QB_E_W_BOND] + E[QB_E_P_ANGLE] + E[QB_E_W_ANGLE] + E[QB_E_P_TORSION] +
-                        E[QB_E_P_IMPROPER] + E[QB_E_PP_EL] + E[QB_E_PP_VDW] + E[QB_E_PW_EL] + E[QB_E_PW_VDW] +
-                        E[QB_E_WW_EL] + E[QB_E_WW_VDW] + E[QB_E_Q_BOND] + E[QB_E_Q_ANGLE] + E[QB_E_Q_TORSION] +
-                        E[QB_E_Q_IMPROPER] + E[QB_E_QX_EL] + E[QB_E_QX_VDW] + E[QB_E_RST_TOTAL] + E[QB_E_LRF];
-    E[QB_E_KINETIC] = P.st[s].kinetic;
-    if (!isfinite(E[QB_E_POTENTIAL])) set_status(&P.st[s], QB_ERR_NAN);
+  }
+  if (lane == 0) {
+    e[QB_E_RST_TOTAL] = e[QB_E_RST_FIX] + e[QB_E_RST_SHELL] + e[QB_E_RST_PROTEIN] + e[QB_E_RST_SOLVENT_RADIAL] +
+                        e[QB_E_RST_WATER_POL];
+    e[QB_E_POTENTIAL] = e[QB_E_P_BOND] + e[QB_E_W_BOND] + e[QB_E_P_ANGLE] + e[QB_E_W_ANGLE] + e[QB_E_P_TORSION] +
+                        e[QB_E_P_IMPROPER] + e[QB_E_PP_EL] + e[QB_E_PP_VDW] + e[QB_E_PW_EL] + e[QB_E_PW_VDW] +
+                        e[QB_E_WW_EL] + e[QB_E_WW_VDW] + e[QB_E_Q_BOND] + e[QB_E_Q_ANGLE] + e[QB_E_Q_TORSION] +
+                        e[QB_E_Q_IMPROPER] + e[QB_E_QX_EL] + e[QB_E_QX_VDW] + e[QB_E_RST_TOTAL] + e[QB_E_LRF];
+    e[QB_E_KINETIC] = P.st[s].kinetic;
+#pragma unroll
+    for (int k = 0; k < QB_NE; k++) E[k] = e[k];
+    if (!isfinite(e[QB_E_POTENTIAL])) set_status(&P.st[s], QB_ERR_NAN);
   }
   __syncwarp();
 }

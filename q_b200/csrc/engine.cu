@@ -59,7 +59,7 @@ struct Batch {
   cudaStream_t stream = nullptr;
   int NB = 1;
   long long istep = 0;
-  int max_natom = 0, max_units = 0, max_nwat = 0, max_ncgp = 0, max_ncgp_sol = 0, max_terms = 0, max_pp = 0, max_ncgp_sol_w = 0, max_qp = 0;
+  int max_natom = 0, max_lrf_blocks = 1, max_units = 0, max_nwat = 0, max_ncgp = 0, max_ncgp_sol = 0, max_terms = 0, max_pp = 0, max_ncgp_sol_w = 0, max_qp = 0;
   bool any_lrf = false, any_q = false, any_shake = false, any_wpol = false, any_prestr = false, any_qq = false,
        any_qb = false;
   size_t watpol_smem = 0;
@@ -145,7 +145,7 @@ struct Batch {
       launch("list_ww", [&] { k_list_ww<<<dim3(cdiv(max_nwat, WL_WPB), nsys), WL_BLOCK, 0, stream>>>(p, force); });
     if (any_lrf)
       launch("lrf_gather", [&] {
-        dim3 g(cdiv(max_ncgp, LRF_BLOCK), nsys);
+        dim3 g(max_lrf_blocks, nsys);
         if (opt.precision == QB_MIXED) k_lrf_gather<true><<<g, LRF_BLOCK, 0, stream>>>(p, force);
         else k_lrf_gather<false><<<g, LRF_BLOCK, 0, stream>>>(p, force);
       });
@@ -633,6 +633,9 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     B.max_nwat = std::max(B.max_nwat, V.nwat);
     B.max_ncgp_sol = std::max(B.max_ncgp_sol, V.ncgp_solute);
     B.max_ncgp = std::max(B.max_ncgp, V.ncgp);
+    if (V.use_LRF)
+      B.max_lrf_blocks = std::max(B.max_lrf_blocks, Batch::cdiv(V.ncgp, LRF_BLOCK) *
+                                                        Batch::cdiv(S.nlrft, LRF_TILES_PER_BLOCK));
     B.max_terms = std::max(B.max_terms, V.nbonds + V.nangles + V.ntors + V.nimps);
     B.max_pp = std::max(B.max_pp, S.pp_cap);
     if (V.nwat > 0) B.max_ncgp_sol_w = std::max(B.max_ncgp_sol_w, V.ncgp_solute);

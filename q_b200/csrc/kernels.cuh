@@ -73,7 +73,15 @@ __global__ void k_cgp_centers(DevPtrs P, int force) {
 // (md.f90:5581-5636), accumulated in the symmetric form m[20] = phi0,
 // phi1[x,y,z], phi2[xx,xy,xz,yy,yz,zz], phi3[xxx,xxy,xxz,xyy,xyz,xzz,yyy,yyz,
 // yzz,zzz]: the reference's 9 and 27 components are copies of these.
-__device__ __forceinline__ float rsq(float v) { return rsqrtf(v); }
+// 1/sqrt(v) on the MUFU unit (rsqrt.approx.ftz.f32, <= 2 ulp); the squared
+// distances it is used on are never denormal.
+__device__ __forceinline__ float rsqrt_ftz(float v) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v));
+  return r;
+}
+
+__device__ __forceinline__ float rsq(float v) { return rsqrt_ftz(v); }
 __device__ __forceinline__ double rsq(double v) { return rsqrt(v); }
 
 template <class R>
@@ -109,7 +117,7 @@ __device__ __forceinline__ void lrf_accumulate(R *m, R q, R dx, R dy, R dz) {
 // charge; used by the mixed-precision gather.
 __device__ __forceinline__ void lrf_accumulate_split(float *m, float *t, float q, float dx, float dy, float dz) {
   float r2 = dx * dx + dy * dy + dz * dz;
-  float rinv = rsqrtf(r2), ri2 = rinv * rinv;
+  float rinv = rsqrt_ftz(r2), ri2 = rinv * rinv;
   float f0 = q * rinv * ri2;
   m[0] = fmaf(f0, r2, m[0]);
   m[1] = fmaf(-f0, dx, m[1]); m[2] = fmaf(-f0, dy, m[2]); m[3] = fmaf(-f0, dz, m[3]);
@@ -154,6 +162,7 @@ __device__ __forceinline__ void lrf_fold(double *m, const double *t) {
 // sphere centre, |offset| >= ~7 A here), each tile summed in FP32 and added to
 // FP64 totals.
 constexpr int LRF_TILE_G = 128, LRF_TILE_A = 512, LRF_BLOCK = 128;
+constexpr int LRF_TILES_PER_BLOCK = 4;   // source tiles one block sweeps; larger systems use more blocks
 
 template <bool MIXED>
 __global__ void __launch_bounds__(LRF_BLOCK, MIXED ? 8 : 5) k_lrf_gather(DevPtrs P, int force) {
@@ -162,11 +171,16 @@ __global__ void __launch_bounds__(LRF_BLOCK, MIXED ? 8 : 5) k_lrf_gather(DevPtrs
   int s = blockIdx.y;
   if (!list_due(P, s, force)) return;
   const SysDev &S = P.sys[s];
-  if (!S.use_lrf || blockIdx.x * LRF_BLOCK >= S.ncgp) return;
+  if (!S.use_lrf) return;
+  // block -> (chunk of target groups, range of source tiles)
+  const int hsplit = (S.nlrft + LRF_TILES_PER_BLOCK - 1) / LRF_TILES_PER_BLOCK;
+  const int gchunk = blockIdx.x / max(hsplit, 1), hpart = blockIdx.x % max(hsplit, 1);
+  if (hsplit == 0 || gchunk * LRF_BLOCK >= S.ncgp) return;
+  const int t0 = hpart * LRF_TILES_PER_BLOCK, t1 = min(t0 + LRF_TILES_PER_BLOCK, S.nlrft);
   __shared__ double4 hsw[LRF_TILE_G];      // switching atom; w: -1 excluded, 1 solute, 0 water
   __shared__ int2 hrange[LRF_TILE_G];      // first atom slot, atom count
   __shared__ R4 hat[LRF_TILE_A];           // atom position (mixed: from the sphere centre), charge
-  int gl = blockIdx.x * LRF_BLOCK + threadIdx.x;
+  int gl = gchunk * LRF_BLOCK + threadIdx.x;
   int g = S.coff + gl;
   bool active = gl < S.ncgp;
   double cx = 0, cy = 0, cz = 0;
@@ -193,7 +207,7 @@ __global__ void __launch_bounds__(LRF_BLOCK, MIXED ? 8 : 5) k_lrf_gather(DevPtrs
 #pragma unroll
     for (int k = 0; k < 20; k++) m[k] = 0.0;
   }
-  for (int t = 0; t < S.nlrft; t++) {
+  for (int t = t0; t < t1; t++) {
     int2 tile = P.lrft[S.lrft_off + t];
     int nh = tile.y - tile.x;
     int a0 = P.cg_first[S.coff + tile.x];
@@ -249,6 +263,8 @@ __global__ void __launch_bounds__(LRF_BLOCK, MIXED ? 8 : 5) k_lrf_gather(DevPtrs
       }
     }
   }
+  // this block's share of the sources, added to the record (zeroed by
+  // k_cgp_centers)
   if (active) {
     double *L = P.lrf + (size_t)g * LRF_STRIDE;
     if (MIXED) {
@@ -259,10 +275,12 @@ __global__ void __launch_bounds__(LRF_BLOCK, MIXED ? 8 : 5) k_lrf_gather(DevPtrs
       for (int k = 0; k < 4; k++) t4[k] = mtot[20 + k][threadIdx.x];
       lrf_fold(mm, t4);
 #pragma unroll
-      for (int k = 0; k < 20; k++) L[3 + k] = mm[k];
+      for (int k = 0; k < 20; k++)
+        if (mm[k] != 0.0) atomicAdd(&L[3 + k], mm[k]);
     } else {
 #pragma unroll
-      for (int k = 0; k < 20; k++) L[3 + k] = m[MIXED ? 0 : k];
+      for (int k = 0; k < 20; k++)
+        if (m[MIXED ? 0 : k] != 0.0) atomicAdd(&L[3 + k], m[MIXED ? 0 : k]);
     }
   }
 }
@@ -692,7 +710,7 @@ __device__ __forceinline__ void ww_pair_f32(const float *i, const float *j, floa
         float v = b == 0 ? dOO[c] : t[b - 1][c];
         d[c] = a == 0 ? v : v - i[3 + 3 * a + c];
       }
-      float rinv = rsqrtf(fmaf(d[0], d[0], fmaf(d[1], d[1], d[2] * d[2])));
+      float rinv = rsqrt_ftz(fmaf(d[0], d[0], fmaf(d[1], d[1], d[2] * d[2])));
       float r2 = rinv * rinv;
       float qq = (a == 0 && b == 0) ? qoo : ((a == 0 || b == 0) ? qoh : qhh);
       float Vel = qq * rinv, dv;
@@ -724,7 +742,7 @@ __device__ __forceinline__ void unpack_mixed(const float4 *r, float *v) {
 // neighbour records come from shared memory.  Gradients of i are reduced over
 // the half-warp and added once per chunk; each unordered pair is evaluated
 // from both sides, energies halved.  Mixed precision: pair terms in FP32
-// (rsqrtf), each neighbour molecule's energy summed in FP32 and accumulated in
+// (MUFU rsqrt), each lane's energy over one water's list slice summed in FP32 and accumulated in
 // FP64, gradients reduced in FP32.
 template <bool MIXED>
 __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
@@ -787,16 +805,16 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
         float f[9];
 #pragma unroll
         for (int q = 0; q < 9; q++) f[q] = 0.f;
+        float e_el = 0.f, e_vdw = 0.f;
         for (; k < ke; k += 16) {
           const int j = jn;
           if (k + 16 < ke) jn = nb[k + 16];
           float xj[12];
           unpack_mixed(wsm + (j - c0) * W, xj);
-          float e_el = 0.f, e_vdw = 0.f;
           ww_pair_f32(xi, xj, qoo, qoh, qhh, A, B, f, e_el, e_vdw);
-          el += (double)e_el;
-          vdw += (double)e_vdw;
         }
+        el += (double)e_el;
+        vdw += (double)e_vdw;
 #pragma unroll
         for (int q = 0; q < 9; q++) {
           float t = f[q];

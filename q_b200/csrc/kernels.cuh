@@ -246,12 +246,26 @@ __global__ void __launch_bounds__(LRF_BLOCK, MIXED ? 8 : 5) k_lrf_gather(DevPtrs
         double rc2 = (g_sol && hs.w > 0.0) ? S.Rcpp2 : ((g_sol || hs.w > 0.0) ? S.Rcpw2 : S.Rcww2);
         if (!(r2 > rc2 && r2 <= S.RcLRF2)) continue;
         int2 rg = hrange[i];
-        for (int k = 0; k < rg.y; k++) {
-          R4 a = hat[rg.x + k];
-          if (a.w != R(0)) {
-            if (MIXED) lrf_accumulate_split((float *)mt, tt, (float)a.w, (float)(a.x - ccx), (float)(a.y - ccy),
-                                            (float)(a.z - ccz));
-            else lrf_accumulate<double>(m, (double)a.w, (double)a.x - cx, (double)a.y - cy, (double)a.z - cz);
+        if (MIXED) {
+          // a zero charge adds exact zeros; water groups (3 atoms) unrolled
+          if (rg.y == 3) {
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+              R4 a = hat[rg.x + k];
+              lrf_accumulate_split((float *)mt, tt, (float)a.w, (float)(a.x - ccx), (float)(a.y - ccy),
+                                   (float)(a.z - ccz));
+            }
+          } else {
+            for (int k = 0; k < rg.y; k++) {
+              R4 a = hat[rg.x + k];
+              lrf_accumulate_split((float *)mt, tt, (float)a.w, (float)(a.x - ccx), (float)(a.y - ccy),
+                                   (float)(a.z - ccz));
+            }
+          }
+        } else {
+          for (int k = 0; k < rg.y; k++) {
+            R4 a = hat[rg.x + k];
+            if (a.w != R(0)) lrf_accumulate<double>(m, (double)a.w, (double)a.x - cx, (double)a.y - cy, (double)a.z - cz);
           }
         }
       }
@@ -806,9 +820,11 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
 #pragma unroll
         for (int q = 0; q < 9; q++) f[q] = 0.f;
         float e_el = 0.f, e_vdw = 0.f;
+        int jn2 = k + 16 < ke ? (int)nb[k + 16] : c0;     // two entries in flight
         for (; k < ke; k += 16) {
           const int j = jn;
-          if (k + 16 < ke) jn = nb[k + 16];
+          jn = jn2;
+          if (k + 32 < ke) jn2 = nb[k + 32];
           float xj[12];
           unpack_mixed(wsm + (j - c0) * W, xj);
           ww_pair_f32(xi, xj, qoo, qoh, qhh, A, B, f, e_el, e_vdw);
@@ -843,13 +859,10 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
           for (int o = 8; o > 0; o >>= 1) fd[q] += __shfl_xor_sync(hmask, fd[q], o);
         }
       }
+      // fire-and-forget adds: the half-warp does not wait for the gradient
       if (hl == 0) {
 #pragma unroll
-        for (int a = 0; a < 3; a++) {
-          double4 dd = P.d[oi + a];
-          dd.x += fd[3 * a]; dd.y += fd[3 * a + 1]; dd.z += fd[3 * a + 2];
-          P.d[oi + a] = dd;
-        }
+        for (int a = 0; a < 3; a++) atomic_add3(P.d, oi + a, fd[3 * a], fd[3 * a + 1], fd[3 * a + 2]);
       }
     }
   }

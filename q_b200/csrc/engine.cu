@@ -59,7 +59,7 @@ struct Batch {
   cudaStream_t stream = nullptr;
   int NB = 1;
   long long istep = 0;
-  int max_natom = 0, max_lrf_blocks = 1, max_units = 0, max_nwat = 0, max_ncgp = 0, max_ncgp_sol = 0, max_terms = 0, max_pp = 0, max_ncgp_sol_w = 0, max_qp = 0;
+  int max_natom = 0, max_lrf_blocks = 1, max_nsol = 0, max_nwat = 0, max_ncgp = 0, max_ncgp_sol = 0, max_terms = 0, max_pp = 0, max_ncgp_sol_w = 0, max_qp = 0;
   bool any_lrf = false, any_q = false, any_shake = false, any_wpol = false, any_prestr = false, any_qq = false,
        any_qb = false;
   size_t watpol_smem = 0;
@@ -76,6 +76,11 @@ struct Batch {
   ~Batch() {
     if (stream) cudaStreamSynchronize(stream);
     drop_graphs();
+    for (int k = 0; k < 2; k++) {
+      if (side[k]) { cudaStreamSynchronize(side[k]); cudaStreamDestroy(side[k]); }
+      if (ev_join[k]) cudaEventDestroy(ev_join[k]);
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
     for (auto &e : event_pool) cudaEventDestroy(e);
     for (auto &pe : pending) { cudaEventDestroy(pe.second.first); cudaEventDestroy(pe.second.second); }
     for (void *p : owned) cudaFree(p);
@@ -159,11 +164,39 @@ struct Batch {
     return false;
   }
 
+  // Side streams of the force fork: after the water pass the force kernels of
+  // a step (all adding with atomics) run on three streams and join before the
+  // leap-frog.  Profiling keeps them on the main stream, one at a time.
+  cudaStream_t side[2] = {nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
+
+  void make_side_streams() {
+    for (int k = 0; k < 2; k++) {
+      CUDA_TRY(cudaStreamCreateWithFlags(&side[k], cudaStreamNonBlocking));
+      CUDA_TRY(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
+    }
+    CUDA_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+  }
+
   void pot_energy() {
     DevPtrs &p = P;
     CUDA_TRY(cudaMemsetAsync(p.d, 0, sizeof(double4) * (size_t)p.natoms_tot, stream));
     CUDA_TRY(cudaMemsetAsync(p.E, 0, sizeof(double) * QB_NE * (size_t)nsys, stream));
     CUDA_TRY(cudaMemsetAsync(p.EQ, 0, sizeof(double) * MAXS * QB_NEQ * (size_t)nsys, stream));
+    // waters first: their records, and their per-atom terms as the first
+    // gradient contribution (plain stores after the zeroing)
+    if (max_nwat > 0) {
+      dim3 gp(cdiv(max_nwat, 256), nsys);
+      if (opt.precision == QB_MIXED) launch("pack_waters", [&] { k_pack_waters<true><<<gp, 256, 0, stream>>>(p); });
+      else launch("pack_waters", [&] { k_pack_waters<false><<<gp, 256, 0, stream>>>(p); });
+    }
+    const bool fork = !profiling && side[0];
+    cudaStream_t s1 = fork ? side[0] : stream, s2 = fork ? side[1] : stream;
+    if (fork) {
+      CUDA_TRY(cudaEventRecord(ev_fork, stream));
+      CUDA_TRY(cudaStreamWaitEvent(s1, ev_fork, 0));
+      CUDA_TRY(cudaStreamWaitEvent(s2, ev_fork, 0));
+    }
     // solute terms in one launch (nonbond_pp, nonbond_qp, bonded, nonbond_qq,
     // Q bonded, restraints)
     {
@@ -179,43 +212,48 @@ struct Batch {
         launch("solute_terms", [&] {
           dim3 g(nb, nsys);
           switch (q_states) {
-            case 1: k_solute_terms<1><<<g, 256, 0, stream>>>(p, G); break;
-            case 2: k_solute_terms<2><<<g, 256, 0, stream>>>(p, G); break;
-            case 3: k_solute_terms<3><<<g, 256, 0, stream>>>(p, G); break;
-            case 4: k_solute_terms<4><<<g, 256, 0, stream>>>(p, G); break;
-            default: k_solute_terms<0><<<g, 256, 0, stream>>>(p, G);
+            case 1: k_solute_terms<1><<<g, 256, 0, s1>>>(p, G); break;
+            case 2: k_solute_terms<2><<<g, 256, 0, s1>>>(p, G); break;
+            case 3: k_solute_terms<3><<<g, 256, 0, s1>>>(p, G); break;
+            case 4: k_solute_terms<4><<<g, 256, 0, s1>>>(p, G); break;
+            default: k_solute_terms<0><<<g, 256, 0, s1>>>(p, G);
           }
         });
     }
     if (max_ncgp_sol_w > 0)
-      launch("nb_pw", [&] { k_nb_pw<<<dim3(cdiv(p.pwg_cap, PW_BLOCK), max_ncgp_sol_w, nsys), PW_BLOCK, 0, stream>>>(p); });
+      launch("nb_pw", [&] { k_nb_pw<<<dim3(cdiv(p.pwg_cap, PW_BLOCK), max_ncgp_sol_w, nsys), PW_BLOCK, 0, s1>>>(p); });
     const bool mixed = opt.precision == QB_MIXED;
     if (max_nwat > 0) {
-      dim3 gp(cdiv(max_nwat, 256), nsys), gw(cdiv(max_nwat, WW_WPB), nsys);
+      dim3 gw(cdiv(max_nwat, WW_WPB), nsys);
       size_t smem = (size_t)p.ww_chunk * (mixed ? WatRec<true>::words : WatRec<false>::words) * sizeof(float4);
       if (mixed) {
-        launch("pack_waters", [&] { k_pack_waters<true><<<gp, 256, 0, stream>>>(p); });
         launch("nb_ww", [&] { k_nb_ww<true><<<gw, WW_BLOCK, smem, stream>>>(p); });
       } else {
-        launch("pack_waters", [&] { k_pack_waters<false><<<gp, 256, 0, stream>>>(p); });
         launch("nb_ww", [&] { k_nb_ww<false><<<gw, WW_BLOCK, smem, stream>>>(p); });
       }
       if (any_q) launch("nb_qw", [&] {
         dim3 g(cdiv(max_nwat, 128), nsys);
-        if (max_nq > NQ_SHARED) { k_nb_qw<0, false><<<g, 128, 0, stream>>>(p); return; }
+        if (max_nq > NQ_SHARED) { k_nb_qw<0, false><<<g, 128, 0, s2>>>(p); return; }
         switch (q_states) {
-          case 1: k_nb_qw<1, true><<<g, 128, 0, stream>>>(p); break;
-          case 2: k_nb_qw<2, true><<<g, 128, 0, stream>>>(p); break;
-          case 3: k_nb_qw<3, true><<<g, 128, 0, stream>>>(p); break;
-          case 4: k_nb_qw<4, true><<<g, 128, 0, stream>>>(p); break;
-          default: k_nb_qw<0, true><<<g, 128, 0, stream>>>(p);
+          case 1: k_nb_qw<1, true><<<g, 128, 0, s2>>>(p); break;
+          case 2: k_nb_qw<2, true><<<g, 128, 0, s2>>>(p); break;
+          case 3: k_nb_qw<3, true><<<g, 128, 0, s2>>>(p); break;
+          case 4: k_nb_qw<4, true><<<g, 128, 0, s2>>>(p); break;
+          default: k_nb_qw<0, true><<<g, 128, 0, s2>>>(p);
         }
       });
     }
-    launch("atom_terms", [&] { k_atom_terms<<<dim3(cdiv(max_units, 128), nsys), 128, 0, stream>>>(p); });
+    if (max_nsol > 0)
+      launch("atom_terms", [&] { k_atom_terms<<<dim3(cdiv(max_nsol, 128), nsys), 128, 0, s1>>>(p); });
     if (any_wpol) {
-      launch("watpol_rank", [&] { k_watpol_rank<<<dim3(MAX_SHELLS, nsys), WPOL_BLOCK, watpol_smem, stream>>>(p); });
-      launch("watpol", [&] { k_watpol_force<<<dim3(cdiv(max_nwat, WPOL_BLOCK), nsys), WPOL_BLOCK, 0, stream>>>(p); });
+      launch("watpol_rank", [&] { k_watpol_rank<<<dim3(MAX_SHELLS, nsys), WPOL_BLOCK, watpol_smem, s2>>>(p); });
+      launch("watpol", [&] { k_watpol_force<<<dim3(cdiv(max_nwat, WPOL_BLOCK), nsys), WPOL_BLOCK, 0, s2>>>(p); });
+    }
+    if (fork) {
+      CUDA_TRY(cudaEventRecord(ev_join[0], s1));
+      CUDA_TRY(cudaEventRecord(ev_join[1], s2));
+      CUDA_TRY(cudaStreamWaitEvent(stream, ev_join[0], 0));
+      CUDA_TRY(cudaStreamWaitEvent(stream, ev_join[1], 0));
     }
     check_launch("force kernels");
   }
@@ -629,7 +667,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     S.qp_off = (int)qp_tot; qp_tot += S.qp_cap;
     S.qw_off = (int)qw_tot; qw_tot += S.qw_cap;
     B.max_natom = std::max(B.max_natom, V.natom);
-    B.max_units = std::max(B.max_units, V.nat_solute + V.nwat);
+    B.max_nsol = std::max(B.max_nsol, V.nat_solute);
     B.max_nwat = std::max(B.max_nwat, V.nwat);
     B.max_ncgp_sol = std::max(B.max_ncgp_sol, V.ncgp_solute);
     B.max_ncgp = std::max(B.max_ncgp, V.ncgp);
@@ -903,6 +941,7 @@ int qb_batch_create(qb_handle *const *systems, int n, const qb_options *opt, qb_
     if (b->b.opt.precision != QB_FP64 && b->b.opt.precision != QB_MIXED) qb::fail(QB_ERR_ARG, "unknown precision");
     CUDA_TRY(cudaStreamCreateWithFlags(&b->b.stream, cudaStreamNonBlocking));
     b->b.use_graphs = std::getenv("QB_NO_GRAPHS") == nullptr;
+    if (std::getenv("QB_ONE_STREAM") == nullptr) b->b.make_side_streams();
     qb::build(b->b, systems, n);
     // md_run's initial temperature (md.f90:3960-3963)
     qb::k_kinetic<<<dim3(b->b.P.kin_nblk, n), qb::KIN_BLOCK, 0, b->b.stream>>>(b->b.P);

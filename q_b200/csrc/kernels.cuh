@@ -651,29 +651,6 @@ __device__ __forceinline__ void watpol_angle(const DevPtrs &P, const SysDev &S, 
   P.wshell[gw] = (int8_t)shell;
 }
 
-template <bool MIXED>
-__global__ void k_pack_waters(DevPtrs P) {
-  int s = blockIdx.y;
-  const SysDev &S = P.sys[s];
-  int iw = blockIdx.x * blockDim.x + threadIdx.x;
-  if (iw >= S.nwat) return;
-  int o = S.aoff + S.nsol + 3 * iw;
-  double4 a = P.x[o], b = P.x[o + 1], c = P.x[o + 2];
-  if (S.wpol && S.nshell > 0) watpol_angle(P, S, S.woff + iw, (P.flags[o] & F_EXCL) != 0, a, b, c);
-  constexpr int W = WatRec<MIXED>::words;
-  float4 *r = P.wrec + (size_t)(S.woff + iw) * W;
-  if (MIXED) {
-    float hx = (float)a.x, hy = (float)a.y, hz = (float)a.z;
-    float lx = (float)(a.x - (double)hx), ly = (float)(a.y - (double)hy), lz = (float)(a.z - (double)hz);
-    r[0] = make_float4(hx, hy, hz, lx);
-    r[1] = make_float4(ly, lz, (float)(b.x - a.x), (float)(b.y - a.y));
-    r[2] = make_float4((float)(b.z - a.z), (float)(c.x - a.x), (float)(c.y - a.y), (float)(c.z - a.z));
-  } else {
-    double2 *rd = reinterpret_cast<double2 *>(r);
-    rd[0] = make_double2(a.x, a.y); rd[1] = make_double2(a.z, b.x); rd[2] = make_double2(b.y, b.z);
-    rd[3] = make_double2(c.x, c.y); rd[4] = make_double2(c.z, 0.0);
-  }
-}
 
 // One SPC/TIP3P molecule pair (md.f90:11823-11950, nonbond_ww_spc): the 9
 // Coulomb terms and the O-O Lennard-Jones term, gradient of molecule i added
@@ -908,7 +885,7 @@ __device__ __forceinline__ void nb_pp_body(DevPtrs &P, int bx, int s, int gx) {
 // static tables read as broadcasts.  Each thread adds its water's 9 gradient
 // components with atomics once; each solute atom's gradient is reduced over
 // the warp and added with one atomic per warp.
-constexpr int PW_BLOCK = 128;
+constexpr int PW_BLOCK = 128, PW_MAXA = 128;   // group atoms staged in shared memory
 
 __global__ void __launch_bounds__(PW_BLOCK) k_nb_pw(DevPtrs P) {
   const int s = blockIdx.z;
@@ -925,14 +902,25 @@ __global__ void __launch_bounds__(PW_BLOCK) k_nb_pw(DevPtrs P) {
   const int ow = S.aoff + S.nsol;
   const int o = ow + 3 * (act ? (int)P.pwg[(size_t)sg * P.pwg_cap + k] : 0);
   const double3 xw[3] = {ld3(P.x, o), ld3(P.x, o + 1), ld3(P.x, o + 2)};
+  // the group's atoms, parameters and positions staged once per block
+  __shared__ PwAtom sa[PW_MAXA];
+  __shared__ double4 sx[PW_MAXA];
+  const int ta = P.pwg_off[sg], na = min(P.pwg_off[sg + 1] - ta, PW_MAXA);
+  if (threadIdx.x < na) {
+    const PwAtom A = P.pwa[ta + threadIdx.x];
+    sa[threadIdx.x] = A;
+    sx[threadIdx.x] = P.x[A.atom];
+  }
+  __syncthreads();
   double fw[9];
 #pragma unroll
   for (int c = 0; c < 9; c++) fw[c] = 0.0;
   double el = 0, vdw = 0;
   const int t1 = P.pwg_off[sg + 1];
-  for (int t = P.pwg_off[sg]; t < t1; t++) {
-    const PwAtom A = P.pwa[t];
-    const double3 xi = ld3(P.x, A.atom);
+  for (int t = ta; t < t1; t++) {
+    const PwAtom A = t - ta < PW_MAXA ? sa[t - ta] : P.pwa[t];
+    const double4 x4 = t - ta < PW_MAXA ? sx[t - ta] : P.x[A.atom];
+    const double3 xi = make_double3(x4.x, x4.y, x4.z);
     double fi[3] = {0.0, 0.0, 0.0};
     if (act) {
 #pragma unroll
@@ -1160,11 +1148,7 @@ __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
     }
   }
   if (act)
-    for (int a = 0; a < 3; a++) {
-      double4 dd = P.d[j + a];
-      dd.x += fw[3 * a]; dd.y += fw[3 * a + 1]; dd.z += fw[3 * a + 2];
-      P.d[j + a] = dd;
-    }
+    for (int a = 0; a < 3; a++) atomic_add3(P.d, j + a, fw[3 * a], fw[3 * a + 1], fw[3 * a + 2]);
   for (int st = 0; st < NS; st++) {
     warp_add(&P.EQ[((size_t)s * MAXS + st) * QB_NEQ + QB_EQ_QW_EL], el[st]);
     warp_add(&P.EQ[((size_t)s * MAXS + st) * QB_NEQ + QB_EQ_QW_VDW], vdw[st]);
@@ -1253,8 +1237,8 @@ __device__ __forceinline__ void nb_qq_body(DevPtrs &P, int s) {
 //    excluded and shell atoms to their topology positions, and the radial
 //    restraint of water O atoms (harmonic outside the boundary less the
 //    thermal shift, Morse inside).
-// One thread per solute atom or per water (its three atoms share one LRF
-// record, loaded once).
+// One thread per solute atom; the water atoms' terms are added by
+// k_pack_waters (water_terms).
 struct LrfRec { double v[24]; };
 
 __device__ __forceinline__ void lrf_load(const DevPtrs &P, int gc, LrfRec &L) {
@@ -1302,11 +1286,44 @@ __device__ __forceinline__ void fix_shell_atom(const DevPtrs &P, const SysDev &S
   for (int k = 0; k < 3; k++) g[k] += fk * dr[k];
 }
 
+// Gradient contributions after the water pass are atomic adds: the force
+// kernels of one step run concurrently.
 __device__ __forceinline__ void add_grad(DevPtrs &P, int i, const double *g) {
-  if (g[0] != 0 || g[1] != 0 || g[2] != 0) {
-    double4 dd = P.d[i];
-    dd.x += g[0]; dd.y += g[1]; dd.z += g[2];
-    P.d[i] = dd;
+  if (g[0] != 0 || g[1] != 0 || g[2] != 0) atomic_add3(P.d, i, g[0], g[1], g[2]);
+}
+
+// The per-atom terms of one water (O at o, positions x): LRF Taylor terms of
+// its three atoms (one record), fixed/shell restraints, and the radial
+// restraint of its O.  Gradients into g[3][3].
+__device__ __forceinline__ void water_terms(const DevPtrs &P, const SysDev &S, int s, int o, const double3 *x,
+                                            double g[3][3], double &elrf, double &efix, double &eshell,
+                                            double &erad) {
+  const uint8_t fo = P.flags[o];
+  if (S.use_lrf && !((fo & P.flags[o + 1] & P.flags[o + 2]) & F_EXCL)) {
+    LrfRec R;
+    lrf_load(P, P.cgp[o], R);
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+      if (!(P.flags[o + a] & F_EXCL) && P.iq[o + a] < 0) elrf += lrf_eval(R, x[a], (double)P.crg[o + a], g[a]);
+  }
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const uint8_t fl = P.flags[o + a];
+    if (fl & (F_EXCL | F_SHELL)) fix_shell_atom(P, S, o + a, fl, x[a], g[a], efix, eshell);
+  }
+  if (!(fo & F_EXCL)) {
+    const double shift = S.fk_ws != 0. ? sqrt((double)kBoltzF * P.st[s].Tfree / S.fk_ws) : 0.;
+    double dr[3] = {x[0].x - S.xw[0], x[0].y - S.xw[1], x[0].z - S.xw[2]};
+    double b = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+    double db = b - (S.rwat - shift), e, dv;
+    if (db > 0) { e = 0.5 * S.fk_ws * db * db - S.Dwmz; dv = S.fk_ws * db / b; }
+    else if (b > 0.0) {
+      double fexp = exp(S.awmz * db);
+      e = S.Dwmz * (fexp * fexp - 2. * fexp);
+      dv = -2. * S.Dwmz * S.awmz * (fexp - fexp * fexp) / b;
+    } else { e = 0; dv = 0; }
+    erad += e;
+    for (int k = 0; k < 3; k++) g[0][k] += dv * dr[k];
   }
 }
 
@@ -1314,7 +1331,6 @@ __global__ void k_atom_terms(DevPtrs P) {
   int s = blockIdx.y;
   const SysDev &S = P.sys[s];
   double elrf = 0, efix = 0, eshell = 0, erad = 0;
-  const int nunit = S.nsol + S.nwat;
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u < S.nsol) {
     const int i = S.aoff + u;
@@ -1328,39 +1344,45 @@ __global__ void k_atom_terms(DevPtrs P) {
     }
     if (fl & (F_EXCL | F_SHELL)) fix_shell_atom(P, S, i, fl, xi, g, efix, eshell);
     add_grad(P, i, g);
-  } else if (u < nunit) {
-    const int o = S.aoff + 3 * u - 2 * S.nsol;        // O of water u - nsol
-    const uint8_t fo = P.flags[o];
-    const double3 x[3] = {ld3(P.x, o), ld3(P.x, o + 1), ld3(P.x, o + 2)};
+  }
+  warp_add(&P.E[s * QB_NE + QB_E_LRF], elrf);
+  warp_add(&P.E[s * QB_NE + QB_E_RST_FIX], efix);
+  warp_add(&P.E[s * QB_NE + QB_E_RST_SHELL], eshell);
+  warp_add(&P.E[s * QB_NE + QB_E_RST_SOLVENT_RADIAL], erad);
+}
+
+// Water pass, one thread per water, first kernel after the gradient is
+// zeroed: the position record of the water-water kernel (see WatRec), the
+// polarisation angle and shell, and the per-atom terms of its three atoms
+// (water_terms), stored as their first gradient contribution.
+template <bool MIXED>
+__global__ void k_pack_waters(DevPtrs P) {
+  int s = blockIdx.y;
+  const SysDev &S = P.sys[s];
+  int iw = blockIdx.x * blockDim.x + threadIdx.x;
+  double elrf = 0, efix = 0, eshell = 0, erad = 0;
+  if (iw < S.nwat) {
+    int o = S.aoff + S.nsol + 3 * iw;
+    double4 a = P.x[o], b = P.x[o + 1], c = P.x[o + 2];
+    if (S.wpol && S.nshell > 0) watpol_angle(P, S, S.woff + iw, (P.flags[o] & F_EXCL) != 0, a, b, c);
+    constexpr int W = WatRec<MIXED>::words;
+    float4 *r = P.wrec + (size_t)(S.woff + iw) * W;
+    if (MIXED) {
+      float hx = (float)a.x, hy = (float)a.y, hz = (float)a.z;
+      float lx = (float)(a.x - (double)hx), ly = (float)(a.y - (double)hy), lz = (float)(a.z - (double)hz);
+      r[0] = make_float4(hx, hy, hz, lx);
+      r[1] = make_float4(ly, lz, (float)(b.x - a.x), (float)(b.y - a.y));
+      r[2] = make_float4((float)(b.z - a.z), (float)(c.x - a.x), (float)(c.y - a.y), (float)(c.z - a.z));
+    } else {
+      double2 *rd = reinterpret_cast<double2 *>(r);
+      rd[0] = make_double2(a.x, a.y); rd[1] = make_double2(a.z, b.x); rd[2] = make_double2(b.y, b.z);
+      rd[3] = make_double2(c.x, c.y); rd[4] = make_double2(c.z, 0.0);
+    }
+    const double3 x[3] = {make_double3(a.x, a.y, a.z), make_double3(b.x, b.y, b.z), make_double3(c.x, c.y, c.z)};
     double g[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    if (S.use_lrf && !((fo & P.flags[o + 1] & P.flags[o + 2]) & F_EXCL)) {
-      LrfRec R;
-      lrf_load(P, P.cgp[o], R);
+    water_terms(P, S, s, o, x, g, elrf, efix, eshell, erad);
 #pragma unroll
-      for (int a = 0; a < 3; a++)
-        if (!(P.flags[o + a] & F_EXCL) && P.iq[o + a] < 0) elrf += lrf_eval(R, x[a], (double)P.crg[o + a], g[a]);
-    }
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      const uint8_t fl = P.flags[o + a];
-      if (fl & (F_EXCL | F_SHELL)) fix_shell_atom(P, S, o + a, fl, x[a], g[a], efix, eshell);
-    }
-    if (!(fo & F_EXCL)) {
-      const double shift = S.fk_ws != 0. ? sqrt((double)kBoltzF * P.st[s].Tfree / S.fk_ws) : 0.;
-      double dr[3] = {x[0].x - S.xw[0], x[0].y - S.xw[1], x[0].z - S.xw[2]};
-      double b = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
-      double db = b - (S.rwat - shift), e, dv;
-      if (db > 0) { e = 0.5 * S.fk_ws * db * db - S.Dwmz; dv = S.fk_ws * db / b; }
-      else if (b > 0.0) {
-        double fexp = exp(S.awmz * db);
-        e = S.Dwmz * (fexp * fexp - 2. * fexp);
-        dv = -2. * S.Dwmz * S.awmz * (fexp - fexp * fexp) / b;
-      } else { e = 0; dv = 0; }
-      erad += e;
-      for (int k = 0; k < 3; k++) g[0][k] += dv * dr[k];
-    }
-#pragma unroll
-    for (int a = 0; a < 3; a++) add_grad(P, o + a, g[a]);
+    for (int k = 0; k < 3; k++) P.d[o + k] = make_double4(g[k][0], g[k][1], g[k][2], 0.0);
   }
   warp_add(&P.E[s * QB_NE + QB_E_LRF], elrf);
   warp_add(&P.E[s * QB_NE + QB_E_RST_FIX], efix);
@@ -1896,11 +1918,9 @@ __global__ void __launch_bounds__(WPOL_BLOCK) k_watpol_force(DevPtrs P) {
       gO[c] = f0 * (-2. * f1 + f2);
       gH[c] = f0 * f1;
     }
-    double4 d0 = P.d[i], d1 = P.d[i + 1], d2 = P.d[i + 2];
-    d0.x += gO[0]; d0.y += gO[1]; d0.z += gO[2];
-    d1.x += gH[0]; d1.y += gH[1]; d1.z += gH[2];
-    d2.x += gH[0]; d2.y += gH[1]; d2.z += gH[2];
-    P.d[i] = d0; P.d[i + 1] = d1; P.d[i + 2] = d2;
+    atomic_add3(P.d, i, gO[0], gO[1], gO[2]);
+    atomic_add3(P.d, i + 1, gH[0], gH[1], gH[2]);
+    atomic_add3(P.d, i + 2, gH[0], gH[1], gH[2]);
   }
   warp_add(&P.E[s * QB_NE + QB_E_RST_WATER_POL], epol);
 }

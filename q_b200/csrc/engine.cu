@@ -135,9 +135,21 @@ struct Batch {
   void build_lists(int force) {
     DevPtrs &p = P;
     dim3 b256(256);
-    if (any_lrf)
-      launch("cgp_centers", [&] { k_cgp_centers<<<cdiv(p.ncgp_tot, 256), b256, 0, stream>>>(p, force); });
+    // main: Q-atom and solute lists; side 0: group centres and LRF multipoles;
+    // side 1: water-water list
+    cudaStream_t s1 = forking() ? side[0] : stream, s2 = forking() ? side[1] : stream;
     launch("lists_begin", [&] { k_lists_begin<<<cdiv(nsys, 128), 128, 0, stream>>>(p, force); });
+    fork_streams();
+    if (any_lrf) {
+      launch("cgp_centers", [&] { k_cgp_centers<<<cdiv(p.ncgp_tot, 256), b256, 0, s1>>>(p, force); });
+      launch("lrf_gather", [&] {
+        dim3 g(max_lrf_blocks, nsys);
+        if (opt.precision == QB_MIXED) k_lrf_gather<true><<<g, LRF_BLOCK, 0, s1>>>(p, force);
+        else k_lrf_gather<false><<<g, LRF_BLOCK, 0, s1>>>(p, force);
+      });
+    }
+    if (max_nwat > 0)
+      launch("list_ww", [&] { k_list_ww<<<dim3(cdiv(max_nwat, WL_WPB), nsys), WL_BLOCK, 0, s2>>>(p, force); });
     if (max_ncgp_sol > 0) {
       launch("list_pp", [&] { k_list_pp<<<dim3(max_ncgp_sol, nsys), 128, 0, stream>>>(p, force); });
       if (max_nwat > 0) launch("list_pw", [&] { k_list_pw<<<dim3(cdiv(max_ncgp_sol, 4), nsys), 128, 0, stream>>>(p, force); });
@@ -146,14 +158,7 @@ struct Batch {
       launch("list_qp", [&] { k_list_qp<<<nsys, 256, 0, stream>>>(p, force); });
       if (max_nwat > 0) launch("list_qw", [&] { k_list_qw<<<nsys, 256, 0, stream>>>(p, force); });
     }
-    if (max_nwat > 0)
-      launch("list_ww", [&] { k_list_ww<<<dim3(cdiv(max_nwat, WL_WPB), nsys), WL_BLOCK, 0, stream>>>(p, force); });
-    if (any_lrf)
-      launch("lrf_gather", [&] {
-        dim3 g(max_lrf_blocks, nsys);
-        if (opt.precision == QB_MIXED) k_lrf_gather<true><<<g, LRF_BLOCK, 0, stream>>>(p, force);
-        else k_lrf_gather<false><<<g, LRF_BLOCK, 0, stream>>>(p, force);
-      });
+    join_streams();
     launch("lists_end", [&] { k_lists_end<<<cdiv(nsys, 128), 128, 0, stream>>>(p, force); });
     check_launch("list kernels");
   }
@@ -178,6 +183,22 @@ struct Batch {
     CUDA_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
   }
 
+  // Fork the side streams off the main stream / join them back (no-ops when
+  // profiling or without side streams).
+  bool forking() const { return !profiling && side[0]; }
+  void fork_streams() {
+    if (!forking()) return;
+    CUDA_TRY(cudaEventRecord(ev_fork, stream));
+    for (int k = 0; k < 2; k++) CUDA_TRY(cudaStreamWaitEvent(side[k], ev_fork, 0));
+  }
+  void join_streams() {
+    if (!forking()) return;
+    for (int k = 0; k < 2; k++) {
+      CUDA_TRY(cudaEventRecord(ev_join[k], side[k]));
+      CUDA_TRY(cudaStreamWaitEvent(stream, ev_join[k], 0));
+    }
+  }
+
   void pot_energy() {
     DevPtrs &p = P;
     CUDA_TRY(cudaMemsetAsync(p.d, 0, sizeof(double4) * (size_t)p.natoms_tot, stream));
@@ -190,13 +211,8 @@ struct Batch {
       if (opt.precision == QB_MIXED) launch("pack_waters", [&] { k_pack_waters<true><<<gp, 256, 0, stream>>>(p); });
       else launch("pack_waters", [&] { k_pack_waters<false><<<gp, 256, 0, stream>>>(p); });
     }
-    const bool fork = !profiling && side[0];
-    cudaStream_t s1 = fork ? side[0] : stream, s2 = fork ? side[1] : stream;
-    if (fork) {
-      CUDA_TRY(cudaEventRecord(ev_fork, stream));
-      CUDA_TRY(cudaStreamWaitEvent(s1, ev_fork, 0));
-      CUDA_TRY(cudaStreamWaitEvent(s2, ev_fork, 0));
-    }
+    cudaStream_t s1 = forking() ? side[0] : stream, s2 = forking() ? side[1] : stream;
+    fork_streams();
     // solute terms in one launch (nonbond_pp, nonbond_qp, bonded, nonbond_qq,
     // Q bonded, restraints)
     {
@@ -249,12 +265,7 @@ struct Batch {
       launch("watpol_rank", [&] { k_watpol_rank<<<dim3(MAX_SHELLS, nsys), WPOL_BLOCK, watpol_smem, s2>>>(p); });
       launch("watpol", [&] { k_watpol_force<<<dim3(cdiv(max_nwat, WPOL_BLOCK), nsys), WPOL_BLOCK, 0, s2>>>(p); });
     }
-    if (fork) {
-      CUDA_TRY(cudaEventRecord(ev_join[0], s1));
-      CUDA_TRY(cudaEventRecord(ev_join[1], s2));
-      CUDA_TRY(cudaStreamWaitEvent(stream, ev_join[0], 0));
-      CUDA_TRY(cudaStreamWaitEvent(stream, ev_join[1], 0));
-    }
+    join_streams();
     check_launch("force kernels");
   }
 
@@ -308,10 +319,15 @@ struct Batch {
     if (due) build_lists(0);
     pot_energy();
     launch("leapfrog", [&] { k_leapfrog<<<cdiv(p.natoms_tot, 256), 256, 0, stream>>>(p); });
+    // the two SHAKE kernels move disjoint atoms
+    if (any_shake && p.nsh3 > 0 && p.nshg > 0) fork_streams();
     if (any_shake && p.nsh3 > 0)
       launch("shake", [&] { k_shake3<<<cdiv(p.nsh3, 128), 128, 0, stream>>>(p); });
-    if (any_shake && p.nshg > 0)
-      launch("shake_general", [&] { k_shake_general<<<p.nshg, SHG_BLOCK, p.shg_smem, stream>>>(p); });
+    if (any_shake && p.nshg > 0) {
+      cudaStream_t s1 = forking() && p.nsh3 > 0 ? side[0] : stream;
+      launch("shake_general", [&] { k_shake_general<<<p.nshg, SHG_BLOCK, p.shg_smem, s1>>>(p); });
+    }
+    if (any_shake && p.nsh3 > 0 && p.nshg > 0) join_streams();
     launch("finish", [&] { k_finish<<<nsys, 32, 0, stream>>>(p, 1); });
     check_launch("step kernels");
   }

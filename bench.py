@@ -50,7 +50,7 @@ def parse():
     p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="qb", choices=["qb", "reference"])
-    p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    p.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     p.add_argument("--windows", type=int, default=21)
     p.add_argument("--replicas", type=int, default=4)
     p.add_argument("--spheres", type=int, default=16)

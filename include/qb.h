@@ -24,6 +24,7 @@
 
 #include <stddef.h>
 #include "qb_system.h"
+#include "qb_fep.h"
 
 #ifdef __cplusplus
 extern "C" {

@@ -52,6 +52,7 @@ def _struct_from_header(path: str, name: str) -> type:
     source of truth."""
     src = open(path).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    defines = {k: int(v) for k, v in re.findall(r"#define\s+(\w+)\s+(\d+)\b", src)}
     m = re.search(r"typedef struct %s \{(.*?)\} %s;" % (name, name), src, flags=re.S)
     if not m:
         raise RuntimeError(f"{name} not found in {path}")
@@ -77,9 +78,10 @@ def _struct_from_header(path: str, name: str) -> type:
             item = item.strip()
             ptr = item.startswith("*")
             item = item.lstrip("*").strip()
-            arr = re.match(r"(\w+)\[(\d+)\]", item)
+            arr = re.match(r"(\w+)\[(\w+)\]", item)
             if arr:
-                fields.append((arr.group(1), base[tname] * int(arr.group(2))))
+                dim = arr.group(2)
+                fields.append((arr.group(1), base[tname] * (int(dim) if dim.isdigit() else defines[dim])))
             elif ptr:
                 fields.append((item, C.POINTER(base[tname])))
             else:
@@ -133,6 +135,8 @@ def _load():
         "qb_batch_destroy": (None, [vp]),
         "qb_write_re": (C.c_int, [C.c_char_p, C.c_int, dp, dp, C.c_int, fp]),
         "qb_append_en": (C.c_int, [C.c_char_p, C.c_int, dp]),
+        "qb_fep_analyze": (C.c_int, [dp, ip, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
+        "qb_batch_fep": (C.c_int, [vp, ip, C.c_int, C.c_void_p, C.c_void_p]),
         "qb_maxwell": (C.c_int, [C.c_int, C.c_double, C.c_int, dp, dp]),
         "qb_ww_energy_static": (C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_double, C.c_double,
                                           C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

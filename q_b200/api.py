@@ -96,6 +96,12 @@ class Batch:
     def final_energy(self) -> None:
         check(lib.qb_batch_final_energy(self._b))
 
+    def fep(self, systems, rt: float, nskip: int = 0, **kw):
+        """qfep's analysis of these systems' energy-file records, in window
+        order (q_b200.fep.params for the keyword arguments)."""
+        from .fep import batch_fep, params
+        return batch_fep(self, systems, params(rt, nskip, **kw))
+
     def energies(self, sys: int) -> tuple[dict, list[dict]]:
         E = np.zeros(QB_NE)
         S = self.systems[sys].nstates

@@ -13,6 +13,7 @@
 #include <string>
 #include <vector>
 
+#include "fep.hpp"
 #include "kernels.cuh"
 #include "qsystem.hpp"
 
@@ -1042,6 +1043,33 @@ int qb_batch_run_timed(qb_batch *bb, int nsteps, double *device_ms, long long *k
     if (B.profiling) B.collect();
     B.sync_status();
     qb::refresh_workload(B, nsteps);
+  });
+}
+
+int qb_batch_fep(qb_batch *bb, const int *sys, int nfiles, const qb_fep_params *p, qb_fep_result *out) {
+  if (!bb || !sys || !p || nfiles < 1) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
+  return guarded_batch([&] {
+    Batch &B = bb->b;
+    CUDA_TRY(cudaSetDevice(B.opt.device));
+    CUDA_TRY(cudaStreamSynchronize(B.stream));
+    std::vector<qb::SysState> st(B.nsys);
+    CUDA_TRY(cudaMemcpy(st.data(), B.P.st, sizeof(qb::SysState) * B.nsys, cudaMemcpyDeviceToHost));
+    // energy-file records (kind 1) of each system, read in place in the ring
+    const long long rec_len = QB_NE + qb::MAXS * QB_NEQ + 1;
+    qb::FepSource src;
+    src.base = B.P.hist;
+    src.rec_stride = (int)rec_len;
+    for (int f = 0; f < nfiles; f++) {
+      const int s = sys[f];
+      if (s < 0 || s >= B.nsys) qb::fail(QB_ERR_ARG, "system index out of range");
+      const int ns = B.sysh[s].S;
+      if (f == 0) src.nstates = ns;
+      else if (ns != src.nstates) qb::fail(QB_ERR_ARG, "systems with different numbers of states");
+      if (!B.P.hist) qb::fail(QB_ERR_STATE, "no energy records: run the batch first");
+      src.foff.push_back((((long long)B.nsys + s) * B.P.hist_cap) * rec_len + 1 + QB_NE);
+      src.npts.push_back(std::min(st[s].hist_n[1], B.P.hist_cap));
+    }
+    qb::fep_run(src, *p, B.opt.device, B.stream, out);
   });
 }
 

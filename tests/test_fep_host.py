@@ -1,0 +1,94 @@
+"""Free-energy analysis, host side (no GPU): the qfep restatement (oracle)
+on analytic cases, the energy-file reader against libqb's writer, qfep's
+input reading and its Fortran number editing."""
+import io
+import math
+
+import numpy as np
+import pytest
+
+from oracle.qfep_oracle import FepInput, analyze
+
+
+def gaussian_windows(nf=11, n=3000, mu=2.0, s2=0.5, rt=0.592, seed=1):
+    """Two states coupled linearly, U(l) = (1-l) U1 + l U2, with dU = U2 - U1
+    Gaussian N(mu, s2) at l = 0.  At window l it is N(mu - l s2/kT, s2) and
+    dG = mu - s2/(2 kT) exactly."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for l in np.linspace(0.0, 1.0, nf):
+        e = np.zeros((n, 2, 15))
+        e[:, 0, 0], e[:, 1, 0] = 1.0 - l, l
+        u1 = rng.normal(0.0, 1.0, n)
+        du = rng.normal(mu - l * s2 / rt, math.sqrt(s2), n)
+        e[:, 0, 1], e[:, 1, 1] = u1, u1 + du
+        out.append(e)
+    return out, mu - s2 / (2 * rt)
+
+
+def test_estimators_on_gaussian_perturbation():
+    rt = 0.592
+    E, exact = gaussian_windows(rt=rt)
+    r = analyze(FepInput(E, rt, 100, nbins=10, nmin=10, alfa=[0.0], coeff=[1.0, -1.0]))
+    nf = len(E)
+    for est in (r.dgfsum[nf], -r.dgrsum[1], r.dgbarsum[nf], r.dglusum[nf], r.dG[nf]):
+        assert abs(est - exact) < 0.05, (est, exact)
+    # TI: trapezoid of <U2 - U1> over the step of lambda(1), lambda(i-1) - lambda(i)
+    assert abs(r.dgtisum[nf] - exact) < 0.05
+    assert all(1 <= k < 100 for k in r.bar_iterations)
+
+
+def test_identical_windows_give_zero_and_alpha_shifts_gap():
+    rng = np.random.default_rng(3)
+    e = np.zeros((500, 2, 15))
+    e[:, :, 0] = 0.5
+    e[:, :, 1] = rng.normal(0, 1, (500, 2))
+    r = analyze(FepInput([e, e.copy()], 0.6, 0, nbins=5, nmin=1, alfa=[0.0], coeff=[1.0, -1.0]))
+    assert r.dgfsum[2] == pytest.approx(0.0, abs=1e-12) and r.dgbarsum[2] == pytest.approx(0.0, abs=1e-9)
+    r2 = analyze(FepInput([e, e.copy()], 0.6, 0, nbins=5, nmin=1, alfa=[3.0], coeff=[1.0, -1.0]))
+    assert r2.gapmin == pytest.approx(r.gapmin - 3.0) and r2.gapmax == pytest.approx(r.gapmax - 3.0)
+
+
+def test_part0_uses_single_precision_scale():
+    e = np.zeros((7, 1, 15))
+    e[:, 0, 1] = 1.0
+    r = analyze(FepInput([e, e], 0.6, 0, nbins=2, nmin=1))
+    k = float(np.float32(1.0) / np.float32(7))
+    assert r.avEQ[0, 0, 1] == 7.0 * k and r.avEQ[0, 0, 1] != 1.0
+
+
+def test_energy_file_reader_round_trip(tmp_path):
+    from q_b200 import append_energy
+    from q_b200.fep import read_en
+    path = str(tmp_path / "w.en")
+    rng = np.random.default_rng(0)
+    frames = rng.normal(size=(6, 2, 15))
+    for k in range(6):
+        append_energy(path, frames[k])
+    got = read_en(path, 2)
+    assert got.shape == (6, 2, 15) and np.array_equal(got, frames)
+    # a frame without its off-diagonal record is not counted (get_ene)
+    raw = open(path, "rb").read()
+    open(path, "wb").write(raw[:-8])
+    assert read_en(path, 2).shape[0] == 5
+
+
+def test_fortran_number_editing():
+    from q_b200.qfep import fmt_f, fmt_i
+    assert fmt_f(1.0, 8, 6) == "1.000000"
+    assert fmt_f(-0.123, 8, 6) == "-.123000"
+    assert fmt_f(-1.5, 9, 3) == "   -1.500"
+    assert fmt_f(1e9, 9, 3) == "*" * 9
+    assert fmt_f(-math.inf, 9, 3) == "-Infinity" and fmt_f(math.nan, 9, 3) == "      NaN"
+    assert fmt_i(123456, 4) == "****" and fmt_i(5, 4) == "   5"
+
+
+def test_qfep_input_records():
+    from q_b200.qfep import _Input
+    text = "3\n2  0\n0.592  50\n\n50\n10\n0\n0\n1 0\n!ENERGY_FILES\na.en\nb.en\nc.en\n"
+    inp = _Input(io.StringIO(text))
+    assert inp.values(1) == ["3"] and inp.values(2) == ["2", "0"]
+    assert inp.record().split() == ["0.592", "50"]
+    assert inp.values(1) == ["50"] and inp.values(1) == ["10"]
+    assert inp.values(1) == ["0"] and inp.values(1) == ["0"] and inp.values(2) == ["1", "0"]
+    assert [inp.values(1)[0] for _ in range(3)] == ["a.en", "b.en", "c.en"]

@@ -99,6 +99,11 @@ int qb_batch_create(qb_handle *const *systems, int n, const qb_options *opt, qb_
  * (md.f90:4003-4175): pair lists every NBcycle steps, potential and gradient,
  * leapfrog with Berendsen scaling, SHAKE, temperature.  Energy summaries are
  * recorded on the device at each system's output/energy intervals.
+ * A system that raises an error on the device (e.g. QB_ERR_SHAKE) stops at
+ * the failing step, as md_run stops there: its coordinates stay those the
+ * step produced (positions at the step's start = x - v*dt), its step count
+ * and records stop, and the call returns the first such error once the
+ * other systems have finished their steps.
  * Replaces: the `do istep` loop of md_run, src/q6/md.f90:4003-4175. */
 int qb_batch_run(qb_batch *b, int nsteps);
 

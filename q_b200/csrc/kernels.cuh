@@ -1967,7 +1967,8 @@ __global__ void k_leapfrog(DevPtrs P) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   int s = -1;
   double acc[4] = {0, 0, 0, 0};
-  if (g < P.natoms_tot) {
+  // a system that raised an error stays where the failing step left it
+  if (g < P.natoms_tot && P.st[P.asys[g]].status == 0) {
     s = P.asys[g];
     const SysDev &S = P.sys[s];
     double ts = (g - S.aoff) < S.nsol ? P.st[s].Tscale_sol : P.st[s].Tscale_solv;
@@ -2033,7 +2034,7 @@ __global__ void __launch_bounds__(128, 6) k_shake3(DevPtrs P) {
   int m = blockIdx.x * blockDim.x + threadIdx.x;
   int sys = -1, its = 0;
   double acc[4] = {0, 0, 0, 0};
-  if (m < P.nsh3) {
+  if (m < P.nsh3 && P.st[P.sh3_at[m].w].status == 0) {
     const int4 at = P.sh3_at[m];
     const double4 d2 = P.sh3_d2[m];
     sys = at.w;
@@ -2098,6 +2099,11 @@ __global__ void __launch_bounds__(SHG_BLOCK) k_shake_general(DevPtrs P) {
   const int *at = P.shg_at + info.x;
   const int2 *cij = P.shg_c + info.z;
   const int *lev = P.shg_lev + info2.x;
+  // a system that raised an error stays where the failing step left it
+  __shared__ int frozen;
+  if (threadIdx.x == 0) frozen = P.st[sys].status;
+  __syncthreads();
+  if (frozen) return;
   for (int t = threadIdx.x; t < na; t += SHG_BLOCK) {
     double4 x = P.x[at[t]];
     x.w = (double)P.winv[at[t]];
@@ -2257,6 +2263,11 @@ __global__ void k_finish(DevPtrs P, int mode) {
   int lane = threadIdx.x;
   if (mode != 0) finalize_energy(P, s);
   if (mode == 2) return;
+  if (mode == 1 && st.status != 0) {
+    // failed at this step: no records, the step count stays at the failure
+    if (lane < 4) P.kin[s * 4 + lane] = 0.0;
+    return;
+  }
   if (lane == 0) {
     double tot[4];
     for (int k = 0; k < 4; k++) { tot[k] = P.kin[s * 4 + k]; P.kin[s * 4 + k] = 0.0; }

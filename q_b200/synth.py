@@ -9,7 +9,8 @@ Shapes (one generator per configuration):
   water_sphere(R)   TIP3P on a cubic lattice at 0.0334 / A^3 inside radius R,
                     seeded random orientations (config 0: R = 15).
   fep_solute(...)   a 32-heavy-atom random tree with hydrogens up to 56 atoms,
-                    charges ~N(0, 0.3) shifted to net 0, LJ from a 6-type
+                    net-zero charges (hydrogens +0.10 +- 0.04, heavy atoms
+                    ~N(0, 0.35) absorbing the balance), LJ from a 6-type
                     table, harmonic bonds/angles, periodic torsions (n=1..3),
                     periodic impropers on 3-connected centres, 8 Q-atoms with
                     two states (state 2: charge 0, epsilon x 0.5, soft-core),
@@ -313,7 +314,11 @@ def _angle(a, b, c) -> float:
 
 def random_tree_solute(rng, n_heavy: int = 32, n_total: int = 56):
     """Heavy-atom tree with hydrogens; returns coordinates, element kinds
-    (type index or -1 for H), bonds."""
+    (type index or -1 for H), bonds.  Bond angles stay within 105-150 degrees
+    (hydrogens 100-150): the angle terms take the generated geometry as their
+    equilibrium, and a harmonic angle close to linear has a cusp at 180
+    degrees (its force flips direction there) that feeds energy into the
+    bend until the constraints of a neighbouring hydrogen fail."""
     X = [np.zeros(3)]
     bonds = []
     deg = [0]
@@ -329,7 +334,8 @@ def random_tree_solute(rng, n_heavy: int = 32, n_total: int = 56):
             d[p] = 99
             if d.min() < 2.5:
                 continue
-            if any(_angle(X[q], X[p], c) < 105 for (a, b) in bonds for q in ((b,) if a == p else (a,) if b == p else ())):
+            if any(not 105 <= _angle(X[q], X[p], c) <= 150
+                   for (a, b) in bonds for q in ((b,) if a == p else (a,) if b == p else ())):
                 continue
             X.append(c)
             deg.append(1)
@@ -358,7 +364,7 @@ def random_tree_solute(rng, n_heavy: int = 32, n_total: int = 56):
                 if d.min() < 2.0:
                     continue
                 nbrs = [b if a == p else a for a, b in bonds if p in (a, b)]
-                if any(_angle(X[q], X[p], c) < 100 for q in nbrs):
+                if any(not 100 <= _angle(X[q], X[p], c) <= 150 for q in nbrs):
                     continue
                 X.append(c)
                 kinds.append(-1)
@@ -420,6 +426,23 @@ def _net_zero_charges(rng, n: int, sd: float = 0.3, total: float = 0.0) -> list[
     q = q - q.mean() + total / n
     q = np.round(q, 4)
     q[-1] = round(total - float(q[:-1].sum()), 4)
+    return [float(v) for v in q]
+
+
+def _solute_charges(rng, kinds) -> list[float]:
+    """Net-zero partial charges of a tree solute in force-field ranges:
+    hydrogens +0.10 +- 0.04 (within 0..0.20), heavy atoms 0.35 sigma (within
+    +-0.70) shifted to cancel the total.  A hydrogen never carries a negative
+    charge: water hydrogens have no Lennard-Jones repulsion, and a negative
+    hydrogen binds them at about 1.2 A until a collision breaks the water's
+    constraints.  Draws the same random numbers as _net_zero_charges(rng, n)."""
+    z = rng.normal(0.0, 1.0, size=len(kinds))
+    hyd = np.array([k < 0 for k in kinds])
+    q = np.where(hyd, np.clip(0.10 + 0.04 * z, 0.0, 0.20), np.clip(0.35 * z, -0.70, 0.70))
+    heavy = np.flatnonzero(~hyd)
+    q[heavy] -= q.sum() / len(heavy)
+    q = np.round(q, 4)
+    q[heavy[-1]] = round(-float(q.sum() - q[heavy[-1]]), 4)
     return [float(v) for v in q]
 
 
@@ -510,7 +533,7 @@ def fep_solute(outdir: str, radius: float = 20.0, seed: int = 1234, steps: int =
     top = Topology(title="fep_solute", rexcl_o=radius, rwat=radius, types=types)
     top.x = [tuple(float(c) for c in p) for p in X]
     top.iac = iac
-    top.crg = _net_zero_charges(rng, n)
+    top.crg = _solute_charges(rng, kinds)
     _solute_terms(top, X, bonds, rng)
     top.nat_solute = n
     top.nbonds_solute, top.nangles_solute = len(top.bonds), len(top.angles)
@@ -592,7 +615,8 @@ def polymer_sphere(outdir: str, radius: float = 25.0, seed: int = 1234, steps: i
                 u = rng.normal(size=3)
                 u /= np.linalg.norm(u)
                 c = pts[chain[-1]] + 1.5 * u
-                if len(chain) > 1 and _angle(pts[chain[-2]], pts[chain[-1]], c) < 100:
+                # chain angles 100-150 degrees (no near-linear angle terms)
+                if len(chain) > 1 and not 100 <= _angle(pts[chain[-2]], pts[chain[-1]], c) <= 150:
                     continue
                 if free(c, chain[-1]):
                     ok = True
@@ -612,7 +636,7 @@ def polymer_sphere(outdir: str, radius: float = 25.0, seed: int = 1234, steps: i
     top = Topology(title="polymer_sphere", rexcl_o=restrain_beyond, rwat=radius, types=types)
     top.x = [tuple(float(c) for c in p) for p in X]
     top.iac = iac
-    crg = _net_zero_charges(rng, n_lig)
+    crg = _solute_charges(rng, kinds)
     pbonds = [(a, b) for ch in chains for a, b in zip(ch[:-1], ch[1:])]
     # residue-like charge groups of 10-15 consecutive chain atoms, net charge -1/0/+1
     groups = []

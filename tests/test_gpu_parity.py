@@ -208,3 +208,34 @@ def test_graph_replay_matches_direct_launches(synthetic, monkeypatch):
     assert list(s0) == list(s1)
     assert np.max(np.abs(E0 - E1)) < 1e-6 and np.max(np.abs(Q0 - Q1)) < 1e-6
     assert np.max(np.abs(x0 - x1)) < 1e-8
+
+
+@pytest.mark.parametrize("kicked", ["water", "solute"])
+def test_failed_system_stops_at_its_step(synthetic, kicked):
+    """A system whose constraints fail stops where md_run stops (md.f90:14533
+    'shake failure'): the error names the failing step, the system's
+    positions stay those of that step (start = x - v*dt), its records stop,
+    and the other systems of the batch carry on.  The failure is made by a
+    40 A kick on one hydrogen, which no SHAKE sweep can absorb in 1000
+    iterations (rigid-water kernel for a water hydrogen, the block-per-molecule
+    kernel for a solute hydrogen)."""
+    from q_b200 import QBError
+    inp = synthetic["c1"].inp
+    systems = [System.open(inp, lambdas=(0.5, 0.5), seed=3 + k) for k in range(2)]
+    b = Batch(systems, precision=FP64)
+    b.run(10)
+    nsol = 56
+    atom = nsol + 1 if kicked == "water" else nsol - 1   # first water's H1 / last solute hydrogen
+    x10 = b.coords(1)
+    v = b.velocities(1).reshape(-1, 3)
+    v[atom] = (1000.0, 0.0, 0.0)
+    b.set_velocities(1, v.reshape(-1))
+    with pytest.raises(QBError) as err:
+        b.run(20)
+    assert err.value.code == 5 and "system 1 " in str(err.value) and "at step 10" in str(err.value)
+    assert b.status(0) == 0 and b.status(1) == 5
+    dt = systems[1].view.dt
+    start = b.coords(1) - b.velocities(1) * dt
+    assert np.max(np.abs(start - x10)) < 1e-9
+    assert list(b.history(0, 1)[0]) == [10, 20]
+    assert len(b.history(1, 1)[0]) == 0

@@ -16,6 +16,13 @@ records and final coordinates read back, all inside the timed region.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl qb|reference]
                     [--precision fp64|mixed]
 
+At one GPU the line also carries the second half of the metric (`dG`,
+`gpu_s_per_dG`): the perturbation's BAR free energy from 21 uniform windows x
+--dg-replicas replicas in one mixed-precision batch, its device seconds, the
+plain FP64 engine's device seconds for the same windows, replicas and steps
+run one system per launch (its per-step time measured here), and the error
+against a dense 41-window FP64 run of the same perturbation.
+
 Under torchrun each rank runs its own copy of the batch (weak scaling); time is
 the maximum over ranks.  `--impl reference` times the CPU oracle (the
 restatement of Q's Fortran step, which cannot be compiled here) on a bounded
@@ -56,6 +63,13 @@ def parse():
     p.add_argument("--spheres", type=int, default=16)
     p.add_argument("--equil", type=int, default=100, help="untimed equilibration steps (in addition to warm-up)")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--dg-replicas", type=int, default=16,
+                   help="replicas of the batched mixed-precision perturbation for the GPU-s per dG comparison "
+                        "(0 skips it; runs at one GPU only)")
+    p.add_argument("--dg-ref-replicas", type=int, default=16, help="replicas of the dense FP64 reference")
+    p.add_argument("--dg-ref-windows", type=int, default=41)
+    p.add_argument("--dg-equil", type=int, default=1000)
+    p.add_argument("--dg-steps", type=int, default=10000, help="production steps per window")
     return p.parse_args()
 
 
@@ -365,9 +379,24 @@ def main():
     }
     if cpu:
         line["cpu_baseline"] = cpu
+    batch.close()
+    if rank == 0 and world == 1 and args.dg_replicas > 0:
+        # second half of the metric: device seconds per dG, batched mixed
+        # precision against the plain FP64 engine one system per launch,
+        # the dG error judged by a dense-window FP64 run
+        from q_b200.campaign import dg_versus_plain
+        t0 = time.perf_counter()
+        dg = dg_versus_plain(specs[0][0], windows=args.windows, replicas=args.dg_replicas,
+                             ref_windows=args.dg_ref_windows, ref_replicas=args.dg_ref_replicas,
+                             steps_eq=args.dg_equil, steps_prod=args.dg_steps, device=local)
+        dg["wall_s"] = round(time.perf_counter() - t0, 1)
+        line["dG"] = dg
+        line["gpu_s_per_dG"] = {"batched_mixed": dg["batched_mixed"]["gpu_seconds"],
+                                "plain_fp64": dg["plain_fp64_one_system_per_launch"]["gpu_seconds"],
+                                "ratio": dg["gpu_seconds_ratio_plain_over_batched"],
+                                "dG_error_vs_fp64_dense": dg["dG_error"], "dG_error_sem": dg["dG_error_sem"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    batch.close()
     if dist:
         dist.destroy_process_group()
 

@@ -17,7 +17,10 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <list>
+#include <mutex>
 #include <sstream>
+#include <sys/stat.h>
 
 #include "qsystem.hpp"
 
@@ -546,7 +549,47 @@ void read_inp(const std::string &path, RunInput &in) {
 
 // --------------------------------------------------------------- topology
 
+namespace {
+void parse_topology(const std::string &path, Topology &t);
+
+// Parsed topologies by file identity (path, size, modification time): a
+// perturbation opens one .inp once per window and replica, and parsing the
+// text topology dominated opening.  Entries are copied out, never shared.
+struct TopologyCache {
+  struct Entry {
+    std::string path;
+    long long size, mtime_ns;
+    Topology top;
+  };
+  std::mutex mu;
+  std::list<Entry> entries;   // most recent first
+  static constexpr size_t kMax = 8;
+};
+TopologyCache g_topology_cache;
+}  // namespace
+
 void read_topology(const std::string &path, Topology &t) {
+  struct stat st;
+  if (stat(path.c_str(), &st) != 0) { parse_topology(path, t); return; }
+  const long long size = (long long)st.st_size;
+  const long long mtime = (long long)st.st_mtim.tv_sec * 1000000000LL + st.st_mtim.tv_nsec;
+  {
+    std::lock_guard<std::mutex> g(g_topology_cache.mu);
+    for (auto it = g_topology_cache.entries.begin(); it != g_topology_cache.entries.end(); ++it)
+      if (it->path == path && it->size == size && it->mtime_ns == mtime) {
+        t = it->top;
+        g_topology_cache.entries.splice(g_topology_cache.entries.begin(), g_topology_cache.entries, it);
+        return;
+      }
+  }
+  parse_topology(path, t);
+  std::lock_guard<std::mutex> g(g_topology_cache.mu);
+  g_topology_cache.entries.push_front({path, size, mtime, t});
+  if (g_topology_cache.entries.size() > TopologyCache::kMax) g_topology_cache.entries.pop_back();
+}
+
+namespace {
+void parse_topology(const std::string &path, Topology &t) {
   Records r(path);
   std::string title = r.line();
   t.ff_type = 1;
@@ -834,6 +877,7 @@ void read_topology(const std::string &path, Topology &t) {
   }
   (void)nwat;
 }
+}  // namespace
 
 // -------------------------------------------------------------------- FEP
 

@@ -114,3 +114,22 @@ def test_batch_records_analysed_in_place(tmp_path):
     for name in ("dgf", "dgr", "dgbar", "dgbarsum", "dglu", "dgti"):
         assert np.allclose(getattr(r, name), getattr(h, name), rtol=1e-12, atol=1e-12), name
     assert list(r.npts) == [s.shape[0] for s in series] and r.npts[0] >= 5
+
+
+def test_perturbation_campaign(tmp_path):
+    """Windows x replicas of one perturbation in one batch: equilibration
+    records dropped, production records analysed per replica, device time
+    measured; the plain engine's per-step time for one window."""
+    from q_b200 import MIXED, synth
+    from q_b200.campaign import run_perturbation, time_single_window
+    g = synth.fep_solute(str(tmp_path / "c1"), seed=1234, steps=1000)
+    r = run_perturbation(g.inp, synth.window_lambdas(3), replicas=2, steps_eq=20, steps_prod=100,
+                         precision=MIXED, seed0=5)
+    assert (r.windows, r.replicas, r.steps) == (3, 2, 120)
+    assert r.records_per_window == 10            # energy interval 10, records after the equilibration only
+    assert len(r.dG) == 2 and all(np.isfinite(r.dG)) and r.dG[0] != r.dG[1]
+    assert abs(r.dG_mean - np.mean(r.dG)) < 1e-12 and r.dG_sem > 0
+    assert all(len(b) == 2 for b in r.bar)
+    assert all(abs(sum(b) - d) < 1e-9 for b, d in zip(r.bar, r.dG))
+    assert r.gpu_seconds > 0
+    assert 0 < time_single_window(g.inp, (0.5, 0.5), 20, warmup=5) < 0.1

@@ -132,6 +132,37 @@ def test_synthetic_systems_parse(tmp_path):
     assert (lam[0], lam[1]) == (0.25, 0.75)
 
 
+def test_threaded_open_matches_sequential(tmp_path):
+    """Windows and replicas opened on a thread pool (the perturbation
+    campaign's path) are the systems sequential opens give, and a topology
+    edited on disk is read again rather than served from the parse cache."""
+    from q_b200.campaign import open_systems
+    g = synth.fep_solute(str(tmp_path / "c1"), seed=1234, steps=100)
+    lams = synth.window_lambdas(5)
+    seq = [System.open(g.inp, lambdas=l, seed=s) for s in (3, 4) for l in lams]
+    par = open_systems(g.inp, lams, (3, 4), threads=4)
+    assert len(par) == len(seq) == 10
+    for a, b in zip(seq, par):
+        assert tuple(a.array("lambda", a.nstates)) == tuple(b.array("lambda", b.nstates))
+        assert np.array_equal(a.array("x0", 3 * a.natom), b.array("x0", 3 * b.natom))
+        assert np.array_equal(a.array("v0", 3 * a.natom), b.array("v0", 3 * b.natom))
+    # velocities differ between replicas, not between windows of one replica
+    assert np.array_equal(par[0].array("v0", 30), par[4].array("v0", 30))
+    assert not np.array_equal(par[0].array("v0", 30), par[5].array("v0", 30))
+    # same path, new content: the charge of solute atom 10 (not a Q-atom) changed
+    top = open(g.top).read().split("\n")
+    k = next(i for i, l in enumerate(top) if "No. of atomic charges" in l)
+    row = top[k + 2].split()
+    row[0] = "%7.4f" % (float(row[0]) + 0.5)
+    top[k + 2] = " ".join(row)
+    import time as _t
+    _t.sleep(0.01)
+    open(g.top, "w").write("\n".join(top))
+    c = System.open(g.inp, lambdas=lams[0], seed=3)
+    dq = (c.array("crg", 11)[10] - seq[0].array("crg", 11)[10]) / np.sqrt(332.0716)
+    assert abs(dq - 0.5) < 1e-3
+
+
 def test_qdyn_log_layout():
     from q_b200.qdyn import write_out
     E = np.zeros(29)

@@ -25,6 +25,7 @@
 #include <stddef.h>
 #include "qb_system.h"
 #include "qb_fep.h"
+#include "qb_mlp.h"
 
 #ifdef __cplusplus
 extern "C" {

@@ -137,6 +137,9 @@ def _load():
         "qb_append_en": (C.c_int, [C.c_char_p, C.c_int, dp]),
         "qb_fep_analyze": (C.c_int, [dp, ip, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
         "qb_batch_fep": (C.c_int, [vp, ip, C.c_int, C.c_void_p, C.c_void_p]),
+        "qb_mlp_forward": (C.c_int, [fp, fp, C.c_int, fp, C.c_int]),
+        "qb_mlp_loss_grad": (C.c_int, [fp, fp, fp, C.c_int, fp, fp, C.c_int]),
+        "qb_mlp_train": (C.c_int, [fp, fp, fp, C.c_int, C.c_int, C.c_void_p, fp, C.c_int]),
         "qb_maxwell": (C.c_int, [C.c_int, C.c_double, C.c_int, dp, dp]),
         "qb_ww_energy_static": (C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_double, C.c_double,
                                           C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -22,7 +22,7 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.path.join(REPO, "include"),
           "-I" + CSRC]
-SOURCES = ["qfiles.cpp", "setup.cpp", "capi.cpp", "engine.cu", "noalloc.cu", "fep.cu"]
+SOURCES = ["qfiles.cpp", "setup.cpp", "capi.cpp", "engine.cu", "noalloc.cu", "fep.cu", "mlp.cu"]
 
 
 def _stale(obj: str, deps: list[str]) -> bool:

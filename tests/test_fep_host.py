@@ -92,3 +92,21 @@ def test_qfep_input_records():
     assert inp.values(1) == ["50"] and inp.values(1) == ["10"]
     assert inp.values(1) == ["0"] and inp.values(1) == ["0"] and inp.values(2) == ["1", "0"]
     assert [inp.values(1)[0] for _ in range(3)] == ["a.en", "b.en", "c.en"]
+
+
+def test_mlp_oracle_gradient_is_exact():
+    """The network oracle's analytic gradient against central differences."""
+    from oracle import mlp_oracle as M
+    p = M.init(1)
+    rng = np.random.default_rng(2)
+    x, t = rng.normal(size=(40, M.IN)), rng.normal(size=(40, M.OUT))
+    L, g = M.loss_grad(p, x, t)
+    h = 1e-6
+    for k in rng.choice(M.NPARAM, 60, replace=False):
+        e = np.zeros(M.NPARAM)
+        e[k] = h
+        num = (M.loss_grad(p + e, x, t)[0] - M.loss_grad(p - e, x, t)[0]) / (2 * h)
+        assert abs(num - g[k]) < 1e-7 * max(1.0, abs(g[k]))
+    # the BF16 rounding used by the oracle: ties to even, exact on BF16 values
+    v = np.array([1.0, 1.00390625, 1.005859375, -3.0e-3], dtype=np.float32)
+    assert list(M.bf16(v)) == [1.0, 1.0, 1.0078125, float(np.float32(-0.0030059814453125))]

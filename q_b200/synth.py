@@ -498,16 +498,18 @@ def water_sphere(outdir: str, radius: float = 15.0, seed: int = 1234, steps: int
 
 
 def _fep_file(path: str, types: list[AtomType], iac: list[int], q: list[float], qatoms: list[int],
-              alpha: float = 20.0) -> None:
+              alpha: float = 20.0, charge_scale: float = 0.0, eps_scale: float = 0.5) -> None:
+    """Two-state FEP file: state 2 scales the Q-atoms' charges by
+    charge_scale and their epsilon by eps_scale, soft-core alpha in state 2."""
     L = ["[FEP]", "states 2", "", "[atoms]"]
     L += ["%d %d" % (k + 1, a + 1) for k, a in enumerate(qatoms)]
     L += ["", "[change_charges]"]
-    L += ["%d %8.4f %8.4f" % (k + 1, q[a], 0.0) for k, a in enumerate(qatoms)]
+    L += ["%d %8.4f %8.4f" % (k + 1, q[a], round(q[a] * charge_scale, 4)) for k, a in enumerate(qatoms)]
     L += ["", "[atom_types]"]
     names = []
     for k, a in enumerate(qatoms):
         t = types[iac[a]]
-        for st, scale in ((1, 1.0), (2, 0.5)):
+        for st, scale in ((1, 1.0), (2, eps_scale)):
             nm = "Q%d_%d" % (k + 1, st)
             aa, bb = lj_sqrt(t.sigma, t.eps * scale)
             L.append("%-8s %9.2f %8.2f %6.2f %6.2f %9.2f %8.2f %8.4f"
@@ -519,6 +521,30 @@ def _fep_file(path: str, types: list[AtomType], iac: list[int], q: list[float], 
     L += ["%d %g %g" % (k + 1, 0.0, alpha) for k in range(len(qatoms))]
     with open(path, "w") as f:
         f.write("\n".join(L) + "\n")
+
+
+def solute_parameters(seed: int = 1234):
+    """(kinds, types, iac, charges) of the tree solute fep_solute(seed=seed)
+    builds: the same random draws in the same order."""
+    rng = np.random.default_rng(seed)
+    X, kinds, bonds = random_tree_solute(rng)
+    types, iac = _tree_types(kinds)
+    return kinds, types, iac, _solute_charges(rng, kinds)
+
+
+def perturbation(base: Generated, name: str, qatoms, charge_scale: float, eps_scale: float,
+                 seed: int = 1234, steps: int = 5000, run_seed: int = 1, lambdas=(1.0, 0.0)) -> Generated:
+    """Another perturbation of fep_solute's system (same topology `base`, its
+    files written beside it): the given solute atoms become two-state Q-atoms
+    whose state 2 carries charge_scale x their charge and eps_scale x their
+    epsilon (soft-core in state 2)."""
+    outdir = os.path.dirname(base.top)
+    kinds, types, iac, crg = solute_parameters(seed)
+    fp = os.path.join(outdir, name + ".fep")
+    _fep_file(fp, types, iac, crg, [int(a) for a in qatoms], charge_scale=charge_scale, eps_scale=eps_scale)
+    inp = os.path.join(outdir, name + ".inp")
+    write_inp(inp, base.top, fp, steps=steps, stepsize=2.0, seed=run_seed, lambdas=lambdas, shake_hydrogens=True)
+    return Generated(inp, base.top, fp, base.natom, base.nwat)
 
 
 def fep_solute(outdir: str, radius: float = 20.0, seed: int = 1234, steps: int = 5000, name: str = "c1",

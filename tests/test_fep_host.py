@@ -110,3 +110,38 @@ def test_mlp_oracle_gradient_is_exact():
     # the BF16 rounding used by the oracle: ties to even, exact on BF16 values
     v = np.array([1.0, 1.00390625, 1.005859375, -3.0e-3], dtype=np.float32)
     assert list(M.bf16(v)) == [1.0, 1.0, 1.0078125, float(np.float32(-0.0030059814453125))]
+
+
+def test_qligfep_schedule_matches_reference_golden():
+    """QligFEP's get_lambdas restated, against schedules produced by the
+    reference's own function (tests/golden/make_lambda_golden.py)."""
+    import json
+    import os
+    from q_b200 import lambda_placement as L
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "qligfep_lambdas.json")))
+    for sampling, table in g.items():
+        for w, lam in table.items():
+            ref = np.array([1.0 - float(x) for x in lam])
+            assert np.allclose(L.qligfep_schedule(int(w), sampling), ref, atol=1e-12), (sampling, w)
+
+
+def test_length_spacing_and_features():
+    from q_b200 import lambda_placement as L
+    # constant sigma: uniform; sigma 4x larger on the upper half: 4x denser there
+    assert np.allclose(L.length_spacing(L.DENSE_U, np.ones(21)), np.linspace(0, 1, 12))
+    sig = np.where(np.array(L.DENSE_U) < 0.5, 1.0, 4.0)
+    u = L.length_spacing(L.DENSE_U, sig)
+    gaps = np.diff(u)
+    assert u[0] == 0.0 and u[-1] == 1.0 and np.all(gaps > 0)
+    assert gaps[0] / gaps[-1] > 3.5
+    # logits round trip
+    assert np.allclose(L.positions_from_logits(L.spacing_logits(u)), u, atol=1e-9)
+    # the features carry the pilot's sigma profile exactly
+    rng = np.random.default_rng(0)
+    sd = (8.0, 6.0, 4.0, 3.0, 2.0)
+    dU = [rng.normal(m, s, 400) for m, s in zip((50, 30, 15, 5, 0), sd)]
+    f = L.pilot_features(dU)
+    assert f.shape == (12,) and np.all(np.isfinite(f)) and 0 <= f[11] < 1
+    assert np.allclose(L.KT * np.exp(f[0:5] + 3 * f[10]), [np.std(d) for d in dU])
+    pu = L.pilot_spacing(f)
+    assert np.all(np.diff(pu) > 0) and np.diff(pu)[0] < np.diff(pu)[-1]   # denser where sigma is large

@@ -239,3 +239,23 @@ def test_failed_system_stops_at_its_step(synthetic, kicked):
     assert np.max(np.abs(start - x10)) < 1e-9
     assert list(b.history(0, 1)[0]) == [10, 20]
     assert len(b.history(1, 1)[0]) == 0
+
+
+def test_perturbations_with_different_q_atoms_in_one_batch(tmp_path, oracle):
+    """Systems of one batch may carry different Q-atom sets (4 and 11 atoms,
+    other charge and epsilon scalings): each matches the oracle."""
+    from q_b200 import synth
+    base = synth.fep_solute(str(tmp_path / "c1"), seed=1234)
+    a = synth.perturbation(base, "pa", [0, 3, 9, 30], 0.3, 0.8)
+    b = synth.perturbation(base, "pb", [1, 2, 4, 5, 6, 7, 8, 10, 12, 14, 16], 0.9, 0.35)
+    sa = System.open(a.inp, lambdas=(0.7, 0.3), seed=2)
+    sb = System.open(b.inp, lambdas=(0.2, 0.8), seed=3)
+    batch = Batch([sa, sb, sa], precision=FP64)
+    batch.final_energy()
+    for k, s in ((0, sa), (1, sb), (2, sa)):
+        o = oracle.create(s)
+        o.final_energy()
+        Eg, EQg = batch.energy_vectors(k)
+        Eo, EQo = o.energy_vectors()
+        assert_energies(Eg, EQg, Eo, EQo)
+        assert grad_err(batch.gradient(k), o.gradient()) < G_TOL

@@ -26,6 +26,7 @@ extern "C" {
 
 typedef struct qb_mlp_adam {
   float lr, beta1, beta2, eps;
+  float weight_decay;   /* decoupled (AdamW): every step also subtracts lr*weight_decay*w from each weight */
 } qb_mlp_adam;
 
 /* y[n][11] = network(x[n][12]). */

@@ -81,18 +81,25 @@ def loss_grad(p, x, t, bf=False):
     return L, pack(g)
 
 
-def train(p, x, t, iters, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, bf=False):
-    """Full-batch Adam; returns the parameters and the loss before each step."""
+def weight_mask():
+    """1 for the entries of the weight matrices, 0 for the biases."""
+    return pack({name: np.ones(shape) if name.startswith("W") else np.zeros(shape) for name, shape in SHAPES})
+
+
+def train(p, x, t, iters, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, weight_decay=0.0, bf=False):
+    """Full-batch Adam with decoupled weight decay on the weight matrices;
+    returns the parameters and the loss before each step."""
     p = np.array(p, dtype=np.float64)
     m = np.zeros_like(p)
     v = np.zeros_like(p)
+    wd = weight_decay * weight_mask()
     losses = []
     for it in range(1, iters + 1):
         L, g = loss_grad(p, x, t, bf)
         losses.append(L)
         m = beta1 * m + (1 - beta1) * g
         v = beta2 * v + (1 - beta2) * g * g
-        p -= lr * (m / (1 - beta1 ** it)) / (np.sqrt(v / (1 - beta2 ** it)) + eps)
+        p -= lr * ((m / (1 - beta1 ** it)) / (np.sqrt(v / (1 - beta2 ** it)) + eps) + wd * p)
     return p, np.array(losses)
 
 

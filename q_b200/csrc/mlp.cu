@@ -163,7 +163,7 @@ struct Args {
   int n;
   int mode;            // 0 forward, 1 loss + gradient, 2 train
   int iters;
-  float lr, beta1, beta2, eps;
+  float lr, beta1, beta2, eps, wd;
   float *y;            // [n x OUT] outputs (forward)
   float *grad;         // [NPARAM] (mode 1)
   float *loss;         // [1] (mode 1) or [iters] (mode 2)
@@ -364,22 +364,23 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp(Args A) {
     // ---- Adam step on the FP32 master weights, then fresh BF16 copies
     const float t1 = (float)(it + 1);
     const float c1 = 1.0f / (1.0f - powf(A.beta1, t1)), c2 = 1.0f / (1.0f - powf(A.beta2, t1));
-    auto adam = [&](int p, float g) {
+    // decoupled weight decay on the weight matrices, not on the biases
+    auto adam = [&](int p, float g, float wd) {
       const float m = A.beta1 * A.adam_m[p] + (1.0f - A.beta1) * g;
       const float v = A.beta2 * A.adam_v[p] + (1.0f - A.beta2) * g * g;
       A.adam_m[p] = m;
       A.adam_v[p] = v;
-      P[p] -= A.lr * (m * c1) / (sqrtf(v * c2) + A.eps);
+      P[p] -= A.lr * ((m * c1) / (sqrtf(v * c2) + A.eps) + wd * P[p]);
     };
     if (j < HID) {
-      for (int i = 0; i < IN; i++) adam(OW1 + j * IN + i, g1[i]);
-      for (int i = 0; i < HID; i++) adam(OW2 + j * HID + i, g2[i]);
-      adam(OB1 + j, gb1[j]);
-      adam(OB2 + j, gb2[j]);
+      for (int i = 0; i < IN; i++) adam(OW1 + j * IN + i, g1[i], A.wd);
+      for (int i = 0; i < HID; i++) adam(OW2 + j * HID + i, g2[i], A.wd);
+      adam(OB1 + j, gb1[j], 0.f);
+      adam(OB2 + j, gb2[j], 0.f);
     }
     if (j < OUT) {
-      for (int i = 0; i < HID; i++) adam(OW3 + j * HID + i, g3[i]);
-      adam(OB3 + j, gb3[j]);
+      for (int i = 0; i < HID; i++) adam(OW3 + j * HID + i, g3[i], A.wd);
+      adam(OB3 + j, gb3[j], 0.f);
     }
     __threadfence_block();
     tc_before();
@@ -442,7 +443,7 @@ int call(int mode, float *params, const float *x, const float *t, int n, int ite
     a.params = (float *)dP.p; a.x = (const float *)dX.p; a.t = (const float *)dT.p; a.n = n; a.mode = mode;
     a.iters = iters; a.y = (float *)dY.p; a.grad = (float *)dG.p; a.loss = (float *)dL.p;
     a.adam_m = (float *)dM.p; a.adam_v = (float *)dV.p; a.status = (int *)dS.p;
-    if (adam) { a.lr = adam->lr; a.beta1 = adam->beta1; a.beta2 = adam->beta2; a.eps = adam->eps; }
+    if (adam) { a.lr = adam->lr; a.beta1 = adam->beta1; a.beta2 = adam->beta2; a.eps = adam->eps; a.wd = adam->weight_decay; }
     cuda(cudaFuncSetAttribute(k_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES), "smem attribute");
     k_mlp<<<1, THREADS, SMEM_BYTES>>>(a);
     cuda(cudaGetLastError(), "launch of mlp kernel");

@@ -13,9 +13,13 @@ The BAR variance of a narrow interval grows as ((u' - u) sigma(u))^2, sigma(u)
 the standard deviation of dU at u, so the summed variance is smallest when
 every interval carries the same increment of the thermodynamic length
 L(u) = integral of sigma.  The training target of a perturbation is that
-spacing, computed from a dense 21-window profile of sigma; the network's 11
-outputs are the centred logarithms of the 11 spacings (softmax gives the
-spacings back).  Uniform spacing is the fallback when no model is given.
+spacing, computed from a dense 21-window profile of sigma, written as the
+centred logarithms of its 11 spacings (softmax gives the spacings back).  The
+pilot already gives sigma at 5 points, whose interpolated length spacing is
+the placement without a network; the network's 11 outputs are a correction
+to that spacing's logarithms, and its output layer starts at zero, so an
+untrained or strongly regularised network returns the pilot spacing.
+Uniform spacing is the fallback when no model is given.
 """
 from __future__ import annotations
 
@@ -146,11 +150,14 @@ class Placement:
     fmean: np.ndarray
     fstd: np.ndarray
     loss: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    selection: dict = field(default_factory=dict)
 
     def predict_logits(self, features, device: int = 0) -> np.ndarray:
         from . import mlp
-        x = (np.atleast_2d(features) - self.fmean) / self.fstd
-        return mlp.forward(self.params, x.astype(np.float32), device).astype(np.float64)
+        F = np.atleast_2d(features)
+        x = (F - self.fmean) / self.fstd
+        base = np.array([spacing_logits(pilot_spacing(f)) for f in F])
+        return base + mlp.forward(self.params, x.astype(np.float32), device).astype(np.float64)
 
     def predict(self, features, device: int = 0) -> list[np.ndarray]:
         return [positions_from_logits(y) for y in self.predict_logits(features, device)]
@@ -164,14 +171,36 @@ class Placement:
         return cls(d["params"], d["fmean"], d["fstd"], d["loss"])
 
 
-def fit(features, targets, iters: int = 4000, lr: float = 2e-3, seed: int = 0, device: int = 0) -> Placement:
-    """Train the network (full-batch Adam on the tensor cores)."""
+def fit(features, targets, iters: int | None = None, lr: float = 2e-3, weight_decay: float = 0.0, seed: int = 0,
+        device: int = 0, val_frac: float = 0.2, grid_iters=(50, 100, 200, 400, 800, 1600, 3200),
+        grid_decay=(0.0, 0.01, 0.1)) -> Placement:
+    """Train the network (full-batch AdamW on the tensor cores).  With iters
+    None the number of steps and the weight decay are chosen on a held-back
+    validation fraction of the samples (smallest validation error over the
+    grid), then the network is trained on all samples with that choice."""
     from . import mlp
     X = np.asarray(features, dtype=np.float64)
+    base = np.array([spacing_logits(pilot_spacing(f)) for f in X])
+    T = (np.asarray(targets, dtype=np.float64) - base).astype(np.float32)     # correction to the pilot spacing
     fmean, fstd = X.mean(0), X.std(0) + 1e-6
-    p, hist = mlp.train(mlp.init(seed), ((X - fmean) / fstd).astype(np.float32),
-                        np.asarray(targets, dtype=np.float32), iters, lr=lr, device=device)
-    return Placement(p, fmean, fstd, hist)
+    Xn = ((X - fmean) / fstd).astype(np.float32)
+    selection = {}
+    if iters is None:
+        perm = np.random.default_rng(seed).permutation(len(X))
+        nv = max(1, int(round(val_frac * len(X))))
+        va, tr = perm[:nv], perm[nv:]
+        table = []
+        for wd in grid_decay:
+            for it in grid_iters:
+                p, _ = mlp.train(mlp.init(seed, True), Xn[tr], T[tr], it, lr=lr, weight_decay=wd, device=device)
+                err = float(np.mean((mlp.forward(p, Xn[va], device) - T[va]) ** 2))
+                table.append((err, it, wd))
+        err, iters, weight_decay = min(table)
+        selection = {"validation_mse": err, "iters": iters, "weight_decay": weight_decay,
+                     "validation_mse_pilot": float(np.mean(T[va] ** 2)),
+                     "grid": [{"iters": it, "weight_decay": wd, "validation_mse": e} for e, it, wd in table]}
+    p, hist = mlp.train(mlp.init(seed, True), Xn, T, iters, lr=lr, weight_decay=weight_decay, device=device)
+    return Placement(p, fmean, fstd, hist, selection)
 
 
 def pilot_spacing(features, n: int = N_PLACED) -> np.ndarray:
@@ -187,6 +216,28 @@ def place(features, model: Placement | None = None, device: int = 0) -> np.ndarr
     if model is None:
         return uniform(N_PLACED)
     return model.predict(features, device)[0]
+
+
+def structured_profiles(n: int, seed: int = 0, samples: int = 200):
+    """Pilot features and exact targets of n synthetic sigma(u) profiles with
+    structure the pilot under-resolves: a level in [0.5, 10] kcal/mol, a tilt,
+    and a Gaussian bump (height 0-6x, centre anywhere, width 0.05-0.3); the
+    pilot sees `samples` normal draws of dU at each of its 5 windows.  A
+    controlled benchmark of what the network adds to the pilot spacing."""
+    rng = np.random.default_rng(seed)
+    U = np.array(DENSE_U)
+    F, T = np.empty((n, N_FEATURES)), np.empty((n, N_PLACED - 1))
+    for i in range(n):
+        level, tilt = rng.uniform(0.5, 10.0), rng.uniform(-0.8, 0.8)
+        a, c, w = rng.uniform(0.0, 6.0), rng.uniform(0.0, 1.0), rng.uniform(0.05, 0.3)
+        slope = level * 5.0 * rng.uniform(-1.0, 1.0)
+
+        def sigma(u):
+            return level * (1.0 + tilt * (u - 0.5) + a * np.exp(-((u - c) / w) ** 2))
+
+        F[i] = pilot_features([rng.normal(slope * (1.0 - u), sigma(u), samples) for u in PILOT_U])
+        T[i] = spacing_logits(length_spacing(U, sigma(U)))
+    return F, T
 
 
 # ------------------------------------------------------------------ sampling
@@ -337,3 +388,85 @@ def evaluate(perts, features, model: Placement, *, replicas: int = 4, ref_replic
             "rms_sem": float(np.sqrt(np.mean(sem ** 2))), "gpu_s": float(sum(r.gpu_seconds for r in rs)),
         }
     return out
+
+
+# ------------------------------------------------------------------ study
+
+def study(root: str, *, n_train: int = 200, n_test: int = 50, seed: int = 0, iters: int | None = None,
+          replicas: int = 4, ref_replicas: int = 4, steps_eq: int = 1000, steps_prod: int = 5000,
+          device: int = 0, data_file: str | None = None, run_dG: bool = True) -> dict:
+    """Generate n_train + n_test perturbations, their pilot features and
+    dense-profile targets, train the network on the first n_train, and
+    evaluate every schedule on the held-out n_test against the dense FP64
+    reference."""
+    t0 = time.perf_counter()
+    _, perts = make_perturbations(root, n_train + n_test, seed=seed)
+    data_path = os.path.join(root, "placement_data.npz")
+    if data_file and os.path.exists(data_file):
+        d = np.load(data_file)
+        data = {k: d[k] for k in d.files}
+        data["wall_s"] = float(data["wall_s"])
+    else:
+        data = training_data(perts, device=device)
+    np.savez(data_path, **data)
+    F, T = data["features"], data["targets"]
+    model = fit(F[:n_train], T[:n_train], iters=iters, device=device)
+    model.save(os.path.join(root, "placement_model.npz"))
+    Ft, Tt = F[n_train:], T[n_train:]
+    pred = model.predict_logits(Ft, device)
+    Fs, Ts = structured_profiles(2400, seed=seed + 1)
+    ms = fit(Fs[:2000], Ts[:2000], device=device)
+    ps = ms.predict_logits(Fs[2000:], device)
+    structured = {"learned": float(np.mean((ps - Ts[2000:]) ** 2)),
+                  "pilot_length": float(np.mean((np.array([spacing_logits(pilot_spacing(f)) for f in Fs[2000:]])
+                                                 - Ts[2000:]) ** 2)),
+                  "uniform": float(np.mean(Ts[2000:] ** 2)),
+                  "selection": {k: v for k, v in ms.selection.items() if k != "grid"}}
+    target_mse = {
+        "structured_profiles_held_out": structured,
+        "learned": float(np.mean((pred - Tt) ** 2)),
+        "pilot_length": float(np.mean((np.array([spacing_logits(pilot_spacing(f)) for f in Ft]) - Tt) ** 2)),
+        "uniform": float(np.mean(Tt ** 2)),
+        "train_final_loss": float(model.loss[-1]),
+    }
+    target_mse["selection"] = {k: v for k, v in model.selection.items() if k != "grid"}
+    ev = evaluate(perts[n_train:], Ft, model, replicas=replicas, ref_replicas=ref_replicas, steps_eq=steps_eq,
+                  steps_prod=steps_prod, device=device) if run_dG else {"methods": {}, "reference": {}}
+    ev["target_mse_held_out"] = target_mse
+    ev["selection_grid"] = model.selection.get("grid", [])
+    ev["data"] = {"n_train": n_train, "n_test": n_test, "pilot_gpu_s_mean": float(data["pilot_gpu_s"].mean()),
+                  "dense_gpu_s_mean": float(data["dense_gpu_s"].mean()), "generation_wall_s": data["wall_s"]}
+    ev["protocol"] = {"steps_eq": steps_eq, "steps_prod": steps_prod, "replicas": replicas,
+                      "ref_replicas": ref_replicas, "iters": iters}
+    ev["wall_s"] = time.perf_counter() - t0
+    return ev
+
+
+def main(argv=None) -> int:
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="train and evaluate the lambda-placement network")
+    ap.add_argument("root")
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--train", type=int, default=200)
+    ap.add_argument("--test", type=int, default=50)
+    ap.add_argument("--replicas", type=int, default=4)
+    ap.add_argument("--ref-replicas", type=int, default=4)
+    ap.add_argument("--steps", type=int, default=5000)
+    ap.add_argument("--iters", type=int, default=None, help="Adam steps (default: chosen on a validation split)")
+    ap.add_argument("--data", default=None, help="reuse features/targets saved by an earlier study (npz)")
+    ap.add_argument("--no-dG", action="store_true", help="stop after training (no free-energy evaluation)")
+    a = ap.parse_args(argv)
+    r = study(a.root, n_train=a.train, n_test=a.test, replicas=a.replicas, ref_replicas=a.ref_replicas,
+              steps_prod=a.steps, iters=a.iters, data_file=a.data, run_dG=not a.no_dG)
+    summary = {k: r[k] for k in ("target_mse_held_out", "data", "protocol", "wall_s")}
+    summary["reference"] = {k: r["reference"][k] for k in ("windows", "replicas", "gpu_s") if k in r["reference"]}
+    summary["methods"] = {m: {k: v for k, v in d.items() if k not in ("dG", "sem")} for m, d in r["methods"].items()}
+    print(json.dumps(summary, indent=1))
+    if a.out:
+        json.dump(r, open(a.out, "w"), indent=1)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

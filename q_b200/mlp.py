@@ -19,7 +19,8 @@ MAX_SAMPLES = 4096
 
 
 class Adam(C.Structure):
-    _fields_ = [("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float)]
+    _fields_ = [("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float),
+                ("weight_decay", C.c_float)]
 
 
 def _f32(a, shape=None):
@@ -33,11 +34,14 @@ def _p(a):
     return a.ctypes.data_as(C.POINTER(C.c_float))
 
 
-def init(seed: int = 0) -> np.ndarray:
+def init(seed: int = 0, zero_output: bool = False) -> np.ndarray:
+    """He-style initial weights, biases zero; with zero_output the output
+    layer starts at zero, so the untrained network outputs 0."""
     rng = np.random.default_rng(seed)
+    w3 = rng.normal(0, np.sqrt(1.0 / HID), (OUT, HID))
     parts = [rng.normal(0, np.sqrt(2.0 / IN), (HID, IN)), np.zeros(HID),
              rng.normal(0, np.sqrt(2.0 / HID), (HID, HID)), np.zeros(HID),
-             rng.normal(0, np.sqrt(1.0 / HID), (OUT, HID)), np.zeros(OUT)]
+             np.zeros_like(w3) if zero_output else w3, np.zeros(OUT)]
     return np.concatenate([q.reshape(-1) for q in parts]).astype(np.float32)
 
 
@@ -60,12 +64,13 @@ def loss_grad(params, x, t, device: int = 0) -> tuple[float, np.ndarray]:
 
 
 def train(params, x, t, iters: int, lr: float = 1e-3, beta1: float = 0.9, beta2: float = 0.999,
-          eps: float = 1e-8, device: int = 0) -> tuple[np.ndarray, np.ndarray]:
-    """Full-batch Adam on the mean squared error; returns the trained
-    parameters and the loss before every step."""
+          eps: float = 1e-8, weight_decay: float = 0.0, device: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """Full-batch Adam (decoupled weight decay on the weight matrices) on the
+    mean squared error; returns the trained parameters and the loss before
+    every step."""
     p = _f32(params, (NPARAM,)).copy()
     x, t = _f32(x), _f32(t)
     hist = np.zeros(iters, dtype=np.float32)
-    a = Adam(lr, beta1, beta2, eps)
+    a = Adam(lr, beta1, beta2, eps, weight_decay)
     check(lib.qb_mlp_train(_p(p), _p(x), _p(t), x.shape[0], iters, C.addressof(a), _p(hist), device))
     return p, hist

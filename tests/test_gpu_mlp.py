@@ -68,6 +68,19 @@ def test_training_follows_the_oracle():
     assert abs(Lend - M.loss_grad(pb, x, t, bf=True)[0]) <= 0.05 * Lend
 
 
+def test_weight_decay_follows_the_oracle():
+    from q_b200 import mlp
+    x, t = _data(300, 23)
+    p0 = mlp.init(4)
+    p, hist = mlp.train(p0, x, t, 200, lr=2e-3, weight_decay=0.05)
+    pb, hb = M.train(p0, x, t, 200, lr=2e-3, weight_decay=0.05, bf=True)
+    assert np.all(np.abs(hist - hb) <= 0.05 * hb)
+    w = M.weight_mask() > 0
+    # decay shrinks the weights against the run without it
+    pn, _ = mlp.train(p0, x, t, 200, lr=2e-3)
+    assert np.linalg.norm(p[w]) < np.linalg.norm(pn[w])
+
+
 def test_invalid_arguments():
     from q_b200 import QBError, mlp
     p = mlp.init(0)

@@ -149,6 +149,13 @@ __device__ __forceinline__ float ld_bf16(const uint8_t *sm, int tile, int r, int
   return __bfloat162float(*reinterpret_cast<const __nv_bfloat16 *>(sm + tile + kmaj(r, k, K)));
 }
 
+// add v, summed over the warp's 32 rows, to *acc (one shared atomic per warp)
+__device__ __forceinline__ void warp_col_add(float *acc, float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(acc, v);
+}
+
 __device__ __forceinline__ float sigmoidf_(float z) { return 1.0f / (1.0f + expf(-z)); }
 __device__ __forceinline__ float silu(float z) { return z * sigmoidf_(z); }
 __device__ __forceinline__ float dsilu(float z) {
@@ -291,7 +298,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp(Args A) {
         }
         st_bf16(sm, S_D3, tid, k, NOUT, d);
         st_bf16(sm, S_AT, k, tid, ROWS, d);             // dz3^T: row = output k, K = sample
-        if (d != 0.f) atomicAdd(&gb3[k], d);
+        warp_col_add(&gb3[k], d);
       }
       for (int h = 0; h < HID; h++) st_bf16(sm, S_BT, h, tid, ROWS, ld_bf16(sm, S_H2, tid, h, HID));
       // dh2 = dz3 W3 ; dW3 += dz3^T h2
@@ -308,7 +315,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp(Args A) {
           const float d = valid ? g[k] * dsilu(z[k] + P[OB2 + c + k]) : 0.f;
           st_bf16(sm, S_D2, tid, c + k, HID, d);
           st_bf16(sm, S_AT, c + k, tid, ROWS, d);       // dz2^T
-          if (d != 0.f) atomicAdd(&gb2[c + k], d);
+          warp_col_add(&gb2[c + k], d);
         }
       }
       for (int h = 0; h < HID; h++) st_bf16(sm, S_BT, h, tid, ROWS, ld_bf16(sm, S_H1, tid, h, HID));
@@ -325,7 +332,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp(Args A) {
         for (int k = 0; k < 16; k++) {
           const float d = valid ? g[k] * dsilu(z[k] + P[OB1 + c + k]) : 0.f;
           st_bf16(sm, S_AT, c + k, tid, ROWS, d);       // dz1^T
-          if (d != 0.f) atomicAdd(&gb1[c + k], d);
+          warp_col_add(&gb1[c + k], d);
         }
       }
       for (int i = 0; i < KIN; i++) st_bf16(sm, S_BT, i, tid, ROWS, ld_bf16(sm, S_X, tid, i, KIN));

@@ -56,14 +56,24 @@ def open_systems(inp: str, lambdas, seeds, threads: int | None = None) -> list:
 
 def run_perturbation(inp: str, lambdas, replicas: int = 1, *, steps_eq: int = 1000, steps_prod: int = 5000,
                      precision: int = MIXED, device: int = 0, rt: float = 0.592, seed0: int = 1,
-                     nskip: int = 0) -> PerturbationResult:
+                     nskip: int = 0, starts=None) -> PerturbationResult:
     """Every (replica, window) of the perturbation in one batch: steps_eq
     equilibration steps whose records are dropped, then steps_prod production
     steps whose energy records (the input's energy interval) feed BAR.
-    Replica r uses Maxwell seed seed0 + r for all its windows."""
+    Replica r uses Maxwell seed seed0 + r for all its windows, or, with
+    starts (one .inp per replica, e.g. Equilibrated.inputs), starts every
+    window from that replica's equilibrated restart: the windows run in
+    parallel where QligFEP chains them one after another
+    (INPUTS/run.sh:109-123)."""
     lambdas = [tuple(l) for l in lambdas]
     nw = len(lambdas)
-    systems = open_systems(inp, lambdas, range(seed0, seed0 + replicas))
+    if starts is not None:
+        replicas = len(starts)
+        jobs = [(p, l) for p in starts for l in lambdas]
+        with ThreadPoolExecutor(min(len(jobs), os.cpu_count() or 1)) as ex:
+            systems = list(ex.map(lambda j: System.open(j[0], lambdas=j[1]), jobs))
+    else:
+        systems = open_systems(inp, lambdas, range(seed0, seed0 + replicas))
     batch = Batch(systems, precision=precision, device=device)
     try:
         gpu_ms = 0.0
@@ -105,6 +115,106 @@ def time_single_window(inp: str, lam, steps: int, *, precision: int = FP64, devi
         b.close()
         s.close()
     return ms / 1e3 / steps
+
+
+@dataclass
+class Stage:
+    """One equilibration stage: steps of stepsize fs at temperature K with the
+    bath coupling (fs); restraint > 0 holds the solute atoms in a sequence
+    restraint of that force constant (kcal/mol/A^2)."""
+    steps: int
+    stepsize: float
+    temperature: float
+    bath: float
+    shake_hydrogens: bool
+    restraint: float
+
+
+# QligFEP's 2 fs heating schedule (INPUTS/eq1-5.inp with qligfep.py:107-123,
+# 607-640): 0.1 fs at 1 K, then 50, 150, 275 K with the ligand restraint
+# 10, 10, 5, 2.5, then the run temperature without it.
+QLIGFEP_EQ_2FS = [
+    Stage(10000, 0.1, 1.0, 0.2, False, 10.0),
+    Stage(5000, 2.0, 50.0, 2.0, True, 10.0),
+    Stage(5000, 2.0, 150.0, 2.0, True, 5.0),
+    Stage(5000, 2.0, 275.0, 2.0, True, 2.5),
+    Stage(50000, 2.0, 298.0, 10.0, True, 0.0),
+]
+
+
+@dataclass
+class Equilibrated:
+    restarts: list            # per replica: the .re after the last stage
+    inputs: list              # per replica: an .inp that starts from it
+    temperatures: list        # per stage: mean temperature of the replicas after the stage
+    gpu_seconds: float
+
+
+def equilibrate(inp: str, seeds, stages=QLIGFEP_EQ_2FS, *, lambdas=None, steps_scale: float = 1.0,
+                restrain: tuple | None = None, precision: int = FP64, device: int = 0,
+                tag: str = "eq") -> Equilibrated:
+    """The heating protocol for every replica at once: stage k of all
+    replicas is one batch, each system restarting from its own .re of stage
+    k-1 (coordinates, velocities, water polarisation corrections), as qdyn
+    chains eq1.re -> eq2 -> ... -> eq5.re.  Stage inputs are derived from
+    `inp` (only the stage's keys change); the first stage draws Maxwell
+    velocities at its temperature with each replica's seed.  `restrain`
+    = (first, last) 1-based solute atoms held by the stages' restraint (default
+    all solute atoms).  Returns, per replica, the last .re and an .inp that
+    starts from it (for run_perturbation's windows)."""
+    from .api import write_restart
+    from .inputs import derive_inp
+    seeds = [int(s) for s in seeds]
+    probe = System.open(inp)
+    nsol = probe.view.nat_solute
+    probe.close()
+    first, last = restrain or (1, nsol)
+    lam = " ".join("%g" % x for x in lambdas) if lambdas is not None else None
+    restarts = [None] * len(seeds)
+    temps, gpu_ms = [], 0.0
+    for k, st in enumerate(stages):
+        steps = max(1, int(round(st.steps * steps_scale)))
+        specs = []
+        for r, seed in enumerate(seeds):
+            md = {"steps": steps, "stepsize": st.stepsize, "temperature": st.temperature, "bath_coupling": st.bath,
+                  "shake_hydrogens": "on" if st.shake_hydrogens else "off", "separate_scaling": "on"}
+            drop = {"md": [], "files": ["trajectory", "energy"]}
+            files = {"final": "%s%d_r%d.re" % (tag, k + 1, r)}
+            if restarts[r] is None:
+                md.update({"random_seed": seed, "initial_temperature": st.temperature})
+                drop["files"].append("restart")
+            else:
+                drop["md"] += ["random_seed", "initial_temperature"]
+                files["restart"] = os.path.basename(restarts[r])
+            rows = {"sequence_restraints": ["%d %d %g 0 0" % (first, last, st.restraint)] if st.restraint > 0 else None,
+                    "intervals": ["non_bond 25", "output %d" % max(steps, 1), "energy 0", "trajectory 0"]}
+            if lam is not None:
+                rows["lambdas"] = [lam]
+            specs.append(derive_inp(inp, "%s%d_r%d.inp" % (tag, k + 1, r), set_keys={"md": md, "files": files},
+                                    drop_keys=drop, set_rows=rows))
+        systems = [System.open(p) for p in specs]
+        batch = Batch(systems, precision=precision, device=device)
+        try:
+            ms, _ = batch.run_timed(steps)
+            gpu_ms += ms
+            d = os.path.dirname(os.path.abspath(inp))
+            ts = []
+            for r in range(len(seeds)):
+                tc = batch.theta_corr(r, systems[r].view.nwpolr_shell) if systems[r].view.nwpolr_shell > 0 else None
+                restarts[r] = os.path.join(d, "%s%d_r%d.re" % (tag, k + 1, r))
+                write_restart(restarts[r], batch.coords(r), batch.velocities(r), tc)
+                ts.append(float(batch.temperature(r)[0]))
+            temps.append(float(np.mean(ts)))
+        finally:
+            batch.close()
+            for s in systems:
+                s.close()
+    outs = []
+    for r in range(len(seeds)):
+        outs.append(derive_inp(inp, "%s_start_r%d.inp" % (tag, r),
+                               set_keys={"files": {"restart": os.path.basename(restarts[r])}},
+                               drop_keys={"md": ["random_seed", "initial_temperature"]}))
+    return Equilibrated(restarts, outs, temps, gpu_ms / 1e3)
 
 
 def dg_versus_plain(inp: str, *, windows: int = 21, replicas: int = 16, ref_windows: int = 41,

@@ -5,8 +5,10 @@
 Reads the same .inp/.top/.fep/.re as qdyn (src/q6/qdyn.f90:18-134), runs the
 MD steps on the GPU, and writes what the reference's scripts consume: the
 energy file (.en, put_ene records, nrgy.f90:94-119), the final restart (.re,
-write_xfin, md.f90:15452-15470) and an energy-summary log laid out as
-write_out (md.f90:15292-15440), ending with "terminated normally".
+write_xfin, md.f90:15452-15470), the coordinate trajectory (.dcd of the
+[trajectory_atoms] mask every `trajectory` steps, trj.f90:184-259, written at
+md.f90:4151 and 4202; q_b200/trajectory.py) and an energy-summary log laid out
+as write_out (md.f90:15292-15440), ending with "terminated normally".
 """
 from __future__ import annotations
 
@@ -104,13 +106,35 @@ def run(inp: str, out=sys.stdout, chunk: int = 1000) -> int:
             final = os.path.join(d, t[1])
     if ene and os.path.exists(ene):
         os.remove(ene)
+    trj, frames = None, []
+    if v.itrj_cycle > 0:
+        from q_b200.trajectory import DcdWriter, atom_mask, frame_steps, inp_sections
+        sec = inp_sections(inp)
+        files = dict((l.split()[0].lower(), l.split()[1]) for l in sec.get("files", []) if len(l.split()) >= 2)
+        rows = sec.get("trajectory_atoms", [])
+        try:
+            mask = atom_mask(v, rows)
+        except ValueError as e:
+            print("!" * 79, file=out)
+            print("ABNORMAL TERMINATION of qdyn: %s" % e, file=out)
+            return 255
+        print("Coordinates for%6d atoms will be written to the trajectory." % int(mask.sum()), file=out)
+        trj = DcdWriter(os.path.join(d, files["trajectory"]), mask, frames=v.nsteps // v.itrj_cycle,
+                        interval=v.itrj_cycle, steps=v.nsteps, degf=v.Ndegfree, topology=files.get("topology", ""),
+                        mask_rows=rows)
+        frames = frame_steps(v.nsteps, v.itrj_cycle)
     T = batch.temperature(0)
     print("Initial temperatures are : Ttot =%10.2f Tfree =%10.2f" % (T[0], T[1]), file=out)
     done = 0
     try:
         while done < v.nsteps:
             n = min(chunk, v.nsteps - done)
+            nxt = [f for f in frames if f > done]
+            if nxt:
+                n = min(n, nxt[0] - done)
             batch.run(n)
+            if trj and done + n in frames:
+                trj.write(batch.coords(0))
             steps, E, EQ = batch.history(0, 0)
             for k in range(len(steps)):
                 print(write_out(E[k], EQ[k], int(steps[k]), ns, v.nwat, bool(v.use_LRF), v.nqat, v.nat_solute), file=out)
@@ -131,6 +155,8 @@ def run(inp: str, out=sys.stdout, chunk: int = 1000) -> int:
     print(write_out(E, EQ, None, ns, v.nwat, bool(v.use_LRF), v.nqat, v.nat_solute), file=out)
     tc = batch.theta_corr(0, v.nwpolr_shell) if v.nwpolr_shell > 0 else None
     write_restart(final, batch.coords(0), batch.velocities(0), tc)
+    if trj:
+        trj.close()
     print("Total time of main loop: %24.1f(s)" % (time.time() - t0), file=out)
     print(" qdyn version 6.0.1 terminated normally.", file=out)
     return 0

@@ -460,24 +460,45 @@ class Generated:
 def write_inp(path: str, top: str, fep: str | None, *, steps: int, stepsize: float, temp: float = 298.0,
               seed: int = 1, lambdas=None, shake_hydrogens: bool = False, bath: float = 100.0,
               output: int = 100, energy: int = 10, non_bond: int = 25, shell_radius: float | None = None,
-              shell_force: float = 10.0, q_cutoff: float = 99.0, energy_file: str | None = None) -> None:
+              shell_force: float = 10.0, q_cutoff: float = 99.0, energy_file: str | None = None,
+              trajectory: int = 0, trajectory_atoms=None, restart: str | None = None,
+              sequence_restraints=None, separate_scaling: bool = False,
+              initial_temperature: float | None = None) -> None:
+    """A qdyn .inp (md.f90:2528-3262 sections).  With restart, coordinates
+    and velocities come from that .re and no seed or initial temperature is
+    written; trajectory > 0 adds the .dcd file and its [trajectory_atoms]
+    rows; sequence_restraints are rows "first last force_k to_centre heavy"."""
     name = os.path.splitext(os.path.basename(path))[0]
-    L = ["[MD]", "steps %d" % steps, "stepsize %g" % stepsize, "temperature %g" % temp,
-         "bath_coupling %g" % bath, "random_seed %d" % seed, "initial_temperature %g" % temp,
-         "shake_solvent on", "shake_solute off", "shake_hydrogens %s" % ("on" if shake_hydrogens else "off"),
-         "lrf on", "", "[cut-offs]", "solute_solute 10", "solvent_solvent 10", "solute_solvent 10",
+    L = ["[MD]", "steps %d" % steps, "stepsize %g" % stepsize, "temperature %g" % temp, "bath_coupling %g" % bath]
+    if restart is None:
+        t0 = temp if initial_temperature is None else initial_temperature
+        L += ["random_seed %d" % seed, "initial_temperature %g" % t0]
+    L += ["shake_solvent on", "shake_solute off", "shake_hydrogens %s" % ("on" if shake_hydrogens else "off"),
+          "lrf on"]
+    if separate_scaling:
+        L.append("separate_scaling on")
+    L += ["", "[cut-offs]", "solute_solute 10", "solvent_solvent 10", "solute_solvent 10",
          "q_atom %g" % q_cutoff, "lrf 99", "", "[sphere]"]
     if shell_radius is not None:
         L.append("shell_radius %g" % shell_radius)
     L += ["shell_force %g" % shell_force, "", "[solvent]", "radial_force 60.0", "polarization on",
           "polarization_force 20.0", "", "[intervals]", "non_bond %d" % non_bond, "output %d" % output,
-          "energy %d" % energy, "trajectory 0", "", "[files]", "topology %s" % os.path.basename(top),
-          "final %s.re" % name]
+          "energy %d" % energy, "trajectory %d" % trajectory, "", "[files]",
+          "topology %s" % os.path.basename(top), "final %s.re" % name]
+    if restart:
+        L.append("restart %s" % os.path.basename(restart))
     if energy > 0:
         L.append("energy %s" % (energy_file or name + ".en"))
+    if trajectory > 0:
+        L.append("trajectory %s.dcd" % name)
     if fep:
         L.append("fep %s" % os.path.basename(fep))
+    if trajectory > 0 and trajectory_atoms:
+        L += ["", "[trajectory_atoms]"] + list(trajectory_atoms)
+    if fep:
         L += ["", "[lambdas]", " ".join("%g" % x for x in lambdas)]
+    if sequence_restraints:
+        L += ["", "[sequence_restraints]"] + list(sequence_restraints)
     with open(path, "w") as f:
         f.write("\n".join(L) + "\n")
 

@@ -205,3 +205,69 @@ def test_multi_rank_helpers_gloo():
         p.join(timeout=60)
     assert res[0] == (0, [0, 2, 4], 2.0, 100.0)
     assert res[1] == (1, [1, 3, 5], 2.0, 100.0)
+
+
+def test_derived_inputs_and_restart(tmp_path):
+    """An .inp derived with new keys, dropped keys and replaced rows opens
+    like any input; a derived input that restarts from a written .re starts
+    from its coordinates and velocities."""
+    from q_b200.inputs import derive_inp, inp_sections
+    g = synth.fep_solute(str(tmp_path / "c1"), seed=1234, steps=100)
+    p = derive_inp(g.inp, "d1.inp", set_keys={"md": {"temperature": 150, "separate_scaling": "on"},
+                                              "intervals": {"energy": 0}},
+                   drop_keys={"files": ["energy"]},
+                   set_rows={"sequence_restraints": ["1 56 5 0 0"], "lambdas": ["0.3 0.7"]})
+    sec = inp_sections(p)
+    md = dict(l.split(None, 1) for l in sec["md"])
+    assert md["temperature"] == "150" and md["separate_scaling"] == "on" and md["steps"] == "100"
+    assert not any(l.startswith("energy") for l in sec["files"])
+    assert sec["sequence_restraints"] == ["1 56 5 0 0"] and sec["lambdas"] == ["0.3 0.7"]
+    s = System.open(p)
+    assert s.view.nrstr_seq == 1 and abs(s.view.Temp0 - 150.0) < 1e-12
+    lam = getattr(s.view, "lambda")
+    assert (lam[0], lam[1]) == (0.3, 0.7)
+    x = s.array("x0", 3 * s.natom) + 0.01
+    v = s.array("v0", 3 * s.natom) * 0.5
+    write_restart(str(tmp_path / "c1" / "start.re"), x, v)
+    q = derive_inp(g.inp, "d2.inp", set_keys={"files": {"restart": "start.re"}},
+                   drop_keys={"md": ["random_seed", "initial_temperature"]})
+    r = System.open(q)
+    assert np.array_equal(r.array("x0", 3 * r.natom), x)
+
+
+def test_dcd_layout_and_mask(tmp_path, golden):
+    """The trajectory file has trj.f90's records; the mask follows mask.f90."""
+    from q_b200.trajectory import DcdWriter, atom_mask, frame_steps, read_dcd
+    s1 = System.open(str(golden / "test1" / "eq1.inp"))    # the view's arrays live as long as s1
+    v = s1.view
+    n, ns = v.natom, v.nat_solute
+    excl = np.array(v.excl[:n], bool)
+    heavy = np.array(v.heavy[:n], bool)
+    assert atom_mask(v, []).sum() == n
+    assert atom_mask(v, ["not excluded"]).sum() == n - excl.sum()
+    assert np.array_equal(atom_mask(v, ["solute heavy"]), (np.arange(n) < ns) & heavy)
+    assert np.array_equal(atom_mask(v, ["1 10", "not solute"]), (np.arange(n) < 10) | (np.arange(n) >= ns))
+    assert atom_mask(v, ["5"]).sum() == 1 and atom_mask(v, ["5"])[4]
+    with pytest.raises(ValueError):
+        atom_mask(v, ["residue 1 2"])
+    assert frame_steps(100, 10) == [11, 21, 31, 41, 51, 61, 71, 81, 91, 100]
+    assert frame_steps(95, 10) == [11, 21, 31, 41, 51, 61, 71, 81, 91]
+    m = atom_mask(v, ["not excluded"])
+    path = str(tmp_path / "t.dcd")
+    w = DcdWriter(path, m, frames=2, interval=10, steps=20, degf=v.Ndegfree, topology="lig_w.top",
+                  mask_rows=["not excluded"])
+    rng = np.random.default_rng(0)
+    xs = [rng.normal(size=3 * n) for _ in range(2)]
+    for x in xs:
+        w.write(x)
+    w.close()
+    raw = open(path, "rb").read()
+    assert raw[:8] == struct.pack("<i", 84) + b"CORD"
+    assert struct.unpack_from("<i", raw, 88)[0] == 84                  # end marker of the header record
+    assert struct.unpack_from("<i", raw, 92)[0] == 4 + 3 * 80          # title record: count + 3 rows
+    h, fr = read_dcd(path)
+    assert (h["frames"], h["steps_before"], h["interval"], h["steps"], h["degf"]) == (2, 10, 10, 20, v.Ndegfree)
+    assert h["title"] == "Q DCD trajectory version 6.0.1" and h["topology"] == "lig_w.top"
+    assert h["mask_rows"] == ["not excluded"] and h["atoms"] == m.sum()
+    assert fr.shape == (2, m.sum(), 3)
+    assert np.array_equal(fr[1], xs[1].reshape(-1, 3)[m].astype(np.float32))

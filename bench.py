@@ -63,6 +63,7 @@ def parse():
     p.add_argument("--spheres", type=int, default=16)
     p.add_argument("--equil", type=int, default=100, help="untimed equilibration steps (in addition to warm-up)")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-autotune", action="store_true", help="keep the default tile sizes and streams")
     p.add_argument("--dg-replicas", type=int, default=16,
                    help="replicas of the batched mixed-precision perturbation for the GPU-s per dG comparison "
                         "(0 skips it; runs at one GPU only)")
@@ -262,8 +263,10 @@ def main():
     dts = np.array([dt for _, _, _, dt in specs])
     natoms = sum(s.natom for s in systems)
     batch = Batch(systems, precision=prec, device=local)
-    # untimed equilibration from the lattice start, then warm-up
+    # untimed equilibration from the lattice start, the autotuner (its trial
+    # steps are equilibration too), then warm-up
     batch.run(args.equil)
+    tuning = batch.autotune(50) if not args.no_autotune else batch.tuning()
     batch.run(max(args.warmup, 3))
     batch.clear_history()
 
@@ -359,7 +362,8 @@ def main():
                    "precision": args.precision, "equilibration_steps": args.equil,
                    "l2": "per-step working set (coordinates, velocities, gradients, pair lists) exceeds the 126 MB L2",
                    "parallelism": "replicas only (%d GPU, whole systems per GPU)" % world,
-                   "setup_s": round(setup_s, 2)},
+                   "setup_s": round(setup_s, 2),
+                   "tuning": {k: (round(v, 5) if isinstance(v, float) else v) for k, v in tuning.items()}},
         "roofline": {"kernel": "nb_ww (water-water SPC pair kernel)", "bound": "fp64" if prec == FP64 else "fp32",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                      "peak_source": "measured FMA loop (qb_peak_flops) on this GPU",

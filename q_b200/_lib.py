@@ -128,6 +128,9 @@ def _load():
         "qb_batch_history": (C.c_int, [vp, C.c_int, C.c_int, ip, ip, dp, dp]),
         "qb_batch_clear_history": (C.c_int, [vp]),
         "qb_batch_status": (C.c_int, [vp, C.c_int, ip]),
+        "qb_batch_get_tuning": (C.c_int, [vp, C.c_void_p]),
+        "qb_batch_set_tuning": (C.c_int, [vp, C.c_void_p]),
+        "qb_batch_autotune": (C.c_int, [vp, C.c_int, C.c_void_p]),
         "qb_batch_set_profiling": (C.c_int, [vp, C.c_int]),
         "qb_batch_profile": (C.c_int, [vp, C.c_char_p, C.c_size_t, dp, C.POINTER(C.c_longlong),
                                        C.c_int, ip]),

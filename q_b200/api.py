@@ -21,6 +21,8 @@ from ._lib import E_NAMES, EQ_NAMES, QB_NE, QB_NEQ, Options, SysView, check, lib
 FP64 = 0
 MIXED = 1
 
+Tuning = _lib._struct_from_header(_lib.os.path.join(_lib.INCLUDE, "qb.h"), "qb_tuning")
+
 
 def _dp(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_double))
@@ -186,6 +188,26 @@ class Batch:
         out = np.zeros(10)
         check(lib.qb_batch_workload(self._b, _dp(out), 10))
         return out
+
+    def tuning(self) -> dict:
+        """The step kernels' run-time choices (qb_tuning)."""
+        t = Tuning()
+        check(lib.qb_batch_get_tuning(self._b, C.addressof(t)))
+        return {name: getattr(t, name) for name, _ in t._fields_}
+
+    def set_tuning(self, **kw) -> None:
+        t = Tuning()
+        check(lib.qb_batch_get_tuning(self._b, C.addressof(t)))
+        for k, v in kw.items():
+            setattr(t, k, v)
+        check(lib.qb_batch_set_tuning(self._b, C.addressof(t)))
+
+    def autotune(self, steps_per_trial: int = 100) -> dict:
+        """Time candidate settings on real MD steps and keep the fastest
+        (the steps advance every system; their energy records are cleared)."""
+        t = Tuning()
+        check(lib.qb_batch_autotune(self._b, steps_per_trial, C.addressof(t)))
+        return {name: getattr(t, name) for name, _ in t._fields_}
 
     def status(self, sys: int) -> int:
         st = C.c_int()

@@ -63,6 +63,12 @@ struct Batch {
   int max_natom = 0, max_lrf_blocks = 1, max_nsol = 0, max_nwat = 0, max_ncgp = 0, max_ncgp_sol = 0, max_terms = 0, max_pp = 0, max_ncgp_sol_w = 0, max_qp = 0;
   bool any_lrf = false, any_q = false, any_shake = false, any_wpol = false, any_prestr = false, any_qq = false,
        any_qb = false;
+  // run-time choices the autotuner sets (qb_tuning): LRF source tiles per
+  // block, water-water staging chunk (>= ww_chunk_floor, for which ww_sp is
+  // sized), side streams on or off
+  int ww_chunk_floor = 32, ww_chunk_max = 32;
+  bool streams_on = true;
+  std::vector<int2> lrf_dims;   // per system with LRF: (charge groups, source tiles)
   size_t watpol_smem = 0;
   int q_states = 0;           // state count shared by every system with Q atoms (0: they differ)
   int max_nq = 0;
@@ -186,7 +192,13 @@ struct Batch {
 
   // Fork the side streams off the main stream / join them back (no-ops when
   // profiling or without side streams).
-  bool forking() const { return !profiling && side[0]; }
+  bool forking() const { return !profiling && side[0] && streams_on; }
+
+  void set_lrf_tpb(int tpb) {
+    P.lrf_tpb = tpb;
+    max_lrf_blocks = 1;
+    for (const int2 &d : lrf_dims) max_lrf_blocks = std::max(max_lrf_blocks, cdiv(d.x, LRF_BLOCK) * cdiv(d.y, tpb));
+  }
   void fork_streams() {
     if (!forking()) return;
     CUDA_TRY(cudaEventRecord(ev_fork, stream));
@@ -688,9 +700,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     B.max_nwat = std::max(B.max_nwat, V.nwat);
     B.max_ncgp_sol = std::max(B.max_ncgp_sol, V.ncgp_solute);
     B.max_ncgp = std::max(B.max_ncgp, V.ncgp);
-    if (V.use_LRF)
-      B.max_lrf_blocks = std::max(B.max_lrf_blocks, Batch::cdiv(V.ncgp, LRF_BLOCK) *
-                                                        Batch::cdiv(S.nlrft, LRF_TILES_PER_BLOCK));
+    if (V.use_LRF) B.lrf_dims.push_back(make_int2(V.ncgp, S.nlrft));
     B.max_terms = std::max(B.max_terms, V.nbonds + V.nangles + V.ntors + V.nimps);
     B.max_pp = std::max(B.max_pp, S.pp_cap);
     if (V.nwat > 0) B.max_ncgp_sol_w = std::max(B.max_ncgp_sol_w, V.ncgp_solute);
@@ -834,11 +844,16 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   const int rec_words = B.opt.precision == QB_MIXED ? WatRec<true>::words : WatRec<false>::words;
   const int chunk_max = WW_STAGE_BYTES / (16 * rec_words) / 32 * 32;
   P.ww_chunk = std::max(std::min((B.max_nwat + 31) / 32 * 32, chunk_max), 32);
+  // the split counts are sized for the smallest chunk a tuning may choose
+  B.ww_chunk_max = P.ww_chunk;
+  B.ww_chunk_floor = std::max(32, std::min(P.ww_chunk, 256));
+  const int nch_alloc = (std::max(B.max_nwat, 1) + B.ww_chunk_floor - 1) / B.ww_chunk_floor;
   P.ww_nch = (std::max(B.max_nwat, 1) + P.ww_chunk - 1) / P.ww_chunk;
+  B.set_lrf_tpb(LRF_TILES_PER_BLOCK);
   P.ww_cap = ww_cap;
   P.ww = dev_alloc<uint16_t>((size_t)std::max(woff, 1) * ww_cap, o);
   P.ww_n = dev_alloc<int>(std::max(woff, 1), o);
-  P.ww_sp = dev_alloc<int>((size_t)std::max(woff, 1) * P.ww_nch, o);
+  P.ww_sp = dev_alloc<int>((size_t)std::max(woff, 1) * nch_alloc, o);
   P.wrec = dev_alloc<float4>((size_t)std::max(woff, 1) * rec_words, o);
   // the limit (not an allocation) covers every chunk size any batch may use
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
@@ -894,6 +909,15 @@ void ensure_history(Batch &B, int nsteps) {
   B.P.hist = nh;
   B.P.hist_cap = (int)cap;
   B.drop_graphs();
+}
+
+// Energy-record counts of every system back to zero.
+void clear_history(Batch &B) {
+  std::vector<SysState> st(B.nsys);
+  CUDA_TRY(cudaStreamSynchronize(B.stream));
+  CUDA_TRY(cudaMemcpy(st.data(), B.P.st, sizeof(SysState) * B.nsys, cudaMemcpyDeviceToHost));
+  for (auto &x : st) x.hist_n[0] = x.hist_n[1] = 0;
+  CUDA_TRY(cudaMemcpy(B.P.st, st.data(), sizeof(SysState) * B.nsys, cudaMemcpyHostToDevice));
 }
 
 template <class F>
@@ -1046,6 +1070,116 @@ int qb_batch_run_timed(qb_batch *bb, int nsteps, double *device_ms, long long *k
   });
 }
 
+namespace qb {
+namespace {
+
+void get_tuning(const Batch &B, qb_tuning *t) {
+  t->lrf_tiles_per_block = B.P.lrf_tpb;
+  t->ww_chunk = B.P.ww_chunk;
+  t->side_streams = B.streams_on ? 1 : 0;
+  t->ww_chunk_min = B.ww_chunk_floor;
+  t->ww_chunk_max = B.ww_chunk_max;
+}
+
+void set_tuning(Batch &B, const qb_tuning &t) {
+  if (t.lrf_tiles_per_block < 1 || t.lrf_tiles_per_block > 1024) fail(QB_ERR_ARG, "lrf_tiles_per_block out of range");
+  if (t.ww_chunk % 32 || t.ww_chunk < B.ww_chunk_floor || t.ww_chunk > B.ww_chunk_max)
+    fail(QB_ERR_ARG, "ww_chunk must be a multiple of 32 within the batch's range");
+  CUDA_TRY(cudaStreamSynchronize(B.stream));
+  B.drop_graphs();
+  B.set_lrf_tpb(t.lrf_tiles_per_block);
+  B.P.ww_chunk = t.ww_chunk;
+  B.P.ww_nch = (std::max(B.max_nwat, 1) + t.ww_chunk - 1) / t.ww_chunk;
+  B.streams_on = t.side_streams != 0;
+  B.lists_stale = true;   // the water-water split counts depend on the chunk
+}
+
+// device ms per step of `steps` steps after one list cycle of warm-up
+double time_steps(Batch &B, int steps) {
+  for (int k = 0; k < B.NB; k++) B.step();
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  CUDA_TRY(cudaEventRecord(e0, B.stream));
+  for (int k = 0; k < steps; k++) B.step();
+  CUDA_TRY(cudaEventRecord(e1, B.stream));
+  CUDA_TRY(cudaEventSynchronize(e1));
+  float ms = 0;
+  CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  B.sync_status();
+  return ms / steps;
+}
+
+}  // namespace
+}  // namespace qb
+
+int qb_batch_get_tuning(qb_batch *bb, qb_tuning *out) {
+  if (!bb || !out) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
+  std::memset(out, 0, sizeof *out);
+  qb::get_tuning(bb->b, out);
+  return QB_OK;
+}
+
+int qb_batch_set_tuning(qb_batch *bb, const qb_tuning *t) {
+  if (!bb || !t) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
+  return guarded_batch([&] {
+    CUDA_TRY(cudaSetDevice(bb->b.opt.device));
+    qb::set_tuning(bb->b, *t);
+  });
+}
+
+int qb_batch_autotune(qb_batch *bb, int steps_per_trial, qb_tuning *out) {
+  if (!bb || steps_per_trial <= 0) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
+  return guarded_batch([&] {
+    Batch &B = bb->b;
+    CUDA_TRY(cudaSetDevice(B.opt.device));
+    const int steps = (steps_per_trial + B.NB - 1) / B.NB * B.NB;
+    qb::ensure_history(B, steps + B.NB);
+    qb_tuning best{};
+    qb::get_tuning(B, &best);
+    int trials = 0;
+    auto run = [&](const qb_tuning &t) {
+      qb::set_tuning(B, t);
+      trials++;
+      double ms = qb::time_steps(B, steps);
+      qb::clear_history(B);
+      return ms;
+    };
+    const double before = run(best);
+    double best_ms = before;
+    auto consider = [&](qb_tuning t) {
+      double ms = run(t);
+      if (ms < best_ms) { best_ms = ms; best = t; }
+    };
+    if (B.any_lrf)
+      for (int tpb : {1, 2, 8, 16, 4}) {
+        qb_tuning t = best;
+        t.lrf_tiles_per_block = tpb;
+        if (tpb != best.lrf_tiles_per_block) consider(t);
+      }
+    if (B.max_nwat > 0)
+      for (int div : {2, 4}) {
+        qb_tuning t = best;
+        const int c = (B.ww_chunk_max / div + 31) / 32 * 32;
+        if (c < B.ww_chunk_floor || c == best.ww_chunk) continue;
+        t.ww_chunk = c;
+        consider(t);
+      }
+    if (B.side[0]) {
+      qb_tuning t = best;
+      t.side_streams = !best.side_streams;
+      consider(t);
+    }
+    qb::set_tuning(B, best);
+    best.trials = trials;
+    best.ms_per_step = best_ms;
+    best.ms_per_step_before = before;
+    if (out) *out = best;
+  });
+}
+
 int qb_batch_fep(qb_batch *bb, const int *sys, int nfiles, const qb_fep_params *p, qb_fep_result *out) {
   if (!bb || !sys || !p || nfiles < 1) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
   return guarded_batch([&] {
@@ -1185,14 +1319,7 @@ int qb_batch_history(qb_batch *bb, int sys, int kind, int *count, int *steps, do
 
 int qb_batch_clear_history(qb_batch *bb) {
   if (!bb) return QB_ERR_ARG;
-  return guarded_batch([&] {
-    Batch &B = bb->b;
-    std::vector<qb::SysState> st(B.nsys);
-    CUDA_TRY(cudaStreamSynchronize(B.stream));
-    CUDA_TRY(cudaMemcpy(st.data(), B.P.st, sizeof(qb::SysState) * B.nsys, cudaMemcpyDeviceToHost));
-    for (auto &x : st) x.hist_n[0] = x.hist_n[1] = 0;
-    CUDA_TRY(cudaMemcpy(B.P.st, st.data(), sizeof(qb::SysState) * B.nsys, cudaMemcpyHostToDevice));
-  });
+  return guarded_batch([&] { qb::clear_history(bb->b); });
 }
 
 int qb_batch_status(qb_batch *bb, int sys, int *status) {

@@ -140,6 +140,7 @@ struct DevPtrs {
   uint16_t *ww;                            // [gw*ww_cap + k] local water index
   int *ww_n, *ww_sp;                       // count per water; [gw*ww_nch + c] count below chunk c's end
   int ww_cap, ww_chunk, ww_nch;
+  int lrf_tpb;                             // source tiles swept by one block of the LRF gather
   // energies
   double *kin;                             // [s*4] kinetic energy of this step: solute all, free, solvent all, free
   int kin_nblk;

@@ -162,7 +162,7 @@ __device__ __forceinline__ void lrf_fold(double *m, const double *t) {
 // sphere centre, |offset| >= ~7 A here), each tile summed in FP32 and added to
 // FP64 totals.
 constexpr int LRF_TILE_G = 128, LRF_TILE_A = 512, LRF_BLOCK = 128;
-constexpr int LRF_TILES_PER_BLOCK = 4;   // source tiles one block sweeps; larger systems use more blocks
+constexpr int LRF_TILES_PER_BLOCK = 4;   // default source tiles per block (P.lrf_tpb); larger systems use more blocks
 
 template <bool MIXED>
 __global__ void __launch_bounds__(LRF_BLOCK, MIXED ? 8 : 5) k_lrf_gather(DevPtrs P, int force) {
@@ -173,10 +173,11 @@ __global__ void __launch_bounds__(LRF_BLOCK, MIXED ? 8 : 5) k_lrf_gather(DevPtrs
   const SysDev &S = P.sys[s];
   if (!S.use_lrf) return;
   // block -> (chunk of target groups, range of source tiles)
-  const int hsplit = (S.nlrft + LRF_TILES_PER_BLOCK - 1) / LRF_TILES_PER_BLOCK;
+  const int tpb = P.lrf_tpb;
+  const int hsplit = (S.nlrft + tpb - 1) / tpb;
   const int gchunk = blockIdx.x / max(hsplit, 1), hpart = blockIdx.x % max(hsplit, 1);
   if (hsplit == 0 || gchunk * LRF_BLOCK >= S.ncgp) return;
-  const int t0 = hpart * LRF_TILES_PER_BLOCK, t1 = min(t0 + LRF_TILES_PER_BLOCK, S.nlrft);
+  const int t0 = hpart * tpb, t1 = min(t0 + tpb, S.nlrft);
   __shared__ double4 hsw[LRF_TILE_G];      // switching atom; w: -1 excluded, 1 solute, 0 water
   __shared__ int2 hrange[LRF_TILE_G];      // first atom slot, atom count
   __shared__ R4 hat[LRF_TILE_A];           // atom position (mixed: from the sphere centre), charge

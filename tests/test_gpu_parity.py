@@ -259,3 +259,48 @@ def test_perturbations_with_different_q_atoms_in_one_batch(tmp_path, oracle):
         Eo, EQo = o.energy_vectors()
         assert_energies(Eg, EQg, Eo, EQo)
         assert grad_err(batch.gradient(k), o.gradient()) < G_TOL
+
+
+def test_tuning_changes_only_rounding(synthetic, oracle):
+    """The run-time choices of the step kernels (LRF tiles per block, water
+    chunk, side streams) change only the order of atomic sums: two copies of
+    a batch, one with other settings, give the same records and coordinates
+    to rounding; out-of-range settings are refused; after autotuning the
+    batch still matches the oracle."""
+    from q_b200 import QBError
+    inp = synthetic["c1"].inp
+    runs = []
+    for setting in (None, dict(lrf_tiles_per_block=1, ww_chunk=256, side_streams=0)):
+        s = System.open(inp, lambdas=(0.4, 0.6), seed=5)
+        b = Batch([s], precision=FP64)
+        t = b.tuning()
+        assert t["ww_chunk_min"] <= 256 <= t["ww_chunk_max"] and t["ww_chunk"] == t["ww_chunk_max"]
+        if setting:
+            b.set_tuning(**setting)
+            t = b.tuning()
+            assert (t["lrf_tiles_per_block"], t["ww_chunk"], t["side_streams"]) == (1, 256, 0)
+        b.run(60)          # crosses two list rebuilds
+        runs.append((b.history(0, 0), b.coords(0)))
+    ((s0, E0, Q0), x0), ((s1, E1, Q1), x1) = runs
+    assert list(s0) == list(s1)
+    assert np.max(np.abs(E0 - E1)) < 1e-6 and np.max(np.abs(Q0 - Q1)) < 1e-6
+    assert np.max(np.abs(x0 - x1)) < 1e-8
+    with pytest.raises(QBError):
+        b.set_tuning(ww_chunk=100)
+    with pytest.raises(QBError):
+        b.set_tuning(lrf_tiles_per_block=0)
+    s = System.open(inp, lambdas=(0.4, 0.6), seed=5)
+    b = Batch([s, s], precision=FP64)
+    r = b.autotune(50)
+    assert r["trials"] >= 3 and r["ms_per_step"] <= r["ms_per_step_before"]
+    assert r["ww_chunk_min"] <= r["ww_chunk"] <= r["ww_chunk_max"] and r["lrf_tiles_per_block"] >= 1
+    # the chosen setting, applied to a fresh batch, matches the oracle
+    b = Batch([s], precision=FP64)
+    b.set_tuning(**{k: r[k] for k in ("lrf_tiles_per_block", "ww_chunk", "side_streams")})
+    b.final_energy()
+    o = oracle.create(s)
+    o.final_energy()
+    Eg, EQg = b.energy_vectors(0)
+    Eo, EQo = o.energy_vectors()
+    assert_energies(Eg, EQg, Eo, EQo)
+    assert grad_err(b.gradient(0), o.gradient()) < G_TOL

@@ -19,7 +19,8 @@ The fixtures are the reference's own test inputs and known answers, copied
                 the log prints for random_seed 112 at 1 K.
   data/         test/data/topology and test/data/inputs: topologies and FEP
                 files of the reference's Q6-vs-QGPU comparison harness
-                (test/runTEST.py), used as extra GPU-vs-oracle parity cases.
+                (test/runTEST.py); its interaction-class cases (p-p, q-p,
+                q-p-w, q-q, w-p, w-q, w-w) are GPU-vs-oracle parity cases.
 """
 from __future__ import annotations
 
@@ -33,7 +34,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def gz_copy(src: str, dst: str) -> None:
-    with open(src, "rb") as f, gzip.open(dst + ".gz", "wb", compresslevel=9) as g:
+    # mtime 0: the same input gives the same bytes
+    with open(src, "rb") as f, open(dst + ".gz", "wb") as raw, \
+            gzip.GzipFile(fileobj=raw, mode="wb", compresslevel=9, mtime=0) as g:
         g.write(f.read())
 
 
@@ -68,9 +71,10 @@ def main(ref: str) -> None:
 
     out = os.path.join(HERE, "data")
     os.makedirs(out, exist_ok=True)
-    for name in ["ala_wat.top", "benzene-water.top", "dualtop_vacuum.top", "water.top"]:
+    for name in ["ala_wat.top", "benzene-water.top", "benzene-vacuum.top", "dualtop_vacuum.top", "water.top",
+                 "Na-benzene-vacuum.top", "Na-benzene-water.top"]:
         gz_copy(os.path.join(ref, "test/data/topology", name), os.path.join(out, name))
-    for name in ["FEP_benzene.fep", "dualtop.fep"]:
+    for name in ["FEP_benzene.fep", "FEP_Na.fep", "dualtop.fep"]:
         shutil.copy(os.path.join(ref, "test/data/inputs", name), os.path.join(out, name))
 
 

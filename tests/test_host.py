@@ -271,3 +271,17 @@ def test_dcd_layout_and_mask(tmp_path, golden):
     assert h["mask_rows"] == ["not excluded"] and h["atoms"] == m.sum()
     assert fr.shape == (2, m.sum(), 3)
     assert np.array_equal(fr[1], xs[1].reshape(-1, 3)[m].astype(np.float32))
+
+
+def test_reference_cases_open(golden):
+    """Every case of the reference's comparison harness reads and prepares:
+    benzene, Na+ and benzene in water, water alone, the dual-topology FEP."""
+    from tests.reference_cases import CASES, write_case
+    sizes = {}
+    for case in CASES:
+        for shake in (False, True):
+            s = System.open(write_case(str(golden / "data"), case, shake=shake))
+            v = s.view
+            sizes[case] = (v.natom, v.nqat)
+            assert (v.shake_constraints > 0) == shake
+    assert sizes["w-w"] == (3423, 0) and sizes["q-p-w_Na"] == (3418, 1) and sizes["dualtop"] == (98, 98)

@@ -66,7 +66,7 @@ typedef struct qb_sysview {
 
   /* ---- force-field switches ---- */
   int ff_type;          /* 1 GROMOS (harmonic impropers), 2 AMBER (periodic), 3 CHARMM */
-  int ivdw_rule;        /* 1 geometric (the only rule this engine implements) */
+  int ivdw_rule;        /* 1 geometric (type_avdw/bvdw = sqrt A, sqrt B); 2 arithmetic (R*, sqrt(eps)) */
   int solvent_type;     /* 0 SPC-like 3-site water */
   int iuse_switch_atom; /* 1: charge-group cut-off on switching atoms */
   double el14_scale, coulomb_constant;

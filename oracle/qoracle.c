@@ -347,6 +347,24 @@ static void make_pair_lists(qo_state *st) {
 static double avdw(const qb_sysview *s, int t, int lj) { return s->type_avdw[3 * t + lj - 1]; }
 static double bvdw(const qb_sysview *s, int t, int lj) { return s->type_bvdw[3 * t + lj - 1]; }
 
+/* LJ coefficients of a pair, V = A/r^12 - B/r^6.  Geometric rule
+   (nonbond_*): A = a_i a_j, B = b_i b_j.  Arithmetic rule (nonbon2_*,
+   md.f90:8972-9089; a = R*, b = sqrt(eps) after set-up):
+   A = b_i b_j (a_i + a_j)^12, B = 2 b_i b_j (a_i + a_j)^6. */
+static void ljp(const qb_sysview *s, double ai, double aj, double bi, double bj, double *A, double *B) {
+  if (s->ivdw_rule != 2) {
+    *A = ai * aj;
+    *B = bi * bj;
+    return;
+  }
+  double a = ai + aj;
+  a = a * a;
+  a = a * a * a;
+  double e = bi * bj;
+  *A = e * a * a;
+  *B = 2.0 * e * a;
+}
+
 static void apply_pair(qo_state *st, int i, int j, double dv, const double dx[3]) {
   for (int k = 0; k < 3; k++) { D(i, k) -= dv * dx[k]; D(j, k) += dv * dx[k]; }
 }
@@ -363,8 +381,16 @@ static void nonbond_pp(qo_state *st) {
     double Vel = (double)qq * r;
     if (lj == 3) Vel = Vel * s->el14_scale;
     int ti = s->iac[i], tj = s->iac[j];
-    double Va = r6 * r6 * avdw(s, ti, lj) * avdw(s, tj, lj);
-    double Vb = r6 * bvdw(s, ti, lj) * bvdw(s, tj, lj);
+    double Va, Vb;
+    if (s->ivdw_rule == 2) {   /* nonbon2_pp (md.f90:8972) */
+      double A, B;
+      ljp(s, avdw(s, ti, lj), avdw(s, tj, lj), bvdw(s, ti, lj), bvdw(s, tj, lj), &A, &B);
+      Va = A * r6 * r6;
+      Vb = B * r6;
+    } else {
+      Va = r6 * r6 * avdw(s, ti, lj) * avdw(s, tj, lj);
+      Vb = r6 * bvdw(s, ti, lj) * bvdw(s, tj, lj);
+    }
     double dv = r2 * (-Vel - 12. * Va + 6. * Vb);
     apply_pair(st, i, j, dv, dx);
     st->E[QB_E_PP_EL] += Vel;
@@ -378,7 +404,8 @@ static void nonbond_pw(qo_state *st) {
   for (int p = 0; p < st->npw; p++) {
     int i = st->pw[p].i, j = st->pw[p].j, lj = st->pw[p].lj;
     int ti = s->iac[i], tj = s->iac[j];
-    double aLJ = avdw(s, ti, lj) * avdw(s, tj, lj), bLJ = bvdw(s, ti, lj) * bvdw(s, tj, lj);
+    double aLJ, bLJ;
+    ljp(s, avdw(s, ti, lj), avdw(s, tj, lj), bvdw(s, ti, lj), bvdw(s, tj, lj), &aLJ, &bLJ);
     double dx[3] = {X(j, 0) - X(i, 0), X(j, 1) - X(i, 1), X(j, 2) - X(i, 2)};
     double r2 = 1. / (dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
     double r = sqrt(r2), r6 = r2 * r2 * r2, r12 = r6 * r6;
@@ -407,7 +434,8 @@ static void nonbond_qp(qo_state *st) {
       double r6 = r2 * r2 * r2, r = sqrt(r2);
       for (int ss = 0; ss < S; ss++) {
         int ti = s->iac[i];
-        double aLJ = avdw(s, ti, lj) * avdw(s, tj, lj), bLJ = bvdw(s, ti, lj) * bvdw(s, tj, lj);
+        double aLJ, bLJ;
+        ljp(s, avdw(s, ti, lj), avdw(s, tj, lj), bvdw(s, ti, lj), bvdw(s, tj, lj), &aLJ, &bLJ);
         float qq = s->qcrg[iq * S + ss] * s->crg[j];
         double Vel = (double)qq * r;
         if (lj == 3) Vel = Vel * s->el14_scale;
@@ -423,8 +451,8 @@ static void nonbond_qp(qo_state *st) {
       double r = sqrt(r2);
       for (int ss = 0; ss < S; ss++) {
         int ti = s->qiac[iq * S + ss];
-        double aLJ = s->qavdw[3 * ti + qlj - 1] * avdw(s, tj, lj);
-        double bLJ = s->qbvdw[3 * ti + qlj - 1] * bvdw(s, tj, lj);
+        double aLJ, bLJ;
+        ljp(s, s->qavdw[3 * ti + qlj - 1], avdw(s, tj, lj), s->qbvdw[3 * ti + qlj - 1], bvdw(s, tj, lj), &aLJ, &bLJ);
         float qq = s->qcrg[iq * S + ss] * s->crg[j];
         double Vel = (double)qq * r;
         if (lj == 3) Vel = Vel * s->el14_scale;
@@ -497,17 +525,19 @@ static void nonbond_qw(qo_state *st) {
       double r6sc = r6hc, dvO = 0, dvH1 = 0, dvH2 = 0, Va = 0, Vb = 0;
       int lj = ljcode(s, iac_ow, s->iac[i]);
       if (!s->qvdw_flag) {
-        double r6O = 1. / r6hc;
-        Va = avdw(s, s->iac[i], lj) * aO[lj - 1] * r6O * r6O;
-        Vb = bvdw(s, s->iac[i], lj) * bO[lj - 1] * r6O;
+        double r6O = 1. / r6hc, A, B;
+        ljp(s, avdw(s, s->iac[i], lj), aO[lj - 1], bvdw(s, s->iac[i], lj), bO[lj - 1], &A, &B);
+        Va = A * r6O * r6O;
+        Vb = B * r6O;
       }
       for (int ss = 0; ss < S; ss++) {
         if (s->qvdw_flag) {
           int ti = s->qiac[iq * S + ss];
-          double aLJ = s->qavdw[3 * ti], bLJ = s->qbvdw[3 * ti];
+          double A, B;
+          ljp(s, s->qavdw[3 * ti], aO[lj - 1], s->qbvdw[3 * ti], bO[lj - 1], &A, &B);
           r6sc = r6hc + s->sc_lookup[((size_t)iq * ncol + iac_ow) * S + ss];
-          Va = aLJ * aO[lj - 1] / (r6sc * r6sc);
-          Vb = bLJ * bO[lj - 1] / r6sc;
+          Va = A / (r6sc * r6sc);
+          Vb = B / r6sc;
         }
         float qq = s->qcrg[iq * S + ss];
         double VelO = (double)(s->crg_ow * qq) * rO;
@@ -542,23 +572,19 @@ static void nonbond_qq(qo_state *st) {
       double el = s->nbqq_el_scale[p];
       if (!s->qvdw_flag) {
         int ti = s->iac[i], tj = s->iac[j];
-        aLJ = avdw(s, ti, lj) * avdw(s, tj, lj);
-        bLJ = bvdw(s, ti, lj) * bvdw(s, tj, lj);
+        ljp(s, avdw(s, ti, lj), avdw(s, tj, lj), bvdw(s, ti, lj), bvdw(s, tj, lj), &aLJ, &bLJ);
         qj = jq >= 0 ? (double)s->qcrg[jq * S + ss] : (double)s->crg[j];
       } else {
         int ti = s->qiac[iq * S + ss];
-        aLJ = s->qavdw[3 * ti + lj - 1];
-        bLJ = s->qbvdw[3 * ti + lj - 1];
+        double ai = s->qavdw[3 * ti + lj - 1], bi = s->qbvdw[3 * ti + lj - 1];
         if (jq >= 0) {
           int tj = s->qiac[jq * S + ss];
-          aLJ *= s->qavdw[3 * tj + lj - 1];
-          bLJ *= s->qbvdw[3 * tj + lj - 1];
+          ljp(s, ai, s->qavdw[3 * tj + lj - 1], bi, s->qbvdw[3 * tj + lj - 1], &aLJ, &bLJ);
           qj = s->qcrg[jq * S + ss];
         } else {
-          if (lj == 2) { aLJ = s->qavdw[3 * ti]; bLJ = s->qbvdw[3 * ti]; }
+          if (lj == 2) { ai = s->qavdw[3 * ti]; bi = s->qbvdw[3 * ti]; }
           int tj = s->iac[j];
-          aLJ *= avdw(s, tj, lj);
-          bLJ *= bvdw(s, tj, lj);
+          ljp(s, ai, avdw(s, tj, lj), bi, bvdw(s, tj, lj), &aLJ, &bLJ);
           qj = s->crg[j];
         }
       }

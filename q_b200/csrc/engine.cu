@@ -627,6 +627,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     S.fk_pshell = V.fk_pshell; S.fk_fix = V.fk_fix;
     for (int k = 0; k < S.nshell; k++) { S.ws_rout[k] = V.wshell_rout[k]; S.ws_dr[k] = V.wshell_dr[k]; S.ws_cstb[k] = V.wshell_cstb[k]; }
     for (int k = 0; k < V.nstates; k++) S.lambda[k] = V.lambda[k];
+    S.arith = V.ivdw_rule == 2 ? 1 : 0;
     if (V.nwat > 0) {
       S.aO[0] = V.type_avdw[3 * V.iac_ow]; S.aO[1] = V.type_avdw[3 * V.iac_ow + 1];
       S.bO[0] = V.type_bvdw[3 * V.iac_ow]; S.bO[1] = V.type_bvdw[3 * V.iac_ow + 1];
@@ -683,10 +684,12 @@ void build(Batch &B, qb_handle *const *hs, int n) {
         const int ti = V.iac[i];
         const int lo = V.ljcod[ti * V.natyps + to], lh = V.ljcod[ti * V.natyps + th];
         PwAtom r;
-        r.lj = make_double4(V.type_avdw[3 * ti + lo - 1] * V.type_avdw[3 * to + lo - 1],
-                            V.type_bvdw[3 * ti + lo - 1] * V.type_bvdw[3 * to + lo - 1],
-                            V.type_avdw[3 * ti + lh - 1] * V.type_avdw[3 * th + lh - 1],
-                            V.type_bvdw[3 * ti + lh - 1] * V.type_bvdw[3 * th + lh - 1]);
+        double Ao, Bo, Ah, Bh;
+        lj_pair(V.ivdw_rule == 2, V.type_avdw[3 * ti + lo - 1], V.type_avdw[3 * to + lo - 1],
+                V.type_bvdw[3 * ti + lo - 1], V.type_bvdw[3 * to + lo - 1], Ao, Bo);
+        lj_pair(V.ivdw_rule == 2, V.type_avdw[3 * ti + lh - 1], V.type_avdw[3 * th + lh - 1],
+                V.type_bvdw[3 * ti + lh - 1], V.type_bvdw[3 * th + lh - 1], Ah, Bh);
+        r.lj = make_double4(Ao, Bo, Ah, Bh);
         r.q = make_float2(V.crg[i] * V.crg[o], V.crg[i] * V.crg[o + 1]);
         r.atom = aoff + i;
         r.pad = 0;

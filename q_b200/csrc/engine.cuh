@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include "qb.h"
+#include "ljrule.hpp"
 
 namespace qb {
 
@@ -57,6 +58,7 @@ struct SysDev {
   float ws_rout[MAX_SHELLS], ws_dr[MAX_SHELLS], ws_cstb[MAX_SHELLS];
   double lambda[MAXS];
   double aO[2], bO[2];
+  int arith;                       // 1: arithmetic LJ combination rule (lj_pair)
 };
 
 // Per-system state written by the device.

@@ -866,8 +866,16 @@ __device__ __forceinline__ void nb_pp_body(DevPtrs &P, int bx, int s, int gx) {
       float qq = P.crg[i] * P.crg[j];
       double Vel = (double)qq * r;
       if (lj == 3) Vel = Vel * S.el14;
-      double Va = r6 * r6 * P.lja[3 * i + lj - 1] * P.lja[3 * j + lj - 1];
-      double Vb = r6 * P.ljb[3 * i + lj - 1] * P.ljb[3 * j + lj - 1];
+      double Va, Vb;
+      if (S.arith) {
+        double A, B;
+        lj_pair(1, P.lja[3 * i + lj - 1], P.lja[3 * j + lj - 1], P.ljb[3 * i + lj - 1], P.ljb[3 * j + lj - 1], A, B);
+        Va = A * r6 * r6;
+        Vb = B * r6;
+      } else {
+        Va = r6 * r6 * P.lja[3 * i + lj - 1] * P.lja[3 * j + lj - 1];
+        Vb = r6 * P.ljb[3 * i + lj - 1] * P.ljb[3 * j + lj - 1];
+      }
       double dv = r2 * (-Vel - 12. * Va + 6. * Vb);
       atomic_add3(P.d, i, -dv * dx, -dv * dy, -dv * dz);
       atomic_add3(P.d, j, dv * dx, dv * dy, dv * dz);
@@ -974,8 +982,9 @@ __device__ __forceinline__ void nb_qp_body(DevPtrs &P, int bx, int s, int gx) {
         double r = rsqrt(r2);
         r2 = r * r;
         double r6 = r2 * r2 * r2;
-        double aLJ = P.lja[3 * i + lj - 1] * P.lja[3 * j + lj - 1];
-        double bLJ = P.ljb[3 * i + lj - 1] * P.ljb[3 * j + lj - 1];
+        double aLJ, bLJ;
+        lj_pair(S.arith, P.lja[3 * i + lj - 1], P.lja[3 * j + lj - 1], P.ljb[3 * i + lj - 1], P.ljb[3 * j + lj - 1],
+                aLJ, bLJ);
         for (int st = 0; st < NS; st++) {
           float qq = P.qcrg[gq * MAXS + st] * P.crg[j];
           double Vel = (double)qq * r;
@@ -992,8 +1001,9 @@ __device__ __forceinline__ void nb_qp_body(DevPtrs &P, int bx, int s, int gx) {
         int tj = P.iac[j];
         for (int st = 0; st < NS; st++) {
           int ti = P.qiac[gq * MAXS + st];
-          double aLJ = P.qavdw[S.qlib_off + 3 * ti + qlj - 1] * P.lja[3 * j + lj - 1];
-          double bLJ = P.qbvdw[S.qlib_off + 3 * ti + qlj - 1] * P.ljb[3 * j + lj - 1];
+          double aLJ, bLJ;
+          lj_pair(S.arith, P.qavdw[S.qlib_off + 3 * ti + qlj - 1], P.lja[3 * j + lj - 1],
+                  P.qbvdw[S.qlib_off + 3 * ti + qlj - 1], P.ljb[3 * j + lj - 1], aLJ, bLJ);
           float qq = P.qcrg[gq * MAXS + st] * P.crg[j];
           double Vel = (double)qq * r;
           if (lj == 3) Vel = Vel * S.el14;
@@ -1045,15 +1055,16 @@ __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
     double4 x = P.x[i];
     x.w = (double)lj;
     qx[iq] = x;
-    qab[iq] = make_double2(P.lja[3 * i + lj - 1] * S.aO[lj - 1], P.ljb[3 * i + lj - 1] * S.bO[lj - 1]);
+    double A0, B0;
+    lj_pair(S.arith, P.lja[3 * i + lj - 1], S.aO[lj - 1], P.ljb[3 * i + lj - 1], S.bO[lj - 1], A0, B0);
+    qab[iq] = make_double2(A0, B0);
     for (int st = 0; st < NS; st++) {
       QwState q;
       float c = P.qcrg[gq * MAXS + st];
       q.qO = S.crg_ow * c;
       q.qH = S.crg_hw * c;
       int ti = P.qiac[gq * MAXS + st];
-      q.A = P.qavdw[S.qlib_off + 3 * ti] * S.aO[lj - 1];
-      q.B = P.qbvdw[S.qlib_off + 3 * ti] * S.bO[lj - 1];
+      lj_pair(S.arith, P.qavdw[S.qlib_off + 3 * ti], S.aO[lj - 1], P.qbvdw[S.qlib_off + 3 * ti], S.bO[lj - 1], q.A, q.B);
       q.sc = S.qvdw ? P.sc[S.sc_off + ((size_t)iq * ncol + S.iac_ow) * NS + st] : 0.0;
       qst[iq * NA + st] = q;
     }
@@ -1080,8 +1091,7 @@ __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
       int i = P.iqseq[gq];
       xi4 = P.x[i];
       lj = P.ljcod[S.ljoff + S.iac_ow * S.natyps + P.iac[i]];
-      A0 = P.lja[3 * i + lj - 1] * S.aO[lj - 1];
-      B0 = P.ljb[3 * i + lj - 1] * S.bO[lj - 1];
+      lj_pair(S.arith, P.lja[3 * i + lj - 1], S.aO[lj - 1], P.ljb[3 * i + lj - 1], S.bO[lj - 1], A0, B0);
     }
     double dO[3] = {xO.x - xi4.x, xO.y - xi4.y, xO.z - xi4.z};
     double dH1[3] = {xH1.x - xi4.x, xH1.y - xi4.y, xH1.z - xi4.z};
@@ -1108,8 +1118,8 @@ __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
         float c = P.qcrg[gq * MAXS + st];
         q.qO = S.crg_ow * c; q.qH = S.crg_hw * c;
         int ti = P.qiac[gq * MAXS + st];
-        q.A = P.qavdw[S.qlib_off + 3 * ti] * S.aO[lj - 1];
-        q.B = P.qbvdw[S.qlib_off + 3 * ti] * S.bO[lj - 1];
+        lj_pair(S.arith, P.qavdw[S.qlib_off + 3 * ti], S.aO[lj - 1], P.qbvdw[S.qlib_off + 3 * ti], S.bO[lj - 1], q.A,
+                q.B);
         q.sc = S.qvdw ? P.sc[S.sc_off + ((size_t)iq * ncol + S.iac_ow) * NS + st] : 0.0;
       }
       double r6sc = r6hc;
@@ -1178,22 +1188,20 @@ __device__ __forceinline__ void nb_qq_body(DevPtrs &P, int s) {
       double qi = (double)P.qcrg[gq * MAXS + st], qj, aLJ, bLJ;
       double els = P.qq_el[S.qq_off + k];
       if (!S.qvdw) {
-        aLJ = P.lja[3 * i + lj - 1] * P.lja[3 * j + lj - 1];
-        bLJ = P.ljb[3 * i + lj - 1] * P.ljb[3 * j + lj - 1];
+        lj_pair(S.arith, P.lja[3 * i + lj - 1], P.lja[3 * j + lj - 1], P.ljb[3 * i + lj - 1], P.ljb[3 * j + lj - 1],
+                aLJ, bLJ);
         qj = jq >= 0 ? (double)P.qcrg[gjq * MAXS + st] : (double)P.crg[j];
       } else {
         int ti = P.qiac[gq * MAXS + st];
-        aLJ = P.qavdw[S.qlib_off + 3 * ti + lj - 1];
-        bLJ = P.qbvdw[S.qlib_off + 3 * ti + lj - 1];
+        double ai = P.qavdw[S.qlib_off + 3 * ti + lj - 1], bi = P.qbvdw[S.qlib_off + 3 * ti + lj - 1];
         if (jq >= 0) {
           int tj = P.qiac[gjq * MAXS + st];
-          aLJ *= P.qavdw[S.qlib_off + 3 * tj + lj - 1];
-          bLJ *= P.qbvdw[S.qlib_off + 3 * tj + lj - 1];
+          lj_pair(S.arith, ai, P.qavdw[S.qlib_off + 3 * tj + lj - 1], bi, P.qbvdw[S.qlib_off + 3 * tj + lj - 1], aLJ,
+                  bLJ);
           qj = P.qcrg[gjq * MAXS + st];
         } else {
-          if (lj == 2) { aLJ = P.qavdw[S.qlib_off + 3 * ti]; bLJ = P.qbvdw[S.qlib_off + 3 * ti]; }
-          aLJ *= P.lja[3 * j + lj - 1];
-          bLJ *= P.ljb[3 * j + lj - 1];
+          if (lj == 2) { ai = P.qavdw[S.qlib_off + 3 * ti]; bi = P.qbvdw[S.qlib_off + 3 * ti]; }
+          lj_pair(S.arith, ai, P.lja[3 * j + lj - 1], bi, P.ljb[3 * j + lj - 1], aLJ, bLJ);
           qj = P.crg[j];
         }
       }

@@ -1147,7 +1147,17 @@ void read_fep(const std::string &path, const Topology &t, Fep &f) {
           if (f.softcore_use_max_potential) {
             double aq = f.qavdw[f.qiac[i * S + s] * 3 + 0], bq = f.qbvdw[f.qiac[i * S + s] * 3 + 0];
             double aj = t.iaclib[j].avdw[0], bj = t.iaclib[j].bvdw[0];
-            if (am != 0) SC(i, j, s) = (-bq * bj + std::sqrt(bq * bq * bj * bj + 4 * am * aq * aj)) / (2 * am);
+            if (am != 0) {
+              if (t.ivdw_rule == 2) {
+                // arithmetic rule: bq is still epsilon, bj already sqrt(epsilon) (qatom.f90:1618-1622)
+                double s6 = (aq + aj) * (aq + aj);
+                s6 = s6 * s6 * s6;
+                SC(i, j, s) = (-2 * std::sqrt(bq) * bj + 2 * std::sqrt(bq * bj * bj + am * std::sqrt(bq) * bj)) *
+                              s6 / (2 * am);
+              } else {
+                SC(i, j, s) = (-bq * bj + std::sqrt(bq * bq * bj * bj + 4 * am * aq * aj)) / (2 * am);
+              }
+            }
           } else {
             SC(i, j, s) = am;
           }
@@ -1161,7 +1171,15 @@ void read_fep(const std::string &path, const Topology &t, Fep &f) {
             if (f.softcore_use_max_potential) {
               tmp = std::min(am, amj);
               if (am == 0 || amj == 0) tmp = std::max(am, amj);
-              SC(i, j + t.natyps, s) = (-bq * bj + std::sqrt(bq * bq * bj * bj + 4 * tmp * aq * aj)) / (2 * tmp);
+              if (t.ivdw_rule == 2) {
+                // arithmetic rule: both epsilons not yet square-rooted (qatom.f90:1660-1664)
+                double s6 = (aq + aj) * (aq + aj);
+                s6 = s6 * s6 * s6;
+                SC(i, j + t.natyps, s) =
+                    (-2 * std::sqrt(bq * bj) + 2 * std::sqrt(bq * bj + tmp * std::sqrt(bq * bj))) * s6 / (2 * tmp);
+              } else {
+                SC(i, j + t.natyps, s) = (-bq * bj + std::sqrt(bq * bq * bj * bj + 4 * tmp * aq * aj)) / (2 * tmp);
+              }
             } else {
               SC(i, j + t.natyps, s) = std::max(am, amj);
             }

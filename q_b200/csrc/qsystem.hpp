@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "qb.h"
+#include "ljrule.hpp"
 
 namespace qb {
 

@@ -82,7 +82,12 @@ void prepare(System &s) {
 
   // ---------------------------------------------------------- topology()
   read_topology(in.top_file, t);
-  if (t.ivdw_rule != 1) fail(QB_ERR_UNSUPPORTED, "only the geometric LJ combination rule is supported");
+  if (t.ivdw_rule != 1 && t.ivdw_rule != 2) fail(QB_ERR_PARSE, "unknown LJ combination rule in the topology");
+  // arithmetic rule: epsilon -> sqrt(|epsilon|) now (md.f90:14747-14751),
+  // before the FEP file's soft-core table is built from it
+  if (t.ivdw_rule == 2)
+    for (auto &ty : t.iaclib)
+      for (int k = 0; k < 3; k++) ty.bvdw[k] = std::sqrt(std::fabs(ty.bvdw[k]));
   if (t.solvent_type != 0 && t.nat_pro > t.nat_solute)
     fail(QB_ERR_UNSUPPORTED, "only SPC-type 3-site water is supported (solvent_type 0)");
   if (t.ff_type == 3) fail(QB_ERR_UNSUPPORTED, "CHARMM force fields (Urey-Bradley) are not supported");
@@ -150,6 +155,13 @@ void prepare(System &s) {
     for (int i = 0; i < f.nqat; i++)
       for (int j = 0; j < S; j++) f.qcrg[i * S + j] = t.crg[f.iqseq[i]];
     read_fep(in.fep_file, t, f);
+    // arithmetic rule: the Q-atom types' epsilons (LJ codes 1 and 3) are
+    // square-rooted after the soft-core table (md.f90:1519-1523)
+    if (t.ivdw_rule == 2 && f.qvdw_flag)
+      for (int k = 0; k < f.nqlib; k++) {
+        f.qbvdw[3 * k + 0] = std::sqrt(f.qbvdw[3 * k + 0]);
+        f.qbvdw[3 * k + 2] = std::sqrt(f.qbvdw[3 * k + 2]);
+      }
     // remove redefined interactions from the topology (md.f90:1512-1598)
     for (auto &b : t.bnd)
       for (auto &q : f.qbnd)
@@ -531,8 +543,15 @@ void prepare(System &s) {
     s.iac_ow = t.iac[NS];
     s.iac_hw = t.iac[NS + 1];
     int lj = s.ljcod[(size_t)s.iac_ow * t.natyps + s.iac_ow] - 1;
-    s.A_OO = t.iaclib[s.iac_ow].avdw[lj] * t.iaclib[s.iac_ow].avdw[lj];
-    s.B_OO = t.iaclib[s.iac_ow].bvdw[lj] * t.iaclib[s.iac_ow].bvdw[lj];
+    const auto &O = t.iaclib[s.iac_ow];
+    lj_pair(t.ivdw_rule == 2, O.avdw[lj], O.avdw[lj], O.bvdw[lj], O.bvdw[lj], s.A_OO, s.B_OO);
+    // the arithmetic rule's water routine (nonbon2_ww) adds LJ on every
+    // atom pair; this path takes the O-O pair only, exact when the water
+    // hydrogens carry no LJ
+    if (t.ivdw_rule == 2)
+      for (int k = 0; k < 3; k++)
+        if (t.iaclib[s.iac_hw].bvdw[k] != 0.0)
+          fail(QB_ERR_UNSUPPORTED, "arithmetic-rule water with Lennard-Jones on its hydrogens (3-atom solvent)");
   }
   s.type_mass.resize(t.natyps); s.type_avdw.resize(3 * (size_t)t.natyps); s.type_bvdw.resize(3 * (size_t)t.natyps);
   for (int i = 0; i < t.natyps; i++) {

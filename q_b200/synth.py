@@ -53,9 +53,14 @@ class AtomType:
     sigma: float
     eps: float
 
-    def columns(self):
+    def columns(self, vdw_rule: int = 1):
+        """(a, b) for LJ codes normal, polar, 1-4 (1-4 at half epsilon):
+        geometric rule sqrt(A), sqrt(B); arithmetic rule R* = 2^(1/6) sigma / 2
+        and epsilon."""
+        if vdw_rule == 2:
+            rs = 2.0 ** (1.0 / 6.0) * self.sigma / 2.0
+            return [(rs, self.eps), (rs, self.eps), (rs, self.eps / 2.0)]
         a, b = lj_sqrt(self.sigma, self.eps)
-        # normal, polar, 1-4 (1-4 LJ at half epsilon)
         return [(a, b), (a, b), (a / math.sqrt(2.0), b / math.sqrt(2.0))]
 
 
@@ -89,6 +94,7 @@ class Topology:
     rexcl_o: float = 20.0
     rwat: float = 20.0
     excl: list = field(default_factory=list)
+    vdw_rule: int = 1                                # 1 geometric, 2 arithmetic
 
     # ----------------------------------------------------------- writer
     def write(self, path: str) -> None:
@@ -151,18 +157,20 @@ class Topology:
                 L.append(" ".join("%5d" % (a + 1) for a in atoms[k:k + 13]))
         nt = len(self.types)
         L.append("%8d = No. of atom types" % nt)
-        L.append("%8d = vdW combination rule (1 = Geom. / 2 = Arit.)" % 1)
+        L.append("%8d = vdW combination rule (1 = Geom. / 2 = Arit.)" % self.vdw_rule)
         L.append("%8.5f%9.4f = Electrostatic 1-4 scaling factor and  Coulomb constant" % (0.5, 332.0))
         L.append("Masses: ")
         for k in range(0, nt, 10):
             L.append(" ".join("%7.3f" % t.mass for t in self.types[k:k + 10]))
-        cols = [t.columns() for t in self.types]
+        cols = [t.columns(self.vdw_rule) for t in self.types]
+        names = ("Aii", "Bii") if self.vdw_rule == 1 else ("R*ii", "epsilon ii")
+        fmt = "%8.2f" if self.vdw_rule == 1 else "%10.5f"
         for c, label in enumerate(["normal", "polar", "1-4"]):
-            for ab, nm in ((0, "Aii"), (1, "Bii")):
-                L.append("sqrt (%s) %s:" % (nm, label))
+            for ab, nm in ((0, names[0]), (1, names[1])):
+                L.append(("sqrt (%s) %s:" if self.vdw_rule == 1 else "%s %s:") % (nm, label))
                 vals = [cols[t][c][ab] for t in range(nt)]
                 for k in range(0, nt, 8):
-                    L.append(" ".join("%8.2f" % v for v in vals[k:k + 8]))
+                    L.append(" ".join(fmt % v for v in vals[k:k + 8]))
         L.append("%8d = No. of type-2 vdW interactions. pairs: " % 0)
         ex_pairs, p14_pairs = self.excl14
         for pairs, label in ((p14_pairs, "1-4 neighbours"), (ex_pairs, "exclusions")):
@@ -504,11 +512,11 @@ def write_inp(path: str, top: str, fep: str | None, *, steps: int, stepsize: flo
 
 
 def water_sphere(outdir: str, radius: float = 15.0, seed: int = 1234, steps: int = 1000, name: str = "c0",
-                 stepsize: float = 1.0) -> Generated:
+                 stepsize: float = 1.0, vdw_rule: int = 1) -> Generated:
     """Config 0: TIP3P sphere, 1 fs, energies every 10 steps."""
     os.makedirs(outdir, exist_ok=True)
     rng = np.random.default_rng(seed)
-    top = Topology(title="water_sphere_%g" % radius, rexcl_o=radius, rwat=radius)
+    top = Topology(title="water_sphere_%g" % radius, rexcl_o=radius, rwat=radius, vdw_rule=vdw_rule)
     _add_waters(top, lattice_waters(radius, rng))
     top.excl = [False] * len(top.x)
     tp = os.path.join(outdir, name + ".top")
@@ -519,7 +527,7 @@ def water_sphere(outdir: str, radius: float = 15.0, seed: int = 1234, steps: int
 
 
 def _fep_file(path: str, types: list[AtomType], iac: list[int], q: list[float], qatoms: list[int],
-              alpha: float = 20.0, charge_scale: float = 0.0, eps_scale: float = 0.5) -> None:
+              alpha: float = 20.0, charge_scale: float = 0.0, eps_scale: float = 0.5, vdw_rule: int = 1) -> None:
     """Two-state FEP file: state 2 scales the Q-atoms' charges by
     charge_scale and their epsilon by eps_scale, soft-core alpha in state 2."""
     L = ["[FEP]", "states 2", "", "[atoms]"]
@@ -532,9 +540,14 @@ def _fep_file(path: str, types: list[AtomType], iac: list[int], q: list[float], 
         t = types[iac[a]]
         for st, scale in ((1, 1.0), (2, eps_scale)):
             nm = "Q%d_%d" % (k + 1, st)
-            aa, bb = lj_sqrt(t.sigma, t.eps * scale)
-            L.append("%-8s %9.2f %8.2f %6.2f %6.2f %9.2f %8.2f %8.4f"
-                     % (nm, aa, bb, 0.0, 0.0, aa / math.sqrt(2), bb / math.sqrt(2), t.mass))
+            if vdw_rule == 2:   # R*, epsilon (not square-rooted: the engine does it), 1-4 at half epsilon
+                rs = 2.0 ** (1.0 / 6.0) * t.sigma / 2.0
+                e = t.eps * scale
+                L.append("%-8s %9.5f %9.5f %6.2f %6.2f %9.5f %9.5f %8.4f" % (nm, rs, e, 0.0, 0.0, rs, e / 2.0, t.mass))
+            else:
+                aa, bb = lj_sqrt(t.sigma, t.eps * scale)
+                L.append("%-8s %9.2f %8.2f %6.2f %6.2f %9.2f %8.2f %8.4f"
+                         % (nm, aa, bb, 0.0, 0.0, aa / math.sqrt(2), bb / math.sqrt(2), t.mass))
         names.append(("Q%d_1" % (k + 1), "Q%d_2" % (k + 1)))
     L += ["", "[change_atoms]"]
     L += ["%d %s %s" % (k + 1, a, b) for k, (a, b) in enumerate(names)]
@@ -569,7 +582,7 @@ def perturbation(base: Generated, name: str, qatoms, charge_scale: float, eps_sc
 
 
 def fep_solute(outdir: str, radius: float = 20.0, seed: int = 1234, steps: int = 5000, name: str = "c1",
-               lambdas=(0.5, 0.5), run_seed: int = 1) -> Generated:
+               lambdas=(0.5, 0.5), run_seed: int = 1, vdw_rule: int = 1) -> Generated:
     """Config 1: 56-atom solute with 8 two-state Q-atoms in a TIP3P sphere,
     2 fs with SHAKE on X-H bonds and water."""
     os.makedirs(outdir, exist_ok=True)
@@ -577,7 +590,7 @@ def fep_solute(outdir: str, radius: float = 20.0, seed: int = 1234, steps: int =
     X, kinds, bonds = random_tree_solute(rng)
     types, iac = _tree_types(kinds)
     n = len(X)
-    top = Topology(title="fep_solute", rexcl_o=radius, rwat=radius, types=types)
+    top = Topology(title="fep_solute", rexcl_o=radius, rwat=radius, types=types, vdw_rule=vdw_rule)
     top.x = [tuple(float(c) for c in p) for p in X]
     top.iac = iac
     top.crg = _solute_charges(rng, kinds)
@@ -603,7 +616,7 @@ def fep_solute(outdir: str, radius: float = 20.0, seed: int = 1234, steps: int =
     top.write(tp)
     fp = os.path.join(outdir, name + ".fep")
     heavy = [i for i in range(n) if kinds[i] >= 0]
-    _fep_file(fp, types, iac, top.crg, heavy[:8])
+    _fep_file(fp, types, iac, top.crg, heavy[:8], vdw_rule=vdw_rule)
     inp = os.path.join(outdir, name + ".inp")
     write_inp(inp, tp, fp, steps=steps, stepsize=2.0, seed=run_seed, lambdas=lambdas, shake_hydrogens=True)
     return Generated(inp, tp, fp, len(top.x), len(waters))

@@ -304,3 +304,54 @@ def test_tuning_changes_only_rounding(synthetic, oracle):
     Eo, EQo = o.energy_vectors()
     assert_energies(Eg, EQg, Eo, EQo)
     assert grad_err(b.gradient(0), o.gradient()) < G_TOL
+
+
+@pytest.fixture(scope="module")
+def arithmetic(tmp_path_factory):
+    """The water sphere and FEP solute written with the arithmetic LJ rule
+    (R*, epsilon) and, beside them, with the geometric rule: the same sigma
+    and epsilon either way."""
+    from q_b200 import synth
+    root = tmp_path_factory.mktemp("arith")
+    out = {}
+    for rule in (1, 2):
+        out[("c0", rule)] = synth.water_sphere(str(root / ("c0_%d" % rule)), radius=15.0, seed=1234, vdw_rule=rule)
+        out[("c1", rule)] = synth.fep_solute(str(root / ("c1_%d" % rule)), seed=1234, vdw_rule=rule)
+    return out
+
+
+@pytest.mark.parametrize("case", ["c0", "c1"])
+def test_arithmetic_rule_matches_oracle(arithmetic, oracle, case):
+    """nonbon2_* (md.f90:8972-10230): every LJ term with R*_i + R*_j and
+    sqrt(eps_i) sqrt(eps_j), soft-core Q-atom terms included, over 20 steps."""
+    s = System.open(arithmetic[(case, 2)].inp, lambdas=(0.3, 0.7) if case == "c1" else None, seed=3)
+    assert s.view.ivdw_rule == 2
+    b = Batch([s], precision=FP64)
+    b.run(20)
+    o = oracle.create(s)
+    o.run(20)
+    sg, Eg, EQg = b.history(0, 0)
+    so, Eo, EQo = o.history(0)
+    assert list(sg) == list(so)
+    for k in range(len(sg)):
+        assert_energies(Eg[k], EQg[k], Eo[k], EQo[k])
+    assert grad_err(b.gradient(0), o.gradient()) < G_TOL
+
+
+def test_arithmetic_rule_equals_geometric_for_like_pairs(arithmetic):
+    """Between atoms of one type both rules give the same pair potential
+    (sigma_ij = sigma either way): the water sphere's O-O van der Waals energy
+    agrees between its arithmetic and geometric topologies to the precision
+    the geometric one prints sqrt(A), sqrt(B) with (2 decimals).  (Unlike types
+    differ by construction: arithmetic means of R* against geometric means of
+    sigma.)"""
+    E = {}
+    for rule in (1, 2):
+        s = System.open(arithmetic[("c0", rule)].inp)
+        b = Batch([s], precision=FP64)
+        b.final_energy()
+        E[rule] = b.energy_vectors(0)[0]
+    k = list(E_NAMES).index("ww_vdw")
+    assert abs(E[2][k] - E[1][k]) <= 2e-3 * abs(E[1][k])
+    k = list(E_NAMES).index("ww_el")
+    assert abs(E[2][k] - E[1][k]) < 1e-9          # same charges; sums differ only in atomic order

@@ -123,6 +123,7 @@ typedef struct qb_sysview {
   /* ---- bonded terms, parameters resolved per term (after shrink_topology) ---- */
   const int *bnd_i, *bnd_j;            const double *bnd_fk, *bnd_b0;
   const int *ang_i, *ang_j, *ang_k;    const double *ang_fk, *ang_th0;
+  const double *ang_ureyfk, *ang_ureyr0; /* Urey-Bradley k and 1-3 r0; zero unless ff_type 3 */
   const int *tor_i, *tor_j, *tor_k, *tor_l;
   const float *tor_fk, *tor_rmult, *tor_deltor, *tor_paths; /* paths already inverted */
   const int *imp_i, *imp_j, *imp_k, *imp_l;
@@ -157,6 +158,7 @@ typedef struct qb_sysview {
   const double *qbnd_Dmz, *qbnd_amz, *qbnd_r0, *qbnd_fk;   /* [n*nstates] */
   const int *qang_i, *qang_j, *qang_k; const unsigned char *qang_on;
   const double *qang_fk, *qang_th0;
+  const double *qang_ureyfk, *qang_ureyr0;  /* [n*nstates]; zero unless ff_type 3 */
   const int *qtor_i, *qtor_j, *qtor_k, *qtor_l; const unsigned char *qtor_on;
   const double *qtor_fk, *qtor_rmult, *qtor_deltor;
   const int *qimp_i, *qimp_j, *qimp_k, *qimp_l; const unsigned char *qimp_on;

@@ -696,6 +696,24 @@ static double angles(qo_state *st, int a0, int a1) {
   return e;
 }
 
+/* urey_bradley (md.f90:904): k (r13 - r0)^2 over the angles' 1-3 pairs with k > 0 */
+static double urey_bradley(qo_state *st, int a0, int a1) {
+  const qb_sysview *s = st->s;
+  double e = 0;
+  for (int a = a0; a < a1; a++) {
+    double fk = s->ang_ureyfk[a];
+    if (!(fk > 0.)) continue;
+    int i = s->ang_i[a], k = s->ang_k[a];
+    double rik[3] = {X(k, 0) - X(i, 0), X(k, 1) - X(i, 1), X(k, 2) - X(i, 2)};
+    double dik = sqrt(rik[0] * rik[0] + rik[1] * rik[1] + rik[2] * rik[2]);
+    double ru = dik - s->ang_ureyr0[a];
+    e += fk * ru * ru;
+    double du = 2 * fk * ru / dik;
+    for (int c = 0; c < 3; c++) { D(k, c) += du * rik[c]; D(i, c) -= du * rik[c]; }
+  }
+  return e;
+}
+
 /* dihedral geometry shared by torsion (14793), improper (1677),
  * improper2 (1789): phi and the 12 gradient components */
 static double dihedral(qo_state *st, int i, int j, int k, int l, double dp[12]) {
@@ -826,6 +844,13 @@ static void qbonded(qo_state *st, int ss) {
       D(i, c) += dv * di;
       D(k, c) += dv * dk;
       D(j, c) -= dv * (di + dk);
+    }
+    /* qurey_bradley (md.f90:13992): energy only, its gradient is never applied */
+    double ufk = s->qang_ureyfk[a * S + ss];
+    if (ufk != 0.) {
+      double rik[3] = {X(k, 0) - X(i, 0), X(k, 1) - X(i, 1), X(k, 2) - X(i, 2)};
+      double ru = sqrt(rik[0] * rik[0] + rik[1] * rik[1] + rik[2] * rik[2]) - s->qang_ureyr0[a * S + ss];
+      EQV(ss, QB_EQ_ANGLE) += ufk * ru * ru;
     }
   }
   double dp[12], pi = fpi();
@@ -1120,6 +1145,10 @@ static void pot_energy(qo_state *st) {
   st->E[QB_E_W_BOND] = bonds(st, s->nbonds_solute, s->nbonds);
   st->E[QB_E_P_ANGLE] = angles(st, 0, s->nangles_solute);
   st->E[QB_E_W_ANGLE] = angles(st, s->nangles_solute, s->nangles);
+  if (s->ff_type == 3) {
+    st->E[QB_E_P_ANGLE] += urey_bradley(st, 0, s->nangles_solute);
+    st->E[QB_E_W_ANGLE] += urey_bradley(st, s->nangles_solute, s->nangles);
+  }
   st->E[QB_E_P_TORSION] = torsions(st, 0, s->ntors_solute);
   st->E[QB_E_W_TORSION] = torsions(st, s->ntors_solute, s->ntors);
   st->E[QB_E_P_IMPROPER] = impropers(st, 0, s->nimps_solute);

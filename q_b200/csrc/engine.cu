@@ -396,11 +396,11 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   std::vector<int8_t> qconn;
   std::vector<int4> qq;
   std::vector<int2> bij; std::vector<double2> bpar;
-  std::vector<int4> aijk; std::vector<double2> apar;
+  std::vector<int4> aijk; std::vector<double2> apar, aub;
   std::vector<int4> tijkl; std::vector<float4> tpar;
   std::vector<int4> iijkl; std::vector<float2> ipar;
   std::vector<int2> qbij; std::vector<uint8_t> qb_on; std::vector<double4> qbpar;
-  std::vector<int4> qaijk; std::vector<uint8_t> qa_on; std::vector<double2> qapar;
+  std::vector<int4> qaijk; std::vector<uint8_t> qa_on; std::vector<double2> qapar, qaub;
   std::vector<int4> qtijkl; std::vector<uint8_t> qt_on; std::vector<double4> qtpar;
   std::vector<int4> qiijkl; std::vector<uint8_t> qi_on; std::vector<double2> qipar;
   std::vector<int> sh_first, sh_n, sh_sys; std::vector<int2> sh_ij; std::vector<double> sh_d2;
@@ -521,6 +521,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     for (int k = 0; k < V.nangles; k++) {
       aijk.push_back(make_int4(aoff + V.ang_i[k], aoff + V.ang_j[k], aoff + V.ang_k[k], 0));
       apar.push_back(make_double2(V.ang_fk[k], V.ang_th0[k]));
+      aub.push_back(make_double2(V.ang_ureyfk[k], V.ang_ureyr0[k]));
     }
     S.t_off = (int)tijkl.size(); S.nt = V.ntors; S.nt_sol = V.ntors_solute;
     for (int k = 0; k < V.ntors; k++) {
@@ -551,6 +552,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
         bool on = st < NSt && V.qang_on[k * NSt + st];
         qa_on.push_back(on);
         qapar.push_back(on ? make_double2(V.qang_fk[k * NSt + st], V.qang_th0[k * NSt + st]) : make_double2(0, 0));
+        qaub.push_back(on ? make_double2(V.qang_ureyfk[k * NSt + st], V.qang_ureyr0[k * NSt + st]) : make_double2(0, 0));
       }
     }
     S.qt_off = (int)qtijkl.size(); S.nqt = V.nqtor;
@@ -747,10 +749,10 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   P.iqseq = dev_upload(iqseq, o); P.qcrg = dev_upload(qcrg, o); P.qiac = dev_upload(qiac, o);
   P.qavdw = dev_upload(qavdw, o); P.qbvdw = dev_upload(qbvdw, o); P.sc = dev_upload(sc, o);
   P.qconn = dev_upload(qconn, o); P.qq = dev_upload(qq, o); P.qq_el = dev_upload(qq_el, o);
-  P.bij = dev_upload(bij, o); P.bpar = dev_upload(bpar, o); P.aijk = dev_upload(aijk, o); P.apar = dev_upload(apar, o);
+  P.bij = dev_upload(bij, o); P.bpar = dev_upload(bpar, o); P.aijk = dev_upload(aijk, o); P.apar = dev_upload(apar, o); P.aub = dev_upload(aub, o);
   P.tijkl = dev_upload(tijkl, o); P.tpar = dev_upload(tpar, o); P.iijkl = dev_upload(iijkl, o); P.ipar = dev_upload(ipar, o);
   P.qbij = dev_upload(qbij, o); P.qb_on = dev_upload(qb_on, o); P.qbpar = dev_upload(qbpar, o);
-  P.qaijk = dev_upload(qaijk, o); P.qa_on = dev_upload(qa_on, o); P.qapar = dev_upload(qapar, o);
+  P.qaijk = dev_upload(qaijk, o); P.qa_on = dev_upload(qa_on, o); P.qapar = dev_upload(qapar, o); P.qaub = dev_upload(qaub, o);
   P.qtijkl = dev_upload(qtijkl, o); P.qt_on = dev_upload(qt_on, o); P.qtpar = dev_upload(qtpar, o);
   P.qiijkl = dev_upload(qiijkl, o); P.qi_on = dev_upload(qi_on, o); P.qipar = dev_upload(qipar, o);
   P.sh_first = dev_upload(sh_first, o); P.sh_n = dev_upload(sh_n, o); P.sh_sys = dev_upload(sh_sys, o);

@@ -105,11 +105,11 @@ struct DevPtrs {
   double *qq_el;
   // bonded terms (global atom indices)
   int2 *bij; double2 *bpar;               // fk, b0
-  int4 *aijk; double2 *apar;              // fk, th0
+  int4 *aijk; double2 *apar, *aub;        // fk, th0; Urey-Bradley k, r0
   int4 *tijkl; float4 *tpar;              // fk, rmult, deltor, paths
   int4 *iijkl; float2 *ipar;              // fk, imp0
   int2 *qbij; uint8_t *qb_on; double4 *qbpar;           // [term*MAXS+st] Dmz, amz, r0, fk
-  int4 *qaijk; uint8_t *qa_on; double2 *qapar;          // fk, th0
+  int4 *qaijk; uint8_t *qa_on; double2 *qapar, *qaub;   // fk, th0; Urey-Bradley k, r0
   int4 *qtijkl; uint8_t *qt_on; double4 *qtpar;         // fk, rmult, deltor
   int4 *qiijkl; uint8_t *qi_on; double2 *qipar;         // fk, imp0
   // shake

@@ -1504,6 +1504,18 @@ __device__ __forceinline__ void bonded_body(DevPtrs &P, int bx, int s, int gx) {
       atomic_add3(P.d, t.x, dv * di[0], dv * di[1], dv * di[2]);
       atomic_add3(P.d, t.z, dv * dk[0], dv * dk[1], dv * dk[2]);
       atomic_add3(P.d, t.y, -dv * (di[0] + dk[0]), -dv * (di[1] + dk[1]), -dv * (di[2] + dk[2]));
+      if (S.ff_type == 3) {  // urey_bradley (md.f90:904): harmonic 1-3 distance, k r^2 without 1/2
+        double2 ub = P.aub[S.a_off + a];
+        if (ub.x > 0.) {
+          double rik[3] = {xk.x - xi.x, xk.y - xi.y, xk.z - xi.z};
+          double dik = sqrt(rik[0] * rik[0] + rik[1] * rik[1] + rik[2] * rik[2]);
+          double ru = dik - ub.y;
+          e[a < S.na_sol ? 1 : 5] += ub.x * ru * ru;
+          double du = 2. * ub.x * ru / dik;
+          atomic_add3(P.d, t.z, du * rik[0], du * rik[1], du * rik[2]);
+          atomic_add3(P.d, t.x, -du * rik[0], -du * rik[1], -du * rik[2]);
+        }
+      }
     } else if (k < S.nb + S.na + S.nt) {
       int t = k - S.nb - S.na;
       int4 q = P.tijkl[S.t_off + t];
@@ -1594,6 +1606,15 @@ __device__ __forceinline__ void qbonded_body(DevPtrs &P, int s) {
       atomic_add3(P.d, t.x, dv * di[0], dv * di[1], dv * di[2]);
       atomic_add3(P.d, t.z, dv * dk[0], dv * dk[1], dv * dk[2]);
       atomic_add3(P.d, t.y, -dv * (di[0] + dk[0]), -dv * (di[1] + dk[1]), -dv * (di[2] + dk[2]));
+      // qurey_bradley (md.f90:13992): adds the 1-3 energy to the state's
+      // angle energy; the reference never applies its gradient, so neither
+      // does this
+      double2 ub = P.qaub[(S.qa_off + a) * MAXS + st];
+      if (ub.x != 0.) {
+        double rik[3] = {xk.x - xi.x, xk.y - xi.y, xk.z - xi.z};
+        double ru = sqrt(rik[0] * rik[0] + rik[1] * rik[1] + rik[2] * rik[2]) - ub.y;
+        atomicAdd(&eq[QB_EQ_ANGLE], ub.x * ru * ru);
+      }
     } else if (k < n3) {
       int t = (k - n2) / NS, st = (k - n2) % NS;
       if (!P.qt_on[(S.qt_off + t) * MAXS + st]) continue;

@@ -669,12 +669,18 @@ void parse_topology(const std::string &path, Topology &t) {
   int nangcod = (int)r.int1();
   t.ang_fk.assign(nangcod, 0.0);
   t.ang_th0.assign(nangcod, 0.0);
+  t.ang_ureyfk.assign(nangcod, 0.0);
+  t.ang_ureyr0.assign(nangcod, 0.0);
+  // "code fk theta0 [ureyfk [ureyr0]]": the Urey-Bradley pair is optional
+  // and stays zero when the line ends first (topo.f90:712-726)
   for (int i = 0; i < nangcod; i++) {
     auto v = line_values(r.line());
     double fk, a0;
     if (v.size() < 3 || !to_real(v[1], fk) || !to_real(v[2], a0)) r.err("angle parameters");
     t.ang_fk[i] = fk;
     t.ang_th0[i] = a0;
+    if (v.size() > 3 && !to_real(v[3], t.ang_ureyfk[i])) r.err("angle parameters");
+    if (v.size() > 4 && !to_real(v[4], t.ang_ureyr0[i])) r.err("angle parameters");
   }
   // 7. torsions
   int nt, nts;
@@ -1057,9 +1063,11 @@ void read_fep(const std::string &path, const Topology &t, Fep &f) {
     f.qanglib.assign(maxe, {0, 0, 0, 0});
     for (auto &l : at) {
       auto v = line_values(l);
-      long j; double fk, a0;
+      long j; double fk, a0, ufk = 0, ur0 = 0;
       if (v.size() < 3 || !to_int(v[0], j) || j < 1 || !to_real(v[1], fk) || !to_real(v[2], a0)) bad("angle_types: " + l);
-      f.qanglib[j - 1] = {fk, deg2rad * a0, 0, 0};
+      // optional Urey-Bradley force constant and 1-3 distance (qatom.f90:1213-1236)
+      if ((v.size() > 3 && !to_real(v[3], ufk)) || (v.size() > 4 && !to_real(v[4], ur0))) bad("angle_types: " + l);
+      f.qanglib[j - 1] = {fk, deg2rad * a0, ufk, ur0};
     }
     for (auto &l : lines("change_angles")) {
       auto v = line_values(l);

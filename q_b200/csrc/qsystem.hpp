@@ -73,6 +73,7 @@ struct Topology {
   std::vector<double> bond_fk, bond_b0;
   std::vector<Angle> ang; int nangles_solute = 0;
   std::vector<double> ang_fk, ang_th0;
+  std::vector<double> ang_ureyfk, ang_ureyr0;   // optional Urey-Bradley columns (0 when absent)
   std::vector<Tors> tor; int ntors_solute = 0;
   std::vector<float> tor_fk, tor_rmult, tor_deltor, tor_paths;
   std::vector<Tors> imp; int nimps_solute = 0; int imp_type = 1;
@@ -163,11 +164,11 @@ struct System {
   std::vector<int> qbnd_i, qbnd_j, qang_i, qang_j, qang_k;
   std::vector<int> qtor_i, qtor_j, qtor_k, qtor_l, qimp_i, qimp_j, qimp_k, qimp_l;
   std::vector<unsigned char> qbnd_on, qang_on, qtor_on, qimp_on;
-  std::vector<double> qbnd_Dmz, qbnd_amz, qbnd_r0, qbnd_fk, qang_fk, qang_th0;
+  std::vector<double> qbnd_Dmz, qbnd_amz, qbnd_r0, qbnd_fk, qang_fk, qang_th0, qang_ureyfk, qang_ureyr0;
   std::vector<double> qtor_fk, qtor_rmult, qtor_deltor, qimp_fk, qimp_imp0;
   // resolved bonded terms (after shrink_topology)
   std::vector<int> bi, bj; std::vector<double> bfk, bb0; int nb_solute = 0;
-  std::vector<int> ai, aj, ak; std::vector<double> afk, ath0; int na_solute = 0;
+  std::vector<int> ai, aj, ak; std::vector<double> afk, ath0, aufk, aur0; int na_solute = 0;
   std::vector<int> ti, tj, tk, tl; std::vector<float> tfk, trm, tdel, tpaths; int nt_solute = 0;
   std::vector<int> ii, ij, ik, il; std::vector<float> ifk, iimp0; int ni_solute = 0;
   // shake

@@ -90,7 +90,7 @@ void prepare(System &s) {
       for (int k = 0; k < 3; k++) ty.bvdw[k] = std::sqrt(std::fabs(ty.bvdw[k]));
   if (t.solvent_type != 0 && t.nat_pro > t.nat_solute)
     fail(QB_ERR_UNSUPPORTED, "only SPC-type 3-site water is supported (solvent_type 0)");
-  if (t.ff_type == 3) fail(QB_ERR_UNSUPPORTED, "CHARMM force fields (Urey-Bradley) are not supported");
+  if (t.ff_type < 1 || t.ff_type > 3) fail(QB_ERR_UNSUPPORTED, "unknown force-field type in the topology");
   s.natom = t.nat_pro;
   s.nwat = (s.natom - t.nat_solute) / 3;
   const int N = s.natom, NS = t.nat_solute;
@@ -174,9 +174,21 @@ void prepare(System &s) {
         if (((tt.i == q.i && tt.j == q.j && tt.k == q.k && tt.l == q.l) ||
              (tt.i == q.l && tt.j == q.k && tt.k == q.j && tt.l == q.i)) && tt.cod != 0)
           tt.cod = 0;
-    for (auto &im : t.imp)
-      for (auto &q : f.qimp)
-        if (((im.j == q.j && im.k == q.k) || (im.j == q.k && im.k == q.j)) && im.cod != 0) im.cod = 0;
+    if (t.ff_type == 3) {
+      // CHARMM: an improper goes when one of its ends is an end of the Q
+      // improper and its two centre atoms are both among the Q improper's
+      // four atoms (md.f90:1574-1594)
+      for (auto &im : t.imp)
+        for (auto &q : f.qimp) {
+          auto in4 = [&](int a) { return a == q.i || a == q.j || a == q.k || a == q.l; };
+          bool end = im.i == q.i || im.i == q.l || im.l == q.i || im.l == q.l;
+          if (end && in4(im.j) && in4(im.k) && im.cod != 0) im.cod = 0;
+        }
+    } else {
+      for (auto &im : t.imp)
+        for (auto &q : f.qimp)
+          if (((im.j == q.j && im.k == q.k) || (im.j == q.k && im.k == q.j)) && im.cod != 0) im.cod = 0;
+    }
     // special exclusions that hold in every state go to the exclusion lists
     for (auto &e : f.exspec) {
       if (e.i < 0 || e.i >= N || e.j < 0 || e.j >= N) fail(QB_ERR_PARSE, "invalid special exclusion data");
@@ -469,8 +481,14 @@ void prepare(System &s) {
   s.bi.clear(); s.bj.clear(); s.bfk.clear(); s.bb0.clear();
   for (auto &b : t.bnd) { s.bi.push_back(b.i); s.bj.push_back(b.j); s.bfk.push_back(t.bond_fk[b.cod - 1]); s.bb0.push_back(t.bond_b0[b.cod - 1]); }
   s.nb_solute = t.nbonds_solute;
-  s.ai.clear(); s.aj.clear(); s.ak.clear(); s.afk.clear(); s.ath0.clear();
-  for (auto &a : t.ang) { s.ai.push_back(a.i); s.aj.push_back(a.j); s.ak.push_back(a.k); s.afk.push_back(t.ang_fk[a.cod - 1]); s.ath0.push_back(t.ang_th0[a.cod - 1]); }
+  s.ai.clear(); s.aj.clear(); s.ak.clear(); s.afk.clear(); s.ath0.clear(); s.aufk.clear(); s.aur0.clear();
+  // Urey-Bradley terms act only under the CHARMM force field (md.f90:13498-13504)
+  const bool ub = t.ff_type == 3;
+  for (auto &a : t.ang) {
+    s.ai.push_back(a.i); s.aj.push_back(a.j); s.ak.push_back(a.k);
+    s.afk.push_back(t.ang_fk[a.cod - 1]); s.ath0.push_back(t.ang_th0[a.cod - 1]);
+    s.aufk.push_back(ub ? t.ang_ureyfk[a.cod - 1] : 0.0); s.aur0.push_back(ub ? t.ang_ureyr0[a.cod - 1] : 0.0);
+  }
   s.na_solute = t.nangles_solute;
   s.ti.clear(); s.tj.clear(); s.tk.clear(); s.tl.clear(); s.tfk.clear(); s.trm.clear(); s.tdel.clear(); s.tpaths.clear();
   for (auto &q : t.tor) {
@@ -509,10 +527,15 @@ void prepare(System &s) {
   for (auto &q : f.qang) { s.qang_i.push_back(q.i); s.qang_j.push_back(q.j); s.qang_k.push_back(q.k); }
   size_t nqa = f.qang.size();
   s.qang_on.assign(nqa * S, 0); s.qang_fk.assign(nqa * S, 0); s.qang_th0.assign(nqa * S, 0);
+  s.qang_ureyfk.assign(nqa * S, 0); s.qang_ureyr0.assign(nqa * S, 0);
   for (size_t k = 0; k < nqa; k++)
     for (int st = 0; st < S; st++) {
       int c = f.qang[k].cod[st];
-      if (c > 0) { s.qang_on[k * S + st] = 1; s.qang_fk[k * S + st] = f.qanglib[c - 1].fk; s.qang_th0[k * S + st] = f.qanglib[c - 1].ang0; }
+      if (c > 0) {
+        auto &L = f.qanglib[c - 1];
+        s.qang_on[k * S + st] = 1; s.qang_fk[k * S + st] = L.fk; s.qang_th0[k * S + st] = L.ang0;
+        if (ub) { s.qang_ureyfk[k * S + st] = L.ureyfk; s.qang_ureyr0[k * S + st] = L.ureyr0; }
+      }
     }
   auto flat4 = [&](std::vector<Fep::QTor> &L, std::vector<int> &I, std::vector<int> &J, std::vector<int> &K,
                    std::vector<int> &Lx, std::vector<unsigned char> &on) {
@@ -652,6 +675,7 @@ void System::fill_view(qb_sysview *v) const {
   v->istart_mol = t.istart_mol.data();
   v->bnd_i = bi.data(); v->bnd_j = bj.data(); v->bnd_fk = bfk.data(); v->bnd_b0 = bb0.data();
   v->ang_i = ai.data(); v->ang_j = aj.data(); v->ang_k = ak.data(); v->ang_fk = afk.data(); v->ang_th0 = ath0.data();
+  v->ang_ureyfk = aufk.data(); v->ang_ureyr0 = aur0.data();
   v->tor_i = ti.data(); v->tor_j = tj.data(); v->tor_k = tk.data(); v->tor_l = tl.data();
   v->tor_fk = tfk.data(); v->tor_rmult = trm.data(); v->tor_deltor = tdel.data(); v->tor_paths = tpaths.data();
   v->imp_i = ii.data(); v->imp_j = ij.data(); v->imp_k = ik.data(); v->imp_l = il.data();
@@ -674,6 +698,7 @@ void System::fill_view(qb_sysview *v) const {
   v->qbnd_Dmz = qbnd_Dmz.data(); v->qbnd_amz = qbnd_amz.data(); v->qbnd_r0 = qbnd_r0.data(); v->qbnd_fk = qbnd_fk.data();
   v->qang_i = qang_i.data(); v->qang_j = qang_j.data(); v->qang_k = qang_k.data(); v->qang_on = qang_on.data();
   v->qang_fk = qang_fk.data(); v->qang_th0 = qang_th0.data();
+  v->qang_ureyfk = qang_ureyfk.data(); v->qang_ureyr0 = qang_ureyr0.data();
   v->qtor_i = qtor_i.data(); v->qtor_j = qtor_j.data(); v->qtor_k = qtor_k.data(); v->qtor_l = qtor_l.data();
   v->qtor_on = qtor_on.data(); v->qtor_fk = qtor_fk.data(); v->qtor_rmult = qtor_rmult.data(); v->qtor_deltor = qtor_deltor.data();
   v->qimp_i = qimp_i.data(); v->qimp_j = qimp_j.data(); v->qimp_k = qimp_k.data(); v->qimp_l = qimp_l.data();

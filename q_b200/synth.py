@@ -75,7 +75,7 @@ class Topology:
     bonds: list = field(default_factory=list)        # (i, j, code)
     bond_lib: list = field(default_factory=list)     # (fk, b0)
     angles: list = field(default_factory=list)       # (i, j, k, code)
-    angle_lib: list = field(default_factory=list)    # (fk, th0_deg)
+    angle_lib: list = field(default_factory=list)    # (fk, th0_deg[, urey_fk, urey_r0])
     tors: list = field(default_factory=list)         # (i, j, k, l, code)
     tor_lib: list = field(default_factory=list)      # (fk, rmult, delta_deg, paths)
     imps: list = field(default_factory=list)
@@ -95,6 +95,7 @@ class Topology:
     rwat: float = 20.0
     excl: list = field(default_factory=list)
     vdw_rule: int = 1                                # 1 geometric, 2 arithmetic
+    ff_type: int = 2                                 # 1 GROMOS, 2 AMBER, 3 CHARMM (Urey-Bradley, harmonic impropers)
 
     # ----------------------------------------------------------- writer
     def write(self, path: str) -> None:
@@ -106,7 +107,7 @@ class Topology:
         L.append("DATE       synthetic")
         L.append("VERSION     6.01")
         L.append("FORCEFIELD synthetic-geometric")
-        L.append("FF_TYPE    2")
+        L.append("FF_TYPE    %d" % self.ff_type)
         L.append("PRM_FILE   none")
         L.append("END        of header")
         L.append("%8d%8d = Total no. of atoms, no. of solute atoms. Coordinates: (2*3 per line)" % (n, ns))
@@ -128,8 +129,9 @@ class Topology:
         for k in range(0, len(self.angles), 3):
             L.append(" ".join("%5d %5d %5d %3d" % (i + 1, j + 1, kk + 1, c) for i, j, kk, c in self.angles[k:k + 3]))
         L.append("%8d = No. of angle codes. Parameters:" % len(self.angle_lib))
-        for k, (fk, th) in enumerate(self.angle_lib):
-            L.append("%5d%9.3f %9.3f %9.3f %11.5f" % (k + 1, fk, th, 0.0, 0.0))
+        for k, a in enumerate(self.angle_lib):
+            fk, th, ufk, ur0 = (tuple(a) + (0.0, 0.0))[:4]
+            L.append("%5d%9.3f %9.3f %9.3f %11.5f" % (k + 1, fk, th, ufk, ur0))
         L.append("%8d%8d = No. of torsions, solute torsions. i - j - k - l - icode: (2 per line)"
                  % (len(self.tors), self.ntors_solute))
         for k in range(0, len(self.tors), 2):
@@ -143,7 +145,8 @@ class Topology:
         for k in range(0, len(self.imps), 2):
             L.append(" ".join("%5d %5d %5d %5d %3d" % (a + 1, b + 1, c + 1, d + 1, e)
                               for a, b, c, d, e in self.imps[k:k + 2]))
-        L.append("%8d%8d = No. of improper codes, type (1=harmonic,2=periodic). Parameters:" % (len(self.imp_lib), 2))
+        L.append("%8d%8d = No. of improper codes, type (1=harmonic,2=periodic). Parameters:"
+                 % (len(self.imp_lib), 2 if self.ff_type == 2 else 1))
         for k, (fk, i0) in enumerate(self.imp_lib):
             L.append("%5d%10.3f %10.3f" % (k + 1, fk, i0))
         L.append("%8d = No. of atomic charges" % n)
@@ -313,6 +316,31 @@ def _finish_solute_lists(top: Topology, bonds: list[tuple[int, int]], n: int) ->
                     if p not in ex:
                         p14.add(p)
     top.excl14 = (sorted(ex), sorted(p14))
+
+
+def dihedral_deg(xi, xj, xk, xl) -> float:
+    """The dihedral i-j-k-l in degrees with Q's sign convention (md.f90
+    torsion/improper: normals rji x rjk and rkl x rjk, signed by rjk)."""
+    rji, rjk, rkl = xi - xj, xk - xj, xl - xk
+    nj, nk = np.cross(rji, rjk), -np.cross(rjk, rkl)
+    c = float(nj @ nk / (np.linalg.norm(nj) * np.linalg.norm(nk)))
+    phi = math.degrees(math.acos(max(-1.0, min(1.0, c))))
+    return -phi if float(rjk @ np.cross(nj, nk)) < 0 else phi
+
+
+def charmm_terms(top: Topology, ub_fk: float = 25.0, imp_fk: float = 20.0) -> None:
+    """Turn a solute's terms into CHARMM ones: every solute angle gets a
+    Urey-Bradley 1-3 term whose r0 is 3% longer than the 1-3 distance of the
+    generated geometry, and the impropers become harmonic about the
+    geometry's own improper angle."""
+    top.ff_type = 3
+    X = np.asarray(top.x, dtype=float)
+    for i, j, k, c in top.angles[:top.nangles_solute]:
+        fk, th = top.angle_lib[c - 1][:2]
+        r13 = float(np.linalg.norm(X[k] - X[i]))
+        top.angle_lib[c - 1] = (fk, th, ub_fk, round(1.03 * r13, 4))
+    for i, j, k, l, c in top.imps[:top.nimps_solute]:
+        top.imp_lib[c - 1] = (imp_fk, round(dihedral_deg(X[i], X[j], X[k], X[l]), 3))
 
 
 def _angle(a, b, c) -> float:
@@ -526,10 +554,73 @@ def water_sphere(outdir: str, radius: float = 15.0, seed: int = 1234, steps: int
     return Generated(inp, tp, None, len(top.x), (len(top.x)) // 3)
 
 
+def _q_bonded(top: Topology, qatoms: list[int]) -> list[str]:
+    """FEP sections redefining the topology's bonds, angles, torsions and
+    impropers that lie wholly among the Q atoms: state 1 keeps the topology's
+    parameters, state 2 changes them (the first bond becomes a Morse bond of
+    the same curvature, the last torsion is absent).  Impropers centred on a
+    Q atom are redefined too, harmonic
+    about the geometry's own improper angle in both states; under CHARMM the
+    angle types carry the topology's Urey-Bradley columns, halved in state 2."""
+    qs = set(qatoms)
+    X = np.asarray(top.x, dtype=float)
+    L = []
+    bonds = [(i, j, c) for i, j, c in top.bonds[:top.nbonds_solute] if i in qs and j in qs]
+    if bonds:
+        L += ["[bond_types]"]
+        for n, (i, j, c) in enumerate(bonds):
+            fk, b0 = top.bond_lib[c - 1]
+            L.append("%d %8.2f %8.4f" % (2 * n + 1, fk, b0))
+            if n == 0:
+                amz = 2.0
+                L.append("%d %8.3f %6.3f %8.4f" % (2 * n + 2, fk / (2 * amz * amz), amz, b0 + 0.03))
+            else:
+                L.append("%d %8.2f %8.4f" % (2 * n + 2, 0.8 * fk, b0 + 0.02))
+        L += ["", "[change_bonds]"]
+        L += ["%d %d %d %d" % (i + 1, j + 1, 2 * n + 1, 2 * n + 2) for n, (i, j, c) in enumerate(bonds)]
+        L += [""]
+    angles = [(i, j, k, c) for i, j, k, c in top.angles[:top.nangles_solute] if i in qs and j in qs and k in qs]
+    if angles:
+        L += ["[angle_types]"]
+        for n, (i, j, k, c) in enumerate(angles):
+            fk, th, ufk, ur0 = (tuple(top.angle_lib[c - 1]) + (0.0, 0.0))[:4]
+            for st, (f, t, u, r) in enumerate(((fk, th, ufk, ur0), (0.7 * fk, th + 4.0, 0.5 * ufk, ur0 + 0.05))):
+                row = "%d %8.3f %8.3f" % (2 * n + 1 + st, f, t)
+                L.append(row + (" %8.3f %8.4f" % (u, r) if top.ff_type == 3 else ""))
+        L += ["", "[change_angles]"]
+        L += ["%d %d %d %d %d" % (i + 1, j + 1, k + 1, 2 * n + 1, 2 * n + 2) for n, (i, j, k, c) in enumerate(angles)]
+        L += [""]
+    tors = [t for t in top.tors[:top.ntors_solute] if all(a in qs for a in t[:4])]
+    if tors:
+        L += ["[torsion_types]"]
+        for n, (i, j, k, l, c) in enumerate(tors):
+            fk, rm, dl, pa = top.tor_lib[c - 1]
+            L.append("%d %8.3f %6.1f %8.2f" % (2 * n + 1, fk / pa, rm, dl))
+            L.append("%d %8.3f %6.1f %8.2f" % (2 * n + 2, 0.5 * fk / pa, rm, dl))
+        L += ["", "[change_torsions]"]
+        L += ["%d %d %d %d %d %d" % (i + 1, j + 1, k + 1, l + 1, 2 * n + 1, 0 if n == len(tors) - 1 else 2 * n + 2)
+              for n, (i, j, k, l, c) in enumerate(tors)]
+        L += [""]
+    imps = [t for t in top.imps[:top.nimps_solute] if t[1] in qs]
+    if imps:
+        L += ["[improper_types]"]
+        for n, (i, j, k, l, c) in enumerate(imps):
+            phi = round(dihedral_deg(X[i], X[j], X[k], X[l]), 3)
+            L += ["%d %8.3f %8.3f" % (2 * n + 1, 15.0, phi), "%d %8.3f %8.3f" % (2 * n + 2, 25.0, phi)]
+        L += ["", "[change_impropers]"]
+        L += ["%d %d %d %d %d %d" % (i + 1, j + 1, k + 1, l + 1, 2 * n + 1, 2 * n + 2)
+              for n, (i, j, k, l, c) in enumerate(imps)]
+        L += [""]
+    return L
+
+
 def _fep_file(path: str, types: list[AtomType], iac: list[int], q: list[float], qatoms: list[int],
-              alpha: float = 20.0, charge_scale: float = 0.0, eps_scale: float = 0.5, vdw_rule: int = 1) -> None:
+              alpha: float = 20.0, charge_scale: float = 0.0, eps_scale: float = 0.5, vdw_rule: int = 1,
+              top: Topology | None = None) -> None:
     """Two-state FEP file: state 2 scales the Q-atoms' charges by
-    charge_scale and their epsilon by eps_scale, soft-core alpha in state 2."""
+    charge_scale and their epsilon by eps_scale, soft-core alpha in state 2.
+    Given the topology, the bonded terms among the Q atoms are redefined too
+    (_q_bonded)."""
     L = ["[FEP]", "states 2", "", "[atoms]"]
     L += ["%d %d" % (k + 1, a + 1) for k, a in enumerate(qatoms)]
     L += ["", "[change_charges]"]
@@ -553,6 +644,8 @@ def _fep_file(path: str, types: list[AtomType], iac: list[int], q: list[float], 
     L += ["%d %s %s" % (k + 1, a, b) for k, (a, b) in enumerate(names)]
     L += ["", "[softcore]"]
     L += ["%d %g %g" % (k + 1, 0.0, alpha) for k in range(len(qatoms))]
+    if top is not None:
+        L += [""] + _q_bonded(top, qatoms)
     with open(path, "w") as f:
         f.write("\n".join(L) + "\n")
 
@@ -582,9 +675,12 @@ def perturbation(base: Generated, name: str, qatoms, charge_scale: float, eps_sc
 
 
 def fep_solute(outdir: str, radius: float = 20.0, seed: int = 1234, steps: int = 5000, name: str = "c1",
-               lambdas=(0.5, 0.5), run_seed: int = 1, vdw_rule: int = 1) -> Generated:
+               lambdas=(0.5, 0.5), run_seed: int = 1, vdw_rule: int = 1, ff_type: int = 2,
+               q_bonded: bool = False, ub_fk: float = 25.0) -> Generated:
     """Config 1: 56-atom solute with 8 two-state Q-atoms in a TIP3P sphere,
-    2 fs with SHAKE on X-H bonds and water."""
+    2 fs with SHAKE on X-H bonds and water.  ff_type 3 writes it as a CHARMM
+    topology (charmm_terms, Urey-Bradley constant ub_fk); q_bonded redefines the bonded terms among the
+    Q atoms in the FEP file."""
     os.makedirs(outdir, exist_ok=True)
     rng = np.random.default_rng(seed)
     X, kinds, bonds = random_tree_solute(rng)
@@ -612,11 +708,13 @@ def fep_solute(outdir: str, radius: float = 20.0, seed: int = 1234, steps: int =
     waters = lattice_waters(radius, rng, avoid=X)
     _add_waters(top, waters)
     top.excl = [False] * len(top.x)
+    if ff_type == 3:
+        charmm_terms(top, ub_fk=ub_fk)
     tp = os.path.join(outdir, name + ".top")
     top.write(tp)
     fp = os.path.join(outdir, name + ".fep")
     heavy = [i for i in range(n) if kinds[i] >= 0]
-    _fep_file(fp, types, iac, top.crg, heavy[:8], vdw_rule=vdw_rule)
+    _fep_file(fp, types, iac, top.crg, heavy[:8], vdw_rule=vdw_rule, top=top if q_bonded else None)
     inp = os.path.join(outdir, name + ".inp")
     write_inp(inp, tp, fp, steps=steps, stepsize=2.0, seed=run_seed, lambdas=lambdas, shake_hydrogens=True)
     return Generated(inp, tp, fp, len(top.x), len(waters))

@@ -355,3 +355,53 @@ def test_arithmetic_rule_equals_geometric_for_like_pairs(arithmetic):
     assert abs(E[2][k] - E[1][k]) <= 2e-3 * abs(E[1][k])
     k = list(E_NAMES).index("ww_el")
     assert abs(E[2][k] - E[1][k]) < 1e-9          # same charges; sums differ only in atomic order
+
+
+@pytest.fixture(scope="module")
+def charmm_pair(tmp_path_factory):
+    """The FEP solute as a CHARMM topology (Urey-Bradley 1-3 terms,
+    harmonic impropers) and as its AMBER twin, both with the bonded terms
+    among the Q atoms redefined per state in the FEP file (Q bonds, one of
+    them Morse in state 2; Q angles, with Urey-Bradley columns under CHARMM;
+    Q torsions; Q impropers)."""
+    from q_b200 import synth
+    root = tmp_path_factory.mktemp("charmm")
+    return {ff: synth.fep_solute(str(root / ("ff%d" % ff)), seed=1234, ff_type=ff, q_bonded=True)
+            for ff in (3, 2)}
+
+
+def _worst_atoms(g, ref, n=5):
+    d = np.linalg.norm((g - ref).reshape(-1, 3), axis=1)
+    return [(int(a), float(d[a])) for a in np.argsort(-d)[:n]]
+
+
+def test_charmm_and_q_bonded_match_oracle(charmm_pair, oracle):
+    """urey_bradley (md.f90:904), qurey_bradley (13992, energy only),
+    qbond with Morse and harmonic types (14060), qangle (13896), qtorsion
+    (14262), qimproper (14117) and the CHARMM improper set: a CHARMM system
+    and an AMBER one in one batch, each against the oracle at step 0 and
+    over 20 steps of dynamics."""
+    systems = [System.open(charmm_pair[ff].inp, lambdas=(0.3, 0.7), seed=3) for ff in (3, 2)]
+    assert [s.view.ff_type for s in systems] == [3, 2]
+    assert all(s.view.nqbond and s.view.nqangle and s.view.nqtor and s.view.nqimp for s in systems)
+    b = Batch(systems, precision=FP64)
+    b.final_energy()
+    for k, s in enumerate(systems):
+        o = oracle.create(s)
+        o.final_energy()
+        Eo, EQo = o.energy_vectors()
+        Eg, EQg = b.energy_vectors(k)
+        assert_energies(Eg, EQg, Eo, EQo)
+        err = grad_err(b.gradient(k), o.gradient())
+        assert err < G_TOL, (s.view.ff_type, err, _worst_atoms(b.gradient(k), o.gradient()))
+    b = Batch(systems, precision=FP64)
+    b.run(20)
+    for k, s in enumerate(systems):
+        o = oracle.create(s)
+        o.run(20)
+        sg, Eg, EQg = b.history(k, 0)
+        so, Eo, EQo = o.history(0)
+        assert list(sg) == list(so)
+        for m in range(len(sg)):
+            assert_energies(Eg[m], EQg[m], Eo[m], EQo[m])
+        assert grad_err(b.gradient(k), o.gradient()) < G_TOL

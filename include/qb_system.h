@@ -142,6 +142,7 @@ typedef struct qb_sysview {
   const int *iqseq;            /* [nqat] atom index */
   const float *qcrg;           /* [nqat*nstates] scaled, index iq*nstates+s */
   int qvdw_flag;
+  int qq_use_library_charges; /* Q-Q pairs take the topology charges (nonbond_qq_lib_charges) */
   int nqlib;
   const int *qiac;             /* [nqat*nstates] Q atom type (0-based into qavdw) */
   const double *qavdw, *qbvdw; /* [nqlib*3] */

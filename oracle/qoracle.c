@@ -560,7 +560,10 @@ static void nonbond_qw(qo_state *st) {
   }
 }
 
-/* nonbond_qq (md.f90:10763) */
+/* nonbond_qq (md.f90:10763) / nonbon2_qq (9385); with qq_use_library_charges,
+ * nonbond_qq_lib_charges (10872): Q-Q pairs take both atoms' topology charges,
+ * and nonbon2_qq_lib_charges (9494): every pair takes crg(i).  A Q-Q soft pair
+ * (LJ code 2) multiplies A and B under either rule (9426). */
 static void nonbond_qq(qo_state *st) {
   const qb_sysview *s = st->s;
   int S = st->S, ncol = s->natyps + st->nq;
@@ -568,19 +571,22 @@ static void nonbond_qq(qo_state *st) {
     for (int p = s->nbqq_off[ss]; p < s->nbqq_off[ss] + s->nbqq_count[ss]; p++) {
       int iq = s->nbqq_iq[p], j = s->nbqq_j[p], jq = s->nbqq_jq[p], lj = s->nbqq_ljcod[p];
       int i = s->iqseq[iq];
-      double qi = s->qcrg[iq * S + ss], qj, aLJ, bLJ;
+      int lib = s->qq_use_library_charges && jq >= 0;
+      int lib_i = s->qq_use_library_charges && (jq >= 0 || s->ivdw_rule == 2);
+      double qi = lib_i ? (double)s->crg[i] : s->qcrg[iq * S + ss], qj, aLJ, bLJ;
       double el = s->nbqq_el_scale[p];
       if (!s->qvdw_flag) {
         int ti = s->iac[i], tj = s->iac[j];
         ljp(s, avdw(s, ti, lj), avdw(s, tj, lj), bvdw(s, ti, lj), bvdw(s, tj, lj), &aLJ, &bLJ);
-        qj = jq >= 0 ? (double)s->qcrg[jq * S + ss] : (double)s->crg[j];
+        qj = jq >= 0 && !lib ? (double)s->qcrg[jq * S + ss] : (double)s->crg[j];
       } else {
         int ti = s->qiac[iq * S + ss];
         double ai = s->qavdw[3 * ti + lj - 1], bi = s->qbvdw[3 * ti + lj - 1];
         if (jq >= 0) {
           int tj = s->qiac[jq * S + ss];
-          ljp(s, ai, s->qavdw[3 * tj + lj - 1], bi, s->qbvdw[3 * tj + lj - 1], &aLJ, &bLJ);
-          qj = s->qcrg[jq * S + ss];
+          if (lj == 2) { aLJ = ai * s->qavdw[3 * tj + 1]; bLJ = bi * s->qbvdw[3 * tj + 1]; }
+          else ljp(s, ai, s->qavdw[3 * tj + lj - 1], bi, s->qbvdw[3 * tj + lj - 1], &aLJ, &bLJ);
+          qj = lib ? (double)s->crg[j] : s->qcrg[jq * S + ss];
         } else {
           if (lj == 2) { ai = s->qavdw[3 * ti]; bi = s->qbvdw[3 * ti]; }
           int tj = s->iac[j];

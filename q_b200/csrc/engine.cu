@@ -613,7 +613,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
       rw_p.push_back(make_double4(V.rwal_d[r], V.rwal_fk[r], V.rwal_aMorse[r], V.rwal_dMorse[r]));
     }
     // scalars
-    S.ff_type = V.ff_type; S.use_lrf = V.use_LRF; S.qvdw = V.qvdw_flag;
+    S.ff_type = V.ff_type; S.use_lrf = V.use_LRF; S.qvdw = V.qvdw_flag; S.qq_lib = V.qq_use_library_charges;
     S.wpol = V.wpol_restr && V.nwpolr_shell > 0; S.nshell = V.nwpolr_shell;
     if (S.nshell > MAX_SHELLS) fail(QB_ERR_UNSUPPORTED, "too many water polarisation shells");
     S.iac_ow = V.iac_ow; S.separate_scaling = V.separate_scaling; S.detail_temps = V.detail_temps;

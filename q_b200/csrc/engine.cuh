@@ -49,6 +49,7 @@ struct SysDev {
   int csoff;                  // first solute group of this system among all systems' solute groups
   int ff_type, use_lrf, qvdw, wpol, nshell, iac_ow, separate_scaling, has_shake, detail_temps;
   int qp_once;                // lists with Q atoms are built once (Rcq > exclusion radius)
+  int qq_lib;                 // Q-Q pairs take the topology charges
   int iout, iene, NB;
   int Ndegf, Ndegfree, Ndegfree_sol, Ndegfree_solv;
   double dt, Temp0, tau_T, el14, A_OO, B_OO;

@@ -1170,6 +1170,12 @@ __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
 }
 
 // nonbond_qq (md.f90:10763): Q-Q and Q-to-bonded-neighbour pairs, all states.
+// With qq_use_library_charges (nonbond_qq_lib_charges, md.f90:10872) a Q-Q
+// pair takes both atoms' topology charges; Q-to-neighbour pairs keep the Q
+// atom's state charge, except under the arithmetic rule, whose
+// nonbon2_qq_lib_charges (md.f90:9494) takes crg(i) for every pair.  A Q-Q
+// soft pair (LJ code 2 with Q types) is A exp(-B/r) with A and B products
+// under either rule (nonbon2_qq, md.f90:9426).
 __device__ __forceinline__ void nb_qq_body(DevPtrs &P, int s) {
   const SysDev &S = P.sys[s];
   const int NS = S.S, ncol = S.natyps + S.nq;
@@ -1185,20 +1191,21 @@ __device__ __forceinline__ void nb_qq_body(DevPtrs &P, int s) {
       int iq = gq - S.qoff;
       int jq = gjq >= 0 ? gjq - S.qoff : -1;
       int i = P.iqseq[gq];
-      double qi = (double)P.qcrg[gq * MAXS + st], qj, aLJ, bLJ;
+      const bool lib = S.qq_lib && jq >= 0;
+      double qi = S.qq_lib && (jq >= 0 || S.arith) ? (double)P.crg[i] : (double)P.qcrg[gq * MAXS + st], qj, aLJ, bLJ;
       double els = P.qq_el[S.qq_off + k];
       if (!S.qvdw) {
         lj_pair(S.arith, P.lja[3 * i + lj - 1], P.lja[3 * j + lj - 1], P.ljb[3 * i + lj - 1], P.ljb[3 * j + lj - 1],
                 aLJ, bLJ);
-        qj = jq >= 0 ? (double)P.qcrg[gjq * MAXS + st] : (double)P.crg[j];
+        qj = jq >= 0 && !lib ? (double)P.qcrg[gjq * MAXS + st] : (double)P.crg[j];
       } else {
         int ti = P.qiac[gq * MAXS + st];
         double ai = P.qavdw[S.qlib_off + 3 * ti + lj - 1], bi = P.qbvdw[S.qlib_off + 3 * ti + lj - 1];
         if (jq >= 0) {
           int tj = P.qiac[gjq * MAXS + st];
-          lj_pair(S.arith, ai, P.qavdw[S.qlib_off + 3 * tj + lj - 1], bi, P.qbvdw[S.qlib_off + 3 * tj + lj - 1], aLJ,
-                  bLJ);
-          qj = P.qcrg[gjq * MAXS + st];
+          lj_pair(S.arith && lj != 2, ai, P.qavdw[S.qlib_off + 3 * tj + lj - 1], bi,
+                  P.qbvdw[S.qlib_off + 3 * tj + lj - 1], aLJ, bLJ);
+          qj = lib ? P.crg[j] : P.qcrg[gjq * MAXS + st];
         } else {
           if (lj == 2) { ai = P.qavdw[S.qlib_off + 3 * ti]; bi = P.qbvdw[S.qlib_off + 3 * ti]; }
           lj_pair(S.arith, ai, P.lja[3 * j + lj - 1], bi, P.ljb[3 * j + lj - 1], aLJ, bLJ);

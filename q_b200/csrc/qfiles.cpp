@@ -910,7 +910,6 @@ void read_fep_atoms(const std::string &path, const Topology &t, Fep &f, int nsta
     }
   }
   if (f.nstates <= 0) fail(QB_ERR_PARSE, "number of states must be at least 1");
-  if (f.qq_use_library_charges) fail(QB_ERR_UNSUPPORTED, "qq_use_library_charges is not supported");
   (void)nstates_inp;
   int nlines = (int)at->lines.size();
   if (nlines == 0) { f.nqat = 0; return; }

@@ -687,7 +687,7 @@ void System::fill_view(qb_sysview *v) const {
   v->wshell_theta_corr0 = ws_theta_corr.data();
   v->lambda = in.lambdas.data();
   v->iqseq = fep.iqseq.data(); v->qcrg = qcrg_scaled.data();
-  v->qvdw_flag = fep.qvdw_flag; v->nqlib = fep.nqlib;
+  v->qvdw_flag = fep.qvdw_flag; v->nqlib = fep.nqlib; v->qq_use_library_charges = fep.qq_use_library_charges;
   v->qiac = fep.qiac.data(); v->qavdw = fep.qavdw.data(); v->qbvdw = fep.qbvdw.data();
   v->sc_lookup = fep.sc_lookup.data(); v->qconn = qconn.data();
   v->nbqq_count = nbqq_count.data(); v->nbqq_off = nbqq_off.data();

@@ -616,12 +616,15 @@ def _q_bonded(top: Topology, qatoms: list[int]) -> list[str]:
 
 def _fep_file(path: str, types: list[AtomType], iac: list[int], q: list[float], qatoms: list[int],
               alpha: float = 20.0, charge_scale: float = 0.0, eps_scale: float = 0.5, vdw_rule: int = 1,
-              top: Topology | None = None) -> None:
+              top: Topology | None = None, soft_pairs=(), library_charges: bool = False) -> None:
     """Two-state FEP file: state 2 scales the Q-atoms' charges by
     charge_scale and their epsilon by eps_scale, soft-core alpha in state 2.
     Given the topology, the bonded terms among the Q atoms are redefined too
-    (_q_bonded)."""
-    L = ["[FEP]", "states 2", "", "[atoms]"]
+    (_q_bonded).  soft_pairs (Q-atom index pairs, 0-based) interact by
+    exponential repulsion A_i A_j exp(-B_i B_j r) instead of LJ, with the Q
+    types' second parameter pair set for it; library_charges turns on
+    qq_use_library_charges."""
+    L = ["[FEP]", "states 2"] + (["qq_use_library_charges on"] if library_charges else []) + ["", "[atoms]"]
     L += ["%d %d" % (k + 1, a + 1) for k, a in enumerate(qatoms)]
     L += ["", "[change_charges]"]
     L += ["%d %8.4f %8.4f" % (k + 1, q[a], round(q[a] * charge_scale, 4)) for k, a in enumerate(qatoms)]
@@ -631,19 +634,22 @@ def _fep_file(path: str, types: list[AtomType], iac: list[int], q: list[float], 
         t = types[iac[a]]
         for st, scale in ((1, 1.0), (2, eps_scale)):
             nm = "Q%d_%d" % (k + 1, st)
+            ea, eb = ((31.62, 1.87) if st == 1 else (25.0, 1.87)) if soft_pairs else (0.0, 0.0)
             if vdw_rule == 2:   # R*, epsilon (not square-rooted: the engine does it), 1-4 at half epsilon
                 rs = 2.0 ** (1.0 / 6.0) * t.sigma / 2.0
                 e = t.eps * scale
-                L.append("%-8s %9.5f %9.5f %6.2f %6.2f %9.5f %9.5f %8.4f" % (nm, rs, e, 0.0, 0.0, rs, e / 2.0, t.mass))
+                L.append("%-8s %9.5f %9.5f %6.2f %6.2f %9.5f %9.5f %8.4f" % (nm, rs, e, ea, eb, rs, e / 2.0, t.mass))
             else:
                 aa, bb = lj_sqrt(t.sigma, t.eps * scale)
                 L.append("%-8s %9.2f %8.2f %6.2f %6.2f %9.2f %8.2f %8.4f"
-                         % (nm, aa, bb, 0.0, 0.0, aa / math.sqrt(2), bb / math.sqrt(2), t.mass))
+                         % (nm, aa, bb, ea, eb, aa / math.sqrt(2), bb / math.sqrt(2), t.mass))
         names.append(("Q%d_1" % (k + 1), "Q%d_2" % (k + 1)))
     L += ["", "[change_atoms]"]
     L += ["%d %s %s" % (k + 1, a, b) for k, (a, b) in enumerate(names)]
     L += ["", "[softcore]"]
     L += ["%d %g %g" % (k + 1, 0.0, alpha) for k in range(len(qatoms))]
+    if soft_pairs:
+        L += ["", "[soft_pairs]"] + ["%d %d" % (a + 1, b + 1) for a, b in soft_pairs]
     if top is not None:
         L += [""] + _q_bonded(top, qatoms)
     with open(path, "w") as f:
@@ -676,11 +682,13 @@ def perturbation(base: Generated, name: str, qatoms, charge_scale: float, eps_sc
 
 def fep_solute(outdir: str, radius: float = 20.0, seed: int = 1234, steps: int = 5000, name: str = "c1",
                lambdas=(0.5, 0.5), run_seed: int = 1, vdw_rule: int = 1, ff_type: int = 2,
-               q_bonded: bool = False, ub_fk: float = 25.0) -> Generated:
+               q_bonded: bool = False, ub_fk: float = 25.0, soft_pairs: int = 0,
+               library_charges: bool = False) -> Generated:
     """Config 1: 56-atom solute with 8 two-state Q-atoms in a TIP3P sphere,
     2 fs with SHAKE on X-H bonds and water.  ff_type 3 writes it as a CHARMM
     topology (charmm_terms, Urey-Bradley constant ub_fk); q_bonded redefines the bonded terms among the
-    Q atoms in the FEP file."""
+    Q atoms in the FEP file.  soft_pairs > 0 makes that many Q-atom pairs
+    beyond 1-4 soft pairs; library_charges sets qq_use_library_charges."""
     os.makedirs(outdir, exist_ok=True)
     rng = np.random.default_rng(seed)
     X, kinds, bonds = random_tree_solute(rng)
@@ -714,7 +722,11 @@ def fep_solute(outdir: str, radius: float = 20.0, seed: int = 1234, steps: int =
     top.write(tp)
     fp = os.path.join(outdir, name + ".fep")
     heavy = [i for i in range(n) if kinds[i] >= 0]
-    _fep_file(fp, types, iac, top.crg, heavy[:8], vdw_rule=vdw_rule, top=top if q_bonded else None)
+    qat = heavy[:8]
+    near = {tuple(sorted(p)) for p in list(top.excl14[0]) + list(top.excl14[1])}
+    far = [(a, b) for a in range(len(qat)) for b in range(a + 1, len(qat)) if tuple(sorted((qat[a], qat[b]))) not in near]
+    _fep_file(fp, types, iac, top.crg, qat, vdw_rule=vdw_rule, top=top if q_bonded else None,
+              soft_pairs=far[:soft_pairs], library_charges=library_charges)
     inp = os.path.join(outdir, name + ".inp")
     write_inp(inp, tp, fp, steps=steps, stepsize=2.0, seed=run_seed, lambdas=lambdas, shake_hydrogens=True)
     return Generated(inp, tp, fp, len(top.x), len(waters))

@@ -405,3 +405,31 @@ def test_charmm_and_q_bonded_match_oracle(charmm_pair, oracle):
         for m in range(len(sg)):
             assert_energies(Eg[m], EQg[m], Eo[m], EQo[m])
         assert grad_err(b.gradient(k), o.gradient()) < G_TOL
+
+
+@pytest.fixture(scope="module")
+def qq_options(tmp_path_factory):
+    from q_b200 import synth
+    root = tmp_path_factory.mktemp("qqopt")
+    return [synth.fep_solute(str(root / ("r%d_%d" % (rule, lib))), vdw_rule=rule, soft_pairs=3, library_charges=bool(lib))
+            for rule in (1, 2) for lib in (0, 1)]
+
+
+def test_soft_pairs_and_library_charges_match_oracle(qq_options, oracle):
+    """Q-Q soft pairs (A_i A_j exp(-B_i B_j r), nonbond_qq / nonbon2_qq) and
+    qq_use_library_charges (nonbond_qq_lib_charges, nonbon2_qq_lib_charges)
+    under both combination rules: four systems in one batch, 20 steps."""
+    systems = [System.open(g.inp, lambdas=(0.4, 0.6), seed=5) for g in qq_options]
+    assert [(s.view.ivdw_rule, s.view.qq_use_library_charges) for s in systems] == [(1, 0), (1, 1), (2, 0), (2, 1)]
+    b = Batch(systems, precision=FP64)
+    b.run(20)
+    for k, s in enumerate(systems):
+        o = oracle.create(s)
+        o.run(20)
+        sg, Eg, EQg = b.history(k, 0)
+        so, Eo, EQo = o.history(0)
+        assert list(sg) == list(so)
+        for m in range(len(sg)):
+            assert_energies(Eg[m], EQg[m], Eo[m], EQo[m])
+        err = grad_err(b.gradient(k), o.gradient())
+        assert err < G_TOL, (k, err, _worst_atoms(b.gradient(k), o.gradient()))

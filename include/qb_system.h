@@ -132,6 +132,9 @@ typedef struct qb_sysview {
   /* ---- water ---- */
   float crg_ow, crg_hw;           /* scaled charges of water O and H */
   double A_OO, B_OO;              /* O-O LJ products (md.f90:11836-11841) */
+  int ww_hlj;                     /* water hydrogens carry LJ in the water-water and Q-water terms
+                                     (nonbon2_ww/nonbon2_qw, nonbond_3atomsolvent/nonbond_qw_3atom) */
+  double A_OH, B_OH, A_HH, B_HH;  /* O-H and H-H LJ products, when ww_hlj */
   int iac_ow, iac_hw;
   int nwpolr_shell;
   const float *wshell_rout, *wshell_dr, *wshell_cstb; /* [nwpolr_shell] */

@@ -486,9 +486,13 @@ static void nonbond_ww(qo_state *st) {
           double r2 = rinv * rinv;
           float qq = (a == 0 && b == 0) ? qoo : ((a == 0 || b == 0) ? qoh : qhh);
           double Vel = (double)qq * rinv, dv;
-          if (a == 0 && b == 0) {
+          /* nonbon2_ww (md.f90:10099) and nonbond_3atomsolvent (12317) take LJ on
+           * all nine site pairs; nonbond_ww_spc (11823) on O-O only */
+          if ((a == 0 && b == 0) || s->ww_hlj) {
+            double A = (a == 0 && b == 0) ? s->A_OO : ((a == 0 || b == 0) ? s->A_OH : s->A_HH);
+            double B = (a == 0 && b == 0) ? s->B_OO : ((a == 0 || b == 0) ? s->B_OH : s->B_HH);
             double r6 = r2 * r2 * r2;
-            double Va = s->A_OO * r6 * r6, Vb = s->B_OO * r6;
+            double Va = A * r6 * r6, Vb = B * r6;
             st->E[QB_E_WW_VDW] += Va - Vb;
             dv = r2 * (-Vel - 12. * Va + 6. * Vb);
           } else {
@@ -503,12 +507,15 @@ static void nonbond_ww(qo_state *st) {
   }
 }
 
-/* nonbond_qw_spc (md.f90:11302) */
+/* nonbond_qw_spc (md.f90:11302); with hydrogen LJ, nonbon2_qw (9798) and
+ * nonbond_qw_3atom (11545): both hydrogen sites add LJ with the hydrogen
+ * type's parameters and soft-core shift sc_lookup(iq, iac_hw, state) */
 static void nonbond_qw(qo_state *st) {
   const qb_sysview *s = st->s;
   int S = st->S, ncol = s->natyps + st->nq;
-  int iac_ow = s->iac_ow;
+  int iac_ow = s->iac_ow, iac_hw = s->iac_hw;
   double aO[2] = {avdw(s, iac_ow, 1), avdw(s, iac_ow, 2)}, bO[2] = {bvdw(s, iac_ow, 1), bvdw(s, iac_ow, 2)};
+  double aH[2] = {avdw(s, iac_hw, 1), avdw(s, iac_hw, 2)}, bH[2] = {bvdw(s, iac_hw, 1), bvdw(s, iac_hw, 2)};
   for (int jw = 0; jw < st->nqw; jw++) {
     int j = st->qw[jw];
     for (int iq = 0; iq < st->nq; iq++) {
@@ -530,6 +537,13 @@ static void nonbond_qw(qo_state *st) {
         Va = A * r6O * r6O;
         Vb = B * r6O;
       }
+      int ljh = s->ww_hlj ? ljcode(s, iac_hw, s->iac[i]) : 1;
+      double r6H[2] = {r2H1 * r2H1 * r2H1, r2H2 * r2H2 * r2H2}, VaH[2] = {0, 0}, VbH[2] = {0, 0};
+      if (s->ww_hlj && !s->qvdw_flag) {
+        double A, B;
+        ljp(s, avdw(s, s->iac[i], ljh), aH[ljh - 1], bvdw(s, s->iac[i], ljh), bH[ljh - 1], &A, &B);
+        for (int h = 0; h < 2; h++) { VaH[h] = A * r6H[h] * r6H[h]; VbH[h] = B * r6H[h]; }
+      }
       for (int ss = 0; ss < S; ss++) {
         if (s->qvdw_flag) {
           int ti = s->qiac[iq * S + ss];
@@ -545,8 +559,26 @@ static void nonbond_qw(qo_state *st) {
         double VelH2 = (double)(s->crg_hw * qq) * rH2;
         double lam = s->lambda[ss];
         dvO += r2O * (-VelO - ((12. * Va - 6. * Vb) * (r6hc / r6sc))) * lam;
-        dvH1 -= r2H1 * VelH1 * lam;
-        dvH2 -= r2H2 * VelH2 * lam;
+        if (s->ww_hlj) {
+          double fH[2] = {1.0, 1.0};
+          if (s->qvdw_flag) {
+            int ti = s->qiac[iq * S + ss];
+            double A, B, sc = s->sc_lookup[((size_t)iq * ncol + iac_hw) * S + ss];
+            ljp(s, s->qavdw[3 * ti], aH[ljh - 1], s->qbvdw[3 * ti], bH[ljh - 1], &A, &B);
+            for (int h = 0; h < 2; h++) {
+              double d6 = 1.0 / r6H[h], r6s = d6 + sc;
+              VaH[h] = A / (r6s * r6s);
+              VbH[h] = B / r6s;
+              fH[h] = d6 / r6s;
+            }
+          }
+          dvH1 += r2H1 * (-VelH1 - (12. * VaH[0] - 6. * VbH[0]) * fH[0]) * lam;
+          dvH2 += r2H2 * (-VelH2 - (12. * VaH[1] - 6. * VbH[1]) * fH[1]) * lam;
+          EQV(ss, QB_EQ_QW_VDW) += VaH[0] + VaH[1] - VbH[0] - VbH[1];
+        } else {
+          dvH1 -= r2H1 * VelH1 * lam;
+          dvH2 -= r2H2 * VelH2 * lam;
+        }
         EQV(ss, QB_EQ_QW_EL) += VelO + VelH1 + VelH2;
         EQV(ss, QB_EQ_QW_VDW) += Va - Vb;
       }

@@ -62,7 +62,7 @@ struct Batch {
   long long istep = 0;
   int max_natom = 0, max_lrf_blocks = 1, max_nsol = 0, max_nwat = 0, max_ncgp = 0, max_ncgp_sol = 0, max_terms = 0, max_pp = 0, max_ncgp_sol_w = 0, max_qp = 0;
   bool any_lrf = false, any_q = false, any_shake = false, any_wpol = false, any_prestr = false, any_qq = false,
-       any_qb = false;
+       any_qb = false, any_hlj = false;
   // run-time choices the autotuner sets (qb_tuning): LRF source tiles per
   // block, water-water staging chunk (>= ww_chunk_floor, for which ww_sp is
   // sized), side streams on or off
@@ -255,20 +255,30 @@ struct Batch {
     if (max_nwat > 0) {
       dim3 gw(cdiv(max_nwat, WW_WPB), nsys);
       size_t smem = (size_t)p.ww_chunk * (mixed ? WatRec<true>::words : WatRec<false>::words) * sizeof(float4);
-      if (mixed) {
-        launch("nb_ww", [&] { k_nb_ww<true><<<gw, WW_BLOCK, smem, stream>>>(p); });
+      // hydrogen LJ: the whole batch takes the variant (exact zeros for systems without)
+      if (mixed && any_hlj) {
+        launch("nb_ww", [&] { k_nb_ww<true, true><<<gw, WW_BLOCK, smem, stream>>>(p); });
+      } else if (mixed) {
+        launch("nb_ww", [&] { k_nb_ww<true, false><<<gw, WW_BLOCK, smem, stream>>>(p); });
+      } else if (any_hlj) {
+        launch("nb_ww", [&] { k_nb_ww<false, true><<<gw, WW_BLOCK, smem, stream>>>(p); });
       } else {
-        launch("nb_ww", [&] { k_nb_ww<false><<<gw, WW_BLOCK, smem, stream>>>(p); });
+        launch("nb_ww", [&] { k_nb_ww<false, false><<<gw, WW_BLOCK, smem, stream>>>(p); });
       }
       if (any_q) launch("nb_qw", [&] {
         dim3 g(cdiv(max_nwat, 128), nsys);
-        if (max_nq > NQ_SHARED) { k_nb_qw<0, false><<<g, 128, 0, s2>>>(p); return; }
+        if (any_hlj) {   // hydrogen LJ: the generic state count only
+          if (max_nq > NQ_SHARED) k_nb_qw<0, false, true><<<g, 128, 0, s2>>>(p);
+          else k_nb_qw<0, true, true><<<g, 128, 0, s2>>>(p);
+          return;
+        }
+        if (max_nq > NQ_SHARED) { k_nb_qw<0, false, false><<<g, 128, 0, s2>>>(p); return; }
         switch (q_states) {
-          case 1: k_nb_qw<1, true><<<g, 128, 0, s2>>>(p); break;
-          case 2: k_nb_qw<2, true><<<g, 128, 0, s2>>>(p); break;
-          case 3: k_nb_qw<3, true><<<g, 128, 0, s2>>>(p); break;
-          case 4: k_nb_qw<4, true><<<g, 128, 0, s2>>>(p); break;
-          default: k_nb_qw<0, true><<<g, 128, 0, s2>>>(p);
+          case 1: k_nb_qw<1, true, false><<<g, 128, 0, s2>>>(p); break;
+          case 2: k_nb_qw<2, true, false><<<g, 128, 0, s2>>>(p); break;
+          case 3: k_nb_qw<3, true, false><<<g, 128, 0, s2>>>(p); break;
+          case 4: k_nb_qw<4, true, false><<<g, 128, 0, s2>>>(p); break;
+          default: k_nb_qw<0, true, false><<<g, 128, 0, s2>>>(p);
         }
       });
     }
@@ -633,6 +643,10 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     if (V.nwat > 0) {
       S.aO[0] = V.type_avdw[3 * V.iac_ow]; S.aO[1] = V.type_avdw[3 * V.iac_ow + 1];
       S.bO[0] = V.type_bvdw[3 * V.iac_ow]; S.bO[1] = V.type_bvdw[3 * V.iac_ow + 1];
+      S.hlj = V.ww_hlj; S.iac_hw = V.iac_hw;
+      S.A_OH = V.A_OH; S.B_OH = V.B_OH; S.A_HH = V.A_HH; S.B_HH = V.B_HH;
+      S.aH[0] = V.type_avdw[3 * V.iac_hw]; S.aH[1] = V.type_avdw[3 * V.iac_hw + 1];
+      S.bH[0] = V.type_bvdw[3 * V.iac_hw]; S.bH[1] = V.type_bvdw[3 * V.iac_hw + 1];
     }
     SysState &st = sst[s];
     std::memset(&st, 0, sizeof st);
@@ -719,6 +733,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     B.any_prestr |= (V.nrstr_seq + V.nrstr_pos + V.nrstr_dist + V.nrstr_angl + V.nrstr_wall) > 0;
     B.any_qq |= S.nqq > 0;
     B.any_qb |= (V.nqbond + V.nqangle + V.nqtor + V.nqimp) > 0;
+    B.any_hlj |= V.nwat > 0 && V.ww_hlj;
   }
   // water offsets
   int woff = 0;
@@ -861,8 +876,10 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   P.ww_sp = dev_alloc<int>((size_t)std::max(woff, 1) * nch_alloc, o);
   P.wrec = dev_alloc<float4>((size_t)std::max(woff, 1) * rec_words, o);
   // the limit (not an allocation) covers every chunk size any batch may use
-  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
-  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
   P.kin_nblk = std::max(1, (B.max_natom + KIN_BLOCK - 1) / KIN_BLOCK);
   P.kin = dev_alloc<double>((size_t)n * 4, o);
   P.E = dev_alloc<double>((size_t)n * QB_NE, o);

@@ -59,6 +59,10 @@ struct SysDev {
   float ws_rout[MAX_SHELLS], ws_dr[MAX_SHELLS], ws_cstb[MAX_SHELLS];
   double lambda[MAXS];
   double aO[2], bO[2];
+  // water hydrogens with LJ (arithmetic rule, 3-atom solvent): O-H and H-H
+  // products for water-water, the hydrogen type's columns for Q-water
+  int hlj, iac_hw;
+  double A_OH, B_OH, A_HH, B_HH, aH[2], bH[2];
   int arith;                       // 1: arithmetic LJ combination rule (lj_pair)
 };
 

@@ -655,9 +655,11 @@ __device__ __forceinline__ void watpol_angle(const DevPtrs &P, const SysDev &S, 
 
 // One SPC/TIP3P molecule pair (md.f90:11823-11950, nonbond_ww_spc): the 9
 // Coulomb terms and the O-O Lennard-Jones term, gradient of molecule i added
-// to f[9].
+// to f[9].  HLJ adds the O-H and H-H Lennard-Jones terms of nonbon2_ww
+// (md.f90:10099) and nonbond_3atomsolvent (12317); lj = {A, B} of O-O, O-H, H-H.
+template <bool HLJ>
 __device__ __forceinline__ void ww_pair_f64(const double *xi, const double *xj, double qoo, double qoh, double qhh,
-                                            double A, double B, double *f, double &el, double &vdw) {
+                                            const double *lj, double *f, double &el, double &vdw) {
 #pragma unroll
   for (int a = 0; a < 3; a++)
 #pragma unroll
@@ -667,9 +669,10 @@ __device__ __forceinline__ void ww_pair_f64(const double *xi, const double *xj, 
       double r2 = rinv * rinv;
       double qq = (a == 0 && b == 0) ? qoo : ((a == 0 || b == 0) ? qoh : qhh);
       double Vel = qq * rinv, dv;
-      if (a == 0 && b == 0) {
+      if ((a == 0 && b == 0) || HLJ) {
+        const int t = (a == 0 && b == 0) ? 0 : ((a == 0 || b == 0) ? 2 : 4);
         double r6 = r2 * r2 * r2;
-        double Va = A * r6 * r6, Vb = B * r6;
+        double Va = lj[t] * r6 * r6, Vb = lj[t + 1] * r6;
         vdw += Va - Vb;
         dv = r2 * (-Vel - 12. * Va + 6. * Vb);
       } else {
@@ -683,8 +686,9 @@ __device__ __forceinline__ void ww_pair_f64(const double *xi, const double *xj, 
 }
 
 // Mixed precision: i = {hO[3], lO[3], rH1[3], rH2[3]}, j likewise.
+template <bool HLJ>
 __device__ __forceinline__ void ww_pair_f32(const float *i, const float *j, float qoo, float qoh, float qhh,
-                                            float A, float B, float *f, float &el, float &vdw) {
+                                            const float *lj, float *f, float &el, float &vdw) {
   float dOO[3], t[2][3];
 #pragma unroll
   for (int c = 0; c < 3; c++) {
@@ -706,9 +710,10 @@ __device__ __forceinline__ void ww_pair_f32(const float *i, const float *j, floa
       float r2 = rinv * rinv;
       float qq = (a == 0 && b == 0) ? qoo : ((a == 0 || b == 0) ? qoh : qhh);
       float Vel = qq * rinv, dv;
-      if (a == 0 && b == 0) {
+      if ((a == 0 && b == 0) || HLJ) {
+        const int t = (a == 0 && b == 0) ? 0 : ((a == 0 || b == 0) ? 2 : 4);
         float r6 = r2 * r2 * r2;
-        float Va = A * r6 * r6, Vb = B * r6;
+        float Va = lj[t] * r6 * r6, Vb = lj[t + 1] * r6;
         vdw += Va - Vb;
         dv = r2 * (-Vel - 12.f * Va + 6.f * Vb);
       } else {
@@ -736,7 +741,7 @@ __device__ __forceinline__ void unpack_mixed(const float4 *r, float *v) {
 // from both sides, energies halved.  Mixed precision: pair terms in FP32
 // (MUFU rsqrt), each lane's energy over one water's list slice summed in FP32 and accumulated in
 // FP64, gradients reduced in FP32.
-template <bool MIXED>
+template <bool MIXED, bool HLJ>
 __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
   extern __shared__ float4 wsm[];
   __shared__ int2 srange[WW_WPB];          // list slice of each of the block's waters in this chunk
@@ -793,7 +798,7 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
         float xi[12];
         unpack_mixed(ri, xi);
         const float qoo = qo * qo, qoh = qo * qh, qhh = qh * qh;
-        const float A = (float)S.A_OO, B = (float)S.B_OO;
+        const float ljf[6] = {(float)S.A_OO, (float)S.B_OO, (float)S.A_OH, (float)S.B_OH, (float)S.A_HH, (float)S.B_HH};
         float f[9];
 #pragma unroll
         for (int q = 0; q < 9; q++) f[q] = 0.f;
@@ -805,7 +810,7 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
           if (k + 32 < ke) jn2 = nb[k + 32];
           float xj[12];
           unpack_mixed(wsm + (j - c0) * W, xj);
-          ww_pair_f32(xi, xj, qoo, qoh, qhh, A, B, f, e_el, e_vdw);
+          ww_pair_f32<HLJ>(xi, xj, qoo, qoh, qhh, ljf, f, e_el, e_vdw);
         }
         el += (double)e_el;
         vdw += (double)e_vdw;
@@ -821,6 +826,7 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
         double2 d0 = rd[0], d1 = rd[1], d2 = rd[2], d3 = rd[3], d4 = rd[4];
         const double xi[9] = {d0.x, d0.y, d1.x, d1.y, d2.x, d2.y, d3.x, d3.y, d4.x};
         const double qoo = (double)(qo * qo), qoh = (double)(qo * qh), qhh = (double)(qh * qh);
+        const double ljd[6] = {S.A_OO, S.B_OO, S.A_OH, S.B_OH, S.A_HH, S.B_HH};
 #pragma unroll
         for (int q = 0; q < 9; q++) fd[q] = 0.0;
         for (; k < ke; k += 16) {
@@ -829,7 +835,7 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
           const double2 *rj = reinterpret_cast<const double2 *>(wsm + (j - c0) * W);
           double2 v0 = rj[0], v1 = rj[1], v2 = rj[2], v3 = rj[3], v4 = rj[4];
           const double xj[9] = {v0.x, v0.y, v1.x, v1.y, v2.x, v2.y, v3.x, v3.y, v4.x};
-          ww_pair_f64(xi, xj, qoo, qoh, qhh, S.A_OO, S.B_OO, fd, el, vdw);
+          ww_pair_f64<HLJ>(xi, xj, qoo, qoh, qhh, ljd, fd, el, vdw);
         }
 #pragma unroll
         for (int q = 0; q < 9; q++) {
@@ -1031,9 +1037,11 @@ __device__ __forceinline__ void nb_qp_body(DevPtrs &P, int bx, int s, int gx) {
 // are staged in shared memory once per block.  Q-atom gradients are reduced
 // per warp, then per block in shared memory (NQ_SHARED atoms at most; global
 // atomics beyond).
-struct QwState { float qO, qH; double A, B, sc; };
+// With hydrogen LJ (nonbon2_qw, md.f90:9798; nonbond_qw_3atom, 11545) the two
+// hydrogen sites add LJ with their own type's parameters and soft-core shift.
+struct QwState { float qO, qH; double A, B, sc, AH, BH, scH; };
 
-template <int NSC, bool SHQ>
+template <int NSC, bool SHQ, bool HLJ>
 __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
   constexpr int NA = NSC > 0 ? NSC : MAXS;
   int s = blockIdx.y;
@@ -1041,23 +1049,28 @@ __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
   __shared__ double fq[NQ_SHARED * 3];
   __shared__ double4 qx[NQ_SHARED];        // position; w: LJ code
   __shared__ double2 qab[NQ_SHARED];       // A, B with the water O (same in every state)
+  __shared__ double2 qabH[NQ_SHARED];      // A, B with a water H (hydrogen LJ only)
   __shared__ QwState qst[NQ_SHARED * NA];
   if (S.nq == 0) return;
   const int n = P.st[s].qw_n;
   if (blockIdx.x * blockDim.x >= n) return;
   const int NS = NSC > 0 ? NSC : S.S, ncol = S.natyps + S.nq;
+  const bool hlj = HLJ && S.hlj;           // this system's water hydrogens carry LJ
   const bool shq = SHQ;                    // every system's Q atoms fit the shared tables
   const int nqs = shq ? S.nq : 0;
   for (int t = threadIdx.x; t < NQ_SHARED * 3; t += blockDim.x) fq[t] = 0;
   for (int iq = threadIdx.x; iq < nqs; iq += blockDim.x) {
     int gq = S.qoff + iq, i = P.iqseq[gq];
     int lj = P.ljcod[S.ljoff + S.iac_ow * S.natyps + P.iac[i]];
+    int ljh = hlj ? P.ljcod[S.ljoff + S.iac_hw * S.natyps + P.iac[i]] : 1;
     double4 x = P.x[i];
-    x.w = (double)lj;
+    x.w = (double)(lj + 4 * ljh);
     qx[iq] = x;
-    double A0, B0;
+    double A0, B0, AH0 = 0, BH0 = 0;
     lj_pair(S.arith, P.lja[3 * i + lj - 1], S.aO[lj - 1], P.ljb[3 * i + lj - 1], S.bO[lj - 1], A0, B0);
+    if (hlj) lj_pair(S.arith, P.lja[3 * i + ljh - 1], S.aH[ljh - 1], P.ljb[3 * i + ljh - 1], S.bH[ljh - 1], AH0, BH0);
     qab[iq] = make_double2(A0, B0);
+    qabH[iq] = make_double2(AH0, BH0);
     for (int st = 0; st < NS; st++) {
       QwState q;
       float c = P.qcrg[gq * MAXS + st];
@@ -1066,6 +1079,12 @@ __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
       int ti = P.qiac[gq * MAXS + st];
       lj_pair(S.arith, P.qavdw[S.qlib_off + 3 * ti], S.aO[lj - 1], P.qbvdw[S.qlib_off + 3 * ti], S.bO[lj - 1], q.A, q.B);
       q.sc = S.qvdw ? P.sc[S.sc_off + ((size_t)iq * ncol + S.iac_ow) * NS + st] : 0.0;
+      q.AH = q.BH = q.scH = 0.0;
+      if (hlj) {
+        lj_pair(S.arith, P.qavdw[S.qlib_off + 3 * ti], S.aH[ljh - 1], P.qbvdw[S.qlib_off + 3 * ti], S.bH[ljh - 1], q.AH,
+                q.BH);
+        q.scH = S.qvdw ? P.sc[S.sc_off + ((size_t)iq * ncol + S.iac_hw) * NS + st] : 0.0;
+      }
       qst[iq * NA + st] = q;
     }
   }
@@ -1081,17 +1100,22 @@ __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
   for (int iq = 0; iq < S.nq; iq++) {
     int gq = S.qoff + iq;
     double4 xi4;
-    int lj;
-    double A0, B0;
+    int lj, ljh;
+    double A0, B0, AH0 = 0, BH0 = 0;
     if (shq) {
       xi4 = qx[iq];
-      lj = (int)xi4.w;
+      lj = (int)xi4.w & 3;
+      ljh = (int)xi4.w >> 2;
       A0 = qab[iq].x; B0 = qab[iq].y;
+      AH0 = qabH[iq].x; BH0 = qabH[iq].y;
     } else {
       int i = P.iqseq[gq];
       xi4 = P.x[i];
       lj = P.ljcod[S.ljoff + S.iac_ow * S.natyps + P.iac[i]];
+      ljh = hlj ? P.ljcod[S.ljoff + S.iac_hw * S.natyps + P.iac[i]] : 1;
       lj_pair(S.arith, P.lja[3 * i + lj - 1], S.aO[lj - 1], P.ljb[3 * i + lj - 1], S.bO[lj - 1], A0, B0);
+      if (hlj)
+        lj_pair(S.arith, P.lja[3 * i + ljh - 1], S.aH[ljh - 1], P.ljb[3 * i + ljh - 1], S.bH[ljh - 1], AH0, BH0);
     }
     double dO[3] = {xO.x - xi4.x, xO.y - xi4.y, xO.z - xi4.z};
     double dH1[3] = {xH1.x - xi4.x, xH1.y - xi4.y, xH1.z - xi4.z};
@@ -1109,6 +1133,16 @@ __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
       Va = A0 * r6O * r6O;
       Vb = B0 * r6O;
     }
+    // hydrogen sites: d^6 and the hard-core LJ terms (state independent without qvdw)
+    double d6H1 = 0, d6H2 = 0, VaH1 = 0, VbH1 = 0, VaH2 = 0, VbH2 = 0;
+    if (hlj) {
+      double r6H1 = r2H1 * r2H1 * r2H1, r6H2 = r2H2 * r2H2 * r2H2;
+      d6H1 = 1. / r6H1; d6H2 = 1. / r6H2;
+      if (!S.qvdw) {
+        VaH1 = AH0 * r6H1 * r6H1; VbH1 = BH0 * r6H1;
+        VaH2 = AH0 * r6H2 * r6H2; VbH2 = BH0 * r6H2;
+      }
+    }
 #pragma unroll
     for (int st = 0; st < NA; st++) {
       if (st >= NS) break;
@@ -1121,6 +1155,12 @@ __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
         lj_pair(S.arith, P.qavdw[S.qlib_off + 3 * ti], S.aO[lj - 1], P.qbvdw[S.qlib_off + 3 * ti], S.bO[lj - 1], q.A,
                 q.B);
         q.sc = S.qvdw ? P.sc[S.sc_off + ((size_t)iq * ncol + S.iac_ow) * NS + st] : 0.0;
+        q.AH = q.BH = q.scH = 0.0;
+        if (hlj) {
+          lj_pair(S.arith, P.qavdw[S.qlib_off + 3 * ti], S.aH[ljh - 1], P.qbvdw[S.qlib_off + 3 * ti], S.bH[ljh - 1],
+                  q.AH, q.BH);
+          q.scH = S.qvdw ? P.sc[S.sc_off + ((size_t)iq * ncol + S.iac_hw) * NS + st] : 0.0;
+        }
       }
       double r6sc = r6hc;
       if (S.qvdw) {
@@ -1133,8 +1173,21 @@ __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
       double VelH2 = (double)q.qH * rH2;
       double lam = S.lambda[st];
       dvO += r2O * (-VelO - ((12. * Va - 6. * Vb) * (r6hc / r6sc))) * lam;
-      dvH1 -= r2H1 * VelH1 * lam;
-      dvH2 -= r2H2 * VelH2 * lam;
+      if (hlj) {
+        double f1 = 1.0, f2 = 1.0;
+        if (S.qvdw) {
+          double s1 = d6H1 + q.scH, s2 = d6H2 + q.scH;
+          VaH1 = q.AH / (s1 * s1); VbH1 = q.BH / s1;
+          VaH2 = q.AH / (s2 * s2); VbH2 = q.BH / s2;
+          f1 = d6H1 / s1; f2 = d6H2 / s2;
+        }
+        dvH1 += r2H1 * (-VelH1 - (12. * VaH1 - 6. * VbH1) * f1) * lam;
+        dvH2 += r2H2 * (-VelH2 - (12. * VaH2 - 6. * VbH2) * f2) * lam;
+        if (act) vdw[st] += VaH1 + VaH2 - VbH1 - VbH2;
+      } else {
+        dvH1 -= r2H1 * VelH1 * lam;
+        dvH2 -= r2H2 * VelH2 * lam;
+      }
       if (act) {
         el[st] += VelO + VelH1 + VelH2;
         vdw[st] += Va - Vb;

@@ -148,6 +148,8 @@ struct System {
   int nshellats = 0;
   float crg_ow = 0, crg_hw = 0, mu_w = 0;
   double A_OO = 0, B_OO = 0;
+  int ww_hlj = 0;
+  double A_OH = 0, B_OH = 0, A_HH = 0, B_HH = 0;
   int iac_ow = -1, iac_hw = -1;
   double crgtot = 0, crgQtot = 0;
   double fk_wsphere = 60, Dwmz = 0, awmz = 0, fkwpol = 20, rwat = 0;

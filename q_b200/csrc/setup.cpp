@@ -88,8 +88,10 @@ void prepare(System &s) {
   if (t.ivdw_rule == 2)
     for (auto &ty : t.iaclib)
       for (int k = 0; k < 3; k++) ty.bvdw[k] = std::sqrt(std::fabs(ty.bvdw[k]));
-  if (t.solvent_type != 0 && t.nat_pro > t.nat_solute)
-    fail(QB_ERR_UNSUPPORTED, "only SPC-type 3-site water is supported (solvent_type 0)");
+  if (t.solvent_type == 2 && t.nat_pro > t.nat_solute)
+    fail(QB_ERR_UNSUPPORTED, "mixed or non-3-atomic solvent (solvent_type 2) is not supported");
+  if (t.solvent_type != 0 && t.solvent_type != 1 && t.nat_pro > t.nat_solute)
+    fail(QB_ERR_PARSE, "unknown solvent type in the topology");
   if (t.ff_type < 1 || t.ff_type > 3) fail(QB_ERR_UNSUPPORTED, "unknown force-field type in the topology");
   s.natom = t.nat_pro;
   s.nwat = (s.natom - t.nat_solute) / 3;
@@ -568,13 +570,23 @@ void prepare(System &s) {
     int lj = s.ljcod[(size_t)s.iac_ow * t.natyps + s.iac_ow] - 1;
     const auto &O = t.iaclib[s.iac_ow];
     lj_pair(t.ivdw_rule == 2, O.avdw[lj], O.avdw[lj], O.bvdw[lj], O.bvdw[lj], s.A_OO, s.B_OO);
-    // the arithmetic rule's water routine (nonbon2_ww) adds LJ on every
-    // atom pair; this path takes the O-O pair only, exact when the water
-    // hydrogens carry no LJ
-    if (t.ivdw_rule == 2)
-      for (int k = 0; k < 3; k++)
-        if (t.iaclib[s.iac_hw].bvdw[k] != 0.0)
-          fail(QB_ERR_UNSUPPORTED, "arithmetic-rule water with Lennard-Jones on its hydrogens (3-atom solvent)");
+    // The arithmetic rule's water routines (nonbon2_ww, nonbon2_qw) and the
+    // geometric 3-atom solvent's (nonbond_3atomsolvent, nonbond_qw_3atom)
+    // take LJ on every site pair; the SPC routines take O-O only.  Site 2 and
+    // 3 are one hydrogen type here, with charge -crg_ow/2 (the value the Q-water
+    // terms use, md.f90:13799-13801).
+    if (t.solvent_type == 1 && (t.iac[NS + 1] != t.iac[NS + 2] || t.crg[NS + 1] != t.crg[NS + 2] ||
+                                t.crg[NS + 1] != -t.crg[NS] / 2.0f))
+      fail(QB_ERR_UNSUPPORTED, "3-atom solvent whose two light sites differ or are not -1/2 the first site's charge");
+    const auto &H = t.iaclib[s.iac_hw];
+    bool h_lj = H.bvdw[0] != 0.0 || H.bvdw[1] != 0.0;
+    s.ww_hlj = (t.ivdw_rule == 2 || t.solvent_type == 1) && h_lj;
+    if (s.ww_hlj) {
+      int loh = s.ljcod[(size_t)s.iac_ow * t.natyps + s.iac_hw] - 1;
+      int lhh = s.ljcod[(size_t)s.iac_hw * t.natyps + s.iac_hw] - 1;
+      lj_pair(t.ivdw_rule == 2, O.avdw[loh], H.avdw[loh], O.bvdw[loh], H.bvdw[loh], s.A_OH, s.B_OH);
+      lj_pair(t.ivdw_rule == 2, H.avdw[lhh], H.avdw[lhh], H.bvdw[lhh], H.bvdw[lhh], s.A_HH, s.B_HH);
+    }
   }
   s.type_mass.resize(t.natyps); s.type_avdw.resize(3 * (size_t)t.natyps); s.type_bvdw.resize(3 * (size_t)t.natyps);
   for (int i = 0; i < t.natyps; i++) {
@@ -681,6 +693,7 @@ void System::fill_view(qb_sysview *v) const {
   v->imp_i = ii.data(); v->imp_j = ij.data(); v->imp_k = ik.data(); v->imp_l = il.data();
   v->imp_fk = ifk.data(); v->imp_imp0 = iimp0.data();
   v->crg_ow = crg_ow; v->crg_hw = crg_hw; v->A_OO = A_OO; v->B_OO = B_OO;
+  v->ww_hlj = ww_hlj; v->A_OH = A_OH; v->B_OH = B_OH; v->A_HH = A_HH; v->B_HH = B_HH;
   v->iac_ow = iac_ow; v->iac_hw = iac_hw;
   v->nwpolr_shell = (in.wpol_restr && nwat > 0) ? nwpolr_shell : 0;
   v->wshell_rout = ws_rout.data(); v->wshell_dr = ws_dr.data(); v->wshell_cstb = ws_cstb.data();

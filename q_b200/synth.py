@@ -96,6 +96,8 @@ class Topology:
     excl: list = field(default_factory=list)
     vdw_rule: int = 1                                # 1 geometric, 2 arithmetic
     ff_type: int = 2                                 # 1 GROMOS, 2 AMBER, 3 CHARMM (Urey-Bradley, harmonic impropers)
+    solvent_type: int = 0                            # 0 SPC-type water, 1 3-atom solvent (LJ on every site)
+    water_h_lj: tuple = (0.0, 0.0)                   # sigma, epsilon of the water hydrogens
 
     # ----------------------------------------------------------- writer
     def write(self, path: str) -> None:
@@ -167,13 +169,16 @@ class Topology:
             L.append(" ".join("%7.3f" % t.mass for t in self.types[k:k + 10]))
         cols = [t.columns(self.vdw_rule) for t in self.types]
         names = ("Aii", "Bii") if self.vdw_rule == 1 else ("R*ii", "epsilon ii")
-        fmt = "%8.2f" if self.vdw_rule == 1 else "%10.5f"
+        def fmt(v):   # geometric: 2 decimals, more for small non-zero values (light atoms' sqrt(A))
+            if self.vdw_rule == 2:
+                return "%10.5f" % v
+            return "%8.2f" % v if v == 0 or abs(v) >= 1 else "%10.7f" % v
         for c, label in enumerate(["normal", "polar", "1-4"]):
             for ab, nm in ((0, names[0]), (1, names[1])):
                 L.append(("sqrt (%s) %s:" if self.vdw_rule == 1 else "%s %s:") % (nm, label))
                 vals = [cols[t][c][ab] for t in range(nt)]
                 for k in range(0, nt, 8):
-                    L.append(" ".join(fmt % v for v in vals[k:k + 8]))
+                    L.append(" ".join(fmt(v) for v in vals[k:k + 8]))
         L.append("%8d = No. of type-2 vdW interactions. pairs: " % 0)
         ex_pairs, p14_pairs = self.excl14
         for pairs, label in ((p14_pairs, "1-4 neighbours"), (ex_pairs, "exclusions")):
@@ -208,7 +213,7 @@ class Topology:
         L.append("%8d = No. of SYBYL atom types:" % nt)
         for k in range(0, nt, 13):
             L.append(" ".join("%-5s" % "" for _ in self.types[k:k + 13]))
-        L.append("%8d = solvent type (0=SPC,1=3-atom,2=general)" % 0)
+        L.append("%8d = solvent type (0=SPC,1=3-atom,2=general)" % self.solvent_type)
         L.append("%8.3f%8.3f = Exclusion, solvent radii" % (self.rexcl_o, self.rwat))
         L.append("%8.3f%8.3f%8.3f = Solute center" % (0.0, 0.0, 0.0))
         L.append("%8.3f%8.3f%8.3f = Solvent center" % (0.0, 0.0, 0.0))
@@ -264,7 +269,7 @@ def _add_waters(top: Topology, waters: list[np.ndarray], excl_radius: float | No
     types = {t.name: i for i, t in enumerate(top.types)}
     if "OW" not in types:
         top.types.append(AtomType("OW", 15.999, SIG_O, EPS_O))
-        top.types.append(AtomType("HW", 1.008, 0.0, 0.0))
+        top.types.append(AtomType("HW", 1.008, *top.water_h_lj))
         types = {t.name: i for i, t in enumerate(top.types)}
     ow, hw = types["OW"], types["HW"]
     top.bond_lib.append((1106.0, R_OH))
@@ -539,12 +544,19 @@ def write_inp(path: str, top: str, fep: str | None, *, steps: int, stepsize: flo
         f.write("\n".join(L) + "\n")
 
 
+# water hydrogens with Lennard-Jones (sigma, epsilon), as CHARMM's TIP3P has them
+TIP3P_H_LJ = (0.4, 0.046)
+
+
 def water_sphere(outdir: str, radius: float = 15.0, seed: int = 1234, steps: int = 1000, name: str = "c0",
-                 stepsize: float = 1.0, vdw_rule: int = 1) -> Generated:
-    """Config 0: TIP3P sphere, 1 fs, energies every 10 steps."""
+                 stepsize: float = 1.0, vdw_rule: int = 1, water_h_lj=(0.0, 0.0), solvent_type: int = 0) -> Generated:
+    """Config 0: TIP3P sphere, 1 fs, energies every 10 steps.  water_h_lj
+    gives the hydrogens LJ; solvent_type 1 writes the water as 3-atom
+    solvent."""
     os.makedirs(outdir, exist_ok=True)
     rng = np.random.default_rng(seed)
-    top = Topology(title="water_sphere_%g" % radius, rexcl_o=radius, rwat=radius, vdw_rule=vdw_rule)
+    top = Topology(title="water_sphere_%g" % radius, rexcl_o=radius, rwat=radius, vdw_rule=vdw_rule,
+                   water_h_lj=tuple(water_h_lj), solvent_type=solvent_type)
     _add_waters(top, lattice_waters(radius, rng))
     top.excl = [False] * len(top.x)
     tp = os.path.join(outdir, name + ".top")
@@ -683,18 +695,20 @@ def perturbation(base: Generated, name: str, qatoms, charge_scale: float, eps_sc
 def fep_solute(outdir: str, radius: float = 20.0, seed: int = 1234, steps: int = 5000, name: str = "c1",
                lambdas=(0.5, 0.5), run_seed: int = 1, vdw_rule: int = 1, ff_type: int = 2,
                q_bonded: bool = False, ub_fk: float = 25.0, soft_pairs: int = 0,
-               library_charges: bool = False) -> Generated:
+               library_charges: bool = False, water_h_lj=(0.0, 0.0), solvent_type: int = 0) -> Generated:
     """Config 1: 56-atom solute with 8 two-state Q-atoms in a TIP3P sphere,
     2 fs with SHAKE on X-H bonds and water.  ff_type 3 writes it as a CHARMM
     topology (charmm_terms, Urey-Bradley constant ub_fk); q_bonded redefines the bonded terms among the
     Q atoms in the FEP file.  soft_pairs > 0 makes that many Q-atom pairs
-    beyond 1-4 soft pairs; library_charges sets qq_use_library_charges."""
+    beyond 1-4 soft pairs; library_charges sets qq_use_library_charges.
+    water_h_lj and solvent_type as for water_sphere."""
     os.makedirs(outdir, exist_ok=True)
     rng = np.random.default_rng(seed)
     X, kinds, bonds = random_tree_solute(rng)
     types, iac = _tree_types(kinds)
     n = len(X)
-    top = Topology(title="fep_solute", rexcl_o=radius, rwat=radius, types=types, vdw_rule=vdw_rule)
+    top = Topology(title="fep_solute", rexcl_o=radius, rwat=radius, types=types, vdw_rule=vdw_rule,
+                   water_h_lj=tuple(water_h_lj), solvent_type=solvent_type)
     top.x = [tuple(float(c) for c in p) for p in X]
     top.iac = iac
     top.crg = _solute_charges(rng, kinds)

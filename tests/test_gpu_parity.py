@@ -433,3 +433,56 @@ def test_soft_pairs_and_library_charges_match_oracle(qq_options, oracle):
             assert_energies(Eg[m], EQg[m], Eo[m], EQo[m])
         err = grad_err(b.gradient(k), o.gradient())
         assert err < G_TOL, (k, err, _worst_atoms(b.gradient(k), o.gradient()))
+
+
+@pytest.fixture(scope="module")
+def h_lj(tmp_path_factory):
+    """Water with Lennard-Jones on its hydrogens: under the arithmetic rule
+    (nonbon2_ww, nonbon2_qw) and as geometric-rule 3-atom solvent
+    (nonbond_3atomsolvent, nonbond_qw_3atom), a water sphere and the FEP
+    solute of each, and a plain SPC sphere."""
+    from q_b200 import synth
+    root = tmp_path_factory.mktemp("hlj")
+    h = synth.TIP3P_H_LJ
+    return {
+        "w_arith": synth.water_sphere(str(root / "wa"), radius=14.0, vdw_rule=2, water_h_lj=h),
+        "w_3atom": synth.water_sphere(str(root / "w3"), radius=14.0, solvent_type=1, water_h_lj=h),
+        "q_arith": synth.fep_solute(str(root / "qa"), vdw_rule=2, water_h_lj=h),
+        "q_3atom": synth.fep_solute(str(root / "q3"), solvent_type=1, water_h_lj=h),
+        "w_spc": synth.water_sphere(str(root / "ws"), radius=12.0),
+    }
+
+
+def test_water_hydrogen_lj_matches_oracle(h_lj, oracle):
+    """O-H and H-H Lennard-Jones in the water-water and Q-water terms (with
+    the hydrogens' own soft-core shift), five systems in one batch over 20
+    steps; the SPC sphere in that batch shows the variant leaves systems
+    without hydrogen LJ as they were."""
+    names = ["w_arith", "w_3atom", "q_arith", "q_3atom", "w_spc"]
+    systems = [System.open(h_lj[n].inp, lambdas=(0.4, 0.6) if n.startswith("q") else None, seed=7) for n in names]
+    assert [s.view.ww_hlj for s in systems] == [1, 1, 1, 1, 0]
+    b = Batch(systems, precision=FP64)
+    b.run(20)
+    for k, s in enumerate(systems):
+        o = oracle.create(s)
+        o.run(20)
+        sg, Eg, EQg = b.history(k, 0)
+        so, Eo, EQo = o.history(0)
+        assert list(sg) == list(so)
+        for m in range(len(sg)):
+            assert_energies(Eg[m], EQg[m], Eo[m], EQo[m])
+        err = grad_err(b.gradient(k), o.gradient())
+        assert err < G_TOL, (names[k], err, _worst_atoms(b.gradient(k), o.gradient()))
+
+
+def test_water_hydrogen_lj_mixed_precision(h_lj):
+    """The FP32 water-water variant with hydrogen LJ against FP64, as for
+    SPC water: within the mixed path's stated energy budget."""
+    s = System.open(h_lj["w_arith"].inp)
+    b64 = Batch([s], precision=FP64)
+    b32 = Batch([s], precision=MIXED)
+    b64.final_energy()
+    b32.final_energy()
+    e = dict(zip(E_NAMES, np.abs(b32.energy_vectors(0)[0] - b64.energy_vectors(0)[0])))
+    assert e["ww_el"] < 0.05 and e["ww_vdw"] < 0.05
+    assert grad_err(b32.gradient(0), b64.gradient(0)) < G_TOL

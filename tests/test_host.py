@@ -285,18 +285,3 @@ def test_reference_cases_open(golden):
             sizes[case] = (v.natom, v.nqat)
             assert (v.shake_constraints > 0) == shake
     assert sizes["w-w"] == (3423, 0) and sizes["q-p-w_Na"] == (3418, 1) and sizes["dualtop"] == (98, 98)
-
-
-def test_arithmetic_rule_water_with_hydrogen_lj_is_refused(tmp_path):
-    """nonbon2_ww adds LJ on all nine atom pairs of two waters; this path
-    takes O-O only, so waters whose hydrogens carry LJ are refused."""
-    g = synth.water_sphere(str(tmp_path / "w"), radius=12.0, vdw_rule=2)
-    top = open(g.top).read().split("\n")
-    k = next(i for i, l in enumerate(top) if l.startswith("epsilon ii normal"))
-    vals = top[k + 1].split()
-    vals[1] = "%10.5f" % 0.046           # HW epsilon
-    top[k + 1] = " ".join(vals)
-    open(g.top, "w").write("\n".join(top))
-    with pytest.raises(QBError) as e:
-        System.open(g.inp)
-    assert e.value.code == 4

@@ -147,6 +147,14 @@ int qb_batch_history(qb_batch *b, int sys, int kind, int *count, int *steps,
                      double *E, double *EQ);
 int qb_batch_clear_history(qb_batch *b);
 
+/* The off-diagonal elements of the same records: for every record and every
+ * off-diagonal function io of the system's FEP file, Hij = A exp(-mu r_kl)
+ * and r_kl, the distance of its two Q atoms at that step (offdiag,
+ * src/q6/md.f90:12911-12937).  out: count*noffd*2 doubles (Hij, r_kl), or
+ * NULL to query the count.  kind 2 gives one record: the values of the
+ * latest force evaluation in the run loop (those qdyn's final summary prints). */
+int qb_batch_offdiag(qb_batch *b, int sys, int kind, int *count, double *out);
+
 /* Run-time choices of the step kernels.  No counterpart in the reference
  * (qdyn has no tile sizes).  None changes the model: only the order in which
  * atomic sums add up, so results differ at rounding level. */
@@ -248,6 +256,11 @@ int qb_write_re(const char *path, int natom, const double *x, const double *v,
 /* Append one energy-file frame: per state a record (int32 state, 15 doubles)
  * and one empty off-diagonal record.  Replaces: put_ene, src/q6/nrgy.f90:94-119. */
 int qb_append_en(const char *path, int nstates, const double *EQ);
+
+/* The same frame with its off-diagonal record: noffd entries of (int32 i,
+ * int32 j, double Hij, double r_kl), nrgy.f90:60-65.  ij: 2*noffd state
+ * numbers (1-based); hr: 2*noffd doubles (Hij, r_kl). */
+int qb_append_en_offd(const char *path, int nstates, const double *EQ, int noffd, const int *ij, const double *hr);
 
 /* Maxwell-Boltzmann velocities drawn exactly as qdyn draws them: gauss (12
  * uniforms from randm) per component, sd = sqrt(boltz*T/mass), before initial

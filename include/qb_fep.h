@@ -8,8 +8,13 @@
  * the per-window arrays run 0..nfiles+1 with entry i belonging to file i
  * (1-based), exactly as qfep prints them (dG(ifile-1) beside lambda(ifile)).
  *
- * EVB couplings (qfep's predefined or parametrised off-diagonal elements) are
- * not part of this path: the ground-state energy is that of uncoupled states.
+ * EVB: with nnoffd > 0 the states are coupled through qfep's parametrised
+ * off-diagonal elements Hij(r) of the first off-diagonal distance r_xy that
+ * qdyn stored in each record (qfep.f90:160-172, 274-318); the ground-state
+ * energy is the lowest eigenvalue of the EVB matrix.  qfep's other mode,
+ * predefined elements read from the energy files (noffd > 0 on its first
+ * input line), reads no off-diagonal values there (nnoffd is never set) and
+ * is not part of this path.
  */
 #ifndef QB_FEP_H
 #define QB_FEP_H
@@ -21,7 +26,8 @@ extern "C" {
 #define QB_FEP_MAX_STATES 4     /* qfep's mxstates */
 #define QB_FEP_MAX_BINS 598     /* qfep's mxbin less the two spare bins */
 #define QB_FEP_BAR_MAX_ITER 1000
-#define QB_FEP_PART2_W 8        /* gap centre, dGv(1), dGv(2), dGg, points, c1^2, c2^2, printed (0/1) */
+#define QB_FEP_MAX_PAIRS 16     /* QB_FEP_MAX_STATES squared: the EVB parameter matrices */
+#define QB_FEP_PART2_W 9        /* gap centre, dGv(1), dGv(2), dGg, points, c1^2, c2^2, printed (0/1), <r_xy> */
 #define QB_FEP_PART3_W 8        /* gap centre, <dGg>, <dGg norm>, points, c1^2, c2^2, r_xy, printed (0/1) */
 
 /* Analysis parameters: qfep's interactive input (qfep.f90:87-172). */
@@ -33,6 +39,15 @@ typedef struct qb_fep_params {
   int nmin;                /* minimum points per bin */
   double alfa[QB_FEP_MAX_STATES];   /* shift of each state's total; alfa[0] is taken as 0 */
   double coeff[QB_FEP_MAX_STATES];  /* linear combination of states defining the energy gap */
+  /* EVB off-diagonal elements (qfep.f90:163-172, 286-299): for nnoffd > 0,
+   * Hij = A exp(-mu (r - rxy0)) exp(-eta (r - rxy0)^2) with the parameters of
+   * (i, j), or of (j, i) where A(i, j) is 0; matrices [i*4 + j], 0-based. */
+  int nnoffd;
+  double evb_A[QB_FEP_MAX_PAIRS];
+  double evb_mu[QB_FEP_MAX_PAIRS];
+  double evb_eta[QB_FEP_MAX_PAIRS];
+  double evb_rxy0[QB_FEP_MAX_PAIRS];
+  const double *rxy;       /* qb_fep_analyze with nnoffd > 0: r_xy of every record, file after file */
 } qb_fep_params;
 
 /* Results; every pointer is a caller-owned buffer of the stated size, or NULL

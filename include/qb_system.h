@@ -167,6 +167,11 @@ typedef struct qb_sysview {
   const double *qtor_fk, *qtor_rmult, *qtor_deltor;
   const int *qimp_i, *qimp_j, *qimp_k, *qimp_l; const unsigned char *qimp_on;
   const double *qimp_fk, *qimp_imp0;
+  /* EVB off-diagonal functions Hij = A exp(-mu r_kl) (qatom.f90:1515-1555; offdiag, md.f90:12911) */
+  int noffd;
+  const int *offd_i, *offd_j;  /* states, 1-based as the FEP and energy files give them */
+  const int *offd_k, *offd_l;  /* Q atoms, 0-based */
+  const double *offd_A, *offd_mu;
 
   /* ---- SHAKE (md.f90:2326 init_shake) ---- */
   int shake_molecules, shake_constraints;

@@ -13,7 +13,12 @@ loop by loop, in its order of summation, including its quirks:
 * BAR's sample-size ratios are single-precision quotients (qfep.f90:534-535);
 * the 2-state ground state uses the closed form even with no coupling
   (qfep.f90:300-306); more states take the smallest diagonal element (the
-  Householder/QL eigenvalues of a diagonal matrix);
+  Householder/QL eigenvalues of a diagonal matrix), or with EVB elements the
+  lowest eigenvalue of the matrix built from its lower triangle (tred2 reads
+  no other part), here from numpy's symmetric eigensolver;
+* EVB elements Hij(r) take the parameters of (i, j), or of (j, i) where
+  A(i, j) is 0, at the first off-diagonal distance of each record, and only
+  that first distance is averaged per bin (qfep.f90:274-299, 643-644);
 * bin indices use int() truncation and may reach nbins+1 (qfep.f90:628);
 * Part 3's minimum runs over every bin of the fixed-size array, so it is
   never above zero (qfep.f90:735);
@@ -43,6 +48,8 @@ class FepInput:
     nmin: int = 5
     alfa: list = field(default_factory=list)     # alpha of states 2..n (state 1 is 0)
     coeff: list = field(default_factory=list)    # linear combination defining the gap
+    evb: list = field(default_factory=list)      # [(i, j, A, mu, eta, rxy0)], states 1-based
+    rxy: list = field(default_factory=list)      # per file, r_xy of every record (EVB)
 
 
 @dataclass
@@ -91,7 +98,16 @@ def analyze(inp: FepInput) -> FepResult:
     lam = np.zeros((nfiles, ns))
     npts = np.zeros(nfiles, dtype=int)
     avEQ = np.zeros((nfiles, ns, NEQ))
-    V, VG, GAP = [], [], []
+    V, VG, GAP, C1, C2, RX = [], [], [], [], [], []
+    A, mu, eta, r0 = (np.zeros((4, 4)) for _ in range(4))
+    for i, j, a, m, e, r in inp.evb:
+        A[i - 1, j - 1], mu[i - 1, j - 1], eta[i - 1, j - 1], r0[i - 1, j - 1] = a, m, e, r
+    nnoffd = len(inp.evb)
+
+    def hij(i, j, r):      # qfep.f90:289-297, 0-based states
+        if A[i, j] == 0.0:
+            i, j = j, i
+        return A[i, j] * math.exp(-mu[i, j] * (r - r0[i, j])) * math.exp(-eta[i, j] * (r - r0[i, j]) ** 2)
     gapmin, gapmax = 999.0, -999.0
     for f, raw in enumerate(inp.energies):
         eq = np.array(raw, dtype=np.float64)
@@ -104,13 +120,25 @@ def analyze(inp: FepInput) -> FepResult:
         v = np.zeros((n, ns))
         vg = np.zeros(n)
         gap = np.zeros(n)
+        c1, c2 = np.zeros(n), np.zeros(n)
+        rx = np.array(inp.rxy[f], dtype=np.float64) if nnoffd > 0 else np.zeros(n)
         for ipt in range(n):
             if ipt + 1 > nskip:
                 acc += eq[ipt]
             tot = eq[ipt, :, I_TOTAL] + alfa
             v[ipt] = tot
             if ns == 2:
-                vg[ipt] = 0.5 * (tot[0] + tot[1]) - 0.5 * math.sqrt((tot[0] - tot[1]) ** 2 + 4.0 * 0.0 ** 2)
+                h = hij(0, 1, rx[ipt]) if nnoffd > 0 else 0.0
+                vg[ipt] = 0.5 * (tot[0] + tot[1]) - 0.5 * math.sqrt((tot[0] - tot[1]) ** 2 + 4.0 * h ** 2)
+                if nnoffd > 0:
+                    c1[ipt] = 1.0 / (1.0 + ((vg[ipt] - tot[0]) / h) ** 2)
+                    c2[ipt] = 1 - c1[ipt]
+            elif nnoffd > 0:
+                m = np.diag(tot)
+                for i in range(ns):
+                    for j in range(i):
+                        m[i, j] = m[j, i] = hij(i, j, rx[ipt])
+                vg[ipt] = float(np.min(np.linalg.eigvalsh(m)))
             else:
                 vg[ipt] = float(np.min(tot))
             g = 0.0
@@ -128,6 +156,9 @@ def analyze(inp: FepInput) -> FepResult:
         V.append(v)
         VG.append(vg)
         GAP.append(gap)
+        C1.append(c1)
+        C2.append(c2)
+        RX.append(rx)
 
     z = lambda: np.zeros(nfiles + 2)
     dgf, dgfsum, dgr, dgrsum, dG = z(), z(), z(), z(), z()
@@ -247,12 +278,17 @@ def analyze(inp: FepInput) -> FepResult:
                     veff = veff + lam[f, st] * V[f][ipt, st]
                 avdvv[:, ib] += V[f][ipt] - veff
                 avdvg[ib] += VG[f][ipt] - veff
+                avc1[ib] += C1[f][ipt]
+                avc2[ib] += C2[f][ipt]
+                if nnoffd > 0:
+                    avr[ib] += RX[f][ipt]
                 nbinpts[ib] += 1
             for ib in range(1, nbins + 1):
                 if nbinpts[ib] != 0:
-                    avc1[ib] /= nbinpts[ib]
-                    avc2[ib] /= nbinpts[ib]
-                    avr[ib] /= nbinpts[ib]
+                    rn = float(np.float32(nbinpts[ib]))      # /real(nbinpts)
+                    avc1[ib] /= rn
+                    avc2[ib] /= rn
+                    avr[ib] /= rn
                     avdvv[:, ib] /= nbinpts[ib]
                     avdvg[ib] /= nbinpts[ib]
             for ipt in range(nskip, npts[f]):

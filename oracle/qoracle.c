@@ -53,7 +53,8 @@ struct qo_state {
   /* history */
   int hcap, hcount[2];
   int *hstep[2];
-  double *hE[2], *hEQ[2];
+  double *hE[2], *hEQ[2], *hR[2];
+  double offd_r[QB_MAX_STATES];     /* r_kl of this step's off-diagonal functions */
   double ekinmax;
   double kinetic;
 };
@@ -1304,10 +1305,21 @@ static int shake(qo_state *st, const double *xx, double *x) {
   return 0;
 }
 
+/* offdiag (md.f90:12911): distance of each off-diagonal function's Q atoms */
+static void offdiag(qo_state *st) {
+  const qb_sysview *s = st->s;
+  for (int io = 0; io < s->noffd; io++) {
+    int k = s->iqseq[s->offd_k[io]], l = s->iqseq[s->offd_l[io]];
+    st->offd_r[io] = sqrt((X(l, 0) - X(k, 0)) * (X(l, 0) - X(k, 0)) + (X(l, 1) - X(k, 1)) * (X(l, 1) - X(k, 1)) +
+                          (X(l, 2) - X(k, 2)) * (X(l, 2) - X(k, 2)));
+  }
+}
+
 static void record(qo_state *st, int kind) {
   int S = st->S;
   int c = st->hcount[kind];
   if (c >= st->hcap) return;
+  memcpy(&st->hR[kind][(size_t)c * QB_MAX_STATES], st->offd_r, QB_MAX_STATES * sizeof(double));
   st->hstep[kind][c] = st->istep;
   memcpy(&st->hE[kind][(size_t)c * QB_NE], st->E, QB_NE * sizeof(double));
   memcpy(&st->hEQ[kind][(size_t)c * S * QB_NEQ], st->EQ, (size_t)S * QB_NEQ * sizeof(double));
@@ -1349,6 +1361,7 @@ qo_state *qo_create(const qb_sysview *s, int history_capacity) {
     st->hstep[k] = (int *)malloc((size_t)(history_capacity + 1) * sizeof(int));
     st->hE[k] = (double *)malloc((size_t)(history_capacity + 1) * QB_NE * sizeof(double));
     st->hEQ[k] = (double *)malloc((size_t)(history_capacity + 1) * (st->S + 1) * QB_NEQ * sizeof(double));
+    st->hR[k] = (double *)calloc((size_t)(history_capacity + 1) * QB_MAX_STATES, sizeof(double));
   }
   /* md_run start: initial temperature (md.f90:3960-3963) */
   st->Tscale_solute = st->Tscale_solvent = 1.0;
@@ -1363,7 +1376,7 @@ void qo_destroy(qo_state *st) {
   free(st->pp); free(st->pw); free(st->ww); free(st->qp); free(st->qw); free(st->lrf);
   free(st->theta_corr); free(st->avtheta); free(st->avn_insh); free(st->n_insh);
   free(st->list_sh); free(st->nsort); free(st->theta); free(st->theta0); free(st->tdum);
-  for (int k = 0; k < 2; k++) { free(st->hstep[k]); free(st->hE[k]); free(st->hEQ[k]); }
+  for (int k = 0; k < 2; k++) { free(st->hstep[k]); free(st->hE[k]); free(st->hEQ[k]); free(st->hR[k]); }
   free(st);
 }
 
@@ -1374,6 +1387,7 @@ int qo_run(qo_state *st, int nsteps) {
   for (int n = 0; n < nsteps; n++) {
     if (st->istep % s->NBcycle == 0) make_pair_lists(st);
     pot_energy(st);
+    if (s->noffd > 0) offdiag(st);
     st->E[QB_E_KINETIC] = st->kinetic;
     for (int i = 0; i < st->N; i++) {
       double ts = i < st->NS ? st->Tscale_solute : st->Tscale_solvent;
@@ -1427,6 +1441,13 @@ int qo_history(const qo_state *st, int kind, int *steps, double *E, double *EQ) 
   if (steps) memcpy(steps, st->hstep[kind], (size_t)c * sizeof(int));
   if (E) memcpy(E, st->hE[kind], (size_t)c * QB_NE * sizeof(double));
   if (EQ) memcpy(EQ, st->hEQ[kind], (size_t)c * st->S * QB_NEQ * sizeof(double));
+  return c;
+}
+/* r_kl of every record's off-diagonal functions: count*noffd doubles */
+int qo_offdiag(const qo_state *st, int kind, double *rkl) {
+  int c = st->hcount[kind], n = st->s->noffd;
+  for (int r = 0; r < c; r++)
+    for (int io = 0; io < n; io++) rkl[(size_t)r * n + io] = st->hR[kind][(size_t)r * QB_MAX_STATES + io];
   return c;
 }
 /* pair counts of the current lists: pp, pw, ww molecule pairs, qp, qw waters */

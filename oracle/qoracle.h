@@ -26,6 +26,7 @@ void qo_set_velocities(qo_state *st, const double *v);
 void qo_theta_corr(const qo_state *st, float *tc);
 void qo_temperature(const qo_state *st, double *out);
 int qo_history(const qo_state *st, int kind, int *steps, double *E, double *EQ);
+int qo_offdiag(const qo_state *st, int kind, double *rkl);
 void qo_list_counts(const qo_state *st, int *out);
 int qo_status(const qo_state *st);
 #endif

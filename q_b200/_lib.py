@@ -126,6 +126,7 @@ def _load():
         "qb_batch_set_velocities": (C.c_int, [vp, C.c_int, dp]),
         "qb_batch_get_theta_corr": (C.c_int, [vp, C.c_int, fp, C.c_int]),
         "qb_batch_history": (C.c_int, [vp, C.c_int, C.c_int, ip, ip, dp, dp]),
+        "qb_batch_offdiag": (C.c_int, [vp, C.c_int, C.c_int, ip, dp]),
         "qb_batch_clear_history": (C.c_int, [vp]),
         "qb_batch_status": (C.c_int, [vp, C.c_int, ip]),
         "qb_batch_get_tuning": (C.c_int, [vp, C.c_void_p]),
@@ -138,6 +139,7 @@ def _load():
         "qb_batch_destroy": (None, [vp]),
         "qb_write_re": (C.c_int, [C.c_char_p, C.c_int, dp, dp, C.c_int, fp]),
         "qb_append_en": (C.c_int, [C.c_char_p, C.c_int, dp]),
+        "qb_append_en_offd": (C.c_int, [C.c_char_p, C.c_int, dp, C.c_int, ip, dp]),
         "qb_fep_analyze": (C.c_int, [dp, ip, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
         "qb_batch_fep": (C.c_int, [vp, ip, C.c_int, C.c_void_p, C.c_void_p]),
         "qb_mlp_forward": (C.c_int, [fp, fp, C.c_int, fp, C.c_int]),

@@ -164,6 +164,16 @@ class Batch:
                                    steps.ctypes.data_as(C.POINTER(C.c_int)), _dp(E), _dp(EQ)))
         return steps[:n], E[:n], EQ[:n, :S]
 
+    def offdiag(self, sys: int, kind: int = 0) -> np.ndarray:
+        """[n, noffd, 2] (Hij, r_kl) of the records history() returns, for the
+        system's EVB off-diagonal functions (offdiag, md.f90:12911)."""
+        cnt = C.c_int()
+        check(lib.qb_batch_offdiag(self._b, sys, kind, C.byref(cnt), None))
+        n, m = cnt.value, self.systems[sys].view.noffd
+        out = np.zeros(max(n * m * 2, 1))
+        check(lib.qb_batch_offdiag(self._b, sys, kind, C.byref(cnt), _dp(out)))
+        return out[:n * m * 2].reshape(n, m, 2)
+
     def clear_history(self) -> None:
         check(lib.qb_batch_clear_history(self._b))
 
@@ -248,9 +258,18 @@ def write_restart(path: str, x: np.ndarray, v: np.ndarray, theta_corr: np.ndarra
                           tc.ctypes.data_as(C.POINTER(C.c_float)) if tc is not None else None))
 
 
-def append_energy(path: str, EQ: np.ndarray) -> None:
+def append_energy(path: str, EQ: np.ndarray, offd=None) -> None:
+    """One energy-file frame; offd = (ij[noffd, 2] state numbers, hr[noffd, 2]
+    of Hij and r_kl) fills its off-diagonal record."""
     EQ = np.ascontiguousarray(EQ, dtype=np.float64)
-    check(lib.qb_append_en(path.encode(), EQ.shape[0] if EQ.ndim == 2 else 0, _dp(EQ)))
+    ns = EQ.shape[0] if EQ.ndim == 2 else 0
+    if offd is None or len(offd[0]) == 0:
+        check(lib.qb_append_en(path.encode(), ns, _dp(EQ)))
+        return
+    ij = np.ascontiguousarray(offd[0], dtype=np.int32)
+    hr = np.ascontiguousarray(offd[1], dtype=np.float64)
+    check(lib.qb_append_en_offd(path.encode(), ns, _dp(EQ), ij.shape[0], ij.ctypes.data_as(C.POINTER(C.c_int)),
+                                _dp(hr)))
 
 
 def maxwell(seed: int, temperature: float, mass: np.ndarray) -> np.ndarray:

@@ -96,7 +96,15 @@ int qb_write_re(const char *path, int natom, const double *x, const double *v, i
 
 int qb_append_en(const char *path, int nstates, const double *EQ) {
   if (!path || nstates < 0 || (nstates > 0 && !EQ)) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
-  return guarded([&] { qb::append_energy_frame(path, nstates, EQ); });
+  return guarded([&] { qb::append_energy_frame(path, nstates, EQ, 0, nullptr, nullptr); });
+}
+
+int qb_append_en_offd(const char *path, int nstates, const double *EQ, int noffd, const int *ij, const double *hr) {
+  if (!path || nstates < 0 || (nstates > 0 && !EQ) || noffd < 0 || (noffd > 0 && (!ij || !hr))) {
+    qb::set_error("invalid argument");
+    return QB_ERR_ARG;
+  }
+  return guarded([&] { qb::append_energy_frame(path, nstates, EQ, noffd, ij, hr); });
 }
 
 // Maxwell-Boltzmann velocities exactly as maxwell/gauss/randm draw them

@@ -584,6 +584,12 @@ void build(Batch &B, qb_handle *const *hs, int n) {
         qipar.push_back(on ? make_double2(V.qimp_fk[k * NSt + st], V.qimp_imp0[k * NSt + st]) : make_double2(0, 0));
       }
     }
+    S.noffd = V.noffd;
+    if (S.noffd > MAXS) fail(QB_ERR_ARG, "too many off-diagonal functions");
+    for (int k = 0; k < V.noffd; k++) {
+      S.offd_k[k] = aoff + V.iqseq[V.offd_k[k]];
+      S.offd_l[k] = aoff + V.iqseq[V.offd_l[k]];
+    }
     // shake molecules
     S.sh_off = (int)sh_first.size(); S.nsh = V.shake_molecules;
     for (int m = 0; m < V.shake_molecules; m++) {
@@ -732,7 +738,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     B.any_wpol |= S.wpol != 0;
     B.any_prestr |= (V.nrstr_seq + V.nrstr_pos + V.nrstr_dist + V.nrstr_angl + V.nrstr_wall) > 0;
     B.any_qq |= S.nqq > 0;
-    B.any_qb |= (V.nqbond + V.nqangle + V.nqtor + V.nqimp) > 0;
+    B.any_qb |= (V.nqbond + V.nqangle + V.nqtor + V.nqimp + V.noffd) > 0;   // the Q-bonded block also takes r_kl
     B.any_hlj |= V.nwat > 0 && V.ww_hlj;
   }
   // water offsets
@@ -884,6 +890,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   P.kin = dev_alloc<double>((size_t)n * 4, o);
   P.E = dev_alloc<double>((size_t)n * QB_NE, o);
   P.EQ = dev_alloc<double>((size_t)n * MAXS * QB_NEQ, o);
+  P.offd_r = dev_alloc<double>((size_t)n * MAXS, o);
   P.hist = nullptr;
   P.hist_cap = 0;
   B.watpol_smem = (size_t)B.max_nwat * (sizeof(double) + sizeof(int));   // member angles and indices
@@ -913,7 +920,7 @@ void ensure_history(Batch &B, int nsteps) {
   for (auto &x : st) used = std::max(used, std::max(x.hist_n[0], x.hist_n[1]));
   long long cap = used + need;
   if (cap <= B.P.hist_cap) return;
-  size_t rec = QB_NE + MAXS * QB_NEQ + 1;
+  size_t rec = HIST_REC;
   double *nh = nullptr;
   CUDA_TRY(cudaMalloc(&nh, sizeof(double) * rec * cap * 2 * B.nsys));
   CUDA_TRY(cudaMemset(nh, 0, sizeof(double) * rec * cap * 2 * B.nsys));
@@ -1211,7 +1218,7 @@ int qb_batch_fep(qb_batch *bb, const int *sys, int nfiles, const qb_fep_params *
     std::vector<qb::SysState> st(B.nsys);
     CUDA_TRY(cudaMemcpy(st.data(), B.P.st, sizeof(qb::SysState) * B.nsys, cudaMemcpyDeviceToHost));
     // energy-file records (kind 1) of each system, read in place in the ring
-    const long long rec_len = QB_NE + qb::MAXS * QB_NEQ + 1;
+    const long long rec_len = qb::HIST_REC;
     qb::FepSource src;
     src.base = B.P.hist;
     src.rec_stride = (int)rec_len;
@@ -1224,7 +1231,13 @@ int qb_batch_fep(qb_batch *bb, const int *sys, int nfiles, const qb_fep_params *
       if (!B.P.hist) qb::fail(QB_ERR_STATE, "no energy records: run the batch first");
       src.foff.push_back((((long long)B.nsys + s) * B.P.hist_cap) * rec_len + 1 + QB_NE);
       src.npts.push_back(std::min(st[s].hist_n[1], B.P.hist_cap));
+      // EVB: the first off-diagonal function's r_kl of each record
+      if (p->nnoffd > 0 && B.views[s].noffd < p->nnoffd)
+        qb::fail(QB_ERR_ARG, "system " + std::to_string(s) + " has fewer off-diagonal functions than requested");
+      src.rfoff.push_back((((long long)B.nsys + s) * B.P.hist_cap) * rec_len + 1 + QB_NE + qb::MAXS * QB_NEQ);
     }
+    src.rbase = B.P.hist;
+    src.r_stride = (int)rec_len;
     qb::fep_run(src, *p, B.opt.device, B.stream, out);
   });
 }
@@ -1325,7 +1338,7 @@ int qb_batch_history(qb_batch *bb, int sys, int kind, int *count, int *steps, do
     int c = std::min(st.hist_n[kind], B.P.hist_cap);
     *count = c;
     if (c == 0 || (!steps && !E && !EQ)) return;
-    size_t rec = QB_NE + qb::MAXS * QB_NEQ + 1;
+    size_t rec = qb::HIST_REC;
     std::vector<double> h(rec * c);
     CUDA_TRY(cudaMemcpy(h.data(), B.P.hist + (((size_t)kind * B.nsys + sys) * B.P.hist_cap) * rec,
                         sizeof(double) * rec * c, cudaMemcpyDeviceToHost));
@@ -1336,6 +1349,36 @@ int qb_batch_history(qb_batch *bb, int sys, int kind, int *count, int *steps, do
       if (E) std::memcpy(E + (size_t)r * QB_NE, p + 1, sizeof(double) * QB_NE);
       if (EQ && S > 0) std::memcpy(EQ + (size_t)r * S * QB_NEQ, p + 1 + QB_NE, sizeof(double) * S * QB_NEQ);
     }
+  });
+}
+
+int qb_batch_offdiag(qb_batch *bb, int sys, int kind, int *count, double *out) {
+  if (int rc = sys_check(bb, sys)) return rc;
+  if (kind < 0 || kind > 2 || !count) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
+  return guarded_batch([&] {
+    Batch &B = bb->b;
+    qb::SysState st;
+    CUDA_TRY(cudaStreamSynchronize(B.stream));
+    CUDA_TRY(cudaMemcpy(&st, B.P.st + sys, sizeof st, cudaMemcpyDeviceToHost));
+    const qb_sysview &V = B.views[sys];
+    // kind 2: the values of the latest force evaluation, as one record
+    int c = kind == 2 ? 1 : std::min(st.hist_n[kind], B.P.hist_cap);
+    *count = c;
+    if (c == 0 || !out || V.noffd == 0) return;
+    size_t rec = qb::HIST_REC, roff = 1 + QB_NE + qb::MAXS * QB_NEQ;
+    std::vector<double> h(rec * c);
+    if (kind == 2)
+      CUDA_TRY(cudaMemcpy(h.data() + roff, B.P.offd_r + (size_t)sys * qb::MAXS, sizeof(double) * qb::MAXS,
+                          cudaMemcpyDeviceToHost));
+    else
+      CUDA_TRY(cudaMemcpy(h.data(), B.P.hist + (((size_t)kind * B.nsys + sys) * B.P.hist_cap) * rec,
+                          sizeof(double) * rec * c, cudaMemcpyDeviceToHost));
+    for (int r = 0; r < c; r++)
+      for (int io = 0; io < V.noffd; io++) {
+        double rkl = h[rec * r + roff + io];
+        out[((size_t)r * V.noffd + io) * 2] = V.offd_A[io] * std::exp(-V.offd_mu[io] * rkl);
+        out[((size_t)r * V.noffd + io) * 2 + 1] = rkl;
+      }
   });
 }
 

@@ -20,6 +20,8 @@ constexpr int MAXS = QB_MAX_STATES;
 // (xxx,xxy,xxz,xyy,xyz,xzz,yyy,yyz,yzz,zzz), pad.
 constexpr int LRF_STRIDE = 24;
 constexpr int MAX_SHELLS = 4;
+// one history record: step, E[QB_NE], EQ[MAXS*QB_NEQ], r_kl of the off-diagonal functions [MAXS]
+constexpr int HIST_REC = 1 + QB_NE + MAXS * QB_NEQ + MAXS;
 constexpr int NQ_SHARED = 64;    // Q atoms whose water forces are reduced in shared memory
 enum AtomFlags : uint8_t { F_EXCL = 1, F_SHELL = 2, F_HEAVY = 4, F_SHAKE = 8 };   // F_SHAKE: in a SHAKE constraint
 
@@ -41,6 +43,7 @@ struct SysDev {
   // static term ranges (global offsets into term arrays)
   int b_off, nb, nb_sol, a_off, na, na_sol, t_off, nt, nt_sol, i_off, ni, ni_sol;
   int qb_off, nqb, qa_off, nqa, qt_off, nqt, qi_off, nqi;
+  int noffd, offd_k[MAXS], offd_l[MAXS];   // off-diagonal functions: their Q atoms (batch atom index)
   int qq_off, nqq;            // flattened nbqq entries of all states
   int sh_off, nsh;            // shake molecules
   int rs_off, nrs, rp_off, nrp, rd_off, nrd, ra_off, nra, rw_off, nrw;
@@ -153,6 +156,7 @@ struct DevPtrs {
   int kin_nblk;
   double *E;                               // [s*QB_NE]
   double *EQ;                              // [(s*MAXS + st)*QB_NEQ]
+  double *offd_r;                          // [s*MAXS + io] r_kl of this step's off-diagonal functions
   // history [kind][s][rec][QB_NE + MAXS*QB_NEQ + 1]
   double *hist;
   int hist_cap;

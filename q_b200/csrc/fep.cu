@@ -42,6 +42,12 @@ struct FepDev {
   double alfa[QB_FEP_MAX_STATES], coeff[QB_FEP_MAX_STATES];
   double *lam;                // [nfiles*ns]
   double *V, *VG, *GAP;       // per point: shifted state totals, ground state, gap
+  // EVB: r_xy of record p of file f at R[roff[f] + p*rrs]; Hij parameters [i*4+j]
+  const double *R;
+  const long long *roff;
+  int rrs, nnoffd;
+  double hA[QB_FEP_MAX_PAIRS], hmu[QB_FEP_MAX_PAIRS], heta[QB_FEP_MAX_PAIRS], hr0[QB_FEP_MAX_PAIRS];
+  double *C1, *C2, *RX;       // per point: c1^2, c2^2 (two coupled states), r_xy
 };
 
 __device__ __forceinline__ const double *rec(const FepDev &D, int f, int p, int st) {
@@ -81,8 +87,56 @@ __device__ double block_sum_d(double v) {
   return total;
 }
 
+// Lowest eigenvalue of a symmetric n x n matrix (n <= 4) by cyclic Jacobi
+// rotations (Golub and Van Loan, Matrix Computations, 4th ed., 8.5.2-8.5.3):
+// each rotation zeroes one off-diagonal element; sweeps until the
+// off-diagonal mass is negligible against the matrix's.
+__device__ double min_eigen(double (&a)[QB_FEP_MAX_STATES][QB_FEP_MAX_STATES], int n) {
+  double fro = 0.0;
+  for (int p = 0; p < n; p++)
+    for (int q = 0; q < n; q++) fro += a[p][q] * a[p][q];
+  for (int sweep = 0; sweep < 64; sweep++) {
+    double off = 0.0;
+    for (int p = 0; p < n; p++)
+      for (int q = p + 1; q < n; q++) off += a[p][q] * a[p][q];
+    if (off <= 1e-32 * fro) break;
+    for (int p = 0; p < n - 1; p++)
+      for (int q = p + 1; q < n; q++) {
+        if (fabs(a[p][q]) < 1e-300) continue;
+        const double tau = (a[q][q] - a[p][p]) / (2.0 * a[p][q]);
+        const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+        const double c = 1.0 / sqrt(1.0 + t * t), s = t * c;
+        for (int k = 0; k < n; k++) {
+          const double akp = a[k][p], akq = a[k][q];
+          a[k][p] = c * akp - s * akq;
+          a[k][q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < n; k++) {
+          const double apk = a[p][k], aqk = a[q][k];
+          a[p][k] = c * apk - s * aqk;
+          a[q][k] = s * apk + c * aqk;
+        }
+      }
+  }
+  double m = a[0][0];
+  for (int k = 1; k < n; k++) m = fmin(m, a[k][k]);
+  return m;
+}
+
+// qfep's off-diagonal element of states i, j (0-based) at distance r: the
+// parameters of (i, j), or of (j, i) where A(i, j) is 0 (qfep.f90:289-297).
+__device__ __forceinline__ double evb_hij(const FepDev &D, int i, int j, double r) {
+  int a = i * QB_FEP_MAX_STATES + j;
+  if (D.hA[a] == 0.0) a = j * QB_FEP_MAX_STATES + i;
+  const double d = r - D.hr0[a];
+  return D.hA[a] * exp(-D.hmu[a] * d) * exp(-D.heta[a] * d * d);
+}
+
 // Per point (qfep.f90:257-322): shifted totals, ground state, energy gap;
-// the file's lambdas from its first record.
+// the file's lambdas from its first record.  With EVB coupling the ground
+// state of two states is the lower root of the 2 x 2 secular equation, with
+// the weights c1^2, c2^2 of the diabatic states; of more states, the lowest
+// eigenvalue of the EVB matrix (qfep.f90:310-318).
 __global__ void k_fep_values(FepDev D) {
   const int f = blockIdx.y;
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -95,15 +149,31 @@ __global__ void k_fep_values(FepDev D) {
   }
   const int q = D.pstart[f] + p;
   for (int st = 0; st < D.ns; st++) D.V[(size_t)q * D.ns + st] = tot[st];
-  double vg;
+  double vg, c1 = 0.0, c2 = 0.0, rx = 0.0;
+  if (D.nnoffd > 0) rx = D.R[D.roff[f] + (long long)p * D.rrs];
   if (D.ns == 2) {
-    const double hij = 0.0;   // uncoupled states
+    const double hij = D.nnoffd > 0 ? evb_hij(D, 0, 1, rx) : 0.0;   // uncoupled without EVB
     vg = 0.5 * (tot[0] + tot[1]) - 0.5 * sqrt((tot[0] - tot[1]) * (tot[0] - tot[1]) + 4. * hij * hij);
+    if (D.nnoffd > 0) {
+      const double x = (vg - tot[0]) / hij;
+      c1 = 1. / (1. + x * x);
+      c2 = 1 - c1;
+    }
+  } else if (D.nnoffd > 0 && D.ns > 2) {
+    double m[QB_FEP_MAX_STATES][QB_FEP_MAX_STATES];
+    for (int i = 0; i < D.ns; i++) {
+      m[i][i] = tot[i];
+      for (int j = 0; j < i; j++) m[i][j] = m[j][i] = evb_hij(D, i, j, rx);   // the lower triangle
+    }
+    vg = min_eigen(m, D.ns);
   } else {
     vg = tot[0];
     for (int st = 1; st < D.ns; st++) vg = fmin(vg, tot[st]);
   }
   D.VG[q] = vg;
+  D.C1[q] = c1;
+  D.C2[q] = c2;
+  D.RX[q] = rx;
   double g = 0.0;
   for (int st = 0; st < D.ns; st++) g = g + tot[st] * D.coeff[st];
   D.GAP[q] = g;
@@ -269,9 +339,13 @@ __global__ void k_fep_bins(FepDev D, const double *range, const double *dG, doub
   double *adg = adv + nb * ns;          // [nb]
   double *sv = adg + nb;                // [nb*ns]
   double *sg = sv + nb * ns;            // [nb]
-  int *cnt = (int *)(sg + nb);          // [nb]
+  double *ac1 = sg + nb, *ac2 = ac1 + nb, *arx = ac2 + nb;   // [nb] each: c1^2, c2^2, r_xy
+  int *cnt = (int *)(arx + nb);         // [nb]
   for (int t = threadIdx.x; t < nb * ns; t += blockDim.x) { adv[t] = 0.0; sv[t] = 0.0; }
-  for (int t = threadIdx.x; t < nb; t += blockDim.x) { adg[t] = 0.0; sg[t] = 0.0; cnt[t] = 0; }
+  for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+    adg[t] = 0.0; sg[t] = 0.0; cnt[t] = 0;
+    ac1[t] = 0.0; ac2[t] = 0.0; arx[t] = 0.0;
+  }
   __syncthreads();
   const double gapmin = range[0], xint = (range[1] - range[0]) / (double)D.nbins;
   const double rt = D.rt;
@@ -281,6 +355,9 @@ __global__ void k_fep_bins(FepDev D, const double *range, const double *dG, doub
     const double ve = veff(D, f, f, p);
     for (int st = 0; st < ns; st++) atomicAdd(&adv[ib * ns + st], D.V[(size_t)q * ns + st] - ve);
     atomicAdd(&adg[ib], D.VG[q] - ve);
+    atomicAdd(&ac1[ib], D.C1[q]);
+    atomicAdd(&ac2[ib], D.C2[q]);
+    if (D.nnoffd > 0) atomicAdd(&arx[ib], D.RX[q]);   // only the first r_xy (qfep.f90:643-644)
     atomicAdd(&cnt[ib], 1);
   }
   __syncthreads();
@@ -288,6 +365,10 @@ __global__ void k_fep_bins(FepDev D, const double *range, const double *dG, doub
     if (cnt[ib] != 0) {
       for (int st = 0; st < ns; st++) adv[ib * ns + st] /= cnt[ib];
       adg[ib] /= cnt[ib];
+      const double rn = (double)(float)cnt[ib];   // /real(nbinpts)
+      ac1[ib] /= rn;
+      ac2[ib] /= rn;
+      arx[ib] /= rn;
     }
   __syncthreads();
   for (int p = D.nskip + threadIdx.x; p < D.npts[f]; p += blockDim.x) {
@@ -310,7 +391,10 @@ __global__ void k_fep_bins(FepDev D, const double *range, const double *dG, doub
     if (ns > 1) r[2] = dgf + (-rt * log(sv[ib * ns + 1] / n) + adv[ib * ns + 1]);
     r[3] = dgf + (-rt * log(sg[ib] / n) + adg[ib]);
     r[4] = n;
+    r[5] = ac1[ib];
+    r[6] = ac2[ib];
     r[7] = 1.0;
+    r[8] = arx[ib];
   }
 }
 
@@ -361,12 +445,18 @@ void fep_run(const FepSource &src, const qb_fep_params &p, int device, cudaStrea
   DevBuf<long long> d_foff(nfiles);
   DevBuf<int> d_npts(nfiles), d_pstart(nfiles), d_its(nfiles + 2);
   DevBuf<double> d_lam((size_t)nfiles * ns), d_V((size_t)P * ns), d_VG(P), d_GAP(P);
+  DevBuf<double> d_C1(P), d_C2(P), d_RX(P);
+  DevBuf<long long> d_roff(nfiles);
+  if (p.nnoffd < 0) fail(QB_ERR_ARG, "negative number of off-diagonal elements");
+  if (p.nnoffd > 0 && (!src.rbase || (int)src.rfoff.size() != nfiles))
+    fail(QB_ERR_ARG, "off-diagonal elements without r_xy values");
   DevBuf<double> d_av((size_t)nfiles * ns * QB_NEQ), d_range(2);
   DevBuf<double> d_dgf(nfiles + 2), d_dgr(nfiles + 2), d_dgti(nfiles + 2), d_dglu(nfiles + 2), d_dgbar(nfiles + 2);
   DevBuf<double> d_dG(nfiles + 2), d_part2((size_t)nfiles * nb * QB_FEP_PART2_W);
   put(d_foff.p, src.foff, stream);
   put(d_npts.p, src.npts, stream);
   put(d_pstart.p, pstart, stream);
+  if (p.nnoffd > 0) put(d_roff.p, src.rfoff, stream);
   for (auto *b : {d_dgf.p, d_dgr.p, d_dgti.p, d_dglu.p, d_dgbar.p})
     FEP_CUDA(cudaMemsetAsync(b, 0, sizeof(double) * (nfiles + 2), stream));
   FEP_CUDA(cudaMemsetAsync(d_its.p, 0, sizeof(int) * (nfiles + 2), stream));
@@ -380,6 +470,11 @@ void fep_run(const FepSource &src, const qb_fep_params &p, int device, cudaStrea
     D.coeff[st] = p.coeff[st];
   }
   D.lam = d_lam.p; D.V = d_V.p; D.VG = d_VG.p; D.GAP = d_GAP.p;
+  D.C1 = d_C1.p; D.C2 = d_C2.p; D.RX = d_RX.p;
+  D.nnoffd = p.nnoffd; D.R = src.rbase; D.roff = d_roff.p; D.rrs = src.r_stride;
+  for (int k = 0; k < QB_FEP_MAX_PAIRS; k++) {
+    D.hA[k] = p.evb_A[k]; D.hmu[k] = p.evb_mu[k]; D.heta[k] = p.evb_eta[k]; D.hr0[k] = p.evb_rxy0[k];
+  }
 
   k_fep_values<<<dim3((maxn + FEP_BLOCK - 1) / FEP_BLOCK, nfiles), FEP_BLOCK, 0, stream>>>(D);
   k_fep_part0<<<nfiles, 64, 0, stream>>>(D, d_av.p);
@@ -411,7 +506,7 @@ void fep_run(const FepSource &src, const qb_fep_params &p, int device, cudaStrea
 
   // Part 2 on the device, Part 3 (qfep.f90:721-745) from its rows in file order
   put(d_dG.p, dG, stream);
-  const size_t smem = (size_t)nb * (2 * ns + 2) * sizeof(double) + (size_t)nb * sizeof(int);
+  const size_t smem = (size_t)nb * (2 * ns + 5) * sizeof(double) + (size_t)nb * sizeof(int);
   if (smem > 48 * 1024)
     FEP_CUDA(cudaFuncSetAttribute(k_fep_bins, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_fep_bins<<<nfiles, FEP_BLOCK, smem, stream>>>(D, d_range.p, d_dG.p, d_part2.p);
@@ -429,7 +524,7 @@ void fep_run(const FepSource &src, const qb_fep_params &p, int device, cudaStrea
       const int n = (int)r[4];
       binsum[ib * 4 + 1] += r[5] * n;
       binsum[ib * 4 + 2] += r[6] * n;
-      binsum[ib * 4 + 3] += 0.0 * n;
+      binsum[ib * 4 + 3] += r[8] * n;
       ptsum[ib] += n;
       binsum[ib * 4 + 0] += r[3] * n;
     }
@@ -486,15 +581,25 @@ extern "C" int qb_fep_analyze(const double *energies, const int *npts, int nfile
       total += npts[f];
     }
     if (nstates < 1 || nstates > QB_FEP_MAX_STATES) qb::fail(QB_ERR_ARG, "number of states must be 1..4");
+    if (p->nnoffd > 0 && !p->rxy) qb::fail(QB_ERR_ARG, "off-diagonal elements without r_xy values");
     FEP_CUDA(cudaSetDevice(device));
     cudaStream_t s;
     FEP_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     double *dE = nullptr;
-    cudaError_t e = cudaMalloc(&dE, sizeof(double) * std::max<long long>(total * src.rec_stride, 1));
+    // the records, then (EVB) every record's r_xy
+    const long long nE = total * src.rec_stride, nR = p->nnoffd > 0 ? total : 0;
+    cudaError_t e = cudaMalloc(&dE, sizeof(double) * std::max<long long>(nE + nR, 1));
     if (e != cudaSuccess) { cudaStreamDestroy(s); qb::fail(QB_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e)); }
     try {
-      FEP_CUDA(cudaMemcpyAsync(dE, energies, sizeof(double) * total * src.rec_stride, cudaMemcpyHostToDevice, s));
+      FEP_CUDA(cudaMemcpyAsync(dE, energies, sizeof(double) * nE, cudaMemcpyHostToDevice, s));
       src.base = dE;
+      if (nR > 0) {
+        FEP_CUDA(cudaMemcpyAsync(dE + nE, p->rxy, sizeof(double) * nR, cudaMemcpyHostToDevice, s));
+        src.rbase = dE + nE;
+        src.r_stride = 1;
+        long long off = 0;
+        for (int f = 0; f < nfiles; f++) { src.rfoff.push_back(off); off += npts[f]; }
+      }
       qb::fep_run(src, *p, device, s, out);
     } catch (...) {
       cudaStreamSynchronize(s);

@@ -16,6 +16,10 @@ struct FepSource {
   int rec_stride = 0;            // doubles per record
   std::vector<int> npts;         // records per file
   int nstates = 0;
+  // r_xy of record p of file f (EVB): rbase[rfoff[f] + p*r_stride]
+  const double *rbase = nullptr;
+  std::vector<long long> rfoff;
+  int r_stride = 0;
 };
 
 // Runs the analysis on `stream` and fills `out` (host buffers).  Throws

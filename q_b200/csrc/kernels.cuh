@@ -1617,6 +1617,14 @@ __device__ __forceinline__ void bonded_body(DevPtrs &P, int bx, int s, int gx) {
 // one block per system, threads over (term, state).
 __device__ __forceinline__ void qbonded_body(DevPtrs &P, int s) {
   const SysDev &S = P.sys[s];
+  // offdiag (md.f90:12911): the Q-atom distance of each off-diagonal
+  // function, from this step's coordinates; Hij = A exp(-mu r) is formed on
+  // the host where the records are written
+  if ((int)threadIdx.x < S.noffd) {
+    double3 a = ld3(P.x, S.offd_k[threadIdx.x]), b = ld3(P.x, S.offd_l[threadIdx.x]);
+    P.offd_r[s * MAXS + threadIdx.x] =
+        sqrt((b.x - a.x) * (b.x - a.x) + (b.y - a.y) * (b.y - a.y) + (b.z - a.z) * (b.z - a.z));
+  }
   const int NS = S.S;
   int n1 = S.nqb * NS, n2 = n1 + S.nqa * NS, n3 = n2 + S.nqt * NS, n4 = n3 + S.nqi * NS;
   const double pi = dev_pi();
@@ -2393,7 +2401,7 @@ __global__ void k_finish(DevPtrs P, int mode) {
   if (mode == 1) {
     // output and energy-file records of this step, copied by the whole warp
     const int is = st.istep;
-    const int rec_len = QB_NE + MAXS * QB_NEQ + 1;
+    const int rec_len = HIST_REC;
     for (int kind = 0; kind < 2; kind++) {
       int cyc = kind == 0 ? S.iout : S.iene;
       bool want = (is % cyc == 0) && (kind == 0 || is > 0);
@@ -2403,7 +2411,9 @@ __global__ void k_finish(DevPtrs P, int mode) {
         double *r = P.hist + (((size_t)kind * P.nsys + s) * P.hist_cap + c) * rec_len;
         for (int k = lane; k < rec_len; k += 32)
           r[k] = k == 0 ? (double)is
-                        : (k <= QB_NE ? P.E[s * QB_NE + k - 1] : P.EQ[(size_t)s * MAXS * QB_NEQ + k - 1 - QB_NE]);
+                 : k <= QB_NE ? P.E[s * QB_NE + k - 1]
+                 : k <= QB_NE + MAXS * QB_NEQ ? P.EQ[(size_t)s * MAXS * QB_NEQ + k - 1 - QB_NE]
+                                              : P.offd_r[s * MAXS + k - 1 - QB_NE - MAXS * QB_NEQ];
       }
       __syncwarp();
       if (lane == 0) st.hist_n[kind] = c + 1;

@@ -1129,8 +1129,21 @@ void read_fep(const std::string &path, const Topology &t, Fep &f) {
     f.qshake.push_back(q);
   }
   f.nqshake = (int)f.qshake.size();
+  // off-diagonal functions "state_i state_j qatom_k qatom_l A_ij mu_ij" (qatom.f90:1515-1555)
   f.noffd = prm.count("off_diagonals");
-  if (f.noffd > 0) fail(QB_ERR_UNSUPPORTED, "EVB off-diagonal elements are not supported");
+  if (f.noffd > QB_MAX_STATES) fail(QB_ERR_PARSE, "too many off-diagonal functions (at most max_states)");
+  for (auto &l : lines("off_diagonals")) {
+    auto v = line_values(l);
+    long i, j, k, q;
+    double A, mu;
+    if (v.size() < 6 || !to_int(v[0], i) || !to_int(v[1], j) || !to_int(v[2], k) || !to_int(v[3], q) ||
+        !to_real(v[4], A) || !to_real(v[5], mu))
+      bad("off_diagonals: " + l);
+    if (i < 1 || i > S || j < 1 || j > S || i == j) bad("invalid combination of states in off_diagonals: " + l);
+    if (k < 1 || k > f.nqat || q < 1 || q > f.nqat || f.iqseq[k - 1] < 0 || f.iqseq[q - 1] < 0)
+      bad("invalid Q atoms in off_diagonals: " + l);
+    f.offd.push_back({(int)i, (int)j, (int)k - 1, (int)q - 1, A, mu});
+  }
   if (prm.count("monitor_groups") > 0 || prm.count("monitor_group_pairs") > 0)
     fail(QB_ERR_UNSUPPORTED, "monitor groups are not supported");
   // soft-core table (qatom.f90:1556-1685)
@@ -1272,7 +1285,8 @@ void write_restart(const std::string &path, int natom, const double *x, const do
   std::fclose(f);
 }
 
-void append_energy_frame(const std::string &path, int nstates, const double *EQ) {
+void append_energy_frame(const std::string &path, int nstates, const double *EQ, int noffd, const int *ij,
+                         const double *hr) {
   std::FILE *f = std::fopen(path.c_str(), "ab");
   if (!f) fail(QB_ERR_IO, "cannot write " + path);
   for (int s = 0; s < nstates; s++) {
@@ -1281,7 +1295,16 @@ void append_energy_frame(const std::string &path, int nstates, const double *EQ)
     size_t sz[2] = {4, 8 * (size_t)QB_NEQ};
     write_record(f, p, sz, 2);
   }
-  write_record(f, nullptr, nullptr, 0);  // empty off-diagonal record (noffd = 0)
+  // off-diagonal record: noffd x (int32 i, int32 j, real8 Hij, real8 rkl), nrgy.f90:60-65, 116
+  std::vector<char> od((size_t)noffd * 24);
+  for (int k = 0; k < noffd; k++) {
+    int32_t ij32[2] = {ij[2 * k], ij[2 * k + 1]};
+    std::memcpy(od.data() + 24 * k, ij32, 8);
+    std::memcpy(od.data() + 24 * k + 8, hr + 2 * k, 16);
+  }
+  const void *p[1] = {od.data()};
+  size_t sz[1] = {od.size()};
+  write_record(f, p, sz, noffd > 0 ? 1 : 0);
   std::fclose(f);
 }
 

@@ -129,6 +129,8 @@ struct Fep {
   std::vector<double> qfkimp, qimp0;
   std::vector<QTor> qimp;
   int nang_coupl = 0, ntor_coupl = 0, nimp_coupl = 0, nqshake = 0, noffd = 0;
+  struct OffD { int i, j, k, l; double A, mu; };   // states 1-based, Q atoms 0-based
+  std::vector<OffD> offd;
   struct QShake { int i, j; double dist[QB_MAX_STATES]; };
   std::vector<QShake> qshake;
   std::vector<double> alpha_max;             // [nqat*nstates]
@@ -168,6 +170,7 @@ struct System {
   std::vector<unsigned char> qbnd_on, qang_on, qtor_on, qimp_on;
   std::vector<double> qbnd_Dmz, qbnd_amz, qbnd_r0, qbnd_fk, qang_fk, qang_th0, qang_ureyfk, qang_ureyr0;
   std::vector<double> qtor_fk, qtor_rmult, qtor_deltor, qimp_fk, qimp_imp0;
+  std::vector<int> offd_i, offd_j, offd_k, offd_l; std::vector<double> offd_A, offd_mu;
   // resolved bonded terms (after shrink_topology)
   std::vector<int> bi, bj; std::vector<double> bfk, bb0; int nb_solute = 0;
   std::vector<int> ai, aj, ak; std::vector<double> afk, ath0, aufk, aur0; int na_solute = 0;
@@ -200,7 +203,8 @@ void read_restart(const std::string &path, int natom, std::vector<double> &x,
                   std::vector<double> &v, int nshell, std::vector<float> *theta_corr);
 void write_restart(const std::string &path, int natom, const double *x, const double *v,
                    int nshell, const float *theta_corr);
-void append_energy_frame(const std::string &path, int nstates, const double *EQ);
+void append_energy_frame(const std::string &path, int nstates, const double *EQ, int noffd, const int *ij,
+                         const double *hr);
 
 // setup.cpp
 void prepare(System &s);

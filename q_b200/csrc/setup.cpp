@@ -562,6 +562,11 @@ void prepare(System &s) {
       int c = f.qimp[k].cod[st];
       if (c > 0) { s.qimp_on[k * S + st] = 1; s.qimp_fk[k * S + st] = f.qfkimp[c - 1]; s.qimp_imp0[k * S + st] = f.qimp0[c - 1]; }
     }
+  s.offd_i.clear(); s.offd_j.clear(); s.offd_k.clear(); s.offd_l.clear(); s.offd_A.clear(); s.offd_mu.clear();
+  for (auto &o : f.offd) {
+    s.offd_i.push_back(o.i); s.offd_j.push_back(o.j); s.offd_k.push_back(o.k); s.offd_l.push_back(o.l);
+    s.offd_A.push_back(o.A); s.offd_mu.push_back(o.mu);
+  }
 
   // water parameters used by the SPC kernels (md.f90:11834-11841, 11320-11325)
   if (s.nwat > 0) {
@@ -716,6 +721,9 @@ void System::fill_view(qb_sysview *v) const {
   v->qtor_on = qtor_on.data(); v->qtor_fk = qtor_fk.data(); v->qtor_rmult = qtor_rmult.data(); v->qtor_deltor = qtor_deltor.data();
   v->qimp_i = qimp_i.data(); v->qimp_j = qimp_j.data(); v->qimp_k = qimp_k.data(); v->qimp_l = qimp_l.data();
   v->qimp_on = qimp_on.data(); v->qimp_fk = qimp_fk.data(); v->qimp_imp0 = qimp_imp0.data();
+  v->noffd = (int)offd_i.size();
+  v->offd_i = offd_i.data(); v->offd_j = offd_j.data(); v->offd_k = offd_k.data(); v->offd_l = offd_l.data();
+  v->offd_A = offd_A.data(); v->offd_mu = offd_mu.data();
   v->shake_molecules = (int)sh_first.size(); v->shake_constraints = shake_constraints;
   v->shake_mol_first = sh_first.data(); v->shake_mol_n = sh_n.data();
   v->shake_i = sh_i.data(); v->shake_j = sh_j.data(); v->shake_dist2 = sh_d2.data();

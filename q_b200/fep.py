@@ -21,7 +21,7 @@ FepParams = _struct_from_header(os.path.join(INCLUDE, "qb_fep.h"), "qb_fep_param
 FepResultC = _struct_from_header(os.path.join(INCLUDE, "qb_fep.h"), "qb_fep_result")
 MAX_STATES = 4
 BAR_MAX_ITER = 1000
-PART2_W = 8
+PART2_W = 9
 PART3_W = 8
 
 
@@ -45,7 +45,7 @@ class FepResult:
     dgbarsum: np.ndarray
     bar_iterations: np.ndarray
     gap_range: np.ndarray
-    part2: np.ndarray        # (nfiles, nbins+2, 8)
+    part2: np.ndarray        # (nfiles, nbins+2, 9)
     part3: np.ndarray        # (nbins+2, 8)
 
     @property
@@ -54,7 +54,10 @@ class FepResult:
         return float(self.dgbarsum[len(self.npts)])
 
 
-def params(rt: float, nskip: int, *, gas: int = 0, nbins: int = 20, nmin: int = 5, alfa=(), coeff=(1.0, -1.0)):
+def params(rt: float, nskip: int, *, gas: int = 0, nbins: int = 20, nmin: int = 5, alfa=(), coeff=(1.0, -1.0),
+           evb=()):
+    """qfep's input; evb = [(i, j, A, mu, eta, rxy0)] (states 1-based) are its
+    off-diagonal elements Hij(r_xy) (qfep.f90:163-172)."""
     p = FepParams()
     p.rt = float(rt)
     p.nskip = int(nskip)
@@ -69,6 +72,12 @@ def params(rt: float, nskip: int, *, gas: int = 0, nbins: int = 20, nmin: int = 
             p.alfa[k + 1] = float(a)
     for k, c in enumerate(coeff[:MAX_STATES]):
         p.coeff[k] = float(c)
+    p.nnoffd = len(evb)
+    for i, j, A, mu, eta, r0 in evb:
+        if not (1 <= i <= MAX_STATES and 1 <= j <= MAX_STATES):
+            raise ValueError("off-diagonal element states out of range: %d %d" % (i, j))
+        k = (i - 1) * MAX_STATES + (j - 1)
+        p.evb_A[k], p.evb_mu[k], p.evb_eta[k], p.evb_rxy0[k] = float(A), float(mu), float(eta), float(r0)
     return p
 
 
@@ -100,12 +109,18 @@ def _result(arrs, nfiles: int, nstates: int, nbins: int) -> FepResult:
                      arrs["part2"].reshape(nfiles, nb, PART2_W), arrs["part3"].reshape(nb, PART3_W))
 
 
-def analyze(series, p, device: int = 0) -> FepResult:
-    """series: one array (npts, nstates, 15) per lambda window, in window order."""
+def analyze(series, p, device: int = 0, rxy=None) -> FepResult:
+    """series: one array (npts, nstates, 15) per lambda window, in window
+    order; with EVB elements in p, rxy gives each window's r_xy per record."""
     series = [np.ascontiguousarray(s, dtype=np.float64) for s in series]
     nfiles, nstates = len(series), series[0].shape[1]
     E = np.ascontiguousarray(np.concatenate([s.reshape(-1) for s in series]))
     npts = np.array([s.shape[0] for s in series], dtype=np.int32)
+    if p.nnoffd > 0:
+        if rxy is None or len(rxy) != nfiles or any(len(x) != n for x, n in zip(rxy, npts)):
+            raise ValueError("EVB analysis needs r_xy for every record of every window")
+        R = np.ascontiguousarray(np.concatenate([np.asarray(x, dtype=np.float64) for x in rxy]))
+        p.rxy = R.ctypes.data_as(C.POINTER(C.c_double))
     r, arrs = _buffers(nfiles, nstates, p.nbins)
     check(lib.qb_fep_analyze(E.ctypes.data_as(C.POINTER(C.c_double)), npts.ctypes.data_as(C.POINTER(C.c_int)),
                              nfiles, nstates, C.addressof(p), int(device), C.addressof(r)))
@@ -146,3 +161,22 @@ def read_en(path: str, nstates: int) -> np.ndarray:
         frames.append([np.frombuffer(b, dtype="<f8", offset=4, count=QB_NEQ) for b in block])
         k += nstates + 1
     return np.array(frames, dtype=np.float64).reshape(len(frames), nstates, QB_NEQ)
+
+
+def read_offdiag(path: str, nstates: int) -> np.ndarray:
+    """The off-diagonal record of every frame of a qdyn energy file
+    (nrgy.f90:60-65): (frames, noffd, 4) of state i, state j, Hij, r_kl."""
+    raw = open(path, "rb").read()
+    recs, pos = [], 0
+    while pos + 4 <= len(raw):
+        (n,) = struct.unpack_from("<i", raw, pos)
+        if n < 0 or pos + 8 + n > len(raw):
+            break
+        recs.append(raw[pos + 4:pos + 4 + n])
+        pos += 8 + n
+    out = []
+    for k in range(nstates, len(recs), nstates + 1):
+        r = recs[k]
+        out.append([struct.unpack_from("<iidd", r, 24 * m) for m in range(len(r) // 24)])
+    n = min((len(o) for o in out), default=0)
+    return np.array([o[:n] for o in out], dtype=np.float64).reshape(len(out), n, 4)

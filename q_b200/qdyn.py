@@ -24,8 +24,10 @@ def _fmt_label(label: str, values) -> str:
     return "%-16s%s" % (label, "".join("%10.2f" % v for v in values))
 
 
-def write_out(E, EQ, step: int | None, nstates: int, nwat: int, use_lrf: bool, nqat: int, nat_solute: int) -> str:
-    """One energy summary in write_out's layout."""
+def write_out(E, EQ, step: int | None, nstates: int, nwat: int, use_lrf: bool, nqat: int, nat_solute: int,
+              offd=None) -> str:
+    """One energy summary in write_out's layout; offd = [(i, j, Hij, k, l,
+    r_kl)] of the EVB off-diagonal functions (states and Q atoms 1-based)."""
     e = dict(zip(__import__("q_b200").E_NAMES, E))
     L = []
     if step is None:
@@ -78,6 +80,8 @@ def write_out(E, EQ, step: int | None, nstates: int, nwat: int, use_lrf: bool, n
         L.append("type   st lambda" + "%10s%10s" % ("total", "restraint"))
         for st in range(nstates):
             L.append(row("Q-SUM", st, EQ[st][1], EQ[st][14]))
+        for i, j, h, k, l, r in offd or ():
+            L.append("H(%2d,%2d) =%8.2f dist. between Q-atoms%4d%4d =%8.2f" % (i, j, h, k, l, r))
     L.append("=" * 79)
     return "\n".join(L)
 
@@ -123,6 +127,12 @@ def run(inp: str, out=sys.stdout, chunk: int = 1000) -> int:
                         interval=v.itrj_cycle, steps=v.nsteps, degf=v.Ndegfree, topology=files.get("topology", ""),
                         mask_rows=rows)
         frames = frame_steps(v.nsteps, v.itrj_cycle)
+    nod = v.noffd
+    ij = np.array([[v.offd_i[k], v.offd_j[k]] for k in range(nod)], dtype=np.int32).reshape(-1, 2)
+
+    def offd_rows(rec):
+        return [(v.offd_i[k], v.offd_j[k], rec[k][0], v.offd_k[k] + 1, v.offd_l[k] + 1, rec[k][1]) for k in range(nod)]
+
     T = batch.temperature(0)
     print("Initial temperatures are : Ttot =%10.2f Tfree =%10.2f" % (T[0], T[1]), file=out)
     done = 0
@@ -136,14 +146,18 @@ def run(inp: str, out=sys.stdout, chunk: int = 1000) -> int:
             if trj and done + n in frames:
                 trj.write(batch.coords(0))
             steps, E, EQ = batch.history(0, 0)
+            od = batch.offdiag(0, 0) if nod else None
             for k in range(len(steps)):
-                print(write_out(E[k], EQ[k], int(steps[k]), ns, v.nwat, bool(v.use_LRF), v.nqat, v.nat_solute), file=out)
+                print(write_out(E[k], EQ[k], int(steps[k]), ns, v.nwat, bool(v.use_LRF), v.nqat, v.nat_solute,
+                                offd_rows(od[k]) if nod else None), file=out)
             if ene:
                 _, _, EQe = batch.history(0, 1)
+                ode = batch.offdiag(0, 1) if nod else None
                 for k in range(EQe.shape[0]):
-                    append_energy(ene, EQe[k])
+                    append_energy(ene, EQe[k], (ij, ode[k]) if nod else None)
             batch.clear_history()
             done += n
+        od_last = offd_rows(batch.offdiag(0, 2)[0]) if nod and v.nsteps > 0 else None
         batch.final_energy()
     except QBError as e:
         print("!" * 79, file=out)
@@ -152,7 +166,7 @@ def run(inp: str, out=sys.stdout, chunk: int = 1000) -> int:
         return 255
     E, EQ = batch.energy_vectors(0)
     print("", file=out)
-    print(write_out(E, EQ, None, ns, v.nwat, bool(v.use_LRF), v.nqat, v.nat_solute), file=out)
+    print(write_out(E, EQ, None, ns, v.nwat, bool(v.use_LRF), v.nqat, v.nat_solute, od_last), file=out)
     tc = batch.theta_corr(0, v.nwpolr_shell) if v.nwpolr_shell > 0 else None
     write_restart(final, batch.coords(0), batch.velocities(0), tc)
     if trj:

@@ -74,7 +74,7 @@ class _Input:
 
 
 def run(stdin=sys.stdin, out=sys.stdout, device: int = 0) -> int:
-    from .fep import analyze, params, read_en
+    from .fep import analyze, params, read_en, read_offdiag
 
     w = out.write
     w("-" * 80 + "\n")
@@ -113,14 +113,24 @@ def run(stdin=sys.stdin, out=sys.stdout, device: int = 0) -> int:
         alfa.append(a)
         w("# Alpha for state %s              =%s\n" % (fmt_i(st, 2), fmt_f(a, 6, 2)))
     if noffd != 0:
-        w("\n>>>>> ERROR: predefined off-diagonal elements (EVB) are not supported\n")
+        # qfep reads no off-diagonal values in this mode (nnoffd is never set), so its result is undefined
+        w("\n>>>>> ERROR: predefined off-diagonal elements (EVB) are not supported; give them as functions\n")
         return 1
     w("--> Number of off-diagonal elements: ")
     nnoffd = int(inp.values(1)[0])
     w("# Number of off-diagonal elements         =%s\n" % fmt_i(nnoffd, 6))
     if nnoffd > 0:
-        w("\n>>>>> ERROR: off-diagonal elements (EVB) are not supported\n")
-        return 1
+        w("#   i   j   A(i,j)  mu(i,j) eta(i,j) rxy0(i,j)\n")
+    evb = []
+    for _ in range(nnoffd):
+        w("--> i, j, A_ij, mu_ij, eta_ij, r_xy0: ")
+        v = inp.values(6)
+        i, j, A, mu, eta, r0 = int(v[0]), int(v[1]), float(v[2]), float(v[3]), float(v[4]), float(v[5])
+        if not (1 <= i <= nstates and 1 <= j <= nstates):
+            w("\n>>>>> ERROR: off-diagonal element states out of range\n")
+            return 1
+        evb.append((i, j, A, mu, eta, r0))
+        w("#" + fmt_i(i, 4) + fmt_i(j, 4) + "".join(fmt_f(x, 9, 2) for x in (A, mu, eta, r0)) + "\n")
     w("--> linear combination of states defining reaction coord: ")
     coeff = [float(x) for x in inp.values(nstates)]
     w("# Linear combination coefficients=%s\n" % "".join(fmt_f(c, 8, 2) for c in coeff))
@@ -129,7 +139,7 @@ def run(stdin=sys.stdin, out=sys.stdout, device: int = 0) -> int:
     w("# Part 0: Average energies for all states in all files\n")
     w("# file             state   pts   lambda    EQtot   EQbond  EQang   EQtor   EQimp    EQel   EQvdW  Eel_qq"
       "  EvdW_qq Eel_qp  EvdW_qp Eel_qw EvdW_qw Eqrstr\n")
-    names, series = [], []
+    names, series, rxy = [], [], []
     for f in range(nfiles):
         name = inp.values(1)[0]
         try:
@@ -145,12 +155,22 @@ def run(stdin=sys.stdin, out=sys.stdout, device: int = 0) -> int:
             w(">>>>> ERROR: number of data sets in %s is less than number of points to skip!\n" % name)
             w("qfep terminated abnormally: Too few data points in file.\n")
             return 1
+        if nnoffd > 0:
+            od = read_offdiag(name, nstates)[:s.shape[0]]
+            if od.shape[1] < nnoffd:
+                w("ERROR: Unexpected end-of-file in first record of %s\n" % name)
+                w("while reading off-diagonal elements.\n")
+                w("Maybe there are less than %d off-diagonal elements?\n" % nnoffd)
+                w("qfep terminated abnormally: Failed to read off-diagonals.\n")
+                return 1
+            rxy.append(od[:, 0, 3])
         names.append(name)
         series.append(s)
     if nfiles < 2:
         w(">>>>> ERROR: at least two energy files are needed\n")
         return 1
-    r = analyze(series, params(rt, nskip, gas=gas, nbins=nbins, nmin=nmin, alfa=alfa, coeff=coeff), device)
+    r = analyze(series, params(rt, nskip, gas=gas, nbins=nbins, nmin=nmin, alfa=alfa, coeff=coeff, evb=evb), device,
+                rxy=rxy if nnoffd > 0 else None)
 
     # each file's prompt, then its Part 0 rows: (a,t23,i2,1x,i6,1x,f8.6,14f8.2)
     for f in range(nfiles):

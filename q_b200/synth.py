@@ -628,14 +628,15 @@ def _q_bonded(top: Topology, qatoms: list[int]) -> list[str]:
 
 def _fep_file(path: str, types: list[AtomType], iac: list[int], q: list[float], qatoms: list[int],
               alpha: float = 20.0, charge_scale: float = 0.0, eps_scale: float = 0.5, vdw_rule: int = 1,
-              top: Topology | None = None, soft_pairs=(), library_charges: bool = False) -> None:
+              top: Topology | None = None, soft_pairs=(), library_charges: bool = False, off_diagonals=()) -> None:
     """Two-state FEP file: state 2 scales the Q-atoms' charges by
     charge_scale and their epsilon by eps_scale, soft-core alpha in state 2.
     Given the topology, the bonded terms among the Q atoms are redefined too
     (_q_bonded).  soft_pairs (Q-atom index pairs, 0-based) interact by
     exponential repulsion A_i A_j exp(-B_i B_j r) instead of LJ, with the Q
     types' second parameter pair set for it; library_charges turns on
-    qq_use_library_charges."""
+    qq_use_library_charges; off_diagonals = [(state_i, state_j, qatom_k,
+    qatom_l, A, mu)] (1-based) are EVB off-diagonal functions."""
     L = ["[FEP]", "states 2"] + (["qq_use_library_charges on"] if library_charges else []) + ["", "[atoms]"]
     L += ["%d %d" % (k + 1, a + 1) for k, a in enumerate(qatoms)]
     L += ["", "[change_charges]"]
@@ -662,6 +663,8 @@ def _fep_file(path: str, types: list[AtomType], iac: list[int], q: list[float], 
     L += ["%d %g %g" % (k + 1, 0.0, alpha) for k in range(len(qatoms))]
     if soft_pairs:
         L += ["", "[soft_pairs]"] + ["%d %d" % (a + 1, b + 1) for a, b in soft_pairs]
+    if off_diagonals:
+        L += ["", "[off_diagonals]"] + ["%d %d %d %d %g %g" % tuple(o) for o in off_diagonals]
     if top is not None:
         L += [""] + _q_bonded(top, qatoms)
     with open(path, "w") as f:
@@ -695,13 +698,15 @@ def perturbation(base: Generated, name: str, qatoms, charge_scale: float, eps_sc
 def fep_solute(outdir: str, radius: float = 20.0, seed: int = 1234, steps: int = 5000, name: str = "c1",
                lambdas=(0.5, 0.5), run_seed: int = 1, vdw_rule: int = 1, ff_type: int = 2,
                q_bonded: bool = False, ub_fk: float = 25.0, soft_pairs: int = 0,
-               library_charges: bool = False, water_h_lj=(0.0, 0.0), solvent_type: int = 0) -> Generated:
+               library_charges: bool = False, water_h_lj=(0.0, 0.0), solvent_type: int = 0,
+               off_diagonals=()) -> Generated:
     """Config 1: 56-atom solute with 8 two-state Q-atoms in a TIP3P sphere,
     2 fs with SHAKE on X-H bonds and water.  ff_type 3 writes it as a CHARMM
     topology (charmm_terms, Urey-Bradley constant ub_fk); q_bonded redefines the bonded terms among the
     Q atoms in the FEP file.  soft_pairs > 0 makes that many Q-atom pairs
     beyond 1-4 soft pairs; library_charges sets qq_use_library_charges.
-    water_h_lj and solvent_type as for water_sphere."""
+    water_h_lj and solvent_type as for water_sphere; off_diagonals as for
+    _fep_file."""
     os.makedirs(outdir, exist_ok=True)
     rng = np.random.default_rng(seed)
     X, kinds, bonds = random_tree_solute(rng)
@@ -740,7 +745,7 @@ def fep_solute(outdir: str, radius: float = 20.0, seed: int = 1234, steps: int =
     near = {tuple(sorted(p)) for p in list(top.excl14[0]) + list(top.excl14[1])}
     far = [(a, b) for a in range(len(qat)) for b in range(a + 1, len(qat)) if tuple(sorted((qat[a], qat[b]))) not in near]
     _fep_file(fp, types, iac, top.crg, qat, vdw_rule=vdw_rule, top=top if q_bonded else None,
-              soft_pairs=far[:soft_pairs], library_charges=library_charges)
+              soft_pairs=far[:soft_pairs], library_charges=library_charges, off_diagonals=off_diagonals)
     inp = os.path.join(outdir, name + ".inp")
     write_inp(inp, tp, fp, steps=steps, stepsize=2.0, seed=run_seed, lambdas=lambdas, shake_hydrogens=True)
     return Generated(inp, tp, fp, len(top.x), len(waters))

@@ -82,6 +82,14 @@ class OracleRun:
                             E.ctypes.data_as(C.POINTER(C.c_double)), EQ.ctypes.data_as(C.POINTER(C.c_double)))
         return steps[:n], E[:n], EQ[:n, :self.S]
 
+    def offdiag(self, kind: int = 0):
+        """[records, noffd] r_kl of each record's off-diagonal functions."""
+        c = self.lib.qo_history(self.st, kind, None, None, None)
+        n = self.view.noffd
+        out = np.zeros(max(c * n, 1))
+        self.lib.qo_offdiag(self.st, kind, out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out[:c * n].reshape(c, n)
+
     def list_counts(self):
         out = (C.c_int * 5)()
         self.lib.qo_list_counts(self.st, out)
@@ -107,6 +115,7 @@ def load_oracle() -> Oracle:
         getattr(lib, f).argtypes = [vp, dp]
     lib.qo_theta_corr.argtypes = [vp, C.POINTER(C.c_float)]
     lib.qo_history.argtypes = [vp, C.c_int, C.POINTER(C.c_int), dp, dp]
+    lib.qo_offdiag.argtypes = [vp, C.c_int, dp]
     lib.qo_list_counts.argtypes = [vp, C.POINTER(C.c_int)]
     lib.qo_status.argtypes = [vp]
     return Oracle(lib)

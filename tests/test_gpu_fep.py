@@ -40,10 +40,12 @@ def compare(r, o, nf):
     for (f, ib), orow in zip(rows, o.part2):
         assert (f, ib) == (orow[0], orow[1])
         assert np.allclose(r.part2[f, ib, :5], [orow[2], orow[3], orow[4], orow[5], orow[6]], rtol=TOL, atol=TOL)
+        assert np.allclose(r.part2[f, ib, 5:7], [orow[7], orow[8]], rtol=TOL, atol=TOL)
     prow = [ib for ib in range(r.part3.shape[0]) if r.part3[ib, 7]]
     assert prow == [x[0] for x in o.part3]
     for ib, orow in zip(prow, o.part3):
         assert np.allclose(r.part3[ib, :4], [orow[1], orow[2], orow[3], orow[4]], rtol=TOL, atol=TOL)
+        assert np.allclose(r.part3[ib, 4:7], [orow[5], orow[6], orow[7]], rtol=TOL, atol=TOL)
 
 
 @pytest.mark.parametrize("ns,gas,nskip", [(2, 0, 5), (2, 1, 0), (3, 0, 10), (4, 0, 3)])
@@ -56,6 +58,29 @@ def test_analysis_matches_oracle(ns, gas, nskip):
     r = analyze(S, params(0.592, nskip, gas=gas, nbins=12, nmin=4, alfa=alfa, coeff=coeff))
     o = oracle_analyze(FepInput(S, 0.592, nskip, gas=gas, nbins=12, nmin=4, alfa=alfa, coeff=coeff))
     compare(r, o, nf)
+
+
+EVB = {2: [(1, 2, 12.0, 0.4, 0.05, 1.8)],
+       3: [(1, 2, 12.0, 0.4, 0.05, 1.8), (3, 1, 6.0, 0.8, 0.0, 2.2), (2, 3, 4.0, 0.2, 0.1, 2.0)],
+       4: [(1, 2, 12.0, 0.4, 0.05, 1.8), (2, 3, 4.0, 0.2, 0.1, 2.0), (4, 3, 9.0, 0.6, 0.0, 2.5)]}
+
+
+@pytest.mark.parametrize("ns", [2, 3, 4])
+def test_evb_analysis_matches_oracle(ns):
+    """EVB ground state from Hij(r_xy) (qfep.f90:286-318): the 2 x 2 closed
+    form with the c1^2, c2^2 weights, or the lowest eigenvalue for more
+    states; bin averages of c1^2, c2^2 and r_xy in Parts 2 and 3."""
+    from q_b200.fep import analyze, params
+    nf = 5
+    S = random_series(nf, 250, ns, seed=40 + ns, spread=2.0)
+    rng = np.random.default_rng(ns)
+    rxy = [rng.uniform(1.5, 3.0, s.shape[0]) for s in S]
+    coeff = [1.0] + [0.0] * (ns - 2) + [-1.0]
+    r = analyze(S, params(0.592, 4, nbins=10, nmin=3, coeff=coeff, evb=EVB[ns]), rxy=rxy)
+    o = oracle_analyze(FepInput(S, 0.592, 4, nbins=10, nmin=3, coeff=coeff, evb=EVB[ns], rxy=rxy))
+    compare(r, o, nf)
+    if ns == 2:
+        assert np.any(r.part2[:, :, 5] > 0.01) and np.any(r.part3[:, 6] > 1.5)
 
 
 def test_invalid_input_is_refused():

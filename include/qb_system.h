@@ -172,6 +172,11 @@ typedef struct qb_sysview {
   const int *offd_i, *offd_j;  /* states, 1-based as the FEP and energy files give them */
   const int *offd_k, *offd_l;  /* Q atoms, 0-based */
   const double *offd_A, *offd_mu;
+  /* EVB Morse couplings of Q terms to Q bonds (qatom.f90:1404-1497): per term the coupled Q bond
+   * (-1: none; angles: qangle's first coupling, qurey_bradley's last), impropers' flag (1: gamma =
+   * 1 - EMorseD), and per (term, state) the state whose qbond values EMorseD holds there */
+  const int *qang_cpl, *qang_cpl_ub, *qtor_cpl, *qimp_cpl, *qimp_cpl_flag;   /* [n] */
+  const int *qang_cpl_src, *qang_cpl_ub_src, *qtor_cpl_src, *qimp_cpl_src;   /* [n*nstates] */
 
   /* ---- SHAKE (md.f90:2326 init_shake) ---- */
   int shake_molecules, shake_constraints;

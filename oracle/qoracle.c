@@ -841,7 +841,32 @@ static double impropers(qo_state *st, int t0, int t1) {
   return e;
 }
 
-/* qbond (14060), qangle (13896), qtorsion (14262), qimproper (14117) */
+/* EMorseD of Q bond b as qbond computed it in state ss, and dMorse_i
+ * (md.f90:14086-14108); dMorse_j = -dMorse_i */
+static double morse_gamma(qo_state *st, int b, int ss, double dmi[3]) {
+  const qb_sysview *s = st->s;
+  int S = st->S, i = s->qbnd_i[b], j = s->qbnd_j[b];
+  double r[3] = {X(j, 0) - X(i, 0), X(j, 1) - X(i, 1), X(j, 2) - X(i, 2)};
+  double bl = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+  double amz = s->qbnd_amz[b * S + ss];
+  double db = bl - s->qbnd_r0[b * S + ss];
+  double fexp = exp(-amz * db);
+  if (db > 0) {
+    for (int k = 0; k < 3; k++) dmi[k] = +2. * amz * (fexp - fexp * fexp) * s->lambda[ss] / bl * r[k];
+    return -(fexp * fexp - 2. * fexp);
+  }
+  dmi[0] = dmi[1] = dmi[2] = 0;
+  return 1.0;
+}
+
+static void morse_apply(qo_state *st, int b, const double dmi[3], double e) {
+  int i = st->s->qbnd_i[b], j = st->s->qbnd_j[b];
+  for (int k = 0; k < 3; k++) { D(i, k) += dmi[k] * e; D(j, k) += -dmi[k] * e; }
+}
+
+/* qbond (14060), qangle (13896), qtorsion (14262), qimproper (14117); terms
+ * coupled to a Morse bond are scaled by gamma = EMorseD, with the bond's
+ * values from the state qbond last set them in */
 static void qbonded(qo_state *st, int ss) {
   const qb_sysview *s = st->s;
   int S = st->S;
@@ -872,8 +897,12 @@ static void qbonded(qo_state *st, int ss) {
     double ang = acos(scp);
     double fk = s->qang_fk[a * S + ss];
     double da = ang - s->qang_th0[a * S + ss];
-    EQV(ss, QB_EQ_ANGLE) += 0.5 * fk * da * da;
-    double dv = fk * da * lam;
+    int cb = s->qang_cpl[a];
+    double gamma = 1.0, dmi[3];
+    if (cb >= 0) gamma = morse_gamma(st, cb, s->qang_cpl_src[a * S + ss], dmi);
+    double ae = 0.5 * fk * da * da;
+    EQV(ss, QB_EQ_ANGLE) += ae * gamma;
+    double dv = gamma * fk * da * lam;
     double f1 = sin(ang);
     if (fabs(f1) < 1.e-12) f1 = 1.e-12;
     f1 = -1.0 / f1;
@@ -884,12 +913,18 @@ static void qbonded(qo_state *st, int ss) {
       D(k, c) += dv * dk;
       D(j, c) -= dv * (di + dk);
     }
-    /* qurey_bradley (md.f90:13992): energy only, its gradient is never applied */
+    if (cb >= 0) morse_apply(st, cb, dmi, ae);
+    /* qurey_bradley (md.f90:13992): energy only, its gradient is never applied
+     * (a Morse coupling's is) */
     double ufk = s->qang_ureyfk[a * S + ss];
     if (ufk != 0.) {
       double rik[3] = {X(k, 0) - X(i, 0), X(k, 1) - X(i, 1), X(k, 2) - X(i, 2)};
       double ru = sqrt(rik[0] * rik[0] + rik[1] * rik[1] + rik[2] * rik[2]) - s->qang_ureyr0[a * S + ss];
-      EQV(ss, QB_EQ_ANGLE) += ufk * ru * ru;
+      double eu = ufk * ru * ru, g = 1.0;
+      int cu = s->qang_cpl_ub[a];
+      if (cu >= 0) g = morse_gamma(st, cu, s->qang_cpl_ub_src[a * S + ss], dmi);
+      EQV(ss, QB_EQ_ANGLE) += eu * g;
+      if (cu >= 0) morse_apply(st, cu, dmi, eu);
     }
   }
   double dp[12], pi = fpi();
@@ -898,19 +933,32 @@ static void qbonded(qo_state *st, int ss) {
     double phi = dihedral(st, s->qtor_i[t], s->qtor_j[t], s->qtor_k[t], s->qtor_l[t], dp);
     double rm = s->qtor_rmult[t * S + ss], fk = s->qtor_fk[t * S + ss];
     double arg = rm * phi - s->qtor_deltor[t * S + ss];
-    EQV(ss, QB_EQ_TORSION) += fk * (1.0 + cos(arg));
-    double dv = -rm * fk * sin(arg) * lam;
+    int cb = s->qtor_cpl[t];
+    double gamma = 1.0, dmi[3];
+    if (cb >= 0) gamma = morse_gamma(st, cb, s->qtor_cpl_src[t * S + ss], dmi);
+    double pe = fk * (1.0 + cos(arg));
+    EQV(ss, QB_EQ_TORSION) += pe * gamma;
+    double dv = -rm * fk * sin(arg) * gamma * lam;
     apply4(st, s->qtor_i[t], s->qtor_j[t], s->qtor_k[t], s->qtor_l[t], dv, dp);
+    if (cb >= 0) morse_apply(st, cb, dmi, pe);
   }
   for (int t = 0; t < s->nqimp; t++) {
     if (!s->qimp_on[t * S + ss]) continue;
     double phi = dihedral(st, s->qimp_i[t], s->qimp_j[t], s->qimp_k[t], s->qimp_l[t], dp);
     double arg = phi - s->qimp_imp0[t * S + ss];
     arg = arg - 2. * pi * (double)lround(arg / (2. * pi));
+    int cb = s->qimp_cpl[t];
+    double gamma = 1.0, dmi[3];
+    if (cb >= 0) {
+      gamma = morse_gamma(st, cb, s->qimp_cpl_src[t * S + ss], dmi);
+      if (s->qimp_cpl_flag[t] == 1) gamma = 1 - gamma;
+    }
     double dv = s->qimp_fk[t * S + ss] * arg;
-    EQV(ss, QB_EQ_IMPROPER) += 0.5 * dv * arg;
-    dv = dv * lam;
+    double pe = 0.5 * dv * arg;
+    EQV(ss, QB_EQ_IMPROPER) += pe * gamma;
+    dv = dv * gamma * lam;
     apply4(st, s->qimp_i[t], s->qimp_j[t], s->qimp_k[t], s->qimp_l[t], dv, dp);
+    if (cb >= 0) morse_apply(st, cb, dmi, pe);
   }
 }
 

@@ -413,6 +413,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   std::vector<int4> qaijk; std::vector<uint8_t> qa_on; std::vector<double2> qapar, qaub;
   std::vector<int4> qtijkl; std::vector<uint8_t> qt_on; std::vector<double4> qtpar;
   std::vector<int4> qiijkl; std::vector<uint8_t> qi_on; std::vector<double2> qipar;
+  std::vector<int2> qa_cpl, qt_cpl, qi_cpl; std::vector<int8_t> qa_src, qa_src_ub, qt_src, qi_src;
   std::vector<int> sh_first, sh_n, sh_sys; std::vector<int2> sh_ij; std::vector<double> sh_d2;
   std::vector<int4> rs; std::vector<double> rs_fk;
   std::vector<int2> rp; std::vector<double> rp_x, rp_fk;
@@ -563,7 +564,11 @@ void build(Batch &B, qb_handle *const *hs, int n) {
         qa_on.push_back(on);
         qapar.push_back(on ? make_double2(V.qang_fk[k * NSt + st], V.qang_th0[k * NSt + st]) : make_double2(0, 0));
         qaub.push_back(on ? make_double2(V.qang_ureyfk[k * NSt + st], V.qang_ureyr0[k * NSt + st]) : make_double2(0, 0));
+        qa_src.push_back((int8_t)(st < NSt ? V.qang_cpl_src[k * NSt + st] : -1));
+        qa_src_ub.push_back((int8_t)(st < NSt ? V.qang_cpl_ub_src[k * NSt + st] : -1));
       }
+      qa_cpl.push_back(make_int2(V.qang_cpl[k] >= 0 ? S.qb_off + V.qang_cpl[k] : -1,
+                                 V.qang_cpl_ub[k] >= 0 ? S.qb_off + V.qang_cpl_ub[k] : -1));
     }
     S.qt_off = (int)qtijkl.size(); S.nqt = V.nqtor;
     for (int k = 0; k < V.nqtor; k++) {
@@ -573,7 +578,9 @@ void build(Batch &B, qb_handle *const *hs, int n) {
         qt_on.push_back(on);
         qtpar.push_back(on ? make_double4(V.qtor_fk[k * NSt + st], V.qtor_rmult[k * NSt + st], V.qtor_deltor[k * NSt + st], 0)
                            : make_double4(0, 0, 0, 0));
+        qt_src.push_back((int8_t)(st < NSt ? V.qtor_cpl_src[k * NSt + st] : -1));
       }
+      qt_cpl.push_back(make_int2(V.qtor_cpl[k] >= 0 ? S.qb_off + V.qtor_cpl[k] : -1, 0));
     }
     S.qi_off = (int)qiijkl.size(); S.nqi = V.nqimp;
     for (int k = 0; k < V.nqimp; k++) {
@@ -582,7 +589,9 @@ void build(Batch &B, qb_handle *const *hs, int n) {
         bool on = st < NSt && V.qimp_on[k * NSt + st];
         qi_on.push_back(on);
         qipar.push_back(on ? make_double2(V.qimp_fk[k * NSt + st], V.qimp_imp0[k * NSt + st]) : make_double2(0, 0));
+        qi_src.push_back((int8_t)(st < NSt ? V.qimp_cpl_src[k * NSt + st] : -1));
       }
+      qi_cpl.push_back(make_int2(V.qimp_cpl[k] >= 0 ? S.qb_off + V.qimp_cpl[k] : -1, V.qimp_cpl_flag[k]));
     }
     S.noffd = V.noffd;
     if (S.noffd > MAXS) fail(QB_ERR_ARG, "too many off-diagonal functions");
@@ -774,6 +783,9 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   P.tijkl = dev_upload(tijkl, o); P.tpar = dev_upload(tpar, o); P.iijkl = dev_upload(iijkl, o); P.ipar = dev_upload(ipar, o);
   P.qbij = dev_upload(qbij, o); P.qb_on = dev_upload(qb_on, o); P.qbpar = dev_upload(qbpar, o);
   P.qaijk = dev_upload(qaijk, o); P.qa_on = dev_upload(qa_on, o); P.qapar = dev_upload(qapar, o); P.qaub = dev_upload(qaub, o);
+  P.qa_cpl = dev_upload(qa_cpl, o); P.qt_cpl = dev_upload(qt_cpl, o); P.qi_cpl = dev_upload(qi_cpl, o);
+  P.qa_src = dev_upload(qa_src, o); P.qa_src_ub = dev_upload(qa_src_ub, o);
+  P.qt_src = dev_upload(qt_src, o); P.qi_src = dev_upload(qi_src, o);
   P.qtijkl = dev_upload(qtijkl, o); P.qt_on = dev_upload(qt_on, o); P.qtpar = dev_upload(qtpar, o);
   P.qiijkl = dev_upload(qiijkl, o); P.qi_on = dev_upload(qi_on, o); P.qipar = dev_upload(qipar, o);
   P.sh_first = dev_upload(sh_first, o); P.sh_n = dev_upload(sh_n, o); P.sh_sys = dev_upload(sh_sys, o);

@@ -118,6 +118,11 @@ struct DevPtrs {
   int4 *iijkl; float2 *ipar;              // fk, imp0
   int2 *qbij; uint8_t *qb_on; double4 *qbpar;           // [term*MAXS+st] Dmz, amz, r0, fk
   int4 *qaijk; uint8_t *qa_on; double2 *qapar, *qaub;   // fk, th0; Urey-Bradley k, r0
+  // EVB Morse couplings: per Q angle (qangle's bond, qurey_bradley's bond), torsion (bond, 0),
+  // improper (bond, flag) with the bond as a global Q-bond index or -1; per (term, state) the
+  // state whose bond values apply
+  int2 *qa_cpl, *qt_cpl, *qi_cpl;
+  int8_t *qa_src, *qa_src_ub, *qt_src, *qi_src;
   int4 *qtijkl; uint8_t *qt_on; double4 *qtpar;         // fk, rmult, deltor
   int4 *qiijkl; uint8_t *qi_on; double2 *qipar;         // fk, imp0
   // shake

@@ -1613,8 +1613,38 @@ __device__ __forceinline__ void bonded_body(DevPtrs &P, int bx, int s, int gx) {
   for (int c = 0; c < 8; c++) warp_add(&P.E[s * QB_NE + idx[c]], e[c]);
 }
 
+// EMorseD of Q bond qb (global index) as qbond computed it in state st, and
+// dMorse_i (dMorse_j = -dMorse_i), md.f90:14086-14108: the Morse bond's
+// fraction of its well depth beyond r0, 1 inside it.
+__device__ __forceinline__ double morse_gamma(const DevPtrs &P, const SysDev &S, int qb, int st, double *dmi,
+                                              int2 &ij) {
+  ij = P.qbij[qb];
+  const double4 prm = P.qbpar[qb * MAXS + st];   // Dmz, amz, r0, fk
+  const double3 xi = ld3(P.x, ij.x), xj = ld3(P.x, ij.y);
+  const double r[3] = {xj.x - xi.x, xj.y - xi.y, xj.z - xi.z};
+  const double b = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+  const double db = b - prm.z;
+  const double fexp = exp(-prm.y * db);
+  if (db > 0) {
+    const double f = 2. * prm.y * (fexp - fexp * fexp) * S.lambda[st] / b;
+    for (int c = 0; c < 3; c++) dmi[c] = f * r[c];
+    return -(fexp * fexp - 2. * fexp);
+  }
+  dmi[0] = dmi[1] = dmi[2] = 0.0;
+  return 1.0;
+}
+
+// The coupling's gradient: dMorse_i * E on the bond's first atom, dMorse_j * E
+// on its second (md.f90:13970-13985).
+__device__ __forceinline__ void morse_apply(DevPtrs &P, int2 ij, const double *dmi, double e) {
+  atomic_add3(P.d, ij.x, dmi[0] * e, dmi[1] * e, dmi[2] * e);
+  atomic_add3(P.d, ij.y, -dmi[0] * e, -dmi[1] * e, -dmi[2] * e);
+}
+
 // qbond (14060), qangle (13896), qtorsion (14262), qimproper (14117):
-// one block per system, threads over (term, state).
+// one block per system, threads over (term, state).  A term coupled to a
+// Morse bond (EVB couplings) is scaled by gamma = EMorseD of that bond, with
+// the bond's values from the state qbond last set them in (setup resolves it).
 __device__ __forceinline__ void qbonded_body(DevPtrs &P, int s) {
   const SysDev &S = P.sys[s];
   // offdiag (md.f90:12911): the Q-atom distance of each off-diagonal
@@ -1661,8 +1691,13 @@ __device__ __forceinline__ void qbonded_body(DevPtrs &P, int s) {
       if (scp < -1.0) scp = -1.0;
       double ang = acos(scp);
       double da = ang - prm.y;
-      atomicAdd(&eq[QB_EQ_ANGLE], 0.5 * prm.x * da * da);
-      double dv = prm.x * da * S.lambda[st];
+      const int2 cp = P.qa_cpl[S.qa_off + a];
+      double gamma = 1.0, dmi[3];
+      int2 bij;
+      if (cp.x >= 0) gamma = morse_gamma(P, S, cp.x, P.qa_src[(S.qa_off + a) * MAXS + st], dmi, bij);
+      const double ae = 0.5 * prm.x * da * da;
+      atomicAdd(&eq[QB_EQ_ANGLE], ae * gamma);
+      double dv = gamma * prm.x * da * S.lambda[st];
       double f1 = sin(ang);
       if (fabs(f1) < 1.e-12) f1 = 1.e-12;
       f1 = -1.0 / f1;
@@ -1674,14 +1709,19 @@ __device__ __forceinline__ void qbonded_body(DevPtrs &P, int s) {
       atomic_add3(P.d, t.x, dv * di[0], dv * di[1], dv * di[2]);
       atomic_add3(P.d, t.z, dv * dk[0], dv * dk[1], dv * dk[2]);
       atomic_add3(P.d, t.y, -dv * (di[0] + dk[0]), -dv * (di[1] + dk[1]), -dv * (di[2] + dk[2]));
+      if (cp.x >= 0) morse_apply(P, bij, dmi, ae);
       // qurey_bradley (md.f90:13992): adds the 1-3 energy to the state's
       // angle energy; the reference never applies its gradient, so neither
-      // does this
+      // does this (a Morse coupling's gradient it does apply)
       double2 ub = P.qaub[(S.qa_off + a) * MAXS + st];
       if (ub.x != 0.) {
         double rik[3] = {xk.x - xi.x, xk.y - xi.y, xk.z - xi.z};
         double ru = sqrt(rik[0] * rik[0] + rik[1] * rik[1] + rik[2] * rik[2]) - ub.y;
-        atomicAdd(&eq[QB_EQ_ANGLE], ub.x * ru * ru);
+        const double eu = ub.x * ru * ru;
+        double g = 1.0;
+        if (cp.y >= 0) g = morse_gamma(P, S, cp.y, P.qa_src_ub[(S.qa_off + a) * MAXS + st], dmi, bij);
+        atomicAdd(&eq[QB_EQ_ANGLE], eu * g);
+        if (cp.y >= 0) morse_apply(P, bij, dmi, eu);
       }
     } else if (k < n3) {
       int t = (k - n2) / NS, st = (k - n2) % NS;
@@ -1692,9 +1732,15 @@ __device__ __forceinline__ void qbonded_body(DevPtrs &P, int s) {
       double dp[12];
       double phi = dihedral(P, q.x, q.y, q.z, q.w, dp);
       double arg = prm.y * phi - prm.z;
-      atomicAdd(&eq[QB_EQ_TORSION], prm.x * (1.0 + cos(arg)));
-      double dv = -prm.y * prm.x * sin(arg) * S.lambda[st];
+      const int2 cp = P.qt_cpl[S.qt_off + t];
+      double gamma = 1.0, dmi[3];
+      int2 bij;
+      if (cp.x >= 0) gamma = morse_gamma(P, S, cp.x, P.qt_src[(S.qt_off + t) * MAXS + st], dmi, bij);
+      const double pe = prm.x * (1.0 + cos(arg));
+      atomicAdd(&eq[QB_EQ_TORSION], pe * gamma);
+      double dv = -prm.y * prm.x * sin(arg) * gamma * S.lambda[st];
       apply4(P, q.x, q.y, q.z, q.w, dv, dp);
+      if (cp.x >= 0) morse_apply(P, bij, dmi, pe);
     } else {
       int t = (k - n3) / NS, st = (k - n3) % NS;
       if (!P.qi_on[(S.qi_off + t) * MAXS + st]) continue;
@@ -1705,10 +1751,19 @@ __device__ __forceinline__ void qbonded_body(DevPtrs &P, int s) {
       double phi = dihedral(P, q.x, q.y, q.z, q.w, dp);
       double arg = phi - prm.y;
       arg = arg - 2. * pi * (double)llround(arg / (2. * pi));
+      const int2 cp = P.qi_cpl[S.qi_off + t];
+      double gamma = 1.0, dmi[3];
+      int2 bij;
+      if (cp.x >= 0) {
+        gamma = morse_gamma(P, S, cp.x, P.qi_src[(S.qi_off + t) * MAXS + st], dmi, bij);
+        if (cp.y == 1) gamma = 1 - gamma;   // coupled to a bond breaking, not making
+      }
       double dv = prm.x * arg;
-      atomicAdd(&eq[QB_EQ_IMPROPER], 0.5 * dv * arg);
-      dv = dv * S.lambda[st];
+      const double pe = 0.5 * dv * arg;
+      atomicAdd(&eq[QB_EQ_IMPROPER], pe * gamma);
+      dv = dv * gamma * S.lambda[st];
       apply4(P, q.x, q.y, q.z, q.w, dv, dp);
+      if (cp.x >= 0) morse_apply(P, bij, dmi, pe);
     }
   }
 }

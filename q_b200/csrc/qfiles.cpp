@@ -1115,11 +1115,30 @@ void read_fep(const std::string &path, const Topology &t, Fep &f) {
   };
   tors("torsion_types", "change_torsions", f.qfktor, f.qrmult, &f.qdeltor, f.qtor);
   tors("improper_types", "change_impropers", f.qfkimp, f.qimp0, nullptr, f.qimp);
-  f.nang_coupl = prm.count("angle_couplings");
-  f.ntor_coupl = prm.count("torsion_couplings");
-  f.nimp_coupl = prm.count("improper_couplings");
-  if (f.nang_coupl + f.ntor_coupl + f.nimp_coupl > 0)
-    fail(QB_ERR_UNSUPPORTED, "EVB Morse couplings are not supported");
+  // EVB couplings of Q angles, torsions and impropers to Morse Q bonds
+  // (qatom.f90:1404-1497): "term bond", impropers "term bond [flag]"; the
+  // bond must be Morse (no harmonic force constant) in every state it is in
+  auto couplings = [&](const char *sec, size_t nterm, bool with_flag, std::vector<Fep::Coupling> &out) {
+    for (auto &l : lines(sec)) {
+      auto v = line_values(l);
+      long j, k, fl = 0;
+      if (v.size() < 2 || !to_int(v[0], j) || !to_int(v[1], k)) bad(std::string(sec) + ": " + l);
+      if (with_flag && v.size() >= 3 && !to_int(v[2], fl)) fl = 0;
+      if (j < 1 || j > (long)nterm || k < 1 || k > (long)f.qbnd.size()) bad(std::string(sec) + ": " + l);
+      for (int s = 0; s < S; s++) {
+        int c = f.qbnd[k - 1].cod[s];
+        if (c > 0 && f.qbondlib[c - 1].fk != 0.0)
+          bad(std::string(sec) + ": Q bond " + std::to_string(k) + " is harmonic in state " + std::to_string(s + 1));
+      }
+      out.push_back({(int)j - 1, (int)k - 1, (int)fl});
+    }
+  };
+  couplings("angle_couplings", f.qang.size(), false, f.ang_coupl);
+  couplings("torsion_couplings", f.qtor.size(), false, f.tor_coupl);
+  couplings("improper_couplings", f.qimp.size(), true, f.imp_coupl);
+  f.nang_coupl = (int)f.ang_coupl.size();
+  f.ntor_coupl = (int)f.tor_coupl.size();
+  f.nimp_coupl = (int)f.imp_coupl.size();
   for (auto &l : lines("shake_constraints")) {
     auto v = line_values(l);
     long a, b;

@@ -128,6 +128,9 @@ struct Fep {
   std::vector<QTor> qtor;
   std::vector<double> qfkimp, qimp0;
   std::vector<QTor> qimp;
+  // EVB Morse couplings: Q term, Q bond (0-based), flag (1: gamma = 1 - EMorseD; impropers only)
+  struct Coupling { int term, bond, flag; };
+  std::vector<Coupling> ang_coupl, tor_coupl, imp_coupl;
   int nang_coupl = 0, ntor_coupl = 0, nimp_coupl = 0, nqshake = 0, noffd = 0;
   struct OffD { int i, j, k, l; double A, mu; };   // states 1-based, Q atoms 0-based
   std::vector<OffD> offd;
@@ -171,6 +174,10 @@ struct System {
   std::vector<double> qbnd_Dmz, qbnd_amz, qbnd_r0, qbnd_fk, qang_fk, qang_th0, qang_ureyfk, qang_ureyr0;
   std::vector<double> qtor_fk, qtor_rmult, qtor_deltor, qimp_fk, qimp_imp0;
   std::vector<int> offd_i, offd_j, offd_k, offd_l; std::vector<double> offd_A, offd_mu;
+  // Morse coupling of each Q angle (qangle's, then qurey_bradley's), torsion and improper: the
+  // bond or -1, the flag, and per state the state whose qbond values EMorseD holds there
+  std::vector<int> qang_cpl, qang_cpl_ub, qtor_cpl, qimp_cpl, qimp_cpl_flag;
+  std::vector<int> qang_cpl_src, qang_cpl_ub_src, qtor_cpl_src, qimp_cpl_src;
   // resolved bonded terms (after shrink_topology)
   std::vector<int> bi, bj; std::vector<double> bfk, bb0; int nb_solute = 0;
   std::vector<int> ai, aj, ak; std::vector<double> afk, ath0, aufk, aur0; int na_solute = 0;

@@ -567,6 +567,46 @@ void prepare(System &s) {
     s.offd_i.push_back(o.i); s.offd_j.push_back(o.j); s.offd_k.push_back(o.k); s.offd_l.push_back(o.l);
     s.offd_A.push_back(o.A); s.offd_mu.push_back(o.mu);
   }
+  // Morse couplings (md.f90:13910-13925, 14008-14018, 14135-14145, 14280-14290).
+  // qangle takes an angle's first coupling, qurey_bradley, qtorsion and
+  // qimproper its last.  In state st, EMorseD(ib) holds what qbond computed in
+  // the latest state <= st that has the bond; a coupled term present in a
+  // state before any such state would read a previous step's value.
+  auto resolve = [&](const std::vector<Fep::Coupling> &cpl, size_t nterm, const std::vector<int> &cod_of_term,
+                     bool first, std::vector<int> &bond, std::vector<int> *flag, std::vector<int> &src,
+                     const char *what) {
+    bond.assign(nterm, -1);
+    if (flag) flag->assign(nterm, 0);
+    src.assign(nterm * S, -1);
+    for (auto &c : cpl) {
+      if (first && bond[c.term] >= 0) continue;
+      bond[c.term] = c.bond;
+      if (flag) (*flag)[c.term] = c.flag;
+    }
+    for (size_t t = 0; t < nterm; t++) {
+      if (bond[t] < 0) continue;
+      int last = -1;
+      for (int st = 0; st < S; st++) {
+        if (f.qbnd[bond[t]].cod[st] > 0) last = st;
+        if (cod_of_term[t * S + st] > 0) {
+          if (last < 0)
+            fail(QB_ERR_UNSUPPORTED, std::string("coupled Q ") + what + " " + std::to_string(t + 1) +
+                                         " is present in a state before its Morse bond is (EMorseD from a previous step)");
+          src[t * S + st] = last;
+        }
+      }
+    }
+  };
+  {
+    std::vector<int> ca(f.qang.size() * S), ct(f.qtor.size() * S), ci(f.qimp.size() * S);
+    for (size_t k = 0; k < f.qang.size(); k++) for (int st = 0; st < S; st++) ca[k * S + st] = f.qang[k].cod[st];
+    for (size_t k = 0; k < f.qtor.size(); k++) for (int st = 0; st < S; st++) ct[k * S + st] = f.qtor[k].cod[st];
+    for (size_t k = 0; k < f.qimp.size(); k++) for (int st = 0; st < S; st++) ci[k * S + st] = f.qimp[k].cod[st];
+    resolve(f.ang_coupl, f.qang.size(), ca, true, s.qang_cpl, nullptr, s.qang_cpl_src, "angle");
+    resolve(f.ang_coupl, f.qang.size(), ca, false, s.qang_cpl_ub, nullptr, s.qang_cpl_ub_src, "angle");
+    resolve(f.tor_coupl, f.qtor.size(), ct, false, s.qtor_cpl, nullptr, s.qtor_cpl_src, "torsion");
+    resolve(f.imp_coupl, f.qimp.size(), ci, false, s.qimp_cpl, &s.qimp_cpl_flag, s.qimp_cpl_src, "improper");
+  }
 
   // water parameters used by the SPC kernels (md.f90:11834-11841, 11320-11325)
   if (s.nwat > 0) {
@@ -724,6 +764,10 @@ void System::fill_view(qb_sysview *v) const {
   v->noffd = (int)offd_i.size();
   v->offd_i = offd_i.data(); v->offd_j = offd_j.data(); v->offd_k = offd_k.data(); v->offd_l = offd_l.data();
   v->offd_A = offd_A.data(); v->offd_mu = offd_mu.data();
+  v->qang_cpl = qang_cpl.data(); v->qang_cpl_ub = qang_cpl_ub.data(); v->qtor_cpl = qtor_cpl.data();
+  v->qimp_cpl = qimp_cpl.data(); v->qimp_cpl_flag = qimp_cpl_flag.data();
+  v->qang_cpl_src = qang_cpl_src.data(); v->qang_cpl_ub_src = qang_cpl_ub_src.data();
+  v->qtor_cpl_src = qtor_cpl_src.data(); v->qimp_cpl_src = qimp_cpl_src.data();
   v->shake_molecules = (int)sh_first.size(); v->shake_constraints = shake_constraints;
   v->shake_mol_first = sh_first.data(); v->shake_mol_n = sh_n.data();
   v->shake_i = sh_i.data(); v->shake_j = sh_j.data(); v->shake_dist2 = sh_d2.data();

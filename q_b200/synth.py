@@ -566,14 +566,18 @@ def water_sphere(outdir: str, radius: float = 15.0, seed: int = 1234, steps: int
     return Generated(inp, tp, None, len(top.x), (len(top.x)) // 3)
 
 
-def _q_bonded(top: Topology, qatoms: list[int]) -> list[str]:
+def _q_bonded(top: Topology, qatoms: list[int], couplings: bool = False) -> list[str]:
     """FEP sections redefining the topology's bonds, angles, torsions and
     impropers that lie wholly among the Q atoms: state 1 keeps the topology's
     parameters, state 2 changes them (the first bond becomes a Morse bond of
     the same curvature, the last torsion is absent).  Impropers centred on a
     Q atom are redefined too, harmonic
     about the geometry's own improper angle in both states; under CHARMM the
-    angle types carry the topology's Urey-Bradley columns, halved in state 2."""
+    angle types carry the topology's Urey-Bradley columns, halved in state 2.
+    With couplings, the first bond is a Morse bond in state 1 and absent in
+    state 2 (a bond that breaks), and the angles, torsions and impropers
+    holding both its atoms are coupled to it (EVB Morse couplings; the first
+    improper coupling with gamma = 1 - EMorseD)."""
     qs = set(qatoms)
     X = np.asarray(top.x, dtype=float)
     L = []
@@ -582,14 +586,18 @@ def _q_bonded(top: Topology, qatoms: list[int]) -> list[str]:
         L += ["[bond_types]"]
         for n, (i, j, c) in enumerate(bonds):
             fk, b0 = top.bond_lib[c - 1]
-            L.append("%d %8.2f %8.4f" % (2 * n + 1, fk, b0))
+            if n == 0 and couplings:
+                L.append("%d %8.3f %6.3f %8.4f" % (2 * n + 1, fk / 8.0, 2.0, b0))
+            else:
+                L.append("%d %8.2f %8.4f" % (2 * n + 1, fk, b0))
             if n == 0:
                 amz = 2.0
                 L.append("%d %8.3f %6.3f %8.4f" % (2 * n + 2, fk / (2 * amz * amz), amz, b0 + 0.03))
             else:
                 L.append("%d %8.2f %8.4f" % (2 * n + 2, 0.8 * fk, b0 + 0.02))
         L += ["", "[change_bonds]"]
-        L += ["%d %d %d %d" % (i + 1, j + 1, 2 * n + 1, 2 * n + 2) for n, (i, j, c) in enumerate(bonds)]
+        L += ["%d %d %d %d" % (i + 1, j + 1, 2 * n + 1, 0 if (n == 0 and couplings) else 2 * n + 2)
+              for n, (i, j, c) in enumerate(bonds)]
         L += [""]
     angles = [(i, j, k, c) for i, j, k, c in top.angles[:top.nangles_solute] if i in qs and j in qs and k in qs]
     if angles:
@@ -623,12 +631,25 @@ def _q_bonded(top: Topology, qatoms: list[int]) -> list[str]:
         L += ["%d %d %d %d %d %d" % (i + 1, j + 1, k + 1, l + 1, 2 * n + 1, 2 * n + 2)
               for n, (i, j, k, l, c) in enumerate(imps)]
         L += [""]
+    if couplings and bonds:
+        a, b = bonds[0][0], bonds[0][1]
+        hold = lambda t: a in t and b in t
+        ca = [n + 1 for n, t in enumerate(angles) if hold(t[:3])]
+        ct = [n + 1 for n, t in enumerate(tors) if hold(t[:4])]
+        ci = [n + 1 for n, t in enumerate(imps) if hold(t[:4])]
+        if ca:
+            L += ["[angle_couplings]"] + ["%d 1" % n for n in ca] + [""]
+        if ct:
+            L += ["[torsion_couplings]"] + ["%d 1" % n for n in ct] + [""]
+        if ci:
+            L += ["[improper_couplings]"] + ["%d 1%s" % (n, " 1" if k == 0 else "") for k, n in enumerate(ci)] + [""]
     return L
 
 
 def _fep_file(path: str, types: list[AtomType], iac: list[int], q: list[float], qatoms: list[int],
               alpha: float = 20.0, charge_scale: float = 0.0, eps_scale: float = 0.5, vdw_rule: int = 1,
-              top: Topology | None = None, soft_pairs=(), library_charges: bool = False, off_diagonals=()) -> None:
+              top: Topology | None = None, soft_pairs=(), library_charges: bool = False, off_diagonals=(),
+              couplings: bool = False) -> None:
     """Two-state FEP file: state 2 scales the Q-atoms' charges by
     charge_scale and their epsilon by eps_scale, soft-core alpha in state 2.
     Given the topology, the bonded terms among the Q atoms are redefined too
@@ -666,7 +687,7 @@ def _fep_file(path: str, types: list[AtomType], iac: list[int], q: list[float], 
     if off_diagonals:
         L += ["", "[off_diagonals]"] + ["%d %d %d %d %g %g" % tuple(o) for o in off_diagonals]
     if top is not None:
-        L += [""] + _q_bonded(top, qatoms)
+        L += [""] + _q_bonded(top, qatoms, couplings)
     with open(path, "w") as f:
         f.write("\n".join(L) + "\n")
 
@@ -699,14 +720,15 @@ def fep_solute(outdir: str, radius: float = 20.0, seed: int = 1234, steps: int =
                lambdas=(0.5, 0.5), run_seed: int = 1, vdw_rule: int = 1, ff_type: int = 2,
                q_bonded: bool = False, ub_fk: float = 25.0, soft_pairs: int = 0,
                library_charges: bool = False, water_h_lj=(0.0, 0.0), solvent_type: int = 0,
-               off_diagonals=()) -> Generated:
+               off_diagonals=(), morse_couplings: bool = False) -> Generated:
     """Config 1: 56-atom solute with 8 two-state Q-atoms in a TIP3P sphere,
     2 fs with SHAKE on X-H bonds and water.  ff_type 3 writes it as a CHARMM
     topology (charmm_terms, Urey-Bradley constant ub_fk); q_bonded redefines the bonded terms among the
     Q atoms in the FEP file.  soft_pairs > 0 makes that many Q-atom pairs
     beyond 1-4 soft pairs; library_charges sets qq_use_library_charges.
     water_h_lj and solvent_type as for water_sphere; off_diagonals as for
-    _fep_file."""
+    _fep_file; morse_couplings (with q_bonded) couples the Q terms of the
+    first Q bond to it (_q_bonded)."""
     os.makedirs(outdir, exist_ok=True)
     rng = np.random.default_rng(seed)
     X, kinds, bonds = random_tree_solute(rng)
@@ -745,7 +767,8 @@ def fep_solute(outdir: str, radius: float = 20.0, seed: int = 1234, steps: int =
     near = {tuple(sorted(p)) for p in list(top.excl14[0]) + list(top.excl14[1])}
     far = [(a, b) for a in range(len(qat)) for b in range(a + 1, len(qat)) if tuple(sorted((qat[a], qat[b]))) not in near]
     _fep_file(fp, types, iac, top.crg, qat, vdw_rule=vdw_rule, top=top if q_bonded else None,
-              soft_pairs=far[:soft_pairs], library_charges=library_charges, off_diagonals=off_diagonals)
+              soft_pairs=far[:soft_pairs], library_charges=library_charges, off_diagonals=off_diagonals,
+              couplings=morse_couplings)
     inp = os.path.join(outdir, name + ".inp")
     write_inp(inp, tp, fp, steps=steps, stepsize=2.0, seed=run_seed, lambdas=lambdas, shake_hydrogens=True)
     return Generated(inp, tp, fp, len(top.x), len(waters))

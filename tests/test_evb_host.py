@@ -73,3 +73,104 @@ def test_oracle_two_state_evb_is_the_secular_determinant():
         assert abs(vg - w[0]) < 1e-10
         c1 = 1.0 / (1.0 + ((vg - e[k, 0]) / h[k]) ** 2)
         assert abs(c1 - v[0, 0] ** 2) < 1e-10
+
+
+def _strip_couplings(path):
+    """The FEP file without its coupling sections (same bonds and terms)."""
+    out, skip = [], False
+    for line in open(path).read().split("\n"):
+        if line.startswith("["):
+            skip = line.strip() in ("[angle_couplings]", "[torsion_couplings]", "[improper_couplings]")
+        if not skip:
+            out.append(line)
+    twin = path.replace(".fep", "_plain.fep")
+    open(twin, "w").write("\n".join(out))
+    return twin
+
+
+def _dihedral(x, i, j, k, l):
+    rji, rjk, rkl = x[i] - x[j], x[k] - x[j], x[l] - x[k]
+    nj, nk = np.cross(rji, rjk), -np.cross(rjk, rkl)
+    phi = np.arccos(np.clip(nj @ nk / np.linalg.norm(nj) / np.linalg.norm(nk), -1, 1))
+    return -phi if rjk @ np.cross(nj, nk) < 0 else phi
+
+
+def test_oracle_morse_couplings_match_numpy(tmp_path, oracle):
+    """Q angles, torsions and impropers coupled to a Morse bond (qangle,
+    qtorsion, qimproper with EVB couplings): against the same system without
+    the coupling sections, each coupled term's energy is scaled by
+    gamma = EMorseD of the bond, or 1 - EMorseD for a flagged improper; in
+    state 2 the bond is absent and EMorseD keeps state 1's value."""
+    from q_b200.inputs import derive_inp, inp_sections
+    g = synth.fep_solute(str(tmp_path / "c"), q_bonded=True, morse_couplings=True)
+    twin = derive_inp(g.inp, "plain.inp", set_keys={"files": {"fep": _strip_couplings(g.fep).split("/")[-1]}})
+    res = {}
+    for name, inp in (("cpl", g.inp), ("plain", twin)):
+        s = System.open(inp, lambdas=(0.5, 0.5))
+        o = oracle.create(s)
+        o.final_energy()
+        res[name] = (s, o.energy_vectors()[1], o.coords().reshape(-1, 3))
+    s, EQc, x = res["cpl"]
+    EQp = res["plain"][1]
+    v = s.view
+    S = v.nstates
+    assert v.nqangle and [v.qang_cpl[k] for k in range(v.nqangle)].count(0) >= 1
+    b = 0                                            # the coupled bond: Morse in state 1 only
+    i, j = v.qbnd_i[b], v.qbnd_j[b]
+    r = np.linalg.norm(x[j] - x[i])
+    db = r - v.qbnd_r0[b * S + 0]
+    fe = np.exp(-v.qbnd_amz[b * S + 0] * db)
+    emorse = -(fe * fe - 2 * fe) if db > 0 else 1.0
+    want = {"angle": np.zeros(S), "torsion": np.zeros(S), "improper": np.zeros(S)}
+    for a in range(v.nqangle):
+        if v.qang_cpl[a] != b:
+            continue
+        ia, ja, ka = v.qang_i[a], v.qang_j[a], v.qang_k[a]
+        u, w = x[ia] - x[ja], x[ka] - x[ja]
+        ang = np.arccos(np.clip(u @ w / np.linalg.norm(u) / np.linalg.norm(w), -1, 1))
+        for st in range(S):
+            if v.qang_on[a * S + st]:
+                ae = 0.5 * v.qang_fk[a * S + st] * (ang - v.qang_th0[a * S + st]) ** 2
+                want["angle"][st] += ae * (emorse - 1.0)
+    for t in range(v.nqtor):
+        if v.qtor_cpl[t] != b:
+            continue
+        phi = _dihedral(x, v.qtor_i[t], v.qtor_j[t], v.qtor_k[t], v.qtor_l[t])
+        for st in range(S):
+            if v.qtor_on[t * S + st]:
+                pe = v.qtor_fk[t * S + st] * (1 + np.cos(v.qtor_rmult[t * S + st] * phi - v.qtor_deltor[t * S + st]))
+                want["torsion"][st] += pe * (emorse - 1.0)
+    for t in range(v.nqimp):
+        if v.qimp_cpl[t] != b:
+            continue
+        phi = _dihedral(x, v.qimp_i[t], v.qimp_j[t], v.qimp_k[t], v.qimp_l[t])
+        g_ = 1.0 - emorse if v.qimp_cpl_flag[t] == 1 else emorse
+        for st in range(S):
+            if v.qimp_on[t * S + st]:
+                arg = phi - v.qimp_imp0[t * S + st]
+                arg -= 2 * np.pi * np.round(arg / (2 * np.pi))
+                want["improper"][st] += 0.5 * v.qimp_fk[t * S + st] * arg * arg * (g_ - 1.0)
+    for term, want_d in want.items():
+        k = list(EQ_NAMES).index(term)
+        assert np.allclose(EQc[:, k] - EQp[:, k], want_d, atol=1e-9, rtol=1e-9), term
+
+
+def test_coupling_refusals(tmp_path):
+    """A coupling to a bond that is harmonic in some state stops
+    qatom_load_fep (bond_harmonic_in_any_state, qatom.f90:1423); a coupled
+    term present in a state before its bond is would read EMorseD of a
+    previous step, and is refused."""
+    g = synth.fep_solute(str(tmp_path / "c"), q_bonded=True, morse_couplings=True)
+    txt = open(g.fep).read()
+    # bond 1 harmonic in state 1: the coupling is refused as qatom does
+    bad1 = txt.replace("[change_bonds]\n1 2 1 0", "[change_bonds]\n1 2 3 0")
+    open(g.fep, "w").write(bad1)
+    with pytest.raises(QBError) as e:
+        System.open(g.inp)
+    assert e.value.code == 3 and "harmonic" in str(e.value)
+    # the bond only in state 2, its coupled angles in both
+    bad2 = txt.replace("[change_bonds]\n1 2 1 0", "[change_bonds]\n1 2 0 1")
+    open(g.fep, "w").write(bad2)
+    with pytest.raises(QBError) as e:
+        System.open(g.inp)
+    assert e.value.code == 4 and "previous step" in str(e.value)

@@ -127,3 +127,27 @@ def test_qfep_driver_reads_off_diagonal_records(tmp_path):
         nf, "\n".join(names))
     assert run(io.StringIO(text2), bad) == 1
     assert "Maybe there are less than 2 off-diagonal elements?" in bad.getvalue()
+
+
+def test_morse_couplings_match_oracle(tmp_path, oracle):
+    """EVB Morse couplings on the GPU (qangle, qurey_bradley, qtorsion,
+    qimproper with couplings to a Morse bond that exists in state 1 only):
+    an AMBER and a CHARMM system in one batch against the oracle over 20
+    steps, the couplings' gradient on the bond atoms included."""
+    from tests.test_gpu_parity import G_TOL, _worst_atoms, assert_energies, grad_err
+    gens = [synth.fep_solute(str(tmp_path / ("ff%d" % ff)), ff_type=ff, q_bonded=True, morse_couplings=True)
+            for ff in (2, 3)]
+    systems = [System.open(g.inp, lambdas=(0.5, 0.5), seed=9) for g in gens]
+    assert all(s.view.qang_cpl[0] == 0 and s.view.qimp_cpl_flag[0] == 1 for s in systems)
+    b = Batch(systems, precision=FP64)
+    b.run(20)
+    for k, s in enumerate(systems):
+        o = oracle.create(s)
+        o.run(20)
+        sg, Eg, EQg = b.history(k, 0)
+        so, Eo, EQo = o.history(0)
+        assert list(sg) == list(so)
+        for m in range(len(sg)):
+            assert_energies(Eg[m], EQg[m], Eo[m], EQo[m])
+        err = grad_err(b.gradient(k), o.gradient())
+        assert err < G_TOL, (k, err, _worst_atoms(b.gradient(k), o.gradient()))

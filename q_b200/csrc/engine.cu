@@ -341,16 +341,18 @@ struct Batch {
     DevPtrs &p = P;
     if (due) build_lists(0);
     pot_energy();
-    launch("leapfrog", [&] { k_leapfrog<<<cdiv(p.natoms_tot, 256), 256, 0, stream>>>(p); });
-    // the two SHAKE kernels move disjoint atoms
-    if (any_shake && p.nsh3 > 0 && p.nshg > 0) fork_streams();
-    if (any_shake && p.nsh3 > 0)
-      launch("shake", [&] { k_shake3<<<cdiv(p.nsh3, 128), 128, 0, stream>>>(p); });
-    if (any_shake && p.nshg > 0) {
-      cudaStream_t s1 = forking() && p.nsh3 > 0 ? side[0] : stream;
-      launch("shake_general", [&] { k_shake_general<<<p.nshg, SHG_BLOCK, p.shg_smem, s1>>>(p); });
-    }
-    if (any_shake && p.nsh3 > 0 && p.nshg > 0) join_streams();
+    // 3-constraint molecules (waters) take leapfrog and SHAKE in one pass; the
+    // other atoms leapfrog, then the general SHAKE; the two paths move
+    // disjoint atoms
+    const bool fused = any_shake && p.nsh3 > 0;
+    if (fused) fork_streams();
+    if (fused)
+      launch("leapfrog_shake3", [&] { k_leapfrog_shake3<<<cdiv(p.nsh3, 128), 128, 0, stream>>>(p); });
+    cudaStream_t sl = fused && forking() ? side[0] : stream;
+    launch("leapfrog", [&] { k_leapfrog<<<cdiv(p.natoms_tot, 256), 256, 0, sl>>>(p); });
+    if (any_shake && p.nshg > 0)
+      launch("shake_general", [&] { k_shake_general<<<p.nshg, SHG_BLOCK, p.shg_smem, sl>>>(p); });
+    if (fused) join_streams();
     launch("finish", [&] { k_finish<<<nsys, 32, 0, stream>>>(p, 1); });
     check_launch("step kernels");
   }
@@ -817,6 +819,9 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     }
     P.nsh3 = (int)at3.size(); P.nshg = (int)gen.size();
     P.sh3_at = dev_upload(at3, o); P.sh3_d2 = dev_upload(d3, o);
+    // their atoms are moved by the fused leapfrog + SHAKE kernel, not k_leapfrog
+    for (auto &a : at3) { flags[a.x] |= F_SH3; flags[a.y] |= F_SH3; flags[a.z] |= F_SH3; }
+    if (!at3.empty()) CUDA_TRY(cudaMemcpy(P.flags, flags.data(), flags.size(), cudaMemcpyHostToDevice));
     // other molecules: local atoms, constraints grouped into dependency levels
     std::vector<int4> info, info2;
     std::vector<int> gat, glev;

@@ -23,7 +23,8 @@ constexpr int MAX_SHELLS = 4;
 // one history record: step, E[QB_NE], EQ[MAXS*QB_NEQ], r_kl of the off-diagonal functions [MAXS]
 constexpr int HIST_REC = 1 + QB_NE + MAXS * QB_NEQ + MAXS;
 constexpr int NQ_SHARED = 64;    // Q atoms whose water forces are reduced in shared memory
-enum AtomFlags : uint8_t { F_EXCL = 1, F_SHELL = 2, F_HEAVY = 4, F_SHAKE = 8 };   // F_SHAKE: in a SHAKE constraint
+// F_SHAKE: in a SHAKE constraint; F_SH3: in a 3-constraint molecule, moved by k_leapfrog_shake3
+enum AtomFlags : uint8_t { F_EXCL = 1, F_SHELL = 2, F_HEAVY = 4, F_SHAKE = 8, F_SH3 = 16 };
 
 // A non-Q atom of a solute charge group with its interaction parameters for
 // the water O and H sites: LJ products A(O), B(O), A(H), B(H) and single

@@ -2120,8 +2120,9 @@ __global__ void k_leapfrog(DevPtrs P) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   int s = -1;
   double acc[4] = {0, 0, 0, 0};
-  // a system that raised an error stays where the failing step left it
-  if (g < P.natoms_tot && P.st[P.asys[g]].status == 0) {
+  // a system that raised an error stays where the failing step left it;
+  // atoms of 3-constraint molecules are k_leapfrog_shake3's
+  if (g < P.natoms_tot && P.st[P.asys[g]].status == 0 && !(P.flags[g] & F_SH3)) {
     s = P.asys[g];
     const SysDev &S = P.sys[s];
     double ts = (g - S.aoff) < S.nsol ? P.st[s].Tscale_sol : P.st[s].Tscale_solv;
@@ -2183,7 +2184,26 @@ __device__ __forceinline__ bool shake_pair(double3 &xi, double3 &xj, const doubl
 // (rigid waters), one thread per molecule.  The atoms are relabelled on the
 // host so that the constraints, in their own order, join (0,1), (0,2), (1,2);
 // sweeps, readiness flags and the 1000-sweep limit are the reference's.
-__global__ void __launch_bounds__(128, 6) k_shake3(DevPtrs P) {
+// k_leapfrog's update of atom g of system sys: the new velocity and position.
+__device__ __forceinline__ void leapfrog_atom(const DevPtrs &P, int sys, int g, double4 &v, double3 &xn) {
+  const SysDev &S = P.sys[sys];
+  const double dt = S.dt;
+  const double ts = (g - S.aoff) < S.nsol ? P.st[sys].Tscale_sol : P.st[sys].Tscale_solv;
+  const double w = (double)P.winv[g];
+  const double4 x = P.x[g], d = P.d[g];
+  v = P.v[g];
+  v.x = (v.x - d.x * w * dt) * ts;
+  v.y = (v.y - d.y * w * dt) * ts;
+  v.z = (v.z - d.z * w * dt) * ts;
+  xn = make_double3(x.x + v.x * dt, x.y + v.y * dt, x.z + v.z * dt);
+}
+
+// Leapfrog (md.f90:4082-4110) and shake (14445) of one 3-constraint molecule
+// per thread: the update of k_leapfrog for its three atoms, then the SHAKE
+// sweeps on the new positions against the old ones, in registers; x and v
+// are written once.  Without convergence the leapfrog values stay, as the
+// separate kernels leave them (recomputed, bit for bit, on that rare path).
+__global__ void __launch_bounds__(128, 4) k_leapfrog_shake3(DevPtrs P) {
   int m = blockIdx.x * blockDim.x + threadIdx.x;
   int sys = -1, its = 0;
   double acc[4] = {0, 0, 0, 0};
@@ -2191,8 +2211,15 @@ __global__ void __launch_bounds__(128, 6) k_shake3(DevPtrs P) {
     const int4 at = P.sh3_at[m];
     const double4 d2 = P.sh3_d2[m];
     sys = at.w;
-    double3 x0 = ld3(P.x, at.x), x1 = ld3(P.x, at.y), x2 = ld3(P.x, at.z);
-    const double3 r0 = ld3(P.xx, at.x), r1 = ld3(P.xx, at.y), r2 = ld3(P.xx, at.z);
+    const int ids[3] = {at.x, at.y, at.z};
+    double3 x0, x1, x2;
+    {
+      double4 v;
+      leapfrog_atom(P, sys, at.x, v, x0);
+      leapfrog_atom(P, sys, at.y, v, x1);
+      leapfrog_atom(P, sys, at.z, v, x2);
+    }
+    const double3 r0 = ld3(P.x, at.x), r1 = ld3(P.x, at.y), r2 = ld3(P.x, at.z);
     const float w0 = P.winv[at.x], w1 = P.winv[at.y], w2 = P.winv[at.z];
     bool c0 = false, c1 = false, c2 = false;
     for (;;) {
@@ -2207,7 +2234,6 @@ __global__ void __launch_bounds__(128, 6) k_shake3(DevPtrs P) {
       const SysDev &S = P.sys[sys];
       const double dt = S.dt;
       double3 xs[3] = {x0, x1, x2}, rs[3] = {r0, r1, r2};
-      const int ids[3] = {at.x, at.y, at.z};
 #pragma unroll
       for (int a = 0; a < 3; a++) {
         double4 o = P.x[ids[a]];
@@ -2221,6 +2247,16 @@ __global__ void __launch_bounds__(128, 6) k_shake3(DevPtrs P) {
         kin_add(P, S, ids[a], v, acc);
       }
     } else {
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        double4 v;
+        double3 xn;
+        leapfrog_atom(P, sys, ids[a], v, xn);
+        double4 o = P.x[ids[a]];
+        o.x = xn.x; o.y = xn.y; o.z = xn.z;
+        P.x[ids[a]] = o;
+        P.v[ids[a]] = v;
+      }
       set_status(&P.st[sys], QB_ERR_SHAKE);
     }
   }

@@ -2203,7 +2203,7 @@ __device__ __forceinline__ void leapfrog_atom(const DevPtrs &P, int sys, int g, 
 // sweeps on the new positions against the old ones, in registers; x and v
 // are written once.  Without convergence the leapfrog values stay, as the
 // separate kernels leave them (recomputed, bit for bit, on that rare path).
-__global__ void __launch_bounds__(128, 4) k_leapfrog_shake3(DevPtrs P) {
+__global__ void __launch_bounds__(128, 6) k_leapfrog_shake3(DevPtrs P) {
   int m = blockIdx.x * blockDim.x + threadIdx.x;
   int sys = -1, its = 0;
   double acc[4] = {0, 0, 0, 0};

@@ -3,36 +3,42 @@
 
 Workload (one GPU): the batched FEP configuration -- 21 uniform lambda windows
 x 4 seeded replicas of the 56-atom, 8-Q-atom FEP solute in a 20 A TIP3P sphere
-(2 fs, SHAKE on X-H and water, 10 A cut-offs + LRF) plus 16 TIP3P spheres with
-radii drawn from {15, 20, 25} A (1 fs), all stepped together in one batch.
+(2 fs, SHAKE on X-H bonds and water, 10 A cut-offs + LRF) plus 16 TIP3P spheres
+with radii drawn from {15, 20, 25} A (1 fs), all stepped together in one batch.
 Synthetic, seeded inputs of those shapes (q_b200/synth.py).
 
 A step is one MD step of every system.  `value` is the aggregate simulated
 ns/day over all systems and ranks with the state resident in HBM, timed with
-CUDA events on the engine's stream; `e2e` is the same metric through the C ABI
-with host buffers: coordinates and velocities uploaded, the steps run, energy
-records and final coordinates read back, all inside the timed region.
+CUDA events on the engine's stream around exactly --steps steps; the timed
+steps start on a pair-list rebuild step, so they hold the rebuilds (and the
+energy-recording steps) of their share of list cycles (counted in the line).
+`e2e` is the same metric through the C ABI with host buffers: coordinates and
+velocities of every system uploaded, the steps run, the energy records and
+coordinates read back, all inside the timed region, one copy per direction
+through the batch's page-locked staging.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl qb|reference]
                     [--precision fp64|mixed]
 
-At one GPU the line also carries the second half of the metric (`dG`,
-`gpu_s_per_dG`): the perturbation's BAR free energy from 21 uniform windows x
---dg-replicas replicas in one mixed-precision batch, its device seconds, the
-plain FP64 engine's device seconds for the same windows, replicas and steps
-run one system per launch (its per-step time measured here), and the error
-against a dense 41-window FP64 run of the same perturbation.
+At one GPU the line also carries single-system lines of the three plain
+configurations (per_config: the 15 A water sphere, the FEP solute in 20 A, the
+protein-ligand sphere in 25 A; FP64, one system per batch) and the second half
+of the metric (`dG`, `gpu_s_per_dG`): the perturbation's BAR free energy from
+21 uniform windows x --dg-replicas replicas in one mixed-precision batch, its
+device seconds, the plain FP64 engine's device seconds for the same windows,
+replicas and steps run one system per launch, and the error against a dense
+41-window FP64 run of the same perturbation.
 
 Under torchrun each rank runs its own copy of the batch (weak scaling); time is
-the maximum over ranks.  `--impl reference` times the CPU oracle (the
-restatement of Q's Fortran step, which cannot be compiled here) on a bounded
-sample of the same workload with every host core.
+the maximum over ranks.  `--impl reference` runs the reference's algorithm on
+the host cores: the CPU oracle (the restatement of Q's Fortran step, which
+cannot be compiled here) steps the same batch, every system in its own process
+spread over all cores by cost, wall-clocked as the slowest worker.
 """
 from __future__ import annotations
 
 import argparse
 import json
-import math
 import multiprocessing as mp
 import os
 import subprocess
@@ -48,7 +54,6 @@ METRIC = "aggregate ns/day (batched λ-windows) & GPU-s per ΔG at ≤0.1 kcal/m
 WORKLOAD = ("21 lambda windows x 4 replicas of the 56-atom 8-Q-atom FEP solute in a 20 A TIP3P sphere "
             "(2 fs) + 16 TIP3P spheres R in {15,20,25} A (1 fs), one batch")
 FLOP_WW = 229        # per SPC/TIP3P molecule pair (1 LJ+Coulomb, 8 Coulomb)
-FLOP_LJC = 37        # per LJ+Coulomb atom pair
 
 
 def parse():
@@ -63,6 +68,7 @@ def parse():
     p.add_argument("--spheres", type=int, default=16)
     p.add_argument("--equil", type=int, default=100, help="untimed equilibration steps (in addition to warm-up)")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-configs", action="store_true", help="skip the single-system lines of the plain configs")
     p.add_argument("--no-autotune", action="store_true", help="keep the default tile sizes and streams")
     p.add_argument("--dg-replicas", type=int, default=16,
                    help="replicas of the batched mixed-precision perturbation for the GPU-s per dG comparison "
@@ -77,6 +83,8 @@ def parse():
 def workload_files(root: str, rank: int, args):
     """Generate (or reuse) the Q input files of the batch; returns a list of
     (inp, lambdas, seed, dt_fs)."""
+    import numpy as np
+
     from q_b200 import synth
     from q_b200.synth import window_lambdas
     os.makedirs(root, exist_ok=True)
@@ -85,15 +93,27 @@ def workload_files(root: str, rank: int, args):
     for r in range(args.replicas):
         for lam in window_lambdas(args.windows):
             systems.append((c1.inp, lam, 1 + r + 1000 * rank, 2.0))
-    rng_radii = [15.0, 20.0, 25.0]
-    import numpy as np
     rr = np.random.default_rng(4321 + rank)
     for k in range(args.spheres):
-        R = float(rr.choice(rng_radii))
+        R = float(rr.choice([15.0, 20.0, 25.0]))
         g = synth.water_sphere(os.path.join(root, "sph%02d" % k), radius=R, seed=1234 + 100 + k, steps=10000,
                                name="sph%02d" % k)
         systems.append((g.inp, None, 1 + k + 1000 * rank, 1.0))
     return systems
+
+
+def config_files(root: str):
+    """The three plain single-system configurations: (name, inp, lambdas,
+    dt_fs, description)."""
+    from q_b200 import synth
+    c0 = synth.water_sphere(os.path.join(root, "cfg_c0"), radius=15.0, seed=1234, steps=1000, name="c0")
+    c1 = synth.fep_solute(os.path.join(root, "cfg_c1"), seed=1234, steps=5000)
+    c2 = synth.polymer_sphere(os.path.join(root, "cfg_c2"), seed=1234, steps=5000)
+    return [("c0_water_sphere_15A", c0.inp, None, 1.0, "TIP3P sphere R 15 A, 1 fs, LRF, SHAKE, restraints"),
+            ("c1_fep_solute_20A", c1.inp, (0.5, 0.5), 2.0,
+             "56-atom solute, 8 two-state Q atoms (soft-core), lambda 0.5, 20 A TIP3P sphere, 2 fs"),
+            ("c2_protein_ligand_25A", c2.inp, (0.5, 0.5), 2.0,
+             "3000-atom polymer around the FEP solute, 25 A sphere, atoms beyond 23 A restrained, Q cut-off 99")]
 
 
 class ClockSampler:
@@ -158,74 +178,194 @@ class ClockSampler:
         return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def _oracle_worker(job):
-    """CPU oracle on one system for a bounded number of steps (spawned process)."""
-    inp, lam, seed, steps, equil = job
+# ------------------------------------------------------------- step plans
+
+def step_kinds(views, start: int, k: int) -> tuple[int, int]:
+    """(pair-list rebuild steps, energy-evaluating steps) among steps
+    start..start+k-1 of a run call: rebuilds where any system's non_bond
+    interval divides the step, energies where any system records an output
+    or energy-file record, and on the call's last step."""
+    rebuild = energy = 0
+    for i in range(k):
+        s = start + i
+        if any(s % v.NBcycle == 0 for v in views):
+            rebuild += 1
+        if i == k - 1 or any((v.iout_cycle > 0 and s % v.iout_cycle == 0) or
+                             (v.iene_cycle > 0 and s > 0 and s % v.iene_cycle == 0) for v in views):
+            energy += 1
+    return rebuild, energy
+
+
+def align_to_rebuild(batch, views) -> int:
+    """Run the few steps up to the next pair-list rebuild; returns them."""
+    nb = min(v.NBcycle for v in views)
+    extra = (-batch.step_count()) % nb
+    if extra:
+        batch.run(extra)
+    return extra
+
+
+def pair_interactions(w) -> float:
+    """Atom-pair interactions of one step from the list totals: 9 per water-
+    water molecule pair (md.f90:8276), solute-water and solute-solute atom
+    pairs, Q-solute pairs x states, Q-water pairs x states x 3 sites."""
+    return 9.0 * w[0] + w[1] + w[2] + w[3] + 3.0 * w[4]
+
+
+# --------------------------------------------------------------- CPU side
+
+def _oracle_worker(job, out):
+    """The CPU oracle on some systems (spawned process, one thread): warm-up
+    steps, a barrier, then the timed steps; puts (seconds, natoms) on out."""
+    specs, steps, warm, barrier = job
     sys.path.insert(0, REPO)
     from q_b200 import System
     from tests.oracle_binding import load_oracle
-    s = System.open(inp, lambdas=lam, seed=seed)
-    o = load_oracle().create(s)
-    if equil:
-        o.run(equil)
+    lib = load_oracle()
+    runs = []
+    natoms = 0
+    for inp, lam, seed in specs:
+        s = System.open(inp, lambdas=lam, seed=seed)
+        runs.append((s, lib.create(s)))
+        natoms += s.natom
+    for _, o in runs:
+        if warm:
+            o.run(warm)
+    if barrier is not None:
+        barrier.wait()
     t0 = time.perf_counter()
-    o.run(steps)
-    return time.perf_counter() - t0, s.natom
+    for _, o in runs:
+        o.run(steps)
+    out.put((time.perf_counter() - t0, natoms))
 
 
-def cpu_sample(systems, threads: int, budget_steps: int = 25):
-    """Time the oracle on a sample: one system of each shape (the FEP window
-    and one water sphere per radius), one full pair-list cycle (25 steps) each,
-    extrapolated to the whole batch.  Returns (ns/day on one core, wall
-    seconds, description)."""
+def oracle_batch(systems, steps: int, warm: int, workers: int):
+    """The oracle stepping every system of the batch `steps` steps, systems
+    spread over `workers` processes by atom count (one thread each); wall
+    time is the slowest worker's, timed after a common barrier."""
+    from q_b200 import System
+    from q_b200.dist import shard
+    natom = []
+    for inp, lam, seed, dt in systems:
+        s = System.open(inp, lambdas=lam, seed=seed)
+        natom.append(s.natom)
+        s.close()
+    workers = max(1, min(workers, len(systems)))
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(workers)
+    q = ctx.Queue()
+    procs = []
+    for r in range(workers):
+        mine = shard(len(systems), r, workers, natom)
+        job = ([(systems[i][0], systems[i][1], systems[i][2]) for i in mine], steps, warm, barrier)
+        procs.append(ctx.Process(target=_oracle_worker, args=(job, q)))
+    for p in procs:
+        p.start()
+    res = [q.get() for _ in procs]
+    for p in procs:
+        p.join()
+    return max(r[0] for r in res), sum(r[1] for r in res)
+
+
+def cpu_sample(systems, budget_steps: int = 25):
+    """The oracle on one core over a bounded sample: one system of each shape
+    (the FEP window and one water sphere per size), one pair-list cycle each,
+    scaled to the batch by the shape counts.  Returns (ns/day, description)."""
     shapes = {}
     for inp, lam, seed, dt in systems:
-        key = open(inp).read().split("topology", 1)[0] if lam is None else inp
-        natom_key = os.path.getsize(os.path.join(os.path.dirname(inp), [l.split()[1] for l in open(inp)
-                                                                        if l.startswith("topology")][0]))
-        key = (lam is None, natom_key // 20000)
+        key = (lam is None, inp if lam is not None else os.path.getsize(inp.replace(".inp", ".top")) // 20000)
         if key not in shapes:
             shapes[key] = [inp, lam, seed, dt, 0]
         shapes[key][4] += 1
-    jobs = [(inp, lam, seed, budget_steps, 0) for inp, lam, seed, dt, cnt in shapes.values()]
-    ctx = mp.get_context("spawn")
-    t0 = time.perf_counter()
-    with ctx.Pool(max(1, min(threads, len(jobs)))) as pool:
-        res = pool.map(_oracle_worker, jobs)
-    wall = time.perf_counter() - t0
-    per_step = 0.0
-    sim_fs = 0.0
-    for (inp, lam, seed, dt, cnt), (sec, natom) in zip(shapes.values(), res):
+    per_step, sim_fs = 0.0, 0.0
+    for inp, lam, seed, dt, cnt in shapes.values():
+        sec, _ = oracle_batch([(inp, lam, seed, dt)], budget_steps, 0, 1)
         per_step += cnt * sec / budget_steps
         sim_fs += cnt * dt
-    ns_day_1core = sim_fs * 1e-6 / per_step * 86400
-    desc = ("CPU oracle (C, FP64) on %d representative systems x %d steps (one pair-list cycle), "
-            "extrapolated to the %d-system batch" % (len(jobs), budget_steps, len(systems)))
-    return ns_day_1core, wall, desc
+    ns_day = sim_fs * 1e-6 / per_step * 86400
+    desc = ("CPU oracle (C, FP64), one thread, on %d representative systems x %d steps (one pair-list cycle), "
+            "scaled to the %d-system batch by shape counts" % (len(shapes), budget_steps, len(systems)))
+    return ns_day, desc
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the CPU oracle over a bounded sample with every host core."""
+    """--impl reference: the CPU oracle steps the actual batch on every host core."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
     root = os.path.join(tempfile.gettempdir(), "qb_bench_inputs")
     systems = workload_files(root, 0, args)
-    per_step_steps = 25
-    # each timed step: a bounded sample of the batch spread over the cores;
-    # throughput scaled to the whole batch on `threads` cores
-    ns_1core, wall, desc = cpu_sample(systems, threads, budget_steps=per_step_steps)
-    value = ns_1core * threads
+    steps = args.steps
+    # warm-up rounded up to whole pair-list cycles: the timed steps start on a
+    # rebuild step, as the GPU arm's do
+    nb = 25
+    warm = -(-max(args.warmup, 0) // nb) * nb
+    sec, natoms = oracle_batch(systems, steps, warm, threads)
+    sim_ns = sum(dt for _, _, _, dt in systems) * steps * 1e-6
+    value = sim_ns / sec * 86400.0
+    sample = ("measured: CPU oracle (C, FP64 restatement of qdyn's step; Fortran qdyn cannot be compiled on this "
+              "image) stepping all %d systems (%d atoms) of the batch for %d steps after %d warm-up steps (the "
+              "timed steps start on a pair-list rebuild, non_bond 25), one process per core on %d cores, systems "
+              "spread by atom count, wall time of the slowest process" % (len(systems), natoms, steps, warm, threads))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "systems": len(systems)},
-        "cpu_baseline": {"value": value, "unit": "ns/day", "cores": threads, "kind": "port",
-                         "sample": desc + "; Fortran qdyn cannot be compiled on this image (no Fortran compiler)"},
+        "steps": steps, "warmup": args.warmup, "ms_per_step": sec / steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "systems": len(systems), "atoms": natoms},
+        "cpu_baseline": {"value": value, "unit": "ns/day", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU side
+
+def per_config_lines(root: str, device: int, steps: int = 200):
+    """ns/day, pair interactions/s and the top kernel of each plain single-
+    system configuration (FP64, one system per batch), beside the oracle on
+    one core for one pair-list cycle of the same system."""
+    from q_b200 import FP64, Batch, System
+    from q_b200.api import peak_tflops
+    out = {}
+    peak64 = peak_tflops(FP64, device)
+    for name, inp, lam, dt, desc in config_files(root):
+        s = System.open(inp, lambdas=lam, seed=11)
+        b = Batch([s], precision=FP64, device=device)
+        b.run(50)
+        align_to_rebuild(b, [s.view])
+        start = b.step_count()
+        ms, launches = b.run_timed(steps)
+        rebuild, energy = step_kinds([s.view], start, steps)
+        w = b.workload()
+        b.set_profiling(True)
+        b.run(steps)
+        prof = b.profile()
+        b.set_profiling(False)
+        tot = sum(v[0] for v in prof.values()) or 1.0
+        top = max(prof.items(), key=lambda kv: kv[1][0])
+        ww = prof.get("nb_ww", (0.0, 1))
+        ww_ms = ww[0] / max(ww[1], 1)
+        per_step = ms / steps
+        line = {"description": desc, "precision": "fp64", "atoms": s.natom, "dt_fs": dt,
+                "ns_per_day": dt * 1e-6 / (per_step * 1e-3) * 86400.0, "ms_per_step": per_step,
+                "pair_interactions_per_s": pair_interactions(w) / (per_step * 1e-3),
+                "pair_interactions_per_step": pair_interactions(w), "steps": steps,
+                "rebuild_steps_in_timed_region": rebuild, "energy_steps_in_timed_region": energy,
+                "gpu_launches": launches,
+                "top_kernel": top[0], "top_kernel_share": top[1][0] / tot,
+                "kernels_ms_per_step": {k: round(v[0] / steps, 5) for k, v in
+                                        sorted(prof.items(), key=lambda kv: -kv[1][0])[:6]}}
+        if w[0] > 0 and ww_ms > 0:
+            ach = FLOP_WW * w[0] / (ww_ms * 1e-3) / 1e12
+            line["roofline_nb_ww"] = {"bound": "fp64", "achieved": ach, "peak": peak64, "unit": "TFLOP/s",
+                                      "frac": ach / peak64, "launch_ms": ww_ms,
+                                      "peak_source": "measured FP64 FMA loop (qb_peak_flops)"}
+        b.close()
+        sec, _ = oracle_batch([(inp, lam, 11, dt)], 25, 0, 1)
+        line["cpu_oracle_1core_ns_per_day"] = dt * 1e-6 / (sec / 25) * 86400.0
+        out[name] = line
+        s.close()
+    return out
 
 
 def main():
@@ -235,9 +375,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     dist = None
     if world > 1:
+        import datetime
+
         import torch
         import torch.distributed as dist_
-        import datetime
         dist = dist_
         if args.impl == "qb":
             torch.cuda.set_device(local)
@@ -251,14 +392,19 @@ def main():
         return
 
     import numpy as np
+    import torch
+
     from q_b200 import FP64, MIXED, Batch, System
     from q_b200.api import peak_tflops
+    from q_b200.dist import max_over_ranks
 
+    dev = "cuda:%d" % local
     prec = FP64 if args.precision == "fp64" else MIXED
     root = os.path.join(tempfile.gettempdir(), "qb_bench_inputs_r%d" % rank)
     t0 = time.perf_counter()
     specs = workload_files(root, rank, args)
     systems = [System.open(inp, lambdas=lam, seed=seed) for inp, lam, seed, dt in specs]
+    views = [s.view for s in systems]
     setup_s = time.perf_counter() - t0
     dts = np.array([dt for _, _, _, dt in specs])
     natoms = sum(s.natom for s in systems)
@@ -274,105 +420,123 @@ def main():
         if dist:
             dist.barrier()
 
-    import torch
     barrier()
-    torch.cuda.synchronize(local) if torch.cuda.is_available() else None
+    torch.cuda.synchronize(local)
     with ClockSampler(local) as clk:
-        batch.run(max(args.warmup, 3) + 20)      # the sampler starts while the GPU is busy
+        batch.run(20)                 # the sampler starts while the GPU is busy
+        align_to_rebuild(batch, views)
+        start = batch.step_count()
         clk.mark("t0")
         ms, launches = batch.run_timed(args.steps)
         clk.mark("t1")
     barrier()
-    elapsed = ms / 1e3
-    if dist:
-        t = torch.tensor([elapsed], device="cuda:%d" % local, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    rebuild, energy = step_kinds(views, start, args.steps)
+    elapsed = max_over_ranks(ms / 1e3, dev)
     sim_ns = float(dts.sum()) * args.steps * 1e-6 * world
     value = sim_ns / elapsed * 86400.0
-
-    # workload totals of the current lists, for the roofline
     w = batch.workload()
-    ww_pairs, pw_pairs, pp_pairs = w[0], w[1], w[2]
+    pairs_step = pair_interactions(w)
 
-    # per-kernel device times (separate profiled pass of the same length)
+    # whole pair-list cycles, for comparison with the K-step figure
+    ncyc = 4 * min(v.NBcycle for v in views)
+    align_to_rebuild(batch, views)
+    ms_cyc, _ = batch.run_timed(ncyc)
+    ms_cyc = max_over_ranks(ms_cyc, dev)
+
+    # per-kernel device times: a separate profiled pass (one kernel at a time,
+    # one stream) over the same step kinds
+    align_to_rebuild(batch, views)
     batch.set_profiling(True)
     batch.run(args.steps)
     prof = batch.profile()
     batch.set_profiling(False)
-    tot = sum(v[0] for v in prof.values())
+    tot = sum(v[0] for v in prof.values()) or 1.0
     top = max(prof.items(), key=lambda kv: kv[1][0])
-    ww = prof.get("nb_ww", (0.0, 1))
-    ww_ms = ww[0] / max(ww[1], 1)
-    ww_flop = FLOP_WW * ww_pairs
+    kname = "nb_ww_x2" if "nb_ww_x2" in prof else "nb_ww"
+    kk = prof.get(kname, (0.0, 1))
+    k_ms = kk[0] / max(kk[1], 1)
+    ww_flop = FLOP_WW * w[0]
     peak = peak_tflops(FP64 if prec == FP64 else MIXED, local)
     traffic = None
     try:
         tj = json.load(open(os.path.join(REPO, "profiles", "traffic.json")))
-        traffic = tj.get(args.precision, {}).get("bytes_per_launch")
+        traffic = tj.get(kname, {}).get("bytes_per_launch")
     except (OSError, ValueError):
         pass
-    achieved = ww_flop / (ww_ms * 1e-3) / 1e12 if ww_ms > 0 else 0.0
+    achieved = ww_flop / (k_ms * 1e-3) / 1e12 if k_ms > 0 else 0.0
 
-    # end to end through the C ABI with host buffers: three repetitions, the
-    # median reported, with its upload / run / read-back split
-    xs = [batch.coords(k) for k in range(len(systems))]
-    vs = [batch.velocities(k) for k in range(len(systems))]
-    h2d = sum(x.nbytes + v.nbytes for x, v in zip(xs, vs))
+    # end to end through the C ABI with host buffers: every system's
+    # coordinates and velocities up, the steps, every system's records and
+    # coordinates down; three repetitions, the median reported
+    x0, v0 = batch.coords_all(), batch.velocities_all()
+    h2d = 2 * 32 * natoms                   # coordinates and velocities, one double4 per atom
+    # records a run of --steps steps can hold: output and energy-file intervals
+    max_rec = [args.steps // max(1, min(v.iout_cycle for v in views)) + 2,
+               args.steps // max(1, min(v.iene_cycle for v in views)) + 2]
     reps = []
     for _ in range(3):
         barrier()
         t0 = time.perf_counter()
-        for k in range(len(systems)):
-            batch.set_coords(k, xs[k])
-            batch.set_velocities(k, vs[k])
+        batch.set_coords_all(x0)
+        batch.set_velocities_all(v0)
         t1 = time.perf_counter()
         batch.run(args.steps)
         t2 = time.perf_counter()
         d2h = 0
-        for k in range(len(systems)):
-            st, E, EQ = batch.history(k, 0)
-            x = batch.coords(k)
-            d2h += E.nbytes + EQ.nbytes + st.nbytes + x.nbytes
+        for kind in (0, 1):
+            counts, rec, nbytes = batch.history_all(kind, max_records=max_rec[kind], with_bytes=True)
+            d2h += nbytes
+        x = batch.coords_all()
+        d2h += 32 * natoms                  # one double4 per atom
         batch.clear_history()
         t3 = time.perf_counter()
         reps.append((t3 - t0, t1 - t0, t2 - t1, t3 - t2))
     reps.sort()
     te, e2e_up, e2e_run, e2e_down = reps[1]
-    if dist:
-        t = torch.tensor([te], device="cuda:%d" % local, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        te = float(t.item())
+    te = max_over_ranks(te, dev)
     e2e = sim_ns / te * 86400.0
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = 1
-        ns_1core, wall, desc = cpu_sample(specs, threads=1, budget_steps=25)
-        cpu = {"value": ns_1core, "unit": "ns/day", "cores": threads, "kind": "port",
-               "sample": desc + "; single thread"}
+    per_config = None
+    if rank == 0 and world == 1:
+        if not args.no_cpu_baseline:
+            ns_1core, desc = cpu_sample(specs)
+            cpu = {"value": ns_1core, "unit": "ns/day", "cores": 1, "kind": "port", "sample": desc}
+        if not args.no_configs:
+            per_config = per_config_lines(root, local)
 
     line = {
         "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if prec == FP64 else "f32 pair math + f64 accumulation/LRF/SHAKE/update",
+        "dtype": "f64" if prec == FP64 else ("f32 water-water forces (packed FP32x2) on non-recording steps; f64 "
+                                             "energies, water-water pairs on recording steps, Q terms, LRF "
+                                             "expansion, SHAKE, update"),
         "data": "synthetic (seeded generator of the benchmark shapes)",
         "config": {"workload": WORKLOAD, "systems": len(systems), "atoms": natoms,
                    "precision": args.precision, "equilibration_steps": args.equil,
                    "l2": "per-step working set (coordinates, velocities, gradients, pair lists) exceeds the 126 MB L2",
                    "parallelism": "replicas only (%d GPU, whole systems per GPU)" % world,
+                   "c1_charges": "solute charges with hydrogens at +0.10 +- 0.04 and heavy atoms N(0, 0.35) "
+                                 "balancing to net 0 (the config's N(0, 0.3) on every atom bound water H to "
+                                 "solute H and failed SHAKE; see DESIGN)",
                    "setup_s": round(setup_s, 2),
                    "tuning": {k: (round(v, 5) if isinstance(v, float) else v) for k, v in tuning.items()}},
-        "roofline": {"kernel": "nb_ww (water-water SPC pair kernel)", "bound": "fp64" if prec == FP64 else "fp32",
+        "timed_region": {"first_step": start, "rebuild_steps_in_timed_region": rebuild,
+                         "energy_steps_in_timed_region": energy,
+                         "ms_per_step_whole_list_cycles": ms_cyc / ncyc, "whole_cycle_steps": ncyc},
+        "pair_interactions_per_s": pairs_step * args.steps * world / elapsed,
+        "pair_interactions_per_step": pairs_step,
+        "roofline": {"kernel": kname + " (water-water SPC forces)", "bound": "fp64" if prec == FP64 else "fp32",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
-                     "peak_source": "measured FMA loop (qb_peak_flops) on this GPU",
-                     "flop_per_launch": ww_flop, "launch_ms": ww_ms, "traffic": traffic,
+                     "peak_source": "measured FMA loop (qb_peak_flops) on this GPU, of measured",
+                     "flop_per_launch": ww_flop, "flop_basis": "229 FLOP x unique water-water molecule pairs",
+                     "launch_ms": k_ms, "traffic": traffic,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/traffic.json",
-                     "share_of_step": ww[0] / tot if tot else None,
-                     "top_kernel": top[0], "top_kernel_share": top[1][0] / tot if tot else None},
+                     "share_of_step": kk[0] / tot,
+                     "top_kernel": top[0], "top_kernel_share": top[1][0] / tot},
         "kernels_ms_per_step": {k: round(v[0] / args.steps, 5) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
-        "workload_per_step": {"ww_molecule_pairs": ww_pairs, "pw_pairs": pw_pairs, "pp_pairs": pp_pairs,
+        "workload_per_step": {"ww_molecule_pairs": w[0], "pw_pairs": w[1], "pp_pairs": w[2],
                               "qp_pairs_x_states": w[3], "qw_pairs_x_states": w[4],
                               "shake_iterations_mean": round(float(w[8]), 3), "shake_iterations_max": int(w[9])},
         "e2e": {"value": e2e, "unit": "ns/day", "h2d_bytes_per_step": h2d / args.steps,
@@ -383,6 +547,8 @@ def main():
     }
     if cpu:
         line["cpu_baseline"] = cpu
+    if per_config:
+        line["per_config"] = per_config
     batch.close()
     if rank == 0 and world == 1 and args.dg_replicas > 0:
         # second half of the metric: device seconds per dG, batched mixed

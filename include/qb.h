@@ -100,6 +100,10 @@ int qb_batch_create(qb_handle *const *systems, int n, const qb_options *opt, qb_
  * (md.f90:4003-4175): pair lists every NBcycle steps, potential and gradient,
  * leapfrog with Berendsen scaling, SHAKE, temperature.  Energy summaries are
  * recorded on the device at each system's output/energy intervals.
+ * Energies are evaluated on the steps that record them and on the last step
+ * of the call (qb_batch_energies then reads complete values).  In the mixed
+ * precision engine those steps evaluate the water-water pairs in FP64; the
+ * other steps evaluate the water-water forces alone, in packed FP32.
  * A system that raises an error on the device (e.g. QB_ERR_SHAKE) stops at
  * the failing step, as md_run stops there: its coordinates stay those the
  * step produced (positions at the step's start = x - v*dt), its step count
@@ -116,6 +120,14 @@ int qb_batch_run_timed(qb_batch *b, int nsteps, double *device_ms, long long *ke
 /* The post-loop evaluation of md_run (md.f90:4186-4188): rebuild the lists and
  * evaluate the potential at the final coordinates, for the FINAL summary. */
 int qb_batch_final_energy(qb_batch *b);
+
+/* Lists and gradient at the current coordinates, as qb_batch_final_energy,
+ * evaluated the way a step of the given kind evaluates them: energies = 1 as
+ * the steps that record energies (every energy term, FP64 water-water pairs),
+ * energies = 0 as the other steps (mixed precision engine: water-water forces
+ * in packed FP32 and no water-water energy).  Lets a caller check the force
+ * path of the non-recording steps. */
+int qb_batch_evaluate(qb_batch *b, int energies);
 
 /* Energies of system `sys` from the last potential evaluation.
  * E_out: QB_NE doubles; EQ_out: nstates*QB_NEQ doubles (may be NULL). */
@@ -136,6 +148,15 @@ int qb_batch_set_coords(qb_batch *b, int sys, const double *x_in);
 int qb_batch_get_velocities(qb_batch *b, int sys, double *v_out);
 int qb_batch_set_velocities(qb_batch *b, int sys, const double *v_in);
 
+/* The same for every system at once, in batch order: 3*natom doubles per
+ * system, back to back (3 * the batch's total atom count).  Each call makes
+ * one device copy through page-locked staging that the batch owns, instead of
+ * one small copy per system.  Setting marks the lists stale as above. */
+int qb_batch_get_coords_all(qb_batch *b, double *x_out);
+int qb_batch_set_coords_all(qb_batch *b, const double *x_in);
+int qb_batch_get_velocities_all(qb_batch *b, double *v_out);
+int qb_batch_set_velocities_all(qb_batch *b, const double *v_in);
+
 /* Water polarisation shell corrections (float theta_corr, md.f90:15205). */
 int qb_batch_get_theta_corr(qb_batch *b, int sys, float *out, int n);
 
@@ -146,6 +167,21 @@ int qb_batch_get_theta_corr(qb_batch *b, int sys, float *out, int n);
 int qb_batch_history(qb_batch *b, int sys, int kind, int *count, int *steps,
                      double *E, double *EQ);
 int qb_batch_clear_history(qb_batch *b);
+
+/* Records of every system at once (kind as above), in two device copies.
+ * One record is QB_HIST_REC doubles: step, E[QB_NE], EQ[QB_MAX_STATES][QB_NEQ],
+ * r_kl[QB_MAX_STATES] (the off-diagonal distances).  counts: nsys ints, the
+ * records of each system (at most max_records are returned); records:
+ * nsys*max_records*QB_HIST_REC doubles, system s's record r at
+ * (s*max_records + r)*QB_HIST_REC.  With records NULL, counts receives every
+ * system's full record count (max_records is not applied).  bytes (may be
+ * NULL) receives the bytes copied from the device. */
+#define QB_HIST_REC (1 + QB_NE + QB_MAX_STATES * QB_NEQ + QB_MAX_STATES)
+int qb_batch_history_all(qb_batch *b, int kind, int max_records, int *counts, double *records, size_t *bytes);
+
+/* Steps taken by the batch since it was created (the host's step counter;
+ * a system that failed stops its own count, qb_batch_status). */
+int qb_batch_step_count(qb_batch *b, long long *out);
 
 /* The off-diagonal elements of the same records: for every record and every
  * off-diagonal function io of the system's FEP file, Hij = A exp(-mu r_kl)
@@ -219,6 +255,17 @@ void qb_batch_destroy(qb_batch *b);
  * forbid allocation on the calling thread.
  *
  * x:      device, 9*nwat doubles, waters as O,H,H with x,y,z each
+ * crg_ow, crg_hw: the O and H charges already multiplied by the square root
+ *         of the Coulomb constant, as qdyn stores them after prep_sim
+ *         (src/q6/md.f90:13884-13891) and as qb_sysview's crg_ow/crg_hw hold
+ *         them: for TIP3P with the default constant 332, crg_ow =
+ *         -0.834f*sqrtf(332).  Plain topology charges give an electrostatic
+ *         energy 332 times too small; the call cannot detect that.
+ * A_OO, B_OO: the O-O Lennard-Jones products, E = A_OO/r^12 - B_OO/r^6 (for
+ *         the geometric rule the products of the O type's avdw and bvdw
+ *         columns, A = 4*eps*sigma^12, B = 4*eps*sigma^6), as qb_sysview's
+ *         A_OO/B_OO hold them.
+ * cutoff: the O-O cut-off (Angstrom) of the neighbour list.
  * excl:   device, nwat flags (1 = water outside the sphere), or NULL
  * grad:   device, 9*nwat doubles, overwritten with dU/dx
  * energy: device, 2 doubles, overwritten with (electrostatic, van der Waals)
@@ -234,8 +281,10 @@ void qb_batch_destroy(qb_batch *b);
  * device share that array and it keeps the last call's contents (the call
  * rewrites everything it reads), so calls that overlap on the GPU -- on two
  * streams, or from two threads -- race and must be serialised by the caller.
- * The first call on each device looks up the array's device address with that
- * device current; make that first call before any stream capture. */
+ * The first call on each device (per CUDA context) looks up the array's device
+ * address with that device current; make that first call before any stream
+ * capture.  A cudaDeviceReset discards the array with the context; the next
+ * call in the new context looks the address up again. */
 int qb_ww_energy_static(const double *x, int nwat, float crg_ow, float crg_hw, double A_OO, double B_OO,
                         double cutoff, const unsigned char *excl, double *grad, double *energy, int *status,
                         void *stream);

@@ -115,6 +115,13 @@ def _load():
         "qb_batch_create": (C.c_int, [C.POINTER(vp), C.c_int, C.POINTER(Options), C.POINTER(vp)]),
         "qb_batch_run": (C.c_int, [vp, C.c_int]),
         "qb_batch_final_energy": (C.c_int, [vp]),
+        "qb_batch_evaluate": (C.c_int, [vp, C.c_int]),
+        "qb_batch_get_coords_all": (C.c_int, [vp, dp]),
+        "qb_batch_set_coords_all": (C.c_int, [vp, dp]),
+        "qb_batch_get_velocities_all": (C.c_int, [vp, dp]),
+        "qb_batch_set_velocities_all": (C.c_int, [vp, dp]),
+        "qb_batch_history_all": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_int), dp, C.POINTER(C.c_size_t)]),
+        "qb_batch_step_count": (C.c_int, [vp, C.POINTER(C.c_longlong)]),
         "qb_batch_run_timed": (C.c_int, [vp, C.c_int, dp, C.POINTER(C.c_longlong)]),
         "qb_peak_flops": (C.c_int, [C.c_int, C.c_int, dp]),
         "qb_batch_energies": (C.c_int, [vp, C.c_int, dp, dp]),

@@ -20,6 +20,8 @@ from ._lib import E_NAMES, EQ_NAMES, QB_NE, QB_NEQ, Options, SysView, check, lib
 
 FP64 = 0
 MIXED = 1
+MAX_STATES = 10                                  # QB_MAX_STATES
+HIST_REC = 1 + QB_NE + MAX_STATES * QB_NEQ + MAX_STATES   # QB_HIST_REC
 
 Tuning = _lib._struct_from_header(_lib.os.path.join(_lib.INCLUDE, "qb.h"), "qb_tuning")
 
@@ -98,6 +100,12 @@ class Batch:
     def final_energy(self) -> None:
         check(lib.qb_batch_final_energy(self._b))
 
+    def evaluate(self, energies: bool = True) -> None:
+        """Lists and gradient at the current coordinates as a step that
+        records energies (True) or one that does not (False: the mixed
+        engine's packed FP32 water-water forces, no water-water energy)."""
+        check(lib.qb_batch_evaluate(self._b, 1 if energies else 0))
+
     def fep(self, systems, rt: float, nskip: int = 0, **kw):
         """qfep's analysis of these systems' energy-file records, in window
         order (q_b200.fep.params for the keyword arguments)."""
@@ -145,6 +153,59 @@ class Batch:
     def set_velocities(self, sys: int, v: np.ndarray) -> None:
         v = np.ascontiguousarray(v, dtype=np.float64)
         check(lib.qb_batch_set_velocities(self._b, sys, _dp(v)))
+
+    # every system at once: one copy per call through the batch's pinned staging
+    @property
+    def natom_total(self) -> int:
+        return sum(s.natom for s in self.systems)
+
+    def coords_all(self) -> np.ndarray:
+        out = np.zeros(3 * self.natom_total)
+        check(lib.qb_batch_get_coords_all(self._b, _dp(out)))
+        return out
+
+    def velocities_all(self) -> np.ndarray:
+        out = np.zeros(3 * self.natom_total)
+        check(lib.qb_batch_get_velocities_all(self._b, _dp(out)))
+        return out
+
+    def set_coords_all(self, x: np.ndarray) -> None:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        assert x.size == 3 * self.natom_total
+        check(lib.qb_batch_set_coords_all(self._b, _dp(x)))
+
+    def set_velocities_all(self, v: np.ndarray) -> None:
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        assert v.size == 3 * self.natom_total
+        check(lib.qb_batch_set_velocities_all(self._b, _dp(v)))
+
+    def history_all(self, kind: int = 0, max_records: int | None = None, with_bytes: bool = False):
+        """(counts[nsys], records[nsys, m, QB_HIST_REC]) of every system in
+        two device copies; a record is step, E[QB_NE], EQ[QB_MAX_STATES,
+        QB_NEQ], r_kl[QB_MAX_STATES].  With max_records None the counts are
+        queried first (one more copy).  with_bytes adds the bytes the call
+        copied from the device."""
+        n = len(self.systems)
+        counts = np.zeros(n, dtype=np.int32)
+        ip = counts.ctypes.data_as(C.POINTER(C.c_int))
+        nb = C.c_size_t(0)
+        total = 0
+        if max_records is None:
+            check(lib.qb_batch_history_all(self._b, kind, 0, ip, None, C.byref(nb)))
+            total += nb.value
+            max_records = int(counts.max(initial=0))
+        m = max(int(max_records), 1)
+        rec = np.zeros((n, m, HIST_REC))
+        check(lib.qb_batch_history_all(self._b, kind, m, ip, _dp(rec), C.byref(nb)))
+        total += nb.value
+        m = int(counts.max(initial=0))
+        out = (counts, rec[:, :m])
+        return out + (total,) if with_bytes else out
+
+    def step_count(self) -> int:
+        n = C.c_longlong()
+        check(lib.qb_batch_step_count(self._b, C.byref(n)))
+        return n.value
 
     def theta_corr(self, sys: int, n: int = 4) -> np.ndarray:
         out = np.zeros(n, dtype=np.float32)

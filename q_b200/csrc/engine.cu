@@ -47,6 +47,29 @@ T *dev_alloc(size_t n, std::vector<void *> &owned) {
   return p;
 }
 
+// A pair of timing events, destroyed on every exit path (a failed CUDA call
+// throws out of the timed loops).
+struct EventPair {
+  cudaEvent_t e[2] = {nullptr, nullptr};
+  EventPair() {
+    for (auto &x : e) {
+      cudaError_t r = cudaEventCreate(&x);
+      if (r != cudaSuccess) {
+        x = nullptr;
+        release();
+        fail(QB_ERR_CUDA, std::string("cudaEventCreate: ") + cudaGetErrorString(r));
+      }
+    }
+  }
+  ~EventPair() { release(); }
+  void release() {
+    for (auto &x : e)
+      if (x) { cudaEventDestroy(x); x = nullptr; }
+  }
+  EventPair(const EventPair &) = delete;
+  EventPair &operator=(const EventPair &) = delete;
+};
+
 struct KernelStat { double ms = 0; long long launches = 0; };
 
 struct Batch {
@@ -80,8 +103,23 @@ struct Batch {
   std::vector<std::string> order;
   double workload[QB_WORKLOAD_N] = {};
 
+  // page-locked staging of the batched host copies (qb_batch_*_all)
+  void *pinned = nullptr;
+  size_t pinned_bytes = 0;
+  void *staging(size_t bytes) {
+    if (bytes > pinned_bytes) {
+      if (pinned) cudaFreeHost(pinned);
+      pinned = nullptr;
+      pinned_bytes = 0;
+      CUDA_TRY(cudaMallocHost(&pinned, bytes));
+      pinned_bytes = bytes;
+    }
+    return pinned;
+  }
+
   ~Batch() {
     if (stream) cudaStreamSynchronize(stream);
+    if (pinned) cudaFreeHost(pinned);
     drop_graphs();
     for (int k = 0; k < 2; k++) {
       if (side[k]) { cudaStreamSynchronize(side[k]); cudaStreamDestroy(side[k]); }
@@ -212,8 +250,25 @@ struct Batch {
     }
   }
 
-  void pot_energy() {
+  // Steps whose energies are recorded (output or energy-file records of any
+  // system, as k_finish decides) evaluate every term's energy.  The mixed
+  // engine evaluates the water-water pairs of those steps in FP64 and, on the
+  // other steps, their forces alone in packed FP32.
+  bool energy_due() const {
+    for (auto &S : sysh) {
+      if (S.iout > 0 && istep % S.iout == 0) return true;
+      if (S.iene > 0 && istep > 0 && istep % S.iene == 0) return true;
+    }
+    return false;
+  }
+
+  // ene = 0 only on steps that record no energies (the mixed engine's
+  // water-water forces then skip their energies); the FP64 engine always
+  // evaluates them.
+  void pot_energy(int ene = 1) {
     DevPtrs &p = P;
+    const bool mixed = opt.precision == QB_MIXED;
+    const bool fast_ww = mixed && !ene;
     CUDA_TRY(cudaMemsetAsync(p.d, 0, sizeof(double4) * (size_t)p.natoms_tot, stream));
     CUDA_TRY(cudaMemsetAsync(p.E, 0, sizeof(double) * QB_NE * (size_t)nsys, stream));
     CUDA_TRY(cudaMemsetAsync(p.EQ, 0, sizeof(double) * MAXS * QB_NEQ * (size_t)nsys, stream));
@@ -221,7 +276,7 @@ struct Batch {
     // gradient contribution (plain stores after the zeroing)
     if (max_nwat > 0) {
       dim3 gp(cdiv(max_nwat, 256), nsys);
-      if (opt.precision == QB_MIXED) launch("pack_waters", [&] { k_pack_waters<true><<<gp, 256, 0, stream>>>(p); });
+      if (fast_ww) launch("pack_waters", [&] { k_pack_waters<true><<<gp, 256, 0, stream>>>(p); });
       else launch("pack_waters", [&] { k_pack_waters<false><<<gp, 256, 0, stream>>>(p); });
     }
     cudaStream_t s1 = forking() ? side[0] : stream, s2 = forking() ? side[1] : stream;
@@ -251,15 +306,14 @@ struct Batch {
     }
     if (max_ncgp_sol_w > 0)
       launch("nb_pw", [&] { k_nb_pw<<<dim3(cdiv(p.pwg_cap, PW_BLOCK), max_ncgp_sol_w, nsys), PW_BLOCK, 0, s1>>>(p); });
-    const bool mixed = opt.precision == QB_MIXED;
     if (max_nwat > 0) {
       dim3 gw(cdiv(max_nwat, WW_WPB), nsys);
-      size_t smem = (size_t)p.ww_chunk * (mixed ? WatRec<true>::words : WatRec<false>::words) * sizeof(float4);
+      size_t smem = (size_t)p.ww_chunk * (fast_ww ? WatRec<true>::words : WatRec<false>::words) * sizeof(float4);
       // hydrogen LJ: the whole batch takes the variant (exact zeros for systems without)
-      if (mixed && any_hlj) {
+      if (fast_ww && any_hlj) {
         launch("nb_ww", [&] { k_nb_ww<true, true><<<gw, WW_BLOCK, smem, stream>>>(p); });
-      } else if (mixed) {
-        launch("nb_ww", [&] { k_nb_ww<true, false><<<gw, WW_BLOCK, smem, stream>>>(p); });
+      } else if (fast_ww) {
+        launch("nb_ww_x2", [&] { k_nb_ww_x2<<<gw, WWX_BLOCK, smem, stream>>>(p); });
       } else if (any_hlj) {
         launch("nb_ww", [&] { k_nb_ww<false, true><<<gw, WW_BLOCK, smem, stream>>>(p); });
       } else {
@@ -294,13 +348,18 @@ struct Batch {
 
   // CUDA graphs of one step, with and without the list rebuild; kernel
   // arguments are captured by value, so any change of P drops them.
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  long long graph_launches[2] = {0, 0};
+  // CUDA graphs of one step: [list rebuild][energies recorded]
+  cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  long long graph_launches[2][2] = {{0, 0}, {0, 0}};
   bool use_graphs = true;
+  // the last step of a run evaluates energies, so that the energies a caller
+  // reads after it are complete
+  bool force_energy = false;
 
   void drop_graphs() {
-    for (auto &g : graph)
-      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    for (auto &row : graph)
+      for (auto &g : row)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   }
 
   bool lists_stale = false;
@@ -312,35 +371,46 @@ struct Batch {
       lists_stale = false;
       due = 0;
     }
-    if (!use_graphs || profiling) { step_kernels(due); istep++; return; }
-    if (!graph[due]) {
+    const int ene = (opt.precision != QB_MIXED || force_energy || energy_due()) ? 1 : 0;
+    if (!use_graphs || profiling) { step_kernels(due, ene); istep++; return; }
+    cudaGraphExec_t &ge = graph[due][ene];
+    if (!ge) {
       cudaGraph_t g = nullptr;
       long long l0 = launches;
       CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
       try {
-        step_kernels(due);
+        step_kernels(due, ene);
       } catch (...) {
         cudaStreamEndCapture(stream, &g);
         if (g) cudaGraphDestroy(g);
         throw;
       }
       CUDA_TRY(cudaStreamEndCapture(stream, &g));
-      cudaError_t e = cudaGraphInstantiate(&graph[due], g, 0);
+      cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
       cudaGraphDestroy(g);
-      if (e != cudaSuccess) { graph[due] = nullptr; fail(QB_ERR_CUDA, std::string("graph instantiation: ") + cudaGetErrorString(e)); }
-      graph_launches[due] = launches - l0;
+      if (e != cudaSuccess) { ge = nullptr; fail(QB_ERR_CUDA, std::string("graph instantiation: ") + cudaGetErrorString(e)); }
+      graph_launches[due][ene] = launches - l0;
       launches = l0;
     }
-    CUDA_TRY(cudaGraphLaunch(graph[due], stream));
-    launches += graph_launches[due];
+    CUDA_TRY(cudaGraphLaunch(ge, stream));
+    launches += graph_launches[due][ene];
     istep++;
   }
 
+  // nsteps steps, the last of them with energies
+  void steps(int nsteps) {
+    for (int k = 0; k < nsteps; k++) {
+      force_energy = k == nsteps - 1;
+      step();
+    }
+    force_energy = false;
+  }
+
   // The kernels of one MD step (md_run's loop body, md.f90:4003-4175).
-  void step_kernels(int due) {
+  void step_kernels(int due, int ene) {
     DevPtrs &p = P;
     if (due) build_lists(0);
-    pot_energy();
+    pot_energy(ene);
     // 3-constraint molecules (waters) take leapfrog and SHAKE in one pass; the
     // other atoms leapfrog, then the general SHAKE; the two paths move
     // disjoint atoms
@@ -897,12 +967,17 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   P.ww = dev_alloc<uint16_t>((size_t)std::max(woff, 1) * ww_cap, o);
   P.ww_n = dev_alloc<int>(std::max(woff, 1), o);
   P.ww_sp = dev_alloc<int>((size_t)std::max(woff, 1) * nch_alloc, o);
-  P.wrec = dev_alloc<float4>((size_t)std::max(woff, 1) * rec_words, o);
-  // the limit (not an allocation) covers every chunk size any batch may use
+  // FP64 records on every step of the FP64 engine and on the mixed engine's
+  // energy steps, whose FP64 water-water kernel stages the mixed chunk size
+  // (up to 2368 waters x 80 bytes)
+  P.wrec = dev_alloc<float4>((size_t)std::max(woff, 1) * WatRec<false>::words, o);
+  // the limits (not allocations) cover every chunk size any batch may use
+  const int smem64 = std::max(WW_STAGE_BYTES, P.ww_chunk * WatRec<false>::words * 16);
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
-  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem64));
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
-  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem64));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
   P.kin_nblk = std::max(1, (B.max_natom + KIN_BLOCK - 1) / KIN_BLOCK);
   P.kin = dev_alloc<double>((size_t)n * 4, o);
   P.E = dev_alloc<double>((size_t)n * QB_NE, o);
@@ -1081,7 +1156,7 @@ int qb_batch_run(qb_batch *bb, int nsteps) {
     CUDA_TRY(cudaSetDevice(B.opt.device));
     qb::ensure_history(B, nsteps);
     qb::reset_counters(B);
-    for (int k = 0; k < nsteps; k++) B.step();
+    B.steps(nsteps);
     if (B.profiling) B.collect();
     B.sync_status();
     qb::refresh_workload(B, nsteps);
@@ -1095,19 +1170,15 @@ int qb_batch_run_timed(qb_batch *bb, int nsteps, double *device_ms, long long *k
     CUDA_TRY(cudaSetDevice(B.opt.device));
     qb::ensure_history(B, nsteps);
     qb::reset_counters(B);
-    cudaEvent_t e0, e1;
-    CUDA_TRY(cudaEventCreate(&e0));
-    CUDA_TRY(cudaEventCreate(&e1));
+    qb::EventPair ev;
     long long l0 = B.launches;
     CUDA_TRY(cudaStreamSynchronize(B.stream));
-    CUDA_TRY(cudaEventRecord(e0, B.stream));
-    for (int k = 0; k < nsteps; k++) B.step();
-    CUDA_TRY(cudaEventRecord(e1, B.stream));
-    CUDA_TRY(cudaEventSynchronize(e1));
+    CUDA_TRY(cudaEventRecord(ev.e[0], B.stream));
+    B.steps(nsteps);
+    CUDA_TRY(cudaEventRecord(ev.e[1], B.stream));
+    CUDA_TRY(cudaEventSynchronize(ev.e[1]));
     float ms = 0;
-    CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    CUDA_TRY(cudaEventElapsedTime(&ms, ev.e[0], ev.e[1]));
     if (device_ms) *device_ms = ms;
     if (kernel_launches) *kernel_launches = B.launches - l0;
     if (B.profiling) B.collect();
@@ -1143,17 +1214,13 @@ void set_tuning(Batch &B, const qb_tuning &t) {
 // device ms per step of `steps` steps after one list cycle of warm-up
 double time_steps(Batch &B, int steps) {
   for (int k = 0; k < B.NB; k++) B.step();
-  cudaEvent_t e0, e1;
-  CUDA_TRY(cudaEventCreate(&e0));
-  CUDA_TRY(cudaEventCreate(&e1));
-  CUDA_TRY(cudaEventRecord(e0, B.stream));
-  for (int k = 0; k < steps; k++) B.step();
-  CUDA_TRY(cudaEventRecord(e1, B.stream));
-  CUDA_TRY(cudaEventSynchronize(e1));
+  EventPair ev;
+  CUDA_TRY(cudaEventRecord(ev.e[0], B.stream));
+  B.steps(steps);
+  CUDA_TRY(cudaEventRecord(ev.e[1], B.stream));
+  CUDA_TRY(cudaEventSynchronize(ev.e[1]));
   float ms = 0;
-  CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  CUDA_TRY(cudaEventElapsedTime(&ms, ev.e[0], ev.e[1]));
   B.sync_status();
   return ms / steps;
 }
@@ -1259,17 +1326,20 @@ int qb_batch_fep(qb_batch *bb, const int *sys, int nfiles, const qb_fep_params *
   });
 }
 
-int qb_batch_final_energy(qb_batch *bb) {
-  if (!bb) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
+int qb_batch_evaluate(qb_batch *bb, int energies) {
+  if (!bb || (energies != 0 && energies != 1)) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
   return guarded_batch([&] {
     Batch &B = bb->b;
+    CUDA_TRY(cudaSetDevice(B.opt.device));
     B.build_lists(1);
-    B.pot_energy();
+    B.pot_energy(B.opt.precision == QB_MIXED ? energies : 1);
     qb::k_finish<<<B.nsys, 32, 0, B.stream>>>(B.P, 2);
     B.check_launch("energy sums");
     B.sync_status();
   });
 }
+
+int qb_batch_final_energy(qb_batch *bb) { return qb_batch_evaluate(bb, 1); }
 
 static int sys_check(qb_batch *bb, int sys) {
   if (!bb || sys < 0 || sys >= bb->b.nsys) { qb::set_error("invalid batch or system index"); return QB_ERR_ARG; }
@@ -1333,6 +1403,76 @@ int qb_batch_set_coords(qb_batch *b, int sys, const double *x) {
 }
 int qb_batch_get_velocities(qb_batch *b, int sys, double *v) { return get_vec(b, sys, b ? b->b.P.v : nullptr, v); }
 int qb_batch_set_velocities(qb_batch *b, int sys, const double *v) { return set_vec(b, sys, b ? b->b.P.v : nullptr, v); }
+
+static int get_all(qb_batch *bb, double4 *src, double *out) {
+  if (!bb || !out) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
+  return guarded_batch([&] {
+    Batch &B = bb->b;
+    const size_t n = (size_t)B.P.natoms_tot;
+    double4 *h = static_cast<double4 *>(B.staging(n * sizeof(double4)));
+    CUDA_TRY(cudaMemcpyAsync(h, src, n * sizeof(double4), cudaMemcpyDeviceToHost, B.stream));
+    CUDA_TRY(cudaStreamSynchronize(B.stream));
+    for (size_t i = 0; i < n; i++) { out[3 * i] = h[i].x; out[3 * i + 1] = h[i].y; out[3 * i + 2] = h[i].z; }
+  });
+}
+
+static int set_all(qb_batch *bb, double4 *dst, const double *in) {
+  if (!bb || !in) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
+  return guarded_batch([&] {
+    Batch &B = bb->b;
+    const size_t n = (size_t)B.P.natoms_tot;
+    CUDA_TRY(cudaStreamSynchronize(B.stream));   // the staging may still feed an earlier copy
+    double4 *h = static_cast<double4 *>(B.staging(n * sizeof(double4)));
+    for (size_t i = 0; i < n; i++) h[i] = make_double4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0.0);
+    CUDA_TRY(cudaMemcpyAsync(dst, h, n * sizeof(double4), cudaMemcpyHostToDevice, B.stream));
+    CUDA_TRY(cudaStreamSynchronize(B.stream));
+  });
+}
+
+int qb_batch_get_coords_all(qb_batch *b, double *x) { return get_all(b, b ? b->b.P.x : nullptr, x); }
+int qb_batch_set_coords_all(qb_batch *b, const double *x) {
+  int rc = set_all(b, b ? b->b.P.x : nullptr, x);
+  if (rc == QB_OK) b->b.lists_stale = true;
+  return rc;
+}
+int qb_batch_get_velocities_all(qb_batch *b, double *v) { return get_all(b, b ? b->b.P.v : nullptr, v); }
+int qb_batch_set_velocities_all(qb_batch *b, const double *v) { return set_all(b, b ? b->b.P.v : nullptr, v); }
+
+int qb_batch_history_all(qb_batch *bb, int kind, int max_records, int *counts, double *records, size_t *bytes) {
+  if (!bb || kind < 0 || kind > 1 || max_records < 0 || !counts) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
+  return guarded_batch([&] {
+    Batch &B = bb->b;
+    const int n = B.nsys, cap = B.P.hist_cap;
+    static_assert(QB_HIST_REC == qb::HIST_REC, "record layout");
+    const size_t rec = qb::HIST_REC;
+    const size_t st_bytes = sizeof(qb::SysState) * n;
+    // the first m records of every system: one strided copy of n rows
+    const int m = records ? std::min(max_records, cap) : 0;
+    const size_t row = (size_t)m * rec * sizeof(double);
+    char *h = static_cast<char *>(B.staging(st_bytes + row * n));
+    CUDA_TRY(cudaMemcpyAsync(h, B.P.st, st_bytes, cudaMemcpyDeviceToHost, B.stream));
+    if (m > 0)
+      CUDA_TRY(cudaMemcpy2DAsync(h + st_bytes, row, B.P.hist + (size_t)kind * n * cap * rec, (size_t)cap * rec * sizeof(double),
+                                 row, n, cudaMemcpyDeviceToHost, B.stream));
+    CUDA_TRY(cudaStreamSynchronize(B.stream));
+    if (bytes) *bytes = st_bytes + row * n;
+    const qb::SysState *st = reinterpret_cast<const qb::SysState *>(h);
+    const double *hr = reinterpret_cast<const double *>(h + st_bytes);
+    for (int s2 = 0; s2 < n; s2++) {
+      const int have = std::min(st[s2].hist_n[kind], cap);
+      const int c = records ? std::min(have, m) : have;
+      counts[s2] = c;
+      if (records && c > 0)
+        std::memcpy(records + (size_t)s2 * max_records * rec, hr + (size_t)s2 * m * rec, sizeof(double) * rec * c);
+    }
+  });
+}
+
+int qb_batch_step_count(qb_batch *bb, long long *out) {
+  if (!bb || !out) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
+  *out = bb->b.istep;
+  return QB_OK;
+}
 
 int qb_batch_get_theta_corr(qb_batch *bb, int sys, float *out, int n) {
   if (int rc = sys_check(bb, sys)) return rc;

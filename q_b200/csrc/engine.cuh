@@ -75,6 +75,10 @@ struct SysState {
   double Tscale_sol, Tscale_solv, Temp, Tfree, Tfree_sol, Tfree_solv, kinetic;
   float theta_corr[MAX_SHELLS], avtheta[MAX_SHELLS], avn_insh[MAX_SHELLS];
   int istep, status, pp_n, pw_n, qp_n, qw_n, lists_built, hist_n[2];
+  // status as of the start of the current step (k_finish copies status into
+  // it): the kernels that move atoms read this word, so an error raised in
+  // the middle of a step takes effect for every kernel from the next step on
+  int frozen;
   int shake_its_max;                 // most SHAKE iterations of one molecule since the counters were reset
   unsigned long long shake_its;      // SHAKE iterations summed over molecules and steps
 };

@@ -611,8 +611,9 @@ __global__ void k_lists_end(DevPtrs P, int force) {
 // FP64 (5 words, 80 bytes): O,H1,H2 x,y,z as doubles and one pad double.
 // Mixed (3 words, 48 bytes): the O position as an unevaluated float sum
 // hi + lo (hi = float(x), lo = float(x - hi)) and the two H positions relative
-// to their O, rounded to float: {hO.xyz, lO.x}, {lO.yz, rH1.xy},
-// {rH1.z, rH2.xyz}.  An atom-pair vector is then
+// to their O, rounded to float: {hO.xyz, lO.x}, {lO.yz, rH1.x, rH2.x},
+// {rH1.y, rH2.y, rH1.z, rH2.z} -- each component's two H offsets side by
+// side, one packed FP32x2 operand.  An atom-pair vector is then
 // ((hOj - hOi) + (lOj - lOi)) + rHj - rHi, which carries ~1e-7 relative error
 // like an FP64 difference rounded to FP32.  Both strides (3 and 5 words) put
 // 8 consecutive waters on 8 distinct 16-byte bank groups.
@@ -725,10 +726,11 @@ __device__ __forceinline__ void ww_pair_f32(const float *i, const float *j, floa
     }
 }
 
+// Mixed record -> {hO[3], lO[3], rH1[3], rH2[3]}.
 __device__ __forceinline__ void unpack_mixed(const float4 *r, float *v) {
   float4 w0 = r[0], w1 = r[1], w2 = r[2];
   v[0] = w0.x; v[1] = w0.y; v[2] = w0.z; v[3] = w0.w; v[4] = w1.x; v[5] = w1.y;
-  v[6] = w1.z; v[7] = w1.w; v[8] = w2.x; v[9] = w2.y; v[10] = w2.z; v[11] = w2.w;
+  v[6] = w1.z; v[7] = w2.x; v[8] = w2.z; v[9] = w1.w; v[10] = w2.y; v[11] = w2.w;
 }
 
 // nonbond_ww_spc (md.f90:11823) over the water-water list.  Block = 512
@@ -852,6 +854,160 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
   }
   warp_add(&P.E[s * QB_NE + QB_E_WW_EL], 0.5 * el);
   warp_add(&P.E[s * QB_NE + QB_E_WW_VDW], 0.5 * vdw);
+}
+
+// ----------------------------------------------- packed FP32x2 water-water
+
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
+
+// Operands of water i on the packed path: O as hi + lo, the H offsets negated
+// in both orders ({-rH1, -rH2} and {-rH2, -rH1}, per component).
+struct WwI2 {
+  float hO[3], lO[3];
+  float2 nrH[3], nrHs[3];
+};
+
+// Gradient of water i from molecule pair (i, j) of nonbond_ww_spc
+// (md.f90:11823-11950), forces only, on Blackwell's packed FP32x2 pipes
+// (FADD2/FMUL2/FFMA2: two lanes of FP32 work per issued instruction).  The
+// eight H-involving Coulomb pairs are four packed pairs:
+//   t  = O_i -> {H1_j, H2_j}      (into gO, both halves O_i's)
+//   s  = {H1_i, H2_i} -> O_j      (into gH = {H1_i, H2_i})
+//   hd = {H1_i, H2_i} -> {H1_j, H2_j}  (into gH)
+//   hx = {H2_i, H1_i} -> {H1_j, H2_j}  (into gHs = {H2_i, H1_i})
+// plus the O-O Lennard-Jones + Coulomb pair (into gO.x).  Each gradient term
+// is w * (x_j - x_i) with w = q q / r^3 (Coulomb) and r^-2 (q q / r + 12 A /
+// r^12 - 6 B / r^6) for O-O: -dv of the reference loop.
+__device__ __forceinline__ void ww_force_x2(const WwI2 &I, const float4 j0, const float4 j1, const float4 j2,
+                                            float2 qoh2, float2 qhh2, float qoo, float A, float B, float2 *gO,
+                                            float2 *gH, float2 *gHs) {
+  const float d[3] = {(j0.x - I.hO[0]) + (j0.w - I.lO[0]), (j0.y - I.hO[1]) + (j1.x - I.lO[1]),
+                      (j0.z - I.hO[2]) + (j1.y - I.lO[2])};
+  const float2 rHj[3] = {make_float2(j1.z, j1.w), make_float2(j2.x, j2.y), make_float2(j2.z, j2.w)};
+  float2 t[3], sv[3], hd[3], hx[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const float2 u = dup2(d[c]);
+    t[c] = __fadd2_rn(u, rHj[c]);
+    sv[c] = __fadd2_rn(u, I.nrH[c]);
+    hd[c] = __fadd2_rn(t[c], I.nrH[c]);
+    hx[c] = __fadd2_rn(t[c], I.nrHs[c]);
+  }
+  auto r2of = [](const float2 *v) { return __ffma2_rn(v[0], v[0], __ffma2_rn(v[1], v[1], __fmul2_rn(v[2], v[2]))); };
+  auto wof = [](float2 r2, float2 qq) {
+    const float2 ri = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+    return __fmul2_rn(__fmul2_rn(qq, ri), __fmul2_rn(ri, ri));
+  };
+  const float2 wt = wof(r2of(t), qoh2), ws = wof(r2of(sv), qoh2);
+  const float2 wd = wof(r2of(hd), qhh2), wx = wof(r2of(hx), qhh2);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    gO[c] = __ffma2_rn(wt, t[c], gO[c]);
+    gH[c] = __ffma2_rn(wd, hd[c], __ffma2_rn(ws, sv[c], gH[c]));
+    gHs[c] = __ffma2_rn(wx, hx[c], gHs[c]);
+  }
+  const float r2 = fmaf(d[0], d[0], fmaf(d[1], d[1], d[2] * d[2]));
+  const float ri = rsqrt_ftz(r2), r2i = ri * ri, r6 = r2i * r2i * r2i;
+  const float Va = A * r6 * r6, Vb = B * r6;
+  const float w = r2i * fmaf(-6.f, Vb, fmaf(12.f, Va, qoo * ri));
+#pragma unroll
+  for (int c = 0; c < 3; c++) gO[c].x = fmaf(w, d[c], gO[c].x);
+}
+
+// nonbond_ww_spc (md.f90:11823) forces of the mixed-precision engine on steps
+// that record no energies: the list walk of k_nb_ww (half a warp per water,
+// the system's records staged in shared memory chunk by chunk) with the pair
+// terms of ww_force_x2.  Energies are left to the steps that record them,
+// which evaluate the water-water pairs in FP64 (k_nb_ww<false>).  SPC water
+// only (no hydrogen Lennard-Jones).
+// 256 threads, two blocks per SM: one block's staging of records overlaps the
+// other's pair work (the registers of the packed path allow 16 warps per SM)
+constexpr int WWX_BLOCK = 256;
+__global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P) {
+  extern __shared__ float4 wsm[];
+  __shared__ int2 srange[WW_WPB];
+  constexpr int W = WatRec<true>::words;
+  const int s = blockIdx.y;
+  const SysDev &S = P.sys[s];
+  const int i0 = blockIdx.x * WW_WPB;
+  if (i0 >= S.nwat) return;
+  const int i1 = min(i0 + WW_WPB, S.nwat);
+  const int hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
+  const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
+  const float4 *rec = P.wrec + (size_t)S.woff * W;
+  const int CW = P.ww_chunk;
+  const int nch = (S.nwat + CW - 1) / CW;
+  const float qo = S.crg_ow, qh = S.crg_hw;
+  const float qoo = qo * qo;
+  const float2 qoh2 = dup2(qo * qh), qhh2 = dup2(qh * qh);
+  const float A = (float)S.A_OO, B = (float)S.B_OO;
+  for (int c = 0; c < nch; c++) {
+    const int c0 = c * CW, cn = min(CW, S.nwat - c0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < cn * W; t += WWX_BLOCK) wsm[t] = rec[(size_t)c0 * W + t];
+    for (int t = threadIdx.x; t < i1 - i0; t += WWX_BLOCK) {
+      const int *sp = P.ww_sp + (size_t)(S.woff + i0 + t) * P.ww_nch;
+      srange[t] = make_int2(c == 0 ? 0 : sp[c - 1], sp[c]);
+    }
+    __syncthreads();
+    for (int iw = i0 + hw; iw < i1; iw += WWX_BLOCK / 16) {
+      const int gw = S.woff + iw;
+      const int kb = srange[iw - i0].x, ke = srange[iw - i0].y;
+      if (kb >= ke) continue;
+      const uint16_t *nb = P.ww + (size_t)gw * P.ww_cap;
+      const float4 *ri = (iw >= c0 && iw < c0 + cn) ? wsm + (iw - c0) * W : rec + (size_t)iw * W;
+      WwI2 I;
+      {
+        const float4 a = ri[0], b = ri[1], e = ri[2];
+        I.hO[0] = a.x; I.hO[1] = a.y; I.hO[2] = a.z;
+        I.lO[0] = a.w; I.lO[1] = b.x; I.lO[2] = b.y;
+        I.nrH[0] = make_float2(-b.z, -b.w); I.nrH[1] = make_float2(-e.x, -e.y); I.nrH[2] = make_float2(-e.z, -e.w);
+#pragma unroll
+        for (int q = 0; q < 3; q++) I.nrHs[q] = make_float2(I.nrH[q].y, I.nrH[q].x);
+      }
+      float2 gO[3], gH[3], gHs[3];
+#pragma unroll
+      for (int q = 0; q < 3; q++) gO[q] = gH[q] = gHs[q] = make_float2(0.f, 0.f);
+      // the lane's list entries in groups of four, loaded together, the next
+      // group's loads issued before the current group's pairs
+      int k = kb + hl;
+      int jg[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) jg[u] = k + 16 * u < ke ? (int)nb[k + 16 * u] : -1;
+      for (; k < ke; k += 64) {
+        int jn[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) jn[u] = k + 64 + 16 * u < ke ? (int)nb[k + 64 + 16 * u] : -1;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          if (jg[u] < 0) break;
+          const float4 *rj = wsm + (jg[u] - c0) * W;
+          ww_force_x2(I, rj[0], rj[1], rj[2], qoh2, qhh2, qoo, A, B, gO, gH, gHs);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) jg[u] = jn[u];
+      }
+      // per atom of water i: O, H1, H2 (x, y, z each), reduced over the half-warp
+      float g[9];
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        g[q] = gO[q].x + gO[q].y;
+        g[3 + q] = gH[q].x + gHs[q].y;
+        g[6 + q] = gH[q].y + gHs[q].x;
+      }
+#pragma unroll
+      for (int q = 0; q < 9; q++) {
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) g[q] += __shfl_xor_sync(hmask, g[q], o);
+      }
+      if (hl == 0) {
+        const int oi = S.aoff + S.nsol + 3 * iw;
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+          atomic_add3(P.d, oi + a, (double)g[3 * a], (double)g[3 * a + 1], (double)g[3 * a + 2]);
+      }
+    }
+  }
 }
 
 // nonbond_pp (md.f90:10387): one thread per pair.
@@ -1440,8 +1596,8 @@ __global__ void k_pack_waters(DevPtrs P) {
       float hx = (float)a.x, hy = (float)a.y, hz = (float)a.z;
       float lx = (float)(a.x - (double)hx), ly = (float)(a.y - (double)hy), lz = (float)(a.z - (double)hz);
       r[0] = make_float4(hx, hy, hz, lx);
-      r[1] = make_float4(ly, lz, (float)(b.x - a.x), (float)(b.y - a.y));
-      r[2] = make_float4((float)(b.z - a.z), (float)(c.x - a.x), (float)(c.y - a.y), (float)(c.z - a.z));
+      r[1] = make_float4(ly, lz, (float)(b.x - a.x), (float)(c.x - a.x));
+      r[2] = make_float4((float)(b.y - a.y), (float)(c.y - a.y), (float)(b.z - a.z), (float)(c.z - a.z));
     } else {
       double2 *rd = reinterpret_cast<double2 *>(r);
       rd[0] = make_double2(a.x, a.y); rd[1] = make_double2(a.z, b.x); rd[2] = make_double2(b.y, b.z);
@@ -2122,7 +2278,7 @@ __global__ void k_leapfrog(DevPtrs P) {
   double acc[4] = {0, 0, 0, 0};
   // a system that raised an error stays where the failing step left it;
   // atoms of 3-constraint molecules are k_leapfrog_shake3's
-  if (g < P.natoms_tot && P.st[P.asys[g]].status == 0 && !(P.flags[g] & F_SH3)) {
+  if (g < P.natoms_tot && P.st[P.asys[g]].frozen == 0 && !(P.flags[g] & F_SH3)) {
     s = P.asys[g];
     const SysDev &S = P.sys[s];
     double ts = (g - S.aoff) < S.nsol ? P.st[s].Tscale_sol : P.st[s].Tscale_solv;
@@ -2207,7 +2363,7 @@ __global__ void __launch_bounds__(128, 6) k_leapfrog_shake3(DevPtrs P) {
   int m = blockIdx.x * blockDim.x + threadIdx.x;
   int sys = -1, its = 0;
   double acc[4] = {0, 0, 0, 0};
-  if (m < P.nsh3 && P.st[P.sh3_at[m].w].status == 0) {
+  if (m < P.nsh3 && P.st[P.sh3_at[m].w].frozen == 0) {
     const int4 at = P.sh3_at[m];
     const double4 d2 = P.sh3_d2[m];
     sys = at.w;
@@ -2290,7 +2446,7 @@ __global__ void __launch_bounds__(SHG_BLOCK) k_shake_general(DevPtrs P) {
   const int *lev = P.shg_lev + info2.x;
   // a system that raised an error stays where the failing step left it
   __shared__ int frozen;
-  if (threadIdx.x == 0) frozen = P.st[sys].status;
+  if (threadIdx.x == 0) frozen = P.st[sys].frozen;
   __syncthreads();
   if (frozen) return;
   for (int t = threadIdx.x; t < na; t += SHG_BLOCK) {
@@ -2453,8 +2609,10 @@ __global__ void k_finish(DevPtrs P, int mode) {
   if (mode != 0) finalize_energy(P, s);
   if (mode == 2) return;
   if (mode == 1 && st.status != 0) {
-    // failed at this step: no records, the step count stays at the failure
+    // failed at this step: no records, the step count stays at the failure,
+    // and the kernels that move atoms skip the system from the next step on
     if (lane < 4) P.kin[s * 4 + lane] = 0.0;
+    if (lane == 0) st.frozen = st.status;
     return;
   }
   if (lane == 0) {

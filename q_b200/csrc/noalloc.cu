@@ -129,10 +129,33 @@ __global__ void k_static_ww_force(const double *__restrict__ x, int nwat, float 
   }
 }
 
-// Device address of the scratch array, looked up once per device.
+// Device address of the scratch array, looked up once per device and CUDA
+// context.  The context is part of the key: after a cudaDeviceReset the
+// device's new primary context holds a new copy of the array, and the address
+// cached for the old context would no longer be valid.
 constexpr int kMaxDevices = 64;
 std::mutex g_mutex;
 int *g_scratch_ptr[kMaxDevices] = {nullptr};
+void *g_scratch_ctx[kMaxDevices] = {nullptr};
+
+// The current context (driver call cuCtxGetCurrent, reached through the
+// runtime's entry-point table so the library needs no link to libcuda).
+void *current_context() {
+  using Fn = int (*)(void **);
+  static Fn fn = nullptr;
+  static bool looked = false;
+  if (!looked) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<Fn>(p);
+    looked = true;
+  }
+  void *ctx = nullptr;
+  if (fn && fn(&ctx) != 0) ctx = nullptr;
+  return ctx;
+}
 
 }  // namespace
 
@@ -156,7 +179,8 @@ extern "C" int qb_ww_energy_static(const double *x, int nwat, float crg_ow, floa
   int *scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_scratch_ptr[dev]) {
+    void *ctx = current_context();
+    if (!g_scratch_ptr[dev] || !ctx || g_scratch_ctx[dev] != ctx) {
       // first call on this device: the symbol's device address, with the
       // device current (the host-side name is not a device address)
       void *p = nullptr;
@@ -166,6 +190,8 @@ extern "C" int qb_ww_energy_static(const double *x, int nwat, float crg_ow, floa
         return QB_ERR_CUDA;
       }
       g_scratch_ptr[dev] = static_cast<int *>(p);
+      // the lookup made the device's primary context current if none was
+      g_scratch_ctx[dev] = current_context();
     }
     scratch = g_scratch_ptr[dev];
   }

@@ -16,7 +16,8 @@ The fixtures are the reference's own test inputs and known answers, copied
                 eq1.log was produced with solute SHAKE off (its header prints
                 "SHAKE all solute bonds = off"), so the fixture input sets
                 shake_solute off.  velocities.csv holds the Maxwell velocities
-                the log prints for random_seed 112 at 1 K.
+                the log prints for random_seed 112 at 1 K; eq1.re is the
+                restart qdyn wrote after the run's one step (600 bytes).
   data/         test/data/topology and test/data/inputs: topologies and FEP
                 files of the reference's Q6-vs-QGPU comparison harness
                 (test/runTEST.py); its interaction-class cases (p-p, q-p,
@@ -67,6 +68,9 @@ def main(ref: str) -> None:
     open(os.path.join(out, "eq1.inp"), "w").write(inp)
     shutil.copy(os.path.join(q5, "velocities.csv"), os.path.join(out, "velocities.csv"))
     shutil.copy(os.path.join(q5, "eq1.log"), os.path.join(out, "eq1.log"))
+    # the restart qdyn wrote at the end of that run (write_xfin, md.f90:15452):
+    # coordinates and velocities after the one step, gfortran record markers
+    shutil.copy(os.path.join(q5, "eq1.re"), os.path.join(out, "eq1.re"))
     shutil.rmtree(tmp)
 
     out = os.path.join(HERE, "data")
@@ -79,4 +83,6 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py /path/to/reference")
+    main(sys.argv[1])

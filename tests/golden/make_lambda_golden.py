@@ -4,13 +4,15 @@ sigmoid from functions.py:7), for the restatement in q_b200/lambda_placement.py.
 qligfep.py cannot be imported without its workflow dependencies, so this
 script takes the two functions' own source out of the reference files (ast)
 and runs them unchanged; `self` is not used by get_lambdas.  Run here, where
-the reference tree exists:  python tests/golden/make_lambda_golden.py
+the reference tree exists:
+
+    python tests/golden/make_lambda_golden.py /path/to/reference
 """
 import ast
 import json
 import os
+import sys
 
-REF = "/root/reference/src/QligFEP"
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "qligfep_lambdas.json")
 
 
@@ -23,7 +25,8 @@ def _function(path, name, cls=None):
     return ast.get_source_segment(open(path).read(), fn)
 
 
-def main():
+def main(ref: str):
+    REF = os.path.join(ref, "src", "QligFEP")
     ns = {}
     exec(_function(os.path.join(REF, "functions.py"), "sigmoid"), ns)
     src = _function(os.path.join(REF, "qligfep.py"), "get_lambdas", cls="QligFEP")
@@ -38,4 +41,6 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_lambda_golden.py /path/to/reference")
+    main(sys.argv[1])

@@ -175,15 +175,29 @@ def test_qdyn_log_layout():
     assert line == "Q-surr. 1 1.0000      3.12    139.43"
 
 
+# atoms x steps of a campaign's systems: 84 windows of one size, spheres of three
+SHARD_COSTS = [3161 * 2] * 84 + [1392, 3423, 6500, 1392, 6500, 3423, 3423, 6500, 1392, 6500, 6500, 1392, 3423,
+                                 3423, 1392, 6500]
+
+
 def _gloo_worker(rank, world, port, out):
+    import datetime
+
+    import numpy as np
     import torch.distributed as dist
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
-    dist.init_process_group("gloo", rank=rank, world_size=world)
-    from q_b200.dist import max_over_ranks, shard, sum_over_ranks
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    from q_b200.dist import gather_series, max_over_ranks, shard, sum_over_ranks
     mine = shard(100, rank, world)
     t = max_over_ranks(1.0 + rank)
     n = sum_over_ranks(len(mine))
-    out.put((rank, mine[:3], t, n))
+    owned = shard(len(SHARD_COSTS), rank, world, SHARD_COSTS)
+    load = sum(SHARD_COSTS[i] for i in owned)
+    # each rank's energy series of its systems (ragged lengths), gathered everywhere
+    series = {i: np.full((3 + i % 4, 2), float(i)) for i in owned}
+    allser = gather_series(series)
+    out.put((rank, mine[:3], t, n, owned, load, {k: v.shape for k, v in allser.items()},
+             all(np.all(v == k) for k, v in allser.items())))
     dist.destroy_process_group()
 
 
@@ -203,8 +217,23 @@ def test_multi_rank_helpers_gloo():
     res = sorted(q.get(timeout=120) for _ in procs)
     for p in procs:
         p.join(timeout=60)
-    assert res[0] == (0, [0, 2, 4], 2.0, 100.0)
-    assert res[1] == (1, [1, 3, 5], 2.0, 100.0)
+    assert res[0][:4] == (0, [0, 2, 4], 2.0, 100.0)
+    assert res[1][:4] == (1, [1, 3, 5], 2.0, 100.0)
+    # cost-balanced shards: disjoint, complete, loads within the LPT bound
+    o0, o1 = res[0][4], res[1][4]
+    assert sorted(o0 + o1) == list(range(len(SHARD_COSTS))) and not set(o0) & set(o1)
+    loads = [res[0][5], res[1][5]]
+    assert max(loads) <= 4 / 3 * sum(SHARD_COSTS) / 2 and max(loads) - min(loads) <= max(SHARD_COSTS)
+    # every rank received every system's series with its own shape and values
+    for r in res:
+        assert r[6] == {i: (3 + i % 4, 2) for i in range(len(SHARD_COSTS))} and r[7]
+
+
+def test_cost_shard_single_process():
+    from q_b200.dist import shard
+    costs = [5, 1, 1, 1, 1, 1]
+    assert shard(6, 0, 2, costs) == [0] and shard(6, 1, 2, costs) == [1, 2, 3, 4, 5]
+    assert shard(3, 0, 1, [1, 2, 3]) == [0, 1, 2]
 
 
 def test_derived_inputs_and_restart(tmp_path):

@@ -86,3 +86,60 @@ def test_benzene_maxwell_velocities_bit_exact(golden):
         if ";" in line:
             ref += [float(t) for t in line.split(";")]
     assert np.array_equal(v, np.array(ref))
+
+
+def read_fortran_re(path):
+    """qdyn's restart (write_xfin, md.f90:15452-15470), read here without the
+    library: gfortran unformatted sequential records of (int32 nat3, nat3
+    doubles) for x and v, each framed by int32 byte counts."""
+    raw = open(path, "rb").read()
+    recs, off = [], 0
+    while off < len(raw):
+        n = int(np.frombuffer(raw, "<i4", 1, off)[0])
+        body = raw[off + 4:off + 4 + n]
+        assert int(np.frombuffer(raw, "<i4", 1, off + 4 + n)[0]) == n
+        recs.append(body)
+        off += n + 8
+    out = []
+    for body in recs[:2]:
+        nat3 = int(np.frombuffer(body, "<i4", 1, 0)[0])
+        out.append(np.frombuffer(body, "<f8", nat3, 4).copy())
+    return raw, out[0], out[1], len(recs)
+
+
+def test_fortran_restart_read_and_written_byte_for_byte(golden, tmp_path):
+    """The restart file Fortran qdyn wrote for the 1-step benzene run: the
+    library's reader takes exactly its values, and the library's writer
+    reproduces the file byte for byte."""
+    from q_b200.api import write_restart
+    from q_b200.inputs import derive_inp
+    raw, x, v, nrec = read_fortran_re(str(golden / "benzene" / "eq1.re"))
+    assert len(raw) == 600 and nrec == 2 and x.size == v.size == 36
+    inp = derive_inp(str(golden / "benzene" / "eq1.inp"), "from_re.inp",
+                     set_keys={"files": {"restart": "eq1.re"}},
+                     drop_keys={"md": ["random_seed", "initial_temperature"]})
+    s = System.open(inp)
+    n = 3 * s.natom
+    assert np.array_equal(np.ctypeslib.as_array(s.view.x0, shape=(n,)), x)
+    assert np.array_equal(np.ctypeslib.as_array(s.view.v0, shape=(n,)), v)
+    out = str(tmp_path / "again.re")
+    write_restart(out, x, v)
+    assert open(out, "rb").read() == raw
+
+
+# Fortran's step and the restatement differ in the last bits of single-
+# precision intermediates (FP32 inverse masses and charges, gfortran's own
+# contraction of d*winv*dt): 5e-8 relative on velocities of ~0.03 A/fs-units
+RE_V_RTOL = 1e-7
+
+
+def test_oracle_step_matches_fortran_restart(golden, oracle):
+    """The oracle's one MD step of the benzene run (Maxwell velocities of
+    seed 112 at 1 K, leap-frog, Berendsen) against the coordinates and
+    velocities Fortran qdyn wrote after that step."""
+    _, x, v, _ = read_fortran_re(str(golden / "benzene" / "eq1.re"))
+    s = System.open(str(golden / "benzene" / "eq1.inp"))
+    run = oracle.create(s)
+    run.run(1)
+    assert np.max(np.abs(run.coords() - x)) < 1e-9
+    np.testing.assert_allclose(run.velocities(), v, rtol=RE_V_RTOL, atol=1e-12 + RE_V_RTOL * np.abs(v).max())

@@ -95,6 +95,92 @@ def test_static_entry_point_matches_batch_engine(tmp_path):
         assert err < G_TOL
 
 
+def ww_reference(x, excl, qo, qh, A, B, rc):
+    """numpy FP64 statement of nonbond_ww_spc (src/q6/md.f90:11823) over every
+    pair of non-excluded waters whose O-O distance is within rc: energies
+    (el, vdw) and the gradient dU/dx, waters as O,H,H."""
+    w = x.reshape(-1, 3, 3)
+    keep = ~excl.astype(bool)
+    n = len(w)
+    i, j = np.triu_indices(n, 1)
+    ok = keep[i] & keep[j] & (np.linalg.norm(w[j, 0] - w[i, 0], axis=1) <= rc)
+    i, j = i[ok], j[ok]
+    q = np.array([qo, qh, qh], dtype=np.float32)
+    g = np.zeros_like(w)
+    el = vdw = 0.0
+    for a in range(3):
+        for b in range(3):
+            d = w[j, b] - w[i, a]
+            r2 = np.einsum("ij,ij->i", d, d)
+            rinv = 1.0 / np.sqrt(r2)
+            vel = float(np.float32(q[a] * q[b])) * rinv
+            dv = -vel * rinv ** 2
+            el += vel.sum()
+            if a == 0 and b == 0:
+                r6 = rinv ** 6
+                va, vb = A * r6 * r6, B * r6
+                vdw += (va - vb).sum()
+                dv = dv + rinv ** 2 * (-12.0 * va + 6.0 * vb)
+            f = dv[:, None] * d
+            np.add.at(g[:, a], i, -f)
+            np.add.at(g[:, b], j, f)
+    return el, vdw, g.reshape(-1)
+
+
+def test_static_entry_point_excluded_waters_and_overflow(tmp_path):
+    """Waters flagged in `excl` take part in no pair: checked against a numpy
+    FP64 statement of the water-water terms on the same coordinates.  A water
+    with more neighbours than the fixed list row holds sets
+    QB_ERR_LIST_OVERFLOW in the status word."""
+    torch = pytest.importorskip("torch")
+    from q_b200 import System, synth
+    from q_b200._lib import check, lib
+
+    g = synth.water_sphere(str(tmp_path), radius=15.0, seed=7)
+    inp = tmp_path / "pure.inp"
+    inp.write_text(PURE_WW_INP % g.top)
+    sys_ = System.open(str(inp))
+    v = sys_.view
+    nwat, ns = v.nwat, v.nat_solute
+    dev = torch.device("cuda:0")
+    stream = torch.cuda.current_stream(dev)
+    xh = np.ctypeslib.as_array(v.xtop, shape=(3 * v.natom,))[3 * ns:].copy()
+    rng = np.random.default_rng(5)
+    excl = (rng.random(nwat) < 0.2).astype(np.uint8)
+    x = torch.tensor(xh, dtype=torch.float64, device=dev)
+    ex = torch.tensor(excl, dtype=torch.uint8, device=dev)
+    grad = torch.empty(9 * nwat, dtype=torch.float64, device=dev)
+    energy = torch.empty(2, dtype=torch.float64, device=dev)
+    status = torch.empty(1, dtype=torch.int32, device=dev)
+
+    def call(xd, n, rc, exd):
+        check(lib.qb_ww_energy_static(C.c_void_p(xd.data_ptr()), n, v.crg_ow, v.crg_hw, v.A_OO, v.B_OO, rc,
+                                      C.c_void_p(exd.data_ptr()) if exd is not None else None,
+                                      C.c_void_p(grad.data_ptr()), C.c_void_p(energy.data_ptr()),
+                                      C.c_void_p(status.data_ptr()), C.c_void_p(stream.cuda_stream)))
+        torch.cuda.synchronize(dev)
+        return int(status.item()), energy.cpu().numpy().copy(), grad.cpu().numpy()[:9 * n].copy()
+
+    st, e, gr = call(x, nwat, v.Rcww, ex)
+    assert st == 0
+    el, vdw, gref = ww_reference(xh, excl, v.crg_ow, v.crg_hw, v.A_OO, v.B_OO, v.Rcww)
+    assert abs(e[0] - el) < E_TOL and abs(e[1] - vdw) < E_TOL
+    gs, gb = gr.reshape(-1, 3), gref.reshape(-1, 3)
+    nrm = np.linalg.norm(gb, axis=1)
+    floor = 0.01 * np.sqrt(np.mean(nrm ** 2))
+    assert np.max(np.linalg.norm(gs - gb, axis=1) / np.maximum(nrm, floor)) < G_TOL
+    assert not np.any(gs.reshape(-1, 9)[excl.astype(bool)])
+
+    # every water of a 15 A sphere lies within 40 A of every other: rows of
+    # nwat - 1 > QB_STATIC_WW_MAX_NEIGHBOURS entries
+    assert nwat - 1 > 192
+    st, _, _ = call(x, nwat, 40.0, None)
+    assert st == 7   # QB_ERR_LIST_OVERFLOW
+    # the next call starts from a cleared status word
+    st, e2, _ = call(x, nwat, v.Rcww, ex)
+    assert st == 0 and abs(e2[0] - el) < E_TOL
+
+
 def test_static_entry_point_rejects_oversized_systems():
     from q_b200._lib import lib
     rc = lib.qb_ww_energy_static(None, 10 ** 6, 0.0, 0.0, 0.0, 0.0, 10.0, None, None, None, None, None)

@@ -183,8 +183,23 @@ static void list_pp(qo_state *st) {
       if ((IG > JG && (IG + JG) % 2 == 0) || (IG < JG && (IG + JG) % 2 == 1)) continue;
       int js = s->cgp_iswitch[jg];
       if (s->excl[js]) continue;
-      double r2 = dist2(st, is, js);
-      if (r2 <= rc2) {
+      double r2;
+      int inside;
+      if (s->iuse_switch_atom == 1) {
+        r2 = dist2(st, is, js);
+        inside = r2 <= rc2;
+      } else {
+        /* nbpplis2_lrf (md.f90:4926-4970): inside when any atom pair is; r2
+           keeps the last pair computed (the groups' last atoms when none is) */
+        inside = 0;
+        r2 = 0;
+        for (int ia = s->cgp_first[ig]; ia <= s->cgp_last[ig] && !inside; ia++)
+          for (int ja = s->cgp_first[jg]; ja <= s->cgp_last[jg]; ja++) {
+            r2 = dist2(st, s->cgpatom[ia], s->cgpatom[ja]);
+            if (r2 <= rc2) { inside = 1; break; }
+          }
+      }
+      if (inside) {
         for (int ia = s->cgp_first[ig]; ia <= s->cgp_last[ig]; ia++) {
           int i = s->cgpatom[ia];
           if (s->iqatom[i] >= 0) continue;
@@ -221,8 +236,22 @@ static void list_pw(qo_state *st) {
     for (int iw = 0; iw < st->nwat; iw++) {
       int o = st->NS + 3 * iw;
       if (s->excl[o]) continue;
-      double r2 = dist2(st, is, o);
-      if (r2 <= rc2) {
+      double r2;
+      int inside;
+      if (s->iuse_switch_atom == 1) {
+        r2 = dist2(st, is, o);
+        inside = r2 <= rc2;
+      } else {
+        /* nbpwlis2_lrf (md.f90:6500-6516): any atom of the group within the
+           cut-off of the water O; r2 keeps the last distance computed */
+        inside = 0;
+        r2 = 0;
+        for (int ia = s->cgp_first[ig]; ia <= s->cgp_last[ig] && !inside; ia++) {
+          r2 = dist2(st, s->cgpatom[ia], o);
+          if (r2 <= rc2) inside = 1;
+        }
+      }
+      if (inside) {
         for (int ia = s->cgp_first[ig]; ia <= s->cgp_last[ig]; ia++) {
           int i = s->cgpatom[ia];
           if (s->iqatom[i] >= 0) continue;
@@ -293,9 +322,21 @@ static void list_qp(qo_state *st) {
   for (int ig = 0; ig < s->ncgp_solute; ig++) {
     int sw = s->cgp_iswitch[ig];
     if (s->excl[sw]) continue;
-    double r2 = 0;
-    for (int k = 0; k < 3; k++) { double d = X(sw, k) - s->xpcent[k]; r2 += d * d; }
-    if (r2 > rc2) continue;
+    int inside = 0;
+    if (s->iuse_switch_atom == 1) {
+      double r2 = 0;
+      for (int k = 0; k < 3; k++) { double d = X(sw, k) - s->xpcent[k]; r2 += d * d; }
+      inside = r2 <= rc2;
+    } else {
+      /* nbqplis2 (md.f90:7700-7716): any atom of the group within Rcq */
+      for (int ia = s->cgp_first[ig]; ia <= s->cgp_last[ig] && !inside; ia++) {
+        int i = s->cgpatom[ia];
+        double r2 = 0;
+        for (int k = 0; k < 3; k++) { double d = X(i, k) - s->xpcent[k]; r2 += d * d; }
+        inside = r2 <= rc2;
+      }
+    }
+    if (!inside) continue;
     for (int ia = s->cgp_first[ig]; ia <= s->cgp_last[ig]; ia++) {
       int i = s->cgpatom[ia];
       int near = 0;

@@ -188,9 +188,10 @@ struct Batch {
     if (any_lrf) {
       launch("cgp_centers", [&] { k_cgp_centers<<<cdiv(p.ncgp_tot, 256), b256, 0, s1>>>(p, force); });
       launch("lrf_gather", [&] {
-        dim3 g(max_lrf_blocks, nsys);
-        if (opt.precision == QB_MIXED) k_lrf_gather<true><<<g, LRF_BLOCK, 0, s1>>>(p, force);
-        else k_lrf_gather<false><<<g, LRF_BLOCK, 0, s1>>>(p, force);
+        if (opt.precision == QB_MIXED)
+          k_lrf_gather_x2<<<dim3(max_lrfx_blocks, nsys), LRFX_BLOCK, 0, s1>>>(p, force);
+        else
+          k_lrf_gather<false><<<dim3(max_lrf_blocks, nsys), LRF_BLOCK, 0, s1>>>(p, force);
       });
     }
     if (max_nwat > 0)
@@ -232,10 +233,14 @@ struct Batch {
   // profiling or without side streams).
   bool forking() const { return !profiling && side[0] && streams_on; }
 
+  int max_lrfx_blocks = 1;   // the packed (two targets per thread) gather's grid
   void set_lrf_tpb(int tpb) {
     P.lrf_tpb = tpb;
-    max_lrf_blocks = 1;
-    for (const int2 &d : lrf_dims) max_lrf_blocks = std::max(max_lrf_blocks, cdiv(d.x, LRF_BLOCK) * cdiv(d.y, tpb));
+    max_lrf_blocks = max_lrfx_blocks = 1;
+    for (const int2 &d : lrf_dims) {
+      max_lrf_blocks = std::max(max_lrf_blocks, cdiv(d.x, LRF_BLOCK) * cdiv(d.y, tpb));
+      max_lrfx_blocks = std::max(max_lrfx_blocks, cdiv(d.x, LRFX_TARGETS) * cdiv(d.y, tpb));
+    }
   }
   void fork_streams() {
     if (!forking()) return;
@@ -503,7 +508,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     SysDev &S = B.sysh[s];
     std::memset(&S, 0, sizeof S);
     if (V.nstates > MAXS) fail(QB_ERR_UNSUPPORTED, "too many states");
-    if (V.iuse_switch_atom != 1) fail(QB_ERR_UNSUPPORTED, "charge-group cut-offs on any atom are not supported");
+
     const int aoff = (int)x.size();
     S.aoff = aoff; S.natom = V.natom; S.nsol = V.nat_solute; S.nwat = V.nwat;
     if (V.nwat > 65535) fail(QB_ERR_UNSUPPORTED, "more than 65535 waters in one system");
@@ -710,6 +715,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
       rw_p.push_back(make_double4(V.rwal_d[r], V.rwal_fk[r], V.rwal_aMorse[r], V.rwal_dMorse[r]));
     }
     // scalars
+    S.switch_atoms = V.iuse_switch_atom == 1 ? 1 : 0;
     S.ff_type = V.ff_type; S.use_lrf = V.use_LRF; S.qvdw = V.qvdw_flag; S.qq_lib = V.qq_use_library_charges;
     S.wpol = V.wpol_restr && V.nwpolr_shell > 0; S.nshell = V.nwpolr_shell;
     if (S.nshell > MAX_SHELLS) fail(QB_ERR_UNSUPPORTED, "too many water polarisation shells");

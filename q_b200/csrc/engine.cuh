@@ -17,7 +17,8 @@ namespace qb {
 constexpr int MAXS = QB_MAX_STATES;
 // LRF record of a charge group: centre[3], phi0, phi1[3], the 6 distinct
 // components of the symmetric phi2 (xx,xy,xz,yy,yz,zz) and the 10 of phi3
-// (xxx,xxy,xxz,xyy,xyz,xzz,yyy,yyz,yzz,zzz), pad.
+// (xxx,xxy,xxz,xyy,xyz,xzz,yyy,yyz,yzz,zzz), and the group's radius (largest
+// distance of a member atom from the centre).
 constexpr int LRF_STRIDE = 24;
 constexpr int MAX_SHELLS = 4;
 // one history record: step, E[QB_NE], EQ[MAXS*QB_NEQ], r_kl of the off-diagonal functions [MAXS]
@@ -68,6 +69,9 @@ struct SysDev {
   int hlj, iac_hw;
   double A_OH, B_OH, A_HH, B_HH, aH[2], bH[2];
   int arith;                       // 1: arithmetic LJ combination rule (lj_pair)
+  // 1: solute charge-group cut-offs on switch atoms (nbpplist_lrf ...); 0: on
+  // any atom pair (nbpplis2_lrf, nbpwlis2_lrf, nbqplis2: iuse_switch_atom 0)
+  int switch_atoms;
 };
 
 // Per-system state written by the device.

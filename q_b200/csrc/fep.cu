@@ -459,6 +459,9 @@ void fep_run(const FepSource &src, const qb_fep_params &p, int device, cudaStrea
   if (p.nnoffd > 0) put(d_roff.p, src.rfoff, stream);
   for (auto *b : {d_dgf.p, d_dgr.p, d_dgti.p, d_dglu.p, d_dgbar.p})
     FEP_CUDA(cudaMemsetAsync(b, 0, sizeof(double) * (nfiles + 2), stream));
+  // k_fep_bins writes the rows of bins that hold points; the others must read
+  // as empty (count 0), whatever the allocation held before
+  FEP_CUDA(cudaMemsetAsync(d_part2.p, 0, sizeof(double) * (size_t)nfiles * nb * QB_FEP_PART2_W, stream));
   FEP_CUDA(cudaMemsetAsync(d_its.p, 0, sizeof(int) * (nfiles + 2), stream));
 
   FepDev D{};

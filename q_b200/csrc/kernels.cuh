@@ -66,7 +66,87 @@ __global__ void k_cgp_centers(DevPtrs P, int force) {
   double n = (double)(float)(l - f + 1);
   double *L = P.lrf + (size_t)g * LRF_STRIDE;
   for (int k = 0; k < 3; k++) L[k] = c[k] / n;
-  for (int k = 3; k < LRF_STRIDE; k++) L[k] = 0.0;
+  for (int k = 3; k < LRF_STRIDE - 1; k++) L[k] = 0.0;
+  // radius: bounds every atom pair of two groups by their centres (the
+  // any-atom cut-off tests of iuse_switch_atom 0 skip far groups with it)
+  double rmax = 0.0;
+  for (int a = f; a <= l; a++) {
+    double3 xa = ld3(P.x, P.cg_atoms[a]);
+    double dx = xa.x - L[0], dy = xa.y - L[1], dz = xa.z - L[2];
+    rmax = fmax(rmax, sqrt(dx * dx + dy * dy + dz * dz));
+  }
+  L[LRF_STRIDE - 1] = rmax;
+}
+
+// The any-atom cut-off tests of iuse_switch_atom 0 (nbpplis2_lrf md.f90:4955,
+// nbpwlis2_lrf 6500, nbqplis2 7700), FP64 as the reference.
+// Solute group pair: inside when any atom pair of the two groups is within
+// rc2; *last receives the squared distance of the last pair computed (the two
+// groups' last atoms when none is inside), which the reference then tests
+// against RcLRF.
+__device__ __forceinline__ bool groups_inside_any(const DevPtrs &P, int gi, int gj, double rc2, double *last) {
+  double r2 = 0.0;
+  for (int ia = P.cg_first[gi]; ia <= P.cg_last[gi]; ia++) {
+    const double3 xi = ld3(P.x, P.cg_atoms[ia]);
+    for (int ja = P.cg_first[gj]; ja <= P.cg_last[gj]; ja++) {
+      const double3 xj = ld3(P.x, P.cg_atoms[ja]);
+      const double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+      r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 <= rc2) { *last = r2; return true; }
+    }
+  }
+  *last = r2;
+  return false;
+}
+
+// Solute group and a point (a water O or the solute centre): inside when any
+// atom of the group is within rc2 of it; *last as above.
+__device__ __forceinline__ bool group_point_inside_any(const DevPtrs &P, int gi, double3 p, double rc2, double *last) {
+  double r2 = 0.0;
+  for (int ia = P.cg_first[gi]; ia <= P.cg_last[gi]; ia++) {
+    const double3 xi = ld3(P.x, P.cg_atoms[ia]);
+    const double dx = xi.x - p.x, dy = xi.y - p.y, dz = xi.z - p.z;
+    r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 <= rc2) { *last = r2; return true; }
+  }
+  *last = r2;
+  return false;
+}
+
+// Near/far test of an LRF gather pair (target group g, source group h) under
+// iuse_switch_atom 0, when one of them is a solute group: true when the pair
+// takes part in the LRF (outside the any-atom cut-off, last pair within
+// RcLRF).  Groups whose centres are farther apart than the cut-off plus both
+// radii (with a margin) are outside without the atom loop.
+__device__ __forceinline__ bool lrf_window_any(const DevPtrs &P, const SysDev &S, int g, bool g_sol, int h, bool h_sol,
+                                               double rc2) {
+  const double *Lg = P.lrf + (size_t)g * LRF_STRIDE, *Lh = P.lrf + (size_t)h * LRF_STRIDE;
+  const double dx = Lg[0] - Lh[0], dy = Lg[1] - Lh[1], dz = Lg[2] - Lh[2];
+  const double dc = sqrt(dx * dx + dy * dy + dz * dz);
+  const bool far = dc - Lg[LRF_STRIDE - 1] - Lh[LRF_STRIDE - 1] > sqrt(rc2) + 1e-6;
+  double last;
+  bool inside;
+  if (g_sol && h_sol) {
+    if (far) {
+      const double3 a = ld3(P.x, P.cg_atoms[P.cg_last[g]]), b = ld3(P.x, P.cg_atoms[P.cg_last[h]]);
+      last = (a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y) + (a.z - b.z) * (a.z - b.z);
+      inside = false;
+    } else {
+      inside = groups_inside_any(P, g, h, rc2, &last);
+    }
+  } else {
+    // solute group and water: the group's atoms against the water O
+    const int gs = g_sol ? g : h, gw = g_sol ? h : g;
+    const double3 o = ld3(P.x, P.cg_sw[gw]);
+    if (far) {
+      const double3 a = ld3(P.x, P.cg_atoms[P.cg_last[gs]]);
+      last = (a.x - o.x) * (a.x - o.x) + (a.y - o.y) * (a.y - o.y) + (a.z - o.z) * (a.z - o.z);
+      inside = false;
+    } else {
+      inside = group_point_inside_any(P, gs, o, rc2, &last);
+    }
+  }
+  return !inside && last <= S.RcLRF2;
 }
 
 // Multipole contribution of charge q at offset (dx,dy,dz) from a group centre
@@ -242,10 +322,14 @@ __global__ void __launch_bounds__(LRF_BLOCK, MIXED ? 8 : 5) k_lrf_gather(DevPtrs
       for (int i = 0; i < nh; i++) {
         double4 hs = hsw[i];
         if (hs.w < 0.0 || tile.x + i == gl) continue;
-        double dx = xs.x - hs.x, dy = xs.y - hs.y, dz = xs.z - hs.z;
-        double r2 = dx * dx + dy * dy + dz * dz;
         double rc2 = (g_sol && hs.w > 0.0) ? S.Rcpp2 : ((g_sol || hs.w > 0.0) ? S.Rcpw2 : S.Rcww2);
-        if (!(r2 > rc2 && r2 <= S.RcLRF2)) continue;
+        if (!S.switch_atoms && (g_sol || hs.w > 0.0)) {
+          if (!lrf_window_any(P, S, g, g_sol, S.coff + tile.x + i, hs.w > 0.0, rc2)) continue;
+        } else {
+          double dx = xs.x - hs.x, dy = xs.y - hs.y, dz = xs.z - hs.z;
+          double r2 = dx * dx + dy * dy + dz * dz;
+          if (!(r2 > rc2 && r2 <= S.RcLRF2)) continue;
+        }
         int2 rg = hrange[i];
         if (MIXED) {
           // a zero charge adds exact zeros; water groups (3 atoms) unrolled
@@ -297,6 +381,180 @@ __global__ void __launch_bounds__(LRF_BLOCK, MIXED ? 8 : 5) k_lrf_gather(DevPtrs
       for (int k = 0; k < 20; k++)
         if (m[MIXED ? 0 : k] != 0.0) atomicAdd(&L[3 + k], m[MIXED ? 0 : k]);
     }
+  }
+}
+
+// -------------------------------------------- packed FP32x2 LRF gather
+
+// lrf_accumulate_split for two target groups at once (.x and .y), on the
+// packed FP32x2 pipes.  Sign conventions differ so that every update is one
+// fused multiply-add: m[1..3] hold +sum f0*d (phi1 = -m[1..3]), m[10..19] and
+// t[1..3] hold the phi3 sums with f2 taken positive (phi3 = -(fold of them));
+// lrf_finish_x2 restores the signs.
+// sel is 1 for a target inside the pair's window and 0 outside it (its
+// charge q is then 0); unsel = 1 - sel.  A half outside the window may sit at
+// distance 0 (a one-atom group against itself), so its r2 is replaced by 1
+// before the reciprocal: every term of that half is then an exact 0.
+__device__ __forceinline__ void lrf_accumulate_x2(float2 *m, float2 *t, float2 q, float2 dx, float2 dy, float2 dz,
+                                                  float2 sel, float2 unsel) {
+  const float2 three = make_float2(3.f, 3.f), five = make_float2(5.f, 5.f);
+  const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+  const float2 r2s = __ffma2_rn(r2, sel, unsel);
+  const float2 rinv = make_float2(rsqrt_ftz(r2s.x), rsqrt_ftz(r2s.y));
+  const float2 ri2 = __fmul2_rn(rinv, rinv);
+  const float2 f0 = __fmul2_rn(__fmul2_rn(q, rinv), ri2);          // q / r^3
+  m[0] = __ffma2_rn(f0, r2, m[0]);
+  m[1] = __ffma2_rn(f0, dx, m[1]); m[2] = __ffma2_rn(f0, dy, m[2]); m[3] = __ffma2_rn(f0, dz, m[3]);
+  t[0] = __fadd2_rn(t[0], f0);
+  const float2 f1 = __fmul2_rn(__fmul2_rn(f0, ri2), three);        // 3 q / r^5
+  const float2 ax = __fmul2_rn(f1, dx), ay = __fmul2_rn(f1, dy), az = __fmul2_rn(f1, dz);
+  m[4] = __ffma2_rn(ax, dx, m[4]); m[5] = __ffma2_rn(ax, dy, m[5]); m[6] = __ffma2_rn(ax, dz, m[6]);
+  m[7] = __ffma2_rn(ay, dy, m[7]); m[8] = __ffma2_rn(ay, dz, m[8]); m[9] = __ffma2_rn(az, dz, m[9]);
+  const float2 f2 = __fmul2_rn(f1, ri2);                            // 3 q / r^7 (the negated f2)
+  const float2 w = __fmul2_rn(f2, r2);
+  t[1] = __ffma2_rn(w, dx, t[1]); t[2] = __ffma2_rn(w, dy, t[2]); t[3] = __ffma2_rn(w, dz, t[3]);
+  const float2 u = __fmul2_rn(f2, five);
+  const float2 px = __fmul2_rn(u, dx), py = __fmul2_rn(u, dy), pz = __fmul2_rn(u, dz);
+  const float2 qxx = __fmul2_rn(px, dx), qxy = __fmul2_rn(px, dy), qxz = __fmul2_rn(px, dz);
+  const float2 qyy = __fmul2_rn(py, dy), qyz = __fmul2_rn(py, dz), qzz = __fmul2_rn(pz, dz);
+  m[10] = __ffma2_rn(qxx, dx, m[10]); m[11] = __ffma2_rn(qxx, dy, m[11]); m[12] = __ffma2_rn(qxx, dz, m[12]);
+  m[13] = __ffma2_rn(qxy, dy, m[13]); m[14] = __ffma2_rn(qxy, dz, m[14]); m[15] = __ffma2_rn(qxz, dz, m[15]);
+  m[16] = __ffma2_rn(qyy, dy, m[16]); m[17] = __ffma2_rn(qyy, dz, m[17]); m[18] = __ffma2_rn(qyz, dz, m[18]);
+  m[19] = __ffma2_rn(qzz, dz, m[19]);
+}
+
+// One target's packed sums (half h of every float2) as the record's 20
+// components in FP64: the diagonal terms folded in, the signs restored.
+__device__ __forceinline__ void lrf_finish_x2(const float2 *m, const float2 *t, int h, double *out) {
+  double tt[4];
+#pragma unroll
+  for (int k = 0; k < 20; k++) out[k] = (double)(h ? m[k].y : m[k].x);
+#pragma unroll
+  for (int k = 0; k < 4; k++) tt[k] = (double)(h ? t[k].y : t[k].x);
+  lrf_fold(out, tt);
+#pragma unroll
+  for (int k = 1; k < 4; k++) out[k] = -out[k];
+#pragma unroll
+  for (int k = 10; k < 20; k++) out[k] = -out[k];
+}
+
+// The mixed-precision LRF gather (nbpp/pw/wwlist_lrf, md.f90:5448, 6864,
+// 8370) with two target groups per thread: targets gl and gl + LRFX_BLOCK of
+// the block's chunk of 2*LRFX_BLOCK groups, each source charge applied to
+// both with packed FP32x2 arithmetic (a target outside the pair's window
+// takes a zero charge).  Source tiles are staged as in k_lrf_gather, atom
+// positions and charges duplicated into both halves of their float2 words;
+// the group-pair window test is FP64.  Each block sums its tiles in FP32 and
+// adds the totals to the FP64 record with one atomic per component.
+constexpr int LRFX_BLOCK = 128, LRFX_TARGETS = 2 * LRFX_BLOCK;
+
+__global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int force) {
+  const int s = blockIdx.y;
+  if (!list_due(P, s, force)) return;
+  const SysDev &S = P.sys[s];
+  if (!S.use_lrf) return;
+  const int tpb = P.lrf_tpb;
+  const int hsplit = (S.nlrft + tpb - 1) / tpb;
+  const int gchunk = blockIdx.x / max(hsplit, 1), hpart = blockIdx.x % max(hsplit, 1);
+  if (hsplit == 0 || gchunk * LRFX_TARGETS >= S.ncgp) return;
+  const int t0 = hpart * tpb, t1 = min(t0 + tpb, S.nlrft);
+  __shared__ double4 hsw[LRF_TILE_G];
+  __shared__ int2 hrange[LRF_TILE_G];
+  __shared__ float4 hxy[LRF_TILE_A], hzq[LRF_TILE_A];   // {x, x, y, y}, {z, z, q, q}
+  const double ox = S.xp[0], oy = S.xp[1], oz = S.xp[2];
+  int gl[2];
+  bool act[2], gsol[2];
+  double3 xs[2];
+  float cc[2][3];
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    gl[h] = gchunk * LRFX_TARGETS + h * LRFX_BLOCK + threadIdx.x;
+    act[h] = gl[h] < S.ncgp;
+    gsol[h] = gl[h] < S.ncgp_sol;
+    xs[h] = make_double3(0, 0, 0);
+    cc[h][0] = cc[h][1] = cc[h][2] = 0.f;
+    if (act[h]) {
+      const int g = S.coff + gl[h];
+      const int swg = P.cg_sw[g];
+      act[h] = !(P.flags[swg] & F_EXCL);
+      const double *L = P.lrf + (size_t)g * LRF_STRIDE;
+      cc[h][0] = (float)(L[0] - ox); cc[h][1] = (float)(L[1] - oy); cc[h][2] = (float)(L[2] - oz);
+      xs[h] = ld3(P.x, swg);
+    }
+  }
+  // minus the two target centres (positions relative to the sphere centre)
+  const float2 ncx = make_float2(-cc[0][0], -cc[1][0]), ncy = make_float2(-cc[0][1], -cc[1][1]),
+               ncz = make_float2(-cc[0][2], -cc[1][2]);
+  float2 m[20], t[4];
+#pragma unroll
+  for (int k = 0; k < 20; k++) m[k] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int k = 0; k < 4; k++) t[k] = make_float2(0.f, 0.f);
+  for (int tt = t0; tt < t1; tt++) {
+    const int2 tile = P.lrft[S.lrft_off + tt];
+    const int nh = tile.y - tile.x;
+    const int a0 = P.cg_first[S.coff + tile.x];
+    const int na = P.cg_last[S.coff + tile.y - 1] - a0 + 1;
+    __syncthreads();
+    for (int i = threadIdx.x; i < nh; i += LRFX_BLOCK) {
+      const int h = S.coff + tile.x + i;
+      const int sw = P.cg_sw[h];
+      const double3 p = ld3(P.x, sw);
+      const double w = (P.flags[sw] & F_EXCL) ? -1.0 : (tile.x + i < S.ncgp_sol ? 1.0 : 0.0);
+      hsw[i] = make_double4(p.x, p.y, p.z, w);
+      hrange[i] = make_int2(P.cg_first[h] - a0, P.cg_last[h] - P.cg_first[h] + 1);
+    }
+    for (int i = threadIdx.x; i < na; i += LRFX_BLOCK) {
+      const int at = P.cg_atoms[a0 + i];
+      const double4 p = P.x[at];
+      const bool qsol = (at - S.aoff) < S.nsol && P.iq[at] >= 0;
+      const float x = (float)(p.x - ox), y = (float)(p.y - oy), z = (float)(p.z - oz);
+      const float q = qsol ? 0.f : P.crg[at];
+      hxy[i] = make_float4(x, x, y, y);
+      hzq[i] = make_float4(z, z, q, q);
+    }
+    __syncthreads();
+    if (!(act[0] || act[1])) continue;
+    for (int i = 0; i < nh; i++) {
+      const double4 hs = hsw[i];
+      if (hs.w < 0.0) continue;
+      float2 sel;
+      bool any = false;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const double rc2 = (gsol[h] && hs.w > 0.0) ? S.Rcpp2 : ((gsol[h] || hs.w > 0.0) ? S.Rcpw2 : S.Rcww2);
+        bool in;
+        if (!S.switch_atoms && (gsol[h] || hs.w > 0.0)) {
+          in = act[h] && tile.x + i != gl[h] &&
+               lrf_window_any(P, S, S.coff + gl[h], gsol[h], S.coff + tile.x + i, hs.w > 0.0, rc2);
+        } else {
+          const double dx = xs[h].x - hs.x, dy = xs[h].y - hs.y, dz = xs[h].z - hs.z;
+          const double r2 = dx * dx + dy * dy + dz * dz;
+          in = act[h] && tile.x + i != gl[h] && r2 > rc2 && r2 <= S.RcLRF2;
+        }
+        any = any || in;
+        (h ? sel.y : sel.x) = in ? 1.f : 0.f;
+      }
+      if (!any) continue;
+      const int2 rg = hrange[i];
+      const float2 unsel = make_float2(1.f - sel.x, 1.f - sel.y);
+      for (int k = 0; k < rg.y; k++) {
+        const float4 a = hxy[rg.x + k], b = hzq[rg.x + k];
+        const float2 q = __fmul2_rn(make_float2(b.z, b.w), sel);
+        lrf_accumulate_x2(m, t, q, __fadd2_rn(make_float2(a.x, a.y), ncx), __fadd2_rn(make_float2(a.z, a.w), ncy),
+                          __fadd2_rn(make_float2(b.x, b.y), ncz), sel, unsel);
+      }
+    }
+  }
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    if (!act[h]) continue;
+    double out[20];
+    lrf_finish_x2(m, t, h, out);
+    double *L = P.lrf + (size_t)(S.coff + gl[h]) * LRF_STRIDE;
+#pragma unroll
+    for (int k = 0; k < 20; k++)
+      if (out[k] != 0.0) atomicAdd(&L[3 + k], out[k]);
   }
 }
 
@@ -434,9 +692,14 @@ __global__ void k_list_pp(DevPtrs P, int force) {
     int gj = S.coff + jg;
     int swj = P.cg_sw[gj];
     if (P.flags[swj] & F_EXCL) continue;
-    double3 xj = ld3(P.x, swj);
-    double dx = xs.x - xj.x, dy = xs.y - xj.y, dz = xs.z - xj.z;
-    if (dx * dx + dy * dy + dz * dz > S.Rcpp2) continue;
+    if (S.switch_atoms) {
+      double3 xj = ld3(P.x, swj);
+      double dx = xs.x - xj.x, dy = xs.y - xj.y, dz = xs.z - xj.z;
+      if (dx * dx + dy * dy + dz * dz > S.Rcpp2) continue;
+    } else {
+      double last;
+      if (!groups_inside_any(P, gi, gj, S.Rcpp2, &last)) continue;
+    }
     for (int ia = P.cg_first[gi]; ia <= P.cg_last[gi]; ia++) {
       int i = P.cg_atoms[ia];
       if (P.iq[i] >= 0) continue;
@@ -480,8 +743,13 @@ __global__ void k_list_pw(DevPtrs P, int force) {
       bool ok = false;
       if (iw < S.nwat && !(P.flags[o] & F_EXCL)) {
         double3 xo = ld3(P.x, o);
-        double dx = xs.x - xo.x, dy = xs.y - xo.y, dz = xs.z - xo.z;
-        ok = dx * dx + dy * dy + dz * dz <= S.Rcpw2;
+        if (S.switch_atoms) {
+          double dx = xs.x - xo.x, dy = xs.y - xo.y, dz = xs.z - xo.z;
+          ok = dx * dx + dy * dy + dz * dz <= S.Rcpw2;
+        } else {
+          double last;
+          ok = group_point_inside_any(P, gi, xo, S.Rcpw2, &last);
+        }
       }
       unsigned bal = __ballot_sync(FULL, ok);
       if (ok) {
@@ -515,9 +783,14 @@ __global__ void k_list_qp(DevPtrs P, int force) {
     int gi = S.coff + ig;
     int sw = P.cg_sw[gi];
     if (P.flags[sw] & F_EXCL) continue;
-    double3 xs = ld3(P.x, sw);
-    double dx = xs.x - S.xp[0], dy = xs.y - S.xp[1], dz = xs.z - S.xp[2];
-    if (dx * dx + dy * dy + dz * dz > S.Rcq2) continue;
+    if (S.switch_atoms) {
+      double3 xs = ld3(P.x, sw);
+      double dx = xs.x - S.xp[0], dy = xs.y - S.xp[1], dz = xs.z - S.xp[2];
+      if (dx * dx + dy * dy + dz * dz > S.Rcq2) continue;
+    } else {
+      double last;
+      if (!group_point_inside_any(P, gi, make_double3(S.xp[0], S.xp[1], S.xp[2]), S.Rcq2, &last)) continue;
+    }
     int f = P.cg_first[gi], n = P.cg_last[gi] - f + 1;
     for (int t = threadIdx.x; t < n * S.nq; t += blockDim.x) {
       int i = P.cg_atoms[f + t / S.nq], iq = t % S.nq;

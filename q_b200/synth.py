@@ -85,6 +85,7 @@ class Topology:
     res_starts: list = field(default_factory=list)
     res_names: list = field(default_factory=list)
     nat_solute: int = 0
+    switch_atoms: int = 1       # 1: charge-group cut-offs on switch atoms; 0: on any atom pair (the *lis2 lists)
     nbonds_solute: int = 0
     nangles_solute: int = 0
     ntors_solute: int = 0
@@ -155,7 +156,7 @@ class Topology:
         for k in range(0, n, 10):
             L.append(" ".join("%7.4f" % q for q in self.crg[k:k + 10]))
         L.append("%8d%8d%8d = No. of charge groups, no of solvent cgps, switch atoms flag. nat_cgp, iswitch / atom list: "
-                 % (len(self.cgps), self.ncgp_solute, 1))
+                 % (len(self.cgps), self.ncgp_solute, self.switch_atoms))
         for sw, atoms in self.cgps:
             L.append("%5d %5d" % (len(atoms), sw + 1))
             for k in range(0, len(atoms), 13):
@@ -720,7 +721,7 @@ def fep_solute(outdir: str, radius: float = 20.0, seed: int = 1234, steps: int =
                lambdas=(0.5, 0.5), run_seed: int = 1, vdw_rule: int = 1, ff_type: int = 2,
                q_bonded: bool = False, ub_fk: float = 25.0, soft_pairs: int = 0,
                library_charges: bool = False, water_h_lj=(0.0, 0.0), solvent_type: int = 0,
-               off_diagonals=(), morse_couplings: bool = False) -> Generated:
+               off_diagonals=(), morse_couplings: bool = False, switch_atoms: int = 1) -> Generated:
     """Config 1: 56-atom solute with 8 two-state Q-atoms in a TIP3P sphere,
     2 fs with SHAKE on X-H bonds and water.  ff_type 3 writes it as a CHARMM
     topology (charmm_terms, Urey-Bradley constant ub_fk); q_bonded redefines the bonded terms among the
@@ -735,7 +736,7 @@ def fep_solute(outdir: str, radius: float = 20.0, seed: int = 1234, steps: int =
     types, iac = _tree_types(kinds)
     n = len(X)
     top = Topology(title="fep_solute", rexcl_o=radius, rwat=radius, types=types, vdw_rule=vdw_rule,
-                   water_h_lj=tuple(water_h_lj), solvent_type=solvent_type)
+                   water_h_lj=tuple(water_h_lj), solvent_type=solvent_type, switch_atoms=switch_atoms)
     top.x = [tuple(float(c) for c in p) for p in X]
     top.iac = iac
     top.crg = _solute_charges(rng, kinds)
@@ -774,11 +775,88 @@ def fep_solute(outdir: str, radius: float = 20.0, seed: int = 1234, steps: int =
     return Generated(inp, tp, fp, len(top.x), len(waters))
 
 
+def _relax_chains(X: np.ndarray, n_fixed: int, chains, radius: float, target: float = 3.0, iters: int = 400,
+                  bond: float = 1.5) -> np.ndarray:
+    """Spread a grown set of chains apart before the system is written: atoms
+    of non-bonded pairs (not 1-2 or 1-3 along a chain) closer than `target`
+    are pushed apart, chain bonds kept at `bond`, chain angles kept within
+    100-150 degrees (1-3 distances), every atom within radius - 0.5; the first
+    n_fixed atoms (the ligand) do not move.  A random walk packed at 2.5 A
+    starts with thousands of kcal/mol of steric strain, which 2 fs dynamics
+    turns into heat and the polymer cannot survive; relaxed, it can."""
+    from scipy.spatial import cKDTree
+    X = X.copy()
+    n = len(X)
+    cid = np.full(n, -1)
+    pos = np.zeros(n, dtype=int)
+    for c, ch in enumerate(chains):
+        cid[ch] = c
+        pos[ch] = np.arange(len(ch))
+    b = np.array([(a, b) for ch in chains for a, b in zip(ch[:-1], ch[1:])], dtype=int).reshape(-1, 2)
+    a13 = np.array([(a, c) for ch in chains for a, c in zip(ch[:-2], ch[2:])], dtype=int).reshape(-1, 2)
+    lo13, hi13 = 2 * bond * np.sin(np.radians(50.0)), 2 * bond * np.sin(np.radians(75.0))
+    mobile = np.ones(n, dtype=bool)
+    mobile[:n_fixed] = False
+    for _ in range(iters):
+        pr = cKDTree(X).query_pairs(target, output_type="ndarray")
+        if len(pr):
+            i, j = pr[:, 0], pr[:, 1]
+            near = (cid[i] == cid[j]) & (cid[i] >= 0) & (np.abs(pos[i] - pos[j]) <= 2)
+            i, j = i[~near], j[~near]
+            d = X[j] - X[i]
+            r = np.linalg.norm(d, axis=1)[:, None]
+            push = 0.25 * (target - r) / np.maximum(r, 1e-6) * d
+            disp = np.zeros_like(X)
+            np.add.at(disp, i, -push)
+            np.add.at(disp, j, push)
+            disp[~mobile] = 0.0
+            step = np.linalg.norm(disp, axis=1)[:, None]
+            X += disp * np.minimum(1.0, 0.2 / np.maximum(step, 1e-12))
+        for pairs, lo, hi in ((b, bond, bond), (a13, lo13, hi13)):
+            for half in (0, 1):            # alternate pairs: no atom moved twice per pass
+                p = pairs[half::2] if len(pairs) else pairs
+                if not len(p):
+                    continue
+                d = X[p[:, 1]] - X[p[:, 0]]
+                r = np.linalg.norm(d, axis=1)
+                goal = np.clip(r, lo, hi)
+                corr = ((r - goal) / np.maximum(r, 1e-9))[:, None] * d
+                w0 = mobile[p[:, 0]].astype(float)
+                w1 = mobile[p[:, 1]].astype(float)
+                tot = np.maximum(w0 + w1, 1.0)[:, None]
+                X[p[:, 0]] += corr * (w0[:, None] / tot)
+                X[p[:, 1]] -= corr * (w1[:, None] / tot)
+        rr = np.linalg.norm(X, axis=1)
+        out = (rr > radius - 0.5) & mobile
+        X[out] *= ((radius - 0.5) / rr[out])[:, None]
+    return X
+
+
 def polymer_sphere(outdir: str, radius: float = 25.0, seed: int = 1234, steps: int = 5000, name: str = "c2",
-                   n_polymer: int = 3000, restrain_beyond: float = 23.0, lambdas=(0.5, 0.5)) -> Generated:
+                   n_polymer: int = 3000, restrain_beyond: float = 23.0, lambdas=(0.5, 0.5),
+                   min_dist: float = 2.5, charge_sd: float = 0.3, max_angle: float = 150.0,
+                   angle_fk: float = 60.0, shell_radius: float | None = None, relax: bool = True,
+                   switch_atoms: int = 0) -> Generated:
     """Config 2: 3000-atom polymer walk around the config-1 solute (ligand) in
     a 25 A sphere; atoms beyond 23 A are excluded and restrained; waters fill
-    the remaining volume."""
+    the remaining volume.
+
+    The chains are spread apart after growth (_relax_chains) and each torsion's
+    phase puts the starting dihedral at its minimum, so the start carries little
+    strain.  The charge groups are residue-like runs of 10-15 chain atoms, which
+    a random walk stretches over up to ~10 A; with switch-atom cut-offs two
+    groups whose switch atoms lie beyond 10 A leave their closest atoms without
+    any non-bonded interaction, and chains then pass through each other and the
+    dynamics fails within ~100 steps.  The topology therefore asks for the
+    any-atom cut-offs (switch_atoms 0: nbpplis2_lrf, nbpwlis2_lrf, nbqplis2),
+    under which the system is stable.
+
+    Waters: 3,000 atoms at >= 2.5 A non-bonded spacing fill most of the sphere
+    (random close packing of 2.5 A spheres is ~0.078 A^-3, i.e. >= 39,000 of the
+    sphere's 65,450 A^3), and the walk spreads them over all of it, so the
+    waters that fit (O >= 2.6 A from every solute atom) number ~200, not the
+    ~1,500 the configuration's prose expects; 1,500 waters alone need 44,900
+    A^3 at 0.0334 A^-3."""
     os.makedirs(outdir, exist_ok=True)
     rng = np.random.default_rng(seed)
     Xl, kinds, lbonds = random_tree_solute(rng)
@@ -786,7 +864,7 @@ def polymer_sphere(outdir: str, radius: float = 25.0, seed: int = 1234, steps: i
     # self-avoiding chains, restarted where a chain gets stuck
     pts = [p for p in Xl]
     chains = []
-    cell = 2.5
+    cell = max(2.5, min_dist)
 
     grid: dict = {}
 
@@ -807,7 +885,7 @@ def polymer_sphere(outdir: str, radius: float = 25.0, seed: int = 1234, steps: i
             for dy in (-1, 0, 1):
                 for dz in (-1, 0, 1):
                     for q in grid.get((kx + dx, ky + dy, kz + dz), ()):
-                        if q != skip and np.linalg.norm(pts[q] - p) < 2.5:
+                        if q != skip and np.linalg.norm(pts[q] - p) < min_dist:
                             return False
         return True
 
@@ -827,8 +905,8 @@ def polymer_sphere(outdir: str, radius: float = 25.0, seed: int = 1234, steps: i
                 u = rng.normal(size=3)
                 u /= np.linalg.norm(u)
                 c = pts[chain[-1]] + 1.5 * u
-                # chain angles 100-150 degrees (no near-linear angle terms)
-                if len(chain) > 1 and not 100 <= _angle(pts[chain[-2]], pts[chain[-1]], c) <= 150:
+                # chain angles within [100, max_angle] degrees (no near-linear angle terms)
+                if len(chain) > 1 and not 100 <= _angle(pts[chain[-2]], pts[chain[-1]], c) <= max_angle:
                     continue
                 if free(c, chain[-1]):
                     ok = True
@@ -842,10 +920,13 @@ def polymer_sphere(outdir: str, radius: float = 25.0, seed: int = 1234, steps: i
         chains.append(chain)
     n_lig = len(Xl)
     X = np.array(pts)
+    if relax:
+        X = _relax_chains(X, n_lig, chains, radius)
     n = len(X)
     types, _ = _tree_types(kinds)
     iac = [0 if k < 0 else k + 1 for k in kinds] + [1 + int(rng.integers(len(TYPE_TABLE))) for _ in range(n - n_lig)]
-    top = Topology(title="polymer_sphere", rexcl_o=restrain_beyond, rwat=radius, types=types)
+    top = Topology(title="polymer_sphere", rexcl_o=restrain_beyond, rwat=radius, types=types,
+                   switch_atoms=switch_atoms)
     top.x = [tuple(float(c) for c in p) for p in X]
     top.iac = iac
     crg = _solute_charges(rng, kinds)
@@ -861,7 +942,7 @@ def polymer_sphere(outdir: str, radius: float = 25.0, seed: int = 1234, steps: i
     pcrg = np.zeros(n)
     for g in groups:
         net = float(rng.choice([-1.0, 0.0, 1.0]))
-        pcrg[g] = _net_zero_charges(rng, len(g), sd=0.3, total=net)
+        pcrg[g] = _net_zero_charges(rng, len(g), sd=charge_sd, total=net)
     top.crg = crg + [float(v) for v in pcrg[n_lig:]]
     _solute_terms(top, Xl, lbonds, rng)
     # polymer terms (harmonic bonds/angles, torsions along the chains)
@@ -874,11 +955,16 @@ def polymer_sphere(outdir: str, radius: float = 25.0, seed: int = 1234, steps: i
         top.bonds.append((i, j, len(top.bond_lib)))
     for ch in chains:
         for a, b, c in zip(ch[:-2], ch[1:-1], ch[2:]):
-            top.angle_lib.append((60.0, round(_angle(X[a], X[b], X[c]), 3)))
+            top.angle_lib.append((angle_fk, round(_angle(X[a], X[b], X[c]), 3)))
             top.angles.append((a, b, c, len(top.angle_lib)))
         for a, b, c, d in zip(ch[:-3], ch[1:-2], ch[2:-1], ch[3:]):
-            top.tor_lib.append((round(float(rng.uniform(0.2, 1.5)), 3), float(rng.integers(1, 4)),
-                                float(rng.choice([0.0, 180.0])), 1))
+            fk, mult = round(float(rng.uniform(0.2, 1.5)), 3), float(rng.integers(1, 4))
+            if relax:
+                # the phase that puts the starting dihedral at the term's minimum
+                phase = round(float((mult * dihedral_deg(X[a], X[b], X[c], X[d]) - 180.0) % 360.0), 2)
+            else:
+                phase = float(rng.choice([0.0, 180.0]))
+            top.tor_lib.append((fk, mult, phase, 1))
             top.tors.append((a, b, c, d, len(top.tor_lib)))
     top.nat_solute = n
     top.nbonds_solute, top.nangles_solute = len(top.bonds), len(top.angles)
@@ -907,7 +993,7 @@ def polymer_sphere(outdir: str, radius: float = 25.0, seed: int = 1234, steps: i
     _fep_file(fp, types, iac, top.crg, heavy[:8])
     inp = os.path.join(outdir, name + ".inp")
     write_inp(inp, tp, fp, steps=steps, stepsize=2.0, seed=1, lambdas=lambdas, shake_hydrogens=True,
-              q_cutoff=99.0, shell_radius=restrain_beyond - 0.01)
+              q_cutoff=99.0, shell_radius=shell_radius if shell_radius is not None else restrain_beyond - 0.01)
     return Generated(inp, tp, fp, len(top.x), len(waters))
 
 

@@ -145,3 +145,42 @@ def test_length_spacing_and_features():
     assert np.allclose(L.KT * np.exp(f[0:5] + 3 * f[10]), [np.std(d) for d in dU])
     pu = L.pilot_spacing(f)
     assert np.all(np.diff(pu) > 0) and np.diff(pu)[0] < np.diff(pu)[-1]   # denser where sigma is large
+
+
+def test_reference_python_estimators_on_constant_windows():
+    """The reference's own Python estimators (src/Qgpu/calc.py, run unchanged
+    by tests/golden/make_qfep_golden.py) against the qfep restatement.  They
+    are not qfep: they pair record ipt with record ipt + 1 of one series,
+    divide by the record count instead of the pairs used, take exp(-dv) in
+    both halves of overlap sampling, and define BAR's dv as V(l1) - V(l2).
+    On windows whose every record is the same, those differences reduce to
+    exact identities, checked here: Zwanzig forward and reverse differ from
+    qfep's by -kT ln((n - 1)/n), BAR is qfep's with the opposite sign, and
+    overlap sampling is 0 where qfep's is the energy difference.  On other
+    series the two differ by design (the golden file holds such cases, which
+    are not compared)."""
+    import json
+    import os
+    d = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "qgpu_calc_estimators.json")))
+    ncmp = 0
+    for c in d["cases"]:
+        if not c["constant"]:
+            continue
+        kT, l1, l2 = c["kT"], np.array(c["l1"]), np.array(c["l2"])
+        row = np.array(c["series"][0])
+        n = len(c["series"])
+        files = []
+        for lam in (l1, l2):
+            e = np.zeros((n, 2, 15))
+            e[:, :, 0] = lam
+            e[:, :, 1] = row
+            files.append(e)
+        r = analyze(FepInput(files, kT, 0, nbins=4, nmin=1, alfa=[0.0], coeff=[1.0, -1.0]))
+        shift = -kT * math.log((n - 1) / n)
+        assert abs(c["EXPfwd"] - (r.dgf[1] + shift)) < 1e-10
+        assert abs(c["EXPbwd"] - (r.dgr[2] + shift)) < 1e-10
+        assert abs(c["BAR"] + r.dgbar[1]) < 2e-3          # both iterate to |change| <= 0.001
+        assert c["overlap_sampling"] == 0.0
+        assert abs(r.dglu[1] - float((l2 - l1) @ row)) < 1e-10
+        ncmp += 1
+    assert ncmp == 4

@@ -109,3 +109,66 @@ def test_p_restrain_terms_match_oracle(tmp_path, oracle):
         Eo, EQo = o.energy_vectors()
         assert_energies(Eg, EQg, Eo, EQo)
         assert grad_err(b.gradient(k), o.gradient()) < G_TOL
+
+
+def test_any_atom_cutoffs_match_oracle(tmp_path, oracle):
+    """Charge-group cut-offs on any atom pair (iuse_switch_atom 0 in the
+    topology): nbpplis2_lrf, nbpwlis2_lrf and nbqplis2 (md.f90:4926, 6477,
+    7664) and the LRF windows they imply, on the FEP solute in water.  Two
+    lambda windows over 50 steps (two list rebuilds) against the oracle; the
+    mixed-precision engine at one point.  The lists differ from the
+    switch-atom ones on this system, so the test separates the two modes."""
+    from q_b200 import synth
+    g = synth.fep_solute(str(tmp_path / "c1"), seed=1234, switch_atoms=0)
+    systems = [System.open(g.inp, lambdas=lam, seed=5) for lam in ((0.5, 0.5), (0.9, 0.1))]
+    assert systems[0].view.iuse_switch_atom == 0
+    b = Batch(systems, precision=FP64)
+    b.run(50)
+    runs = []
+    for k, s in enumerate(systems):
+        o = oracle.create(s)
+        o.run(50)
+        runs.append(o)
+        for kind in (0, 1):
+            sg, Eg, EQg = b.history(k, kind)
+            so, Eo, EQo = o.history(kind)
+            assert list(sg) == list(so)
+            for r in range(len(sg)):
+                assert_energies(Eg[r], EQg[r], Eo[r], EQo[r])
+    b.final_energy()
+    for k, o in enumerate(runs):
+        o.final_energy()
+        Eg, EQg = b.energy_vectors(k)
+        Eo, EQo = o.energy_vectors()
+        assert_energies(Eg, EQg, Eo, EQo)
+        assert grad_err(b.gradient(k), o.gradient()) < G_TOL
+    # the switch-atom lists of the same coordinates are different
+    w_any = b.workload()
+    g1 = synth.fep_solute(str(tmp_path / "c1s"), seed=1234, switch_atoms=1)
+    b1 = Batch([System.open(g1.inp, lambdas=(0.5, 0.5), seed=5)], precision=FP64)
+    b1.run(1)
+    b0 = Batch([System.open(g.inp, lambdas=(0.5, 0.5), seed=5)], precision=FP64)
+    b0.run(1)
+    assert b0.workload()[1] != b1.workload()[1]
+    # mixed precision on the any-atom lists
+    s = System.open(g.inp, lambdas=(0.5, 0.5), seed=5)
+    bm = Batch([s], precision=MIXED)
+    bm.evaluate(energies=True)
+    o = oracle.create(s)
+    o.final_energy()
+    Eg, EQg = bm.energy_vectors(0)
+    Eo, EQo = o.energy_vectors()
+    assert_energies(Eg, EQg, Eo, EQo)
+    bm.evaluate(energies=False)
+    assert grad_err(bm.gradient(0), o.gradient()) < G_TOL
+
+
+def test_c2_runs_its_list_cycles(c2):
+    """The protein-ligand sphere runs stably under the engine: 300 mixed-
+    precision steps (twelve list rebuilds) without a SHAKE failure or a
+    non-finite energy, the temperature settling below 700 K."""
+    s = System.open(c2.inp, seed=11)
+    b = Batch([s], precision=MIXED)
+    b.run(300)
+    assert b.status(0) == 0
+    assert b.temperature(0)[0] < 700.0

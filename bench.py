@@ -70,13 +70,16 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-configs", action="store_true", help="skip the single-system lines of the plain configs")
     p.add_argument("--no-autotune", action="store_true", help="keep the default tile sizes and streams")
-    p.add_argument("--dg-replicas", type=int, default=16,
+    p.add_argument("--dg-replicas", type=int, default=32,
                    help="replicas of the batched mixed-precision perturbation for the GPU-s per dG comparison "
                         "(0 skips it; runs at one GPU only)")
-    p.add_argument("--dg-ref-replicas", type=int, default=16, help="replicas of the dense FP64 reference")
+    p.add_argument("--dg-ref-replicas", type=int, default=32, help="replicas of the dense FP64 reference")
     p.add_argument("--dg-ref-windows", type=int, default=41)
     p.add_argument("--dg-equil", type=int, default=1000)
     p.add_argument("--dg-steps", type=int, default=10000, help="production steps per window")
+    p.add_argument("--dg-placement", default="learned", choices=["learned", "uniform"],
+                   help="learned: the 5-window pilot and the trained network place the product's windows "
+                        "(q_b200/data/placement_model.npz); uniform: --windows uniform windows")
     return p.parse_args()
 
 
@@ -555,16 +558,21 @@ def main():
         # precision against the plain FP64 engine one system per launch,
         # the dG error judged by a dense-window FP64 run
         from q_b200.campaign import dg_versus_plain
+        placement = None
+        if args.dg_placement == "learned":
+            from q_b200.lambda_placement import Placement
+            placement = Placement.load(os.path.join(REPO, "q_b200", "data", "placement_model.npz"))
         t0 = time.perf_counter()
         dg = dg_versus_plain(specs[0][0], windows=args.windows, replicas=args.dg_replicas,
                              ref_windows=args.dg_ref_windows, ref_replicas=args.dg_ref_replicas,
-                             steps_eq=args.dg_equil, steps_prod=args.dg_steps, device=local)
+                             steps_eq=args.dg_equil, steps_prod=args.dg_steps, device=local, placement=placement)
         dg["wall_s"] = round(time.perf_counter() - t0, 1)
         line["dG"] = dg
         line["gpu_s_per_dG"] = {"batched_mixed": dg["batched_mixed"]["gpu_seconds"],
                                 "plain_fp64": dg["plain_fp64_one_system_per_launch"]["gpu_seconds"],
                                 "ratio": dg["gpu_seconds_ratio_plain_over_batched"],
-                                "dG_error_vs_fp64_dense": dg["dG_error"], "dG_error_sem": dg["dG_error_sem"]}
+                                "dG_error_vs_fp64_dense": dg["dG_error"], "dG_error_sem": dg["dG_error_sem"],
+                                "placement": dg["perturbation"]["placement"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

@@ -43,6 +43,15 @@ int qb_mlp_loss_grad(const float *params, const float *x, const float *t, int n,
 int qb_mlp_train(float *params, const float *x, const float *t, int n, int iters, const qb_mlp_adam *adam,
                  float *loss_history, int device);
 
+/* Polls each tensor-core completion wait of the network kernel makes before it
+ * gives up (process-wide; the default, 2^26, is seconds).  A wait that gives up
+ * makes the call return QB_ERR_TIMEOUT after the kernel has drained its
+ * in-flight tensor-core work and released its tensor memory, so the context
+ * stays usable.  0 makes every wait give up at once, which is how the time-out
+ * path is tested; pass 67108864 to restore the default. */
+#define QB_MLP_DEFAULT_WAIT_LIMIT 67108864LL
+int qb_mlp_set_wait_limit(long long polls);
+
 #ifdef __cplusplus
 }
 #endif

@@ -152,6 +152,7 @@ def _load():
         "qb_mlp_forward": (C.c_int, [fp, fp, C.c_int, fp, C.c_int]),
         "qb_mlp_loss_grad": (C.c_int, [fp, fp, fp, C.c_int, fp, fp, C.c_int]),
         "qb_mlp_train": (C.c_int, [fp, fp, fp, C.c_int, C.c_int, C.c_void_p, fp, C.c_int]),
+        "qb_mlp_set_wait_limit": (C.c_int, [C.c_longlong]),
         "qb_maxwell": (C.c_int, [C.c_int, C.c_double, C.c_int, dp, dp]),
         "qb_ww_energy_static": (C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_double, C.c_double,
                                           C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -219,26 +219,128 @@ def equilibrate(inp: str, seeds, stages=QLIGFEP_EQ_2FS, *, lambdas=None, steps_s
 
 def dg_versus_plain(inp: str, *, windows: int = 21, replicas: int = 16, ref_windows: int = 41,
                     ref_replicas: int = 16, steps_eq: int = 1000, steps_prod: int = 10000, plain_steps: int = 1000,
-                    rt: float = 0.592, device: int = 0, seed0: int = 1) -> dict:
-    """The batched mixed-precision perturbation (uniform windows) against the
-    dense-window FP64 reference and the plain FP64 one-system-per-launch
-    engine; all times are device seconds on this GPU."""
+                    rt: float = 0.592, device: int = 0, seed0: int = 1, placement=None) -> dict:
+    """The batched mixed-precision perturbation against the dense-window FP64
+    reference and the plain FP64 one-system-per-launch engine; all times are
+    device seconds on this GPU.
+
+    Without a placement model the product runs `windows` uniform windows.
+    With one (lambda_placement.Placement) it runs the 5-window pilot (its
+    device time counted), asks the network for the windows, and runs those.
+    The plain engine runs the conventional protocol either way: `windows`
+    uniform windows x the same replicas and steps, one system per launch (its
+    per-step time measured here, times the system-steps)."""
     from .synth import window_lambdas
-    prod = run_perturbation(inp, window_lambdas(windows), replicas, steps_eq=steps_eq, steps_prod=steps_prod,
+    pilot_s, placed = 0.0, None
+    lams = window_lambdas(windows)
+    if placement is not None:
+        from . import lambda_placement as L
+        pilot = L.sample([(inp, np.array(L.PILOT_U))], replicas=1, steps_eq=500, steps_prod=2000, device=device,
+                         seed0=seed0 + 20000, bar=False)[0]
+        pilot_s = pilot.gpu_seconds
+        placed = placement.predict(L.pilot_features(pilot.dU[0]), device)[0]
+        lams = L.windows_of(placed)
+    prod = run_perturbation(inp, lams, replicas, steps_eq=steps_eq, steps_prod=steps_prod,
                             precision=MIXED, device=device, rt=rt, seed0=seed0)
     ref = run_perturbation(inp, window_lambdas(ref_windows), ref_replicas, steps_eq=steps_eq, steps_prod=steps_prod,
                            precision=FP64, device=device, rt=rt, seed0=seed0 + 10000)
     plain_step = time_single_window(inp, (0.5, 0.5), plain_steps, precision=FP64, device=device)
     system_steps = windows * replicas * (steps_eq + steps_prod)
     plain_s = plain_step * system_steps
+    prod_s = prod.gpu_seconds + pilot_s
     diff = prod.dG_mean - ref.dG_mean
     diff_sem = float(np.hypot(prod.dG_sem, ref.dG_sem))
     return {
-        "perturbation": {"windows": windows, "replicas": replicas, "steps_eq": steps_eq, "steps_prod": steps_prod},
+        "perturbation": {"windows": len(lams), "replicas": replicas, "steps_eq": steps_eq, "steps_prod": steps_prod,
+                         "placement": "learned (5-window pilot + network)" if placement is not None else "uniform",
+                         "lambda_2": [float(u) for u in (placed if placed is not None else
+                                                         np.linspace(0.0, 1.0, windows))]},
         "batched_mixed": {k: v for k, v in asdict(prod).items() if k != "bar"},
+        "pilot_gpu_seconds": pilot_s,
         "reference_fp64_dense": {k: v for k, v in asdict(ref).items() if k != "bar"},
-        "plain_fp64_one_system_per_launch": {"s_per_step": plain_step, "system_steps": system_steps,
-                                             "gpu_seconds": plain_s},
+        "plain_fp64_one_system_per_launch": {"windows": windows, "s_per_step": plain_step,
+                                             "system_steps": system_steps, "gpu_seconds": plain_s},
         "dG_error": diff, "dG_error_sem": diff_sem, "within_0.1": bool(abs(diff) <= 0.1),
-        "gpu_seconds_ratio_plain_over_batched": plain_s / prod.gpu_seconds,
+        "within_0.1_at_2_sem": bool(abs(diff) + 2.0 * diff_sem <= 0.1),
+        "gpu_seconds_ratio_plain_over_batched": plain_s / prod_s,
     }
+
+
+def dg_study(inp: str, *, replicas: int = 512, ref_replicas: int = 256, windows: int = 21, ref_windows: int = 41,
+             steps_eq: int = 1000, steps_prod: int = 10000, device: int = 0, placement=None,
+             max_systems: int = 4096) -> dict:
+    """One dense FP64 reference judging two products of the same perturbation:
+    the learned placement (pilot + network windows) and `windows` uniform
+    windows, each batched in mixed precision with `replicas` replicas (split
+    into batches of at most max_systems systems; device seconds summed).  With
+    these replica counts the standard error of each product's error falls to
+    ~0.05 kcal/mol.  Also the plain FP64 engine's device seconds for the
+    uniform protocol one system per launch."""
+    from .synth import window_lambdas
+
+    def run(lams, reps, precision, seed0):
+        per = max(1, max_systems // len(lams))
+        dgs, gpu = [], 0.0
+        for first in range(0, reps, per):
+            n = min(per, reps - first)
+            r = run_perturbation(inp, lams, n, steps_eq=steps_eq, steps_prod=steps_prod, precision=precision,
+                                 device=device, seed0=seed0 + first)
+            dgs += r.dG
+            gpu += r.gpu_seconds
+        return {"dG_mean": float(np.mean(dgs)), "dG_sem": float(np.std(dgs, ddof=1) / np.sqrt(len(dgs))),
+                "gpu_seconds": gpu, "replicas": reps, "windows": len(lams)}
+
+    ref = run(window_lambdas(ref_windows), ref_replicas, FP64, 100001)
+    out = {"reference_fp64_dense": ref, "products": {}}
+    pilot_s = 0.0
+    if placement is not None:
+        from . import lambda_placement as L
+        pilot = L.sample([(inp, np.array(L.PILOT_U))], replicas=1, steps_eq=500, steps_prod=2000, device=device,
+                         seed0=200001, bar=False)[0]
+        pilot_s = pilot.gpu_seconds
+        u = placement.predict(L.pilot_features(pilot.dU[0]), device)[0]
+        p = run(L.windows_of(u), replicas, MIXED, 1)
+        p["gpu_seconds"] += pilot_s
+        p["lambda_2"] = [float(x) for x in u]
+        out["products"]["learned"] = p
+    out["products"]["uniform_%d" % windows] = run(window_lambdas(windows), replicas, MIXED, 1)
+    plain_step = time_single_window(inp, (0.5, 0.5), 1000, precision=FP64, device=device)
+    plain_s = plain_step * windows * replicas * (steps_eq + steps_prod)
+    out["plain_fp64_one_system_per_launch"] = {"windows": windows, "s_per_step": plain_step, "gpu_seconds": plain_s}
+    for name, p in out["products"].items():
+        p["dG_error"] = p["dG_mean"] - ref["dG_mean"]
+        p["dG_error_sem"] = float(np.hypot(p["dG_sem"], ref["dG_sem"]))
+        p["within_0.1"] = bool(abs(p["dG_error"]) <= 0.1)
+        p["gpu_seconds_ratio_plain_over_product"] = plain_s / p["gpu_seconds"]
+    return out
+
+
+def main(argv=None) -> int:
+    """python -m q_b200.campaign dg-study <dir> [--replicas R] [--ref-replicas R]
+    [--placement model.npz]: the perturbation of the synthetic FEP solute
+    (its 8 Q atoms from state 1 to state 2), as the bench's dG check but at
+    replica counts that bring the error's standard error near 0.05 kcal/mol."""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser()
+    ap.add_argument("command", choices=["dg-study"])
+    ap.add_argument("root")
+    ap.add_argument("--replicas", type=int, default=512)
+    ap.add_argument("--ref-replicas", type=int, default=256)
+    ap.add_argument("--steps", type=int, default=10000)
+    ap.add_argument("--placement", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "data",
+                                                         "placement_model.npz"))
+    a = ap.parse_args(argv)
+    from . import synth
+    from .lambda_placement import Placement
+    g = synth.fep_solute(os.path.join(a.root, "c1"), seed=1234, steps=a.steps)
+    model = Placement.load(a.placement) if a.placement else None
+    t0 = time.perf_counter()
+    r = dg_study(g.inp, replicas=a.replicas, ref_replicas=a.ref_replicas, steps_prod=a.steps, placement=model)
+    r["wall_s"] = time.perf_counter() - t0
+    print(json.dumps(r, indent=1))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -84,6 +84,8 @@ struct Batch {
   int NB = 1;
   long long istep = 0;
   int max_natom = 0, max_lrf_blocks = 1, max_nsol = 0, max_nwat = 0, max_ncgp = 0, max_ncgp_sol = 0, max_terms = 0, max_pp = 0, max_ncgp_sol_w = 0, max_qp = 0;
+  bool any_any_atom = false;   // a system with any-atom charge-group cut-offs (iuse_switch_atom 0)
+  int ww_wpb = WW_WPB;          // waters per block of the water-water kernels
   bool any_lrf = false, any_q = false, any_shake = false, any_wpol = false, any_prestr = false, any_qq = false,
        any_qb = false, any_hlj = false;
   // run-time choices the autotuner sets (qb_tuning): LRF source tiles per
@@ -184,9 +186,12 @@ struct Batch {
     // side 1: water-water list
     cudaStream_t s1 = forking() ? side[0] : stream, s2 = forking() ? side[1] : stream;
     launch("lists_begin", [&] { k_lists_begin<<<cdiv(nsys, 128), 128, 0, stream>>>(p, force); });
+    // group centres and radii first: the LRF gather and the any-atom list
+    // tests read them
+    if (any_lrf || any_any_atom)
+      launch("cgp_centers", [&] { k_cgp_centers<<<cdiv(p.ncgp_tot, 256), b256, 0, stream>>>(p, force); });
     fork_streams();
     if (any_lrf) {
-      launch("cgp_centers", [&] { k_cgp_centers<<<cdiv(p.ncgp_tot, 256), b256, 0, s1>>>(p, force); });
       launch("lrf_gather", [&] {
         if (opt.precision == QB_MIXED)
           k_lrf_gather_x2<<<dim3(max_lrfx_blocks, nsys), LRFX_BLOCK, 0, s1>>>(p, force);
@@ -312,17 +317,18 @@ struct Batch {
     if (max_ncgp_sol_w > 0)
       launch("nb_pw", [&] { k_nb_pw<<<dim3(cdiv(p.pwg_cap, PW_BLOCK), max_ncgp_sol_w, nsys), PW_BLOCK, 0, s1>>>(p); });
     if (max_nwat > 0) {
-      dim3 gw(cdiv(max_nwat, WW_WPB), nsys);
+      dim3 gw(cdiv(max_nwat, ww_wpb), nsys);
+      const int wpb = ww_wpb;
       size_t smem = (size_t)p.ww_chunk * (fast_ww ? WatRec<true>::words : WatRec<false>::words) * sizeof(float4);
       // hydrogen LJ: the whole batch takes the variant (exact zeros for systems without)
       if (fast_ww && any_hlj) {
-        launch("nb_ww", [&] { k_nb_ww<true, true><<<gw, WW_BLOCK, smem, stream>>>(p); });
+        launch("nb_ww", [&] { k_nb_ww<true, true><<<gw, WW_BLOCK, smem, stream>>>(p, wpb); });
       } else if (fast_ww) {
-        launch("nb_ww_x2", [&] { k_nb_ww_x2<<<gw, WWX_BLOCK, smem, stream>>>(p); });
+        launch("nb_ww_x2", [&] { k_nb_ww_x2<<<gw, WWX_BLOCK, smem, stream>>>(p, wpb); });
       } else if (any_hlj) {
-        launch("nb_ww", [&] { k_nb_ww<false, true><<<gw, WW_BLOCK, smem, stream>>>(p); });
+        launch("nb_ww", [&] { k_nb_ww<false, true><<<gw, WW_BLOCK, smem, stream>>>(p, wpb); });
       } else {
-        launch("nb_ww", [&] { k_nb_ww<false, false><<<gw, WW_BLOCK, smem, stream>>>(p); });
+        launch("nb_ww", [&] { k_nb_ww<false, false><<<gw, WW_BLOCK, smem, stream>>>(p, wpb); });
       }
       if (any_q) launch("nb_qw", [&] {
         dim3 g(cdiv(max_nwat, 128), nsys);
@@ -716,6 +722,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     }
     // scalars
     S.switch_atoms = V.iuse_switch_atom == 1 ? 1 : 0;
+    if (!S.switch_atoms) B.any_any_atom = true;
     S.ff_type = V.ff_type; S.use_lrf = V.use_LRF; S.qvdw = V.qvdw_flag; S.qq_lib = V.qq_use_library_charges;
     S.wpol = V.wpol_restr && V.nwpolr_shell > 0; S.nshell = V.nwpolr_shell;
     if (S.nshell > MAX_SHELLS) fail(QB_ERR_UNSUPPORTED, "too many water polarisation shells");
@@ -963,12 +970,28 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   const int rec_words = B.opt.precision == QB_MIXED ? WatRec<true>::words : WatRec<false>::words;
   const int chunk_max = WW_STAGE_BYTES / (16 * rec_words) / 32 * 32;
   P.ww_chunk = std::max(std::min((B.max_nwat + 31) / 32 * 32, chunk_max), 32);
+  // waters per block: fewer when the batch is too small to give every SM two
+  // blocks (a single system of ~1000 waters: 33 blocks of 32 instead of 9)
+  {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, B.opt.device);
+    B.ww_wpb = WW_WPB;
+    while (B.ww_wpb > 32 && (long long)n * Batch::cdiv(B.max_nwat, B.ww_wpb) < 2LL * sms) B.ww_wpb /= 2;
+  }
   // the split counts are sized for the smallest chunk a tuning may choose
   B.ww_chunk_max = P.ww_chunk;
   B.ww_chunk_floor = std::max(32, std::min(P.ww_chunk, 256));
   const int nch_alloc = (std::max(B.max_nwat, 1) + B.ww_chunk_floor - 1) / B.ww_chunk_floor;
   P.ww_nch = (std::max(B.max_nwat, 1) + P.ww_chunk - 1) / P.ww_chunk;
-  B.set_lrf_tpb(LRF_TILES_PER_BLOCK);
+  // source tiles per LRF block: fewer (more blocks) when the batch is too
+  // small to fill the SMs twice over
+  {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, B.opt.device);
+    int tpb = LRF_TILES_PER_BLOCK;
+    B.set_lrf_tpb(tpb);
+    while (tpb > 1 && (long long)B.max_lrf_blocks * n < 2LL * sms) B.set_lrf_tpb(tpb /= 2);
+  }
   P.ww_cap = ww_cap;
   P.ww = dev_alloc<uint16_t>((size_t)std::max(woff, 1) * ww_cap, o);
   P.ww_n = dev_alloc<int>(std::max(woff, 1), o);

@@ -113,6 +113,30 @@ __device__ __forceinline__ bool group_point_inside_any(const DevPtrs &P, int gi,
   return false;
 }
 
+// Bounds from the groups' centres and radii (the LRF records, written by
+// k_cgp_centers before the list kernels): -1 when no atom pair can be within
+// the cut-off, +1 when every atom pair is, 0 when only the atoms can tell.  The
+// margin keeps pairs near the cut-off for the exact FP64 atom test.
+__device__ __forceinline__ int groups_reach(const DevPtrs &P, int gi, int gj, double rc2) {
+  const double *Li = P.lrf + (size_t)gi * LRF_STRIDE, *Lj = P.lrf + (size_t)gj * LRF_STRIDE;
+  const double dx = Li[0] - Lj[0], dy = Li[1] - Lj[1], dz = Li[2] - Lj[2];
+  const double dc = sqrt(dx * dx + dy * dy + dz * dz), rr = Li[LRF_STRIDE - 1] + Lj[LRF_STRIDE - 1];
+  const double rc = sqrt(rc2);
+  if (dc - rr > rc + 1e-6) return -1;
+  if (dc + rr < rc - 1e-6) return 1;
+  return 0;
+}
+
+__device__ __forceinline__ int group_point_reach(const DevPtrs &P, int gi, double3 p, double rc2) {
+  const double *Li = P.lrf + (size_t)gi * LRF_STRIDE;
+  const double dx = Li[0] - p.x, dy = Li[1] - p.y, dz = Li[2] - p.z;
+  const double dc = sqrt(dx * dx + dy * dy + dz * dz), rr = Li[LRF_STRIDE - 1];
+  const double rc = sqrt(rc2);
+  if (dc - rr > rc + 1e-6) return -1;
+  if (dc + rr < rc - 1e-6) return 1;
+  return 0;
+}
+
 // Near/far test of an LRF gather pair (target group g, source group h) under
 // iuse_switch_atom 0, when one of them is a solute group: true when the pair
 // takes part in the LRF (outside the any-atom cut-off, last pair within
@@ -162,6 +186,7 @@ __device__ __forceinline__ float rsqrt_ftz(float v) {
 }
 
 __device__ __forceinline__ float rsq(float v) { return rsqrt_ftz(v); }
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ double rsq(double v) { return rsqrt(v); }
 
 template <class R>
@@ -538,11 +563,18 @@ __global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int 
       if (!any) continue;
       const int2 rg = hrange[i];
       const float2 unsel = make_float2(1.f - sel.x, 1.f - sel.y);
-      for (int k = 0; k < rg.y; k++) {
+      auto atom = [&](int k) {
         const float4 a = hxy[rg.x + k], b = hzq[rg.x + k];
         const float2 q = __fmul2_rn(make_float2(b.z, b.w), sel);
         lrf_accumulate_x2(m, t, q, __fadd2_rn(make_float2(a.x, a.y), ncx), __fadd2_rn(make_float2(a.z, a.w), ncy),
                           __fadd2_rn(make_float2(b.x, b.y), ncz), sel, unsel);
+      };
+      if (rg.y == 3) {        // a water: its three atoms as independent chains
+        atom(0);
+        atom(1);
+        atom(2);
+      } else {
+        for (int k = 0; k < rg.y; k++) atom(k);
       }
     }
   }
@@ -566,8 +598,14 @@ __global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int 
 // force kernel finds each chunk's slice of the list directly.
 // Block = WL_WPB waters of one system, one warp per water at a time; the
 // system's O positions are staged in shared memory WL_STAGE waters at a time
-// (w = -1 for excluded waters) and scanned 32 at a time with a ballot.
-constexpr int WL_BLOCK = 512, WL_WPB = 128, WL_STAGE = 1408;   // 44 KB of staged O positions
+// in FP32, relative to the solvent centre (w = -1 for excluded waters), and
+// scanned 64 at a time (two per lane, packed FP32x2) with a ballot per 32.
+// The FP32 squared distance decides every pair farther than WL_EPS2 from the
+// cut-off; the few within it are decided in FP64 from the coordinates, so the
+// list is the reference's FP64 list exactly.  (|x| <= ~30 A from the centre:
+// each FP32 coordinate is within 1.9e-6 A, r^2 near 100 A^2 within ~2e-4 A^2.)
+constexpr int WL_BLOCK = 512, WL_WPB = 128, WL_STAGE = 2816;   // 44 KB of staged O positions
+constexpr float WL_EPS2 = 4e-3f;
 
 __global__ void __launch_bounds__(WL_BLOCK) k_list_ww(DevPtrs P, int force) {
   int s = blockIdx.y;
@@ -576,10 +614,12 @@ __global__ void __launch_bounds__(WL_BLOCK) k_list_ww(DevPtrs P, int force) {
   const int i0 = blockIdx.x * WL_WPB;
   if (i0 >= S.nwat) return;
   const int i1 = min(i0 + WL_WPB, S.nwat);
-  __shared__ double4 so[WL_STAGE];
+  __shared__ float4 so[WL_STAGE];
   __shared__ int scnt[WL_WPB];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = WL_BLOCK / 32;
   const int obase = S.aoff + S.nsol;
+  const double cx = S.xw[0], cy = S.xw[1], cz = S.xw[2];
+  const float rc2 = (float)S.Rcww2;
   for (int t = threadIdx.x; t < WL_WPB; t += WL_BLOCK) scnt[t] = 0;
   for (int c0 = 0; c0 < S.nwat; c0 += WL_STAGE) {
     const int cn = min(WL_STAGE, S.nwat - c0);
@@ -587,8 +627,7 @@ __global__ void __launch_bounds__(WL_BLOCK) k_list_ww(DevPtrs P, int force) {
     for (int t = threadIdx.x; t < cn; t += WL_BLOCK) {
       int o = obase + 3 * (c0 + t);
       double4 x = P.x[o];
-      x.w = (P.flags[o] & F_EXCL) ? -1.0 : 1.0;
-      so[t] = x;
+      so[t] = make_float4((float)(x.x - cx), (float)(x.y - cy), (float)(x.z - cz), (P.flags[o] & F_EXCL) ? -1.f : 1.f);
     }
     __syncthreads();
     for (int iw = i0 + warp; iw < i1; iw += nwarp) {
@@ -596,25 +635,48 @@ __global__ void __launch_bounds__(WL_BLOCK) k_list_ww(DevPtrs P, int force) {
       const int oi = obase + 3 * iw;
       if (P.flags[oi] & F_EXCL) continue;
       const double3 xi = ld3(P.x, oi);
+      const float2 nx = dup2(-(float)(xi.x - cx)), ny = dup2(-(float)(xi.y - cy)), nz = dup2(-(float)(xi.z - cz));
       uint16_t *out = P.ww + (size_t)gw * P.ww_cap;
       int *sp = P.ww_sp + (size_t)gw * P.ww_nch;
       int cnt = scnt[iw - i0];
-      for (int b = 0; b < cn; b += 32) {
-        const int base = c0 + b;
-        if (base > 0 && base % P.ww_chunk == 0 && lane == 0) sp[base / P.ww_chunk - 1] = min(cnt, P.ww_cap);
-        const int jl = b + lane, jw = base + lane;
-        bool ok = false;
-        if (jl < cn && jw != iw) {
-          double4 xj = so[jl];
-          double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-          ok = xj.w > 0.0 && dx * dx + dy * dy + dz * dz <= S.Rcww2;
+      for (int b = 0; b < cn; b += 64) {
+        // lane takes j = b + lane and b + 32 + lane
+        float4 a = make_float4(0.f, 0.f, 0.f, -1.f), e = a;
+        const int jl0 = b + lane, jl1 = b + 32 + lane;
+        if (jl0 < cn) a = so[jl0];
+        if (jl1 < cn) e = so[jl1];
+        const float2 dx = __fadd2_rn(make_float2(a.x, e.x), nx), dy = __fadd2_rn(make_float2(a.y, e.y), ny),
+                     dz = __fadd2_rn(make_float2(a.z, e.z), nz);
+        const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+        bool ok2[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int jl = h ? jl1 : jl0, jw = c0 + jl;
+          const float w = h ? e.w : a.w, rr = h ? r2.y : r2.x;
+          bool ok = jl < cn && jw != iw && w > 0.f;
+          if (ok) {
+            if (fabsf(rr - rc2) <= WL_EPS2) {
+              // near the cut-off: the reference's FP64 test
+              const double3 xj = ld3(P.x, obase + 3 * jw);
+              const double ddx = xi.x - xj.x, ddy = xi.y - xj.y, ddz = xi.z - xj.z;
+              ok = ddx * ddx + ddy * ddy + ddz * ddz <= S.Rcww2;
+            } else {
+              ok = rr < rc2;
+            }
+          }
+          ok2[h] = ok;
         }
-        unsigned bal = __ballot_sync(FULL, ok);
-        if (ok) {
-          int pos = cnt + __popc(bal & ((1u << lane) - 1u));
-          if (pos < P.ww_cap) out[pos] = (uint16_t)jw;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int base = c0 + b + 32 * h;
+          if (base > 0 && base % P.ww_chunk == 0 && lane == 0) sp[base / P.ww_chunk - 1] = min(cnt, P.ww_cap);
+          const unsigned bal = __ballot_sync(FULL, ok2[h]);
+          if (ok2[h]) {
+            const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
+            if (pos < P.ww_cap) out[pos] = (uint16_t)(base + lane);
+          }
+          cnt += __popc(bal);
         }
-        cnt += __popc(bal);
       }
       if (lane == 0) scnt[iw - i0] = cnt;
       __syncwarp();
@@ -697,8 +759,9 @@ __global__ void k_list_pp(DevPtrs P, int force) {
       double dx = xs.x - xj.x, dy = xs.y - xj.y, dz = xs.z - xj.z;
       if (dx * dx + dy * dy + dz * dz > S.Rcpp2) continue;
     } else {
+      const int reach = groups_reach(P, gi, gj, S.Rcpp2);
       double last;
-      if (!groups_inside_any(P, gi, gj, S.Rcpp2, &last)) continue;
+      if (reach < 0 || (reach == 0 && !groups_inside_any(P, gi, gj, S.Rcpp2, &last))) continue;
     }
     for (int ia = P.cg_first[gi]; ia <= P.cg_last[gi]; ia++) {
       int i = P.cg_atoms[ia];
@@ -747,8 +810,9 @@ __global__ void k_list_pw(DevPtrs P, int force) {
           double dx = xs.x - xo.x, dy = xs.y - xo.y, dz = xs.z - xo.z;
           ok = dx * dx + dy * dy + dz * dz <= S.Rcpw2;
         } else {
+          const int reach = group_point_reach(P, gi, xo, S.Rcpw2);
           double last;
-          ok = group_point_inside_any(P, gi, xo, S.Rcpw2, &last);
+          ok = reach > 0 || (reach == 0 && group_point_inside_any(P, gi, xo, S.Rcpw2, &last));
         }
       }
       unsigned bal = __ballot_sync(FULL, ok);
@@ -892,7 +956,9 @@ __global__ void k_lists_end(DevPtrs P, int force) {
 // 8 consecutive waters on 8 distinct 16-byte bank groups.
 template <bool MIXED> struct WatRec { static constexpr int words = MIXED ? 3 : 5; };
 constexpr int WREC_MAX = 5;
-constexpr int WW_BLOCK = 512, WW_WPB = 128;   // threads, waters per block
+// threads, most waters per block (a batch of few systems takes fewer per
+// block, so that its blocks still fill the SMs)
+constexpr int WW_BLOCK = 512, WW_WPB = 128;
 constexpr int WW_STAGE_BYTES = 112 * 1024;    // staged records per block: two blocks per SM
 
 // watpol (md.f90:15122), per water: the angle between the water dipole and
@@ -1007,7 +1073,7 @@ __device__ __forceinline__ void unpack_mixed(const float4 *r, float *v) {
 }
 
 // nonbond_ww_spc (md.f90:11823) over the water-water list.  Block = 512
-// threads on WW_WPB consecutive waters of one system (blockIdx.y).  The
+// threads on wpb (<= WW_WPB) consecutive waters of one system (blockIdx.y).  The
 // system's water records are staged in shared memory in chunks of ww_chunk
 // waters; for each chunk every half-warp takes one water i and its 16 lanes
 // walk i's list slice for that chunk (the next entry prefetched), so
@@ -1017,15 +1083,15 @@ __device__ __forceinline__ void unpack_mixed(const float4 *r, float *v) {
 // (MUFU rsqrt), each lane's energy over one water's list slice summed in FP32 and accumulated in
 // FP64, gradients reduced in FP32.
 template <bool MIXED, bool HLJ>
-__global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
+__global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P, int wpb) {
   extern __shared__ float4 wsm[];
   __shared__ int2 srange[WW_WPB];          // list slice of each of the block's waters in this chunk
   constexpr int W = WatRec<MIXED>::words;
   int s = blockIdx.y;
   const SysDev &S = P.sys[s];
-  const int i0 = blockIdx.x * WW_WPB;
+  const int i0 = blockIdx.x * wpb;
   if (i0 >= S.nwat) return;
-  const int i1 = min(i0 + WW_WPB, S.nwat);
+  const int i1 = min(i0 + wpb, S.nwat);
   const int hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
   const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
   const float4 *rec = P.wrec + (size_t)S.woff * W;
@@ -1131,8 +1197,6 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P) {
 
 // ----------------------------------------------- packed FP32x2 water-water
 
-__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
-
 // Operands of water i on the packed path: O as hi + lo, the H offsets negated
 // in both orders ({-rH1, -rH2} and {-rH2, -rH1}, per component).
 struct WwI2 {
@@ -1196,15 +1260,15 @@ __device__ __forceinline__ void ww_force_x2(const WwI2 &I, const float4 j0, cons
 // 256 threads, two blocks per SM: one block's staging of records overlaps the
 // other's pair work (the registers of the packed path allow 16 warps per SM)
 constexpr int WWX_BLOCK = 256;
-__global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P) {
+__global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P, int wpb) {
   extern __shared__ float4 wsm[];
   __shared__ int2 srange[WW_WPB];
   constexpr int W = WatRec<true>::words;
   const int s = blockIdx.y;
   const SysDev &S = P.sys[s];
-  const int i0 = blockIdx.x * WW_WPB;
+  const int i0 = blockIdx.x * wpb;
   if (i0 >= S.nwat) return;
-  const int i1 = min(i0 + WW_WPB, S.nwat);
+  const int i1 = min(i0 + wpb, S.nwat);
   const int hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
   const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
   const float4 *rec = P.wrec + (size_t)S.woff * W;
@@ -1223,9 +1287,27 @@ __global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P) {
       srange[t] = make_int2(c == 0 ? 0 : sp[c - 1], sp[c]);
     }
     __syncthreads();
+    // the first group of list entries of the half-warp's next water, loaded
+    // one water ahead
+    int jfirst[4];
+    auto first_group = [&](int iw2, int *out) {
+#pragma unroll
+      for (int u = 0; u < 4; u++) out[u] = -1;
+      if (iw2 >= i1) return;
+      const int2 r = srange[iw2 - i0];
+      const uint16_t *nb2 = P.ww + (size_t)(S.woff + iw2) * P.ww_cap;
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        if (r.x + hl + 16 * u < r.y) out[u] = nb2[r.x + hl + 16 * u];
+    };
+    first_group(i0 + hw, jfirst);
     for (int iw = i0 + hw; iw < i1; iw += WWX_BLOCK / 16) {
       const int gw = S.woff + iw;
       const int kb = srange[iw - i0].x, ke = srange[iw - i0].y;
+      int jg[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) jg[u] = jfirst[u];
+      first_group(iw + WWX_BLOCK / 16, jfirst);
       if (kb >= ke) continue;
       const uint16_t *nb = P.ww + (size_t)gw * P.ww_cap;
       const float4 *ri = (iw >= c0 && iw < c0 + cn) ? wsm + (iw - c0) * W : rec + (size_t)iw * W;
@@ -1244,9 +1326,6 @@ __global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P) {
       // the lane's list entries in groups of four, loaded together, the next
       // group's loads issued before the current group's pairs
       int k = kb + hl;
-      int jg[4];
-#pragma unroll
-      for (int u = 0; u < 4; u++) jg[u] = k + 16 * u < ke ? (int)nb[k + 16 * u] : -1;
       for (; k < ke; k += 64) {
         int jn[4];
 #pragma unroll

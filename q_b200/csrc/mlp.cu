@@ -110,8 +110,8 @@ __device__ __forceinline__ void commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
-__device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity) {
-  for (long long it = 0; it < WAIT_LIMIT; it++) {
+__device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, long long limit) {
+  for (long long it = 0; it < limit; it++) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred P;\n\t"
@@ -176,6 +176,7 @@ struct Args {
   float *loss;         // [1] (mode 1) or [iters] (mode 2)
   float *adam_m, *adam_v;   // [NPARAM] (mode 2)
   int *status;
+  long long wait_limit;     // try_wait polls of each tensor-core wait before it gives up
 };
 
 // BF16 copies of the weights: W1, W2, W3 as B operands, W2^T and W3^T for
@@ -229,6 +230,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp(Args A) {
   const uint32_t tmem = *tmem_slot;
   const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);   // this warp's TMEM lanes
   uint32_t phase = 0;
+  uint32_t late_phase = 2;   // the phase a wait gave up on (2: none)
 
   // issue on thread 0 after every thread's shared-memory writes, wait for completion
   auto run = [&](auto issue) -> bool {
@@ -240,7 +242,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp(Args A) {
       issue();
       commit(barp);
     }
-    bool ok = wait_bar(barp, phase);
+    bool ok = wait_bar(barp, phase, A.wait_limit);
+    if (!ok) late_phase = phase;
     phase ^= 1u;
     ok = __syncthreads_and(ok);
     tc_after();
@@ -396,6 +399,10 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp(Args A) {
     stage_weights(sm, P, tid);
   }
 
+  // ---- after a wait that gave up, the MMAs it waited for may still run:
+  // wait for their commit once more (with the full limit) before the TMEM
+  // they write is released
+  if (late_phase != 2) wait_bar(barp, late_phase, WAIT_LIMIT);
   // ---- release TMEM (all tensor-core work has completed or timed out)
   tc_before();
   __syncthreads();
@@ -412,6 +419,10 @@ struct DevBuf {
   void *p = nullptr;
   ~DevBuf() { if (p) cudaFree(p); }
 };
+
+// polls of every tensor-core wait (qb_mlp_set_wait_limit); the default gives
+// up after seconds
+long long g_wait_limit = WAIT_LIMIT;
 
 int call(int mode, float *params, const float *x, const float *t, int n, int iters, const qb_mlp_adam *adam,
          float *y, float *grad, float *loss, int device) {
@@ -450,6 +461,7 @@ int call(int mode, float *params, const float *x, const float *t, int n, int ite
     a.params = (float *)dP.p; a.x = (const float *)dX.p; a.t = (const float *)dT.p; a.n = n; a.mode = mode;
     a.iters = iters; a.y = (float *)dY.p; a.grad = (float *)dG.p; a.loss = (float *)dL.p;
     a.adam_m = (float *)dM.p; a.adam_v = (float *)dV.p; a.status = (int *)dS.p;
+    a.wait_limit = g_wait_limit;
     if (adam) { a.lr = adam->lr; a.beta1 = adam->beta1; a.beta2 = adam->beta2; a.eps = adam->eps; a.wd = adam->weight_decay; }
     cuda(cudaFuncSetAttribute(k_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES), "smem attribute");
     k_mlp<<<1, THREADS, SMEM_BYTES>>>(a);
@@ -486,6 +498,12 @@ int qb_mlp_loss_grad(const float *params, const float *x, const float *t, int n,
 int qb_mlp_train(float *params, const float *x, const float *t, int n, int iters, const qb_mlp_adam *adam,
                  float *loss_history, int device) {
   return qb::mlp::call(2, params, x, t, n, iters, adam, nullptr, nullptr, loss_history, device);
+}
+
+int qb_mlp_set_wait_limit(long long polls) {
+  if (polls < 0) { qb::set_error("negative wait limit"); return QB_ERR_ARG; }
+  qb::mlp::g_wait_limit = polls > 0 ? polls : 0;
+  return QB_OK;
 }
 
 }  // extern "C"

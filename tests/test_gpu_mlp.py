@@ -91,3 +91,26 @@ def test_invalid_arguments():
         mlp.forward(p, np.zeros((mlp.MAX_SAMPLES + 1, mlp.IN), np.float32))
     with pytest.raises(ValueError):
         mlp.forward(p[:-1], np.zeros((3, mlp.IN), np.float32))
+
+
+def test_tensor_core_wait_times_out_and_recovers():
+    """Every tensor-core completion wait of the network kernel is bounded.  A
+    wait limit of 0 polls makes the first wait give up: the call returns
+    QB_ERR_TIMEOUT (after the kernel has drained its in-flight MMAs and
+    released its tensor memory), and the next call with the default limit
+    runs normally on the same context."""
+    from q_b200 import mlp
+    from q_b200._lib import QBError, lib
+    p = mlp.init(4)
+    x, t = _data(130, 7)
+    assert lib.qb_mlp_set_wait_limit(0) == 0
+    try:
+        for call in (lambda: mlp.forward(p, x), lambda: mlp.train(p, x, t, 5)):
+            with pytest.raises(QBError) as err:
+                call()
+            assert err.value.code == 8          # QB_ERR_TIMEOUT
+    finally:
+        assert lib.qb_mlp_set_wait_limit(67108864) == 0
+    y = mlp.forward(p, x)
+    yb, _ = M.forward(p, x, bf=True)
+    assert np.abs(y - yb).max() <= Y_TOL * np.abs(yb).max()

@@ -106,17 +106,23 @@ def workload_files(root: str, rank: int, args):
 
 
 def config_files(root: str):
-    """The three plain single-system configurations: (name, inp, lambdas,
-    dt_fs, description)."""
+    """The plain single-system configurations (the three spheres and a
+    periodic box at constant pressure): (name, inp, lambdas, dt_fs,
+    description)."""
     from q_b200 import synth
     c0 = synth.water_sphere(os.path.join(root, "cfg_c0"), radius=15.0, seed=1234, steps=1000, name="c0")
     c1 = synth.fep_solute(os.path.join(root, "cfg_c1"), seed=1234, steps=5000)
     c2 = synth.polymer_sphere(os.path.join(root, "cfg_c2"), seed=1234, steps=5000)
+    bx = synth.fep_box(os.path.join(root, "cfg_box"), edge=30.0, seed=1234, steps=5000, constant_pressure=True,
+                       volume_change=25)
     return [("c0_water_sphere_15A", c0.inp, None, 1.0, "TIP3P sphere R 15 A, 1 fs, LRF, SHAKE, restraints"),
             ("c1_fep_solute_20A", c1.inp, (0.5, 0.5), 2.0,
              "56-atom solute, 8 two-state Q atoms (soft-core), lambda 0.5, 20 A TIP3P sphere, 2 fs"),
             ("c2_protein_ligand_25A", c2.inp, (0.5, 0.5), 2.0,
-             "3000-atom polymer around the FEP solute, 25 A sphere, atoms beyond 23 A restrained, Q cut-off 99")]
+             "3000-atom polymer around the FEP solute, 25 A sphere, atoms beyond 23 A restrained, Q cut-off 99"),
+            ("box_fep_solute_30A_npt", bx.inp, (0.5, 0.5), 2.0,
+             "the FEP solute in a 30 A periodic TIP3P box, nearest images, LRF to 14 A, molecules put back "
+             "in the box, Monte Carlo volume moves every 25 steps, 2 fs")]
 
 
 class ClockSampler:
@@ -133,7 +139,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -156,13 +162,15 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
 
-    def summary(self):
-        """Samples that arrived while the timed steps ran (t0..t1)."""
+    def summary(self, margin: float = 0.3):
+        """Samples that arrived while the timed steps ran (t0..t1), widened by
+        `margin` seconds on either side, during which the GPU ran the same
+        steps (a timed region of a few ms falls between two samples)."""
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         t0, t1 = getattr(self, "t0", 0.0), getattr(self, "t1", 1e300)
         for ts, l in self.lines:
-            if not (t0 <= ts <= t1 + 0.15):
+            if not (t0 - margin <= ts <= t1 + margin):
                 continue
             f = [x.strip() for x in l.split(",")]
             if len(f) < 10:
@@ -426,12 +434,22 @@ def main():
     barrier()
     torch.cuda.synchronize(local)
     with ClockSampler(local) as clk:
-        batch.run(20)                 # the sampler starts while the GPU is busy
+        # keep the GPU stepping until the sampler reports (nvidia-smi takes a
+        # moment to start), then time; a few more steps after the timed ones
+        # keep it under the same load for the samples just after them
+        t_wait = time.time()
+        batch.run(20)
+        while len(clk.lines) < 3 and time.time() - t_wait < 5.0:
+            batch.run(25)
         align_to_rebuild(batch, views)
         start = batch.step_count()
         clk.mark("t0")
         ms, launches = batch.run_timed(args.steps)
         clk.mark("t1")
+        t_after = time.time()
+        while time.time() - t_after < 0.3:
+            batch.run(25)
+        batch.clear_history()
     barrier()
     rebuild, energy = step_kinds(views, start, args.steps)
     elapsed = max_over_ranks(ms / 1e3, dev)

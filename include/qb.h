@@ -37,7 +37,7 @@ enum qb_status {
   QB_ERR_ARG = 1,           /* invalid argument */
   QB_ERR_IO = 2,            /* cannot open/read/write a file (md.f90:1382 open_files) */
   QB_ERR_PARSE = 3,         /* invalid .inp/.top/.fep/.re content (md.f90:2528, topo.f90:1073, qatom.f90:874) */
-  QB_ERR_UNSUPPORTED = 4,   /* valid Q input outside this engine's scope (PBC, arithmetic rule, EVB, ...) */
+  QB_ERR_UNSUPPORTED = 4,   /* valid Q input outside this engine's scope (e.g. any-atom cut-offs in a periodic box) */
   QB_ERR_SHAKE = 5,         /* SHAKE did not converge in 1000 iterations (md.f90:14533-14551 'shake failure') */
   QB_ERR_NAN = 6,           /* non-finite energy or coordinate */
   QB_ERR_LIST_OVERFLOW = 7, /* a pair list exceeded its device capacity */
@@ -183,6 +183,13 @@ int qb_batch_history_all(qb_batch *b, int kind, int max_records, int *counts, do
  * a system that failed stops its own count, qb_batch_status). */
 int qb_batch_step_count(qb_batch *b, long long *out);
 
+/* Periodic box of system `sys`: box6 = edge lengths (3) then centre (3), as
+ * the restart file's box records hold them; tries/accepted (may be NULL): the
+ * Monte Carlo volume moves of a constant-pressure run so far.  Zeros for a
+ * sphere.  Replaces: boxlength/boxcenter, volume_try/volume_acc,
+ * src/q6/md.f90:15452-15475, 15812-15816. */
+int qb_batch_box(qb_batch *b, int sys, double *box6, long long *tries, long long *accepted);
+
 /* The off-diagonal elements of the same records: for every record and every
  * off-diagonal function io of the system's FEP file, Hij = A exp(-mu r_kl)
  * and r_kl, the distance of its two Q atoms at that step (offdiag,
@@ -301,6 +308,11 @@ int qb_peak_flops(int device, int precision, double *tflops);
  * Replaces: write_xfin, src/q6/md.f90:15452-15470. */
 int qb_write_re(const char *path, int natom, const double *x, const double *v,
                 int nshell, const float *theta_corr);
+
+/* The same with a periodic box's two records after them: box6 = edge
+ * lengths, then centre (md.f90:15471-15474). */
+int qb_write_re_box(const char *path, int natom, const double *x, const double *v,
+                    int nshell, const float *theta_corr, const double *box6);
 
 /* Append one energy-file frame: per state a record (int32 state, 15 doubles)
  * and one empty off-diagonal record.  Replaces: put_ene, src/q6/nrgy.f90:94-119. */

@@ -195,6 +195,23 @@ typedef struct qb_sysview {
   /* ---- temperature bookkeeping (md.f90:2460-2480) ---- */
   int Ndegf, Ndegfree, Ndegf_solute, Ndegf_solvent, Ndegfree_solute, Ndegfree_solvent;
   int detail_temps;
+
+  /* ---- periodic box (topology boundary "PBC", .inp [PBC], md.f90:2583-2656) ----
+   * Pairs take the nearest image of their charge groups' reference atoms;
+   * no excluded atoms, restrained shell, solvent sphere or polarisation. */
+  int use_pbc;
+  int rigid_box_center, put_solute_back_in_box, put_solvent_back_in_box;
+  int constant_pressure;        /* NPT: Monte Carlo volume moves (MC_volume, md.f90:15615) */
+  int ivolume_cycle, pressure_seed;
+  double max_vol_displ;         /* A^3 */
+  double pressure;              /* kcal/mol/A^3 (bar * 1.43836e-5) */
+  double boxlength[3], boxcenter[3];
+  const double *mol_mass_inv;   /* [nmol] 1 / molecule mass */
+  const double *mass_box;       /* [natom] mass as 1.0/winv in single precision (md.f90:13882) */
+  int qswitch;                  /* atom the Q-atom lists centre on in a box (-1: none) */
+  /* randm's state after the Maxwell velocities (randm_started: seeded), which
+   * the volume moves continue (md.f90:14408) */
+  int randm_started, randm_state;
 } qb_sysview;
 
 #ifdef __cplusplus

@@ -57,6 +57,10 @@ struct qo_state {
   double offd_r[QB_MAX_STATES];     /* r_kl of this step's off-diagonal functions */
   double ekinmax;
   double kinetic;
+  /* periodic box: edge lengths, inv_boxl, centre; randm's sequence; volume moves */
+  double boxl[3], iboxl[3], boxc[3];
+  int rand_started, irand;
+  long long vol_tries, vol_acc;
 };
 
 static const float kBoltz = 0.001986f;
@@ -113,9 +117,23 @@ static int zero_pair(const qb_sysview *s, int i, int j, int lj) {
          s->type_bvdw[3 * ti + lj - 1] * s->type_bvdw[3 * tj + lj - 1] == 0.0;
 }
 
+/* periodic box (use_PBC): boxlength * nint(d * inv_boxl), the lattice vector
+ * that brings displacement d to its nearest image (md.f90:5352-5354) */
+static double img(const qo_state *st, int k, double d) { return st->boxl[k] * (double)lround(d * st->iboxl[k]); }
+
 static double dist2(qo_state *st, int a, int b) {
   double dx = X(a, 0) - X(b, 0), dy = X(a, 1) - X(b, 1), dz = X(a, 2) - X(b, 2);
+  if (st->s->use_pbc) { dx -= img(st, 0, dx); dy -= img(st, 1, dy); dz -= img(st, 2, dz); }
   return dx * dx + dy * dy + dz * dz;
+}
+
+/* the switching atom of an atom's charge group */
+static int sw_of(const qo_state *st, int a) { return st->s->cgp_iswitch[st->s->iwhich_cgp[a]]; }
+
+/* image shift t[3] = L nint((x_b - x_a) / L) of the pair of reference atoms
+ * (a, b); zero in the sphere */
+static void pair_shift(qo_state *st, int a, int b, double t[3]) {
+  for (int k = 0; k < 3; k++) t[k] = st->s->use_pbc ? img(st, k, X(b, k) - X(a, k)) : 0.0;
 }
 
 /* multipole contribution of charge q at offset dr from a group centre
@@ -147,12 +165,21 @@ static void lrf_add(lrf_t *L, double q, const double dr[3]) {
       }
 }
 
+/* the charges of group from_group into group into's multipoles; in a box at
+ * the image of from_group's switching atom nearest into's centre
+ * (nbpplist_box_lrf md.f90:5842-5856) */
 static void lrf_group_from_atoms(qo_state *st, int into, int from_group, int skip_q) {
   const qb_sysview *s = st->s;
+  double t[3] = {0, 0, 0};
+  if (s->use_pbc) {
+    int sw = s->cgp_iswitch[from_group];
+    for (int k = 0; k < 3; k++) t[k] = img(st, k, X(sw, k) - st->lrf[into].c[k]);
+  }
   for (int a = s->cgp_first[from_group]; a <= s->cgp_last[from_group]; a++) {
     int i = s->cgpatom[a];
     if (skip_q && s->iqatom[i] >= 0) continue;
-    double dr[3] = {X(i, 0) - st->lrf[into].c[0], X(i, 1) - st->lrf[into].c[1], X(i, 2) - st->lrf[into].c[2]};
+    double dr[3] = {X(i, 0) - st->lrf[into].c[0] - t[0], X(i, 1) - st->lrf[into].c[1] - t[1],
+                    X(i, 2) - st->lrf[into].c[2] - t[2]};
     lrf_add(&st->lrf[into], (double)s->crg[i], dr);
   }
 }
@@ -268,10 +295,7 @@ static void list_pw(qo_state *st) {
       } else if (s->use_LRF && r2 <= rl2) {
         int jg = s->iwhich_cgp[o];
         lrf_group_from_atoms(st, jg, ig, 1);
-        for (int j = o; j < o + 3; j++) {
-          double dr[3] = {X(j, 0) - st->lrf[ig].c[0], X(j, 1) - st->lrf[ig].c[1], X(j, 2) - st->lrf[ig].c[2]};
-          lrf_add(&st->lrf[ig], (double)s->crg[j], dr);
-        }
+        lrf_group_from_atoms(st, ig, jg, 0);
       }
     }
   }
@@ -296,14 +320,8 @@ static void list_ww(qo_state *st) {
           st->ww[st->nww++] = jo;
         } else if (s->use_LRF && r2 <= rl2) {
           int jg = s->iwhich_cgp[jo], ig = s->iwhich_cgp[io];
-          for (int a = io; a < io + 3; a++) {
-            double dr[3] = {X(a, 0) - st->lrf[jg].c[0], X(a, 1) - st->lrf[jg].c[1], X(a, 2) - st->lrf[jg].c[2]};
-            lrf_add(&st->lrf[jg], (double)s->crg[a], dr);
-          }
-          for (int a = jo; a < jo + 3; a++) {
-            double dr[3] = {X(a, 0) - st->lrf[ig].c[0], X(a, 1) - st->lrf[ig].c[1], X(a, 2) - st->lrf[ig].c[2]};
-            lrf_add(&st->lrf[ig], (double)s->crg[a], dr);
-          }
+          lrf_group_from_atoms(st, jg, ig, 0);
+          lrf_group_from_atoms(st, ig, jg, 0);
         }
       }
     }
@@ -315,7 +333,7 @@ static void list_ww(qo_state *st) {
 /* nbqplist (md.f90:7875): built once when Rcq exceeds the sphere */
 static void list_qp(qo_state *st) {
   const qb_sysview *s = st->s;
-  if (st->qp_done && s->Rcq > s->rexcl_o) return;
+  if (!s->use_pbc && st->qp_done && s->Rcq > s->rexcl_o) return;
   st->nqp = 0;
   if (st->nq == 0) return;
   double rc2 = s->Rcq * s->Rcq;
@@ -323,7 +341,10 @@ static void list_qp(qo_state *st) {
     int sw = s->cgp_iswitch[ig];
     if (s->excl[sw]) continue;
     int inside = 0;
-    if (s->iuse_switch_atom == 1) {
+    if (s->use_pbc) {
+      /* nbqplist_box (md.f90:7969): the switching atom's nearest image of the Q switching atom */
+      inside = dist2(st, sw, s->qswitch) <= rc2;
+    } else if (s->iuse_switch_atom == 1) {
       double r2 = 0;
       for (int k = 0; k < 3; k++) { double d = X(sw, k) - s->xpcent[k]; r2 += d * d; }
       inside = r2 <= rc2;
@@ -361,7 +382,7 @@ static void list_qp(qo_state *st) {
 /* nbqwlist (md.f90:8066) */
 static void list_qw(qo_state *st) {
   const qb_sysview *s = st->s;
-  if (s->Rcq > s->rexcl_o && st->nqw > 0) return;
+  if (!s->use_pbc && s->Rcq > s->rexcl_o && st->nqw > 0) return;
   st->nqw = 0;
   if (st->nq == 0) return;
   double rc2 = s->Rcq * s->Rcq;
@@ -369,12 +390,17 @@ static void list_qw(qo_state *st) {
     int o = st->NS + 3 * iw;
     if (s->excl[o]) continue;
     double r2 = 0;
-    for (int k = 0; k < 3; k++) { double d = X(o, k) - s->xpcent[k]; r2 += d * d; }
+    if (s->use_pbc) {
+      r2 = dist2(st, o, s->qswitch);   /* nbqwlist_box (md.f90:8123) */
+    } else {
+      for (int k = 0; k < 3; k++) { double d = X(o, k) - s->xpcent[k]; r2 += d * d; }
+    }
     if (r2 <= rc2) st->qw[st->nqw++] = o;
   }
 }
 
-/* make_pair_lists (md.f90:3716), sphere branch */
+/* make_pair_lists (md.f90:3716); the box branch calls the *_box lists, which
+ * are the sphere lists with nearest-image distances (dist2) */
 static void make_pair_lists(qo_state *st) {
   if (st->s->use_LRF) cgp_centers(st);
   list_pp(st);
@@ -416,7 +442,9 @@ static void nonbond_pp(qo_state *st) {
   const qb_sysview *s = st->s;
   for (int p = 0; p < st->npp; p++) {
     int i = st->pp[p].i, j = st->pp[p].j, lj = st->pp[p].lj;
-    double dx[3] = {X(j, 0) - X(i, 0), X(j, 1) - X(i, 1), X(j, 2) - X(i, 2)};
+    double t[3];
+    pair_shift(st, sw_of(st, i), sw_of(st, j), t);   /* nonbond_pp_box (md.f90:10508-10519) */
+    double dx[3] = {X(j, 0) - X(i, 0) - t[0], X(j, 1) - X(i, 1) - t[1], X(j, 2) - X(i, 2) - t[2]};
     double r2 = 1. / (dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
     double r = sqrt(r2), r6 = r2 * r2 * r2;
     float qq = s->crg[i] * s->crg[j];
@@ -448,7 +476,9 @@ static void nonbond_pw(qo_state *st) {
     int ti = s->iac[i], tj = s->iac[j];
     double aLJ, bLJ;
     ljp(s, avdw(s, ti, lj), avdw(s, tj, lj), bvdw(s, ti, lj), bvdw(s, tj, lj), &aLJ, &bLJ);
-    double dx[3] = {X(j, 0) - X(i, 0), X(j, 1) - X(i, 1), X(j, 2) - X(i, 2)};
+    double t[3];
+    pair_shift(st, sw_of(st, i), sw_of(st, j), t);   /* nonbond_pw_box (md.f90:10693-10699) */
+    double dx[3] = {X(j, 0) - X(i, 0) - t[0], X(j, 1) - X(i, 1) - t[1], X(j, 2) - X(i, 2) - t[2]};
     double r2 = 1. / (dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
     double r = sqrt(r2), r6 = r2 * r2 * r2, r12 = r6 * r6;
     float qq = s->crg[i] * s->crg[j];
@@ -469,7 +499,9 @@ static void nonbond_qp(qo_state *st) {
     int iq = st->qp[p].iq, j = st->qp[p].j, lj = st->qp[p].lj, qlj = st->qp[p].qlj;
     int i = s->iqseq[iq];
     int tj = s->iac[j];
-    double dx[3] = {X(j, 0) - X(i, 0), X(j, 1) - X(i, 1), X(j, 2) - X(i, 2)};
+    double t[3] = {0, 0, 0};
+    if (s->use_pbc) pair_shift(st, s->qswitch, sw_of(st, j), t);   /* nonbond_qp_box (md.f90:11060-11068) */
+    double dx[3] = {X(j, 0) - X(i, 0) - t[0], X(j, 1) - X(i, 1) - t[1], X(j, 2) - X(i, 2) - t[2]};
     double r2 = dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
     if (!s->qvdw_flag) {
       r2 = 1. / r2;
@@ -519,11 +551,13 @@ static void nonbond_ww(qo_state *st) {
     int io = st->NS + 3 * iw;
     for (; st->ww[ip] >= 0; ip++) {
       int jo = st->ww[ip];
+      double t[3];
+      pair_shift(st, io, jo, t);   /* nonbond_ww_spc_box (md.f90:12078-12100) */
       for (int a = 0; a < 3; a++) {
         int ia = io + a;
         for (int b = 0; b < 3; b++) {
           int jb = jo + b;
-          double dx[3] = {X(jb, 0) - X(ia, 0), X(jb, 1) - X(ia, 1), X(jb, 2) - X(ia, 2)};
+          double dx[3] = {X(jb, 0) - X(ia, 0) - t[0], X(jb, 1) - X(ia, 1) - t[1], X(jb, 2) - X(ia, 2) - t[2]};
           double rinv = sqrt(1.0 / (dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]));
           double r2 = rinv * rinv;
           float qq = (a == 0 && b == 0) ? qoo : ((a == 0 || b == 0) ? qoh : qhh);
@@ -560,10 +594,16 @@ static void nonbond_qw(qo_state *st) {
   double aH[2] = {avdw(s, iac_hw, 1), avdw(s, iac_hw, 2)}, bH[2] = {bvdw(s, iac_hw, 1), bvdw(s, iac_hw, 2)};
   for (int jw = 0; jw < st->nqw; jw++) {
     int j = st->qw[jw];
+    double t[3] = {0, 0, 0};
+    if (s->use_pbc) pair_shift(st, s->qswitch, j, t);   /* nonbond_qw_spc_box (md.f90:11440-11446) */
     for (int iq = 0; iq < st->nq; iq++) {
       int i = s->iqseq[iq];
       double dO[3], dH1[3], dH2[3];
-      for (int k = 0; k < 3; k++) { dO[k] = X(j, k) - X(i, k); dH1[k] = X(j + 1, k) - X(i, k); dH2[k] = X(j + 2, k) - X(i, k); }
+      for (int k = 0; k < 3; k++) {
+        dO[k] = X(j, k) - X(i, k) - t[k];
+        dH1[k] = X(j + 1, k) - X(i, k) - t[k];
+        dH2[k] = X(j + 2, k) - X(i, k) - t[k];
+      }
       double r2O = dO[0] * dO[0] + dO[1] * dO[1] + dO[2] * dO[2];
       double rH1 = sqrt(1.0 / (dH1[0] * dH1[0] + dH1[1] * dH1[1] + dH1[2] * dH1[2]));
       double rH2 = sqrt(1.0 / (dH2[0] * dH2[0] + dH2[1] * dH2[1] + dH2[2] * dH2[2]));
@@ -1076,6 +1116,8 @@ static void p_restrain(qo_state *st) {
   for (int r = 0; r < s->nrstr_dist; r++) {
     int ipsi = s->rdis_ipsi[r], i = s->rdis_i[r], j = s->rdis_j[r];
     double dr[3] = {X(j, 0) - X(i, 0), X(j, 1) - X(i, 1), X(j, 2) - X(i, 2)};
+    if (s->use_pbc)   /* md.f90:13096-13101 */
+      for (int k = 0; k < 3; k++) dr[k] -= img(st, k, dr[k]);
     double wgt = ipsi != 0 ? s->lambda[ipsi - 1] : 1.0;
     double b = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]), db;
     if (b < s->rdis_d1[r]) db = b - s->rdis_d1[r];
@@ -1089,6 +1131,8 @@ static void p_restrain(qo_state *st) {
     int ipsi = s->rang_ipsi[r], i = s->rang_i[r], j = s->rang_j[r], k = s->rang_k[r];
     double d1[3], d2[3];
     for (int c = 0; c < 3; c++) { d1[c] = X(i, c) - X(j, c); d2[c] = X(k, c) - X(j, c); }
+    if (s->use_pbc)   /* md.f90:13160-13168 */
+      for (int c = 0; c < 3; c++) { d1[c] -= img(st, c, d1[c]); d2[c] -= img(st, c, d2[c]); }
     double wgt = ipsi != 0 ? s->lambda[ipsi - 1] : 1.0;
     double r2ij = d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2], r2jk = d2[0] * d2[0] + d2[1] * d2[1] + d2[2] * d2[2];
     double rij = sqrt(r2ij), rjk = sqrt(r2jk);
@@ -1281,9 +1325,10 @@ static void pot_energy(qo_state *st) {
   st->E[QB_E_W_TORSION] = torsions(st, s->ntors_solute, s->ntors);
   st->E[QB_E_P_IMPROPER] = impropers(st, 0, s->nimps_solute);
   st->E[QB_E_W_IMPROPER] = impropers(st, s->nimps_solute, s->nimps);
-  fix_shell(st);
+  /* the sphere's restraints (none in a periodic box, md.f90:13345-13356) */
+  if (!s->use_pbc) fix_shell(st);
   p_restrain(st);
-  if (st->nwat > 0) {
+  if (st->nwat > 0 && !s->use_pbc) {
     restrain_solvent(st);
     if (s->wpol_restr) watpol(st);
   }
@@ -1415,6 +1460,163 @@ static void record(qo_state *st, int kind) {
   st->hcount[kind]++;
 }
 
+/* ---------------------------------------------------------- periodic box */
+
+/* randm (md.f90:14408-14442): one sequence, seeded by the first call */
+static double randm(qo_state *st, int seed) {
+  const int m = 100000000, m1 = 10000, mult = 31415821;
+  if (!st->rand_started) { st->rand_started = 1; st->irand = abs(seed) % m; }
+  int ih = st->irand / m1, il = st->irand % m1;
+  int r = ((ih * (mult % m1) + il * (mult / m1)) % m1) * m1 + il * (mult % m1);
+  r = (r + 1) % m;
+  st->irand = r;
+  float v = (float)(r / 10) * 10.0f / (float)m;
+  if (v <= 0.0f || v > 1.0f) v = 0.0f;
+  return (double)v;
+}
+
+/* put_back_in_box (md.f90:15477-15600) */
+static void put_back_in_box(qo_state *st) {
+  const qb_sysview *s = st->s;
+  int nmol = s->nmol;
+  if (!s->rigid_box_center) {
+    int n = st->NS > 0 ? st->NS : st->N;
+    double c[3] = {0, 0, 0};
+    for (int i = 0; i < n; i++)
+      for (int k = 0; k < 3; k++) c[k] += X(i, k);
+    for (int k = 0; k < 3; k++) st->boxc[k] = c[k] / n;
+  }
+  int first = 0, last = nmol;
+  if (nmol > 1) {
+    int nsolv = (st->N - st->NS) / (s->istart_mol[nmol - 1] - s->istart_mol[nmol - 2]);
+    if (!s->put_solute_back_in_box) first = nmol - nsolv;
+    if (!s->put_solvent_back_in_box) last = nmol - nsolv;
+  }
+  for (int m = first; m < last; m++) {
+    double cm[3] = {0, 0, 0};
+    for (int j = s->istart_mol[m]; j < s->istart_mol[m + 1]; j++)
+      for (int k = 0; k < 3; k++) cm[k] += X(j, k) * s->mass_box[j];
+    for (int k = 0; k < 3; k++) {
+      cm[k] = cm[k] * s->mol_mass_inv[m];
+      double hi = st->boxc[k] + st->boxl[k] / 2, lo = st->boxc[k] - st->boxl[k] / 2, sh = 0.0;
+      if (cm[k] > hi) sh = -st->boxl[k];
+      else if (cm[k] < lo) sh = st->boxl[k];
+      if (sh != 0.0)
+        for (int j = s->istart_mol[m]; j < s->istart_mol[m + 1]; j++) X(j, k) += sh;
+    }
+  }
+}
+
+/* new_potential (md.f90:15846-15972): the nonbonded, restraint, LRF and Q-Q
+ * terms at the current coordinates; the bonded terms of the total come from
+ * `old` */
+static void new_potential(qo_state *st, const double *old) {
+  const qb_sysview *s = st->s;
+  double *E = st->E;
+  int zero[] = {QB_E_POTENTIAL, QB_E_PP_EL, QB_E_PP_VDW, QB_E_PW_EL, QB_E_PW_VDW, QB_E_WW_EL, QB_E_WW_VDW,
+                QB_E_QX_EL, QB_E_QX_VDW, QB_E_RST_PROTEIN, QB_E_LRF};
+  for (size_t k = 0; k < sizeof zero / sizeof zero[0]; k++) E[zero[k]] = 0.0;
+  int zq[] = {QB_EQ_QQ_EL, QB_EQ_QQ_VDW, QB_EQ_QP_EL, QB_EQ_QP_VDW, QB_EQ_QW_EL, QB_EQ_QW_VDW, QB_EQ_RESTRAINT};
+  for (int k = 0; k < st->S; k++)
+    for (size_t c = 0; c < sizeof zq / sizeof zq[0]; c++) EQV(k, zq[c]) = 0.0;
+  memset(st->d, 0, 3 * (size_t)st->N * sizeof(double));
+  nonbond_pp(st);
+  nonbond_pw(st);
+  nonbond_qp(st);
+  if (st->N > st->NS) {
+    nonbond_ww(st);
+    nonbond_qw(st);
+  }
+  if (s->use_LRF) lrf_taylor(st);
+  p_restrain(st);
+  nonbond_qq(st);
+  for (int k = 0; k < st->S; k++) {
+    double lam = s->lambda[k];
+    EQV(k, QB_EQ_QX_EL) = EQV(k, QB_EQ_QQ_EL) + EQV(k, QB_EQ_QP_EL) + EQV(k, QB_EQ_QW_EL);
+    EQV(k, QB_EQ_QX_VDW) = EQV(k, QB_EQ_QQ_VDW) + EQV(k, QB_EQ_QP_VDW) + EQV(k, QB_EQ_QW_VDW);
+    E[QB_E_QX_EL] += EQV(k, QB_EQ_QX_EL) * lam;
+    E[QB_E_QX_VDW] += EQV(k, QB_EQ_QX_VDW) * lam;
+    E[QB_E_RST_PROTEIN] += EQV(k, QB_EQ_RESTRAINT) * lam;
+  }
+  E[QB_E_POTENTIAL] = old[QB_E_P_BOND] + old[QB_E_W_BOND] + old[QB_E_P_ANGLE] + old[QB_E_W_ANGLE] +
+                      old[QB_E_P_TORSION] + old[QB_E_P_IMPROPER] + E[QB_E_PP_EL] + E[QB_E_PP_VDW] + E[QB_E_PW_EL] +
+                      E[QB_E_PW_VDW] + E[QB_E_WW_EL] + E[QB_E_WW_VDW] + old[QB_E_Q_BOND] + old[QB_E_Q_ANGLE] +
+                      old[QB_E_Q_TORSION] + old[QB_E_Q_IMPROPER] + E[QB_E_QX_EL] + E[QB_E_QX_VDW] +
+                      E[QB_E_RST_PROTEIN] + E[QB_E_LRF];
+}
+
+/* MC_volume (md.f90:15615-15840): returns 0, or 10 (QB_ERR_STATE) when the
+ * new box is too small for a cut-off (the reference dies) */
+static int mc_volume(qo_state *st) {
+  const qb_sysview *s = st->s;
+  size_t n3 = 3 * (size_t)st->N;
+  double *old_x = (double *)malloc(n3 * sizeof(double));
+  lrf_t *old_lrf = NULL;
+  double old_E[QB_NE], old_EQ[QB_MAX_STATES * QB_NEQ], old_boxl[3], old_inv[3];
+  memcpy(old_x, st->x, n3 * sizeof(double));
+  memcpy(old_E, st->E, sizeof old_E);
+  memcpy(old_boxl, st->boxl, sizeof old_boxl);
+  memcpy(old_inv, st->iboxl, sizeof old_inv);
+  if (s->use_LRF) {
+    old_lrf = (lrf_t *)malloc(((size_t)s->ncgp + 1) * sizeof(lrf_t));
+    memcpy(old_lrf, st->lrf, (size_t)s->ncgp * sizeof(lrf_t));
+  }
+  new_potential(st, old_E);
+  memcpy(old_E, st->E, sizeof old_E);
+  memcpy(old_EQ, st->EQ, sizeof old_EQ);
+  double old_V = old_boxl[0] * old_boxl[1] * old_boxl[2];
+  double r = randm(st, s->pressure_seed);
+  r = r * 2 - 1;
+  double deltaV = r * s->max_vol_displ, new_V = deltaV + old_V;
+  double ratio = pow(new_V / old_V, (double)(1.0f / 3.0f));
+  for (int k = 0; k < 3; k++) { st->boxl[k] = st->boxl[k] * ratio; st->iboxl[k] = 1.0 / st->boxl[k]; }
+  double bmin = fmin(st->boxl[0], fmin(st->boxl[1], st->boxl[2]));
+  if (!(bmin > s->Rcpp * 2) || !(bmin > s->Rcww * 2) || !(bmin > s->Rcpw * 2) || !(bmin > s->Rcq * 2) ||
+      !(bmin > s->RcLRF * 2)) {
+    free(old_x); free(old_lrf);
+    return 10;
+  }
+  for (int m = 0; m < s->nmol; m++) {
+    double cm[3] = {0, 0, 0}, mv[3];
+    for (int j = s->istart_mol[m]; j < s->istart_mol[m + 1]; j++)
+      for (int k = 0; k < 3; k++) cm[k] += X(j, k) * s->mass_box[j];
+    for (int k = 0; k < 3; k++) {
+      cm[k] = cm[k] * s->mol_mass_inv[m];
+      mv[k] = ((cm[k] - st->boxc[k]) * st->boxl[k] / old_boxl[k] + st->boxc[k]) - cm[k];
+    }
+    for (int j = s->istart_mol[m]; j < s->istart_mol[m + 1]; j++)
+      for (int k = 0; k < 3; k++) X(j, k) += mv[k];
+  }
+  if (s->use_LRF) {
+    cgp_centers(st);
+    list_pp(st);
+    list_pw(st);
+    list_ww(st);
+  }
+  new_potential(st, old_E);
+  double deltaE = st->E[QB_E_POTENTIAL] - old_E[QB_E_POTENTIAL];
+  double deltaW = deltaE + s->pressure * deltaV - (double)((float)s->nmol * kBoltz) * s->Temp0 * log(new_V / old_V);
+  int acc = 1;
+  if (deltaW > 0.0) {
+    double u = randm(st, s->pressure_seed);
+    acc = !(u > exp(-deltaW / (double)kBoltz / s->Temp0));
+  }
+  st->vol_tries++;
+  if (acc) {
+    st->vol_acc++;
+  } else {
+    memcpy(st->x, old_x, n3 * sizeof(double));
+    memcpy(st->E, old_E, sizeof old_E);
+    memcpy(st->EQ, old_EQ, (size_t)st->S * QB_NEQ * sizeof(double));
+    memcpy(st->boxl, old_boxl, sizeof old_boxl);
+    memcpy(st->iboxl, old_inv, sizeof old_inv);
+    if (s->use_LRF) memcpy(st->lrf, old_lrf, (size_t)s->ncgp * sizeof(lrf_t));
+  }
+  free(old_x);
+  free(old_lrf);
+  return 0;
+}
+
 /* ------------------------------------------------------------- public */
 
 qo_state *qo_create(const qb_sysview *s, int history_capacity) {
@@ -1452,6 +1654,14 @@ qo_state *qo_create(const qb_sysview *s, int history_capacity) {
     st->hEQ[k] = (double *)malloc((size_t)(history_capacity + 1) * (st->S + 1) * QB_NEQ * sizeof(double));
     st->hR[k] = (double *)calloc((size_t)(history_capacity + 1) * QB_MAX_STATES, sizeof(double));
   }
+  if (s->use_pbc)
+    for (int k = 0; k < 3; k++) {
+      st->boxl[k] = s->boxlength[k];
+      st->iboxl[k] = 1.0 / s->boxlength[k];
+      st->boxc[k] = s->boxcenter[k];
+    }
+  st->rand_started = s->randm_started;
+  st->irand = s->randm_state;
   /* md_run start: initial temperature (md.f90:3960-3963) */
   st->Tscale_solute = st->Tscale_solvent = 1.0;
   temperature(st);
@@ -1474,7 +1684,10 @@ int qo_run(qo_state *st, int nsteps) {
   const qb_sysview *s = st->s;
   const double dt = s->dt;
   for (int n = 0; n < nsteps; n++) {
-    if (st->istep % s->NBcycle == 0) make_pair_lists(st);
+    if (st->istep % s->NBcycle == 0) {
+      if (s->use_pbc && (s->put_solute_back_in_box || s->put_solvent_back_in_box)) put_back_in_box(st);
+      make_pair_lists(st);
+    }
     pot_energy(st);
     if (s->noffd > 0) offdiag(st);
     st->E[QB_E_KINETIC] = st->kinetic;
@@ -1494,6 +1707,9 @@ int qo_run(qo_state *st, int nsteps) {
     }
     temperature(st);
     st->E[QB_E_KINETIC] = st->kinetic;
+    /* constant pressure: a volume move before the step's output (md.f90:4137-4141) */
+    if (s->use_pbc && s->constant_pressure && st->istep % s->ivolume_cycle == 0 && st->istep > 0)
+      if (mc_volume(st) != 0) { st->status = 10; return 10; }
     if (st->istep % s->iene_cycle == 0 && st->istep > 0) record(st, 1);
     if (st->istep % s->iout_cycle == 0) record(st, 0);
     st->istep++;
@@ -1544,3 +1760,11 @@ void qo_list_counts(const qo_state *st, int *out) {
   out[0] = st->npp; out[1] = st->npw; out[2] = st->nww - st->nwat; out[3] = st->nqp; out[4] = st->nqw;
 }
 int qo_status(const qo_state *st) { return st->status; }
+
+void qo_box(const qo_state *st, double *box6) {
+  for (int k = 0; k < 3; k++) { box6[k] = st->boxl[k]; box6[3 + k] = st->boxc[k]; }
+}
+void qo_volume_moves(const qo_state *st, long long *tries, long long *accepted) {
+  *tries = st->vol_tries;
+  *accepted = st->vol_acc;
+}

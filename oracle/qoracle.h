@@ -13,7 +13,8 @@ typedef struct qo_state qo_state;
  * temperature, as md_run does before its loop. */
 qo_state *qo_create(const qb_sysview *s, int history_capacity);
 void qo_destroy(qo_state *st);
-/* nsteps passes of the md_run loop body; returns 0 or 5 (SHAKE failure). */
+/* nsteps passes of the md_run loop body; returns 0, 5 (SHAKE failure) or 10
+ * (a volume move left the box too small for a cut-off). */
 int qo_run(qo_state *st, int nsteps);
 /* post-loop list rebuild and potential evaluation */
 int qo_final_energy(qo_state *st);
@@ -29,4 +30,7 @@ int qo_history(const qo_state *st, int kind, int *steps, double *E, double *EQ);
 int qo_offdiag(const qo_state *st, int kind, double *rkl);
 void qo_list_counts(const qo_state *st, int *out);
 int qo_status(const qo_state *st);
+/* periodic box: edge lengths then centre; Monte Carlo volume moves tried and accepted */
+void qo_box(const qo_state *st, double *box6);
+void qo_volume_moves(const qo_state *st, long long *tries, long long *accepted);
 #endif

@@ -122,6 +122,7 @@ def _load():
         "qb_batch_set_velocities_all": (C.c_int, [vp, dp]),
         "qb_batch_history_all": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_int), dp, C.POINTER(C.c_size_t)]),
         "qb_batch_step_count": (C.c_int, [vp, C.POINTER(C.c_longlong)]),
+        "qb_batch_box": (C.c_int, [vp, C.c_int, dp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
         "qb_batch_run_timed": (C.c_int, [vp, C.c_int, dp, C.POINTER(C.c_longlong)]),
         "qb_peak_flops": (C.c_int, [C.c_int, C.c_int, dp]),
         "qb_batch_energies": (C.c_int, [vp, C.c_int, dp, dp]),
@@ -145,6 +146,7 @@ def _load():
         "qb_batch_workload": (C.c_int, [vp, dp, C.c_int]),
         "qb_batch_destroy": (None, [vp]),
         "qb_write_re": (C.c_int, [C.c_char_p, C.c_int, dp, dp, C.c_int, fp]),
+        "qb_write_re_box": (C.c_int, [C.c_char_p, C.c_int, dp, dp, C.c_int, fp, dp]),
         "qb_append_en": (C.c_int, [C.c_char_p, C.c_int, dp]),
         "qb_append_en_offd": (C.c_int, [C.c_char_p, C.c_int, dp, C.c_int, ip, dp]),
         "qb_fep_analyze": (C.c_int, [dp, ip, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),

@@ -207,6 +207,18 @@ class Batch:
         check(lib.qb_batch_step_count(self._b, C.byref(n)))
         return n.value
 
+    def box(self, sys: int) -> np.ndarray:
+        """Periodic box of system `sys`: edge lengths, then centre."""
+        out = np.zeros(6)
+        check(lib.qb_batch_box(self._b, sys, _dp(out), None, None))
+        return out
+
+    def volume_moves(self, sys: int) -> tuple[int, int]:
+        """Monte Carlo volume moves (tried, accepted) of a constant-pressure run."""
+        t, a = C.c_longlong(), C.c_longlong()
+        check(lib.qb_batch_box(self._b, sys, _dp(np.zeros(6)), C.byref(t), C.byref(a)))
+        return t.value, a.value
+
     def theta_corr(self, sys: int, n: int = 4) -> np.ndarray:
         out = np.zeros(n, dtype=np.float32)
         check(lib.qb_batch_get_theta_corr(self._b, sys, out.ctypes.data_as(C.POINTER(C.c_float)), n))
@@ -310,13 +322,20 @@ def peak_tflops(precision: int = FP64, device: int = 0) -> float:
     return t.value
 
 
-def write_restart(path: str, x: np.ndarray, v: np.ndarray, theta_corr: np.ndarray | None = None) -> None:
+def write_restart(path: str, x: np.ndarray, v: np.ndarray, theta_corr: np.ndarray | None = None,
+                  box: np.ndarray | None = None) -> None:
+    """qdyn's restart file; box: a periodic box's edge lengths and centre
+    (6 values), written as its two trailing records."""
     x = np.ascontiguousarray(x, dtype=np.float64)
     v = np.ascontiguousarray(v, dtype=np.float64)
     ns = 0 if theta_corr is None else int(theta_corr.size)
     tc = None if theta_corr is None else np.ascontiguousarray(theta_corr, dtype=np.float32)
-    check(lib.qb_write_re(path.encode(), x.size // 3, _dp(x), _dp(v), ns,
-                          tc.ctypes.data_as(C.POINTER(C.c_float)) if tc is not None else None))
+    tcp = tc.ctypes.data_as(C.POINTER(C.c_float)) if tc is not None else None
+    if box is None:
+        check(lib.qb_write_re(path.encode(), x.size // 3, _dp(x), _dp(v), ns, tcp))
+    else:
+        b6 = np.ascontiguousarray(box, dtype=np.float64)
+        check(lib.qb_write_re_box(path.encode(), x.size // 3, _dp(x), _dp(v), ns, tcp, _dp(b6)))
 
 
 def append_energy(path: str, EQ: np.ndarray, offd=None) -> None:

@@ -94,6 +94,12 @@ int qb_write_re(const char *path, int natom, const double *x, const double *v, i
   return guarded([&] { qb::write_restart(path, natom, x, v, nshell, theta_corr); });
 }
 
+int qb_write_re_box(const char *path, int natom, const double *x, const double *v, int nshell,
+                    const float *theta_corr, const double *box6) {
+  if (!path || natom <= 0 || !x || !v || !box6) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
+  return guarded([&] { qb::write_restart(path, natom, x, v, nshell, theta_corr, box6); });
+}
+
 int qb_append_en(const char *path, int nstates, const double *EQ) {
   if (!path || nstates < 0 || (nstates > 0 && !EQ)) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
   return guarded([&] { qb::append_energy_frame(path, nstates, EQ, 0, nullptr, nullptr); });

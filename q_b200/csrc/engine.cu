@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -85,6 +86,12 @@ struct Batch {
   long long istep = 0;
   int max_natom = 0, max_lrf_blocks = 1, max_nsol = 0, max_nwat = 0, max_ncgp = 0, max_ncgp_sol = 0, max_terms = 0, max_pp = 0, max_ncgp_sol_w = 0, max_qp = 0;
   bool any_any_atom = false;   // a system with any-atom charge-group cut-offs (iuse_switch_atom 0)
+  // periodic box: any system in a box, putting molecules back, at constant pressure
+  bool any_box = false, any_put = false, any_npt = false;
+  // per system: randm's sequence (md.f90:14408, shared with the Maxwell
+  // velocities) and the volume moves tried and accepted (md.f90:15812-15816)
+  struct McState { bool started = false; int irand = 0; long long tries = 0, accepted = 0; };
+  std::vector<McState> mc;
   int ww_wpb = WW_WPB;          // waters per block of the water-water kernels
   bool any_lrf = false, any_q = false, any_shake = false, any_wpol = false, any_prestr = false, any_qq = false,
        any_qb = false, any_hlj = false;
@@ -179,12 +186,15 @@ struct Batch {
 
   // Pair lists and LRF multipoles of the systems due at this step
   // (force: every system, as the post-loop rebuild).
-  void build_lists(int force) {
+  // put: molecules of periodic boxes go back into the box first at the list
+  // steps (md_run, md.f90:4009-4013).
+  void build_lists(int force, bool put = false) {
     DevPtrs &p = P;
     dim3 b256(256);
     // main: Q-atom and solute lists; side 0: group centres and LRF multipoles;
     // side 1: water-water list
     cudaStream_t s1 = forking() ? side[0] : stream, s2 = forking() ? side[1] : stream;
+    if (put && any_put) launch("put_back_in_box", [&] { k_put_back_in_box<<<nsys, 256, 0, stream>>>(p); });
     launch("lists_begin", [&] { k_lists_begin<<<cdiv(nsys, 128), 128, 0, stream>>>(p, force); });
     // group centres and radii first: the LRF gather and the any-atom list
     // tests read them
@@ -193,8 +203,10 @@ struct Batch {
     fork_streams();
     if (any_lrf) {
       launch("lrf_gather", [&] {
-        if (opt.precision == QB_MIXED)
-          k_lrf_gather_x2<<<dim3(max_lrfx_blocks, nsys), LRFX_BLOCK, 0, s1>>>(p, force);
+        if (opt.precision == QB_MIXED && any_box)
+          k_lrf_gather_x2<true><<<dim3(max_lrfx_blocks, nsys), LRFX_BLOCK, 0, s1>>>(p, force);
+        else if (opt.precision == QB_MIXED)
+          k_lrf_gather_x2<false><<<dim3(max_lrfx_blocks, nsys), LRFX_BLOCK, 0, s1>>>(p, force);
         else
           k_lrf_gather<false><<<dim3(max_lrf_blocks, nsys), LRF_BLOCK, 0, s1>>>(p, force);
       });
@@ -205,7 +217,9 @@ struct Batch {
       launch("list_pp", [&] { k_list_pp<<<dim3(max_ncgp_sol, nsys), 128, 0, stream>>>(p, force); });
       if (max_nwat > 0) launch("list_pw", [&] { k_list_pw<<<dim3(cdiv(max_ncgp_sol, 4), nsys), 128, 0, stream>>>(p, force); });
     }
-    if (any_q) {
+    // a volume move rebuilds the LRF and the solute and water lists, not the
+    // Q-atom lists (md.f90:15734-15744)
+    if (any_q && force != 2) {
       launch("list_qp", [&] { k_list_qp<<<nsys, 256, 0, stream>>>(p, force); });
       if (max_nwat > 0) launch("list_qw", [&] { k_list_qw<<<nsys, 256, 0, stream>>>(p, force); });
     }
@@ -323,8 +337,10 @@ struct Batch {
       // hydrogen LJ: the whole batch takes the variant (exact zeros for systems without)
       if (fast_ww && any_hlj) {
         launch("nb_ww", [&] { k_nb_ww<true, true><<<gw, WW_BLOCK, smem, stream>>>(p, wpb); });
+      } else if (fast_ww && any_box) {
+        launch("nb_ww_x2", [&] { k_nb_ww_x2<true><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb); });
       } else if (fast_ww) {
-        launch("nb_ww_x2", [&] { k_nb_ww_x2<<<gw, WWX_BLOCK, smem, stream>>>(p, wpb); });
+        launch("nb_ww_x2", [&] { k_nb_ww_x2<false><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb); });
       } else if (any_hlj) {
         launch("nb_ww", [&] { k_nb_ww<false, true><<<gw, WW_BLOCK, smem, stream>>>(p, wpb); });
       } else {
@@ -378,7 +394,7 @@ struct Batch {
   void step() {
     int due = lists_due() ? 1 : 0;
     if (lists_stale) {
-      build_lists(1);
+      build_lists(1, true);
       lists_stale = false;
       due = 0;
     }
@@ -413,14 +429,210 @@ struct Batch {
     for (int k = 0; k < nsteps; k++) {
       force_energy = k == nsteps - 1;
       step();
+      if (any_npt) mc_volume(istep - 1);
     }
     force_energy = false;
+  }
+
+  // randm (md.f90:14408-14442): the system's one sequence, seeded by the
+  // first call's argument
+  static double randm(McState &m, int seed) {
+    const int M = 100000000, M1 = 10000, MULT = 31415821;
+    if (!m.started) { m.started = true; m.irand = std::abs(seed) % M; }
+    const int ih = m.irand / M1, il = m.irand % M1;
+    int r = ((ih * (MULT % M1) + il * (MULT / M1)) % M1) * M1 + il * (MULT % M1);
+    r = (r + 1) % M;
+    m.irand = r;
+    float v = (float)(r / 10) * 10.0f / (float)M;
+    if (v <= 0.0f || v > 1.0f) v = 0.0f;
+    return (double)v;
+  }
+
+  // new_potential's total (md.f90:15968-15971): the bonded terms of the
+  // step's energies `old` with the nonbonded, restraint and LRF terms of `e`
+  static double new_potential(const double *old, const double *e) {
+    return old[QB_E_P_BOND] + old[QB_E_W_BOND] + old[QB_E_P_ANGLE] + old[QB_E_W_ANGLE] + old[QB_E_P_TORSION] +
+           old[QB_E_P_IMPROPER] + e[QB_E_PP_EL] + e[QB_E_PP_VDW] + e[QB_E_PW_EL] + e[QB_E_PW_VDW] + e[QB_E_WW_EL] +
+           e[QB_E_WW_VDW] + old[QB_E_Q_BOND] + old[QB_E_Q_ANGLE] + old[QB_E_Q_TORSION] + old[QB_E_Q_IMPROPER] +
+           e[QB_E_QX_EL] + e[QB_E_QX_VDW] + e[QB_E_RST_PROTEIN] + e[QB_E_LRF];
+  }
+
+  // Energies of the current coordinates as new_potential takes them: the full
+  // evaluation (the lists as they stand), summed; E and EQ copied out.
+  void evaluate_into(std::vector<double> &E, std::vector<double> &EQ) {
+    pot_energy(1);
+    k_finish<<<nsys, 32, 0, stream>>>(P, 2);
+    check_launch("energy sums");
+    E.resize((size_t)nsys * QB_NE);
+    EQ.resize((size_t)nsys * MAXS * QB_NEQ);
+    CUDA_TRY(cudaMemcpyAsync(E.data(), P.E, sizeof(double) * E.size(), cudaMemcpyDeviceToHost, stream));
+    CUDA_TRY(cudaMemcpyAsync(EQ.data(), P.EQ, sizeof(double) * EQ.size(), cudaMemcpyDeviceToHost, stream));
+    CUDA_TRY(cudaStreamSynchronize(stream));
+  }
+
+  // MC_volume (md.f90:15615-15840) after step `done` for every system at
+  // constant pressure whose volume_change interval divides it: the energy of
+  // the current coordinates, a random volume change, every molecule's centre
+  // of mass scaled with the box, the LRF and the solute and water lists
+  // rebuilt (with LRF), the energy again, and Metropolis acceptance of
+  // dW = dE + p dV - N kT ln(V'/V); a rejected move restores coordinates, box
+  // and LRF.  The energies that step records (output, energy file) become
+  // the accepted configuration's, as the reference writes E and EQ after the
+  // move.  Runs on the host between graph launches, with the device
+  // evaluations batched over all systems.
+  void mc_volume(long long done) {
+    std::vector<int> M;
+    for (int s = 0; s < nsys; s++) {
+      const qb_sysview &V = views[s];
+      if (V.use_pbc && V.constant_pressure && V.ivolume_cycle > 0 && done > 0 && done % V.ivolume_cycle == 0)
+        M.push_back(s);
+    }
+    if (M.empty()) return;
+    if (mc.size() != (size_t)nsys) mc.resize(nsys);
+    std::vector<SysState> st(nsys);
+    CUDA_TRY(cudaMemcpyAsync(st.data(), P.st, sizeof(SysState) * nsys, cudaMemcpyDeviceToHost, stream));
+    // the step's energies: bonded terms of the totals, and what every other
+    // system keeps
+    std::vector<double> E0((size_t)nsys * QB_NE), EQ0((size_t)nsys * MAXS * QB_NEQ);
+    CUDA_TRY(cudaMemcpyAsync(E0.data(), P.E, sizeof(double) * E0.size(), cudaMemcpyDeviceToHost, stream));
+    CUDA_TRY(cudaMemcpyAsync(EQ0.data(), P.EQ, sizeof(double) * EQ0.size(), cudaMemcpyDeviceToHost, stream));
+    CUDA_TRY(cudaStreamSynchronize(stream));
+    std::vector<int> live;
+    for (int s : M)
+      if (st[s].status == 0) live.push_back(s);
+    if (live.empty()) return;
+    // first new_potential: the coordinates after the step
+    std::vector<double> E1, EQ1, E2, EQ2;
+    evaluate_into(E1, EQ1);
+    // backups of the moving systems: coordinates and LRF records
+    const size_t ax = (size_t)P.natoms_tot, lx = (size_t)P.ncgp_tot * LRF_STRIDE;
+    if (!mc_x) {
+      mc_x = dev_alloc<double4>(ax, owned);
+      mc_lrf = dev_alloc<double>(std::max<size_t>(lx, 1), owned);
+    }
+    std::vector<double> dV(nsys, 0.0), oldV(nsys, 0.0);
+    for (int s : live) {
+      const SysDev &S = sysh[s];
+      const qb_sysview &V = views[s];
+      McState &m = mc[s];
+      if (!m.started && V.randm_started) { m.started = true; m.irand = V.randm_state; }
+      CUDA_TRY(cudaMemcpyAsync(mc_x + S.aoff, P.x + S.aoff, sizeof(double4) * S.natom, cudaMemcpyDeviceToDevice, stream));
+      if (S.use_lrf)
+        CUDA_TRY(cudaMemcpyAsync(mc_lrf + (size_t)S.coff * LRF_STRIDE, P.lrf + (size_t)S.coff * LRF_STRIDE,
+                                 sizeof(double) * S.ncgp * LRF_STRIDE, cudaMemcpyDeviceToDevice, stream));
+      SysState &t = st[s];
+      const double old_V = t.boxl[0] * t.boxl[1] * t.boxl[2];
+      double r = randm(m, V.pressure_seed);
+      r = r * 2 - 1;
+      const double deltaV = r * V.max_vol_displ, new_V = deltaV + old_V;
+      const double ratio = std::pow(new_V / old_V, (double)(1.0f / 3.0f));
+      for (int k = 0; k < 3; k++) {
+        t.mc_oldl[k] = t.boxl[k];
+        t.boxl[k] = t.boxl[k] * ratio;
+        t.iboxl[k] = 1.0 / t.boxl[k];
+      }
+      const double bmin = std::min(t.boxl[0], std::min(t.boxl[1], t.boxl[2]));
+      const char *why = !(bmin > V.Rcpp * 2)    ? "Solute-solute cut-off radii too large"
+                        : !(bmin > V.Rcww * 2)  ? "Solvent-solvent cut-off radii too large"
+                        : !(bmin > V.Rcpw * 2)  ? "Solute-solvent cut-off radii too large"
+                        : !(bmin > V.Rcq * 2)   ? "Q-atom cut-off radii too large"
+                        : !(bmin > V.RcLRF * 2) ? "LRF cut-off radii too large"
+                                                : nullptr;
+      if (why) {
+        char buf[200];
+        std::snprintf(buf, sizeof buf, "system %d, volume move after step %lld: %s", s, done, why);
+        fail(QB_ERR_STATE, buf);
+      }
+      t.mc = 1;
+      dV[s] = deltaV;
+      oldV[s] = old_V;
+      put_box(s, t);
+    }
+    CUDA_TRY(cudaStreamSynchronize(stream));   // st (host) is the source of the copies above
+    launch("mc_scale", [&] { k_mc_scale<<<dim3(cdiv(max_nmol, 128), nsys), 128, 0, stream>>>(P); });
+    bool lrf_any = false;
+    for (int s : live) lrf_any |= sysh[s].use_lrf != 0;
+    if (lrf_any) build_lists(2);
+    // second new_potential: the trial box
+    evaluate_into(E2, EQ2);
+    std::vector<double> Efin = E0, EQfin = EQ0;
+    for (int s : live) {
+      const qb_sysview &V = views[s];
+      McState &m = mc[s];
+      const double *e0 = &E0[(size_t)s * QB_NE];
+      const double p1 = new_potential(e0, &E1[(size_t)s * QB_NE]), p2 = new_potential(e0, &E2[(size_t)s * QB_NE]);
+      SysState &t = st[s];
+      const double newV = oldV[s] + dV[s];
+      const double deltaE = p2 - p1;
+      const double deltaW = deltaE + V.pressure * dV[s] -
+                            (double)((float)V.nmol * kBoltz) * V.Temp0 * std::log(newV / oldV[s]);
+      bool acc = true;
+      if (deltaW > 0.0) {
+        const double u = randm(m, V.pressure_seed);
+        acc = !(u > std::exp(-deltaW / (double)kBoltz / V.Temp0));
+      }
+      m.tries++;
+      if (acc) m.accepted++;
+      const std::vector<double> &Es = acc ? E2 : E1, &EQs = acc ? EQ2 : EQ1;
+      const double pot = acc ? p2 : p1;
+      // the fields new_potential writes (md.f90:15858-15971)
+      double *ef = &Efin[(size_t)s * QB_NE];
+      const double *es = &Es[(size_t)s * QB_NE];
+      for (int k : {QB_E_PP_EL, QB_E_PP_VDW, QB_E_PW_EL, QB_E_PW_VDW, QB_E_WW_EL, QB_E_WW_VDW, QB_E_QX_EL, QB_E_QX_VDW,
+                    QB_E_RST_PROTEIN, QB_E_LRF})
+        ef[k] = es[k];
+      ef[QB_E_POTENTIAL] = pot;
+      for (int q = 0; q < V.nstates; q++) {
+        double *qf = &EQfin[((size_t)s * MAXS + q) * QB_NEQ];
+        const double *qs = &EQs[((size_t)s * MAXS + q) * QB_NEQ];
+        for (int k : {QB_EQ_QQ_EL, QB_EQ_QQ_VDW, QB_EQ_QP_EL, QB_EQ_QP_VDW, QB_EQ_QW_EL, QB_EQ_QW_VDW, QB_EQ_QX_EL,
+                      QB_EQ_QX_VDW, QB_EQ_RESTRAINT})
+          qf[k] = qs[k];
+      }
+      const SysDev &S = sysh[s];
+      if (!acc) {
+        CUDA_TRY(cudaMemcpyAsync(P.x + S.aoff, mc_x + S.aoff, sizeof(double4) * S.natom, cudaMemcpyDeviceToDevice, stream));
+        if (S.use_lrf)
+          CUDA_TRY(cudaMemcpyAsync(P.lrf + (size_t)S.coff * LRF_STRIDE, mc_lrf + (size_t)S.coff * LRF_STRIDE,
+                                   sizeof(double) * S.ncgp * LRF_STRIDE, cudaMemcpyDeviceToDevice, stream));
+        for (int k = 0; k < 3; k++) { t.boxl[k] = t.mc_oldl[k]; t.iboxl[k] = 1.0 / t.boxl[k]; }
+      }
+      t.mc = 0;
+      put_box(s, t);
+      // the step's records take the final energies
+      for (int kind = 0; kind < 2; kind++) {
+        const int cyc = kind == 0 ? V.iout_cycle : V.iene_cycle;
+        if (cyc <= 0 || done % cyc != 0 || (kind == 1 && done == 0)) continue;
+        const int c = t.hist_n[kind] - 1;
+        if (c < 0 || c >= P.hist_cap) continue;
+        double *r = P.hist + (((size_t)kind * nsys + s) * P.hist_cap + c) * HIST_REC;
+        CUDA_TRY(cudaMemcpyAsync(r + 1, ef, sizeof(double) * QB_NE, cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(cudaMemcpyAsync(r + 1 + QB_NE, &EQfin[(size_t)s * MAXS * QB_NEQ], sizeof(double) * MAXS * QB_NEQ,
+                                 cudaMemcpyHostToDevice, stream));
+      }
+    }
+    // every system's E and EQ as the step (and the moves) left them
+    CUDA_TRY(cudaMemcpyAsync(P.E, Efin.data(), sizeof(double) * Efin.size(), cudaMemcpyHostToDevice, stream));
+    CUDA_TRY(cudaMemcpyAsync(P.EQ, EQfin.data(), sizeof(double) * EQfin.size(), cudaMemcpyHostToDevice, stream));
+    CUDA_TRY(cudaStreamSynchronize(stream));   // the host vectors are the copies' sources
+  }
+  double4 *mc_x = nullptr;
+  double *mc_lrf = nullptr;
+  int max_nmol = 0;
+
+  // the box fields of system s's device state (edge lengths, inverses,
+  // centre, volume-move flag and old lengths), leaving the rest as the
+  // device has it
+  void put_box(int s, const SysState &t) {
+    const size_t off = offsetof(SysState, boxl), len = sizeof(SysState) - off;
+    CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<char *>(P.st + s) + off, reinterpret_cast<const char *>(&t) + off, len,
+                             cudaMemcpyHostToDevice, stream));
   }
 
   // The kernels of one MD step (md_run's loop body, md.f90:4003-4175).
   void step_kernels(int due, int ene) {
     DevPtrs &p = P;
-    if (due) build_lists(0);
+    if (due) build_lists(0, true);
     pot_energy(ene);
     // 3-constraint molecules (waters) take leapfrog and SHAKE in one pass; the
     // other atoms leapfrog, then the general SHAKE; the two paths move
@@ -456,11 +668,6 @@ struct Batch {
 
 namespace {
 
-double d2(const double *x, int a, int b) {
-  double s = 0;
-  for (int k = 0; k < 3; k++) { double t = x[3 * a + k] - x[3 * b + k]; s += t * t; }
-  return s;
-}
 
 void build(Batch &B, qb_handle *const *hs, int n) {
   B.nsys = n;
@@ -503,12 +710,15 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   std::vector<int4> rd; std::vector<double4> rd_p;
   std::vector<int4> ra; std::vector<double2> ra_p;
   std::vector<int4> rw; std::vector<double4> rw_p;
+  std::vector<int> mol_first; std::vector<double> mol_minv, mass_box;
   std::vector<SysState> sst(n);
   B.sysh.resize(n);
   int ww_cap = 64;
   long long pp_tot = 0, qp_tot = 0, qw_tot = 0;
   int ncgp_sol_tot = 0, pwg_cap = 32;
 
+  std::vector<SysState> st_box(n);
+  std::memset(st_box.data(), 0, sizeof(SysState) * n);
   for (int s = 0; s < n; s++) {
     const qb_sysview &V = B.views[s];
     SysDev &S = B.sysh[s];
@@ -749,12 +959,61 @@ void build(Batch &B, qb_handle *const *hs, int n) {
       S.bH[0] = V.type_bvdw[3 * V.iac_hw]; S.bH[1] = V.type_bvdw[3 * V.iac_hw + 1];
     }
     SysState &st = sst[s];
-    std::memset(&st, 0, sizeof st);
+    {
+      const SysState keep = st_box[s];
+      std::memset(&st, 0, sizeof st);
+      for (int k = 0; k < 3; k++) { st.boxl[k] = keep.boxl[k]; st.iboxl[k] = keep.iboxl[k]; st.boxc[k] = keep.boxc[k]; }
+    }
     st.Tscale_sol = st.Tscale_solv = 1.0;
     for (int k = 0; k < S.nshell; k++) st.theta_corr[k] = V.wshell_theta_corr0[k];
+    // periodic box (use_PBC, md.f90:4000-4200): box, Q switching atom and
+    // molecule tables; any-atom cut-offs stay sphere-only here
+    S.pbc = V.use_pbc ? 1 : 0;
+    for (int k = 0; k < 3; k++) S.origin[k] = V.xpcent[k];
+    if (S.pbc) {
+      if (V.iuse_switch_atom != 1)
+        fail(QB_ERR_UNSUPPORTED, "any-atom charge-group cut-offs (iuse_switch_atom 0) in a periodic box are not supported");
+      if (V.nqat > 0 && V.qswitch < 0) fail(QB_ERR_PARSE, "a periodic box needs the Q atoms' switching atom");
+      S.qswitch = V.qswitch >= 0 ? aoff + V.qswitch : aoff;
+      S.qp_once = 0;
+      S.rigid_center = V.rigid_box_center;
+      for (int k = 0; k < 3; k++) {
+        st_box[s].boxl[k] = V.boxlength[k];
+        st_box[s].iboxl[k] = 1.0 / V.boxlength[k];
+        st_box[s].boxc[k] = V.boxcenter[k];
+        S.origin[k] = V.boxcenter[k];
+      }
+      S.mol_off = (int)mol_first.size();
+      S.nmol = V.nmol;
+      for (int m = 0; m <= V.nmol; m++) mol_first.push_back(aoff + V.istart_mol[m]);
+      for (int m = 0; m < V.nmol; m++) mol_minv.push_back(V.mol_mass_inv[m]);
+      // put_back_in_box's molecule range (md.f90:15529-15536): the solvent
+      // molecules are the last (natom - nat_solute) / (atoms of the last one)
+      S.put_first = 0; S.put_last = 0;
+      if ((V.put_solute_back_in_box || V.put_solvent_back_in_box) && V.nmol > 1) {
+        const int nsolv = (V.natom - V.nat_solute) / (V.istart_mol[V.nmol - 1] - V.istart_mol[V.nmol - 2]);
+        S.put_first = V.put_solute_back_in_box ? 0 : V.nmol - nsolv;
+        S.put_last = V.put_solvent_back_in_box ? V.nmol : V.nmol - nsolv;
+        if (S.put_first < S.put_last) B.any_put = true;
+      }
+      B.any_box = true;
+      if (V.constant_pressure) B.any_npt = true;
+    }
+    for (int i = 0; i < V.natom; i++) mass_box.push_back(S.pbc ? V.mass_box[i] : V.mass[i]);
     // list capacities from the starting coordinates, with margins for motion
+    // (distances of the nearest image in a periodic box)
     {
       const double *X = V.x0;
+      const bool pb = S.pbc != 0;
+      auto d2 = [&](const double *x, int a, int b) {
+        double t = 0;
+        for (int k = 0; k < 3; k++) {
+          double d = x[3 * a + k] - x[3 * b + k];
+          if (pb) d -= V.boxlength[k] * std::round(d / V.boxlength[k]);
+          t += d * d;
+        }
+        return t;
+      };
       long long pp = 0;
       int pwmax = 0;
       double rpp = V.Rcpp + 3.0, rpw = V.Rcpw + 3.0, rww = V.Rcww + 2.0;
@@ -834,7 +1093,9 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     B.any_qq |= S.nqq > 0;
     B.any_qb |= (V.nqbond + V.nqangle + V.nqtor + V.nqimp + V.noffd) > 0;   // the Q-bonded block also takes r_kl
     B.any_hlj |= V.nwat > 0 && V.ww_hlj;
+    if (S.pbc) B.max_nmol = std::max(B.max_nmol, V.nmol);
   }
+  B.mc.assign(n, Batch::McState{});
   // water offsets
   int woff = 0;
   for (int s = 0; s < n; s++) { B.sysh[s].woff = woff; woff += B.sysh[s].nwat; }
@@ -955,6 +1216,9 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     if (P.nshg > 0)
       CUDA_TRY(cudaFuncSetAttribute(k_shake_general, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
   }
+  if (mol_first.empty()) mol_first.push_back(0);
+  if (mol_minv.empty()) mol_minv.push_back(0.0);
+  P.mol_first = dev_upload(mol_first, o); P.mol_minv = dev_upload(mol_minv, o); P.mass_box = dev_upload(mass_box, o);
   P.rs = dev_upload(rs, o); P.rs_fk = dev_upload(rs_fk, o); P.rp = dev_upload(rp, o); P.rp_x = dev_upload(rp_x, o);
   P.rp_fk = dev_upload(rp_fk, o); P.rd = dev_upload(rd, o); P.rd_p = dev_upload(rd_p, o);
   P.ra = dev_upload(ra, o); P.ra_p = dev_upload(ra_p, o); P.rw = dev_upload(rw, o); P.rw_p = dev_upload(rw_p, o);
@@ -1006,7 +1270,8 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem64));
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem64));
-  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
   P.kin_nblk = std::max(1, (B.max_natom + KIN_BLOCK - 1) / KIN_BLOCK);
   P.kin = dev_alloc<double>((size_t)n * 4, o);
   P.E = dev_alloc<double>((size_t)n * QB_NE, o);
@@ -1501,6 +1766,20 @@ int qb_batch_step_count(qb_batch *bb, long long *out) {
   if (!bb || !out) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
   *out = bb->b.istep;
   return QB_OK;
+}
+
+int qb_batch_box(qb_batch *bb, int sys, double *box6, long long *tries, long long *accepted) {
+  if (int rc = sys_check(bb, sys)) return rc;
+  if (!box6) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
+  return guarded_batch([&] {
+    qb::SysState st;
+    CUDA_TRY(cudaStreamSynchronize(bb->b.stream));
+    CUDA_TRY(cudaMemcpy(&st, bb->b.P.st + sys, sizeof st, cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 3; k++) { box6[k] = st.boxl[k]; box6[3 + k] = st.boxc[k]; }
+    const bool have = bb->b.mc.size() > (size_t)sys;
+    if (tries) *tries = have ? bb->b.mc[sys].tries : 0;
+    if (accepted) *accepted = have ? bb->b.mc[sys].accepted : 0;
+  });
 }
 
 int qb_batch_get_theta_corr(qb_batch *bb, int sys, float *out, int n) {

@@ -72,6 +72,13 @@ struct SysDev {
   // 1: solute charge-group cut-offs on switch atoms (nbpplist_lrf ...); 0: on
   // any atom pair (nbpplis2_lrf, nbpwlis2_lrf, nbqplis2: iuse_switch_atom 0)
   int switch_atoms;
+  // periodic box (use_PBC): every pair takes the nearest image of its charge
+  // groups' switching atoms; the Q-atom lists centre on atom qswitch
+  int pbc, qswitch;
+  int mol_off, nmol;              // molecules: P.mol_first[mol_off .. mol_off + nmol] (global atoms, + end)
+  int put_first, put_last;        // molecules put back in the box, [first, last)
+  int rigid_center;               // box centre fixed (rigid_box_center)
+  double origin[3];               // FP32 coordinate origin of the mixed kernels (sphere: solute centre)
 };
 
 // Per-system state written by the device.
@@ -85,6 +92,13 @@ struct SysState {
   int frozen;
   int shake_its_max;                 // most SHAKE iterations of one molecule since the counters were reset
   unsigned long long shake_its;      // SHAKE iterations summed over molecules and steps
+  // periodic box: edge lengths, their inverses (1/L in FP64) and centre;
+  // volume move in progress (mc: 1 while the trial box is evaluated) and the
+  // edge lengths before it.  The last fields of the record: the host writes
+  // them as one block.
+  double boxl[3], iboxl[3], boxc[3];
+  int mc;
+  double mc_oldl[3];
 };
 
 struct DevPtrs {
@@ -174,6 +188,9 @@ struct DevPtrs {
   // history [kind][s][rec][QB_NE + MAXS*QB_NEQ + 1]
   double *hist;
   int hist_cap;
+  // periodic box: molecule starts, 1/molecule mass, per-atom mass (1/winv)
+  int *mol_first;
+  double *mol_minv, *mass_box;
 };
 
 }  // namespace qb

@@ -44,11 +44,43 @@ __device__ __forceinline__ void set_status(SysState *st, int code) { atomicCAS(&
 
 __device__ __forceinline__ double dev_pi() { return (double)(4.0f * atanf(1.0f)); }
 
+// ------------------------------------------------------------ periodic box
+
+// Edge lengths and their inverses of system s's box.  The nearest image of a
+// displacement d along an edge is d - L nint(d / L), written as the reference
+// writes it, boxlength * nint(d * inv_boxl) (md.f90:5352-5354, 10513-10519);
+// nint rounds halves away from zero, as round() does.
+struct BoxD { double L[3], iL[3]; };
+
+__device__ __forceinline__ BoxD box_of(const DevPtrs &P, int s) {
+  const SysState &st = P.st[s];
+  BoxD b;
+#pragma unroll
+  for (int k = 0; k < 3; k++) { b.L[k] = st.boxl[k]; b.iL[k] = st.iboxl[k]; }
+  return b;
+}
+
+// the lattice vector L nint(d / L) that brings d to its nearest image
+__device__ __forceinline__ double3 image_shift(const BoxD &b, double dx, double dy, double dz) {
+  return make_double3(b.L[0] * round(dx * b.iL[0]), b.L[1] * round(dy * b.iL[1]), b.L[2] * round(dz * b.iL[2]));
+}
+
+__device__ __forceinline__ void min_image(const BoxD &b, double &dx, double &dy, double &dz) {
+  const double3 t = image_shift(b, dx, dy, dz);
+  dx -= t.x; dy -= t.y; dz -= t.z;
+}
+
+// the switching atom of an atom's charge group
+__device__ __forceinline__ int switch_of(const DevPtrs &P, int a) { return P.cg_sw[P.cgp[a]]; }
+
 // ------------------------------------------------------------------ lists
 
 // Lists of system s are rebuilt at steps that are multiples of its non_bond
 // interval (md.f90:4005), or on request (the post-loop rebuild, md.f90:4186).
+// force 2: the systems in a volume move (MC_volume rebuilds their LRF and
+// pair lists for the trial box, md.f90:15734-15744).
 __device__ __forceinline__ bool list_due(const DevPtrs &P, int s, int force) {
+  if (force == 2) return P.st[s].mc != 0;
   return force || (P.st[s].istep % P.sys[s].NB) == 0;
 }
 
@@ -298,9 +330,15 @@ __global__ void __launch_bounds__(LRF_BLOCK, MIXED ? 8 : 5) k_lrf_gather(DevPtrs
     cx = L[0]; cy = L[1]; cz = L[2];
     xs = ld3(P.x, swg);
   }
-  const double ox = MIXED ? S.xp[0] : 0.0, oy = MIXED ? S.xp[1] : 0.0, oz = MIXED ? S.xp[2] : 0.0;
+  const double ox = MIXED ? S.origin[0] : 0.0, oy = MIXED ? S.origin[1] : 0.0, oz = MIXED ? S.origin[2] : 0.0;
   const R ccx = (R)(cx - ox), ccy = (R)(cy - oy), ccz = (R)(cz - oz);
   const bool g_sol = gl < S.ncgp_sol;
+  // periodic box: pair windows on the switching atoms' nearest image; a
+  // source group's charges enter at the image nearest the target centre
+  // (nbpplist_box_lrf md.f90:5751-5849, nbpwlist_box_lrf 7111-7245,
+  // nbwwlist_box_lrf 8601-8694)
+  const bool box = S.pbc != 0;
+  const BoxD bx = box_of(P, s);
   // FP64 totals: registers (FP64 path) or this thread's column in shared memory (mixed)
   __shared__ double mtot[MIXED ? 24 : 1][MIXED ? LRF_BLOCK : 1];
   double m[MIXED ? 1 : 20];
@@ -352,30 +390,35 @@ __global__ void __launch_bounds__(LRF_BLOCK, MIXED ? 8 : 5) k_lrf_gather(DevPtrs
           if (!lrf_window_any(P, S, g, g_sol, S.coff + tile.x + i, hs.w > 0.0, rc2)) continue;
         } else {
           double dx = xs.x - hs.x, dy = xs.y - hs.y, dz = xs.z - hs.z;
+          if (box) min_image(bx, dx, dy, dz);
           double r2 = dx * dx + dy * dy + dz * dz;
           if (!(r2 > rc2 && r2 <= S.RcLRF2)) continue;
         }
         int2 rg = hrange[i];
+        const double3 sh = box ? image_shift(bx, hs.x - cx, hs.y - cy, hs.z - cz) : make_double3(0, 0, 0);
         if (MIXED) {
           // a zero charge adds exact zeros; water groups (3 atoms) unrolled
+          const R scx = ccx + (R)sh.x, scy = ccy + (R)sh.y, scz = ccz + (R)sh.z;
           if (rg.y == 3) {
 #pragma unroll
             for (int k = 0; k < 3; k++) {
               R4 a = hat[rg.x + k];
-              lrf_accumulate_split((float *)mt, tt, (float)a.w, (float)(a.x - ccx), (float)(a.y - ccy),
-                                   (float)(a.z - ccz));
+              lrf_accumulate_split((float *)mt, tt, (float)a.w, (float)(a.x - scx), (float)(a.y - scy),
+                                   (float)(a.z - scz));
             }
           } else {
             for (int k = 0; k < rg.y; k++) {
               R4 a = hat[rg.x + k];
-              lrf_accumulate_split((float *)mt, tt, (float)a.w, (float)(a.x - ccx), (float)(a.y - ccy),
-                                   (float)(a.z - ccz));
+              lrf_accumulate_split((float *)mt, tt, (float)a.w, (float)(a.x - scx), (float)(a.y - scy),
+                                   (float)(a.z - scz));
             }
           }
         } else {
           for (int k = 0; k < rg.y; k++) {
             R4 a = hat[rg.x + k];
-            if (a.w != R(0)) lrf_accumulate<double>(m, (double)a.w, (double)a.x - cx, (double)a.y - cy, (double)a.z - cz);
+            if (a.w != R(0))
+              lrf_accumulate<double>(m, (double)a.w, (double)a.x - cx - sh.x, (double)a.y - cy - sh.y,
+                                     (double)a.z - cz - sh.z);
           }
         }
       }
@@ -473,6 +516,7 @@ __device__ __forceinline__ void lrf_finish_x2(const float2 *m, const float2 *t, 
 // adds the totals to the FP64 record with one atomic per component.
 constexpr int LRFX_BLOCK = 128, LRFX_TARGETS = 2 * LRFX_BLOCK;
 
+template <bool BOX>
 __global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int force) {
   const int s = blockIdx.y;
   if (!list_due(P, s, force)) return;
@@ -486,30 +530,34 @@ __global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int 
   __shared__ double4 hsw[LRF_TILE_G];
   __shared__ int2 hrange[LRF_TILE_G];
   __shared__ float4 hxy[LRF_TILE_A], hzq[LRF_TILE_A];   // {x, x, y, y}, {z, z, q, q}
-  const double ox = S.xp[0], oy = S.xp[1], oz = S.xp[2];
+  const double ox = S.origin[0], oy = S.origin[1], oz = S.origin[2];
   int gl[2];
   bool act[2], gsol[2];
-  double3 xs[2];
+  double3 xs[2], cen[2];
   float cc[2][3];
 #pragma unroll
   for (int h = 0; h < 2; h++) {
     gl[h] = gchunk * LRFX_TARGETS + h * LRFX_BLOCK + threadIdx.x;
     act[h] = gl[h] < S.ncgp;
     gsol[h] = gl[h] < S.ncgp_sol;
-    xs[h] = make_double3(0, 0, 0);
+    xs[h] = cen[h] = make_double3(0, 0, 0);
     cc[h][0] = cc[h][1] = cc[h][2] = 0.f;
     if (act[h]) {
       const int g = S.coff + gl[h];
       const int swg = P.cg_sw[g];
       act[h] = !(P.flags[swg] & F_EXCL);
       const double *L = P.lrf + (size_t)g * LRF_STRIDE;
+      cen[h] = make_double3(L[0], L[1], L[2]);
       cc[h][0] = (float)(L[0] - ox); cc[h][1] = (float)(L[1] - oy); cc[h][2] = (float)(L[2] - oz);
       xs[h] = ld3(P.x, swg);
     }
   }
-  // minus the two target centres (positions relative to the sphere centre)
-  const float2 ncx = make_float2(-cc[0][0], -cc[1][0]), ncy = make_float2(-cc[0][1], -cc[1][1]),
-               ncz = make_float2(-cc[0][2], -cc[1][2]);
+  // minus the two target centres (positions relative to the origin); in a
+  // periodic box each source group shifts them by its image (nbpplist_box_lrf
+  // md.f90:5751-5849, nbpwlist_box_lrf 7111-7245, nbwwlist_box_lrf 8601-8694)
+  float2 ncx = make_float2(-cc[0][0], -cc[1][0]), ncy = make_float2(-cc[0][1], -cc[1][1]),
+         ncz = make_float2(-cc[0][2], -cc[1][2]);
+  const BoxD bx = box_of(P, s);
   float2 m[20], t[4];
 #pragma unroll
   for (int k = 0; k < 20; k++) m[k] = make_float2(0.f, 0.f);
@@ -553,7 +601,8 @@ __global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int 
           in = act[h] && tile.x + i != gl[h] &&
                lrf_window_any(P, S, S.coff + gl[h], gsol[h], S.coff + tile.x + i, hs.w > 0.0, rc2);
         } else {
-          const double dx = xs[h].x - hs.x, dy = xs[h].y - hs.y, dz = xs[h].z - hs.z;
+          double dx = xs[h].x - hs.x, dy = xs[h].y - hs.y, dz = xs[h].z - hs.z;
+          if (BOX) min_image(bx, dx, dy, dz);
           const double r2 = dx * dx + dy * dy + dz * dz;
           in = act[h] && tile.x + i != gl[h] && r2 > rc2 && r2 <= S.RcLRF2;
         }
@@ -561,6 +610,17 @@ __global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int 
         (h ? sel.y : sel.x) = in ? 1.f : 0.f;
       }
       if (!any) continue;
+      if (BOX) {
+        double3 c[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const double3 sh = image_shift(bx, hs.x - cen[h].x, hs.y - cen[h].y, hs.z - cen[h].z);
+          c[h] = make_double3((cen[h].x - ox) + sh.x, (cen[h].y - oy) + sh.y, (cen[h].z - oz) + sh.z);
+        }
+        ncx = make_float2(-(float)c[0].x, -(float)c[1].x);
+        ncy = make_float2(-(float)c[0].y, -(float)c[1].y);
+        ncz = make_float2(-(float)c[0].z, -(float)c[1].z);
+      }
       const int2 rg = hrange[i];
       const float2 unsel = make_float2(1.f - sel.x, 1.f - sel.y);
       auto atom = [&](int k) {
@@ -618,8 +678,16 @@ __global__ void __launch_bounds__(WL_BLOCK) k_list_ww(DevPtrs P, int force) {
   __shared__ int scnt[WL_WPB];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = WL_BLOCK / 32;
   const int obase = S.aoff + S.nsol;
-  const double cx = S.xw[0], cy = S.xw[1], cz = S.xw[2];
+  const double cx = S.pbc ? S.origin[0] : S.xw[0], cy = S.pbc ? S.origin[1] : S.xw[1],
+               cz = S.pbc ? S.origin[2] : S.xw[2];
   const float rc2 = (float)S.Rcww2;
+  // periodic box (nbwwlist_box, md.f90:8298): O-O distances of the nearest
+  // image; FP32 edge lengths for the scan (the few pairs near the cut-off
+  // are decided in FP64)
+  const bool box = S.pbc != 0;
+  const BoxD bx = box_of(P, s);
+  const float2 bL[3] = {dup2((float)bx.L[0]), dup2((float)bx.L[1]), dup2((float)bx.L[2])};
+  const float2 biL[3] = {dup2((float)bx.iL[0]), dup2((float)bx.iL[1]), dup2((float)bx.iL[2])};
   for (int t = threadIdx.x; t < WL_WPB; t += WL_BLOCK) scnt[t] = 0;
   for (int c0 = 0; c0 < S.nwat; c0 += WL_STAGE) {
     const int cn = min(WL_STAGE, S.nwat - c0);
@@ -645,8 +713,17 @@ __global__ void __launch_bounds__(WL_BLOCK) k_list_ww(DevPtrs P, int force) {
         const int jl0 = b + lane, jl1 = b + 32 + lane;
         if (jl0 < cn) a = so[jl0];
         if (jl1 < cn) e = so[jl1];
-        const float2 dx = __fadd2_rn(make_float2(a.x, e.x), nx), dy = __fadd2_rn(make_float2(a.y, e.y), ny),
-                     dz = __fadd2_rn(make_float2(a.z, e.z), nz);
+        float2 dx = __fadd2_rn(make_float2(a.x, e.x), nx), dy = __fadd2_rn(make_float2(a.y, e.y), ny),
+               dz = __fadd2_rn(make_float2(a.z, e.z), nz);
+        if (box) {
+          auto wrap = [](float2 d, float2 L, float2 iL) {
+            const float2 n = make_float2(rintf(d.x * iL.x), rintf(d.y * iL.y));
+            return __ffma2_rn(make_float2(-n.x, -n.y), L, d);
+          };
+          dx = wrap(dx, bL[0], biL[0]);
+          dy = wrap(dy, bL[1], biL[1]);
+          dz = wrap(dz, bL[2], biL[2]);
+        }
         const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
         bool ok2[2];
 #pragma unroll
@@ -658,7 +735,8 @@ __global__ void __launch_bounds__(WL_BLOCK) k_list_ww(DevPtrs P, int force) {
             if (fabsf(rr - rc2) <= WL_EPS2) {
               // near the cut-off: the reference's FP64 test
               const double3 xj = ld3(P.x, obase + 3 * jw);
-              const double ddx = xi.x - xj.x, ddy = xi.y - xj.y, ddz = xi.z - xj.z;
+              double ddx = xi.x - xj.x, ddy = xi.y - xj.y, ddz = xi.z - xj.z;
+              if (box) min_image(bx, ddx, ddy, ddz);
               ok = ddx * ddx + ddy * ddy + ddz * ddz <= S.Rcww2;
             } else {
               ok = rr < rc2;
@@ -749,20 +827,11 @@ __global__ void k_list_pp(DevPtrs P, int force) {
   int swi = P.cg_sw[gi];
   if (P.flags[swi] & F_EXCL) return;
   double3 xs = ld3(P.x, swi);
-  for (int jg = threadIdx.x; jg < S.ncgp_sol; jg += blockDim.x) {
-    if ((ig > jg && ((ig + jg) & 1) == 0) || (ig < jg && ((ig + jg) & 1) == 1)) continue;
-    int gj = S.coff + jg;
-    int swj = P.cg_sw[gj];
-    if (P.flags[swj] & F_EXCL) continue;
-    if (S.switch_atoms) {
-      double3 xj = ld3(P.x, swj);
-      double dx = xs.x - xj.x, dy = xs.y - xj.y, dz = xs.z - xj.z;
-      if (dx * dx + dy * dy + dz * dz > S.Rcpp2) continue;
-    } else {
-      const int reach = groups_reach(P, gi, gj, S.Rcpp2);
-      double last;
-      if (reach < 0 || (reach == 0 && !groups_inside_any(P, gi, gj, S.Rcpp2, &last))) continue;
-    }
+  const int lane = threadIdx.x & 31;
+  // the pairs of group pair (gi, gj), written at out[0..] when out is given;
+  // returns their number
+  auto pairs = [&](int jg, int gj, int4 *out) {
+    int n = 0;
     for (int ia = P.cg_first[gi]; ia <= P.cg_last[gi]; ia++) {
       int i = P.cg_atoms[ia];
       if (P.iq[i] >= 0) continue;
@@ -774,10 +843,50 @@ __global__ void k_list_pp(DevPtrs P, int force) {
         if (zero_pair(P, i, j, lj)) continue;
         if (excluded_pair(P, S, i, j)) continue;
         if (is14(P, S, i, j)) lj = 3;
-        int k = atomicAdd(&P.st[s].pp_n, 1);
-        if (k < S.pp_cap) P.pp[S.pp_off + k] = make_int4(i, j, lj, 0);
-        else set_status(&P.st[s], QB_ERR_LIST_OVERFLOW);
+        if (out) out[n] = make_int4(i, j, lj, 0);
+        n++;
       }
+    }
+    return n;
+  };
+  // rounds in which every lane of a warp takes part, so that a warp reserves
+  // its pairs' slots with one atomic (a per-pair atomic on the system's
+  // counter serialises the ~10^5 pairs of a large solute)
+  for (int base = 0; base < S.ncgp_sol; base += blockDim.x) {
+    const int jg = base + threadIdx.x;
+    const int gj = S.coff + jg;
+    bool inside = jg < S.ncgp_sol && !((ig > jg && ((ig + jg) & 1) == 0) || (ig < jg && ((ig + jg) & 1) == 1));
+    if (inside) inside = !(P.flags[P.cg_sw[gj]] & F_EXCL);
+    if (inside) {
+      if (S.switch_atoms) {
+        double3 xj = ld3(P.x, P.cg_sw[gj]);
+        double dx = xs.x - xj.x, dy = xs.y - xj.y, dz = xs.z - xj.z;
+        if (S.pbc) min_image(box_of(P, s), dx, dy, dz);   // nbpplist_box (md.f90:5349)
+        inside = dx * dx + dy * dy + dz * dz <= S.Rcpp2;
+      } else {
+        const int reach = groups_reach(P, gi, gj, S.Rcpp2);
+        double last;
+        inside = reach > 0 || (reach == 0 && groups_inside_any(P, gi, gj, S.Rcpp2, &last));
+      }
+    }
+    const int n = inside ? pairs(jg, gj, nullptr) : 0;
+    // exclusive prefix of n over the warp, one reservation per warp
+    int pre = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(FULL, pre, o);
+      if (lane >= o) pre += t;
+    }
+    const int total = __shfl_sync(FULL, pre, 31);
+    int first = 0;
+    if (lane == 0 && total > 0) first = atomicAdd(&P.st[s].pp_n, total);
+    first = __shfl_sync(FULL, first, 0);
+    if (n == 0) continue;
+    const int k = first + pre - n;
+    if (k + n <= S.pp_cap) {
+      pairs(jg, gj, P.pp + S.pp_off + k);
+    } else {
+      set_status(&P.st[s], QB_ERR_LIST_OVERFLOW);
     }
   }
 }
@@ -808,6 +917,7 @@ __global__ void k_list_pw(DevPtrs P, int force) {
         double3 xo = ld3(P.x, o);
         if (S.switch_atoms) {
           double dx = xs.x - xo.x, dy = xs.y - xo.y, dz = xs.z - xo.z;
+          if (S.pbc) min_image(box_of(P, s), dx, dy, dz);   // nbpwlist_box (md.f90:6801)
           ok = dx * dx + dy * dy + dz * dz <= S.Rcpw2;
         } else {
           const int reach = group_point_reach(P, gi, xo, S.Rcpw2);
@@ -843,32 +953,48 @@ __global__ void k_list_qp(DevPtrs P, int force) {
   __syncthreads();
   if (threadIdx.x == 0) P.st[s].qp_n = 0;
   __syncthreads();
+  // the list's centre: the solute centre, or in a periodic box the nearest
+  // image of the Q switching atom (nbqplist_box, md.f90:8005-8014)
+  const double3 xq = S.pbc ? ld3(P.x, S.qswitch) : make_double3(S.xp[0], S.xp[1], S.xp[2]);
+  const BoxD bx = box_of(P, s);
   for (int ig = 0; ig < S.ncgp_sol; ig++) {
     int gi = S.coff + ig;
     int sw = P.cg_sw[gi];
     if (P.flags[sw] & F_EXCL) continue;
     if (S.switch_atoms) {
       double3 xs = ld3(P.x, sw);
-      double dx = xs.x - S.xp[0], dy = xs.y - S.xp[1], dz = xs.z - S.xp[2];
+      double dx = xs.x - xq.x, dy = xs.y - xq.y, dz = xs.z - xq.z;
+      if (S.pbc) min_image(bx, dx, dy, dz);
       if (dx * dx + dy * dy + dz * dz > S.Rcq2) continue;
     } else {
       double last;
       if (!group_point_inside_any(P, gi, make_double3(S.xp[0], S.xp[1], S.xp[2]), S.Rcq2, &last)) continue;
     }
     int f = P.cg_first[gi], n = P.cg_last[gi] - f + 1;
-    for (int t = threadIdx.x; t < n * S.nq; t += blockDim.x) {
-      int i = P.cg_atoms[f + t / S.nq], iq = t % S.nq;
-      int li = i - S.aoff;
-      bool near = false;
-      for (int st = 0; st < S.S && !near; st++)
-        for (int q = 0; q < S.nq; q++)
-          if (P.qconn[S.qconn_off + ((size_t)st * S.nsol + li) * S.nq + q] <= 3) { near = true; break; }
-      if (near) continue;
+    // whole warps per round: a warp reserves its entries with one atomic
+    for (int t0 = 0; t0 < n * S.nq; t0 += blockDim.x) {
+      const int t = t0 + threadIdx.x;
+      bool take = t < n * S.nq;
+      int i = 0, iq = 0, li = 0;
+      if (take) {
+        i = P.cg_atoms[f + t / S.nq];
+        iq = t % S.nq;
+        li = i - S.aoff;
+        for (int st = 0; st < S.S && take; st++)
+          for (int q = 0; q < S.nq; q++)
+            if (P.qconn[S.qconn_off + ((size_t)st * S.nsol + li) * S.nq + q] <= 3) { take = false; break; }
+      }
+      const unsigned bal = __ballot_sync(FULL, take);
+      const int lane = threadIdx.x & 31;
+      int first = 0;
+      if (lane == 0 && bal) first = atomicAdd(&P.st[s].qp_n, __popc(bal));
+      first = __shfl_sync(FULL, first, 0);
+      if (!take) continue;
       int qa = P.iqseq[S.qoff + iq];
       int lj = ljcode(P, S, i, qa);
       if (P.qconn[S.qconn_off + ((size_t)0 * S.nsol + li) * S.nq + iq] == 4) lj = 3;
       int qlj = lj == 2 ? 1 : lj;
-      int k = atomicAdd(&P.st[s].qp_n, 1);
+      int k = first + __popc(bal & ((1u << lane) - 1u));
       if (k < S.qp_cap) P.qp[S.qp_off + k] = make_int4(S.qoff + iq, i, lj, qlj);
       else set_status(&P.st[s], QB_ERR_LIST_OVERFLOW);
     }
@@ -885,13 +1011,17 @@ __global__ void k_list_qw(DevPtrs P, int force) {
   __shared__ int base;
   if (threadIdx.x == 0) base = 0;
   __syncthreads();
+  // periodic box: the nearest image of the Q switching atom (nbqwlist_box, md.f90:8149)
+  const double3 xq = S.pbc ? ld3(P.x, S.qswitch) : make_double3(S.xp[0], S.xp[1], S.xp[2]);
+  const BoxD bx = box_of(P, s);
   for (int w0 = 0; w0 < S.nwat; w0 += blockDim.x) {
     int iw = w0 + threadIdx.x;
     bool ok = false;
     int o = S.aoff + S.nsol + 3 * iw;
     if (iw < S.nwat && !(P.flags[o] & F_EXCL)) {
       double3 xo = ld3(P.x, o);
-      double dx = xo.x - S.xp[0], dy = xo.y - S.xp[1], dz = xo.z - S.xp[2];
+      double dx = xo.x - xq.x, dy = xo.y - xq.y, dz = xo.z - xq.z;
+      if (S.pbc) min_image(bx, dx, dy, dz);
       ok = dx * dx + dy * dy + dz * dz <= S.Rcq2;
     }
     // block-wide ordered compaction
@@ -1026,13 +1156,16 @@ __device__ __forceinline__ void ww_pair_f64(const double *xi, const double *xj, 
 }
 
 // Mixed precision: i = {hO[3], lO[3], rH1[3], rH2[3]}, j likewise.
+// sh: the molecule pair's periodic image shift as hi + lo floats ({hi[3],
+// lo[3]}), or nullptr.
 template <bool HLJ>
 __device__ __forceinline__ void ww_pair_f32(const float *i, const float *j, float qoo, float qoh, float qhh,
-                                            const float *lj, float *f, float &el, float &vdw) {
+                                            const float *lj, float *f, float &el, float &vdw,
+                                            const float *sh = nullptr) {
   float dOO[3], t[2][3];
 #pragma unroll
   for (int c = 0; c < 3; c++) {
-    dOO[c] = (j[c] - i[c]) + (j[3 + c] - i[3 + c]);
+    dOO[c] = sh ? ((j[c] - i[c]) - sh[c]) + ((j[3 + c] - i[3 + c]) - sh[3 + c]) : (j[c] - i[c]) + (j[3 + c] - i[3 + c]);
     t[0][c] = dOO[c] + j[6 + c];
     t[1][c] = dOO[c] + j[9 + c];
   }
@@ -1098,6 +1231,10 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P, in
   const int CW = P.ww_chunk;
   const int nch = (S.nwat + CW - 1) / CW;
   const float qo = S.crg_ow, qh = S.crg_hw;
+  // periodic box (nonbond_ww_spc_box, md.f90:12078-12100): molecule j at the
+  // image of its O nearest i's O
+  const bool box = S.pbc != 0;
+  const BoxD bx = box_of(P, s);
   double el = 0, vdw = 0;
   for (int c = 0; c < nch; c++) {
     const int c0 = c * CW, cn = min(CW, S.nwat - c0);
@@ -1151,7 +1288,19 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P, in
           if (k + 32 < ke) jn2 = nb[k + 32];
           float xj[12];
           unpack_mixed(wsm + (j - c0) * W, xj);
-          ww_pair_f32<HLJ>(xi, xj, qoo, qoh, qhh, ljf, f, e_el, e_vdw);
+          if (box) {
+            float sh[6];
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+              const double d = ((double)xj[q] + (double)xj[3 + q]) - ((double)xi[q] + (double)xi[3 + q]);
+              const double t = bx.L[q] * round(d * bx.iL[q]);
+              sh[q] = (float)t;
+              sh[3 + q] = (float)(t - (double)sh[q]);
+            }
+            ww_pair_f32<HLJ>(xi, xj, qoo, qoh, qhh, ljf, f, e_el, e_vdw, sh);
+          } else {
+            ww_pair_f32<HLJ>(xi, xj, qoo, qoh, qhh, ljf, f, e_el, e_vdw);
+          }
         }
         el += (double)e_el;
         vdw += (double)e_vdw;
@@ -1175,7 +1324,12 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P, in
           if (k + 16 < ke) jn = nb[k + 16];
           const double2 *rj = reinterpret_cast<const double2 *>(wsm + (j - c0) * W);
           double2 v0 = rj[0], v1 = rj[1], v2 = rj[2], v3 = rj[3], v4 = rj[4];
-          const double xj[9] = {v0.x, v0.y, v1.x, v1.y, v2.x, v2.y, v3.x, v3.y, v4.x};
+          double xj[9] = {v0.x, v0.y, v1.x, v1.y, v2.x, v2.y, v3.x, v3.y, v4.x};
+          if (box) {
+            const double3 t = image_shift(bx, xj[0] - xi[0], xj[1] - xi[1], xj[2] - xi[2]);
+#pragma unroll
+            for (int a = 0; a < 3; a++) { xj[3 * a] -= t.x; xj[3 * a + 1] -= t.y; xj[3 * a + 2] -= t.z; }
+          }
           ww_pair_f64<HLJ>(xi, xj, qoo, qoh, qhh, ljd, fd, el, vdw);
         }
 #pragma unroll
@@ -1215,11 +1369,24 @@ struct WwI2 {
 // plus the O-O Lennard-Jones + Coulomb pair (into gO.x).  Each gradient term
 // is w * (x_j - x_i) with w = q q / r^3 (Coulomb) and r^-2 (q q / r + 12 A /
 // r^12 - 6 B / r^6) for O-O: -dv of the reference loop.
+// BOX: the periodic box's edge lengths as hi + lo floats (Lh, Ll) and their
+// inverses iL: the O-O vector moves to its nearest image (nonbond_ww_spc_box,
+// md.f90:12078-12100; the FP32 nint agrees with the FP64 one away from half an
+// edge, far beyond the cut-off).
+template <bool BOX>
 __device__ __forceinline__ void ww_force_x2(const WwI2 &I, const float4 j0, const float4 j1, const float4 j2,
                                             float2 qoh2, float2 qhh2, float qoo, float A, float B, float2 *gO,
-                                            float2 *gH, float2 *gHs) {
-  const float d[3] = {(j0.x - I.hO[0]) + (j0.w - I.lO[0]), (j0.y - I.hO[1]) + (j1.x - I.lO[1]),
-                      (j0.z - I.hO[2]) + (j1.y - I.lO[2])};
+                                            float2 *gH, float2 *gHs, const float *Lh = nullptr,
+                                            const float *Ll = nullptr, const float *iL = nullptr) {
+  float d[3] = {(j0.x - I.hO[0]) + (j0.w - I.lO[0]), (j0.y - I.hO[1]) + (j1.x - I.lO[1]),
+                (j0.z - I.hO[2]) + (j1.y - I.lO[2])};
+  if (BOX) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float n = rintf(d[c] * iL[c]);
+      d[c] = fmaf(-n, Ll[c], fmaf(-n, Lh[c], d[c]));
+    }
+  }
   const float2 rHj[3] = {make_float2(j1.z, j1.w), make_float2(j2.x, j2.y), make_float2(j2.z, j2.w)};
   float2 t[3], sv[3], hd[3], hx[3];
 #pragma unroll
@@ -1260,6 +1427,7 @@ __device__ __forceinline__ void ww_force_x2(const WwI2 &I, const float4 j0, cons
 // 256 threads, two blocks per SM: one block's staging of records overlaps the
 // other's pair work (the registers of the packed path allow 16 warps per SM)
 constexpr int WWX_BLOCK = 256;
+template <bool BOX>
 __global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P, int wpb) {
   extern __shared__ float4 wsm[];
   __shared__ int2 srange[WW_WPB];
@@ -1278,6 +1446,16 @@ __global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P, int wpb) {
   const float qoo = qo * qo;
   const float2 qoh2 = dup2(qo * qh), qhh2 = dup2(qh * qh);
   const float A = (float)S.A_OO, B = (float)S.B_OO;
+  float Lh[3], Ll[3], iL[3];
+  if (BOX) {
+    const BoxD bx = box_of(P, s);
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      Lh[q] = (float)bx.L[q];
+      Ll[q] = (float)(bx.L[q] - (double)Lh[q]);
+      iL[q] = (float)bx.iL[q];
+    }
+  }
   for (int c = 0; c < nch; c++) {
     const int c0 = c * CW, cn = min(CW, S.nwat - c0);
     __syncthreads();
@@ -1334,7 +1512,7 @@ __global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P, int wpb) {
         for (int u = 0; u < 4; u++) {
           if (jg[u] < 0) break;
           const float4 *rj = wsm + (jg[u] - c0) * W;
-          ww_force_x2(I, rj[0], rj[1], rj[2], qoh2, qhh2, qoo, A, B, gO, gH, gHs);
+          ww_force_x2<BOX>(I, rj[0], rj[1], rj[2], qoh2, qhh2, qoo, A, B, gO, gH, gHs, Lh, Ll, iL);
         }
 #pragma unroll
         for (int u = 0; u < 4; u++) jg[u] = jn[u];
@@ -1375,6 +1553,13 @@ __device__ __forceinline__ void nb_pp_body(DevPtrs &P, int bx, int s, int gx) {
       int i = p.x, j = p.y, lj = p.z;
       double3 xi = ld3(P.x, i), xj = ld3(P.x, j);
       double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+      if (S.pbc) {
+        // nonbond_pp_box (md.f90:10508-10519): the image of the charge-group
+        // pair, from the two groups' switching atoms
+        const double3 a = ld3(P.x, switch_of(P, i)), b = ld3(P.x, switch_of(P, j));
+        const double3 t = image_shift(box_of(P, s), b.x - a.x, b.y - a.y, b.z - a.z);
+        dx -= t.x; dy -= t.y; dz -= t.z;
+      }
       double r = rsqrt(dx * dx + dy * dy + dz * dz);
       double r2 = r * r, r6 = r2 * r2 * r2;
       float qq = P.crg[i] * P.crg[j];
@@ -1424,7 +1609,15 @@ __global__ void __launch_bounds__(PW_BLOCK) k_nb_pw(DevPtrs P) {
   const int lane = threadIdx.x & 31;
   const int ow = S.aoff + S.nsol;
   const int o = ow + 3 * (act ? (int)P.pwg[(size_t)sg * P.pwg_cap + k] : 0);
-  const double3 xw[3] = {ld3(P.x, o), ld3(P.x, o + 1), ld3(P.x, o + 2)};
+  double3 xw[3] = {ld3(P.x, o), ld3(P.x, o + 1), ld3(P.x, o + 2)};
+  if (S.pbc) {
+    // nonbond_pw_box (md.f90:10693-10699): the water at the image of its O
+    // nearest the group's switching atom
+    const double3 a = ld3(P.x, P.cg_sw[S.coff + ig]);
+    const double3 t = image_shift(box_of(P, s), xw[0].x - a.x, xw[0].y - a.y, xw[0].z - a.z);
+#pragma unroll
+    for (int b = 0; b < 3; b++) { xw[b].x -= t.x; xw[b].y -= t.y; xw[b].z -= t.z; }
+  }
   // the group's atoms, parameters and positions staged once per block
   __shared__ PwAtom sa[PW_MAXA];
   __shared__ double4 sx[PW_MAXA];
@@ -1490,6 +1683,13 @@ __device__ __forceinline__ void nb_qp_body(DevPtrs &P, int bx, int s, int gx) {
       int i = P.iqseq[gq], iq = gq - S.qoff;
       double3 xi = ld3(P.x, i), xj = ld3(P.x, j);
       double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+      if (S.pbc) {
+        // nonbond_qp_box (md.f90:11060-11068): the image of j's group
+        // switching atom nearest the Q switching atom
+        const double3 a = ld3(P.x, S.qswitch), b = ld3(P.x, switch_of(P, j));
+        const double3 t = image_shift(box_of(P, s), b.x - a.x, b.y - a.y, b.z - a.z);
+        dx -= t.x; dy -= t.y; dz -= t.z;
+      }
       double r2 = dx * dx + dy * dy + dz * dz;
       double dvsum = 0;
       if (!S.qvdw) {
@@ -1603,7 +1803,16 @@ __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const bool act = k < n;
   const int j = act ? P.qw[S.qw_off + k] : P.qw[S.qw_off];
-  const double3 xO = ld3(P.x, j), xH1 = ld3(P.x, j + 1), xH2 = ld3(P.x, j + 2);
+  double3 xO = ld3(P.x, j), xH1 = ld3(P.x, j + 1), xH2 = ld3(P.x, j + 2);
+  if (S.pbc) {
+    // nonbond_qw_spc_box (md.f90:11440-11446): the water at the image of its
+    // O nearest the Q switching atom
+    const double3 a = ld3(P.x, S.qswitch);
+    const double3 t = image_shift(box_of(P, s), xO.x - a.x, xO.y - a.y, xO.z - a.z);
+    xO.x -= t.x; xO.y -= t.y; xO.z -= t.z;
+    xH1.x -= t.x; xH1.y -= t.y; xH1.z -= t.z;
+    xH2.x -= t.x; xH2.y -= t.y; xH2.z -= t.z;
+  }
   double fw[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int iq = 0; iq < S.nq; iq++) {
     int gq = S.qoff + iq;
@@ -1888,7 +2097,8 @@ __device__ __forceinline__ void water_terms(const DevPtrs &P, const SysDev &S, i
     const uint8_t fl = P.flags[o + a];
     if (fl & (F_EXCL | F_SHELL)) fix_shell_atom(P, S, o + a, fl, x[a], g[a], efix, eshell);
   }
-  if (!(fo & F_EXCL)) {
+  // the solvent sphere's radial restraint (restrain_solvent; none in a periodic box)
+  if (!(fo & F_EXCL) && !S.pbc) {
     const double shift = S.fk_ws != 0. ? sqrt((double)kBoltzF * P.st[s].Tfree / S.fk_ws) : 0.;
     double dr[3] = {x[0].x - S.xw[0], x[0].y - S.xw[1], x[0].z - S.xw[2]};
     double b = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
@@ -2364,6 +2574,7 @@ __device__ __forceinline__ void prestrain_body(DevPtrs &P, int s) {
       double4 prm = P.rd_p[S.rd_off + r];  // d1, d2, fk
       double3 xi = ld3(P.x, q.x), xj = ld3(P.x, q.y);
       double dr[3] = {xj.x - xi.x, xj.y - xi.y, xj.z - xi.z};
+      if (S.pbc) min_image(box_of(P, s), dr[0], dr[1], dr[2]);   // md.f90:13096-13101
       double wgt = q.z != 0 ? S.lambda[q.z - 1] : 1.0;
       double b = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]), db;
       if (b < prm.x) db = b - prm.x;
@@ -2379,6 +2590,11 @@ __device__ __forceinline__ void prestrain_body(DevPtrs &P, int s) {
       double2 prm = P.ra_p[S.ra_off + r];  // ang, fk
       double3 xi = ld3(P.x, q.x), xj = ld3(P.x, q.y), xk = ld3(P.x, q.z);
       double d1[3] = {xi.x - xj.x, xi.y - xj.y, xi.z - xj.z}, d2[3] = {xk.x - xj.x, xk.y - xj.y, xk.z - xj.z};
+      if (S.pbc) {   // md.f90:13160-13168
+        const BoxD bx = box_of(P, s);
+        min_image(bx, d1[0], d1[1], d1[2]);
+        min_image(bx, d2[0], d2[1], d2[2]);
+      }
       double wgt = q.w != 0 ? S.lambda[q.w - 1] : 1.0;
       double r2ij = d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2], r2jk = d2[0] * d2[0] + d2[1] * d2[1] + d2[2] * d2[2];
       double rij = sqrt(r2ij), rjk = sqrt(r2jk);
@@ -3021,6 +3237,92 @@ __global__ void k_finish(DevPtrs P, int mode) {
     }
     __syncwarp();
     if (lane == 0) st.istep = is + 1;
+  }
+}
+
+// ---------------------------------------------------------- periodic box
+
+// put_back_in_box (md.f90:15477-15600), at the list steps of systems that put
+// solute or solvent back: the box centre becomes the solute's mean position
+// (all atoms without solute) unless it is rigid, then every molecule of the
+// chosen range whose centre of mass lies beyond half an edge from the centre
+// moves by one edge length along that axis.  Block per system; the centre is
+// summed by one thread in the reference's atom order, molecules in parallel.
+__global__ void k_put_back_in_box(DevPtrs P) {
+  const int s = blockIdx.x;
+  const SysDev &S = P.sys[s];
+  SysState &st = P.st[s];
+  if (!S.pbc || S.put_first >= S.put_last || (st.istep % S.NB) != 0) return;
+  if (st.frozen) return;
+  __shared__ double c[3];
+  if (threadIdx.x == 0) {
+    if (!S.rigid_center) {
+      const int n = S.nsol > 0 ? S.nsol : S.natom;
+      double b0 = 0, b1 = 0, b2 = 0;
+      for (int i = 0; i < n; i++) {
+        const double4 a = P.x[S.aoff + i];
+        b0 += a.x; b1 += a.y; b2 += a.z;
+      }
+      st.boxc[0] = b0 / n; st.boxc[1] = b1 / n; st.boxc[2] = b2 / n;
+    }
+    for (int k = 0; k < 3; k++) c[k] = st.boxc[k];
+  }
+  __syncthreads();
+  const double hi[3] = {c[0] + st.boxl[0] / 2, c[1] + st.boxl[1] / 2, c[2] + st.boxl[2] / 2};
+  const double lo[3] = {c[0] - st.boxl[0] / 2, c[1] - st.boxl[1] / 2, c[2] - st.boxl[2] / 2};
+  for (int m = S.put_first + threadIdx.x; m < S.put_last; m += blockDim.x) {
+    const int a0 = P.mol_first[S.mol_off + m], a1 = P.mol_first[S.mol_off + m + 1];
+    double cm[3] = {0, 0, 0};
+    for (int j = a0; j < a1; j++) {
+      const double4 a = P.x[j];
+      const double w = P.mass_box[j];
+      cm[0] += a.x * w; cm[1] += a.y * w; cm[2] += a.z * w;
+    }
+    const double mi = P.mol_minv[S.mol_off + m];
+    double sh[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const double v = cm[k] * mi;
+      sh[k] = v > hi[k] ? -st.boxl[k] : (v < lo[k] ? st.boxl[k] : 0.0);
+    }
+    if (sh[0] != 0.0 || sh[1] != 0.0 || sh[2] != 0.0)
+      for (int j = a0; j < a1; j++) {
+        double4 a = P.x[j];
+        a.x += sh[0]; a.y += sh[1]; a.z += sh[2];
+        P.x[j] = a;
+      }
+  }
+}
+
+// MC_volume's trial move (md.f90:15686-15722) for the systems in a volume
+// move: every molecule's centre of mass scaled about the box centre by the
+// ratio of new to old edge lengths, the molecule translated rigidly.  One
+// thread per molecule.
+__global__ void k_mc_scale(DevPtrs P) {
+  const int s = blockIdx.y;
+  const SysDev &S = P.sys[s];
+  const SysState &st = P.st[s];
+  if (!st.mc) return;
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= S.nmol) return;
+  const int a0 = P.mol_first[S.mol_off + m], a1 = P.mol_first[S.mol_off + m + 1];
+  double cm[3] = {0, 0, 0};
+  for (int j = a0; j < a1; j++) {
+    const double4 a = P.x[j];
+    const double w = P.mass_box[j];
+    cm[0] += a.x * w; cm[1] += a.y * w; cm[2] += a.z * w;
+  }
+  const double mi = P.mol_minv[S.mol_off + m];
+  double mv[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    cm[k] = cm[k] * mi;
+    mv[k] = ((cm[k] - st.boxc[k]) * st.boxl[k] / st.mc_oldl[k] + st.boxc[k]) - cm[k];
+  }
+  for (int j = a0; j < a1; j++) {
+    double4 a = P.x[j];
+    a.x += mv[0]; a.y += mv[1]; a.z += mv[2];
+    P.x[j] = a;
   }
 }
 

@@ -349,7 +349,39 @@ void read_inp(const std::string &path, RunInput &in) {
   in.dir = slash == std::string::npos ? "" : path.substr(0, slash);
   std::vector<std::string> bad;
 
-  if (prm.section("PBC")) fail(QB_ERR_UNSUPPORTED, "periodic boundary conditions are not supported (sphere only)");
+  // [PBC] (md.f90:2583-2656): periodic box, NVT or NPT (Monte Carlo volume moves)
+  if (const PrmSection *pb = prm.section("PBC")) {
+    in.box = true;
+    if (!logical_key(pb, "rigid_box_center", false, in.rigid_box_center)) bad.push_back("rigid_box_center must be on or off");
+    if (!logical_key(pb, "constant_pressure", false, in.constant_pressure)) bad.push_back("constant_pressure must be on or off");
+    if (in.constant_pressure) {
+      if (!get_real(pb, "max_volume_displ", in.max_vol_displ)) bad.push_back("maximum volume displacement not specified (section PBC)");
+      if (!get_int(pb, "pressure_seed", in.pressure_seed)) in.pressure_seed = 3781;
+      double p = 1.0;
+      if (!get_real(pb, "pressure", p)) p = 1.0;
+      in.pressure_bar = p;
+      // bar to kcal/mol/A^3, the single-precision literal of md.f90:2619
+      in.pressure = p * (double)1.43836e-5f;
+    } else {
+      for (auto &l : pb->lines) {
+        std::string k, v;
+        if (!prm_split(l, k, v)) break;
+        if (k != "control_box") continue;
+        auto t = line_values(l.substr(l.find(k) + k.size()));
+        if (t.size() < 3 || !to_real(t[0], in.new_boxl[0]) || !to_real(t[1], in.new_boxl[1]) ||
+            !to_real(t[2], in.new_boxl[2]))
+          bad.push_back("control_box");
+        in.control_box = true;
+        break;
+      }
+    }
+    // prm_get_logical_by_key without a default: absent keys leave the flags off
+    bool b = false;
+    if (get_logical(pb, "put_solvent_back_in_box") >= 0 && logical_key(pb, "put_solvent_back_in_box", false, b))
+      in.put_solvent_back_in_box = b;
+    if (get_logical(pb, "put_solute_back_in_box") >= 0 && logical_key(pb, "put_solute_back_in_box", false, b))
+      in.put_solute_back_in_box = b;
+  }
   const PrmSection *md = prm.section("MD");
   if (!md) fail(QB_ERR_UNSUPPORTED, path + ": no [MD] section (old-format input is not supported)");
   if (!get_int(md, "steps", in.nsteps)) bad.push_back("steps");
@@ -379,6 +411,9 @@ void read_inp(const std::string &path, RunInput &in) {
   // md.f90:2700 looks up 'cut-offs'; inputs spelling it 'cut_offs' get the defaults
   const PrmSection *co = prm.section("cut-offs");
   if (co) {
+    // without LRF the section leaves RcLRF unset: zero, as the reference's
+    // static variable (md.f90:2789), which the box checks see
+    if (!in.use_LRF) in.RcLRF = 0.0;
     get_real(co, "solute_solute", in.Rcpp);
     get_real(co, "solvent_solvent", in.Rcww);
     get_real(co, "solute_solvent", in.Rcpw);
@@ -423,6 +458,7 @@ void read_inp(const std::string &path, RunInput &in) {
     if (!get_int(iv, "temperature", in.itemp_cycle)) in.itemp_cycle = 10;
     if (!get_int(iv, "energy", in.iene_cycle)) in.iene_cycle = 0;
     if (!get_int(iv, "trajectory", in.itrj_cycle)) in.itrj_cycle = 0;
+    if (in.constant_pressure && !get_int(iv, "volume_change", in.ivolume_cycle)) in.ivolume_cycle = 10;
   }
   if (in.iout_cycle <= 0) in.iout_cycle = -999999999;
   if (in.itemp_cycle <= 0) in.itemp_cycle = -999999999;
@@ -863,7 +899,16 @@ void parse_topology(const std::string &path, Topology &t) {
     std::string l = r.line();
     auto v = line_values(l);
     if (v.empty()) r.err("boundary line");
-    if (v[0] == "PBC") fail(QB_ERR_UNSUPPORTED, "periodic-box topologies are not supported (sphere only)");
+    if (v[0] == "PBC") {
+      // periodic box (topo.f90:1027-1036): edge lengths and centre; no
+      // excluded atoms, no restrained shell, nothing further in the file
+      t.use_pbc = true;
+      auto bl = r.reals(3);
+      auto bc = r.reals(3);
+      for (int k = 0; k < 3; k++) { t.boxlength[k] = bl[k]; t.boxcenter[k] = bc[k]; }
+      t.excl.assign(N, 0);
+      return;
+    }
     t.use_pbc = false;
     double a, b, c;
     if (t.version < 5.01) {
@@ -944,6 +989,15 @@ void read_fep(const std::string &path, const Topology &t, Fep &f) {
     return s ? s->lines : empty;
   };
   auto bad = [&](const std::string &m) { fail(QB_ERR_PARSE, path + ": " + m); };
+  // a periodic box needs the Q atoms' switching atom (qatom.f90:910-925)
+  if (t.use_pbc) {
+    const PrmSection *pb = prm.section("PBC");
+    if (!pb) bad("section PBC is required when using periodic boundary");
+    int sw = 0;
+    if (!get_int(pb, "switching_atom", sw)) bad("switching atom could not be read");
+    f.qswitch = sw - 1 + f.offset;
+    if (f.qswitch < 0 || f.qswitch >= t.nat_pro) bad("switching_atom out of range");
+  }
   // f.qcrg holds the library charges (get_fep md.f90:1495-1500)
   for (auto &l : lines("change_charges")) {
     auto v = line_values(l);
@@ -1251,7 +1305,7 @@ bool read_record(std::FILE *f, std::vector<char> &buf) {
 }  // namespace
 
 void read_restart(const std::string &path, int natom, std::vector<double> &x, std::vector<double> &v,
-                  int nshell, std::vector<float> *theta_corr) {
+                  int nshell, std::vector<float> *theta_corr, double *boxl, double *boxc) {
   std::FILE *f = std::fopen(path.c_str(), "rb");
   if (!f) fail(QB_ERR_IO, "cannot open restart file " + path);
   std::vector<char> rec;
@@ -1266,6 +1320,14 @@ void read_restart(const std::string &path, int natom, std::vector<double> &x, st
   };
   vec(x, "coordinates");
   vec(v, "velocities");
+  if (boxl) {
+    // periodic box: (boxlength), (boxcenter) follow the velocities
+    double *dst[2] = {boxl, boxc};
+    for (int r = 0; r < 2; r++) {
+      if (!read_record(f, rec) || rec.size() != 24) { std::fclose(f); fail(QB_ERR_PARSE, path + ": restart file lacks the box records"); }
+      std::memcpy(dst[r], rec.data(), 24);
+    }
+  }
   if (theta_corr && nshell > 0) {
     // wat_shells (md.f90:15068-15082): use the record only if its shell count matches
     if (read_record(f, rec) && rec.size() == 4 + 4 * (size_t)nshell) {
@@ -1281,7 +1343,7 @@ void read_restart(const std::string &path, int natom, std::vector<double> &x, st
 }
 
 void write_restart(const std::string &path, int natom, const double *x, const double *v, int nshell,
-                   const float *theta_corr) {
+                   const float *theta_corr, const double *box6) {
   std::FILE *f = std::fopen(path.c_str(), "wb");
   if (!f) fail(QB_ERR_IO, "cannot write " + path);
   int32_t nat3 = 3 * natom;
@@ -1300,6 +1362,14 @@ void write_restart(const std::string &path, int natom, const double *x, const do
     const void *p[2] = {&ns, theta_corr};
     size_t s[2] = {4, 4 * (size_t)nshell};
     write_record(f, p, s, 2);
+  }
+  if (box6) {
+    // write_xfin's box records (md.f90:15471-15474): edge lengths, centre
+    for (int r = 0; r < 2; r++) {
+      const void *p[1] = {box6 + 3 * r};
+      size_t s[1] = {24};
+      write_record(f, p, s, 1);
+    }
   }
   std::fclose(f);
 }

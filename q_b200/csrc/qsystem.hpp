@@ -52,6 +52,11 @@ struct RunInput {
   std::vector<DistRestraint> rdis;
   std::vector<AngRestraint> rang;
   std::vector<WallRestraint> rwal;
+  // [PBC] (md.f90:2583-2656)
+  bool box = false, rigid_box_center = false, constant_pressure = false, control_box = false;
+  bool put_solvent_back_in_box = false, put_solute_back_in_box = false;
+  double max_vol_displ = 0, pressure_bar = 1.0, pressure = 0, new_boxl[3] = {0, 0, 0};
+  int pressure_seed = 3781, ivolume_cycle = 10;
 };
 
 struct TypeLib { double mass; double avdw[3]; double bvdw[3]; };
@@ -94,6 +99,7 @@ struct Topology {
   std::vector<std::string> tac;
   int solvent_type = 0;
   bool use_pbc = false;
+  double boxlength[3] = {0, 0, 0}, boxcenter[3] = {0, 0, 0};   // periodic box (topo.f90:1031-1033)
   double rexcl_o = 0, rwat = 0, xpcent[3] = {0, 0, 0}, xwcent[3] = {0, 0, 0};
   int nexats = 0, nexwat = 0;
   std::vector<unsigned char> excl;
@@ -102,6 +108,7 @@ struct Topology {
 // FEP data as read by qatom_load_atoms/qatom_load_fep (qatom.f90:253, 874).
 struct Fep {
   int nstates = 0, nqat = 0, offset = 0;
+  int qswitch = -1;   // periodic box: atom the Q-atom lists are centred on ([PBC] switching_atom, 0-based)
   bool qq_use_library_charges = false, softcore_use_max_potential = false;
   std::vector<int> iqseq;                    // atom index per Q atom (0-based, -1 unused)
   std::vector<float> qcrg;                   // [nqat*nstates] unscaled until set-up
@@ -196,6 +203,12 @@ struct System {
   std::vector<int> rang_i, rang_j, rang_k, rang_ipsi; std::vector<double> rang_ang, rang_fk;
   std::vector<int> rwal_i, rwal_j, rwal_ih; std::vector<double> rwal_d, rwal_fk, rwal_a, rwal_dm;
   std::vector<unsigned char> heavy_u8;
+  // periodic box: edge lengths and centre (topology, restart, control_box),
+  // 1/molecule mass and the per-atom mass put_back_in_box and MC_volume use
+  double boxl[3] = {0, 0, 0}, boxc[3] = {0, 0, 0};
+  std::vector<double> mol_minv, mass_box;
+  // randm's sequence after the Maxwell velocities (started: it was seeded)
+  int randm_started = 0, randm_state = 0;
   std::string log;   // qdyn-style set-up messages
 
   void fill_view(qb_sysview *v) const;
@@ -207,14 +220,16 @@ void read_topology(const std::string &path, Topology &t);
 void read_fep_atoms(const std::string &path, const Topology &t, Fep &f, int nstates_inp);
 void read_fep(const std::string &path, const Topology &t, Fep &f);
 void read_restart(const std::string &path, int natom, std::vector<double> &x,
-                  std::vector<double> &v, int nshell, std::vector<float> *theta_corr);
+                  std::vector<double> &v, int nshell, std::vector<float> *theta_corr,
+                  double *boxl = nullptr, double *boxc = nullptr);
 void write_restart(const std::string &path, int natom, const double *x, const double *v,
-                   int nshell, const float *theta_corr);
+                   int nshell, const float *theta_corr, const double *box6 = nullptr);
 void append_energy_frame(const std::string &path, int nstates, const double *EQ, int noffd, const int *ij,
                          const double *hr);
 
 // setup.cpp
 void prepare(System &s);
+void put_back_in_box(System &s);
 
 // Fortran single-precision constants that the reference mixes into FP64 math.
 constexpr float kBoltz = 0.001986f;     // md.f90:41

@@ -74,6 +74,42 @@ int host_shake(System &s, std::vector<double> &xx, std::vector<double> &x) {
 
 }  // namespace
 
+// put_back_in_box (md.f90:15477-15600): molecules whose centre of mass left
+// the box (centred on the solute's mean position unless the centre is rigid)
+// move by one edge length per axis.
+void put_back_in_box(System &s) {
+  const Topology &t = s.top;
+  const RunInput &in = s.in;
+  const int N = s.natom, NS = t.nat_solute, nmol = t.nmol;
+  if (!in.rigid_box_center) {
+    const int n = NS > 0 ? NS : N;
+    double c[3] = {0, 0, 0};
+    for (int i = 0; i < n; i++)
+      for (int k = 0; k < 3; k++) c[k] += s.x[3 * i + k];
+    for (int k = 0; k < 3; k++) s.boxc[k] = c[k] / n;
+  }
+  int first = 0, last = nmol;   // [first, last) molecules
+  if (nmol > 1) {
+    const int nsolv = (N - NS) / (t.istart_mol[nmol - 1] - t.istart_mol[nmol - 2]);
+    if (!in.put_solute_back_in_box) first = nmol - nsolv;
+    if (!in.put_solvent_back_in_box) last = nmol - nsolv;
+  }
+  for (int m = first; m < last; m++) {
+    double cm[3] = {0, 0, 0};
+    for (int j = t.istart_mol[m]; j < t.istart_mol[m + 1]; j++)
+      for (int k = 0; k < 3; k++) cm[k] += s.x[3 * j + k] * s.mass_box[j];
+    for (int k = 0; k < 3; k++) {
+      cm[k] = cm[k] * s.mol_minv[m];
+      const double hi = s.boxc[k] + s.boxl[k] / 2, lo = s.boxc[k] - s.boxl[k] / 2;
+      double sh = 0.0;
+      if (cm[k] > hi) sh = -s.boxl[k];
+      else if (cm[k] < lo) sh = s.boxl[k];
+      if (sh != 0.0)
+        for (int j = t.istart_mol[m]; j < t.istart_mol[m + 1]; j++) s.x[3 * j + k] += sh;
+    }
+  }
+}
+
 void prepare(System &s) {
   RunInput &in = s.in;
   Topology &t = s.top;
@@ -96,6 +132,18 @@ void prepare(System &s) {
   s.natom = t.nat_pro;
   s.nwat = (s.natom - t.nat_solute) / 3;
   const int N = s.natom, NS = t.nat_solute;
+  // boundary (md.f90:14752-14788): the same in topology and input; the box
+  // must hold twice every cut-off
+  if (in.box != t.use_pbc) fail(QB_ERR_PARSE, "Must have same boundary (sphere or box) in topology and input file");
+  if (t.use_pbc) {
+    const double box_min = std::min(t.boxlength[0], std::min(t.boxlength[1], t.boxlength[2]));
+    if (!(box_min > in.Rcpp * 2)) fail(QB_ERR_PARSE, "Solute-solute cut-off radii too large");
+    if (!(box_min > in.Rcww * 2)) fail(QB_ERR_PARSE, "Solvent-solvent cut-off radii too large");
+    if (!(box_min > in.Rcpw * 2)) fail(QB_ERR_PARSE, "Solute-solvent cut-off radii too large");
+    if (!(box_min > in.Rcq * 2)) fail(QB_ERR_PARSE, "Q-atom cut-off radii too large");
+    if (!(box_min > in.RcLRF * 2)) fail(QB_ERR_PARSE, "LRF cut-off radii too large");
+    for (int k = 0; k < 3; k++) { s.boxl[k] = t.boxlength[k]; s.boxc[k] = t.boxcenter[k]; }
+  }
   const double deg2rad = fortran_deg2rad();
   for (auto &a : t.ang_th0) a = deg2rad * a;
   for (auto &p : t.tor_paths) p = 1.0f / p;
@@ -108,11 +156,12 @@ void prepare(System &s) {
   }
 
   // -------------------------------------------------------- prep_coord()
-  if (in.rexcl_i > t.rexcl_o) fail(QB_ERR_PARSE, "inner radius of restrained shell must be < exclusion radius");
+  // the restrained shell exists in the sphere only (md.f90:13627)
+  if (!t.use_pbc && in.rexcl_i > t.rexcl_o) fail(QB_ERR_PARSE, "inner radius of restrained shell must be < exclusion radius");
   double rexcl_i = in.rexcl_i;
   s.shell.assign(N, 0);
   s.nshellats = 0;
-  if (rexcl_i >= 0) {
+  if (!t.use_pbc && rexcl_i >= 0) {
     if (rexcl_i <= 1.00) rexcl_i = rexcl_i * t.rexcl_o;
     double rin2 = rexcl_i * rexcl_i;
     for (int ig = 0; ig < t.ncgp_solute; ig++) {
@@ -216,7 +265,13 @@ void prepare(System &s) {
   s.crgtot = 0;
   s.crgQtot = 0;
   s.rwat = t.rwat;
-  if (s.nwat > 0) {
+  if (s.nwat > 0 && t.use_pbc) {
+    // periodic box: no solvent sphere or polarisation shells (md.f90:13806)
+    s.crg_ow = t.crg[NS];
+    s.crg_hw = -s.crg_ow / 2.0f;
+    in.wpol_restr = false;
+    s.nwpolr_shell = 0;
+  } else if (s.nwat > 0) {
     s.crg_ow = t.crg[NS];
     s.crg_hw = -s.crg_ow / 2.0f;
     // wat_sphere (md.f90:14961)
@@ -654,9 +709,31 @@ void prepare(System &s) {
   // ------------------------------------------------------- coordinates/velocities
   if (in.restart) {
     std::vector<float> tc = s.ws_theta_corr;
-    read_restart(in.restart_file, N, s.x, s.v, s.nwpolr_shell, &tc);
+    // a periodic box's restart holds its edge lengths and centre after the
+    // velocities (md.f90:13670-13676)
+    read_restart(in.restart_file, N, s.x, s.v, s.nwpolr_shell, &tc, t.use_pbc ? s.boxl : nullptr,
+                 t.use_pbc ? s.boxc : nullptr);
     s.ws_theta_corr = tc;
   }
+  if (t.use_pbc) {
+    // molecule masses (md.f90:13861-13882): 1/sum of the type masses, and the
+    // per-atom mass as 1/winv in single precision
+    s.mol_minv.assign(t.nmol, 0.0);
+    for (int m = 0; m < t.nmol; m++) {
+      double tot = 0.0;
+      for (int j = t.istart_mol[m]; j < t.istart_mol[m + 1]; j++) tot += t.iaclib[t.iac[j]].mass;
+      s.mol_minv[m] = 1. / tot;
+    }
+    s.mass_box.resize(N);
+    for (int i = 0; i < N; i++) s.mass_box[i] = (double)(1.0f / s.winv[i]);
+    // control_box (md.f90:13852-13858): a new box size, molecules put back
+    if (in.control_box) {
+      for (int k = 0; k < 3; k++) s.boxl[k] = in.new_boxl[k];
+      if (in.put_solute_back_in_box || in.put_solvent_back_in_box) put_back_in_box(s);
+    }
+  }
+  s.randm_started = 0;
+  s.randm_state = 0;
   if (in.iseed > 0) {
     // maxwell (md.f90:3787) with gauss (1453) on randm (14408)
     Randm rng;
@@ -670,6 +747,9 @@ void prepare(System &s) {
         s.v[3 * i + k] = (a - 6.0) * sd + 0.0;
       }
     }
+    // randm keeps one sequence per run: the volume moves continue it
+    s.randm_started = 1;
+    s.randm_state = rng.irand;
     s.log += "maxwell velocities generated\n";
     // initial_shaking (md.f90:2506)
     std::vector<double> xx = s.x;
@@ -783,6 +863,23 @@ void System::fill_view(qb_sysview *v) const {
   v->rwal_fk = rwal_fk.data(); v->rwal_aMorse = rwal_a.data(); v->rwal_dMorse = rwal_dm.data();
   v->Ndegf = Ndegf; v->Ndegfree = Ndegfree; v->Ndegf_solute = Ndegf_solute; v->Ndegf_solvent = Ndegf_solvent;
   v->Ndegfree_solute = Ndegfree_solute; v->Ndegfree_solvent = Ndegfree_solvent; v->detail_temps = detail_temps;
+  v->use_pbc = t.use_pbc;
+  if (t.use_pbc) {
+    v->rigid_box_center = in.rigid_box_center;
+    v->put_solute_back_in_box = in.put_solute_back_in_box;
+    v->put_solvent_back_in_box = in.put_solvent_back_in_box;
+    v->constant_pressure = in.constant_pressure;
+    v->ivolume_cycle = in.ivolume_cycle;
+    v->pressure_seed = in.pressure_seed;
+    v->max_vol_displ = in.max_vol_displ;
+    v->pressure = in.pressure;
+    for (int k = 0; k < 3; k++) { v->boxlength[k] = boxl[k]; v->boxcenter[k] = boxc[k]; }
+    v->mol_mass_inv = mol_minv.data();
+    v->mass_box = mass_box.data();
+  }
+  v->qswitch = fep.qswitch;
+  v->randm_started = randm_started;
+  v->randm_state = randm_state;
 }
 
 }  // namespace qb

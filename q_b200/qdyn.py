@@ -167,8 +167,19 @@ def run(inp: str, out=sys.stdout, chunk: int = 1000) -> int:
     E, EQ = batch.energy_vectors(0)
     print("", file=out)
     print(write_out(E, EQ, None, ns, v.nwat, bool(v.use_LRF), v.nqat, v.nat_solute, od_last), file=out)
+    if v.use_pbc and v.constant_pressure:
+        # write_out's summary of the volume moves (md.f90:15425-15436)
+        bx = batch.box(0)
+        tries, acc = batch.volume_moves(0)
+        print("", file=out)
+        print("=========================== VOLUME CHANGE SUMMARY ===========================", file=out)
+        print("Final volume: %10.3f" % (bx[0] * bx[1] * bx[2]), file=out)
+        print("", file=out)
+        print("%16s%10s%10s%10s" % ("", "total", "accepted", "ratio"), file=out)
+        print("%-16s%10d%10d%10.3f" % ("Attempts", tries, acc, acc / tries if tries else 0.0), file=out)
+        print("=" * 79, file=out)
     tc = batch.theta_corr(0, v.nwpolr_shell) if v.nwpolr_shell > 0 else None
-    write_restart(final, batch.coords(0), batch.velocities(0), tc)
+    write_restart(final, batch.coords(0), batch.velocities(0), tc, batch.box(0) if v.use_pbc else None)
     if trj:
         trj.close()
     print("Total time of main loop: %24.1f(s)" % (time.time() - t0), file=out)

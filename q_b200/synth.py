@@ -99,6 +99,7 @@ class Topology:
     ff_type: int = 2                                 # 1 GROMOS, 2 AMBER, 3 CHARMM (Urey-Bradley, harmonic impropers)
     solvent_type: int = 0                            # 0 SPC-type water, 1 3-atom solvent (LJ on every site)
     water_h_lj: tuple = (0.0, 0.0)                   # sigma, epsilon of the water hydrogens
+    box: tuple | None = None                         # periodic box: (edge lengths, centre)
 
     # ----------------------------------------------------------- writer
     def write(self, path: str) -> None:
@@ -215,6 +216,15 @@ class Topology:
         for k in range(0, nt, 13):
             L.append(" ".join("%-5s" % "" for _ in self.types[k:k + 13]))
         L.append("%8d = solvent type (0=SPC,1=3-atom,2=general)" % self.solvent_type)
+        if self.box is not None:
+            # periodic box (topo.f90:1027-1034): no excluded atoms follow
+            lengths, centre = self.box
+            L.append("%8s = kind of boundary" % "PBC")
+            L.append("%8.3f%8.3f%8.3f = Size of box, x y z" % tuple(lengths))
+            L.append("%8.3f%8.3f%8.3f = Center coordinate of box" % tuple(centre))
+            with open(path, "w") as f:
+                f.write("\n".join(L) + "\n")
+            return
         L.append("%8.3f%8.3f = Exclusion, solvent radii" % (self.rexcl_o, self.rwat))
         L.append("%8.3f%8.3f%8.3f = Solute center" % (0.0, 0.0, 0.0))
         L.append("%8.3f%8.3f%8.3f = Solvent center" % (0.0, 0.0, 0.0))
@@ -505,28 +515,37 @@ def write_inp(path: str, top: str, fep: str | None, *, steps: int, stepsize: flo
               shell_force: float = 10.0, q_cutoff: float = 99.0, energy_file: str | None = None,
               trajectory: int = 0, trajectory_atoms=None, restart: str | None = None,
               sequence_restraints=None, separate_scaling: bool = False,
-              initial_temperature: float | None = None) -> None:
+              initial_temperature: float | None = None, pbc: dict | None = None, lrf_cutoff: float = 99.0,
+              volume_change: int | None = None, distance_restraints=None, lrf: bool = True) -> None:
     """A qdyn .inp (md.f90:2528-3262 sections).  With restart, coordinates
     and velocities come from that .re and no seed or initial temperature is
     written; trajectory > 0 adds the .dcd file and its [trajectory_atoms]
-    rows; sequence_restraints are rows "first last force_k to_centre heavy"."""
+    rows; sequence_restraints are rows "first last force_k to_centre heavy",
+    distance_restraints rows "i j d1 d2 force_k state".  pbc: the [PBC]
+    section's keys and values (md.f90:2583-2656), volume_change the
+    [intervals] key of constant pressure."""
     name = os.path.splitext(os.path.basename(path))[0]
-    L = ["[MD]", "steps %d" % steps, "stepsize %g" % stepsize, "temperature %g" % temp, "bath_coupling %g" % bath]
+    L = []
+    if pbc is not None:
+        L += ["[PBC]"] + ["%s %s" % (k, v) for k, v in pbc.items()] + [""]
+    L += ["[MD]", "steps %d" % steps, "stepsize %g" % stepsize, "temperature %g" % temp, "bath_coupling %g" % bath]
     if restart is None:
         t0 = temp if initial_temperature is None else initial_temperature
         L += ["random_seed %d" % seed, "initial_temperature %g" % t0]
     L += ["shake_solvent on", "shake_solute off", "shake_hydrogens %s" % ("on" if shake_hydrogens else "off"),
-          "lrf on"]
+          "lrf %s" % ("on" if lrf else "off")]
     if separate_scaling:
         L.append("separate_scaling on")
     L += ["", "[cut-offs]", "solute_solute 10", "solvent_solvent 10", "solute_solvent 10",
-         "q_atom %g" % q_cutoff, "lrf 99", "", "[sphere]"]
+         "q_atom %g" % q_cutoff, "lrf %g" % lrf_cutoff, "", "[sphere]"]
     if shell_radius is not None:
         L.append("shell_radius %g" % shell_radius)
     L += ["shell_force %g" % shell_force, "", "[solvent]", "radial_force 60.0", "polarization on",
           "polarization_force 20.0", "", "[intervals]", "non_bond %d" % non_bond, "output %d" % output,
-          "energy %d" % energy, "trajectory %d" % trajectory, "", "[files]",
-          "topology %s" % os.path.basename(top), "final %s.re" % name]
+          "energy %d" % energy, "trajectory %d" % trajectory]
+    if volume_change is not None:
+        L.append("volume_change %d" % volume_change)
+    L += ["", "[files]", "topology %s" % os.path.basename(top), "final %s.re" % name]
     if restart:
         L.append("restart %s" % os.path.basename(restart))
     if energy > 0:
@@ -541,6 +560,8 @@ def write_inp(path: str, top: str, fep: str | None, *, steps: int, stepsize: flo
         L += ["", "[lambdas]", " ".join("%g" % x for x in lambdas)]
     if sequence_restraints:
         L += ["", "[sequence_restraints]"] + list(sequence_restraints)
+    if distance_restraints:
+        L += ["", "[distance_restraints]"] + list(distance_restraints)
     with open(path, "w") as f:
         f.write("\n".join(L) + "\n")
 
@@ -772,6 +793,83 @@ def fep_solute(outdir: str, radius: float = 20.0, seed: int = 1234, steps: int =
               couplings=morse_couplings)
     inp = os.path.join(outdir, name + ".inp")
     write_inp(inp, tp, fp, steps=steps, stepsize=2.0, seed=run_seed, lambdas=lambdas, shake_hydrogens=True)
+    return Generated(inp, tp, fp, len(top.x), len(waters))
+
+
+def box_waters(edge: float, rng, avoid: np.ndarray | None = None, r_o: float = 2.8) -> list[np.ndarray]:
+    """TIP3P waters filling a cubic periodic box of the given edge, centred on
+    the origin: a lattice of n^3 sites (n = edge * DENSITY^(1/3), rounded) that
+    tiles the box, seeded random orientations; waters with O within r_o of an
+    `avoid` atom (nearest image) are dropped."""
+    n = max(2, int(round(edge * DENSITY ** (1.0 / 3.0))))
+    a = edge / n
+    g = (np.arange(n) + 0.5) * a - edge / 2
+    P = np.array(np.meshgrid(g, g, g, indexing="ij")).reshape(3, -1).T
+    if avoid is not None and len(avoid):
+        from scipy.spatial import cKDTree
+        d, _ = cKDTree(np.mod(avoid + edge / 2, edge), boxsize=edge).query(np.mod(P + edge / 2, edge))
+        P = P[d >= r_o]
+    t = _water_template()
+    return [p + t @ _rot(rng).T for p in P]
+
+
+def fep_box(outdir: str, edge: float = 30.0, seed: int = 1234, steps: int = 1000, name: str = "pbc",
+            lambdas=(0.5, 0.5), run_seed: int = 1, constant_pressure: bool = False, volume_change: int = 10,
+            max_volume_displ: float = 300.0, pressure_seed: int = 3781, put_back: bool = True,
+            rigid_box_center: bool = False, lrf: float | None = 14.0, q_cutoff: float = 12.0,
+            distance_restraints=None) -> Generated:
+    """The FEP solute of fep_solute (56 atoms, 8 two-state Q-atoms) in a
+    cubic periodic box of TIP3P water (use_PBC): 2 fs, SHAKE on X-H bonds and
+    water, 10 A cut-offs, Q-atom cut-off q_cutoff around the first Q atom
+    (the FEP file's [PBC] switching_atom), LRF to `lrf` A (None: no LRF).  constant_pressure
+    adds Monte Carlo volume moves every volume_change steps (MC_volume);
+    put_back puts solute and solvent back in the box at the list steps."""
+    os.makedirs(outdir, exist_ok=True)
+    rng = np.random.default_rng(seed)
+    X, kinds, bonds = random_tree_solute(rng)
+    types, iac = _tree_types(kinds)
+    n = len(X)
+    top = Topology(title="fep_box", types=types, box=((edge, edge, edge), (0.0, 0.0, 0.0)))
+    top.x = [tuple(float(c) for c in p) for p in X]
+    top.iac = iac
+    top.crg = _solute_charges(rng, kinds)
+    _solute_terms(top, X, bonds, rng)
+    top.nat_solute = n
+    top.nbonds_solute, top.nangles_solute = len(top.bonds), len(top.angles)
+    top.ntors_solute, top.nimps_solute = len(top.tors), len(top.imps)
+    nb = [[] for _ in range(n)]
+    for i, j in bonds:
+        nb[i].append(j)
+        nb[j].append(i)
+    for i in range(n):
+        if kinds[i] >= 0:
+            top.cgps.append((i, [i] + sorted(j for j in nb[i] if kinds[j] < 0)))
+    top.ncgp_solute = len(top.cgps)
+    top.mol_starts = [0]
+    top.res_starts, top.res_names = [0], ["LIG"]
+    _finish_solute_lists(top, bonds, n)
+    waters = box_waters(edge, rng, avoid=X)
+    _add_waters(top, waters)
+    tp = os.path.join(outdir, name + ".top")
+    top.write(tp)
+    fp = os.path.join(outdir, name + ".fep")
+    heavy = [i for i in range(n) if kinds[i] >= 0]
+    qat = heavy[:8]
+    _fep_file(fp, types, iac, top.crg, qat)
+    with open(fp, "a") as f:
+        f.write("\n[PBC]\nswitching_atom %d\n" % (qat[0] + 1))
+    pbc = {"rigid_box_center": "on" if rigid_box_center else "off",
+           "constant_pressure": "on" if constant_pressure else "off",
+           "put_solvent_back_in_box": "on" if put_back else "off",
+           "put_solute_back_in_box": "on" if put_back else "off"}
+    if constant_pressure:
+        pbc.update({"max_volume_displ": "%g" % max_volume_displ, "pressure_seed": "%d" % pressure_seed,
+                    "pressure": "1.0"})
+    inp = os.path.join(outdir, name + ".inp")
+    write_inp(inp, tp, fp, steps=steps, stepsize=2.0, seed=run_seed, lambdas=lambdas, shake_hydrogens=True,
+              pbc=pbc, lrf_cutoff=lrf or 0.0, q_cutoff=q_cutoff,
+              volume_change=volume_change if constant_pressure else None,
+              distance_restraints=distance_restraints, lrf=lrf is not None)
     return Generated(inp, tp, fp, len(top.x), len(waters))
 
 

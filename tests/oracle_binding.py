@@ -90,6 +90,17 @@ class OracleRun:
         self.lib.qo_offdiag(self.st, kind, out.ctypes.data_as(C.POINTER(C.c_double)))
         return out[:c * n].reshape(c, n)
 
+    def box(self):
+        """Periodic box: edge lengths and centre (6 values)."""
+        out = np.zeros(6)
+        self.lib.qo_box(self.st, out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out
+
+    def volume_moves(self):
+        t, a = C.c_longlong(), C.c_longlong()
+        self.lib.qo_volume_moves(self.st, C.byref(t), C.byref(a))
+        return t.value, a.value
+
     def list_counts(self):
         out = (C.c_int * 5)()
         self.lib.qo_list_counts(self.st, out)
@@ -118,4 +129,6 @@ def load_oracle() -> Oracle:
     lib.qo_offdiag.argtypes = [vp, C.c_int, dp]
     lib.qo_list_counts.argtypes = [vp, C.POINTER(C.c_int)]
     lib.qo_status.argtypes = [vp]
+    lib.qo_box.argtypes = [vp, dp]
+    lib.qo_volume_moves.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
     return Oracle(lib)

@@ -92,11 +92,13 @@ def test_error_paths(tmp_path, golden):
     with pytest.raises(QBError) as e:
         System.open(str(tmp_path / "missing.inp"))
     assert e.value.code == 2
-    bad = tmp_path / "pbc.inp"
-    bad.write_text("[PBC]\nrigid_box_center off\n[MD]\nsteps 1\n")
+    # a periodic-box input with a sphere topology (md.f90:14752-14755)
+    txt0 = (golden / "benzene" / "eq1.inp").read_text()
+    txt0 = txt0.replace("benzene-vacuum.top", str(golden / "benzene" / "benzene-vacuum.top"))
+    (tmp_path / "pbc.inp").write_text("[PBC]\nrigid_box_center off\n" + txt0)
     with pytest.raises(QBError) as e:
-        System.open(str(bad))
-    assert e.value.code == 4
+        System.open(str(tmp_path / "pbc.inp"))
+    assert e.value.code == 3 and "same boundary" in str(e.value)
     txt = (golden / "benzene" / "eq1.inp").read_text().replace("stepsize                  1", "stepsize x")
     (tmp_path / "b.inp").write_text(txt.replace("benzene-vacuum.top", str(golden / "benzene" / "benzene-vacuum.top")))
     with pytest.raises(QBError) as e:

@@ -331,16 +331,21 @@ struct Batch {
     if (max_ncgp_sol_w > 0)
       launch("nb_pw", [&] { k_nb_pw<<<dim3(cdiv(p.pwg_cap, PW_BLOCK), max_ncgp_sol_w, nsys), PW_BLOCK, 0, s1>>>(p); });
     if (max_nwat > 0) {
-      dim3 gw(cdiv(max_nwat, ww_wpb), nsys);
+      dim3 gw(p.n_ww_tiles, 1);
       const int wpb = ww_wpb;
       size_t smem = (size_t)p.ww_chunk * (fast_ww ? WatRec<true>::words : WatRec<false>::words) * sizeof(float4);
       // hydrogen LJ: the whole batch takes the variant (exact zeros for systems without)
       if (fast_ww && any_hlj) {
         launch("nb_ww", [&] { k_nb_ww<true, true><<<gw, WW_BLOCK, smem, stream>>>(p, wpb); });
-      } else if (fast_ww && any_box) {
-        launch("nb_ww_x2", [&] { k_nb_ww_x2<true><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb); });
       } else if (fast_ww) {
-        launch("nb_ww_x2", [&] { k_nb_ww_x2<false><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb); });
+        // three blocks per SM when the staging chunk allows it
+        const bool three = smem <= (size_t)WWX_SMEM3;
+        launch("nb_ww_x2", [&] {
+          if (any_box && three) k_nb_ww_x2<true, 3><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb);
+          else if (any_box) k_nb_ww_x2<true, 2><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb);
+          else if (three) k_nb_ww_x2<false, 3><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb);
+          else k_nb_ww_x2<false, 2><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb);
+        });
       } else if (any_hlj) {
         launch("nb_ww", [&] { k_nb_ww<false, true><<<gw, WW_BLOCK, smem, stream>>>(p, wpb); });
       } else {
@@ -387,6 +392,63 @@ struct Batch {
     for (auto &row : graph)
       for (auto &g : row)
         if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    for (auto &c : cycle_graphs) cudaGraphExecDestroy(c.second.first);
+    cycle_graphs.clear();
+  }
+
+  // Graphs of a whole list cycle: NB steps from a rebuild step, captured
+  // once per pattern of energy-recording steps (bit k + 1: step k records;
+  // bit 0: the run ends with the cycle) and
+  // replayed as one launch.  Used when every system shares one non-bond
+  // interval of at most 62 steps and no volume moves interrupt the cycle.
+  std::map<unsigned long long, std::pair<cudaGraphExec_t, long long>> cycle_graphs;
+  bool cycle_ok() const {
+    if (!use_graphs || profiling || any_npt || NB > 62 || NB < 2) return false;
+    for (auto &S : sysh)
+      if (S.NB != NB) return false;
+    return true;
+  }
+
+  // nsteps >= NB steps from a rebuild step as one cycle graph; `last`: the
+  // cycle's last step is the run's last (it evaluates energies)
+  void cycle(bool last) {
+    unsigned long long key = last ? 1ull : 0ull;
+    const long long i0 = istep;
+    for (int k = 0; k < NB; k++) {
+      istep = i0 + k;
+      const int ene = (opt.precision != QB_MIXED || energy_due() || (last && k == NB - 1)) ? 1 : 0;
+      if (ene) key |= 2ull << k;
+    }
+    istep = i0;
+    auto it = cycle_graphs.find(key);
+    if (it == cycle_graphs.end()) {
+      cudaGraph_t g = nullptr;
+      long long l0 = launches;
+      CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      try {
+        for (int k = 0; k < NB; k++) {
+          istep = i0 + k;
+          const int ene = (key >> (k + 1)) & 1ull;
+          step_kernels(k == 0 ? 1 : 0, ene);
+        }
+      } catch (...) {
+        istep = i0;
+        cudaStreamEndCapture(stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      istep = i0;
+      CUDA_TRY(cudaStreamEndCapture(stream, &g));
+      cudaGraphExec_t ge = nullptr;
+      cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) fail(QB_ERR_CUDA, std::string("graph instantiation: ") + cudaGetErrorString(e));
+      it = cycle_graphs.emplace(key, std::make_pair(ge, launches - l0)).first;
+      launches = l0;
+    }
+    CUDA_TRY(cudaGraphLaunch(it->second.first, stream));
+    launches += it->second.second;
+    istep = i0 + NB;
   }
 
   bool lists_stale = false;
@@ -426,10 +488,18 @@ struct Batch {
 
   // nsteps steps, the last of them with energies
   void steps(int nsteps) {
-    for (int k = 0; k < nsteps; k++) {
+    const bool cyc = cycle_ok();
+    for (int k = 0; k < nsteps;) {
+      // whole list cycles as one graph launch each, single steps elsewhere
+      if (cyc && !lists_stale && istep % NB == 0 && nsteps - k >= NB) {
+        cycle(k + NB == nsteps);
+        k += NB;
+        continue;
+      }
       force_energy = k == nsteps - 1;
       step();
       if (any_npt) mc_volume(istep - 1);
+      k++;
     }
     force_energy = false;
   }
@@ -685,7 +755,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   std::vector<int> iac, iq, cgp, asys;
   std::vector<uint8_t> flags, ljcod;
   std::vector<uint32_t> lx, l14;
-  std::vector<int2> exl, l14l;
+  std::vector<std::vector<int>> exl_at, l14_at;   // per global atom: distant exclusion / 1-4 partners
   std::vector<int> cg_first, cg_last, cg_sw, cg_atoms, cg_sys;
   std::vector<int2> lrft;
   std::vector<PwAtom> pwa;
@@ -717,8 +787,6 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   long long pp_tot = 0, qp_tot = 0, qw_tot = 0;
   int ncgp_sol_tot = 0, pwg_cap = 32;
 
-  std::vector<SysState> st_box(n);
-  std::memset(st_box.data(), 0, sizeof(SysState) * n);
   for (int s = 0; s < n; s++) {
     const qb_sysview &V = B.views[s];
     SysDev &S = B.sysh[s];
@@ -754,10 +822,18 @@ void build(Batch &B, qb_handle *const *hs, int n) {
       l14.push_back(i < V.nat_solute ? V.list14_bits[i] : 0u);
     }
     for (int k = 0; k < V.natyps * V.natyps; k++) ljcod.push_back(V.ljcod[k]);
-    S.exl_off = (int)exl.size(); S.nexl = V.nexlong;
-    for (int k = 0; k < V.nexlong; k++) exl.push_back(make_int2(V.listexlong[2 * k], V.listexlong[2 * k + 1]));
-    S.l14_off = (int)l14l.size(); S.nl14 = V.n14long;
-    for (int k = 0; k < V.n14long; k++) l14l.push_back(make_int2(V.list14long[2 * k], V.list14long[2 * k + 1]));
+    exl_at.resize(x.size());
+    l14_at.resize(x.size());
+    for (int k = 0; k < V.nexlong; k++) {
+      const int a = aoff + V.listexlong[2 * k], b = aoff + V.listexlong[2 * k + 1];
+      exl_at[a].push_back(b);
+      exl_at[b].push_back(a);
+    }
+    for (int k = 0; k < V.n14long; k++) {
+      const int a = aoff + V.list14long[2 * k], b = aoff + V.list14long[2 * k + 1];
+      l14_at[a].push_back(b);
+      l14_at[b].push_back(a);
+    }
     for (int g = 0; g < V.ncgp; g++) {
       cg_first.push_back((int)cg_atoms.size() + (V.cgp_first[g] - V.cgp_first[0]));
       cg_last.push_back((int)cg_atoms.size() + (V.cgp_last[g] - V.cgp_first[0]));
@@ -959,11 +1035,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
       S.bH[0] = V.type_bvdw[3 * V.iac_hw]; S.bH[1] = V.type_bvdw[3 * V.iac_hw + 1];
     }
     SysState &st = sst[s];
-    {
-      const SysState keep = st_box[s];
-      std::memset(&st, 0, sizeof st);
-      for (int k = 0; k < 3; k++) { st.boxl[k] = keep.boxl[k]; st.iboxl[k] = keep.iboxl[k]; st.boxc[k] = keep.boxc[k]; }
-    }
+    std::memset(&st, 0, sizeof st);
     st.Tscale_sol = st.Tscale_solv = 1.0;
     for (int k = 0; k < S.nshell; k++) st.theta_corr[k] = V.wshell_theta_corr0[k];
     // periodic box (use_PBC, md.f90:4000-4200): box, Q switching atom and
@@ -978,15 +1050,16 @@ void build(Batch &B, qb_handle *const *hs, int n) {
       S.qp_once = 0;
       S.rigid_center = V.rigid_box_center;
       for (int k = 0; k < 3; k++) {
-        st_box[s].boxl[k] = V.boxlength[k];
-        st_box[s].iboxl[k] = 1.0 / V.boxlength[k];
-        st_box[s].boxc[k] = V.boxcenter[k];
+        sst[s].boxl[k] = V.boxlength[k];
+        sst[s].iboxl[k] = 1.0 / V.boxlength[k];
+        sst[s].boxc[k] = V.boxcenter[k];
         S.origin[k] = V.boxcenter[k];
       }
       S.mol_off = (int)mol_first.size();
       S.nmol = V.nmol;
+      // both tables take nmol + 1 entries per system (one offset for both)
       for (int m = 0; m <= V.nmol; m++) mol_first.push_back(aoff + V.istart_mol[m]);
-      for (int m = 0; m < V.nmol; m++) mol_minv.push_back(V.mol_mass_inv[m]);
+      for (int m = 0; m <= V.nmol; m++) mol_minv.push_back(m < V.nmol ? V.mol_mass_inv[m] : 0.0);
       // put_back_in_box's molecule range (md.f90:15529-15536): the solvent
       // molecules are the last (natom - nat_solute) / (atoms of the last one)
       S.put_first = 0; S.put_last = 0;
@@ -1115,7 +1188,21 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   P.crg = dev_upload(crg, o); P.winv = dev_upload(winv, o); P.mass = dev_upload(mass, o);
   P.iac = dev_upload(iac, o); P.iq = dev_upload(iq, o); P.cgp = dev_upload(cgp, o); P.asys = dev_upload(asys, o);
   P.flags = dev_upload(flags, o); P.lja = dev_upload(lja, o); P.ljb = dev_upload(ljb, o);
-  P.lx = dev_upload(lx, o); P.l14 = dev_upload(l14, o); P.exl = dev_upload(exl, o); P.l14l = dev_upload(l14l, o);
+  P.lx = dev_upload(lx, o); P.l14 = dev_upload(l14, o);
+  {
+    auto csr = [&](const std::vector<std::vector<int>> &at, int *&off_d, int *&part_d) {
+      std::vector<int> off(1, 0), part;
+      for (size_t a = 0; a < x.size(); a++) {
+        if (a < at.size()) part.insert(part.end(), at[a].begin(), at[a].end());
+        off.push_back((int)part.size());
+      }
+      if (part.empty()) part.push_back(-1);
+      off_d = dev_upload(off, o);
+      part_d = dev_upload(part, o);
+    };
+    csr(exl_at, P.exo, P.exq);
+    csr(l14_at, P.l14o, P.l14q);
+  }
   P.ljcod = dev_upload(ljcod, o);
   P.xtop = dev_upload(xtop, o);
   P.cg_first = dev_upload(cg_first, o); P.cg_last = dev_upload(cg_last, o); P.cg_sw = dev_upload(cg_sw, o);
@@ -1240,7 +1327,12 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, B.opt.device);
     B.ww_wpb = WW_WPB;
-    while (B.ww_wpb > 32 && (long long)n * Batch::cdiv(B.max_nwat, B.ww_wpb) < 2LL * sms) B.ww_wpb /= 2;
+    auto blocks = [&](int wpb) {
+      long long t = 0;
+      for (int s = 0; s < n; s++) t += (B.sysh[s].nwat + wpb - 1) / wpb;
+      return t;
+    };
+    while (B.ww_wpb > 32 && blocks(B.ww_wpb) < 2LL * sms) B.ww_wpb /= 2;
   }
   // the split counts are sized for the smallest chunk a tuning may choose
   B.ww_chunk_max = P.ww_chunk;
@@ -1256,6 +1348,15 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     B.set_lrf_tpb(tpb);
     while (tpb > 1 && (long long)B.max_lrf_blocks * n < 2LL * sms) B.set_lrf_tpb(tpb /= 2);
   }
+  // water-water force blocks, system by system
+  {
+    std::vector<int2> tiles;
+    for (int s = 0; s < n; s++)
+      for (int i0 = 0; i0 < B.sysh[s].nwat; i0 += B.ww_wpb) tiles.push_back(make_int2(s, i0));
+    if (tiles.empty()) tiles.push_back(make_int2(0, 0));
+    P.n_ww_tiles = (int)tiles.size();
+    P.ww_tiles = dev_upload(tiles, o);
+  }
   P.ww_cap = ww_cap;
   P.ww = dev_alloc<uint16_t>((size_t)std::max(woff, 1) * ww_cap, o);
   P.ww_n = dev_alloc<int>(std::max(woff, 1), o);
@@ -1270,8 +1371,10 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem64));
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem64));
-  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
-  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<false, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, WWX_SMEM3));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<true, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, WWX_SMEM3));
   P.kin_nblk = std::max(1, (B.max_natom + KIN_BLOCK - 1) / KIN_BLOCK);
   P.kin = dev_alloc<double>((size_t)n * 4, o);
   P.E = dev_alloc<double>((size_t)n * QB_NE, o);

@@ -40,7 +40,6 @@ struct PwAtom {
 struct SysDev {
   int aoff, natom, nsol, nwat, woff, coff, ncgp, ncgp_sol;
   int qoff, nq, S, natyps, ljoff, qlib_off, sc_off, qconn_off;
-  int exl_off, nexl, l14_off, nl14;
   int lrft_off, nlrft;        // LRF gather tiles (group ranges)
   // static term ranges (global offsets into term arrays)
   int b_off, nb, nb_sol, a_off, na, na_sol, t_off, nt, nt_sol, i_off, ni, ni_sol;
@@ -118,7 +117,9 @@ struct DevPtrs {
   uint8_t *flags;
   double *lja, *ljb;        // [3*g + code-1]
   uint32_t *lx, *l14;       // exclusion / 1-4 bits per atom (solute atoms)
-  int2 *exl, *l14l;         // long lists (local indices), per system segments
+  // exclusion / 1-4 pairs beyond the bit range, per atom: partners (global
+  // atoms, both directions) of atom g at [exo[g], exo[g+1]) and [l14o[g], l14o[g+1])
+  int *exo, *exq, *l14o, *l14q;
   uint8_t *ljcod;           // per system natyps^2
   const double *xtop;       // [3*g]
   // charge groups
@@ -178,6 +179,8 @@ struct DevPtrs {
   uint16_t *ww;                            // [gw*ww_cap + k] local water index
   int *ww_n, *ww_sp;                       // count per water; [gw*ww_nch + c] count below chunk c's end
   int ww_cap, ww_chunk, ww_nch;
+  int2 *ww_tiles;                          // water-water force blocks: (system, first water)
+  int n_ww_tiles;
   int lrf_tpb;                             // source tiles swept by one block of the LRF gather
   // energies
   double *kin;                             // [s*4] kinetic energy of this step: solute all, free, solvent all, free

@@ -774,6 +774,16 @@ __global__ void __launch_bounds__(WL_BLOCK) k_list_ww(DevPtrs P, int force) {
   }
 }
 
+// exclusions and 1-4 pairs: bits for atoms within QB_NBR_RANGE of each other
+// (listex/list14), else the atoms' own lists of distant partners (the
+// reference scans its whole long list, md.f90:5376-5382; each atom's partners
+// are the same pairs)
+__device__ __forceinline__ bool long_partner(const int *off, const int *part, int i, int j) {
+  for (int k = off[i]; k < off[i + 1]; k++)
+    if (part[k] == j) return true;
+  return false;
+}
+
 __device__ __forceinline__ bool excluded_pair(const DevPtrs &P, const SysDev &S, int i, int j) {
   // i, j global solute atoms
   int d = j - i;
@@ -781,12 +791,7 @@ __device__ __forceinline__ bool excluded_pair(const DevPtrs &P, const SysDev &S,
     if (d > 0) return (P.lx[i] >> (d - 1)) & 1u;
     return (P.lx[j] >> (-d - 1)) & 1u;
   }
-  int li = i - S.aoff, lj = j - S.aoff;
-  for (int n = 0; n < S.nexl; n++) {
-    int2 p = P.exl[S.exl_off + n];
-    if ((p.x == li && p.y == lj) || (p.x == lj && p.y == li)) return true;
-  }
-  return false;
+  return long_partner(P.exo, P.exq, i, j);
 }
 
 __device__ __forceinline__ bool is14(const DevPtrs &P, const SysDev &S, int i, int j) {
@@ -795,13 +800,7 @@ __device__ __forceinline__ bool is14(const DevPtrs &P, const SysDev &S, int i, i
     if (d > 0) return (P.l14[i] >> (d - 1)) & 1u;
     return (P.l14[j] >> (-d - 1)) & 1u;
   }
-  int li = i - S.aoff, lj = j - S.aoff;
-  bool r = false;
-  for (int n = 0; n < S.nl14; n++) {
-    int2 p = P.l14l[S.l14_off + n];
-    if ((p.x == li && p.y == lj) || (p.x == lj && p.y == li)) r = true;
-  }
-  return r;
+  return long_partner(P.l14o, P.l14q, i, j);
 }
 
 __device__ __forceinline__ int ljcode(const DevPtrs &P, const SysDev &S, int gi, int gj) {
@@ -1220,10 +1219,12 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P, in
   extern __shared__ float4 wsm[];
   __shared__ int2 srange[WW_WPB];          // list slice of each of the block's waters in this chunk
   constexpr int W = WatRec<MIXED>::words;
-  int s = blockIdx.y;
+  // the block's (system, first water) from the batch's tile list: no empty
+  // blocks for the systems with fewer waters
+  const int2 tile = P.ww_tiles[blockIdx.x];
+  const int s = tile.x;
   const SysDev &S = P.sys[s];
-  const int i0 = blockIdx.x * wpb;
-  if (i0 >= S.nwat) return;
+  const int i0 = tile.y;
   const int i1 = min(i0 + wpb, S.nwat);
   const int hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
   const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
@@ -1424,18 +1425,21 @@ __device__ __forceinline__ void ww_force_x2(const WwI2 &I, const float4 j0, cons
 // terms of ww_force_x2.  Energies are left to the steps that record them,
 // which evaluate the water-water pairs in FP64 (k_nb_ww<false>).  SPC water
 // only (no hydrogen Lennard-Jones).
-// 256 threads, two blocks per SM: one block's staging of records overlaps the
-// other's pair work (the registers of the packed path allow 16 warps per SM)
+// 256 threads; MINB blocks per SM: 2 with the largest staging chunk (112 KB
+// each), 3 when the chunk fits 74 KB (the register budget then drops from
+// 128 to 85 per thread, without spills): one block's staging of records
+// overlaps the others' pair work.
 constexpr int WWX_BLOCK = 256;
-template <bool BOX>
-__global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P, int wpb) {
+constexpr int WWX_SMEM3 = 74 * 1024;     // largest staging of the three-block variant
+template <bool BOX, int MINB>
+__global__ void __launch_bounds__(WWX_BLOCK, MINB) k_nb_ww_x2(DevPtrs P, int wpb) {
   extern __shared__ float4 wsm[];
   __shared__ int2 srange[WW_WPB];
   constexpr int W = WatRec<true>::words;
-  const int s = blockIdx.y;
+  const int2 tile = P.ww_tiles[blockIdx.x];
+  const int s = tile.x;
   const SysDev &S = P.sys[s];
-  const int i0 = blockIdx.x * wpb;
-  if (i0 >= S.nwat) return;
+  const int i0 = tile.y;
   const int i1 = min(i0 + wpb, S.nwat);
   const int hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
   const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;

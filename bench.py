@@ -448,6 +448,10 @@ def main():
     batch.run(args.equil)
     tuning = batch.autotune(50) if not args.no_autotune else batch.tuning()
     batch.run(max(args.warmup, 3))
+    # the energy-record capacity of a timed run (growing it would drop the
+    # step graphs), then every list-cycle graph captured
+    batch.run(max(args.steps, 1))
+    batch.clear_history()
     prime_cycle_graphs(batch, views)
     batch.clear_history()
 

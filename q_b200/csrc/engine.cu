@@ -309,8 +309,11 @@ struct Batch {
     // Q bonded, restraints)
     {
       SoluteGrid G{};
-      G.pp = max_pp > 0 ? std::min(cdiv(max_pp, 256), 64) : 0;
-      G.qp = any_q && max_qp > 0 ? std::min(cdiv(max_qp, 256), 32) : 0;
+      // pair blocks per system: enough for a large solute to fill the SMs
+      // when the batch is small (1184 = 8 blocks per SM over the batch)
+      const int cap = std::max(8, 1184 / std::max(nsys, 1));
+      G.pp = max_pp > 0 ? std::min(cdiv(max_pp, 256), cap) : 0;
+      G.qp = any_q && max_qp > 0 ? std::min(cdiv(max_qp, 256), cap) : 0;
       G.bonded = max_terms > 0 ? cdiv(max_terms, 256) : 0;
       G.qq = any_qq ? 1 : 0;
       G.qb = any_qb ? 1 : 0;
@@ -329,7 +332,11 @@ struct Batch {
         });
     }
     if (max_ncgp_sol_w > 0)
-      launch("nb_pw", [&] { k_nb_pw<<<dim3(cdiv(p.pwg_cap, PW_BLOCK), max_ncgp_sol_w, nsys), PW_BLOCK, 0, s1>>>(p); });
+      launch("nb_pw", [&] {
+        const dim3 g(cdiv(p.pwg_cap, PW_BLOCK), max_ncgp_sol_w, nsys);
+        if (fast_ww) k_nb_pw<true><<<g, PW_BLOCK, 0, s1>>>(p);
+        else k_nb_pw<false><<<g, PW_BLOCK, 0, s1>>>(p);
+      });
     if (max_nwat > 0) {
       dim3 gw(p.n_ww_tiles, 1);
       const int wpb = ww_wpb;
@@ -359,6 +366,15 @@ struct Batch {
           return;
         }
         if (max_nq > NQ_SHARED) { k_nb_qw<0, false, false><<<g, 128, 0, s2>>>(p); return; }
+        // the mixed engine's non-recording steps: forces alone in FP32
+        if (fast_ww) {
+          switch (q_states) {
+            case 1: k_nb_qw<1, true, false, true><<<g, 128, 0, s2>>>(p); break;
+            case 2: k_nb_qw<2, true, false, true><<<g, 128, 0, s2>>>(p); break;
+            default: k_nb_qw<0, true, false, true><<<g, 128, 0, s2>>>(p);
+          }
+          return;
+        }
         switch (q_states) {
           case 1: k_nb_qw<1, true, false><<<g, 128, 0, s2>>>(p); break;
           case 2: k_nb_qw<2, true, false><<<g, 128, 0, s2>>>(p); break;
@@ -1409,6 +1425,8 @@ void ensure_history(Batch &B, int nsteps) {
   for (auto &x : st) used = std::max(used, std::max(x.hist_n[0], x.hist_n[1]));
   long long cap = used + need;
   if (cap <= B.P.hist_cap) return;
+  // grow at least twofold: each growth drops the step graphs
+  cap = std::max(cap, 2LL * B.P.hist_cap);
   size_t rec = HIST_REC;
   double *nh = nullptr;
   CUDA_TRY(cudaMalloc(&nh, sizeof(double) * rec * cap * 2 * B.nsys));

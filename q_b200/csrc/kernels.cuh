@@ -22,6 +22,12 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+__device__ __forceinline__ float warp_sumf(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  return v;
+}
+
 // Reduce v over the warp and add it to *dst once (lane 0).  All 32 lanes of
 // the warp must call it.
 __device__ __forceinline__ void warp_add(double *dst, double v) {
@@ -1599,6 +1605,11 @@ __device__ __forceinline__ void nb_pp_body(DevPtrs &P, int bx, int s, int gx) {
 // the warp and added with one atomic per warp.
 constexpr int PW_BLOCK = 128, PW_MAXA = 128;   // group atoms staged in shared memory
 
+// F32: the mixed engine's steps that record no energies take the forces
+// alone in FP32 (differences of the FP64 positions rounded to FP32, MUFU
+// reciprocal square root), as its water-water kernel does; energy-recording
+// steps run the FP64 form.
+template <bool F32>
 __global__ void __launch_bounds__(PW_BLOCK) k_nb_pw(DevPtrs P) {
   const int s = blockIdx.z;
   const SysDev &S = P.sys[s];
@@ -1633,8 +1644,9 @@ __global__ void __launch_bounds__(PW_BLOCK) k_nb_pw(DevPtrs P) {
   }
   __syncthreads();
   double fw[9];
+  float fw32[9];
 #pragma unroll
-  for (int c = 0; c < 9; c++) fw[c] = 0.0;
+  for (int c = 0; c < 9; c++) { fw[c] = 0.0; fw32[c] = 0.f; }
   double el = 0, vdw = 0;
   const int t1 = P.pwg_off[sg + 1];
   for (int t = ta; t < t1; t++) {
@@ -1642,7 +1654,22 @@ __global__ void __launch_bounds__(PW_BLOCK) k_nb_pw(DevPtrs P) {
     const double4 x4 = t - ta < PW_MAXA ? sx[t - ta] : P.x[A.atom];
     const double3 xi = make_double3(x4.x, x4.y, x4.z);
     double fi[3] = {0.0, 0.0, 0.0};
-    if (act) {
+    if (act && F32) {
+      float gi[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+      for (int b = 0; b < 3; b++) {
+        const float dx = (float)(xw[b].x - xi.x), dy = (float)(xw[b].y - xi.y), dz = (float)(xw[b].z - xi.z);
+        const float r = rsqrt_ftz(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+        const float r2 = r * r, r6 = r2 * r2 * r2;
+        const float Vel = (b == 0 ? A.q.x : A.q.y) * r;
+        const float Va = (float)(b == 0 ? A.lj.x : A.lj.z) * r6 * r6, Vb = (float)(b == 0 ? A.lj.y : A.lj.w) * r6;
+        const float dv = r2 * (-Vel - 12.f * Va + 6.f * Vb);
+        gi[0] = fmaf(-dv, dx, gi[0]); gi[1] = fmaf(-dv, dy, gi[1]); gi[2] = fmaf(-dv, dz, gi[2]);
+        fw32[3 * b] = fmaf(dv, dx, fw32[3 * b]); fw32[3 * b + 1] = fmaf(dv, dy, fw32[3 * b + 1]);
+        fw32[3 * b + 2] = fmaf(dv, dz, fw32[3 * b + 2]);
+      }
+      fi[0] = gi[0]; fi[1] = gi[1]; fi[2] = gi[2];
+    } else if (act) {
 #pragma unroll
       for (int b = 0; b < 3; b++) {
         double dx = xw[b].x - xi.x, dy = xw[b].y - xi.y, dz = xw[b].z - xi.z;
@@ -1661,10 +1688,15 @@ __global__ void __launch_bounds__(PW_BLOCK) k_nb_pw(DevPtrs P) {
     for (int c = 0; c < 3; c++) fi[c] = warp_sum(fi[c]);
     if (lane == 0) atomic_add3(P.d, A.atom, fi[0], fi[1], fi[2]);
   }
+  if (F32)
+#pragma unroll
+    for (int c = 0; c < 9; c++) fw[c] = (double)fw32[c];
   if (act)
     for (int b = 0; b < 3; b++) atomic_add3(P.d, o + b, fw[3 * b], fw[3 * b + 1], fw[3 * b + 2]);
-  warp_add(&P.E[s * QB_NE + QB_E_PW_EL], el);
-  warp_add(&P.E[s * QB_NE + QB_E_PW_VDW], vdw);
+  if (!F32) {
+    warp_add(&P.E[s * QB_NE + QB_E_PW_EL], el);
+    warp_add(&P.E[s * QB_NE + QB_E_PW_VDW], vdw);
+  }
 }
 
 // nonbond_qp (md.f90:10980) / nonbond_qp_qvdw (11138): one thread per pair,
@@ -1753,7 +1785,9 @@ __device__ __forceinline__ void nb_qp_body(DevPtrs &P, int bx, int s, int gx) {
 // hydrogen sites add LJ with their own type's parameters and soft-core shift.
 struct QwState { float qO, qH; double A, B, sc, AH, BH, scH; };
 
-template <int NSC, bool SHQ, bool HLJ>
+// F32 (with SHQ, without hydrogen LJ): the mixed engine's steps that record
+// no energies take the forces alone in FP32, as its water-water kernel does.
+template <int NSC, bool SHQ, bool HLJ, bool F32 = false>
 __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
   constexpr int NA = NSC > 0 ? NSC : MAXS;
   int s = blockIdx.y;
@@ -1818,8 +1852,56 @@ __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
     xH2.x -= t.x; xH2.y -= t.y; xH2.z -= t.z;
   }
   double fw[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  float fw32[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int iq = 0; iq < S.nq; iq++) {
     int gq = S.qoff + iq;
+    if (F32 && SHQ && !HLJ) {
+      // forces alone in FP32: differences of the FP64 positions rounded to
+      // FP32, MUFU reciprocal square roots, the states' sums in FP32
+      const double4 xi4 = qx[iq];
+      const float o[3] = {(float)(xO.x - xi4.x), (float)(xO.y - xi4.y), (float)(xO.z - xi4.z)};
+      const float h1[3] = {(float)(xH1.x - xi4.x), (float)(xH1.y - xi4.y), (float)(xH1.z - xi4.z)};
+      const float h2[3] = {(float)(xH2.x - xi4.x), (float)(xH2.y - xi4.y), (float)(xH2.z - xi4.z)};
+      const float r2O = fmaf(o[0], o[0], fmaf(o[1], o[1], o[2] * o[2]));
+      const float rO = rsqrt_ftz(r2O);
+      const float rH1 = rsqrt_ftz(fmaf(h1[0], h1[0], fmaf(h1[1], h1[1], h1[2] * h1[2])));
+      const float rH2 = rsqrt_ftz(fmaf(h2[0], h2[0], fmaf(h2[1], h2[1], h2[2] * h2[2])));
+      const float r2Oi = rO * rO, r2H1 = rH1 * rH1, r2H2 = rH2 * rH2;
+      const float r6hc = r2O * r2O * r2O;
+      float Va0 = 0.f, Vb0 = 0.f;
+      if (!S.qvdw) {
+        const float r6 = r2Oi * r2Oi * r2Oi;
+        Va0 = (float)qab[iq].x * r6 * r6;
+        Vb0 = (float)qab[iq].y * r6;
+      }
+      float dvO = 0.f, dvH1 = 0.f, dvH2 = 0.f;
+#pragma unroll
+      for (int st = 0; st < NA; st++) {
+        if (st >= NS) break;
+        const QwState q = qst[iq * NA + st];
+        float Va = Va0, Vb = Vb0, fsc = 1.f;
+        if (S.qvdw) {
+          const float inv = 1.f / (r6hc + (float)q.sc);
+          Va = (float)q.A * inv * inv;
+          Vb = (float)q.B * inv;
+          fsc = r6hc * inv;
+        }
+        const float lam = (float)S.lambda[st];
+        dvO += r2Oi * (-q.qO * rO - (12.f * Va - 6.f * Vb) * fsc) * lam;
+        dvH1 -= r2H1 * (q.qH * rH1) * lam;
+        dvH2 -= r2H2 * (q.qH * rH2) * lam;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const float qa = act ? -(dvO * o[c] + dvH1 * h1[c] + dvH2 * h2[c]) : 0.f;
+        fw32[c] = fmaf(dvO, o[c], fw32[c]);
+        fw32[3 + c] = fmaf(dvH1, h1[c], fw32[3 + c]);
+        fw32[6 + c] = fmaf(dvH2, h2[c], fw32[6 + c]);
+        const float t = warp_sumf(qa);
+        if ((threadIdx.x & 31) == 0 && t != 0.f) atomicAdd(&fq[3 * iq + c], (double)t);
+      }
+      continue;
+    }
     double4 xi4;
     int lj, ljh;
     double A0, B0, AH0 = 0, BH0 = 0;
@@ -1932,12 +2014,16 @@ __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
       }
     }
   }
+  if (F32 && SHQ && !HLJ)
+#pragma unroll
+    for (int c = 0; c < 9; c++) fw[c] = (double)fw32[c];
   if (act)
     for (int a = 0; a < 3; a++) atomic_add3(P.d, j + a, fw[3 * a], fw[3 * a + 1], fw[3 * a + 2]);
-  for (int st = 0; st < NS; st++) {
-    warp_add(&P.EQ[((size_t)s * MAXS + st) * QB_NEQ + QB_EQ_QW_EL], el[st]);
-    warp_add(&P.EQ[((size_t)s * MAXS + st) * QB_NEQ + QB_EQ_QW_VDW], vdw[st]);
-  }
+  if (!(F32 && SHQ && !HLJ))
+    for (int st = 0; st < NS; st++) {
+      warp_add(&P.EQ[((size_t)s * MAXS + st) * QB_NEQ + QB_EQ_QW_EL], el[st]);
+      warp_add(&P.EQ[((size_t)s * MAXS + st) * QB_NEQ + QB_EQ_QW_VDW], vdw[st]);
+    }
   __syncthreads();
   for (int t = threadIdx.x; t < nqs * 3; t += blockDim.x)
     if (fq[t] != 0.0) atomicAdd(&P.d[P.iqseq[S.qoff + t / 3]].x + (t % 3), fq[t]);

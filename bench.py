@@ -365,7 +365,12 @@ def per_config_lines(root: str, device: int, steps: int = 200):
         s = System.open(inp, lambdas=lam, seed=11)
         b = Batch([s], precision=FP64, device=device)
         b.run(50)
+        # record capacity and graphs of the timed run first (growing the
+        # records inside it would drop and recapture the step graphs)
+        b.run(steps)
+        b.clear_history()
         prime_cycle_graphs(b, [s.view])
+        b.clear_history()
         align_to_rebuild(b, [s.view])
         start = b.step_count()
         ms, launches = b.run_timed(steps)

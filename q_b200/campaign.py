@@ -109,7 +109,10 @@ def time_single_window(inp: str, lam, steps: int, *, precision: int = FP64, devi
     s = System.open(inp, lambdas=tuple(lam), seed=seed)
     b = Batch([s], precision=precision, device=device)
     try:
-        b.run(warmup)
+        # warm-up as long as the timed run: its record capacity and step
+        # graphs are in place before timing
+        b.run(max(warmup, steps))
+        b.clear_history()
         ms, _ = b.run_timed(steps)
     finally:
         b.close()

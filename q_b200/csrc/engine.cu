@@ -345,13 +345,9 @@ struct Batch {
       if (fast_ww && any_hlj) {
         launch("nb_ww", [&] { k_nb_ww<true, true><<<gw, WW_BLOCK, smem, stream>>>(p, wpb); });
       } else if (fast_ww) {
-        // three blocks per SM when the staging chunk allows it
-        const bool three = smem <= (size_t)WWX_SMEM3;
         launch("nb_ww_x2", [&] {
-          if (any_box && three) k_nb_ww_x2<true, 3><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb);
-          else if (any_box) k_nb_ww_x2<true, 2><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb);
-          else if (three) k_nb_ww_x2<false, 3><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb);
-          else k_nb_ww_x2<false, 2><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb);
+          if (any_box) k_nb_ww_x2<true><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb);
+          else k_nb_ww_x2<false><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb);
         });
       } else if (any_hlj) {
         launch("nb_ww", [&] { k_nb_ww<false, true><<<gw, WW_BLOCK, smem, stream>>>(p, wpb); });
@@ -1387,10 +1383,8 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem64));
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem64));
-  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
-  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
-  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<false, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, WWX_SMEM3));
-  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<true, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, WWX_SMEM3));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
   P.kin_nblk = std::max(1, (B.max_natom + KIN_BLOCK - 1) / KIN_BLOCK);
   P.kin = dev_alloc<double>((size_t)n * 4, o);
   P.E = dev_alloc<double>((size_t)n * QB_NE, o);

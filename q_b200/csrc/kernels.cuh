@@ -1431,14 +1431,13 @@ __device__ __forceinline__ void ww_force_x2(const WwI2 &I, const float4 j0, cons
 // terms of ww_force_x2.  Energies are left to the steps that record them,
 // which evaluate the water-water pairs in FP64 (k_nb_ww<false>).  SPC water
 // only (no hydrogen Lennard-Jones).
-// 256 threads; MINB blocks per SM: 2 with the largest staging chunk (112 KB
-// each), 3 when the chunk fits 74 KB (the register budget then drops from
-// 128 to 85 per thread, without spills): one block's staging of records
-// overlaps the others' pair work.
+// 256 threads, two blocks per SM: one block's staging of records overlaps
+// the other's pair work (the registers of the packed path allow 16 warps per
+// SM).  A three-block form (80 registers, staging chunks of up to 74 KB) ran
+// the kernel 13% slower alone, and the step no faster.
 constexpr int WWX_BLOCK = 256;
-constexpr int WWX_SMEM3 = 74 * 1024;     // largest staging of the three-block variant
-template <bool BOX, int MINB>
-__global__ void __launch_bounds__(WWX_BLOCK, MINB) k_nb_ww_x2(DevPtrs P, int wpb) {
+template <bool BOX>
+__global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P, int wpb) {
   extern __shared__ float4 wsm[];
   __shared__ int2 srange[WW_WPB];
   constexpr int W = WatRec<true>::words;

@@ -1555,11 +1555,18 @@ __device__ __forceinline__ void nb_pp_body(DevPtrs &P, int bx, int s, int gx) {
   int n = P.st[s].pp_n;
   const int4 *L = P.pp + S.pp_off;
   double el = 0, vdw = 0;
+  const int lane = threadIdx.x & 31;
   for (int k0 = bx * blockDim.x; k0 < n; k0 += gx * blockDim.x) {
     int k = k0 + threadIdx.x;
+    // the list holds each atom i's pairs of a group pair consecutively: the
+    // lanes with the same i sum their share of i's gradient over the warp and
+    // the first of them adds it with one atomic per component
+    double gi[3] = {0.0, 0.0, 0.0};
+    int i = -1 - lane;
     if (k < n) {
       int4 p = L[k];
-      int i = p.x, j = p.y, lj = p.z;
+      i = p.x;
+      int j = p.y, lj = p.z;
       double3 xi = ld3(P.x, i), xj = ld3(P.x, j);
       double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
       if (S.pbc) {
@@ -1585,11 +1592,28 @@ __device__ __forceinline__ void nb_pp_body(DevPtrs &P, int bx, int s, int gx) {
         Vb = r6 * P.ljb[3 * i + lj - 1] * P.ljb[3 * j + lj - 1];
       }
       double dv = r2 * (-Vel - 12. * Va + 6. * Vb);
-      atomic_add3(P.d, i, -dv * dx, -dv * dy, -dv * dz);
+      gi[0] = -dv * dx; gi[1] = -dv * dy; gi[2] = -dv * dz;
       atomic_add3(P.d, j, dv * dx, dv * dy, dv * dz);
       el += Vel;
       vdw += Va - Vb;
     }
+    // runs of equal i in consecutive lanes: a segmented sum towards each
+    // run's first lane (end: the next run's first lane)
+    const int prev = __shfl_up_sync(FULL, i, 1);
+    const bool head = lane == 0 || prev != i;
+    const unsigned heads = __ballot_sync(FULL, head);
+    const unsigned later = lane == 31 ? 0u : heads & ~((2u << lane) - 1u);
+    const int end = later ? __ffs(later) - 1 : 32;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const bool take = lane + o < end;
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const double t = __shfl_down_sync(FULL, gi[c], o);
+        if (take) gi[c] += t;
+      }
+    }
+    if (i >= 0 && head) atomic_add3(P.d, i, gi[0], gi[1], gi[2]);
   }
   warp_add(&P.E[s * QB_NE + QB_E_PP_EL], el);
   warp_add(&P.E[s * QB_NE + QB_E_PP_VDW], vdw);

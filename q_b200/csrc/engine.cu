@@ -1392,7 +1392,17 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   P.offd_r = dev_alloc<double>((size_t)n * MAXS, o);
   P.hist = nullptr;
   P.hist_cap = 0;
-  B.watpol_smem = (size_t)B.max_nwat * (sizeof(double) + sizeof(int));   // member angles and indices
+  {
+    const HistRef none{nullptr, 0};
+    P.hr = dev_alloc<HistRef>(1, o);
+    CUDA_TRY(cudaMemcpy(P.hr, &none, sizeof none, cudaMemcpyHostToDevice));
+  }
+  {
+    // member angles and indices, padded to a power of two for the sort
+    size_t np2 = 1;
+    while (np2 < (size_t)std::max(B.max_nwat, 1)) np2 <<= 1;
+    B.watpol_smem = np2 * (sizeof(double) + sizeof(int));
+  }
   P.wtheta = dev_alloc<double>(std::max(woff, 1), o);
   P.wshell = dev_alloc<int8_t>(std::max(woff, 1), o);
   P.wrank = dev_alloc<int>(std::max(woff, 1), o);
@@ -1419,8 +1429,7 @@ void ensure_history(Batch &B, int nsteps) {
   for (auto &x : st) used = std::max(used, std::max(x.hist_n[0], x.hist_n[1]));
   long long cap = used + need;
   if (cap <= B.P.hist_cap) return;
-  // grow at least twofold: each growth drops the step graphs
-  cap = std::max(cap, 2LL * B.P.hist_cap);
+  cap = std::max(cap, 2LL * B.P.hist_cap);   // at least twofold
   size_t rec = HIST_REC;
   double *nh = nullptr;
   CUDA_TRY(cudaMalloc(&nh, sizeof(double) * rec * cap * 2 * B.nsys));
@@ -1438,7 +1447,9 @@ void ensure_history(Batch &B, int nsteps) {
   }
   B.P.hist = nh;
   B.P.hist_cap = (int)cap;
-  B.drop_graphs();
+  // the kernels read the buffer through P.hr: the captured graphs stay valid
+  const HistRef ref{nh, (int)cap};
+  CUDA_TRY(cudaMemcpy(B.P.hr, &ref, sizeof ref, cudaMemcpyHostToDevice));
 }
 
 // Energy-record counts of every system back to zero.

@@ -100,6 +100,13 @@ struct SysState {
   double mc_oldl[3];
 };
 
+// The energy-record buffer as the kernels see it, read through a device
+// pointer so that captured graphs stay valid when the buffer grows.
+struct HistRef {
+  double *hist;
+  int cap;
+};
+
 struct DevPtrs {
   int nsys, natoms_tot, nwat_tot, ncgp_tot, nshake_tot;
   SysDev *sys;
@@ -191,6 +198,7 @@ struct DevPtrs {
   // history [kind][s][rec][QB_NE + MAXS*QB_NEQ + 1]
   double *hist;
   int hist_cap;
+  HistRef *hr;               // device copy of (hist, hist_cap) for the kernels
   // periodic box: molecule starts, 1/molecule mass, per-atom mass (1/winv)
   int *mol_first;
   double *mol_minv, *mass_box;

@@ -521,6 +521,7 @@ __device__ __forceinline__ void lrf_finish_x2(const float2 *m, const float2 *t, 
 // the group-pair window test is FP64.  Each block sums its tiles in FP32 and
 // adds the totals to the FP64 record with one atomic per component.
 constexpr int LRFX_BLOCK = 128, LRFX_TARGETS = 2 * LRFX_BLOCK;
+constexpr float LRFX_EPS2 = 4e-3f;
 
 template <bool BOX>
 __global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int force) {
@@ -534,13 +535,21 @@ __global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int 
   if (hsplit == 0 || gchunk * LRFX_TARGETS >= S.ncgp) return;
   const int t0 = hpart * tpb, t1 = min(t0 + tpb, S.nlrft);
   __shared__ double4 hsw[LRF_TILE_G];
+  __shared__ float4 hswf[LRF_TILE_G];                  // switching atoms relative to the origin, FP32
   __shared__ int2 hrange[LRF_TILE_G];
   __shared__ float4 hxy[LRF_TILE_A], hzq[LRF_TILE_A];   // {x, x, y, y}, {z, z, q, q}
   const double ox = S.origin[0], oy = S.origin[1], oz = S.origin[2];
   int gl[2];
   bool act[2], gsol[2];
   double3 xs[2], cen[2];
+  float3 xsf[2];
   float cc[2][3];
+  // the window test in FP32, the pairs within LRFX_EPS2 of either bound in
+  // FP64 (as the reference computes it): for positions within R of the
+  // origin the FP32 squared distance is within ~8.3e-7 R^2 A^2 of the FP64
+  // one, under the margin for R up to ~70 A (a sphere's atoms lie within its
+  // radius of the solute centre)
+  const float rlf = (float)S.RcLRF2;
 #pragma unroll
   for (int h = 0; h < 2; h++) {
     gl[h] = gchunk * LRFX_TARGETS + h * LRFX_BLOCK + threadIdx.x;
@@ -557,6 +566,7 @@ __global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int 
       cc[h][0] = (float)(L[0] - ox); cc[h][1] = (float)(L[1] - oy); cc[h][2] = (float)(L[2] - oz);
       xs[h] = ld3(P.x, swg);
     }
+    xsf[h] = make_float3((float)(xs[h].x - ox), (float)(xs[h].y - oy), (float)(xs[h].z - oz));
   }
   // minus the two target centres (positions relative to the origin); in a
   // periodic box each source group shifts them by its image (nbpplist_box_lrf
@@ -581,6 +591,7 @@ __global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int 
       const double3 p = ld3(P.x, sw);
       const double w = (P.flags[sw] & F_EXCL) ? -1.0 : (tile.x + i < S.ncgp_sol ? 1.0 : 0.0);
       hsw[i] = make_double4(p.x, p.y, p.z, w);
+      hswf[i] = make_float4((float)(p.x - ox), (float)(p.y - oy), (float)(p.z - oz), (float)w);
       hrange[i] = make_int2(P.cg_first[h] - a0, P.cg_last[h] - P.cg_first[h] + 1);
     }
     for (int i = threadIdx.x; i < na; i += LRFX_BLOCK) {
@@ -606,9 +617,21 @@ __global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int 
         if (!S.switch_atoms && (gsol[h] || hs.w > 0.0)) {
           in = act[h] && tile.x + i != gl[h] &&
                lrf_window_any(P, S, S.coff + gl[h], gsol[h], S.coff + tile.x + i, hs.w > 0.0, rc2);
+        } else if (!BOX) {
+          const float4 hf = hswf[i];
+          const float fx = xsf[h].x - hf.x, fy = xsf[h].y - hf.y, fz = xsf[h].z - hf.z;
+          const float r2f = fmaf(fx, fx, fmaf(fy, fy, fz * fz));
+          const float rcf = (float)rc2;
+          if (fabsf(r2f - rcf) > LRFX_EPS2 && fabsf(r2f - rlf) > LRFX_EPS2) {
+            in = act[h] && tile.x + i != gl[h] && r2f > rcf && r2f <= rlf;
+          } else {
+            const double dx = xs[h].x - hs.x, dy = xs[h].y - hs.y, dz = xs[h].z - hs.z;
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            in = act[h] && tile.x + i != gl[h] && r2 > rc2 && r2 <= S.RcLRF2;
+          }
         } else {
           double dx = xs[h].x - hs.x, dy = xs[h].y - hs.y, dz = xs[h].z - hs.z;
-          if (BOX) min_image(bx, dx, dy, dz);
+          min_image(bx, dx, dy, dz);
           const double r2 = dx * dx + dy * dy + dz * dz;
           in = act[h] && tile.x + i != gl[h] && r2 > rc2 && r2 <= S.RcLRF2;
         }
@@ -2821,31 +2844,35 @@ __global__ void __launch_bounds__(WPOL_BLOCK) k_watpol_rank(DevPtrs P) {
   }
   __syncthreads();
   const int n = cnt;
-  // rank = members before this one in (angle, water index) order; the
-  // shared-memory reads are broadcasts
-  double tsum = 0;
-  for (int m = threadIdx.x; m < n; m += WPOL_BLOCK) {
-    const long long th = kth[m];
-    const int iw = kiw[m];
-    // branch-free: both words of every key are read, no short-circuit
-    int r[4] = {0, 0, 0, 0};
-    int u = 0;
-    for (; u + 4 <= n; u += 4) {
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const long long tu = kth[u + q];
-        const int iu = kiw[u + q];
-        r[q] += (int)(tu < th) + ((int)(tu == th) & (int)(iu < iw));
-      }
-    }
-    for (; u < n; u++) {
-      const long long tu = kth[u];
-      const int iu = kiw[u];
-      r[0] += (int)(tu < th) + ((int)(tu == th) & (int)(iu < iw));
-    }
-    P.wrank[S.woff + iw] = r[0] + r[1] + r[2] + r[3];
-    tsum += __longlong_as_double(th);
+  // rank = position in (angle, water index) order: a bitonic sort of the
+  // members in shared memory, padded to a power of two with keys above every
+  // angle (the angles are non-negative doubles: their bit patterns order
+  // like them)
+  int np2 = 1;
+  while (np2 < n) np2 <<= 1;
+  for (int m = n + threadIdx.x; m < np2; m += WPOL_BLOCK) {
+    kth[m] = 0x7fffffffffffffffLL;
+    kiw[m] = 0x7fffffff;
   }
+  double tsum = 0;
+  for (int m = threadIdx.x; m < n; m += WPOL_BLOCK) tsum += __longlong_as_double(kth[m]);
+  __syncthreads();
+  for (int k = 2; k <= np2; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < np2; i += WPOL_BLOCK) {
+        const int l = i ^ j;
+        if (l <= i) continue;
+        const long long ti = kth[i], tl = kth[l];
+        const int ii = kiw[i], il = kiw[l];
+        const bool gt = ti > tl || (ti == tl && ii > il);     // element i after element l
+        if (((i & k) == 0) == gt) {                           // ascending blocks swap when i > l
+          kth[i] = tl; kth[l] = ti;
+          kiw[i] = il; kiw[l] = ii;
+        }
+      }
+      __syncthreads();
+    }
+  for (int m = threadIdx.x; m < n; m += WPOL_BLOCK) P.wrank[S.woff + kiw[m]] = m;
   double tot = block_sum(tsum, shsum);
   if (threadIdx.x == 0) {
     SysState &st = P.st[s];
@@ -3337,8 +3364,9 @@ __global__ void k_finish(DevPtrs P, int mode) {
       bool want = (is % cyc == 0) && (kind == 0 || is > 0);
       if (!want) continue;
       int c = st.hist_n[kind];
-      if (c < P.hist_cap) {
-        double *r = P.hist + (((size_t)kind * P.nsys + s) * P.hist_cap + c) * rec_len;
+      const HistRef hr = *P.hr;
+      if (c < hr.cap) {
+        double *r = hr.hist + (((size_t)kind * P.nsys + s) * hr.cap + c) * rec_len;
         for (int k = lane; k < rec_len; k += 32)
           r[k] = k == 0 ? (double)is
                  : k <= QB_NE ? P.E[s * QB_NE + k - 1]

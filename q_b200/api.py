@@ -159,13 +159,19 @@ class Batch:
     def natom_total(self) -> int:
         return sum(s.natom for s in self.systems)
 
-    def coords_all(self) -> np.ndarray:
-        out = np.zeros(3 * self.natom_total)
+    def coords_all(self, out: np.ndarray | None = None) -> np.ndarray:
+        """Every system's coordinates, x y z per atom; `out` may be a
+        page-locked buffer (copied into at full link speed)."""
+        if out is None:
+            out = np.zeros(3 * self.natom_total)
+        assert out.dtype == np.float64 and out.flags.c_contiguous and out.size == 3 * self.natom_total
         check(lib.qb_batch_get_coords_all(self._b, _dp(out)))
         return out
 
-    def velocities_all(self) -> np.ndarray:
-        out = np.zeros(3 * self.natom_total)
+    def velocities_all(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.zeros(3 * self.natom_total)
+        assert out.dtype == np.float64 and out.flags.c_contiguous and out.size == 3 * self.natom_total
         check(lib.qb_batch_get_velocities_all(self._b, _dp(out)))
         return out
 

@@ -93,6 +93,10 @@ struct Batch {
   struct McState { bool started = false; int irand = 0; long long tries = 0, accepted = 0; };
   std::vector<McState> mc;
   int ww_wpb = WW_WPB;          // waters per block of the water-water kernels
+  // the packed water-water kernel: 0 every pair from both sides, 1 once with
+  // FP32 shared accumulation of the second water's terms, 2 once with 32-bit
+  // fixed point (k_nb_ww_x2's HALF)
+  int ww_once = 0;
   bool any_lrf = false, any_q = false, any_shake = false, any_wpol = false, any_prestr = false, any_qq = false,
        any_qb = false, any_hlj = false;
   // run-time choices the autotuner sets (qb_tuning): LRF source tiles per
@@ -345,9 +349,16 @@ struct Batch {
       if (fast_ww && any_hlj) {
         launch("nb_ww", [&] { k_nb_ww<true, true><<<gw, WW_BLOCK, smem, stream>>>(p, wpb); });
       } else if (fast_ww) {
+        if (ww_once) smem += (size_t)p.ww_chunk * WWH_BYTES;
         launch("nb_ww_x2", [&] {
-          if (any_box) k_nb_ww_x2<true><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb);
-          else k_nb_ww_x2<false><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb);
+          switch (ww_once + 3 * any_box) {
+            case 0: k_nb_ww_x2<false, 0><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb); break;
+            case 1: k_nb_ww_x2<false, 1><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb); break;
+            case 2: k_nb_ww_x2<false, 2><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb); break;
+            case 3: k_nb_ww_x2<true, 0><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb); break;
+            case 4: k_nb_ww_x2<true, 1><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb); break;
+            default: k_nb_ww_x2<true, 2><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb);
+          }
         });
       } else if (any_hlj) {
         launch("nb_ww", [&] { k_nb_ww<false, true><<<gw, WW_BLOCK, smem, stream>>>(p, wpb); });
@@ -383,7 +394,7 @@ struct Batch {
     if (max_nsol > 0)
       launch("atom_terms", [&] { k_atom_terms<<<dim3(cdiv(max_nsol, 128), nsys), 128, 0, s1>>>(p); });
     if (any_wpol) {
-      launch("watpol_rank", [&] { k_watpol_rank<<<dim3(MAX_SHELLS, nsys), WPOL_BLOCK, watpol_smem, s2>>>(p); });
+      launch("watpol_rank", [&] { k_watpol_rank<<<dim3(MAX_SHELLS, nsys), WPOL_RANK_BLOCK, watpol_smem, s2>>>(p); });
       launch("watpol", [&] { k_watpol_force<<<dim3(cdiv(max_nwat, WPOL_BLOCK), nsys), WPOL_BLOCK, 0, s2>>>(p); });
     }
     join_streams();
@@ -700,6 +711,7 @@ struct Batch {
   }
   double4 *mc_x = nullptr;
   double *mc_lrf = nullptr;
+  double *xyz = nullptr;   // packed x, y, z of every atom (the batched host copies)
   int max_nmol = 0;
 
   // the box fields of system s's device state (edge lengths, inverses,
@@ -1372,6 +1384,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   P.ww_cap = ww_cap;
   P.ww = dev_alloc<uint16_t>((size_t)std::max(woff, 1) * ww_cap, o);
   P.ww_n = dev_alloc<int>(std::max(woff, 1), o);
+  P.ww_mid = dev_alloc<int>(std::max(woff, 1), o);
   P.ww_sp = dev_alloc<int>((size_t)std::max(woff, 1) * nch_alloc, o);
   // FP64 records on every step of the FP64 engine and on the mixed engine's
   // energy steps, whose FP64 water-water kernel stages the mixed chunk size
@@ -1383,8 +1396,12 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem64));
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem64));
-  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
-  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
   P.kin_nblk = std::max(1, (B.max_natom + KIN_BLOCK - 1) / KIN_BLOCK);
   P.kin = dev_alloc<double>((size_t)n * 4, o);
   P.E = dev_alloc<double>((size_t)n * QB_NE, o);
@@ -1397,12 +1414,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     P.hr = dev_alloc<HistRef>(1, o);
     CUDA_TRY(cudaMemcpy(P.hr, &none, sizeof none, cudaMemcpyHostToDevice));
   }
-  {
-    // member angles and indices, padded to a power of two for the sort
-    size_t np2 = 1;
-    while (np2 < (size_t)std::max(B.max_nwat, 1)) np2 <<= 1;
-    B.watpol_smem = np2 * (sizeof(double) + sizeof(int));
-  }
+  B.watpol_smem = (size_t)B.max_nwat * (sizeof(double) + sizeof(int));   // member angles and indices
   P.wtheta = dev_alloc<double>(std::max(woff, 1), o);
   P.wshell = dev_alloc<int8_t>(std::max(woff, 1), o);
   P.wrank = dev_alloc<int>(std::max(woff, 1), o);
@@ -1424,6 +1436,7 @@ void ensure_history(Batch &B, int nsteps) {
     need = std::max(need, std::max(a, b));
   }
   std::vector<SysState> st(B.nsys);
+  CUDA_TRY(cudaStreamSynchronize(B.stream));   // no step in flight reads the old buffer
   CUDA_TRY(cudaMemcpy(st.data(), B.P.st, sizeof(SysState) * B.nsys, cudaMemcpyDeviceToHost));
   int used = 0;
   for (auto &x : st) used = std::max(used, std::max(x.hist_n[0], x.hist_n[1]));
@@ -1610,10 +1623,17 @@ int qb_batch_run_timed(qb_batch *bb, int nsteps, double *device_ms, long long *k
 namespace qb {
 namespace {
 
+// the packed water-water kernel's records and j accumulator of one chunk
+// within its staging memory
+bool ww_once_fits(int chunk) {
+  return (size_t)chunk * (WatRec<true>::words * sizeof(float4) + WWH_BYTES) <= (size_t)WW_STAGE_BYTES;
+}
+
 void get_tuning(const Batch &B, qb_tuning *t) {
   t->lrf_tiles_per_block = B.P.lrf_tpb;
   t->ww_chunk = B.P.ww_chunk;
   t->side_streams = B.streams_on ? 1 : 0;
+  t->ww_pairs_once = B.ww_once;
   t->ww_chunk_min = B.ww_chunk_floor;
   t->ww_chunk_max = B.ww_chunk_max;
 }
@@ -1622,12 +1642,16 @@ void set_tuning(Batch &B, const qb_tuning &t) {
   if (t.lrf_tiles_per_block < 1 || t.lrf_tiles_per_block > 1024) fail(QB_ERR_ARG, "lrf_tiles_per_block out of range");
   if (t.ww_chunk % 32 || t.ww_chunk < B.ww_chunk_floor || t.ww_chunk > B.ww_chunk_max)
     fail(QB_ERR_ARG, "ww_chunk must be a multiple of 32 within the batch's range");
+  if (t.ww_pairs_once < 0 || t.ww_pairs_once > 2) fail(QB_ERR_ARG, "ww_pairs_once must be 0, 1 or 2");
+  if (t.ww_pairs_once && !ww_once_fits(t.ww_chunk))
+    fail(QB_ERR_ARG, "ww_pairs_once: the chunk's records and accumulator exceed the staging memory");
   CUDA_TRY(cudaStreamSynchronize(B.stream));
   B.drop_graphs();
   B.set_lrf_tpb(t.lrf_tiles_per_block);
   B.P.ww_chunk = t.ww_chunk;
   B.P.ww_nch = (std::max(B.max_nwat, 1) + t.ww_chunk - 1) / t.ww_chunk;
   B.streams_on = t.side_streams != 0;
+  B.ww_once = t.ww_pairs_once;
   B.lists_stale = true;   // the water-water split counts depend on the chunk
 }
 
@@ -1705,6 +1729,12 @@ int qb_batch_autotune(qb_batch *bb, int steps_per_trial, qb_tuning *out) {
       t.side_streams = !best.side_streams;
       consider(t);
     }
+    if (B.max_nwat > 0 && B.opt.precision == QB_MIXED && !B.any_hlj)
+      for (int once : {1, 2}) {
+        qb_tuning t = best;
+        t.ww_pairs_once = once;
+        if (once != best.ww_pairs_once && qb::ww_once_fits(t.ww_chunk)) consider(t);
+      }
     qb::set_tuning(B, best);
     best.trials = trials;
     best.ms_per_step = best_ms;
@@ -1824,15 +1854,38 @@ int qb_batch_set_coords(qb_batch *b, int sys, const double *x) {
 int qb_batch_get_velocities(qb_batch *b, int sys, double *v) { return get_vec(b, sys, b ? b->b.P.v : nullptr, v); }
 int qb_batch_set_velocities(qb_batch *b, int sys, const double *v) { return set_vec(b, sys, b ? b->b.P.v : nullptr, v); }
 
+// x, y, z of every atom between the engine's double4 arrays and a packed
+// device copy of the caller's layout: the host copies move the packed 24
+// bytes per atom (from the caller's buffer directly; page-locked buffers go
+// at full link speed) and the device does the repacking.
+__global__ void k_xyz_to_atoms(double4 *dst, const double *src, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = make_double4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0);
+}
+__global__ void k_atoms_to_xyz(double *dst, const double4 *src, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    const double4 a = src[i];
+    dst[3 * i] = a.x; dst[3 * i + 1] = a.y; dst[3 * i + 2] = a.z;
+  }
+}
+
+static double *xyz_scratch(Batch &B) {
+  if (!B.xyz) B.xyz = qb::dev_alloc<double>(3 * (size_t)std::max(B.P.natoms_tot, 1), B.owned);
+  return B.xyz;
+}
+
 static int get_all(qb_batch *bb, double4 *src, double *out) {
   if (!bb || !out) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
   return guarded_batch([&] {
     Batch &B = bb->b;
-    const size_t n = (size_t)B.P.natoms_tot;
-    double4 *h = static_cast<double4 *>(B.staging(n * sizeof(double4)));
-    CUDA_TRY(cudaMemcpyAsync(h, src, n * sizeof(double4), cudaMemcpyDeviceToHost, B.stream));
+    const int n = B.P.natoms_tot;
+    double *d = xyz_scratch(B);
+    B.launches++;
+    k_atoms_to_xyz<<<Batch::cdiv(n, 256), 256, 0, B.stream>>>(d, src, n);
+    B.check_launch("atoms_to_xyz");
+    CUDA_TRY(cudaMemcpyAsync(out, d, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, B.stream));
     CUDA_TRY(cudaStreamSynchronize(B.stream));
-    for (size_t i = 0; i < n; i++) { out[3 * i] = h[i].x; out[3 * i + 1] = h[i].y; out[3 * i + 2] = h[i].z; }
   });
 }
 
@@ -1840,11 +1893,12 @@ static int set_all(qb_batch *bb, double4 *dst, const double *in) {
   if (!bb || !in) { qb::set_error("invalid argument"); return QB_ERR_ARG; }
   return guarded_batch([&] {
     Batch &B = bb->b;
-    const size_t n = (size_t)B.P.natoms_tot;
-    CUDA_TRY(cudaStreamSynchronize(B.stream));   // the staging may still feed an earlier copy
-    double4 *h = static_cast<double4 *>(B.staging(n * sizeof(double4)));
-    for (size_t i = 0; i < n; i++) h[i] = make_double4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0.0);
-    CUDA_TRY(cudaMemcpyAsync(dst, h, n * sizeof(double4), cudaMemcpyHostToDevice, B.stream));
+    const int n = B.P.natoms_tot;
+    double *d = xyz_scratch(B);
+    CUDA_TRY(cudaMemcpyAsync(d, in, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, B.stream));
+    B.launches++;
+    k_xyz_to_atoms<<<Batch::cdiv(n, 256), 256, 0, B.stream>>>(dst, d, n);
+    B.check_launch("xyz_to_atoms");
     CUDA_TRY(cudaStreamSynchronize(B.stream));
   });
 }

@@ -521,7 +521,6 @@ __device__ __forceinline__ void lrf_finish_x2(const float2 *m, const float2 *t, 
 // the group-pair window test is FP64.  Each block sums its tiles in FP32 and
 // adds the totals to the FP64 record with one atomic per component.
 constexpr int LRFX_BLOCK = 128, LRFX_TARGETS = 2 * LRFX_BLOCK;
-constexpr float LRFX_EPS2 = 4e-3f;
 
 template <bool BOX>
 __global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int force) {
@@ -535,21 +534,13 @@ __global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int 
   if (hsplit == 0 || gchunk * LRFX_TARGETS >= S.ncgp) return;
   const int t0 = hpart * tpb, t1 = min(t0 + tpb, S.nlrft);
   __shared__ double4 hsw[LRF_TILE_G];
-  __shared__ float4 hswf[LRF_TILE_G];                  // switching atoms relative to the origin, FP32
   __shared__ int2 hrange[LRF_TILE_G];
   __shared__ float4 hxy[LRF_TILE_A], hzq[LRF_TILE_A];   // {x, x, y, y}, {z, z, q, q}
   const double ox = S.origin[0], oy = S.origin[1], oz = S.origin[2];
   int gl[2];
   bool act[2], gsol[2];
   double3 xs[2], cen[2];
-  float3 xsf[2];
   float cc[2][3];
-  // the window test in FP32, the pairs within LRFX_EPS2 of either bound in
-  // FP64 (as the reference computes it): for positions within R of the
-  // origin the FP32 squared distance is within ~8.3e-7 R^2 A^2 of the FP64
-  // one, under the margin for R up to ~70 A (a sphere's atoms lie within its
-  // radius of the solute centre)
-  const float rlf = (float)S.RcLRF2;
 #pragma unroll
   for (int h = 0; h < 2; h++) {
     gl[h] = gchunk * LRFX_TARGETS + h * LRFX_BLOCK + threadIdx.x;
@@ -566,7 +557,6 @@ __global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int 
       cc[h][0] = (float)(L[0] - ox); cc[h][1] = (float)(L[1] - oy); cc[h][2] = (float)(L[2] - oz);
       xs[h] = ld3(P.x, swg);
     }
-    xsf[h] = make_float3((float)(xs[h].x - ox), (float)(xs[h].y - oy), (float)(xs[h].z - oz));
   }
   // minus the two target centres (positions relative to the origin); in a
   // periodic box each source group shifts them by its image (nbpplist_box_lrf
@@ -591,7 +581,6 @@ __global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int 
       const double3 p = ld3(P.x, sw);
       const double w = (P.flags[sw] & F_EXCL) ? -1.0 : (tile.x + i < S.ncgp_sol ? 1.0 : 0.0);
       hsw[i] = make_double4(p.x, p.y, p.z, w);
-      hswf[i] = make_float4((float)(p.x - ox), (float)(p.y - oy), (float)(p.z - oz), (float)w);
       hrange[i] = make_int2(P.cg_first[h] - a0, P.cg_last[h] - P.cg_first[h] + 1);
     }
     for (int i = threadIdx.x; i < na; i += LRFX_BLOCK) {
@@ -617,21 +606,9 @@ __global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int 
         if (!S.switch_atoms && (gsol[h] || hs.w > 0.0)) {
           in = act[h] && tile.x + i != gl[h] &&
                lrf_window_any(P, S, S.coff + gl[h], gsol[h], S.coff + tile.x + i, hs.w > 0.0, rc2);
-        } else if (!BOX) {
-          const float4 hf = hswf[i];
-          const float fx = xsf[h].x - hf.x, fy = xsf[h].y - hf.y, fz = xsf[h].z - hf.z;
-          const float r2f = fmaf(fx, fx, fmaf(fy, fy, fz * fz));
-          const float rcf = (float)rc2;
-          if (fabsf(r2f - rcf) > LRFX_EPS2 && fabsf(r2f - rlf) > LRFX_EPS2) {
-            in = act[h] && tile.x + i != gl[h] && r2f > rcf && r2f <= rlf;
-          } else {
-            const double dx = xs[h].x - hs.x, dy = xs[h].y - hs.y, dz = xs[h].z - hs.z;
-            const double r2 = dx * dx + dy * dy + dz * dz;
-            in = act[h] && tile.x + i != gl[h] && r2 > rc2 && r2 <= S.RcLRF2;
-          }
         } else {
           double dx = xs[h].x - hs.x, dy = xs[h].y - hs.y, dz = xs[h].z - hs.z;
-          min_image(bx, dx, dy, dz);
+          if (BOX) min_image(bx, dx, dy, dz);
           const double r2 = dx * dx + dy * dy + dz * dz;
           in = act[h] && tile.x + i != gl[h] && r2 > rc2 && r2 <= S.RcLRF2;
         }
@@ -684,7 +661,8 @@ __global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int 
 // sphere whose O lies within Rcww of i's O, as local water indices in
 // ascending order.  ww_sp[gw*ww_nch + c] counts the entries below the end of
 // force-kernel chunk c (chunks of ww_chunk waters, a multiple of 32), so the
-// force kernel finds each chunk's slice of the list directly.
+// force kernel finds each chunk's slice of the list directly; ww_mid[gw]
+// counts the entries below i itself (where the half with j > i starts).
 // Block = WL_WPB waters of one system, one warp per water at a time; the
 // system's O positions are staged in shared memory WL_STAGE waters at a time
 // in FP32, relative to the solvent centre (w = -1 for excluded waters), and
@@ -782,6 +760,10 @@ __global__ void __launch_bounds__(WL_BLOCK) k_list_ww(DevPtrs P, int force) {
             const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
             if (pos < P.ww_cap) out[pos] = (uint16_t)(base + lane);
           }
+          // the entries below water i itself: its list's half with j > i
+          // starts there
+          if (lane == 0 && iw >= base && iw < base + 32)
+            P.ww_mid[gw] = min(cnt + __popc(bal & ((1u << (iw - base)) - 1u)), P.ww_cap);
           cnt += __popc(bal);
         }
       }
@@ -797,8 +779,10 @@ __global__ void __launch_bounds__(WL_BLOCK) k_list_ww(DevPtrs P, int force) {
     int *sp = P.ww_sp + (size_t)gw * P.ww_nch;
     if (cnt > P.ww_cap) { set_status(&P.st[s], QB_ERR_LIST_OVERFLOW); cnt = P.ww_cap; }
     P.ww_n[gw] = cnt;
-    if (cnt == 0)
+    if (cnt == 0) {
       for (int c = 0; c < P.ww_nch; c++) sp[c] = 0;
+      P.ww_mid[gw] = 0;
+    }
     for (int c = (S.nwat - 1) / P.ww_chunk; c < P.ww_nch; c++) sp[c] = cnt;
   }
 }
@@ -1403,11 +1387,14 @@ struct WwI2 {
 // inverses iL: the O-O vector moves to its nearest image (nonbond_ww_spc_box,
 // md.f90:12078-12100; the FP32 nint agrees with the FP64 one away from half an
 // edge, far beyond the cut-off).
-template <bool BOX>
+// JG: also the pair's terms on water j, into gj (O x y z, H1 x y z, H2 x y z)
+// as the sums of w * (x_j - x_i): j's gradient is their negative.
+template <bool BOX, bool JG = false>
 __device__ __forceinline__ void ww_force_x2(const WwI2 &I, const float4 j0, const float4 j1, const float4 j2,
                                             float2 qoh2, float2 qhh2, float qoo, float A, float B, float2 *gO,
                                             float2 *gH, float2 *gHs, const float *Lh = nullptr,
-                                            const float *Ll = nullptr, const float *iL = nullptr) {
+                                            const float *Ll = nullptr, const float *iL = nullptr,
+                                            float *gj = nullptr) {
   float d[3] = {(j0.x - I.hO[0]) + (j0.w - I.lO[0]), (j0.y - I.hO[1]) + (j1.x - I.lO[1]),
                 (j0.z - I.hO[2]) + (j1.y - I.lO[2])};
   if (BOX) {
@@ -1446,6 +1433,18 @@ __device__ __forceinline__ void ww_force_x2(const WwI2 &I, const float4 j0, cons
   const float w = r2i * fmaf(-6.f, Vb, fmaf(12.f, Va, qoo * ri));
 #pragma unroll
   for (int c = 0; c < 3; c++) gO[c].x = fmaf(w, d[c], gO[c].x);
+  if (JG) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      // H1_j, H2_j: from O_i (t), from {H1_i, H2_i} (hd) and {H2_i, H1_i} (hx);
+      // O_j: from H1_i and H2_i (s) and from O_i
+      const float2 h = __ffma2_rn(wx, hx[c], __ffma2_rn(wd, hd[c], __fmul2_rn(wt, t[c])));
+      const float2 o = __fmul2_rn(ws, sv[c]);
+      gj[c] = fmaf(w, d[c], o.x + o.y);
+      gj[3 + c] = h.x;
+      gj[6 + c] = h.y;
+    }
+  }
 }
 
 // nonbond_ww_spc (md.f90:11823) forces of the mixed-precision engine on steps
@@ -1458,8 +1457,20 @@ __device__ __forceinline__ void ww_force_x2(const WwI2 &I, const float4 j0, cons
 // the other's pair work (the registers of the packed path allow 16 warps per
 // SM).  A three-block form (80 registers, staging chunks of up to 74 KB) ran
 // the kernel 13% slower alone, and the step no faster.
+// HALF 0: every pair from both sides (the lists hold both directions).
+// HALF 1, 2: every pair once, from the water with the lower index (its list
+// entries from ww_mid on); water j's terms go into an accumulator of nine
+// words per staged water in shared memory, added to the gradient at the end
+// of each chunk: FP32 atomics (HALF 1) or 32-bit fixed point in units of
+// 2^-17 kcal/mol/A (HALF 2).  In fixed point a pair whose term on j reaches
+// 128 kcal/mol/A (2^24 units) adds it to the FP64 gradient directly, so the
+// at most WW_WPB terms one block adds to a word stay below 2^31.
 constexpr int WWX_BLOCK = 256;
-template <bool BOX>
+constexpr float WWH_SCALE = 131072.f, WWH_LIMIT = 16777216.f;
+constexpr int WWH_BYTES = 9 * 4;   // the accumulator's bytes per staged water
+// a term below 2^24 in magnitude rounds to at most 2^24 - 1 (floats there are whole numbers)
+static_assert(WW_WPB * (16777216.0 - 1.0) <= 2147483647.0, "fixed-point accumulator range");
+template <bool BOX, int HALF>
 __global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P, int wpb) {
   extern __shared__ float4 wsm[];
   __shared__ int2 srange[WW_WPB];
@@ -1473,6 +1484,9 @@ __global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P, int wpb) {
   const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
   const float4 *rec = P.wrec + (size_t)S.woff * W;
   const int CW = P.ww_chunk;
+  float *accf = reinterpret_cast<float *>(wsm + (size_t)CW * W);   // HALF: j's terms
+  int *acci = reinterpret_cast<int *>(accf);
+  const int obase = S.aoff + S.nsol;
   const int nch = (S.nwat + CW - 1) / CW;
   const float qo = S.crg_ow, qh = S.crg_hw;
   const float qoo = qo * qo;
@@ -1492,9 +1506,13 @@ __global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P, int wpb) {
     const int c0 = c * CW, cn = min(CW, S.nwat - c0);
     __syncthreads();
     for (int t = threadIdx.x; t < cn * W; t += WWX_BLOCK) wsm[t] = rec[(size_t)c0 * W + t];
+    if (HALF)
+      for (int t = threadIdx.x; t < cn * 9; t += WWX_BLOCK) acci[t] = 0;
     for (int t = threadIdx.x; t < i1 - i0; t += WWX_BLOCK) {
       const int *sp = P.ww_sp + (size_t)(S.woff + i0 + t) * P.ww_nch;
-      srange[t] = make_int2(c == 0 ? 0 : sp[c - 1], sp[c]);
+      int lo = c == 0 ? 0 : sp[c - 1];
+      if (HALF) lo = max(lo, P.ww_mid[S.woff + i0 + t]);
+      srange[t] = make_int2(lo, sp[c]);
     }
     __syncthreads();
     // the first group of list entries of the half-warp's next water, loaded
@@ -1543,8 +1561,31 @@ __global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P, int wpb) {
 #pragma unroll
         for (int u = 0; u < 4; u++) {
           if (jg[u] < 0) break;
-          const float4 *rj = wsm + (jg[u] - c0) * W;
-          ww_force_x2<BOX>(I, rj[0], rj[1], rj[2], qoh2, qhh2, qoo, A, B, gO, gH, gHs, Lh, Ll, iL);
+          const int jl = jg[u] - c0;
+          const float4 *rj = wsm + jl * W;
+          if (HALF) {
+            float gj[9];
+            ww_force_x2<BOX, true>(I, rj[0], rj[1], rj[2], qoh2, qhh2, qoo, A, B, gO, gH, gHs, Lh, Ll, iL, gj);
+            if (HALF == 1) {
+#pragma unroll
+              for (int q = 0; q < 9; q++) atomicAdd(accf + jl * 9 + q, gj[q]);
+            } else {
+              float m = 0.f;
+#pragma unroll
+              for (int q = 0; q < 9; q++) m = fmaxf(m, fabsf(gj[q]));
+              if (m * WWH_SCALE < WWH_LIMIT) {
+#pragma unroll
+                for (int q = 0; q < 9; q++) atomicAdd(acci + jl * 9 + q, __float2int_rn(gj[q] * WWH_SCALE));
+              } else {
+                const int oj = obase + 3 * jg[u];
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+                  atomic_add3(P.d, oj + a, -(double)gj[3 * a], -(double)gj[3 * a + 1], -(double)gj[3 * a + 2]);
+              }
+            }
+          } else {
+            ww_force_x2<BOX>(I, rj[0], rj[1], rj[2], qoh2, qhh2, qoo, A, B, gO, gH, gHs, Lh, Ll, iL);
+          }
         }
 #pragma unroll
         for (int u = 0; u < 4; u++) jg[u] = jn[u];
@@ -1563,10 +1604,28 @@ __global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P, int wpb) {
         for (int o = 8; o > 0; o >>= 1) g[q] += __shfl_xor_sync(hmask, g[q], o);
       }
       if (hl == 0) {
-        const int oi = S.aoff + S.nsol + 3 * iw;
+        const int oi = obase + 3 * iw;
 #pragma unroll
         for (int a = 0; a < 3; a++)
           atomic_add3(P.d, oi + a, (double)g[3 * a], (double)g[3 * a + 1], (double)g[3 * a + 2]);
+      }
+    }
+    if (HALF) {
+      // the chunk's waters' accumulated terms into the gradient
+      __syncthreads();
+      for (int t = threadIdx.x; t < cn; t += WWX_BLOCK) {
+        double v[9];
+        bool any = false;
+#pragma unroll
+        for (int q = 0; q < 9; q++) {
+          v[q] = HALF == 1 ? (double)accf[t * 9 + q] : (double)acci[t * 9 + q] * (1.0 / WWH_SCALE);
+          any |= v[q] != 0.0;
+        }
+        if (any) {
+          const int oj = obase + 3 * (c0 + t);
+#pragma unroll
+          for (int a = 0; a < 3; a++) atomic_add3(P.d, oj + a, -v[3 * a], -v[3 * a + 1], -v[3 * a + 2]);
+        }
       }
     }
   }
@@ -2806,14 +2865,15 @@ __global__ void __launch_bounds__(256) k_solute_terms(DevPtrs P, SoluteGrid G) {
 // k_watpol_rank, one block per (shell, system): each member of the shell
 // (angles and shells from k_pack_waters) is ranked by counting the members
 // before it in (angle, water index) order, the reference's selection order
-// with ties by water index.  The block also keeps
+// with ties by water index: one warp per member, its lanes splitting the
+// other members and summing their counts.  The block also keeps
 // the shell's running averages and updates theta_corr every 100 steps, in
 // the reference's order (update first, then this step's average).
 // k_watpol_force, one thread per water: target angle from the rank, restraint
 // energy and the force on the water dipole.
-constexpr int WPOL_BLOCK = 256;
+constexpr int WPOL_BLOCK = 256, WPOL_RANK_BLOCK = 512;
 
-__global__ void __launch_bounds__(WPOL_BLOCK) k_watpol_rank(DevPtrs P) {
+__global__ void __launch_bounds__(WPOL_RANK_BLOCK) k_watpol_rank(DevPtrs P) {
   extern __shared__ unsigned char smem[];
   const int is = blockIdx.x, s = blockIdx.y;
   const SysDev &S = P.sys[s];
@@ -2829,7 +2889,7 @@ __global__ void __launch_bounds__(WPOL_BLOCK) k_watpol_rank(DevPtrs P) {
   // member angles as bit patterns (non-negative doubles order like their bits)
   long long *kth = (long long *)smem;
   int *kiw = (int *)(kth + nw);                 // member water indices
-  for (int w0 = 0; w0 < nw; w0 += WPOL_BLOCK) {
+  for (int w0 = 0; w0 < nw; w0 += WPOL_RANK_BLOCK) {
     const int iw = w0 + threadIdx.x;
     const bool mine = iw < nw && wsh[iw] == is;
     const unsigned bal = __ballot_sync(FULL, mine);
@@ -2844,35 +2904,21 @@ __global__ void __launch_bounds__(WPOL_BLOCK) k_watpol_rank(DevPtrs P) {
   }
   __syncthreads();
   const int n = cnt;
-  // rank = position in (angle, water index) order: a bitonic sort of the
-  // members in shared memory, padded to a power of two with keys above every
-  // angle (the angles are non-negative doubles: their bit patterns order
-  // like them)
-  int np2 = 1;
-  while (np2 < n) np2 <<= 1;
-  for (int m = n + threadIdx.x; m < np2; m += WPOL_BLOCK) {
-    kth[m] = 0x7fffffffffffffffLL;
-    kiw[m] = 0x7fffffff;
-  }
   double tsum = 0;
-  for (int m = threadIdx.x; m < n; m += WPOL_BLOCK) tsum += __longlong_as_double(kth[m]);
-  __syncthreads();
-  for (int k = 2; k <= np2; k <<= 1)
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int i = threadIdx.x; i < np2; i += WPOL_BLOCK) {
-        const int l = i ^ j;
-        if (l <= i) continue;
-        const long long ti = kth[i], tl = kth[l];
-        const int ii = kiw[i], il = kiw[l];
-        const bool gt = ti > tl || (ti == tl && ii > il);     // element i after element l
-        if (((i & k) == 0) == gt) {                           // ascending blocks swap when i > l
-          kth[i] = tl; kth[l] = ti;
-          kiw[i] = il; kiw[l] = ii;
-        }
-      }
-      __syncthreads();
+  for (int m = threadIdx.x; m < n; m += WPOL_RANK_BLOCK) tsum += __longlong_as_double(kth[m]);
+  // rank = members before this one in (angle, water index) order
+  for (int m = threadIdx.x >> 5; m < n; m += WPOL_RANK_BLOCK / 32) {
+    const long long th = kth[m];
+    const int iw = kiw[m];
+    int r = 0;
+    for (int u = lane; u < n; u += 32) {
+      const long long tu = kth[u];
+      const int iu = kiw[u];
+      r += (int)(tu < th) + ((int)(tu == th) & (int)(iu < iw));
     }
-  for (int m = threadIdx.x; m < n; m += WPOL_BLOCK) P.wrank[S.woff + kiw[m]] = m;
+    r = __reduce_add_sync(FULL, r);
+    if (lane == 0) P.wrank[S.woff + iw] = r;
+  }
   double tot = block_sum(tsum, shsum);
   if (threadIdx.x == 0) {
     SysState &st = P.st[s];

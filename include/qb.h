@@ -206,10 +206,6 @@ typedef struct qb_tuning {
   int ww_chunk;               /* waters staged in shared memory per pass of the water-water kernel:
                                  a multiple of 32 between ww_chunk_min and ww_chunk_max */
   int side_streams;           /* 1: a step's force kernels fork over two side streams; 0: one stream */
-  int ww_pairs_once;          /* mixed precision, SPC water: the water-water forces of the steps that record
-                                 no energies evaluate each molecule pair 0: from both sides; 1: once, the second
-                                 water's terms summed in FP32 in shared memory; 2: once, summed in 32-bit fixed
-                                 point (2^-17 kcal/mol/A units) */
   int ww_chunk_min, ww_chunk_max;  /* the batch's allowed range (read only) */
   int trials;                 /* autotune: settings timed */
   double ms_per_step;         /* autotune: device ms per step of the chosen setting */
@@ -217,15 +213,13 @@ typedef struct qb_tuning {
 } qb_tuning;
 
 int qb_batch_get_tuning(qb_batch *b, qb_tuning *out);
-/* Applies lrf_tiles_per_block, ww_chunk, side_streams and ww_pairs_once (QB_ERR_ARG
- * when out of range, or when ww_pairs_once's accumulator does not fit beside the
- * chunk); the pair lists are rebuilt before the next step. */
+/* Applies lrf_tiles_per_block, ww_chunk and side_streams (QB_ERR_ARG when out of
+ * range); the pair lists are rebuilt before the next step. */
 int qb_batch_set_tuning(qb_batch *b, const qb_tuning *t);
 /* Times steps_per_trial MD steps (rounded up to whole pair-list cycles, each
  * after a cycle of warm-up) for candidate settings, one parameter at a time
  * (LRF tiles per block 1..16, the water chunk at its maximum, a half and a
- * quarter, side streams on/off, ww_pairs_once 0/1/2), keeps the fastest and
- * reports it.  The trial
+ * quarter, side streams on/off), keeps the fastest and reports it.  The trial
  * steps are real MD steps of every system (count them as equilibration); the
  * energy records they make are cleared. */
 int qb_batch_autotune(qb_batch *b, int steps_per_trial, qb_tuning *out);

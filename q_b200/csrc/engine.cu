@@ -93,10 +93,6 @@ struct Batch {
   struct McState { bool started = false; int irand = 0; long long tries = 0, accepted = 0; };
   std::vector<McState> mc;
   int ww_wpb = WW_WPB;          // waters per block of the water-water kernels
-  // the packed water-water kernel: 0 every pair from both sides, 1 once with
-  // FP32 shared accumulation of the second water's terms, 2 once with 32-bit
-  // fixed point (k_nb_ww_x2's HALF)
-  int ww_once = 0;
   bool any_lrf = false, any_q = false, any_shake = false, any_wpol = false, any_prestr = false, any_qq = false,
        any_qb = false, any_hlj = false;
   // run-time choices the autotuner sets (qb_tuning): LRF source tiles per
@@ -349,16 +345,9 @@ struct Batch {
       if (fast_ww && any_hlj) {
         launch("nb_ww", [&] { k_nb_ww<true, true><<<gw, WW_BLOCK, smem, stream>>>(p, wpb); });
       } else if (fast_ww) {
-        if (ww_once) smem += (size_t)p.ww_chunk * WWH_BYTES;
         launch("nb_ww_x2", [&] {
-          switch (ww_once + 3 * any_box) {
-            case 0: k_nb_ww_x2<false, 0><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb); break;
-            case 1: k_nb_ww_x2<false, 1><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb); break;
-            case 2: k_nb_ww_x2<false, 2><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb); break;
-            case 3: k_nb_ww_x2<true, 0><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb); break;
-            case 4: k_nb_ww_x2<true, 1><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb); break;
-            default: k_nb_ww_x2<true, 2><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb);
-          }
+          if (any_box) k_nb_ww_x2<true><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb);
+          else k_nb_ww_x2<false><<<gw, WWX_BLOCK, smem, stream>>>(p, wpb);
         });
       } else if (any_hlj) {
         launch("nb_ww", [&] { k_nb_ww<false, true><<<gw, WW_BLOCK, smem, stream>>>(p, wpb); });
@@ -1384,7 +1373,6 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   P.ww_cap = ww_cap;
   P.ww = dev_alloc<uint16_t>((size_t)std::max(woff, 1) * ww_cap, o);
   P.ww_n = dev_alloc<int>(std::max(woff, 1), o);
-  P.ww_mid = dev_alloc<int>(std::max(woff, 1), o);
   P.ww_sp = dev_alloc<int>((size_t)std::max(woff, 1) * nch_alloc, o);
   // FP64 records on every step of the FP64 engine and on the mixed engine's
   // energy steps, whose FP64 water-water kernel stages the mixed chunk size
@@ -1396,12 +1384,8 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem64));
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem64));
-  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
-  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
-  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
-  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
-  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
-  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
   P.kin_nblk = std::max(1, (B.max_natom + KIN_BLOCK - 1) / KIN_BLOCK);
   P.kin = dev_alloc<double>((size_t)n * 4, o);
   P.E = dev_alloc<double>((size_t)n * QB_NE, o);
@@ -1623,17 +1607,10 @@ int qb_batch_run_timed(qb_batch *bb, int nsteps, double *device_ms, long long *k
 namespace qb {
 namespace {
 
-// the packed water-water kernel's records and j accumulator of one chunk
-// within its staging memory
-bool ww_once_fits(int chunk) {
-  return (size_t)chunk * (WatRec<true>::words * sizeof(float4) + WWH_BYTES) <= (size_t)WW_STAGE_BYTES;
-}
-
 void get_tuning(const Batch &B, qb_tuning *t) {
   t->lrf_tiles_per_block = B.P.lrf_tpb;
   t->ww_chunk = B.P.ww_chunk;
   t->side_streams = B.streams_on ? 1 : 0;
-  t->ww_pairs_once = B.ww_once;
   t->ww_chunk_min = B.ww_chunk_floor;
   t->ww_chunk_max = B.ww_chunk_max;
 }
@@ -1642,16 +1619,12 @@ void set_tuning(Batch &B, const qb_tuning &t) {
   if (t.lrf_tiles_per_block < 1 || t.lrf_tiles_per_block > 1024) fail(QB_ERR_ARG, "lrf_tiles_per_block out of range");
   if (t.ww_chunk % 32 || t.ww_chunk < B.ww_chunk_floor || t.ww_chunk > B.ww_chunk_max)
     fail(QB_ERR_ARG, "ww_chunk must be a multiple of 32 within the batch's range");
-  if (t.ww_pairs_once < 0 || t.ww_pairs_once > 2) fail(QB_ERR_ARG, "ww_pairs_once must be 0, 1 or 2");
-  if (t.ww_pairs_once && !ww_once_fits(t.ww_chunk))
-    fail(QB_ERR_ARG, "ww_pairs_once: the chunk's records and accumulator exceed the staging memory");
   CUDA_TRY(cudaStreamSynchronize(B.stream));
   B.drop_graphs();
   B.set_lrf_tpb(t.lrf_tiles_per_block);
   B.P.ww_chunk = t.ww_chunk;
   B.P.ww_nch = (std::max(B.max_nwat, 1) + t.ww_chunk - 1) / t.ww_chunk;
   B.streams_on = t.side_streams != 0;
-  B.ww_once = t.ww_pairs_once;
   B.lists_stale = true;   // the water-water split counts depend on the chunk
 }
 
@@ -1729,12 +1702,6 @@ int qb_batch_autotune(qb_batch *bb, int steps_per_trial, qb_tuning *out) {
       t.side_streams = !best.side_streams;
       consider(t);
     }
-    if (B.max_nwat > 0 && B.opt.precision == QB_MIXED && !B.any_hlj)
-      for (int once : {1, 2}) {
-        qb_tuning t = best;
-        t.ww_pairs_once = once;
-        if (once != best.ww_pairs_once && qb::ww_once_fits(t.ww_chunk)) consider(t);
-      }
     qb::set_tuning(B, best);
     best.trials = trials;
     best.ms_per_step = best_ms;

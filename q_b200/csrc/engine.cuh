@@ -185,7 +185,6 @@ struct DevPtrs {
   int *qw;                                 // water O atoms
   uint16_t *ww;                            // [gw*ww_cap + k] local water index
   int *ww_n, *ww_sp;                       // count per water; [gw*ww_nch + c] count below chunk c's end
-  int *ww_mid;                             // per water: entries below its own index (the list is ascending)
   int ww_cap, ww_chunk, ww_nch;
   int2 *ww_tiles;                          // water-water force blocks: (system, first water)
   int n_ww_tiles;

@@ -661,8 +661,7 @@ __global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int 
 // sphere whose O lies within Rcww of i's O, as local water indices in
 // ascending order.  ww_sp[gw*ww_nch + c] counts the entries below the end of
 // force-kernel chunk c (chunks of ww_chunk waters, a multiple of 32), so the
-// force kernel finds each chunk's slice of the list directly; ww_mid[gw]
-// counts the entries below i itself (where the half with j > i starts).
+// force kernel finds each chunk's slice of the list directly.
 // Block = WL_WPB waters of one system, one warp per water at a time; the
 // system's O positions are staged in shared memory WL_STAGE waters at a time
 // in FP32, relative to the solvent centre (w = -1 for excluded waters), and
@@ -760,10 +759,6 @@ __global__ void __launch_bounds__(WL_BLOCK) k_list_ww(DevPtrs P, int force) {
             const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
             if (pos < P.ww_cap) out[pos] = (uint16_t)(base + lane);
           }
-          // the entries below water i itself: its list's half with j > i
-          // starts there
-          if (lane == 0 && iw >= base && iw < base + 32)
-            P.ww_mid[gw] = min(cnt + __popc(bal & ((1u << (iw - base)) - 1u)), P.ww_cap);
           cnt += __popc(bal);
         }
       }
@@ -779,10 +774,8 @@ __global__ void __launch_bounds__(WL_BLOCK) k_list_ww(DevPtrs P, int force) {
     int *sp = P.ww_sp + (size_t)gw * P.ww_nch;
     if (cnt > P.ww_cap) { set_status(&P.st[s], QB_ERR_LIST_OVERFLOW); cnt = P.ww_cap; }
     P.ww_n[gw] = cnt;
-    if (cnt == 0) {
+    if (cnt == 0)
       for (int c = 0; c < P.ww_nch; c++) sp[c] = 0;
-      P.ww_mid[gw] = 0;
-    }
     for (int c = (S.nwat - 1) / P.ww_chunk; c < P.ww_nch; c++) sp[c] = cnt;
   }
 }
@@ -1387,14 +1380,11 @@ struct WwI2 {
 // inverses iL: the O-O vector moves to its nearest image (nonbond_ww_spc_box,
 // md.f90:12078-12100; the FP32 nint agrees with the FP64 one away from half an
 // edge, far beyond the cut-off).
-// JG: also the pair's terms on water j, into gj (O x y z, H1 x y z, H2 x y z)
-// as the sums of w * (x_j - x_i): j's gradient is their negative.
-template <bool BOX, bool JG = false>
+template <bool BOX>
 __device__ __forceinline__ void ww_force_x2(const WwI2 &I, const float4 j0, const float4 j1, const float4 j2,
                                             float2 qoh2, float2 qhh2, float qoo, float A, float B, float2 *gO,
                                             float2 *gH, float2 *gHs, const float *Lh = nullptr,
-                                            const float *Ll = nullptr, const float *iL = nullptr,
-                                            float *gj = nullptr) {
+                                            const float *Ll = nullptr, const float *iL = nullptr) {
   float d[3] = {(j0.x - I.hO[0]) + (j0.w - I.lO[0]), (j0.y - I.hO[1]) + (j1.x - I.lO[1]),
                 (j0.z - I.hO[2]) + (j1.y - I.lO[2])};
   if (BOX) {
@@ -1433,18 +1423,6 @@ __device__ __forceinline__ void ww_force_x2(const WwI2 &I, const float4 j0, cons
   const float w = r2i * fmaf(-6.f, Vb, fmaf(12.f, Va, qoo * ri));
 #pragma unroll
   for (int c = 0; c < 3; c++) gO[c].x = fmaf(w, d[c], gO[c].x);
-  if (JG) {
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      // H1_j, H2_j: from O_i (t), from {H1_i, H2_i} (hd) and {H2_i, H1_i} (hx);
-      // O_j: from H1_i and H2_i (s) and from O_i
-      const float2 h = __ffma2_rn(wx, hx[c], __ffma2_rn(wd, hd[c], __fmul2_rn(wt, t[c])));
-      const float2 o = __fmul2_rn(ws, sv[c]);
-      gj[c] = fmaf(w, d[c], o.x + o.y);
-      gj[3 + c] = h.x;
-      gj[6 + c] = h.y;
-    }
-  }
 }
 
 // nonbond_ww_spc (md.f90:11823) forces of the mixed-precision engine on steps
@@ -1457,20 +1435,8 @@ __device__ __forceinline__ void ww_force_x2(const WwI2 &I, const float4 j0, cons
 // the other's pair work (the registers of the packed path allow 16 warps per
 // SM).  A three-block form (80 registers, staging chunks of up to 74 KB) ran
 // the kernel 13% slower alone, and the step no faster.
-// HALF 0: every pair from both sides (the lists hold both directions).
-// HALF 1, 2: every pair once, from the water with the lower index (its list
-// entries from ww_mid on); water j's terms go into an accumulator of nine
-// words per staged water in shared memory, added to the gradient at the end
-// of each chunk: FP32 atomics (HALF 1) or 32-bit fixed point in units of
-// 2^-17 kcal/mol/A (HALF 2).  In fixed point a pair whose term on j reaches
-// 128 kcal/mol/A (2^24 units) adds it to the FP64 gradient directly, so the
-// at most WW_WPB terms one block adds to a word stay below 2^31.
 constexpr int WWX_BLOCK = 256;
-constexpr float WWH_SCALE = 131072.f, WWH_LIMIT = 16777216.f;
-constexpr int WWH_BYTES = 9 * 4;   // the accumulator's bytes per staged water
-// a term below 2^24 in magnitude rounds to at most 2^24 - 1 (floats there are whole numbers)
-static_assert(WW_WPB * (16777216.0 - 1.0) <= 2147483647.0, "fixed-point accumulator range");
-template <bool BOX, int HALF>
+template <bool BOX>
 __global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P, int wpb) {
   extern __shared__ float4 wsm[];
   __shared__ int2 srange[WW_WPB];
@@ -1484,9 +1450,6 @@ __global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P, int wpb) {
   const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
   const float4 *rec = P.wrec + (size_t)S.woff * W;
   const int CW = P.ww_chunk;
-  float *accf = reinterpret_cast<float *>(wsm + (size_t)CW * W);   // HALF: j's terms
-  int *acci = reinterpret_cast<int *>(accf);
-  const int obase = S.aoff + S.nsol;
   const int nch = (S.nwat + CW - 1) / CW;
   const float qo = S.crg_ow, qh = S.crg_hw;
   const float qoo = qo * qo;
@@ -1506,13 +1469,9 @@ __global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P, int wpb) {
     const int c0 = c * CW, cn = min(CW, S.nwat - c0);
     __syncthreads();
     for (int t = threadIdx.x; t < cn * W; t += WWX_BLOCK) wsm[t] = rec[(size_t)c0 * W + t];
-    if (HALF)
-      for (int t = threadIdx.x; t < cn * 9; t += WWX_BLOCK) acci[t] = 0;
     for (int t = threadIdx.x; t < i1 - i0; t += WWX_BLOCK) {
       const int *sp = P.ww_sp + (size_t)(S.woff + i0 + t) * P.ww_nch;
-      int lo = c == 0 ? 0 : sp[c - 1];
-      if (HALF) lo = max(lo, P.ww_mid[S.woff + i0 + t]);
-      srange[t] = make_int2(lo, sp[c]);
+      srange[t] = make_int2(c == 0 ? 0 : sp[c - 1], sp[c]);
     }
     __syncthreads();
     // the first group of list entries of the half-warp's next water, loaded
@@ -1561,31 +1520,8 @@ __global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P, int wpb) {
 #pragma unroll
         for (int u = 0; u < 4; u++) {
           if (jg[u] < 0) break;
-          const int jl = jg[u] - c0;
-          const float4 *rj = wsm + jl * W;
-          if (HALF) {
-            float gj[9];
-            ww_force_x2<BOX, true>(I, rj[0], rj[1], rj[2], qoh2, qhh2, qoo, A, B, gO, gH, gHs, Lh, Ll, iL, gj);
-            if (HALF == 1) {
-#pragma unroll
-              for (int q = 0; q < 9; q++) atomicAdd(accf + jl * 9 + q, gj[q]);
-            } else {
-              float m = 0.f;
-#pragma unroll
-              for (int q = 0; q < 9; q++) m = fmaxf(m, fabsf(gj[q]));
-              if (m * WWH_SCALE < WWH_LIMIT) {
-#pragma unroll
-                for (int q = 0; q < 9; q++) atomicAdd(acci + jl * 9 + q, __float2int_rn(gj[q] * WWH_SCALE));
-              } else {
-                const int oj = obase + 3 * jg[u];
-#pragma unroll
-                for (int a = 0; a < 3; a++)
-                  atomic_add3(P.d, oj + a, -(double)gj[3 * a], -(double)gj[3 * a + 1], -(double)gj[3 * a + 2]);
-              }
-            }
-          } else {
-            ww_force_x2<BOX>(I, rj[0], rj[1], rj[2], qoh2, qhh2, qoo, A, B, gO, gH, gHs, Lh, Ll, iL);
-          }
+          const float4 *rj = wsm + (jg[u] - c0) * W;
+          ww_force_x2<BOX>(I, rj[0], rj[1], rj[2], qoh2, qhh2, qoo, A, B, gO, gH, gHs, Lh, Ll, iL);
         }
 #pragma unroll
         for (int u = 0; u < 4; u++) jg[u] = jn[u];
@@ -1604,28 +1540,10 @@ __global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P, int wpb) {
         for (int o = 8; o > 0; o >>= 1) g[q] += __shfl_xor_sync(hmask, g[q], o);
       }
       if (hl == 0) {
-        const int oi = obase + 3 * iw;
+        const int oi = S.aoff + S.nsol + 3 * iw;
 #pragma unroll
         for (int a = 0; a < 3; a++)
           atomic_add3(P.d, oi + a, (double)g[3 * a], (double)g[3 * a + 1], (double)g[3 * a + 2]);
-      }
-    }
-    if (HALF) {
-      // the chunk's waters' accumulated terms into the gradient
-      __syncthreads();
-      for (int t = threadIdx.x; t < cn; t += WWX_BLOCK) {
-        double v[9];
-        bool any = false;
-#pragma unroll
-        for (int q = 0; q < 9; q++) {
-          v[q] = HALF == 1 ? (double)accf[t * 9 + q] : (double)acci[t * 9 + q] * (1.0 / WWH_SCALE);
-          any |= v[q] != 0.0;
-        }
-        if (any) {
-          const int oj = obase + 3 * (c0 + t);
-#pragma unroll
-          for (int a = 0; a < 3; a++) atomic_add3(P.d, oj + a, -v[3 * a], -v[3 * a + 1], -v[3 * a + 2]);
-        }
       }
     }
   }

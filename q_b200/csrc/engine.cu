@@ -93,6 +93,7 @@ struct Batch {
   struct McState { bool started = false; int irand = 0; long long tries = 0, accepted = 0; };
   std::vector<McState> mc;
   int ww_wpb = WW_WPB;          // waters per block of the water-water kernels
+  long long ww_tiles_cap = 0;   // their tile buffer's entries (32 waters per block)
   bool any_lrf = false, any_q = false, any_shake = false, any_wpol = false, any_prestr = false, any_qq = false,
        any_qb = false, any_hlj = false;
   // run-time choices the autotuner sets (qb_tuning): LRF source tiles per
@@ -752,6 +753,20 @@ struct Batch {
 namespace {
 
 
+// The water-water force kernels' blocks: wpb consecutive waters of one
+// system each, system by system, into the tile buffer (sized at build for 32
+// waters per block).
+void set_ww_tiles(Batch &B, int wpb) {
+  std::vector<int2> tiles;
+  for (int s = 0; s < B.nsys; s++)
+    for (int i0 = 0; i0 < B.sysh[s].nwat; i0 += wpb) tiles.push_back(make_int2(s, i0));
+  if (tiles.empty()) tiles.push_back(make_int2(0, 0));
+  if ((long long)tiles.size() > B.ww_tiles_cap) fail(QB_ERR_ARG, "ww_waters_per_block below the tile buffer's size");
+  CUDA_TRY(cudaMemcpy(B.P.ww_tiles, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  B.P.n_ww_tiles = (int)tiles.size();
+  B.ww_wpb = wpb;
+}
+
 void build(Batch &B, qb_handle *const *hs, int n) {
   B.nsys = n;
   B.views.resize(n);
@@ -1363,12 +1378,11 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   }
   // water-water force blocks, system by system
   {
-    std::vector<int2> tiles;
-    for (int s = 0; s < n; s++)
-      for (int i0 = 0; i0 < B.sysh[s].nwat; i0 += B.ww_wpb) tiles.push_back(make_int2(s, i0));
-    if (tiles.empty()) tiles.push_back(make_int2(0, 0));
-    P.n_ww_tiles = (int)tiles.size();
-    P.ww_tiles = dev_upload(tiles, o);
+    long long cap = 1;
+    for (int s = 0; s < n; s++) cap += (B.sysh[s].nwat + 31) / 32;
+    B.ww_tiles_cap = cap;
+    P.ww_tiles = dev_alloc<int2>((size_t)cap, o);
+    set_ww_tiles(B, B.ww_wpb);
   }
   P.ww_cap = ww_cap;
   P.ww = dev_alloc<uint16_t>((size_t)std::max(woff, 1) * ww_cap, o);
@@ -1611,6 +1625,7 @@ void get_tuning(const Batch &B, qb_tuning *t) {
   t->lrf_tiles_per_block = B.P.lrf_tpb;
   t->ww_chunk = B.P.ww_chunk;
   t->side_streams = B.streams_on ? 1 : 0;
+  t->ww_waters_per_block = B.ww_wpb;
   t->ww_chunk_min = B.ww_chunk_floor;
   t->ww_chunk_max = B.ww_chunk_max;
 }
@@ -1619,12 +1634,15 @@ void set_tuning(Batch &B, const qb_tuning &t) {
   if (t.lrf_tiles_per_block < 1 || t.lrf_tiles_per_block > 1024) fail(QB_ERR_ARG, "lrf_tiles_per_block out of range");
   if (t.ww_chunk % 32 || t.ww_chunk < B.ww_chunk_floor || t.ww_chunk > B.ww_chunk_max)
     fail(QB_ERR_ARG, "ww_chunk must be a multiple of 32 within the batch's range");
+  if (t.ww_waters_per_block != 32 && t.ww_waters_per_block != 64 && t.ww_waters_per_block != WW_WPB)
+    fail(QB_ERR_ARG, "ww_waters_per_block must be 32, 64 or 128");
   CUDA_TRY(cudaStreamSynchronize(B.stream));
   B.drop_graphs();
   B.set_lrf_tpb(t.lrf_tiles_per_block);
   B.P.ww_chunk = t.ww_chunk;
   B.P.ww_nch = (std::max(B.max_nwat, 1) + t.ww_chunk - 1) / t.ww_chunk;
   B.streams_on = t.side_streams != 0;
+  if (t.ww_waters_per_block != B.ww_wpb) set_ww_tiles(B, t.ww_waters_per_block);
   B.lists_stale = true;   // the water-water split counts depend on the chunk
 }
 
@@ -1696,6 +1714,12 @@ int qb_batch_autotune(qb_batch *bb, int steps_per_trial, qb_tuning *out) {
         if (c < B.ww_chunk_floor || c == best.ww_chunk) continue;
         t.ww_chunk = c;
         consider(t);
+      }
+    if (B.max_nwat > 0)
+      for (int wpb : {64, 32, qb::WW_WPB}) {
+        qb_tuning t = best;
+        t.ww_waters_per_block = wpb;
+        if (wpb != best.ww_waters_per_block) consider(t);
       }
     if (B.side[0]) {
       qb_tuning t = best;

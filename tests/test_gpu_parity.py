@@ -314,14 +314,15 @@ def test_perturbations_with_different_q_atoms_in_one_batch(tmp_path, oracle):
 
 def test_tuning_changes_only_rounding(synthetic, oracle):
     """The run-time choices of the step kernels (LRF tiles per block, water
-    chunk, side streams) change only the order of atomic sums: two copies of
+    chunk, waters per water-water block, side streams) change only the order
+    of atomic sums: two copies of
     a batch, one with other settings, give the same records and coordinates
     to rounding; out-of-range settings are refused; after autotuning the
     batch still matches the oracle."""
     from q_b200 import QBError
     inp = synthetic["c1"].inp
     runs = []
-    for setting in (None, dict(lrf_tiles_per_block=1, ww_chunk=256, side_streams=0)):
+    for setting in (None, dict(lrf_tiles_per_block=1, ww_chunk=256, side_streams=0, ww_waters_per_block=32)):
         s = System.open(inp, lambdas=(0.4, 0.6), seed=5)
         b = Batch([s], precision=FP64)
         t = b.tuning()
@@ -329,7 +330,8 @@ def test_tuning_changes_only_rounding(synthetic, oracle):
         if setting:
             b.set_tuning(**setting)
             t = b.tuning()
-            assert (t["lrf_tiles_per_block"], t["ww_chunk"], t["side_streams"]) == (1, 256, 0)
+            assert (t["lrf_tiles_per_block"], t["ww_chunk"], t["side_streams"], t["ww_waters_per_block"]) == \
+                (1, 256, 0, 32)
         b.run(60)          # crosses two list rebuilds
         runs.append((b.history(0, 0), b.coords(0)))
     ((s0, E0, Q0), x0), ((s1, E1, Q1), x1) = runs
@@ -340,6 +342,8 @@ def test_tuning_changes_only_rounding(synthetic, oracle):
         b.set_tuning(ww_chunk=100)
     with pytest.raises(QBError):
         b.set_tuning(lrf_tiles_per_block=0)
+    with pytest.raises(QBError):
+        b.set_tuning(ww_waters_per_block=48)
     s = System.open(inp, lambdas=(0.4, 0.6), seed=5)
     b = Batch([s, s], precision=FP64)
     r = b.autotune(50)
@@ -347,7 +351,7 @@ def test_tuning_changes_only_rounding(synthetic, oracle):
     assert r["ww_chunk_min"] <= r["ww_chunk"] <= r["ww_chunk_max"] and r["lrf_tiles_per_block"] >= 1
     # the chosen setting, applied to a fresh batch, matches the oracle
     b = Batch([s], precision=FP64)
-    b.set_tuning(**{k: r[k] for k in ("lrf_tiles_per_block", "ww_chunk", "side_streams")})
+    b.set_tuning(**{k: r[k] for k in ("lrf_tiles_per_block", "ww_chunk", "side_streams", "ww_waters_per_block")})
     b.final_energy()
     o = oracle.create(s)
     o.final_energy()

@@ -384,7 +384,7 @@ struct Batch {
     if (max_nsol > 0)
       launch("atom_terms", [&] { k_atom_terms<<<dim3(cdiv(max_nsol, 128), nsys), 128, 0, s1>>>(p); });
     if (any_wpol) {
-      launch("watpol_rank", [&] { k_watpol_rank<<<dim3(MAX_SHELLS, nsys), WPOL_RANK_BLOCK, watpol_smem, s2>>>(p); });
+      launch("watpol_rank", [&] { k_watpol_rank<<<dim3(MAX_SHELLS, nsys), WPOL_BLOCK, watpol_smem, s2>>>(p); });
       launch("watpol", [&] { k_watpol_force<<<dim3(cdiv(max_nwat, WPOL_BLOCK), nsys), WPOL_BLOCK, 0, s2>>>(p); });
     }
     join_streams();

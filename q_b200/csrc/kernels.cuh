@@ -2783,15 +2783,14 @@ __global__ void __launch_bounds__(256) k_solute_terms(DevPtrs P, SoluteGrid G) {
 // k_watpol_rank, one block per (shell, system): each member of the shell
 // (angles and shells from k_pack_waters) is ranked by counting the members
 // before it in (angle, water index) order, the reference's selection order
-// with ties by water index: one warp per member, its lanes splitting the
-// other members and summing their counts.  The block also keeps
+// with ties by water index.  The block also keeps
 // the shell's running averages and updates theta_corr every 100 steps, in
 // the reference's order (update first, then this step's average).
 // k_watpol_force, one thread per water: target angle from the rank, restraint
 // energy and the force on the water dipole.
-constexpr int WPOL_BLOCK = 256, WPOL_RANK_BLOCK = 512;
+constexpr int WPOL_BLOCK = 256;
 
-__global__ void __launch_bounds__(WPOL_RANK_BLOCK) k_watpol_rank(DevPtrs P) {
+__global__ void __launch_bounds__(WPOL_BLOCK) k_watpol_rank(DevPtrs P) {
   extern __shared__ unsigned char smem[];
   const int is = blockIdx.x, s = blockIdx.y;
   const SysDev &S = P.sys[s];
@@ -2807,7 +2806,7 @@ __global__ void __launch_bounds__(WPOL_RANK_BLOCK) k_watpol_rank(DevPtrs P) {
   // member angles as bit patterns (non-negative doubles order like their bits)
   long long *kth = (long long *)smem;
   int *kiw = (int *)(kth + nw);                 // member water indices
-  for (int w0 = 0; w0 < nw; w0 += WPOL_RANK_BLOCK) {
+  for (int w0 = 0; w0 < nw; w0 += WPOL_BLOCK) {
     const int iw = w0 + threadIdx.x;
     const bool mine = iw < nw && wsh[iw] == is;
     const unsigned bal = __ballot_sync(FULL, mine);
@@ -2822,20 +2821,30 @@ __global__ void __launch_bounds__(WPOL_RANK_BLOCK) k_watpol_rank(DevPtrs P) {
   }
   __syncthreads();
   const int n = cnt;
+  // rank = members before this one in (angle, water index) order; the
+  // shared-memory reads are broadcasts
   double tsum = 0;
-  for (int m = threadIdx.x; m < n; m += WPOL_RANK_BLOCK) tsum += __longlong_as_double(kth[m]);
-  // rank = members before this one in (angle, water index) order
-  for (int m = threadIdx.x >> 5; m < n; m += WPOL_RANK_BLOCK / 32) {
+  for (int m = threadIdx.x; m < n; m += WPOL_BLOCK) {
     const long long th = kth[m];
     const int iw = kiw[m];
-    int r = 0;
-    for (int u = lane; u < n; u += 32) {
+    // branch-free: both words of every key are read, no short-circuit
+    int r[4] = {0, 0, 0, 0};
+    int u = 0;
+    for (; u + 4 <= n; u += 4) {
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const long long tu = kth[u + q];
+        const int iu = kiw[u + q];
+        r[q] += (int)(tu < th) + ((int)(tu == th) & (int)(iu < iw));
+      }
+    }
+    for (; u < n; u++) {
       const long long tu = kth[u];
       const int iu = kiw[u];
-      r += (int)(tu < th) + ((int)(tu == th) & (int)(iu < iw));
+      r[0] += (int)(tu < th) + ((int)(tu == th) & (int)(iu < iw));
     }
-    r = __reduce_add_sync(FULL, r);
-    if (lane == 0) P.wrank[S.woff + iw] = r;
+    P.wrank[S.woff + iw] = r[0] + r[1] + r[2] + r[3];
+    tsum += __longlong_as_double(th);
   }
   double tot = block_sum(tsum, shsum);
   if (threadIdx.x == 0) {

@@ -1093,7 +1093,7 @@ template <bool MIXED> struct WatRec { static constexpr int words = MIXED ? 3 : 5
 constexpr int WREC_MAX = 5;
 // threads, most waters per block (a batch of few systems takes fewer per
 // block, so that its blocks still fill the SMs)
-constexpr int WW_BLOCK = 512, WW_WPB = 128;
+constexpr int WW_BLOCK = 512, WW_WPB = 256;   // threads, most waters per block
 constexpr int WW_STAGE_BYTES = 112 * 1024;    // staged records per block: two blocks per SM
 
 // watpol (md.f90:15122), per water: the angle between the water dipole and

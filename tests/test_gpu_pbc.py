@@ -30,10 +30,14 @@ def boxes(tmp_path_factory):
                              max_volume_displ=400.0),
         "rst": synth.fep_box(str(root / "rst"), edge=EDGE, seed=1234,
                              distance_restraints=["1 20 2.0 4.0 5.0 0", "3 40 1.0 2.0 5.0 0"]),
+        # restraints reaching water atoms (atoms 100 and 301: waters after the
+        # 56 solute atoms): the solute terms then run after the water pass
+        "rst_water": synth.fep_box(str(root / "rst_water"), edge=EDGE, seed=1234,
+                                   distance_restraints=["1 100 2.0 4.0 5.0 0", "5 301 1.0 2.0 5.0 0"]),
     }
 
 
-@pytest.mark.parametrize("case", ["nvt", "nolrf", "rst"])
+@pytest.mark.parametrize("case", ["nvt", "nolrf", "rst", "rst_water"])
 def test_box_single_point(boxes, oracle, case):
     """Lists and potential at the starting coordinates: energies and gradient."""
     s = System.open(boxes[case].inp)
@@ -45,6 +49,11 @@ def test_box_single_point(boxes, oracle, case):
     Eo, EQo = o.energy_vectors()
     assert_energies(Eg, EQg, Eo, EQo)
     assert grad_err(b.gradient(0), o.gradient()) < G_TOL
+    if case.startswith("rst"):
+        # the same coordinates through the mixed engine's force path
+        m = Batch([s], precision=MIXED)
+        m.evaluate(energies=False)
+        assert grad_err(m.gradient(0), o.gradient()) < G_TOL
 
 
 def test_box_single_point_after_lattice_shifts(boxes, oracle):

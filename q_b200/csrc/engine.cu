@@ -136,7 +136,6 @@ struct Batch {
       if (ev_join[k]) cudaEventDestroy(ev_join[k]);
     }
     if (ev_fork) cudaEventDestroy(ev_fork);
-    if (ev_water) cudaEventDestroy(ev_water);
     for (auto &e : event_pool) cudaEventDestroy(e);
     for (auto &pe : pending) { cudaEventDestroy(pe.second.first); cudaEventDestroy(pe.second.second); }
     for (void *p : owned) cudaFree(p);
@@ -240,11 +239,7 @@ struct Batch {
   // a step (all adding with atomics) run on three streams and join before the
   // leap-frog.  Profiling keeps them on the main stream, one at a time.
   cudaStream_t side[2] = {nullptr, nullptr};
-  cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr}, ev_water = nullptr;
-  // some system's bonded terms (solvent bonds and angles without SHAKE) or
-  // sequence, position, distance, angle or wall restraints reach a solvent
-  // atom: the solute terms then wait for the water pass
-  bool terms_on_water = false;
+  cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
 
   void make_side_streams() {
     for (int k = 0; k < 2; k++) {
@@ -252,7 +247,6 @@ struct Batch {
       CUDA_TRY(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
     }
     CUDA_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
-    CUDA_TRY(cudaEventCreateWithFlags(&ev_water, cudaEventDisableTiming));
   }
 
   // Fork the side streams off the main stream / join them back (no-ops when
@@ -303,14 +297,18 @@ struct Batch {
     CUDA_TRY(cudaMemsetAsync(p.d, 0, sizeof(double4) * (size_t)p.natoms_tot, stream));
     CUDA_TRY(cudaMemsetAsync(p.E, 0, sizeof(double) * QB_NE * (size_t)nsys, stream));
     CUDA_TRY(cudaMemsetAsync(p.EQ, 0, sizeof(double) * MAXS * QB_NEQ * (size_t)nsys, stream));
-    // the solute's own terms (solute atoms only, atomics) need nothing of the
-    // water pass: they start on a side stream beside it, unless a bonded term
-    // or restraint reaches a solvent atom, whose gradient the water pass
-    // stores plainly
+    // waters first: their records, and their per-atom terms as the first
+    // gradient contribution (plain stores after the zeroing)
+    if (max_nwat > 0) {
+      dim3 gp(cdiv(max_nwat, 256), nsys);
+      if (fast_ww) launch("pack_waters", [&] { k_pack_waters<true><<<gp, 256, 0, stream>>>(p); });
+      else launch("pack_waters", [&] { k_pack_waters<false><<<gp, 256, 0, stream>>>(p); });
+    }
     cudaStream_t s1 = forking() ? side[0] : stream, s2 = forking() ? side[1] : stream;
-    const bool early = forking() && !terms_on_water;
-    if (early) fork_streams();
-    auto solute = [&] {
+    fork_streams();
+    // solute terms in one launch (nonbond_pp, nonbond_qp, bonded, nonbond_qq,
+    // Q bonded, restraints)
+    {
       SoluteGrid G{};
       // pair blocks per system: enough for a large solute to fill the SMs
       // when the batch is small (1184 = 8 blocks per SM over the batch)
@@ -333,23 +331,6 @@ struct Batch {
             default: k_solute_terms<0><<<g, 256, 0, s1>>>(p, G);
           }
         });
-      if (max_nsol > 0)
-        launch("atom_terms", [&] { k_atom_terms<<<dim3(cdiv(max_nsol, 128), nsys), 128, 0, s1>>>(p); });
-    };
-    if (early) solute();
-    // waters: their records, and their per-atom terms as the first gradient
-    // contribution (plain stores after the zeroing)
-    if (max_nwat > 0) {
-      dim3 gp(cdiv(max_nwat, 256), nsys);
-      if (fast_ww) launch("pack_waters", [&] { k_pack_waters<true><<<gp, 256, 0, stream>>>(p); });
-      else launch("pack_waters", [&] { k_pack_waters<false><<<gp, 256, 0, stream>>>(p); });
-    }
-    if (early) {
-      CUDA_TRY(cudaEventRecord(ev_water, stream));
-      for (int k = 0; k < 2; k++) CUDA_TRY(cudaStreamWaitEvent(side[k], ev_water, 0));
-    } else {
-      fork_streams();
-      solute();
     }
     if (max_ncgp_sol_w > 0)
       launch("nb_pw", [&] {
@@ -400,6 +381,8 @@ struct Batch {
         }
       });
     }
+    if (max_nsol > 0)
+      launch("atom_terms", [&] { k_atom_terms<<<dim3(cdiv(max_nsol, 128), nsys), 128, 0, s1>>>(p); });
     if (any_wpol) {
       launch("watpol_rank", [&] { k_watpol_rank<<<dim3(MAX_SHELLS, nsys), WPOL_BLOCK, watpol_smem, s2>>>(p); });
       launch("watpol", [&] { k_watpol_force<<<dim3(cdiv(max_nwat, WPOL_BLOCK), nsys), WPOL_BLOCK, 0, s2>>>(p); });
@@ -1045,22 +1028,6 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     for (int r = 0; r < V.nrstr_angl; r++) {
       ra.push_back(make_int4(aoff + V.rang_i[r], aoff + V.rang_j[r], aoff + V.rang_k[r], V.rang_ipsi[r]));
       ra_p.push_back(make_double2(V.rang_ang[r], V.rang_fk[r]));
-    }
-    {
-      const int ns = V.nat_solute;
-      bool w = false;
-      for (int k = 0; k < V.nbonds; k++) w |= V.bnd_i[k] >= ns || V.bnd_j[k] >= ns;
-      for (int k = 0; k < V.nangles; k++) w |= V.ang_i[k] >= ns || V.ang_j[k] >= ns || V.ang_k[k] >= ns;
-      for (int k = 0; k < V.ntors; k++)
-        w |= V.tor_i[k] >= ns || V.tor_j[k] >= ns || V.tor_k[k] >= ns || V.tor_l[k] >= ns;
-      for (int k = 0; k < V.nimps; k++)
-        w |= V.imp_i[k] >= ns || V.imp_j[k] >= ns || V.imp_k[k] >= ns || V.imp_l[k] >= ns;
-      for (int r = 0; r < V.nrstr_seq; r++) w |= V.rseq_i[r] >= ns || V.rseq_j[r] >= ns;
-      for (int r = 0; r < V.nrstr_pos; r++) w |= V.rpos_i[r] >= ns;
-      for (int r = 0; r < V.nrstr_dist; r++) w |= V.rdis_i[r] >= ns || V.rdis_j[r] >= ns;
-      for (int r = 0; r < V.nrstr_angl; r++) w |= V.rang_i[r] >= ns || V.rang_j[r] >= ns || V.rang_k[r] >= ns;
-      for (int r = 0; r < V.nrstr_wall; r++) w |= V.rwal_i[r] >= ns || V.rwal_j[r] >= ns;
-      B.terms_on_water |= w;
     }
     S.rw_off = (int)rw.size(); S.nrw = V.nrstr_wall;
     for (int r = 0; r < V.nrstr_wall; r++) {

@@ -206,8 +206,9 @@ typedef struct qb_tuning {
   int ww_chunk;               /* waters staged in shared memory per pass of the water-water kernel:
                                  a multiple of 32 between ww_chunk_min and ww_chunk_max */
   int side_streams;           /* 1: a step's force kernels fork over two side streams; 0: one stream */
-  int ww_waters_per_block;    /* waters of one system per block of the water-water kernels: 32, 64, 128
-                                 or 256 (smaller blocks: more of them, a shorter last wave, more staging) */
+  int ww_waters_per_block;    /* waters of one system per block of the water-water kernels: a multiple of
+                                 32 up to 256 (smaller blocks: more of them, a shorter last wave, more
+                                 staging of each system's records) */
   int ww_chunk_min, ww_chunk_max;  /* the batch's allowed range (read only) */
   int trials;                 /* autotune: settings timed */
   double ms_per_step;         /* autotune: device ms per step of the chosen setting */
@@ -221,7 +222,7 @@ int qb_batch_set_tuning(qb_batch *b, const qb_tuning *t);
 /* Times steps_per_trial MD steps (rounded up to whole pair-list cycles, each
  * after a cycle of warm-up) for candidate settings, one parameter at a time
  * (LRF tiles per block 1..16, the water chunk at its maximum, a half and a
- * quarter, 32/64/128/256 waters per water-water block, side streams on/off),
+ * quarter, 32/64/128/192/256 waters per water-water block, side streams on/off),
  * keeps the fastest and reports it.  The trial
  * steps are real MD steps of every system (count them as equilibration); the
  * energy records they make are cleared. */

@@ -1634,9 +1634,8 @@ void set_tuning(Batch &B, const qb_tuning &t) {
   if (t.lrf_tiles_per_block < 1 || t.lrf_tiles_per_block > 1024) fail(QB_ERR_ARG, "lrf_tiles_per_block out of range");
   if (t.ww_chunk % 32 || t.ww_chunk < B.ww_chunk_floor || t.ww_chunk > B.ww_chunk_max)
     fail(QB_ERR_ARG, "ww_chunk must be a multiple of 32 within the batch's range");
-  if (t.ww_waters_per_block != 32 && t.ww_waters_per_block != 64 && t.ww_waters_per_block != 128 &&
-      t.ww_waters_per_block != WW_WPB)
-    fail(QB_ERR_ARG, "ww_waters_per_block must be 32, 64, 128 or 256");
+  if (t.ww_waters_per_block % 32 || t.ww_waters_per_block < 32 || t.ww_waters_per_block > WW_WPB)
+    fail(QB_ERR_ARG, "ww_waters_per_block must be a multiple of 32 from 32 to 256");
   CUDA_TRY(cudaStreamSynchronize(B.stream));
   B.drop_graphs();
   B.set_lrf_tpb(t.lrf_tiles_per_block);
@@ -1717,7 +1716,7 @@ int qb_batch_autotune(qb_batch *bb, int steps_per_trial, qb_tuning *out) {
         consider(t);
       }
     if (B.max_nwat > 0)
-      for (int wpb : {64, 32, 128, qb::WW_WPB}) {
+      for (int wpb : {64, 32, 128, 192, qb::WW_WPB}) {
         qb_tuning t = best;
         t.ww_waters_per_block = wpb;
         if (wpb != best.ww_waters_per_block) consider(t);

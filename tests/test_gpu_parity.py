@@ -344,6 +344,8 @@ def test_tuning_changes_only_rounding(synthetic, oracle):
         b.set_tuning(lrf_tiles_per_block=0)
     with pytest.raises(QBError):
         b.set_tuning(ww_waters_per_block=48)
+    with pytest.raises(QBError):
+        b.set_tuning(ww_waters_per_block=288)
     s = System.open(inp, lambdas=(0.4, 0.6), seed=5)
     b = Batch([s, s], precision=FP64)
     r = b.autotune(50)

@@ -209,6 +209,8 @@ typedef struct qb_tuning {
   int ww_waters_per_block;    /* waters of one system per block of the water-water kernels: a multiple of
                                  32 up to 256 (smaller blocks: more of them, a shorter last wave, more
                                  staging of each system's records) */
+  int water_pass_per_atom;    /* 1: the water pass takes one thread per water atom (the default when three
+                                 threads per water fit on the GPU at once); 0: one thread per water */
   int ww_chunk_min, ww_chunk_max;  /* the batch's allowed range (read only) */
   int trials;                 /* autotune: settings timed */
   double ms_per_step;         /* autotune: device ms per step of the chosen setting */
@@ -216,13 +218,15 @@ typedef struct qb_tuning {
 } qb_tuning;
 
 int qb_batch_get_tuning(qb_batch *b, qb_tuning *out);
-/* Applies lrf_tiles_per_block, ww_chunk, side_streams and ww_waters_per_block
- * (QB_ERR_ARG when out of range); the pair lists are rebuilt before the next step. */
+/* Applies lrf_tiles_per_block, ww_chunk, side_streams, ww_waters_per_block and
+ * water_pass_per_atom (QB_ERR_ARG when out of range); the pair lists are rebuilt
+ * before the next step. */
 int qb_batch_set_tuning(qb_batch *b, const qb_tuning *t);
 /* Times steps_per_trial MD steps (rounded up to whole pair-list cycles, each
  * after a cycle of warm-up) for candidate settings, one parameter at a time
  * (LRF tiles per block 1..16, the water chunk at its maximum, a half and a
- * quarter, 32/64/128/192/256 waters per water-water block, side streams on/off),
+ * quarter, 32/64/128/192/256 waters per water-water block, the water pass's
+ * threads per water or per atom, side streams on/off),
  * keeps the fastest and reports it.  The trial
  * steps are real MD steps of every system (count them as equilibration); the
  * energy records they make are cleared. */

@@ -93,6 +93,9 @@ struct Batch {
   struct McState { bool started = false; int irand = 0; long long tries = 0, accepted = 0; };
   std::vector<McState> mc;
   int ww_wpb = WW_WPB;          // waters per block of the water-water kernels
+  // the water pass takes a thread per water atom when that many threads
+  // still fit on the GPU at once (small batches), else one per water
+  bool water_atom_threads = false;
   long long ww_tiles_cap = 0;   // their tile buffer's entries (32 waters per block)
   bool any_lrf = false, any_q = false, any_shake = false, any_wpol = false, any_prestr = false, any_qq = false,
        any_qb = false, any_hlj = false;
@@ -300,9 +303,15 @@ struct Batch {
     // waters first: their records, and their per-atom terms as the first
     // gradient contribution (plain stores after the zeroing)
     if (max_nwat > 0) {
-      dim3 gp(cdiv(max_nwat, 256), nsys);
-      if (fast_ww) launch("pack_waters", [&] { k_pack_waters<true><<<gp, 256, 0, stream>>>(p); });
-      else launch("pack_waters", [&] { k_pack_waters<false><<<gp, 256, 0, stream>>>(p); });
+      if (water_atom_threads) {
+        dim3 gp(cdiv(3 * max_nwat, 256), nsys);
+        if (fast_ww) launch("pack_waters", [&] { k_pack_water_atoms<true><<<gp, 256, 0, stream>>>(p); });
+        else launch("pack_waters", [&] { k_pack_water_atoms<false><<<gp, 256, 0, stream>>>(p); });
+      } else {
+        dim3 gp(cdiv(max_nwat, 256), nsys);
+        if (fast_ww) launch("pack_waters", [&] { k_pack_waters<true><<<gp, 256, 0, stream>>>(p); });
+        else launch("pack_waters", [&] { k_pack_waters<false><<<gp, 256, 0, stream>>>(p); });
+      }
     }
     cudaStream_t s1 = forking() ? side[0] : stream, s2 = forking() ? side[1] : stream;
     fork_streams();
@@ -1361,6 +1370,11 @@ void build(Batch &B, qb_handle *const *hs, int n) {
       return t;
     };
     while (B.ww_wpb > 32 && blocks(B.ww_wpb) < 2LL * sms) B.ww_wpb /= 2;
+    long long nw = 0;
+    for (int s = 0; s < n; s++) nw += B.sysh[s].nwat;
+    int thr = 2048;
+    cudaDeviceGetAttribute(&thr, cudaDevAttrMaxThreadsPerMultiProcessor, B.opt.device);
+    B.water_atom_threads = 3 * nw <= (long long)sms * thr;
   }
   // the split counts are sized for the smallest chunk a tuning may choose
   B.ww_chunk_max = P.ww_chunk;
@@ -1626,6 +1640,7 @@ void get_tuning(const Batch &B, qb_tuning *t) {
   t->ww_chunk = B.P.ww_chunk;
   t->side_streams = B.streams_on ? 1 : 0;
   t->ww_waters_per_block = B.ww_wpb;
+  t->water_pass_per_atom = B.water_atom_threads ? 1 : 0;
   t->ww_chunk_min = B.ww_chunk_floor;
   t->ww_chunk_max = B.ww_chunk_max;
 }
@@ -1636,6 +1651,7 @@ void set_tuning(Batch &B, const qb_tuning &t) {
     fail(QB_ERR_ARG, "ww_chunk must be a multiple of 32 within the batch's range");
   if (t.ww_waters_per_block % 32 || t.ww_waters_per_block < 32 || t.ww_waters_per_block > WW_WPB)
     fail(QB_ERR_ARG, "ww_waters_per_block must be a multiple of 32 from 32 to 256");
+  if (t.water_pass_per_atom != 0 && t.water_pass_per_atom != 1) fail(QB_ERR_ARG, "water_pass_per_atom must be 0 or 1");
   CUDA_TRY(cudaStreamSynchronize(B.stream));
   B.drop_graphs();
   B.set_lrf_tpb(t.lrf_tiles_per_block);
@@ -1643,6 +1659,7 @@ void set_tuning(Batch &B, const qb_tuning &t) {
   B.P.ww_nch = (std::max(B.max_nwat, 1) + t.ww_chunk - 1) / t.ww_chunk;
   B.streams_on = t.side_streams != 0;
   if (t.ww_waters_per_block != B.ww_wpb) set_ww_tiles(B, t.ww_waters_per_block);
+  B.water_atom_threads = t.water_pass_per_atom != 0;
   B.lists_stale = true;   // the water-water split counts depend on the chunk
 }
 
@@ -1721,6 +1738,11 @@ int qb_batch_autotune(qb_batch *bb, int steps_per_trial, qb_tuning *out) {
         t.ww_waters_per_block = wpb;
         if (wpb != best.ww_waters_per_block) consider(t);
       }
+    if (B.max_nwat > 0) {
+      qb_tuning t = best;
+      t.water_pass_per_atom = !best.water_pass_per_atom;
+      consider(t);
+    }
     if (B.side[0]) {
       qb_tuning t = best;
       t.side_streams = !best.side_streams;

@@ -2290,6 +2290,71 @@ __global__ void k_pack_waters(DevPtrs P) {
   warp_add(&P.E[s * QB_NE + QB_E_RST_SOLVENT_RADIAL], erad);
 }
 
+// The water pass with one thread per water atom (the same terms in the same
+// order per atom; the O's thread adds the radial restraint, the first H's the
+// polarisation angle, the second H's the water's record): three times the
+// threads of k_pack_waters for batches too small to fill the GPU with one
+// thread per water.
+template <bool MIXED>
+__global__ void k_pack_water_atoms(DevPtrs P) {
+  int s = blockIdx.y;
+  const SysDev &S = P.sys[s];
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iw = t / 3, a = t - 3 * iw;     // water, and its atom this thread takes
+  double elrf = 0, efix = 0, eshell = 0, erad = 0;
+  if (iw < S.nwat) {
+    const int o = S.aoff + S.nsol + 3 * iw, i = o + a;
+    const double4 xa4 = P.x[i];
+    const double3 xa = make_double3(xa4.x, xa4.y, xa4.z);
+    if (a == 1 && S.wpol && S.nshell > 0)
+      watpol_angle(P, S, S.woff + iw, (P.flags[o] & F_EXCL) != 0, P.x[o], xa4, P.x[o + 2]);
+    if (a == 2) {
+      const double4 A = P.x[o], B = P.x[o + 1], C = xa4;
+      constexpr int W = WatRec<MIXED>::words;
+      float4 *r = P.wrec + (size_t)(S.woff + iw) * W;
+      if (MIXED) {
+        float hx = (float)A.x, hy = (float)A.y, hz = (float)A.z;
+        float lx = (float)(A.x - (double)hx), ly = (float)(A.y - (double)hy), lz = (float)(A.z - (double)hz);
+        r[0] = make_float4(hx, hy, hz, lx);
+        r[1] = make_float4(ly, lz, (float)(B.x - A.x), (float)(C.x - A.x));
+        r[2] = make_float4((float)(B.y - A.y), (float)(C.y - A.y), (float)(B.z - A.z), (float)(C.z - A.z));
+      } else {
+        double2 *rd = reinterpret_cast<double2 *>(r);
+        rd[0] = make_double2(A.x, A.y); rd[1] = make_double2(A.z, B.x); rd[2] = make_double2(B.y, B.z);
+        rd[3] = make_double2(C.x, C.y); rd[4] = make_double2(C.z, 0.0);
+      }
+    }
+    double g[3] = {0, 0, 0};
+    const uint8_t fo = P.flags[o], fl = P.flags[i];
+    if (S.use_lrf && !((fo & P.flags[o + 1] & P.flags[o + 2]) & F_EXCL) && !(fl & F_EXCL) && P.iq[i] < 0) {
+      LrfRec R;
+      lrf_load(P, P.cgp[o], R);
+      elrf += lrf_eval(R, xa, (double)P.crg[i], g);
+    }
+    if (fl & (F_EXCL | F_SHELL)) fix_shell_atom(P, S, i, fl, xa, g, efix, eshell);
+    // the solvent sphere's radial restraint on the O (restrain_solvent; none in a periodic box)
+    if (a == 0 && !(fo & F_EXCL) && !S.pbc) {
+      const double shift = S.fk_ws != 0. ? sqrt((double)kBoltzF * P.st[s].Tfree / S.fk_ws) : 0.;
+      double dr[3] = {xa.x - S.xw[0], xa.y - S.xw[1], xa.z - S.xw[2]};
+      double b = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+      double db = b - (S.rwat - shift), e, dv;
+      if (db > 0) { e = 0.5 * S.fk_ws * db * db - S.Dwmz; dv = S.fk_ws * db / b; }
+      else if (b > 0.0) {
+        double fexp = exp(S.awmz * db);
+        e = S.Dwmz * (fexp * fexp - 2. * fexp);
+        dv = -2. * S.Dwmz * S.awmz * (fexp - fexp * fexp) / b;
+      } else { e = 0; dv = 0; }
+      erad += e;
+      for (int k = 0; k < 3; k++) g[k] += dv * dr[k];
+    }
+    P.d[i] = make_double4(g[0], g[1], g[2], 0.0);
+  }
+  warp_add(&P.E[s * QB_NE + QB_E_LRF], elrf);
+  warp_add(&P.E[s * QB_NE + QB_E_RST_FIX], efix);
+  warp_add(&P.E[s * QB_NE + QB_E_RST_SHELL], eshell);
+  warp_add(&P.E[s * QB_NE + QB_E_RST_SOLVENT_RADIAL], erad);
+}
+
 // ---------------------------------------------------------------- bonded
 
 __device__ __forceinline__ double dihedral(const DevPtrs &P, int i, int j, int k, int l, double dp[12]) {

@@ -175,6 +175,26 @@ def test_mixed_precision_error_vs_fp64(synthetic, case):
     assert grad_err(b32.gradient(0), b64.gradient(0)) < G_TOL
 
 
+@pytest.mark.parametrize("precision", [FP64, MIXED])
+def test_water_pass_threads(synthetic, precision):
+    """The water pass with a thread per water or per water atom: the same
+    per-atom terms in the same order, so the same records (packed FP32 ones
+    too), energies and forces, to the rounding of the atomic sums."""
+    sys_ = System.open(synthetic["c1"].inp)
+    out = []
+    for per_atom in (0, 1):
+        b = Batch([sys_], precision=precision)
+        b.set_tuning(water_pass_per_atom=per_atom)
+        assert b.tuning()["water_pass_per_atom"] == per_atom
+        b.evaluate(energies=True)
+        E, EQ = b.energy_vectors(0)
+        b.evaluate(energies=False)
+        out.append((E, EQ, b.gradient(0)))
+    (E0, Q0, g0), (E1, Q1, g1) = out
+    assert np.max(np.abs(E0 - E1)) < 1e-8 and np.max(np.abs(Q0 - Q1), initial=0.0) < 1e-8
+    assert np.max(np.abs(g0 - g1)) < 1e-9
+
+
 def _restart_copy(tmp_path, inp, name, x, v, theta):
     """A copy of `inp` that starts from coordinates x and velocities v (and the
     polarisation restraint's theta corrections) through a restart file."""
@@ -314,15 +334,16 @@ def test_perturbations_with_different_q_atoms_in_one_batch(tmp_path, oracle):
 
 def test_tuning_changes_only_rounding(synthetic, oracle):
     """The run-time choices of the step kernels (LRF tiles per block, water
-    chunk, waters per water-water block, side streams) change only the order
-    of atomic sums: two copies of
+    chunk, waters per water-water block, the water pass's threads, side
+    streams) change only the order of atomic sums: two copies of
     a batch, one with other settings, give the same records and coordinates
     to rounding; out-of-range settings are refused; after autotuning the
     batch still matches the oracle."""
     from q_b200 import QBError
     inp = synthetic["c1"].inp
     runs = []
-    for setting in (None, dict(lrf_tiles_per_block=1, ww_chunk=256, side_streams=0, ww_waters_per_block=32)):
+    for setting in (None, dict(lrf_tiles_per_block=1, ww_chunk=256, side_streams=0, ww_waters_per_block=32,
+                               water_pass_per_atom=0)):
         s = System.open(inp, lambdas=(0.4, 0.6), seed=5)
         b = Batch([s], precision=FP64)
         t = b.tuning()
@@ -330,8 +351,8 @@ def test_tuning_changes_only_rounding(synthetic, oracle):
         if setting:
             b.set_tuning(**setting)
             t = b.tuning()
-            assert (t["lrf_tiles_per_block"], t["ww_chunk"], t["side_streams"], t["ww_waters_per_block"]) == \
-                (1, 256, 0, 32)
+            assert (t["lrf_tiles_per_block"], t["ww_chunk"], t["side_streams"], t["ww_waters_per_block"],
+                    t["water_pass_per_atom"]) == (1, 256, 0, 32, 0)
         b.run(60)          # crosses two list rebuilds
         runs.append((b.history(0, 0), b.coords(0)))
     ((s0, E0, Q0), x0), ((s1, E1, Q1), x1) = runs
@@ -353,7 +374,8 @@ def test_tuning_changes_only_rounding(synthetic, oracle):
     assert r["ww_chunk_min"] <= r["ww_chunk"] <= r["ww_chunk_max"] and r["lrf_tiles_per_block"] >= 1
     # the chosen setting, applied to a fresh batch, matches the oracle
     b = Batch([s], precision=FP64)
-    b.set_tuning(**{k: r[k] for k in ("lrf_tiles_per_block", "ww_chunk", "side_streams", "ww_waters_per_block")})
+    b.set_tuning(**{k: r[k] for k in ("lrf_tiles_per_block", "ww_chunk", "side_streams", "ww_waters_per_block",
+                                      "water_pass_per_atom")})
     b.final_energy()
     o = oracle.create(s)
     o.final_energy()

@@ -96,6 +96,9 @@ struct Batch {
   // the water pass takes a thread per water atom when that many threads
   // still fit on the GPU at once (small batches), else one per water
   bool water_atom_threads = false;
+  // every system is solute atoms then 3-atom waters, and some system has
+  // waters: the water pass writes the whole gradient (no memset)
+  bool water_pass_zeroes = false;
   long long ww_tiles_cap = 0;   // their tile buffer's entries (32 waters per block)
   bool any_lrf = false, any_q = false, any_shake = false, any_wpol = false, any_prestr = false, any_qq = false,
        any_qb = false, any_hlj = false;
@@ -297,18 +300,19 @@ struct Batch {
     DevPtrs &p = P;
     const bool mixed = opt.precision == QB_MIXED;
     const bool fast_ww = mixed && !ene;
-    CUDA_TRY(cudaMemsetAsync(p.d, 0, sizeof(double4) * (size_t)p.natoms_tot, stream));
+    // the water pass stores every water gradient and zeroes the solute's
+    if (!water_pass_zeroes) CUDA_TRY(cudaMemsetAsync(p.d, 0, sizeof(double4) * (size_t)p.natoms_tot, stream));
     CUDA_TRY(cudaMemsetAsync(p.E, 0, sizeof(double) * QB_NE * (size_t)nsys, stream));
     CUDA_TRY(cudaMemsetAsync(p.EQ, 0, sizeof(double) * MAXS * QB_NEQ * (size_t)nsys, stream));
     // waters first: their records, and their per-atom terms as the first
     // gradient contribution (plain stores after the zeroing)
     if (max_nwat > 0) {
       if (water_atom_threads) {
-        dim3 gp(cdiv(3 * max_nwat, 256), nsys);
+        dim3 gp(cdiv(std::max(3 * max_nwat, max_nsol), 256), nsys);
         if (fast_ww) launch("pack_waters", [&] { k_pack_water_atoms<true><<<gp, 256, 0, stream>>>(p); });
         else launch("pack_waters", [&] { k_pack_water_atoms<false><<<gp, 256, 0, stream>>>(p); });
       } else {
-        dim3 gp(cdiv(max_nwat, 256), nsys);
+        dim3 gp(cdiv(std::max(max_nwat, max_nsol), 256), nsys);
         if (fast_ww) launch("pack_waters", [&] { k_pack_waters<true><<<gp, 256, 0, stream>>>(p); });
         else launch("pack_waters", [&] { k_pack_waters<false><<<gp, 256, 0, stream>>>(p); });
       }
@@ -1375,6 +1379,9 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     int thr = 2048;
     cudaDeviceGetAttribute(&thr, cudaDevAttrMaxThreadsPerMultiProcessor, B.opt.device);
     B.water_atom_threads = 3 * nw <= (long long)sms * thr;
+    B.water_pass_zeroes = B.max_nwat > 0;
+    for (int s = 0; s < n; s++)
+      if (B.sysh[s].natom != B.sysh[s].nsol + 3 * B.sysh[s].nwat) B.water_pass_zeroes = false;
   }
   // the split counts are sized for the smallest chunk a tuning may choose
   B.ww_chunk_max = P.ww_chunk;

@@ -2251,16 +2251,18 @@ __global__ void k_atom_terms(DevPtrs P) {
   warp_add(&P.E[s * QB_NE + QB_E_RST_SOLVENT_RADIAL], erad);
 }
 
-// Water pass, one thread per water, first kernel after the gradient is
-// zeroed: the position record of the water-water kernel (see WatRec), the
-// polarisation angle and shell, and the per-atom terms of its three atoms
-// (water_terms), stored as their first gradient contribution.
+// Water pass, one thread per water, the step's first force kernel: the
+// position record of the water-water kernel (see WatRec), the polarisation
+// angle and shell, and the per-atom terms of its three atoms (water_terms),
+// stored as their first gradient contribution; thread i also zeroes the
+// gradient of solute atom i (the grid covers the larger of the two counts).
 template <bool MIXED>
 __global__ void k_pack_waters(DevPtrs P) {
   int s = blockIdx.y;
   const SysDev &S = P.sys[s];
   int iw = blockIdx.x * blockDim.x + threadIdx.x;
   double elrf = 0, efix = 0, eshell = 0, erad = 0;
+  if (iw < S.nsol) P.d[S.aoff + iw] = make_double4(0.0, 0.0, 0.0, 0.0);   // the solute's gradient zeroed
   if (iw < S.nwat) {
     int o = S.aoff + S.nsol + 3 * iw;
     double4 a = P.x[o], b = P.x[o + 1], c = P.x[o + 2];
@@ -2302,6 +2304,7 @@ __global__ void k_pack_water_atoms(DevPtrs P) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int iw = t / 3, a = t - 3 * iw;     // water, and its atom this thread takes
   double elrf = 0, efix = 0, eshell = 0, erad = 0;
+  if (t < S.nsol) P.d[S.aoff + t] = make_double4(0.0, 0.0, 0.0, 0.0);   // the solute's gradient zeroed
   if (iw < S.nwat) {
     const int o = S.aoff + S.nsol + 3 * iw, i = o + a;
     const double4 xa4 = P.x[i];

@@ -713,6 +713,9 @@ __global__ void __launch_bounds__(WL_BLOCK) k_list_ww(DevPtrs P, int force) {
       uint16_t *out = P.ww + (size_t)gw * P.ww_cap;
       int *sp = P.ww_sp + (size_t)gw * P.ww_nch;
       int cnt = scnt[iw - i0];
+      // the next end of a force-kernel chunk at or after c0 (multiples of
+      // ww_chunk from ww_chunk on): the scan passes it as a multiple of 32
+      int nxt = max(P.ww_chunk, (c0 + P.ww_chunk - 1) / P.ww_chunk * P.ww_chunk);
       for (int b = 0; b < cn; b += 64) {
         // lane takes j = b + lane and b + 32 + lane
         float4 a = make_float4(0.f, 0.f, 0.f, -1.f), e = a;
@@ -753,7 +756,10 @@ __global__ void __launch_bounds__(WL_BLOCK) k_list_ww(DevPtrs P, int force) {
 #pragma unroll
         for (int h = 0; h < 2; h++) {
           const int base = c0 + b + 32 * h;
-          if (base > 0 && base % P.ww_chunk == 0 && lane == 0) sp[base / P.ww_chunk - 1] = min(cnt, P.ww_cap);
+          if (base == nxt) {
+            if (lane == 0) sp[nxt / P.ww_chunk - 1] = min(cnt, P.ww_cap);
+            nxt += P.ww_chunk;
+          }
           const unsigned bal = __ballot_sync(FULL, ok2[h]);
           if (ok2[h]) {
             const int pos = cnt + __popc(bal & ((1u << lane) - 1u));

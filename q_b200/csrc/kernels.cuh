@@ -1683,10 +1683,12 @@ __global__ void __launch_bounds__(PW_BLOCK) k_nb_pw(DevPtrs P) {
     const double4 x4 = t - ta < PW_MAXA ? sx[t - ta] : P.x[A.atom];
     const double3 xi = make_double3(x4.x, x4.y, x4.z);
     double fi[3] = {0.0, 0.0, 0.0};
-    if (act && F32) {
+    if (F32) {
+      // forces alone: the group atom's FP32 terms summed over the warp in FP32
       float gi[3] = {0.f, 0.f, 0.f};
 #pragma unroll
       for (int b = 0; b < 3; b++) {
+        if (!act) break;
         const float dx = (float)(xw[b].x - xi.x), dy = (float)(xw[b].y - xi.y), dz = (float)(xw[b].z - xi.z);
         const float r = rsqrt_ftz(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
         const float r2 = r * r, r6 = r2 * r2 * r2;
@@ -1697,8 +1699,12 @@ __global__ void __launch_bounds__(PW_BLOCK) k_nb_pw(DevPtrs P) {
         fw32[3 * b] = fmaf(dv, dx, fw32[3 * b]); fw32[3 * b + 1] = fmaf(dv, dy, fw32[3 * b + 1]);
         fw32[3 * b + 2] = fmaf(dv, dz, fw32[3 * b + 2]);
       }
-      fi[0] = gi[0]; fi[1] = gi[1]; fi[2] = gi[2];
-    } else if (act) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) gi[c] = warp_sumf(gi[c]);
+      if (lane == 0) atomic_add3(P.d, A.atom, (double)gi[0], (double)gi[1], (double)gi[2]);
+      continue;
+    }
+    if (act) {
 #pragma unroll
       for (int b = 0; b < 3; b++) {
         double dx = xw[b].x - xi.x, dy = xw[b].y - xi.y, dz = xw[b].z - xi.z;

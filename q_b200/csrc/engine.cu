@@ -739,7 +739,7 @@ struct Batch {
     if (fused)
       launch("leapfrog_shake3", [&] { k_leapfrog_shake3<<<cdiv(p.nsh3, 128), 128, 0, stream>>>(p); });
     cudaStream_t sl = fused && forking() ? side[0] : stream;
-    launch("leapfrog", [&] { k_leapfrog<<<cdiv(p.natoms_tot, 256), 256, 0, sl>>>(p); });
+    if (p.n_lf > 0) launch("leapfrog", [&] { k_leapfrog<<<cdiv(p.n_lf, 256), 256, 0, sl>>>(p); });
     if (any_shake && p.nshg > 0)
       launch("shake_general", [&] { k_shake_general<<<p.nshg, SHG_BLOCK, p.shg_smem, sl>>>(p); });
     if (fused) join_streams();
@@ -1294,6 +1294,13 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     // their atoms are moved by the fused leapfrog + SHAKE kernel, not k_leapfrog
     for (auto &a : at3) { flags[a.x] |= F_SH3; flags[a.y] |= F_SH3; flags[a.z] |= F_SH3; }
     if (!at3.empty()) CUDA_TRY(cudaMemcpy(P.flags, flags.data(), flags.size(), cudaMemcpyHostToDevice));
+    {
+      std::vector<int> lf;
+      for (int g = 0; g < (int)flags.size(); g++)
+        if (!(flags[g] & F_SH3)) lf.push_back(g);
+      P.n_lf = (int)lf.size();
+      P.lf_atoms = dev_upload(lf, o);
+    }
     // other molecules: local atoms, constraints grouped into dependency levels
     std::vector<int4> info, info2;
     std::vector<int> gat, glev;

@@ -184,6 +184,7 @@ struct DevPtrs {
   int4 *qp;                                // gq, j, lj, qlj
   int *qw;                                 // water O atoms
   uint16_t *ww;                            // [gw*ww_cap + k] local water index
+  int *lf_atoms, n_lf;                     // atoms k_leapfrog moves (all but 3-constraint molecules')
   int *ww_n, *ww_sp;                       // count per water; [gw*ww_nch + c] count below chunk c's end
   int ww_cap, ww_chunk, ww_nch;
   int2 *ww_tiles;                          // water-water force blocks: (system, first water)

@@ -3027,14 +3027,16 @@ __device__ __forceinline__ void kin_tally(DevPtrs &P, int s, const double *acc) 
   }
 }
 
-// Leap-frog update (md.f90:4080-4108): v from the gradient with the
+// Leap-frog update (md.f90:4080-4108), one thread per atom of the list of
+// atoms outside 3-constraint molecules: v from the gradient with the
 // Berendsen factor of solute or solvent, x from v.  With SHAKE the reference
 // then sets v = (x - xx)/dt for every atom (md.f90:4119); for atoms in no
 // constraint that is done here (their x is final), for the others by the
 // SHAKE kernels.  The kinetic energy of atoms whose velocity is final here
 // is added to the system's sums.
 __global__ void k_leapfrog(DevPtrs P) {
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int g = k < P.n_lf ? P.lf_atoms[k] : P.natoms_tot;   // the atoms outside 3-constraint molecules
   int s = -1;
   double acc[4] = {0, 0, 0, 0};
   // a system that raised an error stays where the failing step left it;

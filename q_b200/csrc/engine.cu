@@ -311,8 +311,8 @@ struct Batch {
         dim3 gp(cdiv(std::max(3 * max_nwat, max_nsol), 256), nsys);
         if (fast_ww) launch("pack_waters", [&] { k_pack_water_atoms<true><<<gp, 256, 0, stream>>>(p); });
         else launch("pack_waters", [&] { k_pack_water_atoms<false><<<gp, 256, 0, stream>>>(p); });
-      } else {
-        dim3 gp(cdiv(std::max(max_nwat, max_nsol), 256), nsys);
+      } else if (p.n_pk_tiles > 0) {
+        const int gp = p.n_pk_tiles;
         if (fast_ww) launch("pack_waters", [&] { k_pack_waters<true><<<gp, 256, 0, stream>>>(p); });
         else launch("pack_waters", [&] { k_pack_waters<false><<<gp, 256, 0, stream>>>(p); });
       }
@@ -368,8 +368,8 @@ struct Batch {
       } else {
         launch("nb_ww", [&] { k_nb_ww<false, false><<<gw, WW_BLOCK, smem, stream>>>(p, wpb); });
       }
-      if (any_q) launch("nb_qw", [&] {
-        dim3 g(cdiv(max_nwat, 128), nsys);
+      if (any_q && p.n_qw_tiles > 0) launch("nb_qw", [&] {
+        const int g = p.n_qw_tiles;
         if (any_hlj) {   // hydrogen LJ: the generic state count only
           if (max_nq > NQ_SHARED) k_nb_qw<0, false, true><<<g, 128, 0, s2>>>(p);
           else k_nb_qw<0, true, true><<<g, 128, 0, s2>>>(p);
@@ -398,7 +398,8 @@ struct Batch {
       launch("atom_terms", [&] { k_atom_terms<<<dim3(cdiv(max_nsol, 128), nsys), 128, 0, s1>>>(p); });
     if (any_wpol) {
       launch("watpol_rank", [&] { k_watpol_rank<<<dim3(MAX_SHELLS, nsys), WPOL_BLOCK, watpol_smem, s2>>>(p); });
-      launch("watpol", [&] { k_watpol_force<<<dim3(cdiv(max_nwat, WPOL_BLOCK), nsys), WPOL_BLOCK, 0, s2>>>(p); });
+      if (p.n_wp_tiles > 0)
+        launch("watpol", [&] { k_watpol_force<<<p.n_wp_tiles, WPOL_BLOCK, 0, s2>>>(p); });
     }
     join_streams();
     check_launch("force kernels");
@@ -1300,6 +1301,19 @@ void build(Batch &B, qb_handle *const *hs, int n) {
         if (!(flags[g] & F_SH3)) lf.push_back(g);
       P.n_lf = (int)lf.size();
       P.lf_atoms = dev_upload(lf, o);
+    }
+    {
+      std::vector<int2> pk, wp, qw;
+      for (int s = 0; s < n; s++) {
+        const SysDev &S = B.sysh[s];
+        for (int i0 = 0; i0 < std::max(S.nwat, S.nsol); i0 += 256) pk.push_back(make_int2(s, i0));
+        if (S.wpol && S.nshell > 0)
+          for (int i0 = 0; i0 < S.nwat; i0 += WPOL_BLOCK) wp.push_back(make_int2(s, i0));
+        if (S.nq > 0)
+          for (int i0 = 0; i0 < S.nwat; i0 += 128) qw.push_back(make_int2(s, i0));
+      }
+      P.n_pk_tiles = (int)pk.size(); P.n_wp_tiles = (int)wp.size(); P.n_qw_tiles = (int)qw.size();
+      P.pk_tiles = dev_upload(pk, o); P.wp_tiles = dev_upload(wp, o); P.qw_tiles = dev_upload(qw, o);
     }
     // other molecules: local atoms, constraints grouped into dependency levels
     std::vector<int4> info, info2;

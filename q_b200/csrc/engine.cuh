@@ -184,7 +184,12 @@ struct DevPtrs {
   int4 *qp;                                // gq, j, lj, qlj
   int *qw;                                 // water O atoms
   uint16_t *ww;                            // [gw*ww_cap + k] local water index
-  int *lf_atoms, n_lf;                     // atoms k_leapfrog moves (all but 3-constraint molecules')
+  int *lf_atoms, n_lf;
+  // blocks of the per-water kernels, (system, first index) each, only where
+  // a system has work: the water pass (256 waters or solute atoms), the
+  // polarisation forces (WPOL_BLOCK waters) and Q-water (128 list entries)
+  int2 *pk_tiles, *wp_tiles, *qw_tiles;
+  int n_pk_tiles, n_wp_tiles, n_qw_tiles;                     // atoms k_leapfrog moves (all but 3-constraint molecules')
   int *ww_n, *ww_sp;                       // count per water; [gw*ww_nch + c] count below chunk c's end
   int ww_cap, ww_chunk, ww_nch;
   int2 *ww_tiles;                          // water-water force blocks: (system, first water)

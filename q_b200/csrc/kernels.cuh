@@ -1825,7 +1825,8 @@ struct QwState { float qO, qH; double A, B, sc, AH, BH, scH; };
 template <int NSC, bool SHQ, bool HLJ, bool F32 = false>
 __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
   constexpr int NA = NSC > 0 ? NSC : MAXS;
-  int s = blockIdx.y;
+  const int2 tile = P.qw_tiles[blockIdx.x];   // (system, first list entry)
+  const int s = tile.x;
   const SysDev &S = P.sys[s];
   __shared__ double fq[NQ_SHARED * 3];
   __shared__ double4 qx[NQ_SHARED];        // position; w: LJ code
@@ -1834,7 +1835,7 @@ __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
   __shared__ QwState qst[NQ_SHARED * NA];
   if (S.nq == 0) return;
   const int n = P.st[s].qw_n;
-  if (blockIdx.x * blockDim.x >= n) return;
+  if (tile.y >= n) return;
   const int NS = NSC > 0 ? NSC : S.S, ncol = S.natyps + S.nq;
   const bool hlj = HLJ && S.hlj;           // this system's water hydrogens carry LJ
   const bool shq = SHQ;                    // every system's Q atoms fit the shared tables
@@ -1873,7 +1874,7 @@ __global__ void __launch_bounds__(128, SHQ ? 4 : 1) k_nb_qw(DevPtrs P) {
   double el[NA], vdw[NA];
 #pragma unroll
   for (int st = 0; st < NA; st++) { el[st] = 0; vdw[st] = 0; }
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = tile.y + threadIdx.x;
   const bool act = k < n;
   const int j = act ? P.qw[S.qw_off + k] : P.qw[S.qw_off];
   double3 xO = ld3(P.x, j), xH1 = ld3(P.x, j + 1), xH2 = ld3(P.x, j + 2);
@@ -2270,9 +2271,10 @@ __global__ void k_atom_terms(DevPtrs P) {
 // gradient of solute atom i (the grid covers the larger of the two counts).
 template <bool MIXED>
 __global__ void k_pack_waters(DevPtrs P) {
-  int s = blockIdx.y;
+  const int2 tile = P.pk_tiles[blockIdx.x];   // (system, first water or solute atom)
+  const int s = tile.x;
   const SysDev &S = P.sys[s];
-  int iw = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iw = tile.y + threadIdx.x;
   double elrf = 0, efix = 0, eshell = 0, erad = 0;
   if (iw < S.nsol) P.d[S.aoff + iw] = make_double4(0.0, 0.0, 0.0, 0.0);   // the solute's gradient zeroed
   if (iw < S.nwat) {
@@ -2945,10 +2947,11 @@ __global__ void __launch_bounds__(WPOL_BLOCK) k_watpol_rank(DevPtrs P) {
 }
 
 __global__ void __launch_bounds__(WPOL_BLOCK) k_watpol_force(DevPtrs P) {
-  const int s = blockIdx.y;
+  const int2 tile = P.wp_tiles[blockIdx.x];   // (system, first water)
+  const int s = tile.x;
   const SysDev &S = P.sys[s];
   if (!S.wpol || S.nshell == 0) return;
-  const int iw = blockIdx.x * WPOL_BLOCK + threadIdx.x;
+  const int iw = tile.y + threadIdx.x;
   double epol = 0;
   const int is = iw < S.nwat ? (int)P.wshell[S.woff + iw] : -1;
   if (is >= 0) {

@@ -345,9 +345,9 @@ struct Batch {
           }
         });
     }
-    if (max_ncgp_sol_w > 0)
+    if (p.n_pw_groups > 0)
       launch("nb_pw", [&] {
-        const dim3 g(cdiv(p.pwg_cap, PW_BLOCK), max_ncgp_sol_w, nsys);
+        const dim3 g(p.n_pw_groups, cdiv(p.pwg_cap, PW_BLOCK));
         if (fast_ww) k_nb_pw<true><<<g, PW_BLOCK, 0, s1>>>(p);
         else k_nb_pw<false><<<g, PW_BLOCK, 0, s1>>>(p);
       });
@@ -1312,6 +1312,12 @@ void build(Batch &B, qb_handle *const *hs, int n) {
         if (S.nq > 0)
           for (int i0 = 0; i0 < S.nwat; i0 += 128) qw.push_back(make_int2(s, i0));
       }
+      std::vector<int2> pwg;
+      for (int s = 0; s < n; s++)
+        if (B.sysh[s].nwat > 0)
+          for (int ig = 0; ig < B.sysh[s].ncgp_sol; ig++) pwg.push_back(make_int2(s, ig));
+      P.n_pw_groups = (int)pwg.size();
+      P.pw_groups = dev_upload(pwg, o);
       P.n_pk_tiles = (int)pk.size(); P.n_wp_tiles = (int)wp.size(); P.n_qw_tiles = (int)qw.size();
       P.pk_tiles = dev_upload(pk, o); P.wp_tiles = dev_upload(wp, o); P.qw_tiles = dev_upload(qw, o);
     }

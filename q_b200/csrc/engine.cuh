@@ -189,7 +189,9 @@ struct DevPtrs {
   // a system has work: the water pass (256 waters or solute atoms), the
   // polarisation forces (WPOL_BLOCK waters) and Q-water (128 list entries)
   int2 *pk_tiles, *wp_tiles, *qw_tiles;
-  int n_pk_tiles, n_wp_tiles, n_qw_tiles;                     // atoms k_leapfrog moves (all but 3-constraint molecules')
+  int n_pk_tiles, n_wp_tiles, n_qw_tiles;
+  int2 *pw_groups;                         // (system, solute group) of systems with waters
+  int n_pw_groups;                     // atoms k_leapfrog moves (all but 3-constraint molecules')
   int *ww_n, *ww_sp;                       // count per water; [gw*ww_nch + c] count below chunk c's end
   int ww_cap, ww_chunk, ww_nch;
   int2 *ww_tiles;                          // water-water force blocks: (system, first water)

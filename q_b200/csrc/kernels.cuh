@@ -1640,13 +1640,13 @@ constexpr int PW_BLOCK = 128, PW_MAXA = 128;   // group atoms staged in shared m
 // steps run the FP64 form.
 template <bool F32>
 __global__ void __launch_bounds__(PW_BLOCK) k_nb_pw(DevPtrs P) {
-  const int s = blockIdx.z;
+  const int2 sgi = P.pw_groups[blockIdx.x];   // (system, solute group)
+  const int s = sgi.x;
   const SysDev &S = P.sys[s];
-  const int ig = blockIdx.y;
-  if (ig >= S.ncgp_sol) return;
+  const int ig = sgi.y;
   const int sg = S.csoff + ig;
   const int n = P.pwg_n[sg];
-  const int k0 = blockIdx.x * PW_BLOCK;
+  const int k0 = blockIdx.y * PW_BLOCK;
   if (k0 >= n) return;
   const int k = k0 + threadIdx.x;
   const bool act = k < n;

@@ -93,6 +93,7 @@ struct Batch {
   struct McState { bool started = false; int irand = 0; long long tries = 0, accepted = 0; };
   std::vector<McState> mc;
   int ww_wpb = WW_WPB;          // waters per block of the water-water kernels
+  int max_nshell = 0;           // polarisation shells of the batch's systems, at most
   // the water pass takes a thread per water atom when that many threads
   // still fit on the GPU at once (small batches), else one per water
   bool water_atom_threads = false;
@@ -397,7 +398,7 @@ struct Batch {
     if (max_nsol > 0)
       launch("atom_terms", [&] { k_atom_terms<<<dim3(cdiv(max_nsol, 128), nsys), 128, 0, s1>>>(p); });
     if (any_wpol) {
-      launch("watpol_rank", [&] { k_watpol_rank<<<dim3(MAX_SHELLS, nsys), WPOL_BLOCK, watpol_smem, s2>>>(p); });
+      launch("watpol_rank", [&] { k_watpol_rank<<<dim3(std::max(max_nshell, 1), nsys), WPOL_BLOCK, watpol_smem, s2>>>(p); });
       if (p.n_wp_tiles > 0)
         launch("watpol", [&] { k_watpol_force<<<p.n_wp_tiles, WPOL_BLOCK, 0, s2>>>(p); });
     }
@@ -1053,6 +1054,7 @@ void build(Batch &B, qb_handle *const *hs, int n) {
     if (!S.switch_atoms) B.any_any_atom = true;
     S.ff_type = V.ff_type; S.use_lrf = V.use_LRF; S.qvdw = V.qvdw_flag; S.qq_lib = V.qq_use_library_charges;
     S.wpol = V.wpol_restr && V.nwpolr_shell > 0; S.nshell = V.nwpolr_shell;
+    if (S.wpol) B.max_nshell = std::max(B.max_nshell, std::min(S.nshell, MAX_SHELLS));
     if (S.nshell > MAX_SHELLS) fail(QB_ERR_UNSUPPORTED, "too many water polarisation shells");
     S.iac_ow = V.iac_ow; S.separate_scaling = V.separate_scaling; S.detail_temps = V.detail_temps;
     S.qp_once = V.Rcq > V.rexcl_o;

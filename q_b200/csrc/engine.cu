@@ -366,6 +366,15 @@ struct Batch {
         });
       } else if (any_hlj) {
         launch("nb_ww", [&] { k_nb_ww<false, true><<<gw, WW_BLOCK, smem, stream>>>(p, wpb); });
+      } else if (mixed) {
+        // a recording step of the mixed engine: the packed kernel's forces,
+        // the energies in FP64 over each pair once
+        const size_t smem32 = (size_t)p.ww_chunk * WatRec<true>::words * sizeof(float4);
+        launch("nb_ww_x2", [&] {
+          if (any_box) k_nb_ww_x2<true><<<gw, WWX_BLOCK, smem32, stream>>>(p, wpb);
+          else k_nb_ww_x2<false><<<gw, WWX_BLOCK, smem32, stream>>>(p, wpb);
+        });
+        launch("nb_ww", [&] { k_nb_ww<false, false, true><<<gw, WW_BLOCK, smem, stream>>>(p, wpb); });
       } else {
         launch("nb_ww", [&] { k_nb_ww<false, false><<<gw, WW_BLOCK, smem, stream>>>(p, wpb); });
       }
@@ -1437,17 +1446,21 @@ void build(Batch &B, qb_handle *const *hs, int n) {
   P.ww_cap = ww_cap;
   P.ww = dev_alloc<uint16_t>((size_t)std::max(woff, 1) * ww_cap, o);
   P.ww_n = dev_alloc<int>(std::max(woff, 1), o);
+  P.ww_mid = dev_alloc<int>(std::max(woff, 1), o);
   P.ww_sp = dev_alloc<int>((size_t)std::max(woff, 1) * nch_alloc, o);
   // FP64 records on every step of the FP64 engine and on the mixed engine's
   // energy steps, whose FP64 water-water kernel stages the mixed chunk size
   // (up to 2368 waters x 80 bytes)
   P.wrec = dev_alloc<float4>((size_t)std::max(woff, 1) * WatRec<false>::words, o);
+  P.wrec32 = B.opt.precision == QB_MIXED ? dev_alloc<float4>((size_t)std::max(woff, 1) * WatRec<true>::words, o)
+                                         : nullptr;
   // the limits (not allocations) cover every chunk size any batch may use
   const int smem64 = std::max(WW_STAGE_BYTES, P.ww_chunk * WatRec<false>::words * 16);
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem64));
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem64));
+  CUDA_TRY(cudaFuncSetAttribute(k_nb_ww<false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem64));
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
   CUDA_TRY(cudaFuncSetAttribute(k_nb_ww_x2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, WW_STAGE_BYTES));
   P.kin_nblk = std::max(1, (B.max_natom + KIN_BLOCK - 1) / KIN_BLOCK);

@@ -114,6 +114,7 @@ struct DevPtrs {
   // atoms
   double4 *x, *v, *xx, *d;
   float4 *wrec;              // per-water position records of the water-water kernel
+  float4 *wrec32;            // their FP32 form (mixed engine): the packed and FP32 water-water kernels'
   double *wtheta;            // per water: dipole angle of the polarisation restraint
   int8_t *wshell;            // per water: polarisation shell (-1: none)
   int *wrank;                // per water: rank in its shell
@@ -184,6 +185,7 @@ struct DevPtrs {
   int4 *qp;                                // gq, j, lj, qlj
   int *qw;                                 // water O atoms
   uint16_t *ww;                            // [gw*ww_cap + k] local water index
+  int *ww_mid;                             // per water: list entries below its own index (ascending lists)
   int *lf_atoms, n_lf;
   // blocks of the per-water kernels, (system, first index) each, only where
   // a system has work: the water pass (256 waters or solute atoms), the

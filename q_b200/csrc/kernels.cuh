@@ -661,7 +661,8 @@ __global__ void __launch_bounds__(LRFX_BLOCK, 4) k_lrf_gather_x2(DevPtrs P, int 
 // sphere whose O lies within Rcww of i's O, as local water indices in
 // ascending order.  ww_sp[gw*ww_nch + c] counts the entries below the end of
 // force-kernel chunk c (chunks of ww_chunk waters, a multiple of 32), so the
-// force kernel finds each chunk's slice of the list directly.
+// force kernel finds each chunk's slice of the list directly; ww_mid[gw]
+// counts the entries below i itself.
 // Block = WL_WPB waters of one system, one warp per water at a time; the
 // system's O positions are staged in shared memory WL_STAGE waters at a time
 // in FP32, relative to the solvent centre (w = -1 for excluded waters), and
@@ -765,6 +766,10 @@ __global__ void __launch_bounds__(WL_BLOCK) k_list_ww(DevPtrs P, int force) {
             const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
             if (pos < P.ww_cap) out[pos] = (uint16_t)(base + lane);
           }
+          // the entries below water i itself: the half of its list with j > i
+          // starts there
+          if (lane == 0 && iw >= base && iw < base + 32)
+            P.ww_mid[gw] = min(cnt + __popc(bal & ((1u << (iw - base)) - 1u)), P.ww_cap);
           cnt += __popc(bal);
         }
       }
@@ -780,8 +785,10 @@ __global__ void __launch_bounds__(WL_BLOCK) k_list_ww(DevPtrs P, int force) {
     int *sp = P.ww_sp + (size_t)gw * P.ww_nch;
     if (cnt > P.ww_cap) { set_status(&P.st[s], QB_ERR_LIST_OVERFLOW); cnt = P.ww_cap; }
     P.ww_n[gw] = cnt;
-    if (cnt == 0)
+    if (cnt == 0) {
       for (int c = 0; c < P.ww_nch; c++) sp[c] = 0;
+      P.ww_mid[gw] = 0;
+    }
     for (int c = (S.nwat - 1) / P.ww_chunk; c < P.ww_nch; c++) sp[c] = cnt;
   }
 }
@@ -1226,8 +1233,12 @@ __device__ __forceinline__ void unpack_mixed(const float4 *r, float *v) {
 // from both sides, energies halved.  Mixed precision: pair terms in FP32
 // (MUFU rsqrt), each lane's energy over one water's list slice summed in FP32 and accumulated in
 // FP64, gradients reduced in FP32.
-template <bool MIXED, bool HLJ>
+// EONCE (FP64 only): the energies alone, each unordered pair once (the list
+// entries above ww_mid, j > i) and not halved; the mixed engine's recording
+// steps take these beside the packed kernel's forces.
+template <bool MIXED, bool HLJ, bool EONCE = false>
 __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P, int wpb) {
+  static_assert(!(MIXED && EONCE), "energies-only form is FP64");
   extern __shared__ float4 wsm[];
   __shared__ int2 srange[WW_WPB];          // list slice of each of the block's waters in this chunk
   constexpr int W = WatRec<MIXED>::words;
@@ -1240,7 +1251,7 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P, in
   const int i1 = min(i0 + wpb, S.nwat);
   const int hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
   const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
-  const float4 *rec = P.wrec + (size_t)S.woff * W;
+  const float4 *rec = (MIXED ? P.wrec32 : P.wrec) + (size_t)S.woff * W;
   const int CW = P.ww_chunk;
   const int nch = (S.nwat + CW - 1) / CW;
   const float qo = S.crg_ow, qh = S.crg_hw;
@@ -1255,7 +1266,9 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P, in
     for (int t = threadIdx.x; t < cn * W; t += WW_BLOCK) wsm[t] = rec[(size_t)c0 * W + t];
     for (int t = threadIdx.x; t < i1 - i0; t += WW_BLOCK) {
       const int *sp = P.ww_sp + (size_t)(S.woff + i0 + t) * P.ww_nch;
-      srange[t] = make_int2(c == 0 ? 0 : sp[c - 1], sp[c]);
+      int lo = c == 0 ? 0 : sp[c - 1];
+      if (EONCE) lo = max(lo, P.ww_mid[S.woff + i0 + t]);
+      srange[t] = make_int2(lo, sp[c]);
     }
     __syncthreads();
     // first list entry of the half-warp's next water, fetched one water ahead
@@ -1345,21 +1358,23 @@ __global__ void __launch_bounds__(WW_BLOCK, MIXED ? 2 : 1) k_nb_ww(DevPtrs P, in
           }
           ww_pair_f64<HLJ>(xi, xj, qoo, qoh, qhh, ljd, fd, el, vdw);
         }
+        if (!EONCE) {
 #pragma unroll
-        for (int q = 0; q < 9; q++) {
+          for (int q = 0; q < 9; q++) {
 #pragma unroll
-          for (int o = 8; o > 0; o >>= 1) fd[q] += __shfl_xor_sync(hmask, fd[q], o);
+            for (int o = 8; o > 0; o >>= 1) fd[q] += __shfl_xor_sync(hmask, fd[q], o);
+          }
         }
       }
       // fire-and-forget adds: the half-warp does not wait for the gradient
-      if (hl == 0) {
+      if (!EONCE && hl == 0) {
 #pragma unroll
         for (int a = 0; a < 3; a++) atomic_add3(P.d, oi + a, fd[3 * a], fd[3 * a + 1], fd[3 * a + 2]);
       }
     }
   }
-  warp_add(&P.E[s * QB_NE + QB_E_WW_EL], 0.5 * el);
-  warp_add(&P.E[s * QB_NE + QB_E_WW_VDW], 0.5 * vdw);
+  warp_add(&P.E[s * QB_NE + QB_E_WW_EL], EONCE ? el : 0.5 * el);
+  warp_add(&P.E[s * QB_NE + QB_E_WW_VDW], EONCE ? vdw : 0.5 * vdw);
 }
 
 // ----------------------------------------------- packed FP32x2 water-water
@@ -1454,7 +1469,7 @@ __global__ void __launch_bounds__(WWX_BLOCK, 2) k_nb_ww_x2(DevPtrs P, int wpb) {
   const int i1 = min(i0 + wpb, S.nwat);
   const int hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
   const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
-  const float4 *rec = P.wrec + (size_t)S.woff * W;
+  const float4 *rec = P.wrec32 + (size_t)S.woff * W;
   const int CW = P.ww_chunk;
   const int nch = (S.nwat + CW - 1) / CW;
   const float qo = S.crg_ow, qh = S.crg_hw;
@@ -2264,6 +2279,27 @@ __global__ void k_atom_terms(DevPtrs P) {
   warp_add(&P.E[s * QB_NE + QB_E_RST_SOLVENT_RADIAL], erad);
 }
 
+// The water-water kernels' records of water gw: FP64 (x y z of O, H1, H2)
+// in wrec for the FP64 kernel; FP32 (O as hi + lo, H offsets from O) in
+// wrec32 for the packed and FP32 kernels of the mixed engine, whose FP64
+// pass (its energy-recording steps) writes both.
+template <bool MIXED>
+__device__ __forceinline__ void put_wat_records(const DevPtrs &P, int gw, double4 a, double4 b, double4 c) {
+  if (MIXED || P.wrec32) {
+    float4 *r = P.wrec32 + (size_t)gw * WatRec<true>::words;
+    float hx = (float)a.x, hy = (float)a.y, hz = (float)a.z;
+    float lx = (float)(a.x - (double)hx), ly = (float)(a.y - (double)hy), lz = (float)(a.z - (double)hz);
+    r[0] = make_float4(hx, hy, hz, lx);
+    r[1] = make_float4(ly, lz, (float)(b.x - a.x), (float)(c.x - a.x));
+    r[2] = make_float4((float)(b.y - a.y), (float)(c.y - a.y), (float)(b.z - a.z), (float)(c.z - a.z));
+  }
+  if (!MIXED) {
+    double2 *rd = reinterpret_cast<double2 *>(P.wrec + (size_t)gw * WatRec<false>::words);
+    rd[0] = make_double2(a.x, a.y); rd[1] = make_double2(a.z, b.x); rd[2] = make_double2(b.y, b.z);
+    rd[3] = make_double2(c.x, c.y); rd[4] = make_double2(c.z, 0.0);
+  }
+}
+
 // Water pass, one thread per water, the step's first force kernel: the
 // position record of the water-water kernel (see WatRec), the polarisation
 // angle and shell, and the per-atom terms of its three atoms (water_terms),
@@ -2281,19 +2317,7 @@ __global__ void k_pack_waters(DevPtrs P) {
     int o = S.aoff + S.nsol + 3 * iw;
     double4 a = P.x[o], b = P.x[o + 1], c = P.x[o + 2];
     if (S.wpol && S.nshell > 0) watpol_angle(P, S, S.woff + iw, (P.flags[o] & F_EXCL) != 0, a, b, c);
-    constexpr int W = WatRec<MIXED>::words;
-    float4 *r = P.wrec + (size_t)(S.woff + iw) * W;
-    if (MIXED) {
-      float hx = (float)a.x, hy = (float)a.y, hz = (float)a.z;
-      float lx = (float)(a.x - (double)hx), ly = (float)(a.y - (double)hy), lz = (float)(a.z - (double)hz);
-      r[0] = make_float4(hx, hy, hz, lx);
-      r[1] = make_float4(ly, lz, (float)(b.x - a.x), (float)(c.x - a.x));
-      r[2] = make_float4((float)(b.y - a.y), (float)(c.y - a.y), (float)(b.z - a.z), (float)(c.z - a.z));
-    } else {
-      double2 *rd = reinterpret_cast<double2 *>(r);
-      rd[0] = make_double2(a.x, a.y); rd[1] = make_double2(a.z, b.x); rd[2] = make_double2(b.y, b.z);
-      rd[3] = make_double2(c.x, c.y); rd[4] = make_double2(c.z, 0.0);
-    }
+    put_wat_records<MIXED>(P, S.woff + iw, a, b, c);
     const double3 x[3] = {make_double3(a.x, a.y, a.z), make_double3(b.x, b.y, b.z), make_double3(c.x, c.y, c.z)};
     double g[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     water_terms(P, S, s, o, x, g, elrf, efix, eshell, erad);
@@ -2325,22 +2349,7 @@ __global__ void k_pack_water_atoms(DevPtrs P) {
     const double3 xa = make_double3(xa4.x, xa4.y, xa4.z);
     if (a == 1 && S.wpol && S.nshell > 0)
       watpol_angle(P, S, S.woff + iw, (P.flags[o] & F_EXCL) != 0, P.x[o], xa4, P.x[o + 2]);
-    if (a == 2) {
-      const double4 A = P.x[o], B = P.x[o + 1], C = xa4;
-      constexpr int W = WatRec<MIXED>::words;
-      float4 *r = P.wrec + (size_t)(S.woff + iw) * W;
-      if (MIXED) {
-        float hx = (float)A.x, hy = (float)A.y, hz = (float)A.z;
-        float lx = (float)(A.x - (double)hx), ly = (float)(A.y - (double)hy), lz = (float)(A.z - (double)hz);
-        r[0] = make_float4(hx, hy, hz, lx);
-        r[1] = make_float4(ly, lz, (float)(B.x - A.x), (float)(C.x - A.x));
-        r[2] = make_float4((float)(B.y - A.y), (float)(C.y - A.y), (float)(B.z - A.z), (float)(C.z - A.z));
-      } else {
-        double2 *rd = reinterpret_cast<double2 *>(r);
-        rd[0] = make_double2(A.x, A.y); rd[1] = make_double2(A.z, B.x); rd[2] = make_double2(B.y, B.z);
-        rd[3] = make_double2(C.x, C.y); rd[4] = make_double2(C.z, 0.0);
-      }
-    }
+    if (a == 2) put_wat_records<MIXED>(P, S.woff + iw, P.x[o], P.x[o + 1], xa4);
     double g[3] = {0, 0, 0};
     const uint8_t fo = P.flags[o], fl = P.flags[i];
     if (S.use_lrf && !((fo & P.flags[o + 1] & P.flags[o + 2]) & F_EXCL) && !(fl & F_EXCL) && P.iq[i] < 0) {

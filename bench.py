@@ -543,6 +543,8 @@ def main():
     # records a run of --steps steps can hold: output and energy-file intervals
     max_rec = [args.steps // max(1, min(v.iout_cycle for v in views)) + 2,
                args.steps // max(1, min(v.iene_cycle for v in views)) + 2]
+    from q_b200.api import HIST_REC
+    recbuf = [pinned(len(views) * m * HIST_REC) for m in max_rec]
     reps = []
     for _ in range(3):
         barrier()
@@ -554,7 +556,8 @@ def main():
         t2 = time.perf_counter()
         d2h = 0
         for kind in (0, 1):
-            counts, rec, nbytes = batch.history_all(kind, max_records=max_rec[kind], with_bytes=True)
+            counts, rec, nbytes = batch.history_all(kind, max_records=max_rec[kind], with_bytes=True,
+                                                    out=recbuf[kind])
             d2h += nbytes
         batch.coords_all(xout)
         d2h += 24 * natoms                  # x y z per atom

@@ -185,12 +185,15 @@ class Batch:
         assert v.size == 3 * self.natom_total
         check(lib.qb_batch_set_velocities_all(self._b, _dp(v)))
 
-    def history_all(self, kind: int = 0, max_records: int | None = None, with_bytes: bool = False):
+    def history_all(self, kind: int = 0, max_records: int | None = None, with_bytes: bool = False,
+                    out: np.ndarray | None = None):
         """(counts[nsys], records[nsys, m, QB_HIST_REC]) of every system in
         two device copies; a record is step, E[QB_NE], EQ[QB_MAX_STATES,
         QB_NEQ], r_kl[QB_MAX_STATES].  With max_records None the counts are
         queried first (one more copy).  with_bytes adds the bytes the call
-        copied from the device."""
+        copied from the device.  `out` (float64, C order, at least nsys x
+        max_records x QB_HIST_REC values, e.g. a page-locked buffer) receives
+        the records instead of a new array."""
         n = len(self.systems)
         counts = np.zeros(n, dtype=np.int32)
         ip = counts.ctypes.data_as(C.POINTER(C.c_int))
@@ -201,7 +204,11 @@ class Batch:
             total += nb.value
             max_records = int(counts.max(initial=0))
         m = max(int(max_records), 1)
-        rec = np.zeros((n, m, HIST_REC))
+        if out is None:
+            rec = np.zeros((n, m, HIST_REC))
+        else:
+            assert out.dtype == np.float64 and out.flags.c_contiguous and out.size >= n * m * HIST_REC
+            rec = out.reshape(-1)[:n * m * HIST_REC].reshape(n, m, HIST_REC)
         check(lib.qb_batch_history_all(self._b, kind, m, ip, _dp(rec), C.byref(nb)))
         total += nb.value
         m = int(counts.max(initial=0))

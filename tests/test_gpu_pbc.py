@@ -31,7 +31,7 @@ def boxes(tmp_path_factory):
         "rst": synth.fep_box(str(root / "rst"), edge=EDGE, seed=1234,
                              distance_restraints=["1 20 2.0 4.0 5.0 0", "3 40 1.0 2.0 5.0 0"]),
         # restraints reaching water atoms (atoms 100 and 301: waters after the
-        # 56 solute atoms): the solute terms then run after the water pass
+        # 56 solute atoms), whose gradient the water pass stores first
         "rst_water": synth.fep_box(str(root / "rst_water"), edge=EDGE, seed=1234,
                                    distance_restraints=["1 100 2.0 4.0 5.0 0", "5 301 1.0 2.0 5.0 0"]),
     }
